@@ -1,0 +1,393 @@
+"""Benchmark of the 2D active multi-phase-field step on B200.
+
+Workload (one GPU): 2D periodic lattice 2048 x 2048, 1024 cells of radius
+R = 12, centres from the sequential periodic initialiser with minimum
+separation 2R, tanh-disk seeds, reference default coefficients, binary32 phi
+with the exact Q5.27 aggregate. A "step" is one time step of every cell (one
+fused kernel launch). Throughput is site-cell updates/s counted over the
+reference's window (144^2 sites per class-0 cell).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl pfb|reference]
+
+Multi-GPU: one process per GPU (torchrun); every rank runs an independent
+replica of the workload with its own seed (the path has no exchange step), so
+scaling is weak and the value is the total over ranks divided by the slowest
+rank's device time.
+
+``--impl reference`` times the reference's algorithm on the host cores: the
+reference has no CPU solver, so this is the OpenMP restatement in oracle/
+(the same code as the ``cpu_baseline`` leg), run on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "phase-field-gh200_b200"))
+
+L_SIDE = 2048
+N_CELLS = 1024
+RADIUS = 12.0
+WORKLOAD = ("2D periodic 2048x2048, 1024 cells R=12, min-separation 2R sequential centres, "
+            "tanh disks, default coefficients (dt=0.01, lambda=7, kappa=10, mu=1, xi=1500, "
+            "tau=1e4, v_A=0.01, M=0.5), f32 phi, Q5.27 aggregate")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def rank_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def workload_params(seed: int):
+    import pfb200
+    return pfb200.SimParams2D(L=L_SIDE, num_cells=N_CELLS, target_radius=RADIUS, seed=seed)
+
+
+def workload_centres(p):
+    import pfb200
+    return pfb200.palmieri_centres(p.num_cells, p.L, 2.0 * p.target_radius, p.seed)
+
+
+def sites_per_step(cells) -> int:
+    import pfb200
+    return int(sum(pfb200.CLASSES[0][0] * pfb200.CLASSES[0][1] for _ in range(len(cells))))
+
+
+def algorithmic_bytes(cells, L: int) -> int:
+    """sum_n A_n * 2 * 4 B (read phi^n + write phi^{n+1} over the processed
+    window) + L^2 * 8 B (one read and one write of the u32 aggregate)."""
+    import pfb200
+    area = sum(pfb200.CLASSES[int(c)][0] * pfb200.CLASSES[int(c)][1] for c in cells["cls"])
+    return int(area * 8 + L * L * 8)
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+
+    QUERY = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.lines: list[str] = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-i", str(self.device), "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def mark(self):
+        return len(self.lines)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+
+    def summary(self, start: int, end: int) -> dict:
+        rows = []
+        for ln in self.lines[start:end] or self.lines[-3:]:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) >= 8:
+                rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[4 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][1]) if rows[0][1].replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def read_peak_hbm():
+    f = REPO / "MEASURED_PEAKS.json"
+    try:
+        d = json.loads(f.read_text())
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback 6.65 TB/s"
+
+
+def read_ncu_traffic():
+    """DRAM bytes per launch of the step kernel from the committed ncu summary
+    of the same workload (profiles/k_step2d_c2.md), or None."""
+    f = REPO / "profiles" / "k_step2d_c2.md"
+    if not f.exists():
+        return None
+    for ln in f.read_text().splitlines():
+        if ln.startswith("dram_bytes_per_launch:"):
+            try:
+                return int(float(ln.split(":", 1)[1].split()[0]))
+            except ValueError:
+                return None
+    return None
+
+
+def cpu_sample(cells, phi, p, steps: int, threads: int):
+    """Time the oracle's OpenMP restatement on a bounded sample of the same
+    workload; returns (site-cell updates/s, seconds, threads)."""
+    sys.path.insert(0, str(REPO / "oracle"))
+    import oracle2d
+    if threads <= 0:
+        threads = os.cpu_count() or 1
+    o = oracle2d.OracleSim(p.to_c(), cells, phi, step=0)
+    o.advance(1, threads)  # warm the caches and the thread pool
+    t0 = time.perf_counter()
+    o.advance(steps, threads)
+    dt = time.perf_counter() - t0
+    o.close()
+    return sites_per_step(cells) * steps / dt, dt, threads
+
+
+def run_reference_arm(a):
+    """Reference arm: the reference's update on the host cores. The reference
+    has no CPU solver, so this is the OpenMP restatement of its update in
+    oracle/. Each bench step is one time step of a subset of the workload's
+    cells (same lattice), sized so the whole run stays within about a minute;
+    throughput is per site-cell, so the subset does not change the rate."""
+    rank, world, _ = rank_env()
+    if rank != 0:
+        return 0
+    p = workload_params(1234)
+    cx, cy = workload_centres(p)
+    sys.path.insert(0, str(REPO / "oracle"))
+    import oracle2d
+    cells, phi = oracle2d.init_state(p.to_c(), cx, cy, _fresh_cells(p))
+    threads = os.cpu_count() or 1
+    full = oracle2d.OracleSim(p.to_c(), cells, phi, step=0)
+    t0 = time.perf_counter()
+    full.advance(1, threads)
+    t_full = time.perf_counter() - t0
+    full.close()
+    budget = float(os.environ.get("PFB_REF_BUDGET_S", "60"))
+    m = int(max(1, min(p.num_cells, p.num_cells * budget / (max(1, a.steps) * t_full))))
+    ps = workload_params(1234)
+    ps.num_cells = m
+    sub = oracle2d.OracleSim(ps.to_c(), cells[:m].copy(), phi[:m].copy(), step=0)
+    for _ in range(min(a.warmup, 3)):
+        sub.advance(1, threads)
+    times = []
+    for _ in range(a.steps):
+        t0 = time.perf_counter()
+        sub.advance(1, threads)
+        times.append(time.perf_counter() - t0)
+    sub.close()
+    tot = sum(times)
+    value = sites_per_step(cells[:m]) * a.steps / tot
+    sample = (f"one time step of {m} of the {p.num_cells} cells (same 2048^2 lattice) per "
+              f"bench step; a full step took {t_full:.2f} s on {threads} threads")
+    line = {
+        "impl": "reference", "metric": "site-cell updates/s", "value": value,
+        "unit": "site-cell updates/s", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1000.0 * tot / a.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "L": L_SIDE, "cells": N_CELLS,
+                   "implementation": "CPU OpenMP restatement of the reference update (oracle/)"},
+        "cpu_baseline": {"value": value, "unit": "site-cell updates/s", "cores": threads,
+                         "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "site-cell updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _fresh_cells(p):
+    import pfb200
+    from pfb200 import CELL_DTYPE
+    L = pfb200.lib()
+    cells = np.zeros(p.num_cells, CELL_DTYPE)
+    pstream = p.polarity_seed or p.seed
+    for i in range(p.num_cells):
+        cells[i]["global_id"] = i
+        cells[i]["gamma"] = p.gamma_normal
+        cells[i]["v_A"] = L.pfb_ic_v_A(i, p.seed, p.v_A, p.v_A_sigma)
+        cells[i]["M_pf"] = p.phase_field_mobility
+        cells[i]["R_tgt"] = p.target_radius
+        cells[i]["theta"] = L.pfb_ic_theta(i, pstream)
+    return cells
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=6000)
+    ap.add_argument("--warmup", type=int, default=60)
+    ap.add_argument("--impl", default="pfb", choices=["pfb", "reference"])
+    ap.add_argument("--cluster", type=int, default=4)
+    ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=int(os.environ.get("PFB_CPU_STEPS", "6")))
+    ap.add_argument("--no-e2e", action="store_true")
+    a = ap.parse_args()
+    if a.warmup < 3:
+        a.warmup = 3
+    if a.impl == "reference":
+        return run_reference_arm(a)
+
+    import torch
+    import pfb200
+
+    rank, world, local = rank_env()
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    device = local
+    torch.cuda.set_device(device)
+
+    p = workload_params(1234 + rank)
+    cx, cy = workload_centres(p)
+    sim = pfb200.Sim2D(p, cx, cy, device=device, cluster=a.cluster, use_graph=not a.no_graph)
+    init_cells = sim.cells()
+    init_phi = sim.phi() if (rank == 0 and world == 1) or not a.no_e2e else None
+    alg = algorithmic_bytes(init_cells, p.L)
+    sites = sites_per_step(init_cells)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(device)
+
+    ext = torch.cuda.ExternalStream(sim.stream, device=device)
+    clocks = ClockSampler(device)
+    clocks.start()
+    time.sleep(0.3)
+
+    sim.advance(a.warmup)
+    sim.sync()
+    barrier()
+    m0 = clocks.mark()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    sim.advance(a.steps)
+    e1.record(ext)
+    sim.sync()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    time.sleep(0.15)
+    m1 = clocks.mark()
+    if dist is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    flags = sim.flags()
+    final_cells = sim.cells()
+    value = world * sites * a.steps / (ms / 1000.0)
+    ms_step = ms / a.steps
+
+    # ---- end to end through the public API with host buffers -------------
+    e2e = None
+    if not a.no_e2e:
+        pin_cells = torch.from_numpy(init_cells.view(np.uint8).copy()).pin_memory()
+        pin_phi = torch.from_numpy(init_phi).pin_memory() if init_phi is not None else None
+        traj = torch.empty((p.num_cells, 48), dtype=torch.uint8).pin_memory()
+        phi_out = torch.empty((p.num_cells, 288, 288), dtype=torch.float32).pin_memory()
+        from pfb200._abi import check, lib
+        L = lib()
+        e2e_steps = a.steps
+        barrier()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(ext)
+        check(L.pfb_sim2d_set_state(sim._h, pin_cells.data_ptr(), pin_phi.data_ptr(), 0),
+              "set_state")
+        for _ in range(e2e_steps):
+            check(L.pfb_sim2d_advance(sim._h, 1), "advance")
+            check(L.pfb_sim2d_pack_traj(sim._h, traj.data_ptr()), "pack_traj")
+        check(L.pfb_sim2d_get_phi(sim._h, phi_out.data_ptr()), "get_phi")
+        f1.record(ext)
+        sim.sync()
+        barrier()
+        el = f0.elapsed_time(f1) / 1000.0
+        if dist is not None:
+            t = torch.tensor([el], dtype=torch.float64, device=f"cuda:{device}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        h2d = pin_cells.numel() + pin_phi.numel() * 4
+        d2h = traj.numel() * e2e_steps + phi_out.numel() * 4
+        e2e = {"value": world * sites * e2e_steps / el, "unit": "site-cell updates/s",
+               "h2d_bytes_per_step": h2d / e2e_steps, "d2h_bytes_per_step": d2h / e2e_steps,
+               "steps": e2e_steps,
+               "note": "state uploaded from pinned host memory once, per-step trajectory "
+                       "record read back every step (graph disabled by the per-step "
+                       "readback), final phi pool read back"}
+    clocks.stop()
+
+    if rank == 0:
+        peak, peak_src = read_peak_hbm()
+        achieved = alg / (ms_step / 1000.0) / 1e9
+        traffic = read_ncu_traffic()
+        cpu = None
+        if world == 1 and a.cpu_steps > 0:
+            v, dt, thr = cpu_sample(init_cells, init_phi, p, a.cpu_steps, 0)
+            cpu = {"value": v, "unit": "site-cell updates/s", "cores": thr, "kind": "port",
+                   "sample": f"{a.cpu_steps} full time steps of the same workload "
+                             f"({dt:.1f} s) on the OpenMP restatement of the update"}
+        line = {
+            "metric": "site-cell updates/s", "value": value, "unit": "site-cell updates/s",
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "L": L_SIDE, "cells": N_CELLS, "radius": RADIUS,
+                       "sites_per_step": sites, "window": "reference class-0 window 144^2",
+                       "cluster_ctas_per_cell": a.cluster, "cuda_graph": not a.no_graph,
+                       "l2": "inputs larger than L2: two 340 MB phi pools; per-step working "
+                             "set 85 MB phi read + 85 MB phi written + 3 x 16.8 MB aggregate "
+                             "slots; no flush between steps",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "pfb::k_step2d<4>", "algorithmic_bytes_per_launch": alg,
+                         "peak_source": peak_src,
+                         "duration_source": "CUDA events over the timed region / steps"},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "clocks": clocks.summary(m0, m1),
+            "gpu_launches": a.steps,
+            "flags": pfb200.flags_report(flags),
+            "cells_class_histogram": np.bincount(final_cells["cls"], minlength=6).tolist(),
+        }
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

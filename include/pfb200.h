@@ -1,0 +1,323 @@
+/*
+ * pfb200.h -- C ABI of the B200-native active multi-phase-field cell update.
+ *
+ * Every entry point takes plain pointers and sizes. The two records below are
+ * byte-for-byte the records the reference passes between its host driver and
+ * its 2D step kernel, so a caller that already owns those buffers (the
+ * reference's `Sim`, or a checkpoint loader) can hand them over unchanged:
+ *
+ *   pfb_cell2d       == pf::CellState   (reference include/kernels.cuh:27-57)
+ *   pfb_step_args2d  == pf::StepArgs    (reference include/kernels.cuh:74-116)
+ *
+ * Conventions (reference include/kernels.cuh:219-225, src/sim.cu:207-230):
+ *   - the caller owns every device buffer; no launcher allocates;
+ *   - launchers return 0 on success and a negative PFB_E* code when the launch
+ *     contract is violated (the reference 3D launchers return false in the same
+ *     situations, src/pf3d/kernels.cu:2747-2787);
+ *   - numerical failures never abort a kernel: they raise the sticky u32
+ *     counters of the `flags` array (PFB_FLAG_*), exactly as the reference does
+ *     (include/params.cuh:433-495);
+ *   - all work is issued on the caller's stream; nothing synchronises.
+ */
+#ifndef PFB200_H
+#define PFB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define PFB_OK 0
+#define PFB_E_ARG (-1)        /* null pointer, bad size or alignment       */
+#define PFB_E_CUDA (-2)       /* a CUDA runtime call failed                */
+#define PFB_E_CONFIG (-3)     /* unsupported configuration (e.g. cluster)  */
+#define PFB_E_STATE (-4)      /* object used in the wrong state            */
+#define PFB_E_NOMEM (-5)      /* host or device allocation failed          */
+
+/* ---- sticky device flags (indices into the u32 flags[8] array) -------
+ * reference include/params.cuh:434-445. All but SUPPORT_CLIP are fatal. */
+#define PFB_FLAG_S_OVERFLOW 0
+#define PFB_FLAG_Q_CLAMP 1
+#define PFB_FLAG_SUPPORT_CLIP 2
+#define PFB_FLAG_CLASS_EXHAUSTED 3
+#define PFB_FLAG_S_NEGATIVE 4
+#define PFB_FLAG_NONFINITE 5
+#define PFB_FLAG_V_NONPOS 6
+#define PFB_FLAG_CLASS_UNSUPPORTED 7
+#define PFB_FLAG_COUNT 8
+
+/* ---- fixed 2D tile geometry (reference include/params.cuh:121-147) ---- */
+#define PFB_TILE_PITCH 288
+#define PFB_TILE_AREA (288 * 288)
+#define PFB_NUM_CLASSES 6
+
+/* Runtime velocity-observer accumulator carried inside the cell record
+ * (reference common/velocity_moments.h:24-27). Unused by the disabled
+ * observation path; kept for layout identity. */
+typedef struct pfb_advection_accum {
+    double q[6];
+    unsigned long long count;
+} pfb_advection_accum;
+
+/* Per-cell state, 192 B, 64-B aligned (reference include/kernels.cuh:27-57). */
+typedef struct pfb_cell2d {
+    int32_t gx0, gy0;          /* global coords of window pixel (0,0)   */
+    uint8_t cls;               /* shape class of the field to be read   */
+    uint8_t cls_written[2];    /* class last written into phi[parity]   */
+    uint8_t pad0;
+    int32_t global_id;         /* Philox key; stable across reordering  */
+    float gamma, v_A, R_tgt;
+    float theta;               /* polarity angle                        */
+    double V;                  /* sum phi^2 of the field to be read     */
+    double Cx, Cy;             /* sum phi^2 x, sum phi^2 y (window)     */
+    double perim;              /* full-moment steps only                */
+    int32_t bb_lo_x, bb_hi_x, bb_lo_y, bb_hi_y;
+    float vx, vy;
+    double Ix, Iy;             /* interaction integral                  */
+    uint32_t promote_ctr;
+    uint32_t shift_ctr;
+    uint32_t tumble_ctr;
+    float phi_max;
+    uint32_t reserved[2];      /* [0] fallback used, [1] no-margin steps */
+    pfb_advection_accum advection;
+    uint32_t reserved_unused;
+    float M_pf;                /* passive Allen-Cahn mobility           */
+}
+#if defined(__GNUC__) || defined(__CUDACC__)
+__attribute__((aligned(64)))
+#endif
+pfb_cell2d;
+
+/* Arguments of one 2D step launch (reference include/kernels.cuh:74-116).
+ * Step counters and cursors are device-resident so a captured CUDA graph can
+ * be replayed; `perm` may be null (identity order); `moments` must be null
+ * (the spatial observer specialisations are not part of this library). */
+typedef struct pfb_step_args2d {
+    const float* phi_in;
+    float* phi_out;
+    const uint32_t* S_rd;
+    uint32_t* S_sc;
+    uint32_t* S_cl;
+    pfb_cell2d* cell;
+    uint8_t* cell_cls;
+    const uint32_t* perm;
+    unsigned long long* cursor_use;
+    unsigned long long* cursor_clear;
+    const unsigned long long* step_rd;
+    unsigned long long* step_wr;
+    uint32_t* flags;
+    void* moments;
+    double physical_dt;
+    int N;
+    int L;
+    int P;
+    int parity_out;
+    float dt;
+    double A0;
+    double vol_scale;
+    float bulk_scale;
+    float rep_coeff;
+    float mot_coeff;
+    unsigned long long seed;
+    unsigned long long polarity_seed;
+    double p_tumble;
+    int full_moment_every;
+    unsigned long long clear_ahead_words;
+} pfb_step_args2d;
+
+/* Simulation parameters (reference include/params.cuh:499-530, SimParams),
+ * as plain C. Only the fields the update consumes are carried. */
+typedef struct pfb_params2d {
+    int L;                        /* domain side (Nx == Ny)                */
+    int num_cells;
+    double dt;
+    double lambda;
+    double target_radius;
+    double kappa;
+    double mu;
+    double xi;
+    double tau;
+    double v_A;
+    double gamma_normal;
+    double gamma_cancer;
+    double cancer_fraction;
+    double v_A_sigma;
+    double phase_field_mobility;
+    unsigned long long seed;
+    unsigned long long polarity_seed; /* 0 follows seed                  */
+    int full_moment_every;
+} pfb_params2d;
+
+/* Compact trajectory record (reference include/kernels.cuh:60-70). */
+typedef struct pfb_traj_cell2d {
+    int32_t global_id;
+    int32_t cls;
+    float cx, cy;
+    float vx, vy;
+    float theta;
+    float volume;
+    float perim;
+    float gamma, v_A;
+    float phi_max;
+} pfb_traj_cell2d;
+
+/* ======================================================================
+ * Library information
+ * ==================================================================== */
+
+/* Version string of this library. */
+const char* pfb_version(void);
+/* Text of the last error raised on the calling host thread ("" if none). */
+const char* pfb_last_error(void);
+/* sizeof() of the ABI records, for binding-layer layout checks:
+ * which = 0 cell2d, 1 step_args2d, 2 params2d, 3 traj_cell2d. */
+size_t pfb_sizeof(int which);
+
+/* ======================================================================
+ * 2D step -- replaces pf::launch_step / configure_k_step_smem / k_step_grid
+ * (reference include/kernels.cuh:219-225, src/kernels.cu:1304-1363)
+ * ==================================================================== */
+
+/* Configure the dynamic shared-memory opt-in of every step kernel on the
+ * current device. Idempotent; called implicitly by pfb_step2d_launch. */
+int pfb_step2d_configure(void);
+
+/* Number of CTAs the step launch uses for N cells with `cluster` CTAs per
+ * cell (cluster = 0 selects the default). Replaces k_step_grid(). */
+int pfb_step2d_grid(int num_cells, int cluster);
+
+/* One full step for every cell: tumble, interaction integral, Euler update,
+ * recentring store, Q5.27 scatter into S_sc, FP64 moments, and clearing of
+ * S_cl (clear_ahead_words words). `cluster` is the number of CTAs that
+ * cooperate on one cell (2, 4 or 8; 0 = default 4).
+ * Returns PFB_E_ARG for a null buffer, a misaligned phi pool (16 B), L not
+ * larger than 286, or a non-null `moments`. */
+int pfb_step2d_launch(const pfb_step_args2d* args, int cluster, void* stream);
+
+/* Library status word kept in device memory: bit 0 is set when a CTA gave up
+ * waiting for its staged band (a bounded wait that is never expected to run
+ * out). `clear` != 0 resets it after reading. */
+int pfb_device_status(unsigned* out, int clear);
+
+/* ======================================================================
+ * 2D initialisation and diagnostics -- replace k_init_tiles,
+ * k_init_moments, k_scatter_all, k_zero_u32, k_verify_cells, k_verify_S,
+ * k_pack_traj (reference include/kernels.cuh:185-207)
+ * ==================================================================== */
+
+/* Seed tanh disks into the class window of each tile of both pools and set
+ * gx0/gy0/cls/cls_written (reference src/kernels.cu:1050-1094). */
+int pfb_init_tiles2d(float* phi_a, float* phi_b, pfb_cell2d* cell,
+                     const uint8_t* cls, int N, int L, const float* seed_cx,
+                     const float* seed_cy, float radius_eff, float kappa_iface,
+                     void* stream);
+/* V, Cx, Cy, support box and phi_max of each cell's window (reference
+ * src/kernels.cu:1098-1165). */
+int pfb_init_moments2d(pfb_cell2d* cell, const uint8_t* cls, const float* phi,
+                       int N, void* stream);
+/* Build the Q5.27 aggregate S from a phi pool (reference
+ * src/kernels.cu:1167-1190). S must be cleared first. */
+int pfb_scatter_all2d(const float* phi, const pfb_cell2d* cell,
+                      const uint8_t* cls, uint32_t* S, int N, int L, int P,
+                      uint32_t* flags, void* stream);
+/* Clear n words. */
+int pfb_zero_u32(uint32_t* p, size_t n, void* stream);
+/* Recompute each cell's V and the largest |phi| outside its window
+ * (reference src/kernels.cu:1193-1232). */
+int pfb_verify_cells2d(const float* phi, const pfb_cell2d* cell,
+                       const uint8_t* cls, int N, double* out_V,
+                       float* out_outside_max, void* stream);
+/* max over an S buffer into *out_max (must be zeroed by the caller). */
+int pfb_verify_S(const uint32_t* S, size_t n, uint32_t* out_max, void* stream);
+/* Pack per-cell observables (reference src/kernels.cu:1242-1265). */
+int pfb_pack_traj2d(const pfb_cell2d* cell, const uint8_t* cls,
+                    pfb_traj_cell2d* out, int N, int L, void* stream);
+
+/* ======================================================================
+ * Host-side helpers shared with the reference's initialisers
+ * ==================================================================== */
+
+/* Philox4x32-10 (reference common/philox.cuh:32-59). out[4]. */
+void pfb_philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                       uint32_t k0, uint32_t k1, uint32_t* out);
+/* 53-bit uniform from two words (reference common/philox.cuh:62-67). */
+double pfb_philox_uniform53(uint32_t a, uint32_t b);
+/* Q5.27 encoding of phi^2 (reference include/params.cuh:103-111). */
+uint32_t pfb_q_of(float phi);
+/* Sequential periodic placement with minimum separation `min_sep`
+ * (reference include/palmieri_initializer.hpp:66-103). Returns 0 or
+ * PFB_E_ARG; x, y receive n binary32 centres. */
+int pfb_palmieri_centres(int n, double side, double min_sep,
+                         unsigned long long seed, float* x, float* y);
+/* Default grid-and-jitter centres (reference src/sim.cu:107-129). */
+int pfb_grid_jitter_centres(int n, int side, unsigned long long seed, float* x,
+                            float* y);
+/* Initial polarity angle (reference include/kernels.cuh:153-158). */
+float pfb_ic_theta(int32_t gid, unsigned long long stream);
+/* Lognormal per-cell speed (reference include/kernels.cuh:161-172). */
+double pfb_ic_v_A(int32_t gid, unsigned long long seed, double v_A,
+                  double sigma);
+/* Domain side for n cells of radius R at packing rho
+ * (reference include/params.cuh:568-574). */
+int pfb_domain_side_for(int n, double radius, double rho);
+/* Step arguments' coefficients from params (reference src/sim.cu:605-616):
+ * fills dt, A0, vol_scale, bulk_scale, rep_coeff, mot_coeff, seed,
+ * polarity_seed, p_tumble, full_moment_every, physical_dt. */
+int pfb_fill_coefficients2d(const pfb_params2d* p, pfb_step_args2d* a);
+
+/* ======================================================================
+ * Host driver -- the reference's `Sim` (reference include/sim.cuh:58-152)
+ * behind an opaque handle. Owns its device buffers.
+ * ==================================================================== */
+typedef struct pfb_sim2d pfb_sim2d;
+
+/* Allocate device state for params on `device`; centres x/y (n floats) seed
+ * the tanh disks. Returns null on failure (see pfb_last_error). */
+pfb_sim2d* pfb_sim2d_create(const pfb_params2d* p, const float* cx,
+                            const float* cy, int device);
+/* Build from an existing host state (checkpoint-style): cells (N records),
+ * phi (N * 288 * 288 floats holding phi^step), at step `step`. S is rebuilt
+ * on the device. */
+pfb_sim2d* pfb_sim2d_create_from_state(const pfb_params2d* p,
+                                       const pfb_cell2d* cells,
+                                       const float* phi, long long step,
+                                       int device);
+void pfb_sim2d_destroy(pfb_sim2d* s);
+/* Tuning knobs: cluster CTAs per cell (2/4/8) and CUDA-graph use. */
+int pfb_sim2d_set_cluster(pfb_sim2d* s, int cluster);
+int pfb_sim2d_set_graph(pfb_sim2d* s, int use_graph);
+/* Advance `steps` steps on the simulator's stream (asynchronous). */
+int pfb_sim2d_advance(pfb_sim2d* s, long long steps);
+/* Wait for the simulator's stream. */
+int pfb_sim2d_sync(pfb_sim2d* s);
+long long pfb_sim2d_step(const pfb_sim2d* s);
+int pfb_sim2d_side(const pfb_sim2d* s);
+int pfb_sim2d_pitch(const pfb_sim2d* s);
+int pfb_sim2d_num_cells(const pfb_sim2d* s);
+/* Copies (synchronous) of the current state to host memory. */
+int pfb_sim2d_get_cells(pfb_sim2d* s, pfb_cell2d* out);
+int pfb_sim2d_get_phi(pfb_sim2d* s, float* out);      /* N*288*288 floats */
+int pfb_sim2d_get_S(pfb_sim2d* s, uint32_t* out);     /* L*P words       */
+int pfb_sim2d_get_flags(pfb_sim2d* s, uint32_t* out); /* 8 words         */
+/* Replace the whole state from host memory (pinned or pageable) on the
+ * simulator's stream; S is rebuilt from phi. */
+int pfb_sim2d_set_state(pfb_sim2d* s, const pfb_cell2d* cells,
+                        const float* phi, long long step);
+/* Pack the per-cell trajectory record into host memory `out` (N records). */
+int pfb_sim2d_pack_traj(pfb_sim2d* s, pfb_traj_cell2d* out);
+/* Timed benchmark in the manner of Sim::bench (reference src/sim.cu:1006):
+ * `warmup` untimed steps, then `steps` steps timed with CUDA events on the
+ * simulator's stream. Writes ms per step. */
+int pfb_sim2d_bench(pfb_sim2d* s, int warmup, int steps, double* ms_per_step);
+/* Device pointers for callers that drive kernels themselves. */
+int pfb_sim2d_step_args(pfb_sim2d* s, pfb_step_args2d* out);
+void* pfb_sim2d_stream(pfb_sim2d* s);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif /* PFB200_H */

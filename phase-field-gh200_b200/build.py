@@ -1,0 +1,91 @@
+"""Build the sm_100a shared library ``pfb200/_lib/libpfb200.so`` in-tree.
+
+Every CUDA translation unit is compiled with
+``nvcc -gencode arch=compute_100a,code=sm_100a -lineinfo -O3`` and linked with
+the static CUDA runtime, so the library carries no dependency on the CUDA
+runtime that PyTorch loads into the same process. Host code is compiled
+without floating-point contraction (the initialisers' placement must be
+reproducible bit for bit).
+
+Usage: ``python phase-field-gh200_b200/build.py [--force] [--verbose]``.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+CSRC = HERE / "csrc"
+OUT_DIR = HERE / "pfb200" / "_lib"
+OBJ_DIR = HERE / "build" / "obj"
+LIB = OUT_DIR / "libpfb200.so"
+INCLUDE = HERE.parent / "include"
+
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = [
+    "-std=c++17",
+    "-O3",
+    "-lineinfo",
+    "--expt-relaxed-constexpr",
+    "-Xcompiler", "-fPIC,-ffp-contract=off,-Wall",
+    "-I", str(INCLUDE),
+]
+SOURCES = ["step2d.cu", "init2d.cu", "sim2d.cu", "host2d.cpp"]
+HEADERS = ["pfb_common.cuh", "device_util.cuh", "pfb_internal.h"]
+
+
+def _newer(target: Path, deps: list[Path]) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(d.stat().st_mtime > t for d in deps)
+
+
+def _run(cmd: list[str], verbose: bool) -> str:
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    p = subprocess.run(cmd, capture_output=True, text=True)
+    if p.returncode != 0:
+        sys.stderr.write(p.stdout + p.stderr)
+        raise RuntimeError(f"command failed ({p.returncode}): {' '.join(cmd[:3])} ...")
+    return p.stdout + p.stderr
+
+
+def build(force: bool = False, verbose: bool = False, ptxas_report: bool = False) -> Path:
+    """Compile changed sources and relink the library; returns its path."""
+    OUT_DIR.mkdir(parents=True, exist_ok=True)
+    OBJ_DIR.mkdir(parents=True, exist_ok=True)
+    headers = [CSRC / h for h in HEADERS] + [INCLUDE / "pfb200.h"]
+    objs = []
+    relink = force or not LIB.exists()
+    for src in SOURCES:
+        s = CSRC / src
+        o = OBJ_DIR / (src + ".o")
+        objs.append(o)
+        if force or _newer(o, [s, *headers, Path(__file__)]):
+            cmd = [NVCC, *ARCH, *COMMON, "-c", str(s), "-o", str(o)]
+            if ptxas_report and src.endswith(".cu"):
+                cmd += ["-Xptxas", "-v"]
+            out = _run(cmd, verbose)
+            if ptxas_report and out:
+                print(out)
+            relink = True
+    if relink or _newer(LIB, objs):
+        tmp = LIB.with_suffix(".so.tmp")
+        _run([NVCC, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-cudart", "static"],
+             verbose)
+        os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--ptxas", action="store_true", help="print the ptxas resource report")
+    a = ap.parse_args()
+    print(build(force=a.force, verbose=a.verbose, ptxas_report=a.ptxas))

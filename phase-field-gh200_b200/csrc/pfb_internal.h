@@ -1,0 +1,35 @@
+// Internal declarations shared by the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "../../include/pfb200.h"
+
+namespace pfb {
+
+// Record an error message for pfb_last_error() and return `code`.
+int set_error(int code, const char* fmt, ...);
+void clear_error();
+
+// step2d.cu
+int step2d_configure_device();
+int step2d_launch(const pfb_step_args2d* a, int cluster, cudaStream_t stream);
+int step2d_smem_bytes(int cluster);
+int step2d_read_status(unsigned* out, int clear);
+
+// init2d.cu
+int init_tiles2d(float* phi_a, float* phi_b, pfb_cell2d* cell, const uint8_t* cls, int N, int L,
+                 const float* cx, const float* cy, float radius_eff, float kappa_iface,
+                 cudaStream_t s);
+int init_moments2d(pfb_cell2d* cell, const uint8_t* cls, const float* phi, int N,
+                   cudaStream_t s);
+int scatter_all2d(const float* phi, const pfb_cell2d* cell, const uint8_t* cls, uint32_t* S,
+                  int N, int L, int P, uint32_t* flags, cudaStream_t s);
+int zero_u32(uint32_t* p, size_t n, cudaStream_t s);
+int verify_cells2d(const float* phi, const pfb_cell2d* cell, const uint8_t* cls, int N,
+                   double* out_V, float* out_outside, cudaStream_t s);
+int verify_S(const uint32_t* S, size_t n, uint32_t* out_max, cudaStream_t s);
+int pack_traj2d(const pfb_cell2d* cell, const uint8_t* cls, pfb_traj_cell2d* out, int N, int L,
+                cudaStream_t s);
+
+}  // namespace pfb

@@ -1,0 +1,465 @@
+// Host driver of the 2D update (the reference's `Sim`, include/sim.cuh:58-152
+// and src/sim.cu:159-1055) and the C-ABI wrappers of the 2D kernels.
+//
+// Buffer scheme kept from the reference so slots, parities and graph replay
+// line up with it: two phi pools (parity = step % 2), three S slots (read
+// step % 3, scatter (step+1) % 3, clear (step+2) % 3), device-resident step
+// counters and cursors in two slots following the phi parity, and a captured
+// CUDA graph of six steps that covers every (parity, slot) pair.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "pfb_common.cuh"
+#include "pfb_internal.h"
+
+using namespace pfb;
+
+#define PFB_CU(expr, what)                                                              \
+    do {                                                                                \
+        const cudaError_t e_ = (expr);                                                  \
+        if (e_ != cudaSuccess) return set_error(PFB_E_CUDA, "%s: %s", what, cudaGetErrorString(e_)); \
+    } while (0)
+
+struct pfb_sim2d {
+    pfb_params2d p{};
+    int device = 0;
+    int L = 0, P = 0, N = 0;
+    size_t s_words = 0;
+    float* d_phi[2] = {nullptr, nullptr};
+    uint32_t* d_S = nullptr;
+    pfb_cell2d* d_cell = nullptr;
+    uint8_t* d_cls = nullptr;
+    unsigned long long* d_cursor = nullptr;
+    unsigned long long* d_step = nullptr;
+    uint32_t* d_flags = nullptr;
+    pfb_traj_cell2d* d_traj = nullptr;
+    cudaStream_t stream = nullptr;
+    long long steps_done = 0;
+    int cluster = 4;
+    bool use_graph = true;
+    bool graph_ready = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+
+    ~pfb_sim2d() {
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (stream) cudaStreamDestroy(stream);
+        cudaFree(d_phi[0]);
+        cudaFree(d_phi[1]);
+        cudaFree(d_S);
+        cudaFree(d_cell);
+        cudaFree(d_cls);
+        cudaFree(d_cursor);
+        cudaFree(d_step);
+        cudaFree(d_flags);
+        cudaFree(d_traj);
+    }
+
+    pfb_step_args2d args_for_slot(int slot) const {
+        const int pin = slot % 2, pout = 1 - pin, rs = slot % 3;
+        pfb_step_args2d a;
+        std::memset(&a, 0, sizeof(a));
+        pfb_fill_coefficients2d(&p, &a);
+        a.phi_in = d_phi[pin];
+        a.phi_out = d_phi[pout];
+        a.S_rd = d_S + (size_t)rs * s_words;
+        a.S_sc = d_S + (size_t)((rs + 1) % 3) * s_words;
+        a.S_cl = d_S + (size_t)((rs + 2) % 3) * s_words;
+        a.cell = d_cell;
+        a.cell_cls = d_cls;
+        a.perm = nullptr;
+        a.cursor_use = d_cursor + pin;
+        a.cursor_clear = d_cursor + pout;
+        a.step_rd = d_step + pin;
+        a.step_wr = d_step + pout;
+        a.flags = d_flags;
+        a.moments = nullptr;
+        a.N = N;
+        a.L = L;
+        a.P = P;
+        a.parity_out = pout;
+        a.clear_ahead_words = (unsigned long long)s_words;
+        return a;
+    }
+
+    int launch_one(int slot) {
+        const pfb_step_args2d a = args_for_slot(slot);
+        return step2d_launch(&a, cluster, stream);
+    }
+
+    void drop_graph() {
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        if (graph) cudaGraphDestroy(graph);
+        graph_exec = nullptr;
+        graph = nullptr;
+        graph_ready = false;
+    }
+
+    int build_graph() {
+        drop_graph();
+        PFB_CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        int rc = PFB_OK;
+        for (int s = 0; s < 6 && rc == PFB_OK; ++s) rc = launch_one(s);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(stream, &g);
+        if (rc != PFB_OK) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        PFB_CU(e, "end capture");
+        graph = g;
+        PFB_CU(cudaGraphInstantiateWithFlags(&graph_exec, graph, 0), "graph instantiate");
+        graph_ready = true;
+        return PFB_OK;
+    }
+
+    int advance(long long steps) {
+        while (steps > 0) {
+            if (use_graph && !graph_ready) {
+                const int rc = build_graph();
+                if (rc) return rc;
+            }
+            if (use_graph && graph_ready && steps_done % 6 == 0 && steps >= 6) {
+                PFB_CU(cudaGraphLaunch(graph_exec, stream), "graph launch");
+                steps_done += 6;
+                steps -= 6;
+            } else {
+                const int rc = launch_one((int)(steps_done % 6));
+                if (rc) return rc;
+                steps_done += 1;
+                steps -= 1;
+            }
+        }
+        return PFB_OK;
+    }
+
+    // Allocate every device buffer for p (reference src/sim.cu:159-232).
+    int alloc(const pfb_params2d& prm, int dev) {
+        p = prm;
+        device = dev;
+        N = p.num_cells;
+        L = p.L;
+        if (N < 1) return set_error(PFB_E_ARG, "num_cells must be positive");
+        if (L <= 286) return set_error(PFB_E_ARG, "domain side %d must exceed 286", L);
+        P = 32 * ((L + 31) / 32);
+        s_words = (size_t)P * (size_t)L;
+        PFB_CU(cudaSetDevice(device), "cudaSetDevice");
+        const size_t pool = (size_t)N * kTileArea * sizeof(float);
+        PFB_CU(cudaMalloc(&d_phi[0], pool), "alloc phi");
+        PFB_CU(cudaMalloc(&d_phi[1], pool), "alloc phi");
+        PFB_CU(cudaMalloc(&d_S, 3 * s_words * sizeof(uint32_t)), "alloc S");
+        PFB_CU(cudaMalloc(&d_cell, (size_t)N * sizeof(pfb_cell2d)), "alloc cells");
+        PFB_CU(cudaMalloc(&d_cls, (size_t)N), "alloc classes");
+        PFB_CU(cudaMalloc(&d_cursor, 2 * sizeof(unsigned long long)), "alloc cursor");
+        PFB_CU(cudaMalloc(&d_step, 2 * sizeof(unsigned long long)), "alloc step");
+        PFB_CU(cudaMalloc(&d_flags, PFB_FLAG_COUNT * sizeof(uint32_t)), "alloc flags");
+        PFB_CU(cudaMalloc(&d_traj, (size_t)N * sizeof(pfb_traj_cell2d)), "alloc traj");
+        PFB_CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
+        PFB_CU(cudaMemsetAsync(d_cursor, 0, 2 * sizeof(unsigned long long), stream), "memset");
+        PFB_CU(cudaMemsetAsync(d_step, 0, 2 * sizeof(unsigned long long), stream), "memset");
+        PFB_CU(cudaMemsetAsync(d_flags, 0, PFB_FLAG_COUNT * sizeof(uint32_t), stream), "memset");
+        PFB_CU(cudaMemsetAsync(d_S, 0, 3 * s_words * sizeof(uint32_t), stream), "memset");
+        return step2d_configure_device();
+    }
+
+    int set_state(const pfb_cell2d* cells, const float* phi, long long step) {
+        if (!cells || !phi || step < 0) return set_error(PFB_E_ARG, "set_state: bad argument");
+        PFB_CU(cudaSetDevice(device), "cudaSetDevice");
+        drop_graph();
+        steps_done = step;
+        const int pin = (int)(step % 2), rot = (int)(step % 3);
+        std::vector<pfb_cell2d> h((size_t)N);
+        std::vector<uint8_t> hc((size_t)N);
+        for (int i = 0; i < N; ++i) {
+            h[(size_t)i] = cells[i];
+            h[(size_t)i].cls_written[0] = cells[i].cls;
+            h[(size_t)i].cls_written[1] = cells[i].cls;
+            hc[(size_t)i] = cells[i].cls;
+        }
+        const size_t pool = (size_t)N * kTileArea * sizeof(float);
+        PFB_CU(cudaMemcpyAsync(d_cell, h.data(), h.size() * sizeof(pfb_cell2d),
+                               cudaMemcpyHostToDevice, stream), "upload cells");
+        PFB_CU(cudaMemcpyAsync(d_cls, hc.data(), hc.size(), cudaMemcpyHostToDevice, stream),
+               "upload classes");
+        PFB_CU(cudaMemcpyAsync(d_phi[pin], phi, pool, cudaMemcpyHostToDevice, stream), "upload phi");
+        PFB_CU(cudaMemsetAsync(d_phi[1 - pin], 0, pool, stream), "clear phi");
+        const unsigned long long hs[2] = {
+            (unsigned long long)(pin == 0 ? step : step + 1),
+            (unsigned long long)(pin == 1 ? step : step + 1)};
+        PFB_CU(cudaMemcpyAsync(d_step, hs, sizeof(hs), cudaMemcpyHostToDevice, stream), "upload step");
+        PFB_CU(cudaMemsetAsync(d_cursor, 0, 2 * sizeof(unsigned long long), stream), "memset");
+        PFB_CU(cudaMemsetAsync(d_S, 0, 3 * s_words * sizeof(uint32_t), stream), "memset S");
+        int rc = scatter_all2d(d_phi[pin], d_cell, d_cls, d_S + (size_t)rot * s_words, N, L, P,
+                               d_flags, stream);
+        if (rc) return rc;
+        PFB_CU(cudaStreamSynchronize(stream), "set_state sync");
+        return PFB_OK;
+    }
+
+    // Fresh start (reference src/sim.cu:308-370).
+    int init_fresh(const float* cx, const float* cy) {
+        if (!cx || !cy) return set_error(PFB_E_ARG, "centres are required");
+        std::vector<pfb_cell2d> h((size_t)N);
+        std::memset(h.data(), 0, h.size() * sizeof(pfb_cell2d));
+        const unsigned long long pstream = p.polarity_seed ? p.polarity_seed : p.seed;
+        const int n_cancer = (int)std::llround(p.cancer_fraction * (double)N);
+        for (int i = 0; i < N; ++i) {
+            pfb_cell2d& c = h[(size_t)i];
+            c.global_id = i;
+            c.gamma = (float)(i < n_cancer ? p.gamma_cancer : p.gamma_normal);
+            c.v_A = (float)pfb_ic_v_A(i, p.seed, p.v_A, p.v_A_sigma);
+            c.M_pf = (float)p.phase_field_mobility;
+            c.R_tgt = (float)p.target_radius;
+            c.theta = pfb_ic_theta(i, pstream);
+            c.cls = 0;
+            c.cls_written[0] = 0;
+            c.cls_written[1] = 0;
+        }
+        std::vector<uint8_t> hc((size_t)N, 0);
+        float *d_cx = nullptr, *d_cy = nullptr;
+        PFB_CU(cudaMemcpyAsync(d_cell, h.data(), h.size() * sizeof(pfb_cell2d),
+                               cudaMemcpyHostToDevice, stream), "upload cells");
+        PFB_CU(cudaMemcpyAsync(d_cls, hc.data(), hc.size(), cudaMemcpyHostToDevice, stream),
+               "upload classes");
+        PFB_CU(cudaMalloc(&d_cx, (size_t)N * sizeof(float)), "alloc centres");
+        PFB_CU(cudaMalloc(&d_cy, (size_t)N * sizeof(float)), "alloc centres");
+        PFB_CU(cudaMemcpyAsync(d_cx, cx, (size_t)N * sizeof(float), cudaMemcpyHostToDevice, stream),
+               "upload centres");
+        PFB_CU(cudaMemcpyAsync(d_cy, cy, (size_t)N * sizeof(float), cudaMemcpyHostToDevice, stream),
+               "upload centres");
+        int rc = init_tiles2d(d_phi[0], d_phi[1], d_cell, d_cls, N, L, d_cx, d_cy,
+                              (float)seed_radius(p.target_radius, p.lambda),
+                              (float)iface_k(p.lambda), stream);
+        if (!rc) rc = init_moments2d(d_cell, d_cls, d_phi[0], N, stream);
+        if (!rc) rc = scatter_all2d(d_phi[0], d_cell, d_cls, d_S, N, L, P, d_flags, stream);
+        const cudaError_t e = cudaStreamSynchronize(stream);
+        cudaFree(d_cx);
+        cudaFree(d_cy);
+        if (rc) return rc;
+        PFB_CU(e, "init sync");
+        steps_done = 0;
+        return PFB_OK;
+    }
+};
+
+namespace {
+cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+}  // namespace
+
+extern "C" {
+
+int pfb_step2d_configure(void) { return step2d_configure_device(); }
+
+int pfb_step2d_grid(int num_cells, int cluster) {
+    if (cluster == 0) cluster = 4;
+    if (num_cells < 0 || (cluster != 2 && cluster != 4 && cluster != 8)) return PFB_E_ARG;
+    return num_cells * cluster;
+}
+
+int pfb_step2d_launch(const pfb_step_args2d* args, int cluster, void* stream) {
+    return step2d_launch(args, cluster, as_stream(stream));
+}
+
+int pfb_init_tiles2d(float* phi_a, float* phi_b, pfb_cell2d* cell, const uint8_t* cls, int N,
+                     int L, const float* seed_cx, const float* seed_cy, float radius_eff,
+                     float kappa_iface, void* stream) {
+    return init_tiles2d(phi_a, phi_b, cell, cls, N, L, seed_cx, seed_cy, radius_eff, kappa_iface,
+                        as_stream(stream));
+}
+
+int pfb_init_moments2d(pfb_cell2d* cell, const uint8_t* cls, const float* phi, int N,
+                       void* stream) {
+    return init_moments2d(cell, cls, phi, N, as_stream(stream));
+}
+
+int pfb_scatter_all2d(const float* phi, const pfb_cell2d* cell, const uint8_t* cls, uint32_t* S,
+                      int N, int L, int P, uint32_t* flags, void* stream) {
+    return scatter_all2d(phi, cell, cls, S, N, L, P, flags, as_stream(stream));
+}
+
+int pfb_zero_u32(uint32_t* p, size_t n, void* stream) { return zero_u32(p, n, as_stream(stream)); }
+
+int pfb_verify_cells2d(const float* phi, const pfb_cell2d* cell, const uint8_t* cls, int N,
+                       double* out_V, float* out_outside_max, void* stream) {
+    return verify_cells2d(phi, cell, cls, N, out_V, out_outside_max, as_stream(stream));
+}
+
+int pfb_verify_S(const uint32_t* S, size_t n, uint32_t* out_max, void* stream) {
+    return verify_S(S, n, out_max, as_stream(stream));
+}
+
+int pfb_pack_traj2d(const pfb_cell2d* cell, const uint8_t* cls, pfb_traj_cell2d* out, int N,
+                    int L, void* stream) {
+    return pack_traj2d(cell, cls, out, N, L, as_stream(stream));
+}
+
+int pfb_device_status(unsigned* out, int clear) { return step2d_read_status(out, clear); }
+
+pfb_sim2d* pfb_sim2d_create(const pfb_params2d* p, const float* cx, const float* cy, int device) {
+    clear_error();
+    if (!p) {
+        set_error(PFB_E_ARG, "null params");
+        return nullptr;
+    }
+    pfb_sim2d* s = new (std::nothrow) pfb_sim2d();
+    if (!s) {
+        set_error(PFB_E_NOMEM, "host allocation failed");
+        return nullptr;
+    }
+    if (s->alloc(*p, device) || s->init_fresh(cx, cy)) {
+        delete s;
+        return nullptr;
+    }
+    return s;
+}
+
+pfb_sim2d* pfb_sim2d_create_from_state(const pfb_params2d* p, const pfb_cell2d* cells,
+                                       const float* phi, long long step, int device) {
+    clear_error();
+    if (!p) {
+        set_error(PFB_E_ARG, "null params");
+        return nullptr;
+    }
+    pfb_sim2d* s = new (std::nothrow) pfb_sim2d();
+    if (!s) {
+        set_error(PFB_E_NOMEM, "host allocation failed");
+        return nullptr;
+    }
+    if (s->alloc(*p, device) || s->set_state(cells, phi, step)) {
+        delete s;
+        return nullptr;
+    }
+    return s;
+}
+
+void pfb_sim2d_destroy(pfb_sim2d* s) {
+    if (s) {
+        cudaSetDevice(s->device);
+        delete s;
+    }
+}
+
+int pfb_sim2d_set_cluster(pfb_sim2d* s, int cluster) {
+    if (!s) return set_error(PFB_E_ARG, "null sim");
+    if (cluster != 2 && cluster != 4 && cluster != 8) return set_error(PFB_E_CONFIG, "cluster must be 2, 4 or 8");
+    if (cluster != s->cluster) s->drop_graph();
+    s->cluster = cluster;
+    return PFB_OK;
+}
+
+int pfb_sim2d_set_graph(pfb_sim2d* s, int use_graph) {
+    if (!s) return set_error(PFB_E_ARG, "null sim");
+    s->use_graph = use_graph != 0;
+    if (!s->use_graph) s->drop_graph();
+    return PFB_OK;
+}
+
+int pfb_sim2d_advance(pfb_sim2d* s, long long steps) {
+    if (!s || steps < 0) return set_error(PFB_E_ARG, "advance: bad argument");
+    PFB_CU(cudaSetDevice(s->device), "cudaSetDevice");
+    return s->advance(steps);
+}
+
+int pfb_sim2d_sync(pfb_sim2d* s) {
+    if (!s) return set_error(PFB_E_ARG, "null sim");
+    PFB_CU(cudaStreamSynchronize(s->stream), "sync");
+    return PFB_OK;
+}
+
+long long pfb_sim2d_step(const pfb_sim2d* s) { return s ? s->steps_done : -1; }
+int pfb_sim2d_side(const pfb_sim2d* s) { return s ? s->L : -1; }
+int pfb_sim2d_pitch(const pfb_sim2d* s) { return s ? s->P : -1; }
+int pfb_sim2d_num_cells(const pfb_sim2d* s) { return s ? s->N : -1; }
+
+int pfb_sim2d_get_cells(pfb_sim2d* s, pfb_cell2d* out) {
+    if (!s || !out) return set_error(PFB_E_ARG, "get_cells: null");
+    PFB_CU(cudaMemcpyAsync(out, s->d_cell, (size_t)s->N * sizeof(pfb_cell2d),
+                           cudaMemcpyDeviceToHost, s->stream), "download cells");
+    PFB_CU(cudaStreamSynchronize(s->stream), "sync");
+    return PFB_OK;
+}
+
+int pfb_sim2d_get_phi(pfb_sim2d* s, float* out) {
+    if (!s || !out) return set_error(PFB_E_ARG, "get_phi: null");
+    const int pin = (int)(s->steps_done % 2);
+    PFB_CU(cudaMemcpyAsync(out, s->d_phi[pin], (size_t)s->N * kTileArea * sizeof(float),
+                           cudaMemcpyDeviceToHost, s->stream), "download phi");
+    PFB_CU(cudaStreamSynchronize(s->stream), "sync");
+    return PFB_OK;
+}
+
+int pfb_sim2d_get_S(pfb_sim2d* s, uint32_t* out) {
+    if (!s || !out) return set_error(PFB_E_ARG, "get_S: null");
+    const int rot = (int)(s->steps_done % 3);
+    PFB_CU(cudaMemcpyAsync(out, s->d_S + (size_t)rot * s->s_words, s->s_words * sizeof(uint32_t),
+                           cudaMemcpyDeviceToHost, s->stream), "download S");
+    PFB_CU(cudaStreamSynchronize(s->stream), "sync");
+    return PFB_OK;
+}
+
+int pfb_sim2d_get_flags(pfb_sim2d* s, uint32_t* out) {
+    if (!s || !out) return set_error(PFB_E_ARG, "get_flags: null");
+    PFB_CU(cudaMemcpyAsync(out, s->d_flags, PFB_FLAG_COUNT * sizeof(uint32_t),
+                           cudaMemcpyDeviceToHost, s->stream), "download flags");
+    PFB_CU(cudaStreamSynchronize(s->stream), "sync");
+    return PFB_OK;
+}
+
+int pfb_sim2d_set_state(pfb_sim2d* s, const pfb_cell2d* cells, const float* phi, long long step) {
+    if (!s) return set_error(PFB_E_ARG, "null sim");
+    return s->set_state(cells, phi, step);
+}
+
+int pfb_sim2d_pack_traj(pfb_sim2d* s, pfb_traj_cell2d* out) {
+    if (!s || !out) return set_error(PFB_E_ARG, "pack_traj: null");
+    int rc = pack_traj2d(s->d_cell, s->d_cls, s->d_traj, s->N, s->L, s->stream);
+    if (rc) return rc;
+    PFB_CU(cudaMemcpyAsync(out, s->d_traj, (size_t)s->N * sizeof(pfb_traj_cell2d),
+                           cudaMemcpyDeviceToHost, s->stream), "download traj");
+    PFB_CU(cudaStreamSynchronize(s->stream), "sync");
+    return PFB_OK;
+}
+
+int pfb_sim2d_bench(pfb_sim2d* s, int warmup, int steps, double* ms_per_step) {
+    if (!s || warmup < 0 || steps < 1 || !ms_per_step) return set_error(PFB_E_ARG, "bench: bad argument");
+    PFB_CU(cudaSetDevice(s->device), "cudaSetDevice");
+    int rc = s->advance(warmup);
+    if (rc) return rc;
+    if (s->use_graph) {
+        const long long align = (6 - s->steps_done % 6) % 6;
+        rc = s->advance(align);
+        if (rc) return rc;
+    }
+    PFB_CU(cudaStreamSynchronize(s->stream), "sync");
+    cudaEvent_t e0, e1;
+    PFB_CU(cudaEventCreate(&e0), "event");
+    PFB_CU(cudaEventCreate(&e1), "event");
+    cudaEventRecord(e0, s->stream);
+    rc = s->advance(steps);
+    cudaEventRecord(e1, s->stream);
+    const cudaError_t e = cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    PFB_CU(e, "bench sync");
+    *ms_per_step = (double)ms / (double)steps;
+    return PFB_OK;
+}
+
+int pfb_sim2d_step_args(pfb_sim2d* s, pfb_step_args2d* out) {
+    if (!s || !out) return set_error(PFB_E_ARG, "step_args: null");
+    *out = s->args_for_slot((int)(s->steps_done % 6));
+    return PFB_OK;
+}
+
+void* pfb_sim2d_stream(pfb_sim2d* s) { return s ? (void*)s->stream : nullptr; }
+
+}  // extern "C"

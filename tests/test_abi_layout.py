@@ -1,0 +1,85 @@
+"""The C-ABI library loads without a GPU, exports every entry point that
+include/pfb200.h declares, and its records have the reference's layout
+(reference include/kernels.cuh:27-57 CellState, :74-116 StepArgs)."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import numpy as np
+
+import pfb200
+from pfb200._abi import CELL_DTYPE, Cell2D, Params2D, StepArgs2D, TrajCell2D
+
+HEADER = Path(__file__).resolve().parent.parent / "include" / "pfb200.h"
+
+
+def declared_functions(path=HEADER):
+    text = re.sub(r"/\*.*?\*/", "", path.read_text(), flags=re.S)
+    names = re.findall(r"\b(pfb_[a-z0-9_]+)\s*\(", text)
+    return sorted(set(names))
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    assert "pfb_step2d_launch" in names and "pfb_sim2d_create" in names
+    assert len(names) >= 40
+
+
+def test_library_exports_every_declared_symbol():
+    L = pfb200.lib()
+    missing = [n for n in declared_functions() if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_binding_covers_every_declared_symbol():
+    assert set(declared_functions()) <= set(pfb200.exported_symbols())
+
+
+def test_record_sizes_match_library():
+    L = pfb200.lib()
+    assert L.pfb_sizeof(0) == 192 == C.sizeof(Cell2D) == CELL_DTYPE.itemsize
+    assert L.pfb_sizeof(1) == 216 == C.sizeof(StepArgs2D)
+    assert L.pfb_sizeof(2) == C.sizeof(Params2D)
+    assert L.pfb_sizeof(3) == 48 == C.sizeof(TrajCell2D)
+
+
+def test_cell_record_offsets():
+    # The reference pins these with static_asserts (include/kernels.cuh:53-57).
+    assert Cell2D.advection.offset == 128
+    assert Cell2D.reserved.offset == 120
+    assert Cell2D.M_pf.offset == 188
+    for name, (dt, off) in CELL_DTYPE.fields.items():
+        if name.startswith("adv_"):
+            continue
+        assert getattr(Cell2D, name).offset == off, name
+
+
+def test_step_args_offsets():
+    expect = {"phi_in": 0, "flags": 96, "moments": 104, "physical_dt": 112, "N": 120,
+              "parity_out": 132, "dt": 136, "A0": 144, "vol_scale": 152, "bulk_scale": 160,
+              "mot_coeff": 168, "seed": 176, "polarity_seed": 184, "p_tumble": 192,
+              "full_moment_every": 200, "clear_ahead_words": 208}
+    for k, v in expect.items():
+        assert getattr(StepArgs2D, k).offset == v, k
+
+
+def test_launcher_rejects_bad_arguments_without_touching_a_device():
+    L = pfb200.lib()
+    assert L.pfb_step2d_launch(None, 4, None) == -1
+    a = StepArgs2D()
+    assert L.pfb_step2d_launch(C.byref(a), 4, None) == -1  # null buffers
+    assert b"null" in L.pfb_last_error()
+    assert L.pfb_step2d_grid(64, 0) == 256
+    assert L.pfb_step2d_grid(64, 3) == -1
+
+
+def test_coefficients_match_reference_defaults():
+    p = pfb200.SimParams2D(L=512, num_cells=64, target_radius=12.0)
+    a = pfb200.step_coefficients(p)
+    assert a.dt == np.float32(0.01)
+    assert abs(a.A0 - np.pi * 144.0) < 1e-12
+    assert a.bulk_scale == np.float32(30.0 / 49.0)
+    assert a.rep_coeff == np.float32(600.0 / 49.0)
+    assert a.mot_coeff == np.float32((600.0 / 49.0) / 1500.0)
+    assert a.p_tumble == -np.expm1(-0.01 / 1e4)
+    assert a.polarity_seed == 1234
