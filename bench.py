@@ -49,6 +49,23 @@ def rank_env():
             int(os.environ.get("LOCAL_RANK", 0)))
 
 
+def max_over_ranks(value: float, dist=None, device=None) -> float:
+    """Largest value over all ranks (device times are taken as the slowest
+    rank's); identity without a process group."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(sites_per_rank_step: int, steps: int, world: int, max_ms: float) -> float:
+    """Site-cell updates/s of the whole job: every rank advances its own
+    replica by `steps`; the job takes as long as its slowest rank."""
+    return world * sites_per_rank_step * steps / (max_ms / 1000.0)
+
+
 def workload_params(seed: int):
     import pfb200
     return pfb200.SimParams2D(L=L_SIDE, num_cells=N_CELLS, target_radius=RADIUS, seed=seed)
@@ -300,13 +317,10 @@ def main():
     ms = e0.elapsed_time(e1)
     time.sleep(0.15)
     m1 = clocks.mark()
-    if dist is not None:
-        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist, f"cuda:{device}")
     flags = sim.flags()
     final_cells = sim.cells()
-    value = world * sites * a.steps / (ms / 1000.0)
+    value = whole_job_rate(sites, a.steps, world, ms)
     ms_step = ms / a.steps
 
     # ---- end to end through the public API with host buffers -------------
@@ -332,11 +346,7 @@ def main():
         f1.record(ext)
         sim.sync()
         barrier()
-        el = f0.elapsed_time(f1) / 1000.0
-        if dist is not None:
-            t = torch.tensor([el], dtype=torch.float64, device=f"cuda:{device}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
+        el = max_over_ranks(f0.elapsed_time(f1) / 1000.0, dist, f"cuda:{device}")
         h2d = pin_cells.numel() + pin_phi.numel() * 4
         d2h = traj.numel() * e2e_steps + phi_out.numel() * 4
         e2e = {"value": world * sites * e2e_steps / el, "unit": "site-cell updates/s",

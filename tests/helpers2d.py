@@ -118,6 +118,8 @@ class DeviceState2D:
         st = np.array([step if pin == 0 else step + 1, step if pin == 1 else step + 1], np.int64)
         self.steps = torch.from_numpy(st).to(device)
         self.flags = torch.zeros(8, dtype=torch.int32, device=device)
+        # identity visit order: the reference kernel dereferences perm
+        self.perm = torch.arange(self.N, dtype=torch.int32, device=device)
         # S^step from the pool
         rc = pfb200.lib().pfb_scatter_all2d(
             self.phi[pin].data_ptr(), self.cells.data_ptr(), self.cls.data_ptr(),
@@ -138,7 +140,7 @@ class DeviceState2D:
         a.S_cl = self.S[(rs + 2) % 3].data_ptr()
         a.cell = self.cells.data_ptr()
         a.cell_cls = self.cls.data_ptr()
-        a.perm = None
+        a.perm = self.perm.data_ptr()
         a.cursor_use = self.cursor.data_ptr() + 8 * pin
         a.cursor_clear = self.cursor.data_ptr() + 8 * pout
         a.step_rd = self.steps.data_ptr() + 8 * pin
