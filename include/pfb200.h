@@ -185,17 +185,25 @@ size_t pfb_sizeof(int which);
  * current device. Idempotent; called implicitly by pfb_step2d_launch. */
 int pfb_step2d_configure(void);
 
-/* Number of CTAs the step launch uses for N cells with `cluster` CTAs per
- * cell (cluster = 0 selects the default). Replaces k_step_grid(). */
+/* Number of CTAs the one-cluster-per-cell launch uses for N cells with
+ * `cluster` CTAs per cell (cluster = 0 selects the default 8). Replaces
+ * k_step_grid(). */
 int pfb_step2d_grid(int num_cells, int cluster);
 
 /* One full step for every cell: tumble, interaction integral, Euler update,
  * recentring store, Q5.27 scatter into S_sc, FP64 moments, and clearing of
  * S_cl (clear_ahead_words words). `cluster` is the number of CTAs that
- * cooperate on one cell (2, 4 or 8; 0 = default 4).
- * Returns PFB_E_ARG for a null buffer, a misaligned phi pool (16 B), L not
- * larger than 286, or a non-null `moments`. */
+ * cooperate on one cell (2, 4 or 8; 0 = default 8). Clusters of 8 run the
+ * persistent pipelined kernel; 2 and 4 launch one cluster per cell.
+ * Returns PFB_E_ARG for a null buffer, a phi pool or S slot not 16-byte
+ * aligned, L not larger than 286, or a non-null `moments`. */
 int pfb_step2d_launch(const pfb_step_args2d* args, int cluster, void* stream);
+
+/* As pfb_step2d_launch with an explicit kernel variant: 0 = default for the
+ * cluster size, 1 = one cluster per cell, 2 = persistent pipelined clusters
+ * (cluster must be 8). Both variants compute the same update. */
+int pfb_step2d_launch_ex(const pfb_step_args2d* args, int cluster, int variant,
+                         void* stream);
 
 /* Library status word kept in device memory: bit 0 is set when a CTA gave up
  * waiting for its staged band (a bounded wait that is never expected to run

@@ -34,8 +34,8 @@ COMMON = [
     "-Xcompiler", "-fPIC,-ffp-contract=off,-Wall",
     "-I", str(INCLUDE),
 ]
-SOURCES = ["step2d.cu", "init2d.cu", "sim2d.cu", "host2d.cpp"]
-HEADERS = ["pfb_common.cuh", "device_util.cuh", "pfb_internal.h"]
+SOURCES = ["step2d.cu", "step2d_persist.cu", "init2d.cu", "sim2d.cu", "host2d.cpp"]
+HEADERS = ["pfb_common.cuh", "device_util.cuh", "pfb_internal.h", "step2d_common.cuh"]
 
 
 def _newer(target: Path, deps: list[Path]) -> bool:

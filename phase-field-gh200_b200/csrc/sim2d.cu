@@ -40,7 +40,7 @@ struct pfb_sim2d {
     pfb_traj_cell2d* d_traj = nullptr;
     cudaStream_t stream = nullptr;
     long long steps_done = 0;
-    int cluster = 4;
+    int cluster = 8;
     bool use_graph = true;
     bool graph_ready = false;
     cudaGraph_t graph = nullptr;
@@ -257,13 +257,17 @@ extern "C" {
 int pfb_step2d_configure(void) { return step2d_configure_device(); }
 
 int pfb_step2d_grid(int num_cells, int cluster) {
-    if (cluster == 0) cluster = 4;
+    if (cluster == 0) cluster = 8;
     if (num_cells < 0 || (cluster != 2 && cluster != 4 && cluster != 8)) return PFB_E_ARG;
     return num_cells * cluster;
 }
 
 int pfb_step2d_launch(const pfb_step_args2d* args, int cluster, void* stream) {
     return step2d_launch(args, cluster, as_stream(stream));
+}
+
+int pfb_step2d_launch_ex(const pfb_step_args2d* args, int cluster, int variant, void* stream) {
+    return step2d_launch_variant(args, cluster, variant, as_stream(stream));
 }
 
 int pfb_init_tiles2d(float* phi_a, float* phi_b, pfb_cell2d* cell, const uint8_t* cls, int N,

@@ -31,35 +31,24 @@
 #include "device_util.cuh"
 #include "pfb_common.cuh"
 #include "pfb_internal.h"
+#include "step2d_common.cuh"
 
 namespace pfb {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kHeaderBytes = 1024;
-// Polls of an mbarrier before a CTA gives up (each poll suspends briefly).
-constexpr uint32_t kWaitPolls = 1u << 24;
 
-// Error word of the library (device side): bit 0 = a CTA gave up waiting for
-// its staged band. Read with pfb_device_status().
+// Status word of this kernel family in device memory: bit 0 = a CTA gave up
+// waiting for its staged band. Read with pfb_device_status().
 __device__ unsigned int g_step2d_status = 0u;
 
 struct __align__(16) StepShared {
     uint64_t bar;
     int abort;
     int gx0, gy0;
-    // decided by thread 0 (phase 0)
-    int sx, sy, gx0n, gy0n, dcls, zero_tile, fm, pctr, tumbled;
-    int dwx, dwy, dtx0, dty0, no_margin;
-    float gam, dwC, volC, vA, pcos, psin, theta, mrel;
-    float vx, vy;
-    // per-warp partials
-    double red_d[kWarps][4];
-    int red_i[kWarps][5];
-    // this CTA's partials, read by rank 0 through distributed shared memory
-    double part_I[2];
-    double part_M[4];
-    int part_B[5];
+    CellPlan plan;
+    RedScratch<kWarps> red;
 };
 static_assert(sizeof(StepShared) <= kHeaderBytes, "shared header too large");
 
@@ -94,290 +83,6 @@ __host__ __device__ constexpr int step_smem_bytes(int k) {
     return m;
 }
 
-// S_other = (q_S - q(phi)) 2^-27; a negative difference is counted, not
-// floored silently (reference src/kernels.cu:19-25).
-__device__ __forceinline__ float s_other(uint32_t qS, float phi, uint32_t* flags) {
-    const uint32_t qc = q_encode(phi);
-    if (qS >= qc) return (float)(qS - qc) * kQInv;
-    if (flags) atomicAdd(flags + PFB_FLAG_S_NEGATIVE, 1u);
-    return 0.0f;
-}
-
-// Tumble, class choice and recentring shift of cell n (reference
-// src/kernels.cu:93-191 and :624-711). Run by one thread of every CTA of the
-// cluster; all CTAs compute identical values from identical inputs, and only
-// the leader raises flags.
-template <int CLS>
-__device__ __forceinline__ void phase0(const pfb_step_args2d& A, int n, StepShared& sh,
-                                       bool leader) {
-    constexpr Window W = window_of(CLS);
-    const pfb_cell2d& cs = A.cell[n];
-    const unsigned long long step = *A.step_rd;
-
-    const Words4 r = philox10((uint32_t)(step & 0xFFFFFFFFull), (uint32_t)(step >> 32),
-                              (uint32_t)cs.global_id, kTumbleTag,
-                              (uint32_t)(A.polarity_seed & 0xFFFFFFFFull),
-                              (uint32_t)(A.polarity_seed >> 32));
-    float theta = cs.theta;
-    int tumbled = 0;
-    if (u53(r.w[0], r.w[1]) < A.p_tumble) {
-        theta = (float)(2.0 * kPi * u53(r.w[2], r.w[3]));
-        tumbled = 1;
-    }
-    float ps, pc;
-    sincosf(theta, &ps, &pc);
-
-    const float gam = cs.gamma;
-    const float dwC = A.bulk_scale * gam;
-    const float volC = (float)(A.vol_scale * (A.A0 - cs.V));
-    const float mrel = cs.M_pf * (float)(1.0 / kMobilityM0);
-
-    const int ex = cs.bb_hi_x - cs.bb_lo_x + 1;
-    const int ey = cs.bb_hi_y - cs.bb_lo_y + 1;
-    int dcls = CLS;
-    int no_margin = 0;
-    unsigned pctr = cs.promote_ctr;
-    if (ex > 0) {
-        if (ex + kPromoteSlack > W.wx || ey + kPromoteSlack > W.wy) {
-            const int grow = smallest_class_holding(ex, ey, kPromoteSlack);
-            if (grow >= 0) {
-                dcls = grow;
-            } else if (CLS == kClassFallback && ex <= W.wx && ey <= W.wy) {
-                no_margin = 1;
-            } else if (leader) {
-                atomicAdd(A.flags + PFB_FLAG_CLASS_EXHAUSTED, 1u);
-            }
-            pctr = 0u;
-        } else {
-            const int small = smallest_class_holding(ex, ey, kDemoteSlack);
-            if (small >= 0 && small != CLS &&
-                window_of(small).wx * window_of(small).wy < W.wx * W.wy) {
-                if (++pctr >= (unsigned)kDemoteDwell) {
-                    dcls = small;
-                    pctr = 0u;
-                }
-            } else {
-                pctr = 0u;
-            }
-        }
-    }
-    const Window D = window_of(dcls);
-
-    int sx = 0, sy = 0;
-    if (cs.V > 0.0) {
-        const double cxr = cs.Cx / cs.V;
-        const double cyr = cs.Cy / cs.V;
-        sx = __double2int_rn(cxr - 0.5 * (double)(D.wx - 1));
-        sy = __double2int_rn(cyr - 0.5 * (double)(D.wy - 1));
-        if (dcls == CLS) {
-            sx = max(-kMaxShift, min(kMaxShift, sx));
-            sy = max(-kMaxShift, min(kMaxShift, sy));
-        } else {
-            sx = max(-W.wx, min(W.wx, sx));
-            sy = max(-W.wy, min(W.wy, sy));
-        }
-    } else if (leader) {
-        atomicOr(A.flags + PFB_FLAG_V_NONPOS, 1u);
-    }
-
-    const int L = A.L;
-    int gx0n = (cs.gx0 + sx) % L;
-    if (gx0n < 0) gx0n += L;
-    int gy0n = (cs.gy0 + sy) % L;
-    if (gy0n < 0) gy0n += L;
-
-    sh.gx0 = cs.gx0;
-    sh.gy0 = cs.gy0;
-    sh.sx = sx;
-    sh.sy = sy;
-    sh.gx0n = gx0n;
-    sh.gy0n = gy0n;
-    sh.dcls = dcls;
-    sh.zero_tile = (dcls != (int)cs.cls_written[A.parity_out]);
-    sh.fm = (A.full_moment_every > 0 &&
-             ((step + 1ull) % (unsigned long long)A.full_moment_every) == 0ull);
-    sh.pctr = (int)pctr;
-    sh.tumbled = tumbled;
-    sh.dwx = D.wx;
-    sh.dwy = D.wy;
-    sh.dtx0 = D.tx0;
-    sh.dty0 = D.ty0;
-    sh.no_margin = no_margin;
-    sh.gam = gam;
-    sh.dwC = dwC;
-    sh.volC = volC;
-    sh.vA = cs.v_A;
-    sh.pcos = pc;
-    sh.psin = ps;
-    sh.theta = theta;
-    sh.mrel = mrel;
-}
-
-// Interaction integral of this CTA -> cluster total -> velocity (all CTAs).
-template <int K>
-__device__ __forceinline__ void reduce_force(const pfb_step_args2d& A, int n, int rank,
-                                             StepShared& sh, double aIx, double aIy) {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    aIx = dev::warp_sum_down(aIx);
-    aIy = dev::warp_sum_down(aIy);
-    if (lane == 0) {
-        sh.red_d[warp][0] = aIx;
-        sh.red_d[warp][1] = aIy;
-    }
-    __syncthreads();
-    if (tid == 0) {
-        double s0 = 0.0, s1 = 0.0;
-        for (int w = 0; w < kWarps; ++w) {
-            s0 += sh.red_d[w][0];
-            s1 += sh.red_d[w][1];
-        }
-        sh.part_I[0] = s0;
-        sh.part_I[1] = s1;
-    }
-    dev::cluster_sync();
-    if (tid == 0) {
-        double sIx = 0.0, sIy = 0.0;
-        const uint32_t base = dev::smem_addr(&sh.part_I[0]);
-        for (int r = 0; r < K; ++r) {
-            const uint32_t a = dev::map_to_rank(base, (uint32_t)r);
-            sIx += dev::ld_cluster_f64(a);
-            sIy += dev::ld_cluster_f64(a + 8);
-        }
-        const double vxd = (double)sh.vA * (double)sh.pcos + (double)A.mot_coeff * sIx;
-        const double vyd = (double)sh.vA * (double)sh.psin + (double)A.mot_coeff * sIy;
-        sh.vx = (float)vxd;
-        sh.vy = (float)vyd;
-        if (rank == 0) {
-            pfb_cell2d& cs = A.cell[n];
-            cs.vx = (float)vxd;
-            cs.vy = (float)vyd;
-            cs.Ix = sIx;
-            cs.Iy = sIy;
-        }
-    }
-    __syncthreads();
-}
-
-// Moments of this CTA -> cluster total -> commit by rank 0 (reference
-// src/kernels.cu:542-590 and :883-935).
-template <int K, bool FALLBACK>
-__device__ __forceinline__ void reduce_commit(const pfb_step_args2d& A, int n, int rank,
-                                              StepShared& sh, double aV, double aCx,
-                                              double aCy, double aPer, int blox, int bhix,
-                                              int bloy, int bhiy, int pmaxb) {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    aV = dev::warp_sum_down(aV);
-    aCx = dev::warp_sum_down(aCx);
-    aCy = dev::warp_sum_down(aCy);
-    aPer = dev::warp_sum_down(aPer);
-    blox = dev::warp_min_down(blox);
-    bhix = dev::warp_max_down(bhix);
-    bloy = dev::warp_min_down(bloy);
-    bhiy = dev::warp_max_down(bhiy);
-    pmaxb = dev::warp_max_down(pmaxb);
-    if (lane == 0) {
-        sh.red_d[warp][0] = aV;
-        sh.red_d[warp][1] = aCx;
-        sh.red_d[warp][2] = aCy;
-        sh.red_d[warp][3] = aPer;
-        sh.red_i[warp][0] = blox;
-        sh.red_i[warp][1] = bhix;
-        sh.red_i[warp][2] = bloy;
-        sh.red_i[warp][3] = bhiy;
-        sh.red_i[warp][4] = pmaxb;
-    }
-    __syncthreads();
-    if (tid == 0) {
-        double m[4] = {0.0, 0.0, 0.0, 0.0};
-        int b[5] = {sh.dwx, -1, sh.dwy, -1, 0};
-        for (int w = 0; w < kWarps; ++w) {
-            for (int k = 0; k < 4; ++k) m[k] += sh.red_d[w][k];
-            b[0] = min(b[0], sh.red_i[w][0]);
-            b[1] = max(b[1], sh.red_i[w][1]);
-            b[2] = min(b[2], sh.red_i[w][2]);
-            b[3] = max(b[3], sh.red_i[w][3]);
-            b[4] = max(b[4], sh.red_i[w][4]);
-        }
-        for (int k = 0; k < 4; ++k) sh.part_M[k] = m[k];
-        for (int k = 0; k < 5; ++k) sh.part_B[k] = b[k];
-    }
-    dev::cluster_sync();
-    if (rank == 0 && tid == 0) {
-        double m[4] = {0.0, 0.0, 0.0, 0.0};
-        int b[5] = {sh.dwx, -1, sh.dwy, -1, 0};
-        const uint32_t bm = dev::smem_addr(&sh.part_M[0]);
-        const uint32_t bb = dev::smem_addr(&sh.part_B[0]);
-        for (int r = 0; r < K; ++r) {
-            const uint32_t am = dev::map_to_rank(bm, (uint32_t)r);
-            const uint32_t ab = dev::map_to_rank(bb, (uint32_t)r);
-            for (int k = 0; k < 4; ++k) m[k] += dev::ld_cluster_f64(am + 8u * k);
-            b[0] = min(b[0], dev::ld_cluster_s32(ab + 0));
-            b[1] = max(b[1], dev::ld_cluster_s32(ab + 4));
-            b[2] = min(b[2], dev::ld_cluster_s32(ab + 8));
-            b[3] = max(b[3], dev::ld_cluster_s32(ab + 12));
-            b[4] = max(b[4], dev::ld_cluster_s32(ab + 16));
-        }
-        pfb_cell2d& cs = A.cell[n];
-        const int dcls = sh.dcls;
-        cs.gx0 = sh.gx0n;
-        cs.gy0 = sh.gy0n;
-        cs.cls = (uint8_t)dcls;
-        cs.cls_written[A.parity_out] = (uint8_t)dcls;
-        cs.theta = sh.theta;
-        cs.V = m[0];
-        cs.Cx = m[1];
-        cs.Cy = m[2];
-        if (sh.fm) cs.perim = m[3];
-        cs.bb_lo_x = b[0];
-        cs.bb_hi_x = b[1];
-        cs.bb_lo_y = b[2];
-        cs.bb_hi_y = b[3];
-        cs.promote_ctr = (uint32_t)sh.pctr;
-        cs.shift_ctr += (sh.sx | sh.sy) ? 1u : 0u;
-        cs.tumble_ctr += (uint32_t)sh.tumbled;
-        cs.phi_max = __uint_as_float((uint32_t)b[4]);
-        A.cell_cls[n] = (uint8_t)dcls;
-        if (FALLBACK) {
-            const bool edge = b[1] >= 0 &&
-                              (b[0] == 0 || b[1] == sh.dwx - 1 || b[2] == 0 || b[3] == sh.dwy - 1);
-            cs.reserved[0] = 1u;
-            if (sh.no_margin || (dcls == kClassFallback && edge)) ++cs.reserved[1];
-        }
-    }
-    // Keep every CTA's shared memory alive until rank 0 has read it.
-    dev::cluster_sync();
-}
-
-// Flags, phi_max, Q5.27 scatter and moments of one destination pixel.
-struct PixelAcc {
-    double V = 0.0, Cx = 0.0, Cy = 0.0, Per = 0.0;
-    int blox, bhix = -1, bloy, bhiy = -1, pmaxb = 0;
-};
-
-__device__ __forceinline__ void dest_pixel(const pfb_step_args2d& A, PixelAcc& acc, float pn,
-                                           int a, int b, uint32_t* srow, int gx0n, int L) {
-    if (!isfinite(pn)) atomicOr(A.flags + PFB_FLAG_NONFINITE, 1u);
-    if (pn * pn > kPhiSqCap) atomicOr(A.flags + PFB_FLAG_Q_CLAMP, 1u);
-    acc.pmaxb = max(acc.pmaxb, (int)__float_as_uint(fabsf(pn)));
-    const uint32_t q = q_encode(pn);
-    if (q) {
-        int gx = gx0n + a;
-        if (gx >= L) gx -= L;
-        const uint32_t old = atomicAdd(srow + gx, q);
-        if (old > 0xFFFFFFFFu - q) atomicOr(A.flags + PFB_FLAG_S_OVERFLOW, 1u);
-    }
-    const double d = (double)pn * (double)pn;
-    acc.V += d;
-    acc.Cx += d * (double)a;
-    acc.Cy += d * (double)b;
-    if (pn > kSupportEps) {
-        acc.blox = min(acc.blox, a);
-        acc.bhix = max(acc.bhix, a);
-        acc.bloy = min(acc.bloy, b);
-        acc.bhiy = max(acc.bhiy, b);
-    }
-}
-
 // ---------------------------------------------------------------------------
 // Staged path: classes 0-3.
 // Shared layout after the header:
@@ -388,7 +93,7 @@ __device__ __forceinline__ void dest_pixel(const pfb_step_args2d& A, PixelAcc& a
 // ---------------------------------------------------------------------------
 template <int CLS, int K>
 __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int rank,
-                                            char* smem) {
+                                            char* smem, unsigned long long step, bool fm) {
     constexpr Window W = window_of(CLS);
     constexpr int WX = W.wx, WY = W.wy, TX0 = W.tx0, TY0 = W.ty0;
     constexpr int RB = band_rows(WY, K);
@@ -398,6 +103,7 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
     static_assert((WX * 4) % 16 == 0 && (TX0 * 4) % 16 == 0, "bulk copies need 16-B rows");
 
     StepShared& sh = *reinterpret_cast<StepShared*>(smem);
+    const CellPlan& P = sh.plan;
     float* phi_s = reinterpret_cast<float*>(smem + kHeaderBytes);
     uint32_t* ps_s = reinterpret_cast<uint32_t*>(smem + kHeaderBytes + PHI_ROWS * PX * 4);
 
@@ -405,7 +111,7 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
     const int y0 = rank * RB;
     const int y1 = y0 + RB;
     const float* tile_in = A.phi_in + (size_t)n * kTileArea;
-    const int L = A.L, P = A.P;
+    const int L = A.L, Pp = A.P;
 
     if (tid == 0) {
         sh.abort = 0;
@@ -423,7 +129,7 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
             dev::bulk_g2s(phi_s + (y - y0 + 2) * PX + 4,
                           tile_in + (size_t)(TY0 + y) * kTilePitch + TX0, (uint32_t)(WX * 4),
                           &sh.bar);
-        if (lane == 0) phase0<CLS>(A, n, sh, rank == 0);
+        if (lane == 0) plan_cell(A, n, CLS, step, sh.plan, rank == 0);
     } else {
         const int t = tid - 32;
         constexpr int NT = kThreads - 32;
@@ -438,7 +144,7 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
             int gy = gy0 + y;
             if (gy >= L) gy -= L;
             const int gx = x < split ? gx0 + x : x - split;
-            ps_s[(y - y0 + 1) * WX + x] = __ldg(A.S_rd + (size_t)gy * P + gx);
+            ps_s[(y - y0 + 1) * WX + x] = __ldg(A.S_rd + (size_t)gy * Pp + gx);
         }
         // Zero ring columns of in-window rows; whole rows outside the window.
         for (int k = t; k < PHI_ROWS; k += NT) {
@@ -477,7 +183,7 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
             float cW = p[-1], cC = p[0], cE = p[1];
             for (int y = ya; y < yb; ++y) {
                 const float nC = p[PX];
-                const float So = s_other(*q, cC, A.flags);
+                const float So = s_other_n(*q, cC, A.flags, 1u);
                 const float gx = 0.5f * (cE - cW);
                 const float gy = 0.5f * (nC - sC);
                 aIx += (double)(cC * gx * So);
@@ -491,12 +197,12 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
             }
         }
     }
-    reduce_force<K>(A, n, rank, sh, aIx, aIy);
+    reduce_force<K, kWarps>(A, P, rank, sh.red, 0, aIx, aIy);
 
     // ---- pass 2: Euler update of own rows plus a one-row halo, in place
     if (!abort) {
-        const float gam = sh.gam, dwC = sh.dwC, volC = sh.volC;
-        const float vx = sh.vx, vy = sh.vy, mrel = sh.mrel;
+        const float gam = P.gam, dwC = P.dwC, volC = P.volC;
+        const float vx = sh.red.vx, vy = sh.red.vy, mrel = P.mrel;
         const float repC = A.rep_coeff, dtf = A.dt;
         const int ua = max(0, y0 - 1), ub = min(WY, y1 + 1);
         constexpr int H = pick_run(WX, RB + 2);
@@ -517,7 +223,7 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
                 const float gx = 0.5f * (cE - cW);
                 const float gy = 0.5f * (nC - sC);
                 const bool own = (y >= y0) && (y < y1);
-                const float So = s_other(*q, cC, own ? A.flags : nullptr);
+                const float So = s_other_n(*q, cC, A.flags, own ? 1u : 0u);
                 const float rhs =
                     rhs_pixel(lap, cC, So, gx, gy, gam, dwC, volC, repC, vx, vy, mrel);
                 const float pnew = cC + dtf * rhs;
@@ -537,13 +243,12 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
 
     // ---- pass 3: recentring store, scatter, moments over owned destination rows
     PixelAcc acc;
-    acc.blox = sh.dwx;
-    acc.bloy = sh.dwy;
+    acc.blox = P.dwx;
+    acc.bloy = P.dwy;
     if (!abort) {
-        const int sx = sh.sx, sy = sh.sy;
-        const int dwx = sh.dwx, dwy = sh.dwy, dtx0 = sh.dtx0, dty0 = sh.dty0;
-        const int gx0n = sh.gx0n, gy0n = sh.gy0n;
-        const bool fm = sh.fm != 0;
+        const int sx = P.sx, sy = P.sy;
+        const int dwx = P.dwx, dwy = P.dwy, dtx0 = P.dtx0, dty0 = P.dty0;
+        const int gx0n = P.gx0n, gy0n = P.gy0n;
         float* tile_out = A.phi_out + (size_t)n * kTileArea;
         // Destination row b reads source row j = b + sy; rows above the window
         // belong to rank 0, rows below it to rank K-1.
@@ -551,7 +256,7 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
         const int jhi = (rank == K - 1) ? (1 << 20) : y1;
         const int b_lo = max(0, jlo - sy), b_hi = min(dwy, jhi - sy);
 
-        if (sh.zero_tile) {
+        if (P.zero_tile) {
             for (int b = b_lo + warp; b < b_hi; b += kWarps) {
                 float* trow = tile_out + (size_t)(dty0 + b) * kTilePitch;
                 for (int c = lane; c < kTilePitch; c += 32)
@@ -571,7 +276,7 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
             int gy = gy0n + b;
             if (gy >= L) gy -= L;
             float* orow = tile_out + (size_t)(dty0 + b) * kTilePitch + dtx0;
-            uint32_t* srow = A.S_sc + (size_t)gy * P;
+            uint32_t* srow = A.S_sc + (size_t)gy * Pp;
             for (int a = lane; a < dwx; a += 32) {
                 const int i = a + sx;
                 const bool iin = (unsigned)i < (unsigned)WX;
@@ -596,132 +301,17 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
             }
         }
     }
-    reduce_commit<K, false>(A, n, rank, sh, acc.V, acc.Cx, acc.Cy, acc.Per, acc.blox, acc.bhix,
-                            acc.bloy, acc.bhiy, acc.pmaxb);
+    reduce_moments<K, kWarps>(A, P, rank, sh.red, 0, fm, acc);
     if (abort) (void)dev::mbar_wait_bounded(&sh.bar, 0, kWaitPolls);
 }
 
-// ---------------------------------------------------------------------------
-// Global-memory path: classes 4 (224^2) and 5 (286^2 fallback). phi^n is read
-// from the tile (its zero ring is the tile invariant), phi^{n+1} is written to
-// the shifted destination in global memory, and after a cluster barrier each
-// CTA re-reads its destination rows for the scatter and moments (reference
-// src/kernels.cu:344-443 and :604-937).
-// ---------------------------------------------------------------------------
 template <int CLS, int K>
-__device__ __noinline__ void global_cell(const pfb_step_args2d& A, int n, int rank, char* smem) {
-    constexpr Window W = window_of(CLS);
-    constexpr int WX = W.wx, WY = W.wy, TX0 = W.tx0, TY0 = W.ty0;
-    constexpr int RB = band_rows(WY, K);
+__device__ __forceinline__ void global_cell_v1(const pfb_step_args2d& A, int n, int rank,
+                                               char* smem, unsigned long long step, bool fm) {
     StepShared& sh = *reinterpret_cast<StepShared*>(smem);
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int y0 = rank * RB;
-    const int y1 = min(WY, y0 + RB);
-    const int L = A.L, P = A.P;
-    const float* tin = A.phi_in + (size_t)n * kTileArea + (size_t)TY0 * kTilePitch + TX0;
-    float* tile_out = A.phi_out + (size_t)n * kTileArea;
-
-    if (tid == 0) phase0<CLS>(A, n, sh, rank == 0);
+    if (threadIdx.x == 0) plan_cell(A, n, CLS, step, sh.plan, rank == 0);
     __syncthreads();
-    const int gx0 = sh.gx0, gy0 = sh.gy0;
-    const int split = min(WX, L - gx0);
-
-    double aIx = 0.0, aIy = 0.0;
-    const int cnt = (y1 - y0) * WX;
-    for (int idx = tid; idx < cnt; idx += kThreads) {
-        const int yy = idx / WX;
-        const int x = idx - yy * WX;
-        const int y = y0 + yy;
-        const float* p = tin + (size_t)y * kTilePitch + x;
-        const float c = __ldg(p);
-        const float gx = 0.5f * (__ldg(p + 1) - __ldg(p - 1));
-        const float gyv = 0.5f * (__ldg(p + kTilePitch) - __ldg(p - kTilePitch));
-        int gy = gy0 + y;
-        if (gy >= L) gy -= L;
-        const int gxg = x < split ? gx0 + x : x - split;
-        const float So = s_other(__ldg(A.S_rd + (size_t)gy * P + gxg), c, A.flags);
-        aIx += (double)(c * gx * So);
-        aIy += (double)(c * gyv * So);
-    }
-    reduce_force<K>(A, n, rank, sh, aIx, aIy);
-
-    const int sx = sh.sx, sy = sh.sy;
-    const int dwx = sh.dwx, dwy = sh.dwy, dtx0 = sh.dtx0, dty0 = sh.dty0;
-    if (sh.zero_tile) {
-        for (int t = rank + K * warp; t < kTilePitch; t += K * kWarps) {
-            float* trow = tile_out + (size_t)t * kTilePitch;
-            for (int c = lane; c < kTilePitch; c += 32) trow[c] = 0.0f;
-        }
-        dev::cluster_sync();
-    }
-
-    {
-        const float gam = sh.gam, dwC = sh.dwC, volC = sh.volC;
-        const float vx = sh.vx, vy = sh.vy, mrel = sh.mrel;
-        const float repC = A.rep_coeff, dtf = A.dt;
-        for (int idx = tid; idx < cnt; idx += kThreads) {
-            const int yy = idx / WX;
-            const int x = idx - yy * WX;
-            const int y = y0 + yy;
-            const float* p = tin + (size_t)y * kTilePitch + x;
-            const float cC = __ldg(p), cW = __ldg(p - 1), cE = __ldg(p + 1);
-            const float nC = __ldg(p + kTilePitch), nW = __ldg(p + kTilePitch - 1),
-                        nE = __ldg(p + kTilePitch + 1);
-            const float sC = __ldg(p - kTilePitch), sW = __ldg(p - kTilePitch - 1),
-                        sE = __ldg(p - kTilePitch + 1);
-            const float lap = lap9(nW, nC, nE, cW, cC, cE, sW, sC, sE);
-            const float gx = 0.5f * (cE - cW);
-            const float gyv = 0.5f * (nC - sC);
-            int gy = gy0 + y;
-            if (gy >= L) gy -= L;
-            const int gxg = x < split ? gx0 + x : x - split;
-            const float So = s_other(__ldg(A.S_rd + (size_t)gy * P + gxg), cC, A.flags);
-            const float rhs =
-                rhs_pixel(lap, cC, So, gx, gyv, gam, dwC, volC, repC, vx, vy, mrel);
-            const float pnew = cC + dtf * rhs;
-            const int a = x - sx, b = y - sy;
-            if ((unsigned)a < (unsigned)dwx && (unsigned)b < (unsigned)dwy)
-                tile_out[(size_t)(dty0 + b) * kTilePitch + dtx0 + a] = pnew;
-        }
-    }
-    const int DB = (dwy + K - 1) / K;
-    const int db0 = min(dwy, rank * DB), db1 = min(dwy, db0 + DB);
-    for (int b = db0 + warp; b < db1; b += kWarps) {
-        const int j = b + sy;
-        const bool jin = (unsigned)j < (unsigned)WY;
-        float* orow = tile_out + (size_t)(dty0 + b) * kTilePitch + dtx0;
-        for (int a = lane; a < dwx; a += 32) {
-            const int i = a + sx;
-            if (!(jin && (unsigned)i < (unsigned)WX)) orow[a] = 0.0f;
-        }
-    }
-    dev::cluster_sync();
-
-    PixelAcc acc;
-    acc.blox = dwx;
-    acc.bloy = dwy;
-    const int gx0n = sh.gx0n, gy0n = sh.gy0n;
-    const bool fm = sh.fm != 0;
-    for (int b = db0 + warp; b < db1; b += kWarps) {
-        int gy = gy0n + b;
-        if (gy >= L) gy -= L;
-        const float* orow = tile_out + (size_t)(dty0 + b) * kTilePitch + dtx0;
-        uint32_t* srow = A.S_sc + (size_t)gy * P;
-        for (int a = lane; a < dwx; a += 32) {
-            const float pn = __ldcg(orow + a);
-            dest_pixel(A, acc, pn, a, b, srow, gx0n, L);
-            if (fm) {
-                const float e = a + 1 < dwx ? __ldcg(orow + a + 1) : 0.0f;
-                const float w = a > 0 ? __ldcg(orow + a - 1) : 0.0f;
-                const float nn = b + 1 < dwy ? __ldcg(orow + kTilePitch + a) : 0.0f;
-                const float ss = b > 0 ? __ldcg(orow - kTilePitch + a) : 0.0f;
-                const float pgx = 0.5f * (e - w), pgy = 0.5f * (nn - ss);
-                acc.Per += (double)sqrtf(pgx * pgx + pgy * pgy);
-            }
-        }
-    }
-    reduce_commit<K, CLS == kClassFallback>(A, n, rank, sh, acc.V, acc.Cx, acc.Cy, acc.Per,
-                                            acc.blox, acc.bhix, acc.bloy, acc.bhiy, acc.pmaxb);
+    global_cell<CLS, K, kWarps>(A, sh.plan, rank, sh.red, 0, fm);
 }
 
 template <int K>
@@ -740,26 +330,30 @@ __global__ void __launch_bounds__(kThreads, (K >= 8 ? 4 : 3))
         for (size_t i = (size_t)blockIdx.x * kThreads + tid; i < nvec; i += stride)
             __stcs(dst + i, z);
     }
+    const unsigned long long step = *A.step_rd;
     if (blockIdx.x == 0 && tid == 0) {
         if (A.cursor_clear) *A.cursor_clear = 0ull;
-        *A.step_wr = *A.step_rd + 1ull;
+        *A.step_wr = step + 1ull;
     }
+    const bool fm = full_moment_step(A, step);
 
     const int rank = (int)dev::cluster_rank();
     const int slot = (int)(blockIdx.x / K);
     const int n = A.perm ? (int)A.perm[slot] : slot;
     const int cls = (int)A.cell_cls[n];
     switch (cls) {
-        case 0: staged_cell<0, K>(A, n, rank, smem); break;
-        case 1: staged_cell<1, K>(A, n, rank, smem); break;
-        case 2: staged_cell<2, K>(A, n, rank, smem); break;
-        case 3: staged_cell<3, K>(A, n, rank, smem); break;
-        case 4: global_cell<4, K>(A, n, rank, smem); break;
-        case 5: global_cell<5, K>(A, n, rank, smem); break;
+        case 0: staged_cell<0, K>(A, n, rank, smem, step, fm); break;
+        case 1: staged_cell<1, K>(A, n, rank, smem, step, fm); break;
+        case 2: staged_cell<2, K>(A, n, rank, smem, step, fm); break;
+        case 3: staged_cell<3, K>(A, n, rank, smem, step, fm); break;
+        case 4: global_cell_v1<4, K>(A, n, rank, smem, step, fm); break;
+        case 5: global_cell_v1<5, K>(A, n, rank, smem, step, fm); break;
         default:
             if (rank == 0 && tid == 0) atomicAdd(A.flags + PFB_FLAG_CLASS_UNSUPPORTED, 1u);
-            break;
+            return;  // uniform over the cluster: no barrier is pending
     }
+    // Keep every CTA's shared memory alive until rank 0 has read the partials.
+    dev::cluster_sync();
 }
 
 // ---------------------------------------------------------------------------
@@ -805,7 +399,8 @@ static cudaError_t launch_k(const pfb_step_args2d& A, cudaStream_t stream) {
     return cudaLaunchKernelEx(&cfg, k_step2d<K>, A);
 }
 
-int step2d_launch(const pfb_step_args2d* a, int cluster, cudaStream_t stream) {
+int step2d_launch_variant(const pfb_step_args2d* a, int cluster, int variant,
+                          cudaStream_t stream) {
     if (!a) return set_error(PFB_E_ARG, "null step arguments");
     const pfb_step_args2d& A = *a;
     if (!A.phi_in || !A.phi_out || !A.S_rd || !A.S_sc || !A.cell || !A.cell_cls || !A.step_rd ||
@@ -813,16 +408,22 @@ int step2d_launch(const pfb_step_args2d* a, int cluster, cudaStream_t stream) {
         return set_error(PFB_E_ARG, "null buffer in step arguments");
     if (A.clear_ahead_words && !A.S_cl) return set_error(PFB_E_ARG, "clear-ahead needs S_cl");
     if (((uintptr_t)A.phi_in & 15u) || ((uintptr_t)A.phi_out & 15u) ||
-        ((uintptr_t)A.S_cl & 15u))
-        return set_error(PFB_E_ARG, "phi pools and S_cl must be 16-byte aligned");
+        ((uintptr_t)A.S_cl & 15u) || ((uintptr_t)A.S_rd & 15u))
+        return set_error(PFB_E_ARG, "phi pools and S slots must be 16-byte aligned");
     if (A.moments) return set_error(PFB_E_ARG, "velocity observation is not supported");
     if (A.N < 0) return set_error(PFB_E_ARG, "negative cell count");
-    if (A.L <= 286 || A.P < A.L) return set_error(PFB_E_ARG, "domain side must exceed 286 and P >= L");
+    if (A.L <= 286 || A.P < A.L || (A.P & 3))
+        return set_error(PFB_E_ARG, "domain side must exceed 286, P >= L and P % 4 == 0");
     if (A.parity_out != 0 && A.parity_out != 1) return set_error(PFB_E_ARG, "parity_out must be 0 or 1");
-    if (cluster == 0) cluster = 4;
+    if (cluster == 0) cluster = 8;
     if (cluster != 2 && cluster != 4 && cluster != 8)
         return set_error(PFB_E_CONFIG, "cluster must be 2, 4 or 8");
+    if (variant == 0) variant = cluster == 8 ? 2 : 1;
+    if (variant == 2 && cluster != 8)
+        return set_error(PFB_E_CONFIG, "the persistent kernel uses clusters of 8");
+    if (variant != 1 && variant != 2) return set_error(PFB_E_CONFIG, "unknown kernel variant");
     if (A.N == 0) return PFB_OK;
+    if (variant == 2) return persist2d_launch(A, stream);
     int rc = step2d_configure_device();
     if (rc) return rc;
     cudaError_t e = cluster == 2   ? launch_k<2>(A, stream)
@@ -832,7 +433,14 @@ int step2d_launch(const pfb_step_args2d* a, int cluster, cudaStream_t stream) {
     return PFB_OK;
 }
 
+int step2d_launch(const pfb_step_args2d* a, int cluster, cudaStream_t stream) {
+    return step2d_launch_variant(a, cluster, 0, stream);
+}
+
 int step2d_read_status(unsigned* out, int clear) {
+    unsigned pv = 0;
+    int rc = persist2d_read_status(&pv, clear);
+    if (rc) return rc;
     unsigned v = 0;
     cudaError_t e = cudaMemcpyFromSymbol(&v, g_step2d_status, sizeof(v));
     if (e != cudaSuccess) return set_error(PFB_E_CUDA, "status read: %s", cudaGetErrorString(e));
@@ -840,7 +448,7 @@ int step2d_read_status(unsigned* out, int clear) {
         const unsigned z = 0;
         cudaMemcpyToSymbol(g_step2d_status, &z, sizeof(z));
     }
-    if (out) *out = v;
+    if (out) *out = v | pv;
     return PFB_OK;
 }
 

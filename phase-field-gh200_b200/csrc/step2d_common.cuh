@@ -1,0 +1,457 @@
+// Device pieces shared by the two 2D step kernels (per-cell clusters in
+// step2d.cu, persistent pipelined clusters in step2d_persist.cu): the
+// per-cell decision record, the tumble/class/shift decision, S_other, and the
+// per-pixel store/scatter/moment update.
+#pragma once
+
+#include <cstdint>
+
+#include "device_util.cuh"
+#include "pfb_common.cuh"
+
+namespace pfb {
+
+// Polls of an mbarrier before a CTA gives up (each poll suspends briefly).
+constexpr uint32_t kWaitPolls = 1u << 24;
+
+// Everything one step decides for a cell before touching its field.
+struct CellPlan {
+    int n;              // cell slot
+    int cls;            // source class
+    int sx, sy;         // recentring shift
+    int gx0, gy0;       // source origin
+    int gx0n, gy0n;     // destination origin
+    int dcls;           // destination class
+    int zero_tile;      // destination tile must be cleared (class changed)
+    int pctr, tumbled, no_margin;
+    int dwx, dwy, dtx0, dty0;
+    float gam, dwC, volC, vA, pcos, psin, theta, mrel;
+};
+
+// S_other = (q_S - q(phi)) 2^-27; a negative difference is counted, not
+// floored silently (reference src/kernels.cu:19-25). `count` adds to the
+// S_other_negative counter (0 to not count).
+__device__ __forceinline__ float s_other_n(uint32_t qS, float phi, uint32_t* flags,
+                                           uint32_t count) {
+    const uint32_t qc = q_encode(phi);
+    if (qS >= qc) return (float)(qS - qc) * kQInv;
+    if (count) atomicAdd(flags + PFB_FLAG_S_NEGATIVE, count);
+    return 0.0f;
+}
+
+// Tumble, class choice and recentring shift of cell n whose field is in class
+// `cls` (reference src/kernels.cu:93-191 and :624-711). Deterministic in its
+// inputs, so every CTA that runs it for the same cell decides the same thing;
+// only `leader` raises flags.
+__device__ __forceinline__ void plan_cell(const pfb_step_args2d& A, int n, int cls,
+                                          unsigned long long step, CellPlan& out, bool leader) {
+    const Window W = window_of(cls);
+    const pfb_cell2d& cs = A.cell[n];
+    const Words4 r = philox10((uint32_t)(step & 0xFFFFFFFFull), (uint32_t)(step >> 32),
+                              (uint32_t)cs.global_id, kTumbleTag,
+                              (uint32_t)(A.polarity_seed & 0xFFFFFFFFull),
+                              (uint32_t)(A.polarity_seed >> 32));
+    float theta = cs.theta;
+    int tumbled = 0;
+    if (u53(r.w[0], r.w[1]) < A.p_tumble) {
+        theta = (float)(2.0 * kPi * u53(r.w[2], r.w[3]));
+        tumbled = 1;
+    }
+    float ps, pc;
+    sincosf(theta, &ps, &pc);
+
+    const float gam = cs.gamma;
+    const float dwC = A.bulk_scale * gam;
+    const float volC = (float)(A.vol_scale * (A.A0 - cs.V));
+    const float mrel = cs.M_pf * (float)(1.0 / kMobilityM0);
+
+    const int ex = cs.bb_hi_x - cs.bb_lo_x + 1;
+    const int ey = cs.bb_hi_y - cs.bb_lo_y + 1;
+    int dcls = cls;
+    int no_margin = 0;
+    unsigned pctr = cs.promote_ctr;
+    if (ex > 0) {
+        if (ex + kPromoteSlack > W.wx || ey + kPromoteSlack > W.wy) {
+            const int grow = smallest_class_holding(ex, ey, kPromoteSlack);
+            if (grow >= 0) {
+                dcls = grow;
+            } else if (cls == kClassFallback && ex <= W.wx && ey <= W.wy) {
+                no_margin = 1;
+            } else if (leader) {
+                atomicAdd(A.flags + PFB_FLAG_CLASS_EXHAUSTED, 1u);
+            }
+            pctr = 0u;
+        } else {
+            const int small = smallest_class_holding(ex, ey, kDemoteSlack);
+            if (small >= 0 && small != cls &&
+                window_of(small).wx * window_of(small).wy < W.wx * W.wy) {
+                if (++pctr >= (unsigned)kDemoteDwell) {
+                    dcls = small;
+                    pctr = 0u;
+                }
+            } else {
+                pctr = 0u;
+            }
+        }
+    }
+    const Window D = window_of(dcls);
+
+    int sx = 0, sy = 0;
+    if (cs.V > 0.0) {
+        const double cxr = cs.Cx / cs.V;
+        const double cyr = cs.Cy / cs.V;
+        sx = __double2int_rn(cxr - 0.5 * (double)(D.wx - 1));
+        sy = __double2int_rn(cyr - 0.5 * (double)(D.wy - 1));
+        if (dcls == cls) {
+            sx = max(-kMaxShift, min(kMaxShift, sx));
+            sy = max(-kMaxShift, min(kMaxShift, sy));
+        } else {
+            sx = max(-W.wx, min(W.wx, sx));
+            sy = max(-W.wy, min(W.wy, sy));
+        }
+    } else if (leader) {
+        atomicOr(A.flags + PFB_FLAG_V_NONPOS, 1u);
+    }
+
+    const int L = A.L;
+    int gx0n = (cs.gx0 + sx) % L;
+    if (gx0n < 0) gx0n += L;
+    int gy0n = (cs.gy0 + sy) % L;
+    if (gy0n < 0) gy0n += L;
+
+    out.n = n;
+    out.cls = cls;
+    out.gx0 = cs.gx0;
+    out.gy0 = cs.gy0;
+    out.sx = sx;
+    out.sy = sy;
+    out.gx0n = gx0n;
+    out.gy0n = gy0n;
+    out.dcls = dcls;
+    out.zero_tile = (dcls != (int)cs.cls_written[A.parity_out]);
+    out.pctr = (int)pctr;
+    out.tumbled = tumbled;
+    out.no_margin = no_margin;
+    out.dwx = D.wx;
+    out.dwy = D.wy;
+    out.dtx0 = D.tx0;
+    out.dty0 = D.ty0;
+    out.gam = gam;
+    out.dwC = dwC;
+    out.volC = volC;
+    out.vA = cs.v_A;
+    out.pcos = pc;
+    out.psin = ps;
+    out.theta = theta;
+    out.mrel = mrel;
+}
+
+__device__ __forceinline__ bool full_moment_step(const pfb_step_args2d& A,
+                                                 unsigned long long step) {
+    return A.full_moment_every > 0 &&
+           ((step + 1ull) % (unsigned long long)A.full_moment_every) == 0ull;
+}
+
+// Running per-thread moments of destination pixels.
+struct PixelAcc {
+    double V = 0.0, Cx = 0.0, Cy = 0.0, Per = 0.0;
+    int blox, bhix = -1, bloy, bhiy = -1, pmaxb = 0;
+};
+
+// Flags, phi_max, Q5.27 scatter and moments of one destination pixel.
+__device__ __forceinline__ void dest_pixel(const pfb_step_args2d& A, PixelAcc& acc, float pn,
+                                           int a, int b, uint32_t* srow, int gx0n, int L) {
+    if (!isfinite(pn)) atomicOr(A.flags + PFB_FLAG_NONFINITE, 1u);
+    if (pn * pn > kPhiSqCap) atomicOr(A.flags + PFB_FLAG_Q_CLAMP, 1u);
+    acc.pmaxb = max(acc.pmaxb, (int)__float_as_uint(fabsf(pn)));
+    const uint32_t q = q_encode(pn);
+    if (q) {
+        int gx = gx0n + a;
+        if (gx >= L) gx -= L;
+        const uint32_t old = atomicAdd(srow + gx, q);
+        if (old > 0xFFFFFFFFu - q) atomicOr(A.flags + PFB_FLAG_S_OVERFLOW, 1u);
+    }
+    const double d = (double)pn * (double)pn;
+    acc.V += d;
+    acc.Cx += d * (double)a;
+    acc.Cy += d * (double)b;
+    if (pn > kSupportEps) {
+        acc.blox = min(acc.blox, a);
+        acc.bhix = max(acc.bhix, a);
+        acc.bloy = min(acc.bloy, b);
+        acc.bhiy = max(acc.bhiy, b);
+    }
+}
+
+// Commit of one cell's step (reference src/kernels.cu:573-590, :914-935).
+// m = {V, Cx, Cy, perimeter}, b = {lo_x, hi_x, lo_y, hi_y, phi_max bits}.
+__device__ __forceinline__ void commit_cell(const pfb_step_args2d& A, const CellPlan& P,
+                                            bool fm, const double* m, const int* b) {
+    pfb_cell2d& cs = A.cell[P.n];
+    cs.gx0 = P.gx0n;
+    cs.gy0 = P.gy0n;
+    cs.cls = (uint8_t)P.dcls;
+    cs.cls_written[A.parity_out] = (uint8_t)P.dcls;
+    cs.theta = P.theta;
+    cs.V = m[0];
+    cs.Cx = m[1];
+    cs.Cy = m[2];
+    if (fm) cs.perim = m[3];
+    cs.bb_lo_x = b[0];
+    cs.bb_hi_x = b[1];
+    cs.bb_lo_y = b[2];
+    cs.bb_hi_y = b[3];
+    cs.promote_ctr = (uint32_t)P.pctr;
+    cs.shift_ctr += (P.sx | P.sy) ? 1u : 0u;
+    cs.tumble_ctr += (uint32_t)P.tumbled;
+    cs.phi_max = __uint_as_float((uint32_t)b[4]);
+    A.cell_cls[P.n] = (uint8_t)P.dcls;
+    if (P.cls == kClassFallback) {
+        const bool edge =
+            b[1] >= 0 && (b[0] == 0 || b[1] == P.dwx - 1 || b[2] == 0 || b[3] == P.dwy - 1);
+        cs.reserved[0] = 1u;
+        if (P.no_margin || (P.dcls == kClassFallback && edge)) ++cs.reserved[1];
+    }
+}
+
+// Reduction scratch in shared memory; the partials that peers read through
+// distributed shared memory are double-buffered by cell parity so that a
+// persistent cluster can move to its next cell after one barrier.
+template <int NW>
+struct RedScratch {
+    double red_d[NW][4];
+    int red_i[NW][5];
+    double part_I[2][2];
+    double part_M[2][4];
+    int part_B[2][5];
+    float vx, vy;
+};
+
+// Interaction integral of this CTA -> cluster total (ascending ranks) ->
+// velocity, identical in every CTA. Rank 0 stores v and I in the cell record.
+template <int K, int NW>
+__device__ __forceinline__ void reduce_force(const pfb_step_args2d& A, const CellPlan& P,
+                                             int rank, RedScratch<NW>& R, int par, double aIx,
+                                             double aIy) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    aIx = dev::warp_sum_down(aIx);
+    aIy = dev::warp_sum_down(aIy);
+    if (lane == 0) {
+        R.red_d[warp][0] = aIx;
+        R.red_d[warp][1] = aIy;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double s0 = 0.0, s1 = 0.0;
+        for (int w = 0; w < NW; ++w) {
+            s0 += R.red_d[w][0];
+            s1 += R.red_d[w][1];
+        }
+        R.part_I[par][0] = s0;
+        R.part_I[par][1] = s1;
+    }
+    dev::cluster_sync();
+    if (tid == 0) {
+        double sIx = 0.0, sIy = 0.0;
+        const uint32_t base = dev::smem_addr(&R.part_I[par][0]);
+        for (int r = 0; r < K; ++r) {
+            const uint32_t a = dev::map_to_rank(base, (uint32_t)r);
+            sIx += dev::ld_cluster_f64(a);
+            sIy += dev::ld_cluster_f64(a + 8);
+        }
+        const double vxd = (double)P.vA * (double)P.pcos + (double)A.mot_coeff * sIx;
+        const double vyd = (double)P.vA * (double)P.psin + (double)A.mot_coeff * sIy;
+        R.vx = (float)vxd;
+        R.vy = (float)vyd;
+        if (rank == 0) {
+            pfb_cell2d& cs = A.cell[P.n];
+            cs.vx = (float)vxd;
+            cs.vy = (float)vyd;
+            cs.Ix = sIx;
+            cs.Iy = sIy;
+        }
+    }
+    __syncthreads();
+}
+
+// Moments of this CTA -> cluster total -> commit by rank 0 (reference
+// src/kernels.cu:542-590). Leaves the caller after the cluster barrier that
+// publishes the partials; the caller's next cluster barrier (or the kernel's
+// final one) keeps them alive until rank 0 has read them.
+template <int K, int NW>
+__device__ __forceinline__ void reduce_moments(const pfb_step_args2d& A, const CellPlan& P,
+                                               int rank, RedScratch<NW>& R, int par, bool fm,
+                                               PixelAcc acc) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    acc.V = dev::warp_sum_down(acc.V);
+    acc.Cx = dev::warp_sum_down(acc.Cx);
+    acc.Cy = dev::warp_sum_down(acc.Cy);
+    acc.Per = dev::warp_sum_down(acc.Per);
+    acc.blox = dev::warp_min_down(acc.blox);
+    acc.bhix = dev::warp_max_down(acc.bhix);
+    acc.bloy = dev::warp_min_down(acc.bloy);
+    acc.bhiy = dev::warp_max_down(acc.bhiy);
+    acc.pmaxb = dev::warp_max_down(acc.pmaxb);
+    if (lane == 0) {
+        R.red_d[warp][0] = acc.V;
+        R.red_d[warp][1] = acc.Cx;
+        R.red_d[warp][2] = acc.Cy;
+        R.red_d[warp][3] = acc.Per;
+        R.red_i[warp][0] = acc.blox;
+        R.red_i[warp][1] = acc.bhix;
+        R.red_i[warp][2] = acc.bloy;
+        R.red_i[warp][3] = acc.bhiy;
+        R.red_i[warp][4] = acc.pmaxb;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double m[4] = {0.0, 0.0, 0.0, 0.0};
+        int b[5] = {P.dwx, -1, P.dwy, -1, 0};
+        for (int w = 0; w < NW; ++w) {
+            for (int k = 0; k < 4; ++k) m[k] += R.red_d[w][k];
+            b[0] = min(b[0], R.red_i[w][0]);
+            b[1] = max(b[1], R.red_i[w][1]);
+            b[2] = min(b[2], R.red_i[w][2]);
+            b[3] = max(b[3], R.red_i[w][3]);
+            b[4] = max(b[4], R.red_i[w][4]);
+        }
+        for (int k = 0; k < 4; ++k) R.part_M[par][k] = m[k];
+        for (int k = 0; k < 5; ++k) R.part_B[par][k] = b[k];
+    }
+    dev::cluster_sync();
+    if (rank == 0 && tid == 0) {
+        double m[4] = {0.0, 0.0, 0.0, 0.0};
+        int b[5] = {P.dwx, -1, P.dwy, -1, 0};
+        const uint32_t bm = dev::smem_addr(&R.part_M[par][0]);
+        const uint32_t bb = dev::smem_addr(&R.part_B[par][0]);
+        for (int r = 0; r < K; ++r) {
+            const uint32_t am = dev::map_to_rank(bm, (uint32_t)r);
+            const uint32_t ab = dev::map_to_rank(bb, (uint32_t)r);
+            for (int k = 0; k < 4; ++k) m[k] += dev::ld_cluster_f64(am + 8u * k);
+            b[0] = min(b[0], dev::ld_cluster_s32(ab + 0));
+            b[1] = max(b[1], dev::ld_cluster_s32(ab + 4));
+            b[2] = min(b[2], dev::ld_cluster_s32(ab + 8));
+            b[3] = max(b[3], dev::ld_cluster_s32(ab + 12));
+            b[4] = max(b[4], dev::ld_cluster_s32(ab + 16));
+        }
+        commit_cell(A, P, fm, m, b);
+    }
+}
+
+// Global-memory path for classes 4 (224^2) and 5 (286^2 fallback): phi^n is
+// read from the tile (its zero ring is the tile invariant), phi^{n+1} is
+// written to the shifted destination in global memory, and after a cluster
+// barrier each CTA re-reads its destination rows for scatter and moments
+// (reference src/kernels.cu:344-443 and :604-937). All NT threads of every CTA
+// of the cluster call it together.
+template <int CLS, int K, int NW>
+__device__ __noinline__ void global_cell(const pfb_step_args2d& A, const CellPlan& P, int rank,
+                                         RedScratch<NW>& R, int par, bool fm) {
+    constexpr int NT = NW * 32;
+    constexpr Window W = window_of(CLS);
+    constexpr int WX = W.wx, WY = W.wy, TX0 = W.tx0, TY0 = W.ty0;
+    constexpr int RB = (WY + K - 1) / K;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int y0 = min(WY, rank * RB);
+    const int y1 = min(WY, y0 + RB);
+    const int L = A.L, Pp = A.P;
+    const float* tin = A.phi_in + (size_t)P.n * kTileArea + (size_t)TY0 * kTilePitch + TX0;
+    float* tile_out = A.phi_out + (size_t)P.n * kTileArea;
+    const int gx0 = P.gx0, gy0 = P.gy0;
+    const int split = min(WX, L - gx0);
+
+    double aIx = 0.0, aIy = 0.0;
+    const int cnt = (y1 - y0) * WX;
+    for (int idx = tid; idx < cnt; idx += NT) {
+        const int yy = idx / WX;
+        const int x = idx - yy * WX;
+        const int y = y0 + yy;
+        const float* p = tin + (size_t)y * kTilePitch + x;
+        const float c = __ldg(p);
+        const float gx = 0.5f * (__ldg(p + 1) - __ldg(p - 1));
+        const float gyv = 0.5f * (__ldg(p + kTilePitch) - __ldg(p - kTilePitch));
+        int gy = gy0 + y;
+        if (gy >= L) gy -= L;
+        const int gxg = x < split ? gx0 + x : x - split;
+        const float So = s_other_n(__ldg(A.S_rd + (size_t)gy * Pp + gxg), c, A.flags, 1u);
+        aIx += (double)(c * gx * So);
+        aIy += (double)(c * gyv * So);
+    }
+    reduce_force<K, NW>(A, P, rank, R, par, aIx, aIy);
+
+    const int sx = P.sx, sy = P.sy;
+    const int dwx = P.dwx, dwy = P.dwy, dtx0 = P.dtx0, dty0 = P.dty0;
+    if (P.zero_tile) {
+        for (int t = rank + K * warp; t < kTilePitch; t += K * NW) {
+            float* trow = tile_out + (size_t)t * kTilePitch;
+            for (int c = lane; c < kTilePitch; c += 32) trow[c] = 0.0f;
+        }
+        dev::cluster_sync();
+    }
+    {
+        const float gam = P.gam, dwC = P.dwC, volC = P.volC, mrel = P.mrel;
+        const float vx = R.vx, vy = R.vy;
+        const float repC = A.rep_coeff, dtf = A.dt;
+        for (int idx = tid; idx < cnt; idx += NT) {
+            const int yy = idx / WX;
+            const int x = idx - yy * WX;
+            const int y = y0 + yy;
+            const float* p = tin + (size_t)y * kTilePitch + x;
+            const float cC = __ldg(p), cW = __ldg(p - 1), cE = __ldg(p + 1);
+            const float nC = __ldg(p + kTilePitch), nW = __ldg(p + kTilePitch - 1),
+                        nE = __ldg(p + kTilePitch + 1);
+            const float sC = __ldg(p - kTilePitch), sW = __ldg(p - kTilePitch - 1),
+                        sE = __ldg(p - kTilePitch + 1);
+            const float lap = lap9(nW, nC, nE, cW, cC, cE, sW, sC, sE);
+            const float gx = 0.5f * (cE - cW);
+            const float gyv = 0.5f * (nC - sC);
+            int gy = gy0 + y;
+            if (gy >= L) gy -= L;
+            const int gxg = x < split ? gx0 + x : x - split;
+            const float So = s_other_n(__ldg(A.S_rd + (size_t)gy * Pp + gxg), cC, A.flags, 1u);
+            const float rhs =
+                rhs_pixel(lap, cC, So, gx, gyv, gam, dwC, volC, repC, vx, vy, mrel);
+            const float pnew = cC + dtf * rhs;
+            const int a = x - sx, b = y - sy;
+            if ((unsigned)a < (unsigned)dwx && (unsigned)b < (unsigned)dwy)
+                tile_out[(size_t)(dty0 + b) * kTilePitch + dtx0 + a] = pnew;
+        }
+    }
+    const int DB = (dwy + K - 1) / K;
+    const int db0 = min(dwy, rank * DB), db1 = min(dwy, db0 + DB);
+    for (int b = db0 + warp; b < db1; b += NW) {
+        const int j = b + sy;
+        const bool jin = (unsigned)j < (unsigned)WY;
+        float* orow = tile_out + (size_t)(dty0 + b) * kTilePitch + dtx0;
+        for (int a = lane; a < dwx; a += 32) {
+            const int i = a + sx;
+            if (!(jin && (unsigned)i < (unsigned)WX)) orow[a] = 0.0f;
+        }
+    }
+    dev::cluster_sync();
+
+    PixelAcc acc;
+    acc.blox = dwx;
+    acc.bloy = dwy;
+    for (int b = db0 + warp; b < db1; b += NW) {
+        int gy = P.gy0n + b;
+        if (gy >= L) gy -= L;
+        const float* orow = tile_out + (size_t)(dty0 + b) * kTilePitch + dtx0;
+        uint32_t* srow = A.S_sc + (size_t)gy * Pp;
+        for (int a = lane; a < dwx; a += 32) {
+            const float pn = __ldcg(orow + a);
+            dest_pixel(A, acc, pn, a, b, srow, P.gx0n, L);
+            if (fm) {
+                const float e = a + 1 < dwx ? __ldcg(orow + a + 1) : 0.0f;
+                const float w = a > 0 ? __ldcg(orow + a - 1) : 0.0f;
+                const float nn = b + 1 < dwy ? __ldcg(orow + kTilePitch + a) : 0.0f;
+                const float ss = b > 0 ? __ldcg(orow - kTilePitch + a) : 0.0f;
+                const float pgx = 0.5f * (e - w), pgy = 0.5f * (nn - ss);
+                acc.Per += (double)sqrtf(pgx * pgx + pgy * pgy);
+            }
+        }
+    }
+    reduce_moments<K, NW>(A, P, rank, R, par, fm, acc);
+}
+
+}  // namespace pfb

@@ -133,6 +133,7 @@ _SIGS = {
     "pfb_step2d_configure": (I, []),
     "pfb_step2d_grid": (I, [I, I]),
     "pfb_step2d_launch": (I, [C.POINTER(StepArgs2D), I, P]),
+    "pfb_step2d_launch_ex": (I, [C.POINTER(StepArgs2D), I, I, P]),
     "pfb_device_status": (I, [C.POINTER(C.c_uint), I]),
     "pfb_init_tiles2d": (I, [P, P, P, P, I, I, P, P, C.c_float, C.c_float, P]),
     "pfb_init_moments2d": (I, [P, P, P, I, P]),

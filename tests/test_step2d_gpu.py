@@ -32,10 +32,15 @@ PHI_TOL_1 = 2e-6
 PHI_TOL_1000 = 1e-5
 
 
-def launch_pfb(cluster):
+def launch_pfb(cluster, variant=0):
     def f(a):
-        return pfb200.lib().pfb_step2d_launch(C.byref(a), cluster, None)
+        return pfb200.lib().pfb_step2d_launch_ex(C.byref(a), cluster, variant, None)
     return f
+
+
+# (cluster size, kernel variant): one cluster per cell with 2/4/8 CTAs, and
+# the persistent pipelined kernel (clusters of 8, the default)
+KERNELS = [(2, 1), (4, 1), (8, 1), (8, 2)]
 
 
 def launch_ref(a):
@@ -61,19 +66,23 @@ def assert_cells_match(a, b, vel_rtol=1e-5, moment_rtol=1e-7):
         np.testing.assert_allclose(a[k], b[k], rtol=1e-6, atol=1e-12, err_msg=k)
 
 
-@pytest.fixture(scope="module")
-def synth():
-    cells, phi = synthetic_all_classes(L=701)
-    p = params(701, 6, R=12.0, tau=0.02, full_moment_every=1)  # p_tumble ~ 0.39; fm every step
+@pytest.fixture(scope="module", params=[(701, 1), (704, 1), (704, 100), (701, 100)],
+                ids=["L701-fm", "L704-fm", "L704", "L701"])
+def synth(request):
+    # odd and multiple-of-4 sides (the second stages S with bulk copies);
+    # full-moment steps every step or not on the tested step
+    L, fme = request.param
+    cells, phi = synthetic_all_classes(L=L)
+    p = params(L, 6, R=12.0, tau=0.02, full_moment_every=fme)  # p_tumble ~ 0.39
     return p, cells, phi
 
 
-@pytest.mark.parametrize("cluster", [2, 4, 8])
-def test_one_step_all_classes_vs_oracle(synth, cluster):
+@pytest.mark.parametrize("cluster,variant", KERNELS)
+def test_one_step_all_classes_vs_oracle(synth, cluster, variant):
     p, cells, phi = synth
     step = 9000037
     ds = DeviceState2D(p, cells, phi, step=step)
-    ds.step_with(launch_pfb(cluster))
+    ds.step_with(launch_pfb(cluster, variant))
     g_cells, g_phi, g_S, g_flags = ds.get_cells(), ds.get_phi(), ds.get_S(), ds.get_flags()
     o = oracle_step(p, cells, phi, step)
     o_cells, o_phi = o.cells(), o.phi()
@@ -95,36 +104,41 @@ def test_one_step_all_classes_vs_oracle(synth, cluster):
     np.testing.assert_array_equal(g_flags, o.flags())
 
 
-def test_cluster_sizes_agree(synth):
+def test_kernel_variants_agree(synth):
     p, cells, phi = synth
     out = {}
-    for k in (2, 4, 8):
+    for kv in KERNELS:
         ds = DeviceState2D(p, cells, phi, step=123)
         for _ in range(3):
-            ds.step_with(launch_pfb(k))
-        out[k] = (ds.get_cells(), ds.get_phi())
-    for k in (2, 8):
-        assert_cells_match(out[k][0], out[4][0], vel_rtol=1e-6, moment_rtol=1e-9)
-        assert max_world_diff(out[k][1], out[k][0], out[4][1], out[4][0], p.L) <= 1e-6
+            ds.step_with(launch_pfb(*kv))
+        out[kv] = (ds.get_cells(), ds.get_phi(), ds.get_S())
+    base = out[(4, 1)]
+    for kv in KERNELS:
+        assert_cells_match(out[kv][0], base[0], vel_rtol=1e-6, moment_rtol=1e-9)
+        assert max_world_diff(out[kv][1], out[kv][0], base[1], base[0], p.L) <= 1e-6
+        np.testing.assert_array_equal(out[kv][2][:, :p.L],
+                                      s_from_phi(out[kv][1], out[kv][0], p.L)[:, :p.L])
 
 
-def test_deterministic_rerun(synth):
+@pytest.mark.parametrize("cluster,variant", [(4, 1), (8, 2)])
+def test_deterministic_rerun(synth, cluster, variant):
     p, cells, phi = synth
     res = []
     for _ in range(2):
         ds = DeviceState2D(p, cells, phi, step=5)
         for _ in range(4):
-            ds.step_with(launch_pfb(4))
+            ds.step_with(launch_pfb(cluster, variant))
         res.append((ds.get_cells().tobytes(), ds.get_phi().tobytes(), ds.get_S().tobytes()))
     assert res[0] == res[1]
 
 
 @pytest.mark.skipif(not oracle2d.ref_available(), reason="reference build absent")
-def test_one_step_all_classes_vs_reference_kernel(synth):
+@pytest.mark.parametrize("cluster,variant", [(4, 1), (8, 2)])
+def test_one_step_all_classes_vs_reference_kernel(synth, cluster, variant):
     p, cells, phi = synth
     step = 9000037
     a = DeviceState2D(p, cells, phi, step=step)
-    a.step_with(launch_pfb(4))
+    a.step_with(launch_pfb(cluster, variant))
     b = DeviceState2D(p, cells, phi, step=step)
     b.step_with(launch_ref)
     ca, cb = a.get_cells(), b.get_cells()
@@ -150,7 +164,7 @@ def test_1000_steps_vs_oracle_and_fp64():
     p, cells, phi = c1_like_state()
     ds = DeviceState2D(p, cells, phi, step=0)
     for _ in range(1000):
-        ds.step_with(launch_pfb(4))
+        ds.step_with(launch_pfb(8, 2))
     g_cells, g_phi = ds.get_cells(), ds.get_phi()
     o32 = oracle_step(p, cells, phi, 0, n=1000)
     o_cells, o_phi = o32.cells(), o32.phi()
@@ -173,13 +187,14 @@ def test_1000_steps_vs_oracle_and_fp64():
 
 @pytest.mark.slow
 @pytest.mark.skipif(not oracle2d.ref_available(), reason="reference build absent")
-def test_1000_steps_vs_reference_kernel():
+@pytest.mark.parametrize("cluster,variant", [(4, 1), (8, 2)])
+def test_1000_steps_vs_reference_kernel(cluster, variant):
     p, cells, phi = c1_like_state()
     a = DeviceState2D(p, cells, phi, step=0)
     b = DeviceState2D(p, cells, phi, step=0)
     worst = {}
     for n in range(1, 1001):
-        a.step_with(launch_pfb(4))
+        a.step_with(launch_pfb(cluster, variant))
         b.step_with(launch_ref)
         if n in (1, 10, 1000):
             ca, cb = a.get_cells(), b.get_cells()
