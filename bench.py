@@ -263,6 +263,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=60)
     ap.add_argument("--impl", default="pfb", choices=["pfb", "reference"])
     ap.add_argument("--cluster", type=int, default=8)
+    ap.add_argument("--variant", type=int, default=0,
+                    help="0 default, 1 one cluster per cell, 2 persistent, 3 pipelined kernel "
+                         "with one cluster per cell")
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=int(os.environ.get("PFB_CPU_STEPS", "6")))
     ap.add_argument("--no-e2e", action="store_true")
@@ -287,7 +290,8 @@ def main():
 
     p = workload_params(1234 + rank)
     cx, cy = workload_centres(p)
-    sim = pfb200.Sim2D(p, cx, cy, device=device, cluster=a.cluster, use_graph=not a.no_graph)
+    sim = pfb200.Sim2D(p, cx, cy, device=device, cluster=a.cluster, use_graph=not a.no_graph,
+                       variant=a.variant)
     init_cells = sim.cells()
     init_phi = sim.phi() if (rank == 0 and world == 1) or not a.no_e2e else None
     alg = algorithmic_bytes(init_cells, p.L)
@@ -374,7 +378,8 @@ def main():
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "L": L_SIDE, "cells": N_CELLS, "radius": RADIUS,
                        "sites_per_step": sites, "window": "reference class-0 window 144^2",
-                       "cluster_ctas_per_cell": a.cluster, "cuda_graph": not a.no_graph,
+                       "cluster_ctas_per_cell": a.cluster, "kernel_variant": a.variant,
+                       "cuda_graph": not a.no_graph,
                        "l2": "inputs larger than L2: two 340 MB phi pools; per-step working "
                              "set 85 MB phi read + 85 MB phi written + 3 x 16.8 MB aggregate "
                              "slots; no flush between steps",

@@ -200,8 +200,9 @@ int pfb_step2d_grid(int num_cells, int cluster);
 int pfb_step2d_launch(const pfb_step_args2d* args, int cluster, void* stream);
 
 /* As pfb_step2d_launch with an explicit kernel variant: 0 = default for the
- * cluster size, 1 = one cluster per cell, 2 = persistent pipelined clusters
- * (cluster must be 8). Both variants compute the same update. */
+ * cluster size, 1 = one cluster per cell, 2 = persistent pipelined clusters,
+ * 3 = the pipelined kernel with one cluster per cell (2 and 3 need cluster
+ * 8). All variants compute the same update. */
 int pfb_step2d_launch_ex(const pfb_step_args2d* args, int cluster, int variant,
                          void* stream);
 
@@ -294,8 +295,10 @@ pfb_sim2d* pfb_sim2d_create_from_state(const pfb_params2d* p,
                                        const float* phi, long long step,
                                        int device);
 void pfb_sim2d_destroy(pfb_sim2d* s);
-/* Tuning knobs: cluster CTAs per cell (2/4/8) and CUDA-graph use. */
+/* Tuning knobs: cluster CTAs per cell (2/4/8), kernel variant (as in
+ * pfb_step2d_launch_ex) and CUDA-graph use. */
 int pfb_sim2d_set_cluster(pfb_sim2d* s, int cluster);
+int pfb_sim2d_set_variant(pfb_sim2d* s, int variant);
 int pfb_sim2d_set_graph(pfb_sim2d* s, int use_graph);
 /* Advance `steps` steps on the simulator's stream (asynchronous). */
 int pfb_sim2d_advance(pfb_sim2d* s, long long steps);

@@ -42,6 +42,32 @@ __device__ __forceinline__ double ld_cluster_f64(uint32_t addr) {
     return v;
 }
 
+__device__ __forceinline__ double2 ld_cluster_v2f64(uint32_t addr) {
+    double2 v;
+    asm volatile("ld.shared::cluster.v2.f64 {%0, %1}, [%2];"
+                 : "=d"(v.x), "=d"(v.y)
+                 : "r"(addr)
+                 : "memory");
+    return v;
+}
+
+__device__ __forceinline__ int4 ld_cluster_v4s32(uint32_t addr) {
+    int4 v;
+    asm volatile("ld.shared::cluster.v4.s32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "r"(addr)
+                 : "memory");
+    return v;
+}
+
+// Sum over lanes 0..n-1 of v in ascending lane order, result in every lane
+// (a fixed order, so the result does not depend on timing).
+__device__ __forceinline__ double ordered_lane_sum(double v, int n) {
+    double s = 0.0;
+    for (int l = 0; l < n; ++l) s += __shfl_sync(0xFFFFFFFFu, v, l);
+    return s;
+}
+
 __device__ __forceinline__ int ld_cluster_s32(uint32_t addr) {
     int v;
     asm volatile("ld.shared::cluster.s32 %0, [%1];" : "=r"(v) : "r"(addr) : "memory");

@@ -41,6 +41,7 @@ struct pfb_sim2d {
     cudaStream_t stream = nullptr;
     long long steps_done = 0;
     int cluster = 8;
+    int variant = 0;
     bool use_graph = true;
     bool graph_ready = false;
     cudaGraph_t graph = nullptr;
@@ -90,7 +91,7 @@ struct pfb_sim2d {
 
     int launch_one(int slot) {
         const pfb_step_args2d a = args_for_slot(slot);
-        return step2d_launch(&a, cluster, stream);
+        return step2d_launch_variant(&a, cluster, variant, stream);
     }
 
     void drop_graph() {
@@ -354,6 +355,14 @@ int pfb_sim2d_set_cluster(pfb_sim2d* s, int cluster) {
     if (cluster != 2 && cluster != 4 && cluster != 8) return set_error(PFB_E_CONFIG, "cluster must be 2, 4 or 8");
     if (cluster != s->cluster) s->drop_graph();
     s->cluster = cluster;
+    return PFB_OK;
+}
+
+int pfb_sim2d_set_variant(pfb_sim2d* s, int variant) {
+    if (!s) return set_error(PFB_E_ARG, "null sim");
+    if (variant < 0 || variant > 3) return set_error(PFB_E_CONFIG, "unknown kernel variant");
+    if (variant != s->variant) s->drop_graph();
+    s->variant = variant;
     return PFB_OK;
 }
 

@@ -419,11 +419,11 @@ int step2d_launch_variant(const pfb_step_args2d* a, int cluster, int variant,
     if (cluster != 2 && cluster != 4 && cluster != 8)
         return set_error(PFB_E_CONFIG, "cluster must be 2, 4 or 8");
     if (variant == 0) variant = cluster == 8 ? 2 : 1;
-    if (variant == 2 && cluster != 8)
-        return set_error(PFB_E_CONFIG, "the persistent kernel uses clusters of 8");
-    if (variant != 1 && variant != 2) return set_error(PFB_E_CONFIG, "unknown kernel variant");
+    if ((variant == 2 || variant == 3) && cluster != 8)
+        return set_error(PFB_E_CONFIG, "the pipelined kernel uses clusters of 8");
+    if (variant < 1 || variant > 3) return set_error(PFB_E_CONFIG, "unknown kernel variant");
     if (A.N == 0) return PFB_OK;
-    if (variant == 2) return persist2d_launch(A, stream);
+    if (variant >= 2) return persist2d_launch(A, stream, variant == 3);
     int rc = step2d_configure_device();
     if (rc) return rc;
     cudaError_t e = cluster == 2   ? launch_k<2>(A, stream)

@@ -221,18 +221,21 @@ template <int NW>
 struct RedScratch {
     double red_d[NW][4];
     int red_i[NW][5];
-    double part_I[2][2];
-    double part_M[2][4];
-    int part_B[2][5];
+    alignas(16) double part_I[2][2];
+    alignas(16) double part_M[2][4];
+    alignas(16) int part_B[2][8];
     float vx, vy;
 };
 
-// Interaction integral of this CTA -> cluster total (ascending ranks) ->
-// velocity, identical in every CTA. Rank 0 stores v and I in the cell record.
+// Interaction integral of this CTA -> cluster total -> velocity, identical
+// in every CTA. Sums run in ascending warp, then ascending rank order: lanes
+// of warp 0 fetch the partials in parallel and add them in lane order. Rank 0
+// stores v and I in the cell record.
 template <int K, int NW>
 __device__ __forceinline__ void reduce_force(const pfb_step_args2d& A, const CellPlan& P,
                                              int rank, RedScratch<NW>& R, int par, double aIx,
                                              double aIy) {
+    static_assert(NW <= 32 && K <= 32, "one lane per warp and per rank");
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     aIx = dev::warp_sum_down(aIx);
     aIy = dev::warp_sum_down(aIy);
@@ -241,34 +244,36 @@ __device__ __forceinline__ void reduce_force(const pfb_step_args2d& A, const Cel
         R.red_d[warp][1] = aIy;
     }
     __syncthreads();
-    if (tid == 0) {
-        double s0 = 0.0, s1 = 0.0;
-        for (int w = 0; w < NW; ++w) {
-            s0 += R.red_d[w][0];
-            s1 += R.red_d[w][1];
+    if (warp == 0) {
+        const double px = lane < NW ? R.red_d[lane][0] : 0.0;
+        const double py = lane < NW ? R.red_d[lane][1] : 0.0;
+        const double s0 = dev::ordered_lane_sum(px, NW);
+        const double s1 = dev::ordered_lane_sum(py, NW);
+        if (lane == 0) {
+            R.part_I[par][0] = s0;
+            R.part_I[par][1] = s1;
         }
-        R.part_I[par][0] = s0;
-        R.part_I[par][1] = s1;
     }
     dev::cluster_sync();
-    if (tid == 0) {
-        double sIx = 0.0, sIy = 0.0;
-        const uint32_t base = dev::smem_addr(&R.part_I[par][0]);
-        for (int r = 0; r < K; ++r) {
-            const uint32_t a = dev::map_to_rank(base, (uint32_t)r);
-            sIx += dev::ld_cluster_f64(a);
-            sIy += dev::ld_cluster_f64(a + 8);
-        }
-        const double vxd = (double)P.vA * (double)P.pcos + (double)A.mot_coeff * sIx;
-        const double vyd = (double)P.vA * (double)P.psin + (double)A.mot_coeff * sIy;
-        R.vx = (float)vxd;
-        R.vy = (float)vyd;
-        if (rank == 0) {
-            pfb_cell2d& cs = A.cell[P.n];
-            cs.vx = (float)vxd;
-            cs.vy = (float)vyd;
-            cs.Ix = sIx;
-            cs.Iy = sIy;
+    if (warp == 0) {
+        double2 v = make_double2(0.0, 0.0);
+        if (lane < K)
+            v = dev::ld_cluster_v2f64(
+                dev::map_to_rank(dev::smem_addr(&R.part_I[par][0]), (uint32_t)lane));
+        const double sIx = dev::ordered_lane_sum(v.x, K);
+        const double sIy = dev::ordered_lane_sum(v.y, K);
+        if (lane == 0) {
+            const double vxd = (double)P.vA * (double)P.pcos + (double)A.mot_coeff * sIx;
+            const double vyd = (double)P.vA * (double)P.psin + (double)A.mot_coeff * sIy;
+            R.vx = (float)vxd;
+            R.vy = (float)vyd;
+            if (rank == 0) {
+                pfb_cell2d& cs = A.cell[P.n];
+                cs.vx = (float)vxd;
+                cs.vy = (float)vyd;
+                cs.Ix = sIx;
+                cs.Iy = sIy;
+            }
         }
     }
     __syncthreads();
@@ -304,37 +309,54 @@ __device__ __forceinline__ void reduce_moments(const pfb_step_args2d& A, const C
         R.red_i[warp][4] = acc.pmaxb;
     }
     __syncthreads();
-    if (tid == 0) {
-        double m[4] = {0.0, 0.0, 0.0, 0.0};
-        int b[5] = {P.dwx, -1, P.dwy, -1, 0};
-        for (int w = 0; w < NW; ++w) {
-            for (int k = 0; k < 4; ++k) m[k] += R.red_d[w][k];
-            b[0] = min(b[0], R.red_i[w][0]);
-            b[1] = max(b[1], R.red_i[w][1]);
-            b[2] = min(b[2], R.red_i[w][2]);
-            b[3] = max(b[3], R.red_i[w][3]);
-            b[4] = max(b[4], R.red_i[w][4]);
+    if (warp == 0) {
+        double m[4];
+        for (int k = 0; k < 4; ++k)
+            m[k] = dev::ordered_lane_sum(lane < NW ? R.red_d[lane][k] : 0.0, NW);
+        int b0 = lane < NW ? R.red_i[lane][0] : P.dwx;
+        int b1 = lane < NW ? R.red_i[lane][1] : -1;
+        int b2 = lane < NW ? R.red_i[lane][2] : P.dwy;
+        int b3 = lane < NW ? R.red_i[lane][3] : -1;
+        int b4 = lane < NW ? R.red_i[lane][4] : 0;
+        b0 = __reduce_min_sync(0xFFFFFFFFu, b0);
+        b1 = __reduce_max_sync(0xFFFFFFFFu, b1);
+        b2 = __reduce_min_sync(0xFFFFFFFFu, b2);
+        b3 = __reduce_max_sync(0xFFFFFFFFu, b3);
+        b4 = __reduce_max_sync(0xFFFFFFFFu, b4);
+        if (lane == 0) {
+            for (int k = 0; k < 4; ++k) R.part_M[par][k] = m[k];
+            R.part_B[par][0] = b0;
+            R.part_B[par][1] = b1;
+            R.part_B[par][2] = b2;
+            R.part_B[par][3] = b3;
+            R.part_B[par][4] = b4;
         }
-        for (int k = 0; k < 4; ++k) R.part_M[par][k] = m[k];
-        for (int k = 0; k < 5; ++k) R.part_B[par][k] = b[k];
     }
     dev::cluster_sync();
-    if (rank == 0 && tid == 0) {
-        double m[4] = {0.0, 0.0, 0.0, 0.0};
-        int b[5] = {P.dwx, -1, P.dwy, -1, 0};
-        const uint32_t bm = dev::smem_addr(&R.part_M[par][0]);
-        const uint32_t bb = dev::smem_addr(&R.part_B[par][0]);
-        for (int r = 0; r < K; ++r) {
-            const uint32_t am = dev::map_to_rank(bm, (uint32_t)r);
-            const uint32_t ab = dev::map_to_rank(bb, (uint32_t)r);
-            for (int k = 0; k < 4; ++k) m[k] += dev::ld_cluster_f64(am + 8u * k);
-            b[0] = min(b[0], dev::ld_cluster_s32(ab + 0));
-            b[1] = max(b[1], dev::ld_cluster_s32(ab + 4));
-            b[2] = min(b[2], dev::ld_cluster_s32(ab + 8));
-            b[3] = max(b[3], dev::ld_cluster_s32(ab + 12));
-            b[4] = max(b[4], dev::ld_cluster_s32(ab + 16));
+    if (rank == 0 && warp == 0) {
+        double2 m01 = make_double2(0.0, 0.0), m23 = make_double2(0.0, 0.0);
+        int4 bq = make_int4(P.dwx, -1, P.dwy, -1);
+        int b4 = 0;
+        if (lane < K) {
+            const uint32_t am = dev::map_to_rank(dev::smem_addr(&R.part_M[par][0]), (uint32_t)lane);
+            const uint32_t ab = dev::map_to_rank(dev::smem_addr(&R.part_B[par][0]), (uint32_t)lane);
+            m01 = dev::ld_cluster_v2f64(am);
+            m23 = dev::ld_cluster_v2f64(am + 16);
+            bq = dev::ld_cluster_v4s32(ab);
+            b4 = dev::ld_cluster_s32(ab + 16);
         }
-        commit_cell(A, P, fm, m, b);
+        double m[4];
+        m[0] = dev::ordered_lane_sum(m01.x, K);
+        m[1] = dev::ordered_lane_sum(m01.y, K);
+        m[2] = dev::ordered_lane_sum(m23.x, K);
+        m[3] = dev::ordered_lane_sum(m23.y, K);
+        int b[5];
+        b[0] = __reduce_min_sync(0xFFFFFFFFu, bq.x);
+        b[1] = __reduce_max_sync(0xFFFFFFFFu, bq.y);
+        b[2] = __reduce_min_sync(0xFFFFFFFFu, bq.z);
+        b[3] = __reduce_max_sync(0xFFFFFFFFu, bq.w);
+        b[4] = __reduce_max_sync(0xFFFFFFFFu, b4);
+        if (lane == 0) commit_cell(A, P, fm, m, b);
     }
 }
 

@@ -75,6 +75,12 @@ template <int CLS> struct PMap {
     static_assert(NQ * G <= kPThreads, "thread map");
 };
 
+// Decisions for one cell, kept out of line: it runs once per cell in one lane.
+__device__ __noinline__ void plan_cell_lane(const pfb_step_args2d& A, int n, int cls,
+                                            unsigned long long step, CellPlan& out, bool leader) {
+    plan_cell(A, n, cls, step, out, leader);
+}
+
 __device__ __forceinline__ void fence_proxy_async() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
@@ -171,15 +177,19 @@ __device__ __noinline__ void staged_persist(const pfb_step_args2d& A, const Cell
     const bool s_tma = (L & 3) == 0;
     const int soff = s_tma ? (P.gx0 & 3) : 0;
 
-    // Zero ring and out-of-window rows (never targets of the copies).
+    // Zero ring of in-window rows and whole out-of-window rows (never targets
+    // of the copies): rank 0 has two rows above the window, the last rank two
+    // below it.
     for (int k = tid; k < RB + 4; k += kPThreads) {
         const int y = y0 - 2 + k;
         if (y >= 0 && y < WY) {
             phi_s[k * PX + 3] = 0.0f;
             phi_s[k * PX + 4 + WX] = 0.0f;
-        } else {
-            for (int c = 0; c < PX; ++c) phi_s[k * PX + c] = 0.0f;
         }
+    }
+    if (rank == 0 || rank == kPK - 1) {
+        const int kb = rank == 0 ? 0 : RB + 2;
+        for (int i = tid; i < 2 * PX; i += kPThreads) phi_s[kb * PX + i] = 0.0f;
     }
     if (!s_tma) {
         // Odd lattice sides: gather S rows with plain loads.
@@ -535,7 +545,7 @@ __global__ void __launch_bounds__(kPThreads, 3)
                 const int kk = k + lane;
                 if (kk < ncells) {
                     const int n = cell_of(kk);
-                    plan_cell(A, n, (int)A.cell_cls[n], step, sh.plan[lane], rank == 0);
+                    plan_cell_lane(A, n, (int)A.cell_cls[n], step, sh.plan[lane], rank == 0);
                 }
             }
             __syncthreads();
@@ -580,7 +590,7 @@ int g_max_clusters[64] = {0};
 
 }  // namespace
 
-int persist2d_launch(const pfb_step_args2d& A, cudaStream_t stream) {
+int persist2d_launch(const pfb_step_args2d& A, cudaStream_t stream, bool one_cell_per_cluster) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return set_error(PFB_E_CUDA, "cudaGetDevice failed");
     if (dev < 0 || dev >= 64) return set_error(PFB_E_CONFIG, "device index out of range");
@@ -606,7 +616,8 @@ int persist2d_launch(const pfb_step_args2d& A, cudaStream_t stream) {
             return set_error(PFB_E_CUDA, "cluster occupancy query: %s", cudaGetErrorString(e));
         g_max_clusters[dev] = nc;
     }
-    const int clusters = A.N < g_max_clusters[dev] ? A.N : g_max_clusters[dev];
+    const int clusters =
+        (one_cell_per_cluster || A.N < g_max_clusters[dev]) ? A.N : g_max_clusters[dev];
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(clusters * kPK), 1, 1);
     cfg.blockDim = dim3(kPThreads, 1, 1);

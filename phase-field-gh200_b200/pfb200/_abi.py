@@ -156,6 +156,7 @@ _SIGS = {
     "pfb_sim2d_destroy": (None, [P]),
     "pfb_sim2d_set_cluster": (I, [P, I]),
     "pfb_sim2d_set_graph": (I, [P, I]),
+    "pfb_sim2d_set_variant": (I, [P, I]),
     "pfb_sim2d_advance": (I, [P, C.c_longlong]),
     "pfb_sim2d_sync": (I, [P]),
     "pfb_sim2d_step": (C.c_longlong, [P]),

@@ -111,7 +111,7 @@ class Sim2D:
 
     def __init__(self, params: SimParams2D, cx=None, cy=None, *, device: int = 0,
                  cells: np.ndarray | None = None, phi: np.ndarray | None = None,
-                 step: int = 0, cluster: int = 4, use_graph: bool = True):
+                 step: int = 0, cluster: int = 8, use_graph: bool = True, variant: int = 0):
         params.validate()
         self.params = params
         self._pc = params.to_c()
@@ -132,6 +132,7 @@ class Sim2D:
             raise RuntimeError("pfb_sim2d_create failed: " + L.pfb_last_error().decode())
         self._h = h
         self.set_cluster(cluster)
+        check(L.pfb_sim2d_set_variant(h, variant), "set_variant")
         check(L.pfb_sim2d_set_graph(h, 1 if use_graph else 0), "set_graph")
 
     # ------------------------------------------------------------------ control

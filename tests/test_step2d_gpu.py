@@ -40,7 +40,7 @@ def launch_pfb(cluster, variant=0):
 
 # (cluster size, kernel variant): one cluster per cell with 2/4/8 CTAs, and
 # the persistent pipelined kernel (clusters of 8, the default)
-KERNELS = [(2, 1), (4, 1), (8, 1), (8, 2)]
+KERNELS = [(2, 1), (4, 1), (8, 1), (8, 2), (8, 3)]
 
 
 def launch_ref(a):
