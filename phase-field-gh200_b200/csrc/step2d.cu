@@ -35,7 +35,7 @@
 
 namespace pfb {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 288;
 constexpr int kWarps = kThreads / 32;
 constexpr int kHeaderBytes = 1024;
 
@@ -54,12 +54,12 @@ static_assert(sizeof(StepShared) <= kHeaderBytes, "shared header too large");
 
 __host__ __device__ constexpr int band_rows(int wy, int k) { return (wy + k - 1) / k; }
 
-// Rows per work item of the column-rolling passes: balances the 256 threads
+// Rows per work item of the column-rolling passes: balances the threads
 // against the (rows + 2) shared loads a column run costs.
 __host__ __device__ constexpr int pick_run(int wx, int rows) {
     int best_h = 1;
     long best = -1;
-    for (int h = 2; h <= 16; ++h) {
+    for (int h = 2; h <= 48; ++h) {
         const int runs = (rows + h - 1) / h;
         const int iters = (wx * runs + kThreads - 1) / kThreads;
         const long cost = (long)iters * (h + 2);
@@ -71,10 +71,9 @@ __host__ __device__ constexpr int pick_run(int wx, int rows) {
     return best_h;
 }
 
+// Both staged arrays use the row pitch WX + 8 words.
 __host__ __device__ constexpr int staged_bytes(int cls, int k) {
-    return kHeaderBytes +
-           (band_rows(window_of(cls).wy, k) + 4) * (window_of(cls).wx + 8) * 4 +
-           (band_rows(window_of(cls).wy, k) + 2) * window_of(cls).wx * 4;
+    return kHeaderBytes + (2 * band_rows(window_of(cls).wy, k) + 6) * (window_of(cls).wx + 8) * 4;
 }
 
 __host__ __device__ constexpr int step_smem_bytes(int k) {
@@ -85,11 +84,14 @@ __host__ __device__ constexpr int step_smem_bytes(int k) {
 
 // ---------------------------------------------------------------------------
 // Staged path: classes 0-3.
-// Shared layout after the header:
-//   phi_s [RB+4][WX+8] f32 : window rows y0-2 .. y0+RB+1; column x at 4+x,
-//                            columns -1 and WX are the synthesized zero ring
-//   ps_s  [RB+2][WX]  u32  : window rows y0-1 .. y0+RB; holds q_S, then
-//                            phi^{n+1} written in place
+// Shared layout after the header (row pitch PX = WX + 8 words):
+//   phi_s [RB+4][PX] f32 : window rows y0-2 .. y1+1; column x at 4+x; columns
+//                          -1 and WX are the synthesized zero ring
+//   ps_s  [RB+2][PX] u32 : window rows y0-1 .. y1; window column x at soff+x
+//                          (soff = gx0 & 3 when S is staged by bulk copies).
+//                          Holds q_S; pass 1 replaces own rows by S_other
+//                          (f32 bits); on full-moment steps phi^{n+1} is
+//                          written over it.
 // ---------------------------------------------------------------------------
 template <int CLS, int K>
 __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int rank,
@@ -112,6 +114,7 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
     const int y1 = y0 + RB;
     const float* tile_in = A.phi_in + (size_t)n * kTileArea;
     const int L = A.L, Pp = A.P;
+    const bool s_tma = (L & 3) == 0;
 
     if (tid == 0) {
         sh.abort = 0;
@@ -120,31 +123,56 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
         dev::mbar_init(&sh.bar, 1);
     }
     __syncthreads();
+    const int gx0 = sh.gx0, gy0 = sh.gy0;
+    const int soff = s_tma ? (gx0 & 3) : 0;
 
     const int ra = max(0, y0 - 2), rb = min(WY, y1 + 2);
+    const int sa = max(0, y0 - 1), sb = min(WY, y1 + 1);
     if (warp == 0) {
-        if (lane == 0) dev::mbar_arrive_expect_tx(&sh.bar, (uint32_t)((rb - ra) * WX * 4));
+        // Bulk copies: one per phi row; one or two per S row (split at the
+        // periodic seam), each starting on a 16-byte boundary.
+        const int gxa = gx0 - soff;
+        const bool wrap = gx0 + WX > L;
+        const int n1 = wrap ? L - gxa : min((soff + WX + 3) & ~3, Pp - gxa);
+        const int n2 = wrap ? ((gx0 + WX - L + 3) & ~3) : 0;
+        uint32_t bytes = 0;
+        for (int y = ra + lane; y < rb; y += 32) bytes += (uint32_t)(WX * 4);
+        if (s_tma)
+            for (int y = sa + lane; y < sb; y += 32) bytes += (uint32_t)((n1 + n2) * 4);
+        bytes = __reduce_add_sync(0xFFFFFFFFu, bytes);
+        if (lane == 0) dev::mbar_arrive_expect_tx(&sh.bar, bytes);
         __syncwarp();
         for (int y = ra + lane; y < rb; y += 32)
             dev::bulk_g2s(phi_s + (y - y0 + 2) * PX + 4,
                           tile_in + (size_t)(TY0 + y) * kTilePitch + TX0, (uint32_t)(WX * 4),
                           &sh.bar);
+        if (s_tma) {
+            for (int y = sa + lane; y < sb; y += 32) {
+                int gy = gy0 + y;
+                if (gy >= L) gy -= L;
+                const uint32_t* row = A.S_rd + (size_t)gy * Pp;
+                uint32_t* dst = ps_s + (y - y0 + 1) * PX;
+                dev::bulk_g2s(dst, row + gxa, (uint32_t)(n1 * 4), &sh.bar);
+                if (n2) dev::bulk_g2s(dst + (L - gxa), row, (uint32_t)(n2 * 4), &sh.bar);
+            }
+        }
         if (lane == 0) plan_cell(A, n, CLS, step, sh.plan, rank == 0);
     } else {
         const int t = tid - 32;
         constexpr int NT = kThreads - 32;
-        const int gx0 = sh.gx0, gy0 = sh.gy0;
-        const int split = min(WX, L - gx0);
-        const int sa = max(0, y0 - 1), sb = min(WY, y1 + 1);
-        const int cnt = (sb - sa) * WX;
-        for (int idx = t; idx < cnt; idx += NT) {
-            const int yy = idx / WX;
-            const int x = idx - yy * WX;
-            const int y = sa + yy;
-            int gy = gy0 + y;
-            if (gy >= L) gy -= L;
-            const int gx = x < split ? gx0 + x : x - split;
-            ps_s[(y - y0 + 1) * WX + x] = __ldg(A.S_rd + (size_t)gy * Pp + gx);
+        if (!s_tma) {
+            // lattice sides that are not a multiple of 4: plain gather
+            const int split = min(WX, L - gx0);
+            const int cnt = (sb - sa) * WX;
+            for (int idx = t; idx < cnt; idx += NT) {
+                const int yy = idx / WX;
+                const int x = idx - yy * WX;
+                const int y = sa + yy;
+                int gy = gy0 + y;
+                if (gy >= L) gy -= L;
+                const int gx = x < split ? gx0 + x : x - split;
+                ps_s[(y - y0 + 1) * PX + x] = __ldg(A.S_rd + (size_t)gy * Pp + gx);
+            }
         }
         // Zero ring columns of in-window rows; whole rows outside the window.
         for (int k = t; k < PHI_ROWS; k += NT) {
@@ -154,10 +182,9 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
                 phi_s[k * PX + 4 + WX] = 0.0f;
             }
         }
-        for (int k = 0; k < PHI_ROWS; ++k) {
-            const int y = y0 - 2 + k;
-            if (y >= 0 && y < WY) continue;
-            for (int c = t; c < PX; c += NT) phi_s[k * PX + c] = 0.0f;
+        if (rank == 0 || rank == K - 1) {
+            const int kb = rank == 0 ? 0 : RB + 2;
+            for (int i = t; i < 2 * PX; i += NT) phi_s[kb * PX + i] = 0.0f;
         }
     }
     if (!dev::mbar_wait_bounded(&sh.bar, 0, kWaitPolls)) {
@@ -167,7 +194,7 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
     __syncthreads();
     const bool abort = sh.abort != 0;
 
-    // ---- pass 1: interaction integral over own rows
+    // ---- pass 1: S_other (kept in place of q_S) and the interaction integral
     double aIx = 0.0, aIy = 0.0;
     if (!abort) {
         constexpr int H = pick_run(WX, RB);
@@ -178,18 +205,20 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
             const int ya = y0 + c * H;
             const int yb = min(y1, ya + H);
             const float* p = phi_s + (ya - y0 + 2) * PX + 4 + x;
-            const uint32_t* q = ps_s + (ya - y0 + 1) * WX + x;
+            uint32_t* q = ps_s + (ya - y0 + 1) * PX + soff + x;
             float sC = p[-PX];
             float cW = p[-1], cC = p[0], cE = p[1];
             for (int y = ya; y < yb; ++y) {
                 const float nC = p[PX];
-                const float So = s_other_n(*q, cC, A.flags, 1u);
+                // counted twice: the reference evaluates S_other in both passes
+                const float So = s_other_n(*q, cC, A.flags, 2u);
+                *q = __float_as_uint(So);
                 const float gx = 0.5f * (cE - cW);
                 const float gy = 0.5f * (nC - sC);
                 aIx += (double)(cC * gx * So);
                 aIy += (double)(cC * gy * So);
                 p += PX;
-                q += WX;
+                q += PX;
                 sC = cC;
                 cC = nC;
                 cW = p[-1];
@@ -199,101 +228,193 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
     }
     reduce_force<K, kWarps>(A, P, rank, sh.red, 0, aIx, aIy);
 
-    // ---- pass 2: Euler update of own rows plus a one-row halo, in place
-    if (!abort) {
-        const float gam = P.gam, dwC = P.dwC, volC = P.volC;
-        const float vx = sh.red.vx, vy = sh.red.vy, mrel = P.mrel;
-        const float repC = A.rep_coeff, dtf = A.dt;
-        const int ua = max(0, y0 - 1), ub = min(WY, y1 + 1);
-        constexpr int H = pick_run(WX, RB + 2);
-        constexpr int RUNS = (RB + 2 + H - 1) / H;
-        for (int item = tid; item < WX * RUNS; item += kThreads) {
-            const int c = item / WX;
-            const int x = item - c * WX;
-            const int ya = ua + c * H;
-            if (ya >= ub) continue;
-            const int yb = min(ub, ya + H);
-            const float* p = phi_s + (ya - y0 + 2) * PX + 4 + x;
-            uint32_t* q = ps_s + (ya - y0 + 1) * WX + x;
-            float sW = p[-PX - 1], sC = p[-PX], sE = p[-PX + 1];
-            float cW = p[-1], cC = p[0], cE = p[1];
-            for (int y = ya; y < yb; ++y) {
-                const float nW = p[PX - 1], nC = p[PX], nE = p[PX + 1];
-                const float lap = lap9(nW, nC, nE, cW, cC, cE, sW, sC, sE);
-                const float gx = 0.5f * (cE - cW);
-                const float gy = 0.5f * (nC - sC);
-                const bool own = (y >= y0) && (y < y1);
-                const float So = s_other_n(*q, cC, A.flags, own ? 1u : 0u);
-                const float rhs =
-                    rhs_pixel(lap, cC, So, gx, gy, gam, dwC, volC, repC, vx, vy, mrel);
-                const float pnew = cC + dtf * rhs;
-                *q = __float_as_uint(pnew);
-                sW = cW;
-                sC = cC;
-                sE = cE;
-                cW = nW;
-                cC = nC;
-                cE = nE;
-                p += PX;
-                q += WX;
-            }
+    const float gam = P.gam, dwC = P.dwC, volC = P.volC;
+    const float vx = sh.red.vx, vy = sh.red.vy, mrel = P.mrel;
+    const float repC = A.rep_coeff, dtf = A.dt;
+    const int sx = P.sx, sy = P.sy;
+    const int dwx = P.dwx, dwy = P.dwy, dtx0 = P.dtx0, dty0 = P.dty0;
+    const int gx0n = P.gx0n, gy0n = P.gy0n;
+    float* tile_out = A.phi_out + (size_t)n * kTileArea;
+    // Destination row b reads source row j = b + sy; rows above the window
+    // belong to rank 0, rows below it to rank K-1.
+    const int jlo = (rank == 0) ? -(1 << 20) : y0;
+    const int jhi = (rank == K - 1) ? (1 << 20) : y1;
+    const int b_lo = max(0, jlo - sy), b_hi = min(dwy, jhi - sy);
+    if (!abort && P.zero_tile) {
+        // the destination tile last held another class: clear outside the window
+        for (int b = b_lo + warp; b < b_hi; b += kWarps) {
+            float* trow = tile_out + (size_t)(dty0 + b) * kTilePitch;
+            for (int c = lane; c < kTilePitch; c += 32)
+                if (c < dtx0 || c >= dtx0 + dwx) trow[c] = 0.0f;
+        }
+        for (int t = rank + K * warp; t < kTilePitch; t += K * kWarps) {
+            if (t >= dty0 && t < dty0 + dwy) continue;
+            float* trow = tile_out + (size_t)t * kTilePitch;
+            for (int c = lane; c < kTilePitch; c += 32) trow[c] = 0.0f;
         }
     }
-    __syncthreads();
 
-    // ---- pass 3: recentring store, scatter, moments over owned destination rows
     PixelAcc acc;
-    acc.blox = P.dwx;
-    acc.bloy = P.dwy;
-    if (!abort) {
-        const int sx = P.sx, sy = P.sy;
-        const int dwx = P.dwx, dwy = P.dwy, dtx0 = P.dtx0, dty0 = P.dty0;
-        const int gx0n = P.gx0n, gy0n = P.gy0n;
-        float* tile_out = A.phi_out + (size_t)n * kTileArea;
-        // Destination row b reads source row j = b + sy; rows above the window
-        // belong to rank 0, rows below it to rank K-1.
-        const int jlo = (rank == 0) ? -(1 << 20) : y0;
-        const int jhi = (rank == K - 1) ? (1 << 20) : y1;
-        const int b_lo = max(0, jlo - sy), b_hi = min(dwy, jhi - sy);
-
-        if (P.zero_tile) {
-            for (int b = b_lo + warp; b < b_hi; b += kWarps) {
-                float* trow = tile_out + (size_t)(dty0 + b) * kTilePitch;
-                for (int c = lane; c < kTilePitch; c += 32)
-                    if (c < dtx0 || c >= dtx0 + dwx) trow[c] = 0.0f;
+    acc.blox = dwx;
+    acc.bloy = dwy;
+    if (!fm) {
+        // ---- pass 2, fused: Euler update, store, scatter and moments
+        const bool ident = sx == 0 && sy == 0 && P.dcls == CLS;
+        if (!abort) {
+            constexpr int H = pick_run(WX, RB);
+            constexpr int RUNS = (RB + H - 1) / H;
+            float pmaxf = 0.0f;
+            for (int item = tid; item < WX * RUNS; item += kThreads) {
+                const int c = item / WX;
+                const int x = item - c * WX;
+                const int ya = y0 + c * H;
+                const int yb = min(y1, ya + H);
+                const float* p = phi_s + (ya - y0 + 2) * PX + 4 + x;
+                const uint32_t* q = ps_s + (ya - y0 + 1) * PX + soff + x;
+                float sW = p[-PX - 1], sC = p[-PX], sE = p[-PX + 1];
+                float cW = p[-1], cC = p[0], cE = p[1];
+                int gxs = gx0 + x;
+                if (gxs >= L) gxs -= L;
+                const double xd = (double)x;
+                int yfirst = -1, ylast = -1;
+                int gy = gy0 + ya;
+                if (gy >= L) gy -= L;
+                float* o = tile_out + (size_t)(TY0 + ya) * kTilePitch + TX0 + x;
+                for (int y = ya; y < yb; ++y) {
+                    const float nW = p[PX - 1], nC = p[PX], nE = p[PX + 1];
+                    const float lap = lap9(nW, nC, nE, cW, cC, cE, sW, sC, sE);
+                    const float gx = 0.5f * (cE - cW);
+                    const float gyv = 0.5f * (nC - sC);
+                    const float rhs = rhs_pixel(lap, cC, __uint_as_float(*q), gx, gyv, gam, dwC,
+                                                volC, repC, vx, vy, mrel);
+                    const float pn = cC + dtf * rhs;
+                    if (ident) {
+                        __stcs(o, pn);
+                        if (fabsf(pn) <= 2.0f) {
+                            pmaxf = fmaxf(pmaxf, fabsf(pn));
+                        } else {
+                            if (!isfinite(pn)) atomicOr(A.flags + PFB_FLAG_NONFINITE, 1u);
+                            if (pn * pn > kPhiSqCap) atomicOr(A.flags + PFB_FLAG_Q_CLAMP, 1u);
+                            acc.pmaxb = max(acc.pmaxb, (int)__float_as_uint(fabsf(pn)));
+                        }
+                        const uint32_t qv = q_encode(pn);
+                        if (qv) {
+                            const uint32_t old = atomicAdd(A.S_sc + (size_t)gy * Pp + gxs, qv);
+                            if (old > 0xFFFFFFFFu - qv) atomicOr(A.flags + PFB_FLAG_S_OVERFLOW, 1u);
+                        }
+                        const double d = (double)pn * (double)pn;
+                        acc.V += d;
+                        acc.Cx += d * xd;
+                        acc.Cy += d * (double)y;
+                        if (pn > kSupportEps) {
+                            if (yfirst < 0) yfirst = y;
+                            ylast = y;
+                        }
+                    } else {
+                        const int a = x - sx, b = y - sy;
+                        if ((unsigned)a < (unsigned)dwx && (unsigned)b < (unsigned)dwy) {
+                            int gyn = gy0n + b;
+                            if (gyn >= L) gyn -= L;
+                            __stcs(tile_out + (size_t)(dty0 + b) * kTilePitch + dtx0 + a, pn);
+                            dest_pixel(A, acc, pn, a, b, A.S_sc + (size_t)gyn * Pp, gx0n, L);
+                        }
+                    }
+                    sW = cW;
+                    sC = cC;
+                    sE = cE;
+                    cW = nW;
+                    cC = nC;
+                    cE = nE;
+                    p += PX;
+                    q += PX;
+                    o += kTilePitch;
+                    if (++gy >= L) gy -= L;
+                }
+                if (yfirst >= 0) {
+                    acc.blox = min(acc.blox, x);
+                    acc.bhix = max(acc.bhix, x);
+                    acc.bloy = min(acc.bloy, yfirst);
+                    acc.bhiy = max(acc.bhiy, ylast);
+                }
             }
-            for (int t = rank + K * warp; t < kTilePitch; t += K * kWarps) {
-                if (t >= dty0 && t < dty0 + dwy) continue;
-                float* trow = tile_out + (size_t)t * kTilePitch;
-                for (int c = lane; c < kTilePitch; c += 32) trow[c] = 0.0f;
+            acc.pmaxb = max(acc.pmaxb, (int)__float_as_uint(pmaxf));
+            if (!ident) {
+                // destination pixels whose source lies outside the window
+                for (int b = b_lo + warp; b < b_hi; b += kWarps) {
+                    const int j = b + sy;
+                    const bool jin = (unsigned)j < (unsigned)WY;
+                    float* orow = tile_out + (size_t)(dty0 + b) * kTilePitch + dtx0;
+                    for (int a = lane; a < dwx; a += 32) {
+                        const int i = a + sx;
+                        if (!(jin && (unsigned)i < (unsigned)WX)) __stcs(orow + a, 0.0f);
+                    }
+                }
             }
         }
-
-        for (int b = b_lo + warp; b < b_hi; b += kWarps) {
-            const int j = b + sy;
-            const bool jin = (unsigned)j < (unsigned)WY;
-            const int jr = j - y0 + 1;  // ps_s row of source row j
-            int gy = gy0n + b;
-            if (gy >= L) gy -= L;
-            float* orow = tile_out + (size_t)(dty0 + b) * kTilePitch + dtx0;
-            uint32_t* srow = A.S_sc + (size_t)gy * Pp;
-            for (int a = lane; a < dwx; a += 32) {
-                const int i = a + sx;
-                const bool iin = (unsigned)i < (unsigned)WX;
-                const float pn = (jin && iin) ? __uint_as_float(ps_s[jr * WX + i]) : 0.0f;
-                __stcs(orow + a, pn);
-                dest_pixel(A, acc, pn, a, b, srow, gx0n, L);
-                if (fm) {
+    } else {
+        // ---- full-moment step: phi^{n+1} of own rows plus a one-row halo over
+        // the staged S (own rows hold S_other, halo rows q_S), then the
+        // destination pass with the perimeter.
+        if (!abort) {
+            const int ua = max(0, y0 - 1), ub = min(WY, y1 + 1);
+            constexpr int H = pick_run(WX, RB + 2);
+            constexpr int RUNS = (RB + 2 + H - 1) / H;
+            for (int item = tid; item < WX * RUNS; item += kThreads) {
+                const int c = item / WX;
+                const int x = item - c * WX;
+                const int ya = ua + c * H;
+                if (ya >= ub) continue;
+                const int yb = min(ub, ya + H);
+                const float* p = phi_s + (ya - y0 + 2) * PX + 4 + x;
+                uint32_t* q = ps_s + (ya - y0 + 1) * PX + soff + x;
+                float sW = p[-PX - 1], sC = p[-PX], sE = p[-PX + 1];
+                float cW = p[-1], cC = p[0], cE = p[1];
+                for (int y = ya; y < yb; ++y) {
+                    const float nW = p[PX - 1], nC = p[PX], nE = p[PX + 1];
+                    const float lap = lap9(nW, nC, nE, cW, cC, cE, sW, sC, sE);
+                    const float gx = 0.5f * (cE - cW);
+                    const float gy = 0.5f * (nC - sC);
+                    const bool own = (y >= y0) && (y < y1);
+                    const float So = own ? __uint_as_float(*q) : s_other_n(*q, cC, A.flags, 0u);
+                    const float rhs =
+                        rhs_pixel(lap, cC, So, gx, gy, gam, dwC, volC, repC, vx, vy, mrel);
+                    *q = __float_as_uint(cC + dtf * rhs);
+                    sW = cW;
+                    sC = cC;
+                    sE = cE;
+                    cW = nW;
+                    cC = nC;
+                    cE = nE;
+                    p += PX;
+                    q += PX;
+                }
+            }
+        }
+        __syncthreads();
+        if (!abort) {
+            for (int b = b_lo + warp; b < b_hi; b += kWarps) {
+                const int j = b + sy;
+                const bool jin = (unsigned)j < (unsigned)WY;
+                const int jr = j - y0 + 1;  // ps_s row of source row j
+                int gy = gy0n + b;
+                if (gy >= L) gy -= L;
+                float* orow = tile_out + (size_t)(dty0 + b) * kTilePitch + dtx0;
+                uint32_t* srow = A.S_sc + (size_t)gy * Pp;
+                const uint32_t* row = ps_s + jr * PX + soff;
+                for (int a = lane; a < dwx; a += 32) {
+                    const int i = a + sx;
+                    const bool iin = (unsigned)i < (unsigned)WX;
+                    const float pn = (jin && iin) ? __uint_as_float(row[i]) : 0.0f;
+                    __stcs(orow + a, pn);
+                    dest_pixel(A, acc, pn, a, b, srow, gx0n, L);
                     float e = 0.0f, w = 0.0f, nn = 0.0f, ss = 0.0f;
                     if (jin) {
-                        if ((unsigned)(i + 1) < (unsigned)WX) e = __uint_as_float(ps_s[jr * WX + i + 1]);
-                        if ((unsigned)(i - 1) < (unsigned)WX) w = __uint_as_float(ps_s[jr * WX + i - 1]);
+                        if ((unsigned)(i + 1) < (unsigned)WX) e = __uint_as_float(row[i + 1]);
+                        if ((unsigned)(i - 1) < (unsigned)WX) w = __uint_as_float(row[i - 1]);
                     }
                     if (iin) {
-                        if ((unsigned)(j + 1) < (unsigned)WY)
-                            nn = __uint_as_float(ps_s[(jr + 1) * WX + i]);
-                        if ((unsigned)(j - 1) < (unsigned)WY)
-                            ss = __uint_as_float(ps_s[(jr - 1) * WX + i]);
+                        if ((unsigned)(j + 1) < (unsigned)WY) nn = __uint_as_float(row[PX + i]);
+                        if ((unsigned)(j - 1) < (unsigned)WY) ss = __uint_as_float(row[-PX + i]);
                     }
                     const float pgx = 0.5f * (e - w), pgy = 0.5f * (nn - ss);
                     acc.Per += (double)sqrtf(pgx * pgx + pgy * pgy);
@@ -315,7 +436,7 @@ __device__ __forceinline__ void global_cell_v1(const pfb_step_args2d& A, int n, 
 }
 
 template <int K>
-__global__ void __launch_bounds__(kThreads, (K >= 8 ? 4 : 3))
+__global__ void __launch_bounds__(kThreads, 3)
     k_step2d(const __grid_constant__ pfb_step_args2d A) {
     extern __shared__ __align__(128) char smem[];
     const int tid = threadIdx.x;
