@@ -262,10 +262,8 @@ def main():
     ap.add_argument("--steps", type=int, default=6000)
     ap.add_argument("--warmup", type=int, default=60)
     ap.add_argument("--impl", default="pfb", choices=["pfb", "reference"])
-    ap.add_argument("--cluster", type=int, default=8)
-    ap.add_argument("--variant", type=int, default=0,
-                    help="0 default, 1 one cluster per cell, 2 persistent, 3 pipelined kernel "
-                         "with one cluster per cell")
+    ap.add_argument("--cluster", type=int, default=4, help="CTAs per cell (2, 4 or 8)")
+    ap.add_argument("--variant", type=int, default=0, help="kernel variant (0 = default)")
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=int(os.environ.get("PFB_CPU_STEPS", "6")))
     ap.add_argument("--no-e2e", action="store_true")
@@ -386,7 +384,7 @@ def main():
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "pfb::k_step2d_persist (clusters of 8)" if a.cluster == 8 else f"pfb::k_step2d<{a.cluster}>", "algorithmic_bytes_per_launch": alg,
+                         "kernel": f"pfb::k_step2d<{a.cluster}>", "algorithmic_bytes_per_launch": alg,
                          "peak_source": peak_src,
                          "duration_source": "CUDA events over the timed region / steps"},
             "cpu_baseline": cpu,

@@ -185,24 +185,21 @@ size_t pfb_sizeof(int which);
  * current device. Idempotent; called implicitly by pfb_step2d_launch. */
 int pfb_step2d_configure(void);
 
-/* Number of CTAs the one-cluster-per-cell launch uses for N cells with
- * `cluster` CTAs per cell (cluster = 0 selects the default 8). Replaces
- * k_step_grid(). */
+/* Number of CTAs the step launch uses for N cells with `cluster` CTAs per
+ * cell (cluster = 0 selects the default 4). Replaces k_step_grid(). */
 int pfb_step2d_grid(int num_cells, int cluster);
 
 /* One full step for every cell: tumble, interaction integral, Euler update,
  * recentring store, Q5.27 scatter into S_sc, FP64 moments, and clearing of
- * S_cl (clear_ahead_words words). `cluster` is the number of CTAs that
- * cooperate on one cell (2, 4 or 8; 0 = default 8). Clusters of 8 run the
- * persistent pipelined kernel; 2 and 4 launch one cluster per cell.
+ * S_cl (clear_ahead_words words). `cluster` is the number of CTAs of the
+ * thread-block cluster that cooperates on one cell (2, 4 or 8; 0 = default
+ * 4).
  * Returns PFB_E_ARG for a null buffer, a phi pool or S slot not 16-byte
  * aligned, L not larger than 286, or a non-null `moments`. */
 int pfb_step2d_launch(const pfb_step_args2d* args, int cluster, void* stream);
 
-/* As pfb_step2d_launch with an explicit kernel variant: 0 = default for the
- * cluster size, 1 = one cluster per cell, 2 = persistent pipelined clusters,
- * 3 = the pipelined kernel with one cluster per cell (2 and 3 need cluster
- * 8). All variants compute the same update. */
+/* As pfb_step2d_launch with an explicit kernel variant (0 = default, 1 = one
+ * thread-block cluster per cell, the only variant of this version). */
 int pfb_step2d_launch_ex(const pfb_step_args2d* args, int cluster, int variant,
                          void* stream);
 

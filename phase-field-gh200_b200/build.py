@@ -34,7 +34,7 @@ COMMON = [
     "-Xcompiler", "-fPIC,-ffp-contract=off,-Wall",
     "-I", str(INCLUDE),
 ]
-SOURCES = ["step2d.cu", "step2d_persist.cu", "init2d.cu", "sim2d.cu", "host2d.cpp"]
+SOURCES = ["step2d.cu", "init2d.cu", "sim2d.cu", "host2d.cpp"]
 HEADERS = ["pfb_common.cuh", "device_util.cuh", "pfb_internal.h", "step2d_common.cuh"]
 
 

@@ -27,6 +27,33 @@ __device__ __forceinline__ void cluster_sync() {
             : "memory");
 }
 
+// Split cluster barrier without memory ordering: enough to publish mbarrier
+// initialisation (after fence.mbarrier_init) before peers signal them.
+__device__ __forceinline__ void cluster_arrive_relaxed() {
+    asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait() {
+    asm volatile("barrier.cluster.wait.aligned;" ::: "memory");
+}
+
+// Asynchronous stores into a peer CTA's shared memory that complete on the
+// peer's mbarrier (addresses from map_to_rank).
+__device__ __forceinline__ void st_async_v2f64(uint32_t addr, double a, double b, uint32_t bar) {
+    asm volatile(
+        "st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f64 [%0], {%1, %2}, [%3];" ::"r"(
+            addr),
+        "d"(a), "d"(b), "r"(bar)
+        : "memory");
+}
+__device__ __forceinline__ void st_async_v4b32(uint32_t addr, int a, int b, int c, int d,
+                                               uint32_t bar) {
+    asm volatile(
+        "st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.b32 [%0], {%1, %2, %3, %4}, "
+        "[%5];" ::"r"(addr),
+        "r"(a), "r"(b), "r"(c), "r"(d), "r"(bar)
+        : "memory");
+}
+
 // Address of the same shared-memory variable in CTA `rank` of the cluster.
 __device__ __forceinline__ uint32_t map_to_rank(uint32_t saddr, uint32_t rank) {
     uint32_t r;

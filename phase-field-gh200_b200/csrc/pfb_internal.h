@@ -16,16 +16,9 @@ int step2d_configure_device();
 int step2d_launch(const pfb_step_args2d* a, int cluster, cudaStream_t stream);
 int step2d_smem_bytes(int cluster);
 int step2d_read_status(unsigned* out, int clear);
-// variant: 0 = default for the cluster size, 1 = one cluster per cell,
-// 2 = persistent pipelined clusters (8 CTAs), 3 = the pipelined kernel with
-// one cluster per cell
+// variant: 0 = default, 1 = one thread-block cluster per cell
 int step2d_launch_variant(const pfb_step_args2d* a, int cluster, int variant,
                           cudaStream_t stream);
-
-// step2d_persist.cu
-int persist2d_launch(const pfb_step_args2d& A, cudaStream_t stream, bool one_cell_per_cluster);
-int persist2d_smem_bytes();
-int persist2d_read_status(unsigned* out, int clear);
 
 // init2d.cu
 int init_tiles2d(float* phi_a, float* phi_b, pfb_cell2d* cell, const uint8_t* cls, int N, int L,

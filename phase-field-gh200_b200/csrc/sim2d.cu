@@ -40,7 +40,7 @@ struct pfb_sim2d {
     pfb_traj_cell2d* d_traj = nullptr;
     cudaStream_t stream = nullptr;
     long long steps_done = 0;
-    int cluster = 8;
+    int cluster = 4;
     int variant = 0;
     bool use_graph = true;
     bool graph_ready = false;
@@ -258,7 +258,7 @@ extern "C" {
 int pfb_step2d_configure(void) { return step2d_configure_device(); }
 
 int pfb_step2d_grid(int num_cells, int cluster) {
-    if (cluster == 0) cluster = 8;
+    if (cluster == 0) cluster = 4;
     if (num_cells < 0 || (cluster != 2 && cluster != 4 && cluster != 8)) return PFB_E_ARG;
     return num_cells * cluster;
 }
@@ -360,7 +360,7 @@ int pfb_sim2d_set_cluster(pfb_sim2d* s, int cluster) {
 
 int pfb_sim2d_set_variant(pfb_sim2d* s, int variant) {
     if (!s) return set_error(PFB_E_ARG, "null sim");
-    if (variant < 0 || variant > 3) return set_error(PFB_E_CONFIG, "unknown kernel variant");
+    if (variant < 0 || variant > 1) return set_error(PFB_E_CONFIG, "unknown kernel variant");
     if (variant != s->variant) s->drop_graph();
     s->variant = variant;
     return PFB_OK;

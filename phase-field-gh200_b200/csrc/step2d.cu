@@ -37,20 +37,21 @@ namespace pfb {
 
 constexpr int kThreads = 288;
 constexpr int kWarps = kThreads / 32;
-constexpr int kHeaderBytes = 1024;
+constexpr int kHeaderBytes = 2048;
 
 // Status word of this kernel family in device memory: bit 0 = a CTA gave up
 // waiting for its staged band. Read with pfb_device_status().
 __device__ unsigned int g_step2d_status = 0u;
 
+template <int K>
 struct __align__(16) StepShared {
     uint64_t bar;
     int abort;
     int gx0, gy0;
     CellPlan plan;
-    RedScratch<kWarps> red;
+    RedScratch<kWarps, K> red;
 };
-static_assert(sizeof(StepShared) <= kHeaderBytes, "shared header too large");
+static_assert(sizeof(StepShared<8>) <= kHeaderBytes, "shared header too large");
 
 __host__ __device__ constexpr int band_rows(int wy, int k) { return (wy + k - 1) / k; }
 
@@ -104,7 +105,7 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
     static_assert(WY % K == 0, "staged classes split into equal bands");
     static_assert((WX * 4) % 16 == 0 && (TX0 * 4) % 16 == 0, "bulk copies need 16-B rows");
 
-    StepShared& sh = *reinterpret_cast<StepShared*>(smem);
+    StepShared<K>& sh = *reinterpret_cast<StepShared<K>*>(smem);
     const CellPlan& P = sh.plan;
     float* phi_s = reinterpret_cast<float*>(smem + kHeaderBytes);
     uint32_t* ps_s = reinterpret_cast<uint32_t*>(smem + kHeaderBytes + PHI_ROWS * PX * 4);
@@ -226,7 +227,7 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
             }
         }
     }
-    reduce_force<K, kWarps>(A, P, rank, sh.red, 0, aIx, aIy);
+    reduce_force<K, kWarps>(A, P, rank, sh.red, aIx, aIy, &g_step2d_status);
 
     const float gam = P.gam, dwC = P.dwC, volC = P.volC;
     const float vx = sh.red.vx, vy = sh.red.vy, mrel = P.mrel;
@@ -422,17 +423,17 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
             }
         }
     }
-    reduce_moments<K, kWarps>(A, P, rank, sh.red, 0, fm, acc);
     if (abort) (void)dev::mbar_wait_bounded(&sh.bar, 0, kWaitPolls);
+    reduce_moments<K, kWarps>(A, P, rank, sh.red, fm, acc, &g_step2d_status);
 }
 
 template <int CLS, int K>
 __device__ __forceinline__ void global_cell_v1(const pfb_step_args2d& A, int n, int rank,
                                                char* smem, unsigned long long step, bool fm) {
-    StepShared& sh = *reinterpret_cast<StepShared*>(smem);
+    StepShared<K>& sh = *reinterpret_cast<StepShared<K>*>(smem);
     if (threadIdx.x == 0) plan_cell(A, n, CLS, step, sh.plan, rank == 0);
     __syncthreads();
-    global_cell<CLS, K, kWarps>(A, sh.plan, rank, sh.red, 0, fm);
+    global_cell<CLS, K, kWarps>(A, sh.plan, rank, sh.red, fm, &g_step2d_status);
 }
 
 template <int K>
@@ -459,6 +460,9 @@ __global__ void __launch_bounds__(kThreads, 3)
     const bool fm = full_moment_step(A, step);
 
     const int rank = (int)dev::cluster_rank();
+    StepShared<K>& sh = *reinterpret_cast<StepShared<K>*>(smem);
+    if (tid == 0) red_init<kWarps, K>(sh.red, rank);
+    dev::cluster_arrive_relaxed();  // matched by the wait in reduce_force
     const int slot = (int)(blockIdx.x / K);
     const int n = A.perm ? (int)A.perm[slot] : slot;
     const int cls = (int)A.cell_cls[n];
@@ -471,10 +475,9 @@ __global__ void __launch_bounds__(kThreads, 3)
         case 5: global_cell_v1<5, K>(A, n, rank, smem, step, fm); break;
         default:
             if (rank == 0 && tid == 0) atomicAdd(A.flags + PFB_FLAG_CLASS_UNSUPPORTED, 1u);
-            return;  // uniform over the cluster: no barrier is pending
+            dev::cluster_wait();  // uniform over the cluster
+            break;
     }
-    // Keep every CTA's shared memory alive until rank 0 has read the partials.
-    dev::cluster_sync();
 }
 
 // ---------------------------------------------------------------------------
@@ -536,15 +539,12 @@ int step2d_launch_variant(const pfb_step_args2d* a, int cluster, int variant,
     if (A.L <= 286 || A.P < A.L || (A.P & 3))
         return set_error(PFB_E_ARG, "domain side must exceed 286, P >= L and P % 4 == 0");
     if (A.parity_out != 0 && A.parity_out != 1) return set_error(PFB_E_ARG, "parity_out must be 0 or 1");
-    if (cluster == 0) cluster = 8;
+    if (cluster == 0) cluster = 4;
     if (cluster != 2 && cluster != 4 && cluster != 8)
         return set_error(PFB_E_CONFIG, "cluster must be 2, 4 or 8");
-    if (variant == 0) variant = cluster == 8 ? 2 : 1;
-    if ((variant == 2 || variant == 3) && cluster != 8)
-        return set_error(PFB_E_CONFIG, "the pipelined kernel uses clusters of 8");
-    if (variant < 1 || variant > 3) return set_error(PFB_E_CONFIG, "unknown kernel variant");
+    if (variant == 0) variant = 1;
+    if (variant != 1) return set_error(PFB_E_CONFIG, "unknown kernel variant");
     if (A.N == 0) return PFB_OK;
-    if (variant >= 2) return persist2d_launch(A, stream, variant == 3);
     int rc = step2d_configure_device();
     if (rc) return rc;
     cudaError_t e = cluster == 2   ? launch_k<2>(A, stream)
@@ -559,9 +559,7 @@ int step2d_launch(const pfb_step_args2d* a, int cluster, cudaStream_t stream) {
 }
 
 int step2d_read_status(unsigned* out, int clear) {
-    unsigned pv = 0;
-    int rc = persist2d_read_status(&pv, clear);
-    if (rc) return rc;
+    const unsigned pv = 0;
     unsigned v = 0;
     cudaError_t e = cudaMemcpyFromSymbol(&v, g_step2d_status, sizeof(v));
     if (e != cudaSuccess) return set_error(PFB_E_CUDA, "status read: %s", cudaGetErrorString(e));

@@ -214,27 +214,42 @@ __device__ __forceinline__ void commit_cell(const pfb_step_args2d& A, const Cell
     }
 }
 
-// Reduction scratch in shared memory; the partials that peers read through
-// distributed shared memory are double-buffered by cell parity so that a
-// persistent cluster can move to its next cell after one barrier.
-template <int NW>
+// Reduction scratch in shared memory. Cluster reductions push each CTA's
+// partial into its peers' receive slots with st.async, completing on the
+// peer's mbarrier: no cluster barrier (and no release fence over the CTA's
+// outstanding global stores) sits on the path. Receive slots are indexed by
+// the sender's rank and summed in ascending rank order.
+template <int NW, int K>
 struct RedScratch {
+    uint64_t barI;  // K force partials (16 B each) received, every CTA
+    uint64_t barM;  // K moment partials (64 B each) received, rank 0
     double red_d[NW][4];
     int red_i[NW][5];
-    alignas(16) double part_I[2][2];
-    alignas(16) double part_M[2][4];
-    alignas(16) int part_B[2][8];
+    alignas(16) double recvI[K][2];
+    alignas(16) double recvM[K][4];
+    alignas(16) int recvB[K][4];
+    alignas(16) int recvP[K][4];
     float vx, vy;
 };
 
+// Receive barriers of one cluster reduction round; thread 0 of every CTA
+// calls it before the kernel's first (relaxed) cluster arrive.
+template <int NW, int K>
+__device__ __forceinline__ void red_init(RedScratch<NW, K>& R, int rank) {
+    dev::mbar_init(&R.barI, 1);
+    dev::mbar_init(&R.barM, 1);
+    dev::mbar_arrive_expect_tx(&R.barI, (uint32_t)(K * 16));
+    if (rank == 0) dev::mbar_arrive_expect_tx(&R.barM, (uint32_t)(K * 64));
+}
+
 // Interaction integral of this CTA -> cluster total -> velocity, identical
-// in every CTA. Sums run in ascending warp, then ascending rank order: lanes
-// of warp 0 fetch the partials in parallel and add them in lane order. Rank 0
-// stores v and I in the cell record.
+// in every CTA. Sums run in ascending warp, then ascending rank order. Rank 0
+// stores v and I in the cell record. All threads call it; the caller has
+// issued the cluster arrive that follows red_init.
 template <int K, int NW>
 __device__ __forceinline__ void reduce_force(const pfb_step_args2d& A, const CellPlan& P,
-                                             int rank, RedScratch<NW>& R, int par, double aIx,
-                                             double aIy) {
+                                             int rank, RedScratch<NW, K>& R, double aIx,
+                                             double aIy, unsigned int* status) {
     static_assert(NW <= 32 && K <= 32, "one lane per warp and per rank");
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     aIx = dev::warp_sum_down(aIx);
@@ -244,22 +259,18 @@ __device__ __forceinline__ void reduce_force(const pfb_step_args2d& A, const Cel
         R.red_d[warp][1] = aIy;
     }
     __syncthreads();
+    dev::cluster_wait();  // every peer's receive barrier is initialised
     if (warp == 0) {
         const double px = lane < NW ? R.red_d[lane][0] : 0.0;
         const double py = lane < NW ? R.red_d[lane][1] : 0.0;
         const double s0 = dev::ordered_lane_sum(px, NW);
         const double s1 = dev::ordered_lane_sum(py, NW);
-        if (lane == 0) {
-            R.part_I[par][0] = s0;
-            R.part_I[par][1] = s1;
-        }
-    }
-    dev::cluster_sync();
-    if (warp == 0) {
-        double2 v = make_double2(0.0, 0.0);
         if (lane < K)
-            v = dev::ld_cluster_v2f64(
-                dev::map_to_rank(dev::smem_addr(&R.part_I[par][0]), (uint32_t)lane));
+            dev::st_async_v2f64(dev::map_to_rank(dev::smem_addr(&R.recvI[rank][0]), lane), s0, s1,
+                                dev::map_to_rank(dev::smem_addr(&R.barI), lane));
+        if (!dev::mbar_wait_bounded(&R.barI, 0, kWaitPolls)) atomicOr(status, 2u);
+        const double2 v = lane < K ? make_double2(R.recvI[lane][0], R.recvI[lane][1])
+                                   : make_double2(0.0, 0.0);
         const double sIx = dev::ordered_lane_sum(v.x, K);
         const double sIy = dev::ordered_lane_sum(v.y, K);
         if (lane == 0) {
@@ -279,14 +290,12 @@ __device__ __forceinline__ void reduce_force(const pfb_step_args2d& A, const Cel
     __syncthreads();
 }
 
-// Moments of this CTA -> cluster total -> commit by rank 0 (reference
-// src/kernels.cu:542-590). Leaves the caller after the cluster barrier that
-// publishes the partials; the caller's next cluster barrier (or the kernel's
-// final one) keeps them alive until rank 0 has read them.
+// Moments of this CTA -> pushed to rank 0 -> summed in rank order and
+// committed by rank 0 (reference src/kernels.cu:542-590).
 template <int K, int NW>
 __device__ __forceinline__ void reduce_moments(const pfb_step_args2d& A, const CellPlan& P,
-                                               int rank, RedScratch<NW>& R, int par, bool fm,
-                                               PixelAcc acc) {
+                                               int rank, RedScratch<NW, K>& R, bool fm,
+                                               PixelAcc acc, unsigned int* status) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     acc.V = dev::warp_sum_down(acc.V);
     acc.Cx = dev::warp_sum_down(acc.Cx);
@@ -309,55 +318,34 @@ __device__ __forceinline__ void reduce_moments(const pfb_step_args2d& A, const C
         R.red_i[warp][4] = acc.pmaxb;
     }
     __syncthreads();
-    if (warp == 0) {
-        double m[4];
-        for (int k = 0; k < 4; ++k)
-            m[k] = dev::ordered_lane_sum(lane < NW ? R.red_d[lane][k] : 0.0, NW);
-        int b0 = lane < NW ? R.red_i[lane][0] : P.dwx;
-        int b1 = lane < NW ? R.red_i[lane][1] : -1;
-        int b2 = lane < NW ? R.red_i[lane][2] : P.dwy;
-        int b3 = lane < NW ? R.red_i[lane][3] : -1;
-        int b4 = lane < NW ? R.red_i[lane][4] : 0;
-        b0 = __reduce_min_sync(0xFFFFFFFFu, b0);
-        b1 = __reduce_max_sync(0xFFFFFFFFu, b1);
-        b2 = __reduce_min_sync(0xFFFFFFFFu, b2);
-        b3 = __reduce_max_sync(0xFFFFFFFFu, b3);
-        b4 = __reduce_max_sync(0xFFFFFFFFu, b4);
-        if (lane == 0) {
-            for (int k = 0; k < 4; ++k) R.part_M[par][k] = m[k];
-            R.part_B[par][0] = b0;
-            R.part_B[par][1] = b1;
-            R.part_B[par][2] = b2;
-            R.part_B[par][3] = b3;
-            R.part_B[par][4] = b4;
-        }
+    if (warp != 0) return;
+    double m[4];
+    for (int k = 0; k < 4; ++k) m[k] = dev::ordered_lane_sum(lane < NW ? R.red_d[lane][k] : 0.0, NW);
+    const int b0 = __reduce_min_sync(0xFFFFFFFFu, lane < NW ? R.red_i[lane][0] : P.dwx);
+    const int b1 = __reduce_max_sync(0xFFFFFFFFu, lane < NW ? R.red_i[lane][1] : -1);
+    const int b2 = __reduce_min_sync(0xFFFFFFFFu, lane < NW ? R.red_i[lane][2] : P.dwy);
+    const int b3 = __reduce_max_sync(0xFFFFFFFFu, lane < NW ? R.red_i[lane][3] : -1);
+    const int b4 = __reduce_max_sync(0xFFFFFFFFu, lane < NW ? R.red_i[lane][4] : 0);
+    if (lane == 0) {
+        const uint32_t bar = dev::map_to_rank(dev::smem_addr(&R.barM), 0);
+        dev::st_async_v2f64(dev::map_to_rank(dev::smem_addr(&R.recvM[rank][0]), 0), m[0], m[1], bar);
+        dev::st_async_v2f64(dev::map_to_rank(dev::smem_addr(&R.recvM[rank][2]), 0), m[2], m[3], bar);
+        dev::st_async_v4b32(dev::map_to_rank(dev::smem_addr(&R.recvB[rank][0]), 0), b0, b1, b2, b3,
+                            bar);
+        dev::st_async_v4b32(dev::map_to_rank(dev::smem_addr(&R.recvP[rank][0]), 0), b4, 0, 0, 0,
+                            bar);
     }
-    dev::cluster_sync();
-    if (rank == 0 && warp == 0) {
-        double2 m01 = make_double2(0.0, 0.0), m23 = make_double2(0.0, 0.0);
-        int4 bq = make_int4(P.dwx, -1, P.dwy, -1);
-        int b4 = 0;
-        if (lane < K) {
-            const uint32_t am = dev::map_to_rank(dev::smem_addr(&R.part_M[par][0]), (uint32_t)lane);
-            const uint32_t ab = dev::map_to_rank(dev::smem_addr(&R.part_B[par][0]), (uint32_t)lane);
-            m01 = dev::ld_cluster_v2f64(am);
-            m23 = dev::ld_cluster_v2f64(am + 16);
-            bq = dev::ld_cluster_v4s32(ab);
-            b4 = dev::ld_cluster_s32(ab + 16);
-        }
-        double m[4];
-        m[0] = dev::ordered_lane_sum(m01.x, K);
-        m[1] = dev::ordered_lane_sum(m01.y, K);
-        m[2] = dev::ordered_lane_sum(m23.x, K);
-        m[3] = dev::ordered_lane_sum(m23.y, K);
-        int b[5];
-        b[0] = __reduce_min_sync(0xFFFFFFFFu, bq.x);
-        b[1] = __reduce_max_sync(0xFFFFFFFFu, bq.y);
-        b[2] = __reduce_min_sync(0xFFFFFFFFu, bq.z);
-        b[3] = __reduce_max_sync(0xFFFFFFFFu, bq.w);
-        b[4] = __reduce_max_sync(0xFFFFFFFFu, b4);
-        if (lane == 0) commit_cell(A, P, fm, m, b);
-    }
+    if (rank != 0) return;
+    if (!dev::mbar_wait_bounded(&R.barM, 0, kWaitPolls)) atomicOr(status, 2u);
+    double t[4];
+    for (int k = 0; k < 4; ++k) t[k] = dev::ordered_lane_sum(lane < K ? R.recvM[lane][k] : 0.0, K);
+    int b[5];
+    b[0] = __reduce_min_sync(0xFFFFFFFFu, lane < K ? R.recvB[lane][0] : P.dwx);
+    b[1] = __reduce_max_sync(0xFFFFFFFFu, lane < K ? R.recvB[lane][1] : -1);
+    b[2] = __reduce_min_sync(0xFFFFFFFFu, lane < K ? R.recvB[lane][2] : P.dwy);
+    b[3] = __reduce_max_sync(0xFFFFFFFFu, lane < K ? R.recvB[lane][3] : -1);
+    b[4] = __reduce_max_sync(0xFFFFFFFFu, lane < K ? R.recvP[lane][0] : 0);
+    if (lane == 0) commit_cell(A, P, fm, t, b);
 }
 
 // Global-memory path for classes 4 (224^2) and 5 (286^2 fallback): phi^n is
@@ -368,7 +356,7 @@ __device__ __forceinline__ void reduce_moments(const pfb_step_args2d& A, const C
 // of the cluster call it together.
 template <int CLS, int K, int NW>
 __device__ __noinline__ void global_cell(const pfb_step_args2d& A, const CellPlan& P, int rank,
-                                         RedScratch<NW>& R, int par, bool fm) {
+                                         RedScratch<NW, K>& R, bool fm, unsigned int* status) {
     constexpr int NT = NW * 32;
     constexpr Window W = window_of(CLS);
     constexpr int WX = W.wx, WY = W.wy, TX0 = W.tx0, TY0 = W.ty0;
@@ -399,7 +387,7 @@ __device__ __noinline__ void global_cell(const pfb_step_args2d& A, const CellPla
         aIx += (double)(c * gx * So);
         aIy += (double)(c * gyv * So);
     }
-    reduce_force<K, NW>(A, P, rank, R, par, aIx, aIy);
+    reduce_force<K, NW>(A, P, rank, R, aIx, aIy, status);
 
     const int sx = P.sx, sy = P.sy;
     const int dwx = P.dwx, dwy = P.dwy, dtx0 = P.dtx0, dty0 = P.dty0;
@@ -473,7 +461,7 @@ __device__ __noinline__ void global_cell(const pfb_step_args2d& A, const CellPla
             }
         }
     }
-    reduce_moments<K, NW>(A, P, rank, R, par, fm, acc);
+    reduce_moments<K, NW>(A, P, rank, R, fm, acc, status);
 }
 
 }  // namespace pfb
