@@ -35,7 +35,7 @@
 
 namespace pfb {
 
-constexpr int kThreads = 288;
+constexpr int kThreads = 224;
 constexpr int kWarps = kThreads / 32;
 constexpr int kHeaderBytes = 2048;
 
@@ -70,6 +70,41 @@ __host__ __device__ constexpr int pick_run(int wx, int rows) {
         }
     }
     return best_h;
+}
+
+// Thread map of the register passes: a thread owns a strip four pixels wide
+// and H rows tall of the band; NQ strips per row, G row groups.
+template <int CLS, int K> struct QuadMap {
+    static constexpr int WX = window_of(CLS).wx;
+    static constexpr int RB = (window_of(CLS).wy + K - 1) / K;
+    static constexpr int NQ = WX / 4;
+    static constexpr int GMAX = kThreads / NQ;
+    static constexpr int H = (RB + GMAX - 1) / GMAX;
+    static constexpr int G = (RB + H - 1) / H;
+    static_assert(WX % 4 == 0 && NQ * G <= kThreads, "strip map");
+};
+
+// Euler update of four consecutive pixels of one row from the rolling
+// three-row window (s = row above, c = this row, n = row below; w/e are the
+// pixels left and right of the four).
+__device__ __forceinline__ void stencil4(float ws, float4 vs, float es, float wc, float4 vc,
+                                         float ec, float wn, float4 vn, float en,
+                                         const float (&so)[4], float gam, float dwC, float volC,
+                                         float repC, float vx, float vy, float mrel, float dtf,
+                                         float (&pn)[4]) {
+    const float S[6] = {ws, vs.x, vs.y, vs.z, vs.w, es};
+    const float C[6] = {wc, vc.x, vc.y, vc.z, vc.w, ec};
+    const float N[6] = {wn, vn.x, vn.y, vn.z, vn.w, en};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const float lap =
+            lap9(N[j], N[j + 1], N[j + 2], C[j], C[j + 1], C[j + 2], S[j], S[j + 1], S[j + 2]);
+        const float gx = 0.5f * (C[j + 2] - C[j]);
+        const float gy = 0.5f * (N[j + 1] - S[j + 1]);
+        const float rhs =
+            rhs_pixel(lap, C[j + 1], so[j], gx, gy, gam, dwC, volC, repC, vx, vy, mrel);
+        pn[j] = C[j + 1] + dtf * rhs;
+    }
 }
 
 // Both staged arrays use the row pitch WX + 8 words.
@@ -195,36 +230,65 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
     __syncthreads();
     const bool abort = sh.abort != 0;
 
-    // ---- pass 1: S_other (kept in place of q_S) and the interaction integral
+    // ---- pass 1: S_other of the thread's strip (kept in registers) and the
+    // interaction integral
+    using QM = QuadMap<CLS, K>;
+    constexpr int H = QM::H;
+    const bool active = !abort && tid < QM::NQ * QM::G;
+    const int x0 = 4 * (tid % QM::NQ);
+    const int r0 = (tid / QM::NQ) * H;
+    const int nr = active ? min(H, RB - r0) : 0;
+    auto load_row = [&](int t, float& w, float4& c, float& e) {
+        const float* row = phi_s + (t + 2) * PX + 4 + x0;
+        c = *reinterpret_cast<const float4*>(row);
+        w = row[-1];
+        e = row[4];
+    };
+    float so[H][4];
     double aIx = 0.0, aIy = 0.0;
-    if (!abort) {
-        constexpr int H = pick_run(WX, RB);
-        constexpr int RUNS = (RB + H - 1) / H;
-        for (int item = tid; item < WX * RUNS; item += kThreads) {
-            const int c = item / WX;
-            const int x = item - c * WX;
-            const int ya = y0 + c * H;
-            const int yb = min(y1, ya + H);
-            const float* p = phi_s + (ya - y0 + 2) * PX + 4 + x;
-            uint32_t* q = ps_s + (ya - y0 + 1) * PX + soff + x;
-            float sC = p[-PX];
-            float cW = p[-1], cC = p[0], cE = p[1];
-            for (int y = ya; y < yb; ++y) {
-                const float nC = p[PX];
-                // counted twice: the reference evaluates S_other in both passes
-                const float So = s_other_n(*q, cC, A.flags, 2u);
-                *q = __float_as_uint(So);
-                const float gx = 0.5f * (cE - cW);
-                const float gy = 0.5f * (nC - sC);
-                aIx += (double)(cC * gx * So);
-                aIy += (double)(cC * gy * So);
-                p += PX;
-                q += PX;
-                sC = cC;
-                cC = nC;
-                cW = p[-1];
-                cE = p[1];
+    if (active) {
+        float ws, es, wc, ec;
+        float4 vs, vc;
+        load_row(r0 - 1, ws, vs, es);
+        load_row(r0, wc, vc, ec);
+#pragma unroll
+        for (int r = 0; r < H; ++r) {
+            if (r < nr) {
+                float wn, en;
+                float4 vn;
+                load_row(r0 + r + 1, wn, vn, en);
+                const uint32_t* qrow = ps_s + (r0 + r + 1) * PX + soff + x0;
+                const float C[6] = {wc, vc.x, vc.y, vc.z, vc.w, ec};
+                const float Sv[4] = {vs.x, vs.y, vs.z, vs.w};
+                const float Nv[4] = {vn.x, vn.y, vn.z, vn.w};
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const float cC = C[j + 1];
+                    // counted twice: the reference evaluates S_other in both passes
+                    const float So = s_other_n(qrow[j], cC, A.flags, 2u);
+                    so[r][j] = So;
+                    const float gx = 0.5f * (C[j + 2] - C[j]);
+                    const float gy = 0.5f * (Nv[j] - Sv[j]);
+                    aIx += (double)(cC * gx * So);
+                    aIy += (double)(cC * gy * So);
+                }
+                ws = wc;
+                vs = vc;
+                es = ec;
+                wc = wn;
+                vc = vn;
+                ec = en;
             }
+        }
+        if (fm) {
+            // the full-moment pass reads S_other of own rows from shared memory
+#pragma unroll
+            for (int r = 0; r < H; ++r)
+                if (r < nr) {
+                    uint32_t* qrow = ps_s + (r0 + r + 1) * PX + soff + x0;
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) qrow[j] = __float_as_uint(so[r][j]);
+                }
         }
     }
     reduce_force<K, kWarps>(A, P, rank, sh.red, aIx, aIy, &g_step2d_status);
@@ -261,101 +325,136 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
     if (!fm) {
         // ---- pass 2, fused: Euler update, store, scatter and moments
         const bool ident = sx == 0 && sy == 0 && P.dcls == CLS;
-        if (!abort) {
-            constexpr int H = pick_run(WX, RB);
-            constexpr int RUNS = (RB + H - 1) / H;
-            float pmaxf = 0.0f;
-            for (int item = tid; item < WX * RUNS; item += kThreads) {
-                const int c = item / WX;
-                const int x = item - c * WX;
-                const int ya = y0 + c * H;
-                const int yb = min(y1, ya + H);
-                const float* p = phi_s + (ya - y0 + 2) * PX + 4 + x;
-                const uint32_t* q = ps_s + (ya - y0 + 1) * PX + soff + x;
-                float sW = p[-PX - 1], sC = p[-PX], sE = p[-PX + 1];
-                float cW = p[-1], cC = p[0], cE = p[1];
-                int gxs = gx0 + x;
-                if (gxs >= L) gxs -= L;
-                const double xd = (double)x;
-                int yfirst = -1, ylast = -1;
-                int gy = gy0 + ya;
+        if (active) {
+            float ws, es, wc, ec;
+            float4 vs, vc;
+            load_row(r0 - 1, ws, vs, es);
+            load_row(r0, wc, vc, ec);
+            if (ident) {
+                float pmaxf = 0.0f;
+                unsigned colmask = 0u;
+                int gy = gy0 + y0 + r0;
                 if (gy >= L) gy -= L;
-                float* o = tile_out + (size_t)(TY0 + ya) * kTilePitch + TX0 + x;
-                for (int y = ya; y < yb; ++y) {
-                    const float nW = p[PX - 1], nC = p[PX], nE = p[PX + 1];
-                    const float lap = lap9(nW, nC, nE, cW, cC, cE, sW, sC, sE);
-                    const float gx = 0.5f * (cE - cW);
-                    const float gyv = 0.5f * (nC - sC);
-                    const float rhs = rhs_pixel(lap, cC, __uint_as_float(*q), gx, gyv, gam, dwC,
-                                                volC, repC, vx, vy, mrel);
-                    const float pn = cC + dtf * rhs;
-                    if (ident) {
-                        __stcs(o, pn);
-                        if (fabsf(pn) <= 2.0f) {
-                            pmaxf = fmaxf(pmaxf, fabsf(pn));
-                        } else {
-                            if (!isfinite(pn)) atomicOr(A.flags + PFB_FLAG_NONFINITE, 1u);
-                            if (pn * pn > kPhiSqCap) atomicOr(A.flags + PFB_FLAG_Q_CLAMP, 1u);
-                            acc.pmaxb = max(acc.pmaxb, (int)__float_as_uint(fabsf(pn)));
+                int gx = gx0 + x0;
+                if (gx >= L) gx -= L;
+                // the strip's four columns wrap at most once
+                int gxj[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) gxj[j] = gx + j < L ? gx + j : gx + j - L;
+                double xd[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) xd[j] = (double)(x0 + j);
+                float* o = tile_out + (size_t)(TY0 + y0 + r0) * kTilePitch + TX0 + x0;
+#pragma unroll
+                for (int r = 0; r < H; ++r) {
+                    if (r < nr) {
+                        float wn, en;
+                        float4 vn;
+                        load_row(r0 + r + 1, wn, vn, en);
+                        float pn[4];
+                        stencil4(ws, vs, es, wc, vc, ec, wn, vn, en, so[r], gam, dwC, volC, repC,
+                                 vx, vy, mrel, dtf, pn);
+                        __stcs(reinterpret_cast<float4*>(o + r * kTilePitch),
+                               make_float4(pn[0], pn[1], pn[2], pn[3]));
+                        uint32_t* srow = A.S_sc + (size_t)gy * Pp;
+                        double rowV = 0.0;
+                        unsigned m = 0u;
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            const float p = pn[j];
+                            if (fabsf(p) <= 2.0f) {
+                                pmaxf = fmaxf(pmaxf, fabsf(p));
+                            } else {
+                                if (!isfinite(p)) atomicOr(A.flags + PFB_FLAG_NONFINITE, 1u);
+                                if (p * p > kPhiSqCap) atomicOr(A.flags + PFB_FLAG_Q_CLAMP, 1u);
+                                acc.pmaxb = max(acc.pmaxb, (int)__float_as_uint(fabsf(p)));
+                            }
+                            const uint32_t qv = q_encode(p);
+                            if (qv) {
+                                const uint32_t old = atomicAdd(srow + gxj[j], qv);
+                                if (old > 0xFFFFFFFFu - qv)
+                                    atomicOr(A.flags + PFB_FLAG_S_OVERFLOW, 1u);
+                            }
+                            const double d = (double)p * (double)p;
+                            rowV += d;
+                            acc.Cx += d * xd[j];
+                            if (p > kSupportEps) m |= 1u << j;
                         }
-                        const uint32_t qv = q_encode(pn);
-                        if (qv) {
-                            const uint32_t old = atomicAdd(A.S_sc + (size_t)gy * Pp + gxs, qv);
-                            if (old > 0xFFFFFFFFu - qv) atomicOr(A.flags + PFB_FLAG_S_OVERFLOW, 1u);
+                        const int y = y0 + r0 + r;
+                        acc.V += rowV;
+                        acc.Cy += rowV * (double)y;
+                        if (m) {
+                            acc.bloy = min(acc.bloy, y);
+                            acc.bhiy = max(acc.bhiy, y);
+                            colmask |= m;
                         }
-                        const double d = (double)pn * (double)pn;
-                        acc.V += d;
-                        acc.Cx += d * xd;
-                        acc.Cy += d * (double)y;
-                        if (pn > kSupportEps) {
-                            if (yfirst < 0) yfirst = y;
-                            ylast = y;
-                        }
-                    } else {
-                        const int a = x - sx, b = y - sy;
-                        if ((unsigned)a < (unsigned)dwx && (unsigned)b < (unsigned)dwy) {
+                        if (++gy >= L) gy -= L;
+                        ws = wc;
+                        vs = vc;
+                        es = ec;
+                        wc = wn;
+                        vc = vn;
+                        ec = en;
+                    }
+                }
+                acc.pmaxb = max(acc.pmaxb, (int)__float_as_uint(pmaxf));
+                if (colmask) {
+                    acc.blox = min(acc.blox, x0 + __ffs(colmask) - 1);
+                    acc.bhix = max(acc.bhix, x0 + 31 - __clz(colmask));
+                }
+            } else {
+                // shifted or re-classed destination: per-pixel map
+#pragma unroll
+                for (int r = 0; r < H; ++r) {
+                    if (r < nr) {
+                        float wn, en;
+                        float4 vn;
+                        load_row(r0 + r + 1, wn, vn, en);
+                        float pn[4];
+                        stencil4(ws, vs, es, wc, vc, ec, wn, vn, en, so[r], gam, dwC, volC, repC,
+                                 vx, vy, mrel, dtf, pn);
+                        const int b = y0 + r0 + r - sy;
+                        if ((unsigned)b < (unsigned)dwy) {
                             int gyn = gy0n + b;
                             if (gyn >= L) gyn -= L;
-                            __stcs(tile_out + (size_t)(dty0 + b) * kTilePitch + dtx0 + a, pn);
-                            dest_pixel(A, acc, pn, a, b, A.S_sc + (size_t)gyn * Pp, gx0n, L);
+                            uint32_t* srow = A.S_sc + (size_t)gyn * Pp;
+                            float* orow = tile_out + (size_t)(dty0 + b) * kTilePitch + dtx0;
+#pragma unroll
+                            for (int j = 0; j < 4; ++j) {
+                                const int a = x0 + j - sx;
+                                if ((unsigned)a < (unsigned)dwx) {
+                                    __stcs(orow + a, pn[j]);
+                                    dest_pixel(A, acc, pn[j], a, b, srow, gx0n, L);
+                                }
+                            }
                         }
+                        ws = wc;
+                        vs = vc;
+                        es = ec;
+                        wc = wn;
+                        vc = vn;
+                        ec = en;
                     }
-                    sW = cW;
-                    sC = cC;
-                    sE = cE;
-                    cW = nW;
-                    cC = nC;
-                    cE = nE;
-                    p += PX;
-                    q += PX;
-                    o += kTilePitch;
-                    if (++gy >= L) gy -= L;
-                }
-                if (yfirst >= 0) {
-                    acc.blox = min(acc.blox, x);
-                    acc.bhix = max(acc.bhix, x);
-                    acc.bloy = min(acc.bloy, yfirst);
-                    acc.bhiy = max(acc.bhiy, ylast);
                 }
             }
-            acc.pmaxb = max(acc.pmaxb, (int)__float_as_uint(pmaxf));
-            if (!ident) {
-                // destination pixels whose source lies outside the window
-                for (int b = b_lo + warp; b < b_hi; b += kWarps) {
-                    const int j = b + sy;
-                    const bool jin = (unsigned)j < (unsigned)WY;
-                    float* orow = tile_out + (size_t)(dty0 + b) * kTilePitch + dtx0;
-                    for (int a = lane; a < dwx; a += 32) {
-                        const int i = a + sx;
-                        if (!(jin && (unsigned)i < (unsigned)WX)) __stcs(orow + a, 0.0f);
-                    }
+        }
+        if (!abort && !ident) {
+            // destination pixels whose source lies outside the window
+            for (int b = b_lo + warp; b < b_hi; b += kWarps) {
+                const int j = b + sy;
+                const bool jin = (unsigned)j < (unsigned)WY;
+                float* orow = tile_out + (size_t)(dty0 + b) * kTilePitch + dtx0;
+                for (int a = lane; a < dwx; a += 32) {
+                    const int i = a + sx;
+                    if (!(jin && (unsigned)i < (unsigned)WX)) __stcs(orow + a, 0.0f);
                 }
             }
         }
     } else {
         // ---- full-moment step: phi^{n+1} of own rows plus a one-row halo over
         // the staged S (own rows hold S_other, halo rows q_S), then the
-        // destination pass with the perimeter.
+        // destination pass with the perimeter. (reduce_force's barrier orders
+        // the S_other stores of pass 1 before these reads.)
         if (!abort) {
             const int ua = max(0, y0 - 1), ub = min(WY, y1 + 1);
             constexpr int H = pick_run(WX, RB + 2);
