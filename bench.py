@@ -262,7 +262,7 @@ def main():
     ap.add_argument("--steps", type=int, default=6000)
     ap.add_argument("--warmup", type=int, default=60)
     ap.add_argument("--impl", default="pfb", choices=["pfb", "reference"])
-    ap.add_argument("--cluster", type=int, default=4, help="CTAs per cell (2, 4 or 8)")
+    ap.add_argument("--cluster", type=int, default=2, help="CTAs per cell (2, 4 or 8)")
     ap.add_argument("--variant", type=int, default=0, help="kernel variant (0 = default)")
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=int(os.environ.get("PFB_CPU_STEPS", "6")))

@@ -186,14 +186,14 @@ size_t pfb_sizeof(int which);
 int pfb_step2d_configure(void);
 
 /* Number of CTAs the step launch uses for N cells with `cluster` CTAs per
- * cell (cluster = 0 selects the default 4). Replaces k_step_grid(). */
+ * cell (cluster = 0 selects the default 2). Replaces k_step_grid(). */
 int pfb_step2d_grid(int num_cells, int cluster);
 
 /* One full step for every cell: tumble, interaction integral, Euler update,
  * recentring store, Q5.27 scatter into S_sc, FP64 moments, and clearing of
  * S_cl (clear_ahead_words words). `cluster` is the number of CTAs of the
  * thread-block cluster that cooperates on one cell (2, 4 or 8; 0 = default
- * 4).
+ * 2).
  * Returns PFB_E_ARG for a null buffer, a phi pool or S slot not 16-byte
  * aligned, L not larger than 286, or a non-null `moments`. */
 int pfb_step2d_launch(const pfb_step_args2d* args, int cluster, void* stream);

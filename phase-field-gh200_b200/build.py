@@ -55,31 +55,41 @@ def _run(cmd: list[str], verbose: bool) -> str:
     return p.stdout + p.stderr
 
 
-def build(force: bool = False, verbose: bool = False, ptxas_report: bool = False) -> Path:
-    """Compile changed sources and relink the library; returns its path."""
-    OUT_DIR.mkdir(parents=True, exist_ok=True)
-    OBJ_DIR.mkdir(parents=True, exist_ok=True)
+def build(force: bool = False, verbose: bool = False, ptxas_report: bool = False,
+          defines: list[str] | None = None, out: Path | None = None) -> Path:
+    """Compile changed sources and relink the library; returns its path.
+
+    ``defines`` (``NAME=VALUE`` strings) and ``out`` build an alternative copy
+    of the library (objects in their own folder) without touching the default
+    one; such a copy is loaded by setting ``PFB_LIB`` to its path."""
+    lib_path = LIB if out is None else Path(out).resolve()
+    obj_dir = OBJ_DIR if out is None else lib_path.parent / (lib_path.stem + "_obj")
+    defines = list(defines or [])
+    if defines or out is not None:
+        force = True
+    lib_path.parent.mkdir(parents=True, exist_ok=True)
+    obj_dir.mkdir(parents=True, exist_ok=True)
     headers = [CSRC / h for h in HEADERS] + [INCLUDE / "pfb200.h"]
     objs = []
-    relink = force or not LIB.exists()
+    relink = force or not lib_path.exists()
     for src in SOURCES:
         s = CSRC / src
-        o = OBJ_DIR / (src + ".o")
+        o = obj_dir / (src + ".o")
         objs.append(o)
         if force or _newer(o, [s, *headers, Path(__file__)]):
-            cmd = [NVCC, *ARCH, *COMMON, "-c", str(s), "-o", str(o)]
+            cmd = [NVCC, *ARCH, *COMMON, *(f"-D{d}" for d in defines), "-c", str(s), "-o", str(o)]
             if ptxas_report and src.endswith(".cu"):
                 cmd += ["-Xptxas", "-v"]
             out = _run(cmd, verbose)
             if ptxas_report and out:
                 print(out)
             relink = True
-    if relink or _newer(LIB, objs):
-        tmp = LIB.with_suffix(".so.tmp")
+    if relink or _newer(lib_path, objs):
+        tmp = lib_path.with_suffix(".so.tmp")
         _run([NVCC, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-cudart", "static"],
              verbose)
-        os.replace(tmp, LIB)
-    return LIB
+        os.replace(tmp, lib_path)
+    return lib_path
 
 
 if __name__ == "__main__":
@@ -87,5 +97,9 @@ if __name__ == "__main__":
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--verbose", action="store_true")
     ap.add_argument("--ptxas", action="store_true", help="print the ptxas resource report")
+    ap.add_argument("-D", dest="defines", action="append", default=[],
+                    help="extra preprocessor definition NAME=VALUE (e.g. PFB_STEP2D_THREADS=256)")
+    ap.add_argument("--out", default=None, help="write the library here instead")
     a = ap.parse_args()
-    print(build(force=a.force, verbose=a.verbose, ptxas_report=a.ptxas))
+    print(build(force=a.force, verbose=a.verbose, ptxas_report=a.ptxas, defines=a.defines,
+                out=a.out))

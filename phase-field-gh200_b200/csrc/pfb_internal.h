@@ -14,6 +14,10 @@ void clear_error();
 // step2d.cu
 int step2d_configure_device();
 int step2d_launch(const pfb_step_args2d* a, int cluster, cudaStream_t stream);
+// CTAs per cell when a caller passes cluster = 0: pairs of CTAs measured
+// fastest on B200 for the class-0 windows (two resident clusters per SM).
+constexpr int kDefaultCluster = 2;
+
 int step2d_smem_bytes(int cluster);
 int step2d_read_status(unsigned* out, int clear);
 // variant: 0 = default, 1 = one thread-block cluster per cell

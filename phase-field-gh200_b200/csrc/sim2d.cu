@@ -40,7 +40,7 @@ struct pfb_sim2d {
     pfb_traj_cell2d* d_traj = nullptr;
     cudaStream_t stream = nullptr;
     long long steps_done = 0;
-    int cluster = 4;
+    int cluster = kDefaultCluster;
     int variant = 0;
     bool use_graph = true;
     bool graph_ready = false;
@@ -258,7 +258,7 @@ extern "C" {
 int pfb_step2d_configure(void) { return step2d_configure_device(); }
 
 int pfb_step2d_grid(int num_cells, int cluster) {
-    if (cluster == 0) cluster = 4;
+    if (cluster == 0) cluster = kDefaultCluster;
     if (num_cells < 0 || (cluster != 2 && cluster != 4 && cluster != 8)) return PFB_E_ARG;
     return num_cells * cluster;
 }

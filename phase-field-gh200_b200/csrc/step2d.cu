@@ -35,7 +35,15 @@
 
 namespace pfb {
 
-constexpr int kThreads = 224;
+// Block shape: threads per CTA and the CTAs per SM the register budget is
+// sized for (overridable at build time to sweep launch shapes).
+#ifndef PFB_STEP2D_THREADS
+#define PFB_STEP2D_THREADS 288
+#endif
+#ifndef PFB_STEP2D_MINB
+#define PFB_STEP2D_MINB 3
+#endif
+constexpr int kThreads = PFB_STEP2D_THREADS;
 constexpr int kWarps = kThreads / 32;
 constexpr int kHeaderBytes = 2048;
 
@@ -230,8 +238,9 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
     __syncthreads();
     const bool abort = sh.abort != 0;
 
-    // ---- pass 1: S_other of the thread's strip (kept in registers) and the
-    // interaction integral
+    // ---- pass 1: S_other of the thread's strip (stored over q_S) and the
+    // interaction integral. A thread owns a strip four pixels wide and up to
+    // H rows tall; rows run in a rolled loop with a three-row register window.
     using QM = QuadMap<CLS, K>;
     constexpr int H = QM::H;
     const bool active = !abort && tid < QM::NQ * QM::G;
@@ -244,51 +253,39 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
         w = row[-1];
         e = row[4];
     };
-    float so[H][4];
     double aIx = 0.0, aIy = 0.0;
     if (active) {
         float ws, es, wc, ec;
         float4 vs, vc;
         load_row(r0 - 1, ws, vs, es);
         load_row(r0, wc, vc, ec);
+        uint32_t* qrow = ps_s + (r0 + 1) * PX + soff + x0;
+#pragma unroll 1
+        for (int r = 0; r < nr; ++r) {
+            float wn, en;
+            float4 vn;
+            load_row(r0 + r + 1, wn, vn, en);
+            const float C[6] = {wc, vc.x, vc.y, vc.z, vc.w, ec};
+            const float Sv[4] = {vs.x, vs.y, vs.z, vs.w};
+            const float Nv[4] = {vn.x, vn.y, vn.z, vn.w};
 #pragma unroll
-        for (int r = 0; r < H; ++r) {
-            if (r < nr) {
-                float wn, en;
-                float4 vn;
-                load_row(r0 + r + 1, wn, vn, en);
-                const uint32_t* qrow = ps_s + (r0 + r + 1) * PX + soff + x0;
-                const float C[6] = {wc, vc.x, vc.y, vc.z, vc.w, ec};
-                const float Sv[4] = {vs.x, vs.y, vs.z, vs.w};
-                const float Nv[4] = {vn.x, vn.y, vn.z, vn.w};
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const float cC = C[j + 1];
-                    // counted twice: the reference evaluates S_other in both passes
-                    const float So = s_other_n(qrow[j], cC, A.flags, 2u);
-                    so[r][j] = So;
-                    const float gx = 0.5f * (C[j + 2] - C[j]);
-                    const float gy = 0.5f * (Nv[j] - Sv[j]);
-                    aIx += (double)(cC * gx * So);
-                    aIy += (double)(cC * gy * So);
-                }
-                ws = wc;
-                vs = vc;
-                es = ec;
-                wc = wn;
-                vc = vn;
-                ec = en;
+            for (int j = 0; j < 4; ++j) {
+                const float cC = C[j + 1];
+                // counted twice: the reference evaluates S_other in both passes
+                const float So = s_other_n(qrow[j], cC, A.flags, 2u);
+                qrow[j] = __float_as_uint(So);
+                const float gx = 0.5f * (C[j + 2] - C[j]);
+                const float gy = 0.5f * (Nv[j] - Sv[j]);
+                aIx += (double)(cC * gx * So);
+                aIy += (double)(cC * gy * So);
             }
-        }
-        if (fm) {
-            // the full-moment pass reads S_other of own rows from shared memory
-#pragma unroll
-            for (int r = 0; r < H; ++r)
-                if (r < nr) {
-                    uint32_t* qrow = ps_s + (r0 + r + 1) * PX + soff + x0;
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) qrow[j] = __float_as_uint(so[r][j]);
-                }
+            qrow += PX;
+            ws = wc;
+            vs = vc;
+            es = ec;
+            wc = wn;
+            vc = vn;
+            ec = en;
         }
     }
     reduce_force<K, kWarps>(A, P, rank, sh.red, aIx, aIy, &g_step2d_status);
@@ -330,6 +327,7 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
             float4 vs, vc;
             load_row(r0 - 1, ws, vs, es);
             load_row(r0, wc, vc, ec);
+            const uint32_t* qrow = ps_s + (r0 + 1) * PX + soff + x0;
             if (ident) {
                 float pmaxf = 0.0f;
                 unsigned colmask = 0u;
@@ -341,62 +339,69 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
                 int gxj[4];
 #pragma unroll
                 for (int j = 0; j < 4; ++j) gxj[j] = gx + j < L ? gx + j : gx + j - L;
-                double xd[4];
-#pragma unroll
-                for (int j = 0; j < 4; ++j) xd[j] = (double)(x0 + j);
                 float* o = tile_out + (size_t)(TY0 + y0 + r0) * kTilePitch + TX0 + x0;
+                // overflow checks of a row's atomics run one row later, so the
+                // atomic round trip overlaps the next row's arithmetic
+                uint32_t old_prev[4] = {0u, 0u, 0u, 0u}, q_prev[4] = {0u, 0u, 0u, 0u};
+#pragma unroll 1
+                for (int r = 0; r < nr; ++r) {
+                    float wn, en;
+                    float4 vn;
+                    load_row(r0 + r + 1, wn, vn, en);
+                    const float so[4] = {__uint_as_float(qrow[0]), __uint_as_float(qrow[1]),
+                                         __uint_as_float(qrow[2]), __uint_as_float(qrow[3])};
+                    float pn[4];
+                    stencil4(ws, vs, es, wc, vc, ec, wn, vn, en, so, gam, dwC, volC, repC, vx,
+                             vy, mrel, dtf, pn);
+                    __stcs(reinterpret_cast<float4*>(o), make_float4(pn[0], pn[1], pn[2], pn[3]));
+                    uint32_t* srow = A.S_sc + (size_t)gy * Pp;
+                    bool ovf = false;
 #pragma unroll
-                for (int r = 0; r < H; ++r) {
-                    if (r < nr) {
-                        float wn, en;
-                        float4 vn;
-                        load_row(r0 + r + 1, wn, vn, en);
-                        float pn[4];
-                        stencil4(ws, vs, es, wc, vc, ec, wn, vn, en, so[r], gam, dwC, volC, repC,
-                                 vx, vy, mrel, dtf, pn);
-                        __stcs(reinterpret_cast<float4*>(o + r * kTilePitch),
-                               make_float4(pn[0], pn[1], pn[2], pn[3]));
-                        uint32_t* srow = A.S_sc + (size_t)gy * Pp;
-                        double rowV = 0.0;
-                        unsigned m = 0u;
+                    for (int j = 0; j < 4; ++j) ovf |= old_prev[j] > 0xFFFFFFFFu - q_prev[j];
+                    if (ovf) atomicOr(A.flags + PFB_FLAG_S_OVERFLOW, 1u);
+                    double rowV = 0.0, rowX = 0.0;
+                    unsigned m = 0u;
 #pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-                            const float p = pn[j];
-                            if (fabsf(p) <= 2.0f) {
-                                pmaxf = fmaxf(pmaxf, fabsf(p));
-                            } else {
-                                if (!isfinite(p)) atomicOr(A.flags + PFB_FLAG_NONFINITE, 1u);
-                                if (p * p > kPhiSqCap) atomicOr(A.flags + PFB_FLAG_Q_CLAMP, 1u);
-                                acc.pmaxb = max(acc.pmaxb, (int)__float_as_uint(fabsf(p)));
-                            }
-                            const uint32_t qv = q_encode(p);
-                            if (qv) {
-                                const uint32_t old = atomicAdd(srow + gxj[j], qv);
-                                if (old > 0xFFFFFFFFu - qv)
-                                    atomicOr(A.flags + PFB_FLAG_S_OVERFLOW, 1u);
-                            }
-                            const double d = (double)p * (double)p;
-                            rowV += d;
-                            acc.Cx += d * xd[j];
-                            if (p > kSupportEps) m |= 1u << j;
+                    for (int j = 0; j < 4; ++j) {
+                        const float p = pn[j];
+                        if (fabsf(p) <= 2.0f) {
+                            pmaxf = fmaxf(pmaxf, fabsf(p));
+                        } else {
+                            if (!isfinite(p)) atomicOr(A.flags + PFB_FLAG_NONFINITE, 1u);
+                            if (p * p > kPhiSqCap) atomicOr(A.flags + PFB_FLAG_Q_CLAMP, 1u);
+                            acc.pmaxb = max(acc.pmaxb, (int)__float_as_uint(fabsf(p)));
                         }
-                        const int y = y0 + r0 + r;
-                        acc.V += rowV;
-                        acc.Cy += rowV * (double)y;
-                        if (m) {
-                            acc.bloy = min(acc.bloy, y);
-                            acc.bhiy = max(acc.bhiy, y);
-                            colmask |= m;
-                        }
-                        if (++gy >= L) gy -= L;
-                        ws = wc;
-                        vs = vc;
-                        es = ec;
-                        wc = wn;
-                        vc = vn;
-                        ec = en;
+                        const uint32_t qv = q_encode(p);
+                        q_prev[j] = qv;
+                        old_prev[j] = qv ? atomicAdd(srow + gxj[j], qv) : 0u;
+                        const double d = (double)p * (double)p;
+                        rowV += d;
+                        rowX += d * (double)j;
+                        if (p > kSupportEps) m |= 1u << j;
                     }
+                    const int y = y0 + r0 + r;
+                    acc.V += rowV;
+                    acc.Cx += rowV * (double)x0 + rowX;
+                    acc.Cy += rowV * (double)y;
+                    if (m) {
+                        acc.bloy = min(acc.bloy, y);
+                        acc.bhiy = max(acc.bhiy, y);
+                        colmask |= m;
+                    }
+                    if (++gy >= L) gy -= L;
+                    o += kTilePitch;
+                    qrow += PX;
+                    ws = wc;
+                    vs = vc;
+                    es = ec;
+                    wc = wn;
+                    vc = vn;
+                    ec = en;
                 }
+                bool ovf = false;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) ovf |= old_prev[j] > 0xFFFFFFFFu - q_prev[j];
+                if (ovf) atomicOr(A.flags + PFB_FLAG_S_OVERFLOW, 1u);
                 acc.pmaxb = max(acc.pmaxb, (int)__float_as_uint(pmaxf));
                 if (colmask) {
                     acc.blox = min(acc.blox, x0 + __ffs(colmask) - 1);
@@ -404,37 +409,38 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
                 }
             } else {
                 // shifted or re-classed destination: per-pixel map
+#pragma unroll 1
+                for (int r = 0; r < nr; ++r) {
+                    float wn, en;
+                    float4 vn;
+                    load_row(r0 + r + 1, wn, vn, en);
+                    const float so[4] = {__uint_as_float(qrow[0]), __uint_as_float(qrow[1]),
+                                         __uint_as_float(qrow[2]), __uint_as_float(qrow[3])};
+                    float pn[4];
+                    stencil4(ws, vs, es, wc, vc, ec, wn, vn, en, so, gam, dwC, volC, repC, vx,
+                             vy, mrel, dtf, pn);
+                    const int b = y0 + r0 + r - sy;
+                    if ((unsigned)b < (unsigned)dwy) {
+                        int gyn = gy0n + b;
+                        if (gyn >= L) gyn -= L;
+                        uint32_t* srow = A.S_sc + (size_t)gyn * Pp;
+                        float* orow = tile_out + (size_t)(dty0 + b) * kTilePitch + dtx0;
 #pragma unroll
-                for (int r = 0; r < H; ++r) {
-                    if (r < nr) {
-                        float wn, en;
-                        float4 vn;
-                        load_row(r0 + r + 1, wn, vn, en);
-                        float pn[4];
-                        stencil4(ws, vs, es, wc, vc, ec, wn, vn, en, so[r], gam, dwC, volC, repC,
-                                 vx, vy, mrel, dtf, pn);
-                        const int b = y0 + r0 + r - sy;
-                        if ((unsigned)b < (unsigned)dwy) {
-                            int gyn = gy0n + b;
-                            if (gyn >= L) gyn -= L;
-                            uint32_t* srow = A.S_sc + (size_t)gyn * Pp;
-                            float* orow = tile_out + (size_t)(dty0 + b) * kTilePitch + dtx0;
-#pragma unroll
-                            for (int j = 0; j < 4; ++j) {
-                                const int a = x0 + j - sx;
-                                if ((unsigned)a < (unsigned)dwx) {
-                                    __stcs(orow + a, pn[j]);
-                                    dest_pixel(A, acc, pn[j], a, b, srow, gx0n, L);
-                                }
+                        for (int j = 0; j < 4; ++j) {
+                            const int a = x0 + j - sx;
+                            if ((unsigned)a < (unsigned)dwx) {
+                                __stcs(orow + a, pn[j]);
+                                dest_pixel(A, acc, pn[j], a, b, srow, gx0n, L);
                             }
                         }
-                        ws = wc;
-                        vs = vc;
-                        es = ec;
-                        wc = wn;
-                        vc = vn;
-                        ec = en;
                     }
+                    qrow += PX;
+                    ws = wc;
+                    vs = vc;
+                    es = ec;
+                    wc = wn;
+                    vc = vn;
+                    ec = en;
                 }
             }
         }
@@ -536,7 +542,7 @@ __device__ __forceinline__ void global_cell_v1(const pfb_step_args2d& A, int n, 
 }
 
 template <int K>
-__global__ void __launch_bounds__(kThreads, 3)
+__global__ void __launch_bounds__(kThreads, PFB_STEP2D_MINB)
     k_step2d(const __grid_constant__ pfb_step_args2d A) {
     extern __shared__ __align__(128) char smem[];
     const int tid = threadIdx.x;
@@ -638,7 +644,7 @@ int step2d_launch_variant(const pfb_step_args2d* a, int cluster, int variant,
     if (A.L <= 286 || A.P < A.L || (A.P & 3))
         return set_error(PFB_E_ARG, "domain side must exceed 286, P >= L and P % 4 == 0");
     if (A.parity_out != 0 && A.parity_out != 1) return set_error(PFB_E_ARG, "parity_out must be 0 or 1");
-    if (cluster == 0) cluster = 4;
+    if (cluster == 0) cluster = kDefaultCluster;
     if (cluster != 2 && cluster != 4 && cluster != 8)
         return set_error(PFB_E_CONFIG, "cluster must be 2, 4 or 8");
     if (variant == 0) variant = 1;

@@ -8,6 +8,7 @@ load, :func:`lib` raises.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 import numpy as np
@@ -182,14 +183,16 @@ class PfbError(RuntimeError):
 
 
 def lib() -> C.CDLL:
-    """Load ``libpfb200.so`` (built by ``build.py``); raise if it is absent."""
+    """Load ``libpfb200.so`` (built by ``build.py``; ``PFB_LIB`` names another
+    build of it); raise if it is absent."""
     global _LIB
     if _LIB is None:
-        if not LIB_PATH.exists():
+        path = Path(os.environ.get("PFB_LIB") or LIB_PATH)
+        if not path.exists():
             raise RuntimeError(
-                f"{LIB_PATH} is missing: build it with "
+                f"{path} is missing: build it with "
                 "`python phase-field-gh200_b200/build.py` (there is no fallback path)")
-        L = C.CDLL(str(LIB_PATH))
+        L = C.CDLL(str(path))
         for name, (res, args) in _SIGS.items():
             f = getattr(L, name)
             f.restype = res

@@ -111,7 +111,7 @@ class Sim2D:
 
     def __init__(self, params: SimParams2D, cx=None, cy=None, *, device: int = 0,
                  cells: np.ndarray | None = None, phi: np.ndarray | None = None,
-                 step: int = 0, cluster: int = 4, use_graph: bool = True, variant: int = 0):
+                 step: int = 0, cluster: int = 2, use_graph: bool = True, variant: int = 0):
         params.validate()
         self.params = params
         self._pc = params.to_c()

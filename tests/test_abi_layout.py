@@ -69,7 +69,7 @@ def test_launcher_rejects_bad_arguments_without_touching_a_device():
     a = StepArgs2D()
     assert L.pfb_step2d_launch(C.byref(a), 4, None) == -1  # null buffers
     assert b"null" in L.pfb_last_error()
-    assert L.pfb_step2d_grid(64, 0) == 256  # default clusters of 4
+    assert L.pfb_step2d_grid(64, 0) == 128  # default clusters of 2
     assert L.pfb_step2d_grid(64, 8) == 512
     assert L.pfb_step2d_grid(64, 3) == -1
 

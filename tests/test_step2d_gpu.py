@@ -119,7 +119,7 @@ def test_kernel_variants_agree(synth):
                                       s_from_phi(out[kv][1], out[kv][0], p.L)[:, :p.L])
 
 
-@pytest.mark.parametrize("cluster,variant", [(4, 1), (8, 1)])
+@pytest.mark.parametrize("cluster,variant", [(2, 1), (4, 1), (8, 1)])
 def test_deterministic_rerun(synth, cluster, variant):
     p, cells, phi = synth
     res = []
@@ -132,7 +132,7 @@ def test_deterministic_rerun(synth, cluster, variant):
 
 
 @pytest.mark.skipif(not oracle2d.ref_available(), reason="reference build absent")
-@pytest.mark.parametrize("cluster,variant", [(4, 1), (8, 1)])
+@pytest.mark.parametrize("cluster,variant", [(2, 1), (4, 1), (8, 1)])
 def test_one_step_all_classes_vs_reference_kernel(synth, cluster, variant):
     p, cells, phi = synth
     step = 9000037
