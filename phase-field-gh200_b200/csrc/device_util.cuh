@@ -146,6 +146,51 @@ __device__ __forceinline__ void bulk_g2s(void* dst_smem, const void* src_gmem, u
         : "memory");
 }
 
+// ---- L2 eviction-priority policies -------------------------------------------
+__device__ __forceinline__ uint64_t l2_policy_evict_first() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t l2_policy_evict_last() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+// Bulk copy as bulk_g2s, with an L2 eviction-priority policy for the source.
+__device__ __forceinline__ void bulk_g2s_hint(void* dst_smem, const void* src_gmem,
+                                              uint32_t bytes, uint64_t* bar, uint64_t policy) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint "
+        "[%0], [%1], %2, [%3], %4;" ::"r"(smem_addr(dst_smem)),
+        "l"(src_gmem), "r"(bytes), "r"(smem_addr(bar)), "l"(policy)
+        : "memory");
+}
+
+// 16-byte global store with an L2 eviction-priority policy.
+__device__ __forceinline__ void st_global_v4_hint(float4* p, float4 v, uint64_t policy) {
+    asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(p),
+                 "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w), "l"(policy)
+                 : "memory");
+}
+
+// atomicAdd of v to *p issued as one predicated instruction when v != 0
+// (adding zero is skipped, as a branch around atomicAdd would); returns the
+// previous value, or 0 when nothing was added. Only S scatter targets are
+// passed here, which the calling pass does not otherwise read.
+__device__ __forceinline__ uint32_t atom_add_nonzero(uint32_t* p, uint32_t v) {
+    uint32_t old;
+    asm volatile(
+        "{\n\t.reg .pred nz;\n\t"
+        "setp.ne.u32 nz, %2, 0;\n\t"
+        "mov.u32 %0, 0;\n\t"
+        "@nz atom.global.add.u32 %0, [%1], %2;\n\t}"
+        : "=r"(old)
+        : "l"(p), "r"(v));
+    return old;
+}
+
 // ---- warp reductions (fixed butterfly-down order) ------------------------
 __device__ __forceinline__ double warp_sum_down(double v) {
 #pragma unroll

@@ -194,6 +194,18 @@ PFB_HD PFB_INLINE float rhs_pixel(float lap, float phi, float s_other, float gx,
            (vx * gx + vy * gy);
 }
 
+#if defined(__CUDACC__)
+// rhs_pixel without the branch on mrel: for mrel == 1 the product mrel * X
+// is X exactly, so both forms of rhs_pixel give the same value.
+__device__ __forceinline__ float rhs_pixel_m(float lap, float phi, float s_other, float gx,
+                                             float gy, float gam, float dwC, float volC,
+                                             float repC, float vx, float vy, float mrel) {
+    return mrel * (gam * lap - dwC * (phi * (1.0f - phi) * (1.0f - 2.0f * phi)) +
+                   volC * phi - repC * phi * s_other) -
+           (vx * gx + vy * gy);
+}
+#endif
+
 // Nine-point isotropic Laplacian (4 edges + diagonals - 20 centre) / 6, h=1.
 PFB_HD PFB_INLINE float lap9(float nW, float nC, float nE, float cW, float cC,
                              float cE, float sW, float sC, float sE) {

@@ -43,6 +43,12 @@ namespace pfb {
 #ifndef PFB_STEP2D_MINB
 #define PFB_STEP2D_MINB 3
 #endif
+// L2 eviction priorities (bit 0: the staged phi_in and S_rd rows are read
+// evict-first; bit 1: phi_out rows are stored evict-last so the next step's
+// staging finds them in L2).
+#ifndef PFB_STEP2D_L2HINTS
+#define PFB_STEP2D_L2HINTS 1
+#endif
 constexpr int kThreads = PFB_STEP2D_THREADS;
 constexpr int kWarps = kThreads / 32;
 constexpr int kHeaderBytes = 2048;
@@ -110,7 +116,7 @@ __device__ __forceinline__ void stencil4(float ws, float4 vs, float es, float wc
         const float gx = 0.5f * (C[j + 2] - C[j]);
         const float gy = 0.5f * (N[j + 1] - S[j + 1]);
         const float rhs =
-            rhs_pixel(lap, C[j + 1], so[j], gx, gy, gam, dwC, volC, repC, vx, vy, mrel);
+            rhs_pixel_m(lap, C[j + 1], so[j], gx, gy, gam, dwC, volC, repC, vx, vy, mrel);
         pn[j] = C[j + 1] + dtf * rhs;
     }
 }
@@ -186,20 +192,26 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
         bytes = __reduce_add_sync(0xFFFFFFFFu, bytes);
         if (lane == 0) dev::mbar_arrive_expect_tx(&sh.bar, bytes);
         __syncwarp();
+#if PFB_STEP2D_L2HINTS & 1
+        const uint64_t pol = dev::l2_policy_evict_first();
+#define PFB_G2S(d, s, n, b) dev::bulk_g2s_hint(d, s, n, b, pol)
+#else
+#define PFB_G2S(d, s, n, b) dev::bulk_g2s(d, s, n, b)
+#endif
         for (int y = ra + lane; y < rb; y += 32)
-            dev::bulk_g2s(phi_s + (y - y0 + 2) * PX + 4,
-                          tile_in + (size_t)(TY0 + y) * kTilePitch + TX0, (uint32_t)(WX * 4),
-                          &sh.bar);
+            PFB_G2S(phi_s + (y - y0 + 2) * PX + 4, tile_in + (size_t)(TY0 + y) * kTilePitch + TX0,
+                    (uint32_t)(WX * 4), &sh.bar);
         if (s_tma) {
             for (int y = sa + lane; y < sb; y += 32) {
                 int gy = gy0 + y;
                 if (gy >= L) gy -= L;
                 const uint32_t* row = A.S_rd + (size_t)gy * Pp;
                 uint32_t* dst = ps_s + (y - y0 + 1) * PX;
-                dev::bulk_g2s(dst, row + gxa, (uint32_t)(n1 * 4), &sh.bar);
-                if (n2) dev::bulk_g2s(dst + (L - gxa), row, (uint32_t)(n2 * 4), &sh.bar);
+                PFB_G2S(dst, row + gxa, (uint32_t)(n1 * 4), &sh.bar);
+                if (n2) PFB_G2S(dst + (L - gxa), row, (uint32_t)(n2 * 4), &sh.bar);
             }
         }
+#undef PFB_G2S
         if (lane == 0) plan_cell(A, n, CLS, step, sh.plan, rank == 0);
     } else {
         const int t = tid - 32;
@@ -260,6 +272,7 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
         load_row(r0 - 1, ws, vs, es);
         load_row(r0, wc, vc, ec);
         uint32_t* qrow = ps_s + (r0 + 1) * PX + soff + x0;
+        uint32_t neg = 0u;
 #pragma unroll 1
         for (int r = 0; r < nr; ++r) {
             float wn, en;
@@ -271,8 +284,7 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const float cC = C[j + 1];
-                // counted twice: the reference evaluates S_other in both passes
-                const float So = s_other_n(qrow[j], cC, A.flags, 2u);
+                const float So = s_other_counted(qrow[j], cC, neg);
                 qrow[j] = __float_as_uint(So);
                 const float gx = 0.5f * (C[j + 2] - C[j]);
                 const float gy = 0.5f * (Nv[j] - Sv[j]);
@@ -287,6 +299,8 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
             vc = vn;
             ec = en;
         }
+        // counted twice: the reference evaluates S_other in both passes
+        if (neg) atomicAdd(A.flags + PFB_FLAG_S_NEGATIVE, 2u * neg);
     }
     reduce_force<K, kWarps>(A, P, rank, sh.red, aIx, aIy, &g_step2d_status);
 
@@ -329,7 +343,10 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
             load_row(r0, wc, vc, ec);
             const uint32_t* qrow = ps_s + (r0 + 1) * PX + soff + x0;
             if (ident) {
-                float pmaxf = 0.0f;
+#if PFB_STEP2D_L2HINTS & 2
+                const uint64_t pol_out = dev::l2_policy_evict_last();
+#endif
+                uint32_t pmaxb = 0u;
                 unsigned colmask = 0u;
                 int gy = gy0 + y0 + r0;
                 if (gy >= L) gy -= L;
@@ -353,27 +370,39 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
                     float pn[4];
                     stencil4(ws, vs, es, wc, vc, ec, wn, vn, en, so, gam, dwC, volC, repC, vx,
                              vy, mrel, dtf, pn);
+#if PFB_STEP2D_L2HINTS & 2
+                    dev::st_global_v4_hint(reinterpret_cast<float4*>(o),
+                                           make_float4(pn[0], pn[1], pn[2], pn[3]), pol_out);
+#else
                     __stcs(reinterpret_cast<float4*>(o), make_float4(pn[0], pn[1], pn[2], pn[3]));
+#endif
                     uint32_t* srow = A.S_sc + (size_t)gy * Pp;
                     bool ovf = false;
 #pragma unroll
                     for (int j = 0; j < 4; ++j) ovf |= old_prev[j] > 0xFFFFFFFFu - q_prev[j];
                     if (ovf) atomicOr(A.flags + PFB_FLAG_S_OVERFLOW, 1u);
+                    // |phi| bit patterns order like the values; NaN and inf
+                    // sort above 2.0, so one compare guards the rare checks
+                    const uint32_t rowb =
+                        max(max(__float_as_uint(fabsf(pn[0])), __float_as_uint(fabsf(pn[1]))),
+                            max(__float_as_uint(fabsf(pn[2])), __float_as_uint(fabsf(pn[3]))));
+                    pmaxb = max(pmaxb, rowb);
+                    if (rowb > 0x40000000u) {  // some |phi| > 2 (or not finite)
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            const float p = pn[j];
+                            if (!isfinite(p)) atomicOr(A.flags + PFB_FLAG_NONFINITE, 1u);
+                            if (p * p > kPhiSqCap) atomicOr(A.flags + PFB_FLAG_Q_CLAMP, 1u);
+                        }
+                    }
                     double rowV = 0.0, rowX = 0.0;
                     unsigned m = 0u;
 #pragma unroll
                     for (int j = 0; j < 4; ++j) {
                         const float p = pn[j];
-                        if (fabsf(p) <= 2.0f) {
-                            pmaxf = fmaxf(pmaxf, fabsf(p));
-                        } else {
-                            if (!isfinite(p)) atomicOr(A.flags + PFB_FLAG_NONFINITE, 1u);
-                            if (p * p > kPhiSqCap) atomicOr(A.flags + PFB_FLAG_Q_CLAMP, 1u);
-                            acc.pmaxb = max(acc.pmaxb, (int)__float_as_uint(fabsf(p)));
-                        }
                         const uint32_t qv = q_encode(p);
                         q_prev[j] = qv;
-                        old_prev[j] = qv ? atomicAdd(srow + gxj[j], qv) : 0u;
+                        old_prev[j] = dev::atom_add_nonzero(srow + gxj[j], qv);
                         const double d = (double)p * (double)p;
                         rowV += d;
                         rowX += d * (double)j;
@@ -402,7 +431,7 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
 #pragma unroll
                 for (int j = 0; j < 4; ++j) ovf |= old_prev[j] > 0xFFFFFFFFu - q_prev[j];
                 if (ovf) atomicOr(A.flags + PFB_FLAG_S_OVERFLOW, 1u);
-                acc.pmaxb = max(acc.pmaxb, (int)__float_as_uint(pmaxf));
+                acc.pmaxb = max(acc.pmaxb, (int)pmaxb);
                 if (colmask) {
                     acc.blox = min(acc.blox, x0 + __ffs(colmask) - 1);
                     acc.bhix = max(acc.bhix, x0 + 31 - __clz(colmask));

@@ -39,6 +39,15 @@ __device__ __forceinline__ float s_other_n(uint32_t qS, float phi, uint32_t* fla
     return 0.0f;
 }
 
+// Branch-free form for the hot loops: the caller counts the negative cases
+// in `neg` and adds them to the flag once.
+__device__ __forceinline__ float s_other_counted(uint32_t qS, float phi, uint32_t& neg) {
+    const uint32_t qc = q_encode(phi);
+    const bool ok = qS >= qc;
+    neg += ok ? 0u : 1u;
+    return ok ? (float)(qS - qc) * kQInv : 0.0f;
+}
+
 // Tumble, class choice and recentring shift of cell n whose field is in class
 // `cls` (reference src/kernels.cu:93-191 and :624-711). Deterministic in its
 // inputs, so every CTA that runs it for the same cell decides the same thing;
