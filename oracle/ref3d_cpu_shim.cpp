@@ -1,0 +1,95 @@
+// ORACLE -- test infrastructure only. C entry points over the reference's
+// dense FP64 one-step evaluation and seed-radius calibration
+// (include/pf3d/reference.hpp, header-only; compiled in place by
+// oracle/Makefile into oracle/_ref/libref3d_cpu.so). The tests pin the 3D
+// oracle against it.
+#include <cstdint>
+#include <cstring>
+#include <exception>
+
+#include "pf3d/reference.hpp"
+#include "pf3d/rng.cuh"
+
+namespace ref = pf3d::reference;
+
+extern "C" {
+
+// Periodic cube of `side`, `cells` cells: phi (cells * side^3, x fastest),
+// gamma/speed per cell, polarity 3 per cell. Outputs: phi_next, volume,
+// integral (3 per cell), velocity (3 per cell). Returns 0, or -1 when the
+// reference rejects the input.
+int ref3d_cpu_one_step(int side, int cells, const double* phi, const double* gamma,
+                       const double* speed, const double* polarity, double dt, double lambda,
+                       double target_radius, double kappa, double mu, double xi,
+                       double* phi_next, double* volume, double* integral, double* velocity) {
+    try {
+        ref::DenseState st;
+        st.side = side;
+        st.cells.resize((size_t)cells);
+        for (int c = 0; c < cells; ++c) {
+            st.cells[(size_t)c].gamma = gamma[c];
+            st.cells[(size_t)c].active_speed = speed[c];
+            st.cells[(size_t)c].polarity = ref::Vector3{polarity[3 * c], polarity[3 * c + 1],
+                                                        polarity[3 * c + 2]};
+        }
+        st.phi.assign(phi, phi + (size_t)cells * side * side * side);
+        ref::ModelParameters m;
+        m.dt = dt;
+        m.lambda = lambda;
+        m.target_radius = target_radius;
+        m.kappa = kappa;
+        m.mu = mu;
+        m.xi = xi;
+        const ref::OneStepResult r = ref::one_euler_step(st, m);
+        std::memcpy(phi_next, r.phi_next.data(), r.phi_next.size() * sizeof(double));
+        for (int c = 0; c < cells; ++c) {
+            volume[c] = r.volume[(size_t)c];
+            integral[3 * c] = r.interaction_integral[(size_t)c].x;
+            integral[3 * c + 1] = r.interaction_integral[(size_t)c].y;
+            integral[3 * c + 2] = r.interaction_integral[(size_t)c].z;
+            velocity[3 * c] = r.velocity[(size_t)c].x;
+            velocity[3 * c + 1] = r.velocity[(size_t)c].y;
+            velocity[3 * c + 2] = r.velocity[(size_t)c].z;
+        }
+        return 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+int ref3d_cpu_calibrate(double radius, double lambda, int edge, double* seed, double* measured) {
+    try {
+        const ref::SeedRadiusCalibration c = ref::calibrate_seed_radius(radius, lambda, edge);
+        *seed = c.seed_radius;
+        *measured = c.measured_volume;
+        return c.converged ? 0 : 1;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+// The reference's 3D Philox draws (include/pf3d/rng.cuh:41-150).
+void ref3d_cpu_initial_polarity(int64_t gid, uint64_t stream, int planar, double* out) {
+    const pf3d::Vec3 v = planar ? pf3d::initial_planar_polarity(gid, stream)
+                                : pf3d::initial_polarity(gid, stream);
+    out[0] = v.x;
+    out[1] = v.y;
+    out[2] = v.z;
+}
+
+double ref3d_cpu_initial_speed(int64_t gid, uint64_t seed, double median, double sigma) {
+    return pf3d::initial_active_speed(gid, seed, median, sigma);
+}
+
+int ref3d_cpu_tumble(uint64_t step, int64_t gid, uint64_t stream, double p, int planar,
+                     double* out) {
+    const pf3d::Vec3 cur{0.0, 0.0, 0.0};
+    const pf3d::TumbleSample t = planar ? pf3d::tumble_sample_planar(step, gid, stream, p, cur)
+                                        : pf3d::tumble_sample(step, gid, stream, p, cur);
+    out[0] = t.polarity.x;
+    out[1] = t.polarity.y;
+    out[2] = t.polarity.z;
+    return t.tumbled ? 1 : 0;
+}
+
+}  // extern "C"

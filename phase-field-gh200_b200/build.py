@@ -34,8 +34,10 @@ COMMON = [
     "-Xcompiler", "-fPIC,-ffp-contract=off,-Wall",
     "-I", str(INCLUDE),
 ]
-SOURCES = ["step2d.cu", "init2d.cu", "sim2d.cu", "host2d.cpp"]
-HEADERS = ["pfb_common.cuh", "device_util.cuh", "pfb_internal.h", "step2d_common.cuh"]
+SOURCES = ["step2d.cu", "init2d.cu", "sim2d.cu", "host2d.cpp", "measure3d.cu", "update3d.cu",
+           "misc3d.cu", "sim3d.cu", "host3d.cpp"]
+HEADERS = ["pfb_common.cuh", "device_util.cuh", "pfb_internal.h", "step2d_common.cuh",
+           "pfb3d_common.cuh", "ring3d.cuh"]
 
 
 def _newer(target: Path, deps: list[Path]) -> bool:
@@ -69,7 +71,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_report: bool = False
         force = True
     lib_path.parent.mkdir(parents=True, exist_ok=True)
     obj_dir.mkdir(parents=True, exist_ok=True)
-    headers = [CSRC / h for h in HEADERS] + [INCLUDE / "pfb200.h"]
+    headers = [CSRC / h for h in HEADERS] + [INCLUDE / "pfb200.h", INCLUDE / "pfb200_3d.h"]
     objs = []
     relink = force or not lib_path.exists()
     for src in SOURCES:

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/pfb200.h"
+#include "../../include/pfb200_3d.h"
 
 namespace pfb {
 
@@ -38,5 +39,20 @@ int verify_cells2d(const float* phi, const pfb_cell2d* cell, const uint8_t* cls,
 int verify_S(const uint32_t* S, size_t n, uint32_t* out_max, cudaStream_t s);
 int pack_traj2d(const pfb_cell2d* cell, const uint8_t* cls, pfb_traj_cell2d* out, int N, int L,
                 cudaStream_t s);
+
+namespace p3 {
+// measure3d.cu / update3d.cu / misc3d.cu (pfb200_3d.h records)
+int measure3d_launch(const pfb_measure_args3d* a, cudaStream_t stream);
+int motion3d_launch(const pfb_measure_args3d* a, cudaStream_t stream);
+int update3d_launch(const pfb_update_args3d* a, cudaStream_t stream);
+// clears S; with a non-null guard only when a fatal global flag is set
+int clear3d_launch(uint32_t* S, const pfb_layout3d* L, const uint32_t* guard,
+                   cudaStream_t stream);
+int repair3d_launch(const pfb_update_args3d* a, cudaStream_t stream);
+int init3d_launch(const pfb_init_args3d* a, cudaStream_t stream);
+int scatter3d_launch(const pfb_scatter_args3d* a, cudaStream_t stream);
+int measure3d_read_status(unsigned* out, int clear);
+int update3d_read_status(unsigned* out, int clear);
+}  // namespace p3
 
 }  // namespace pfb

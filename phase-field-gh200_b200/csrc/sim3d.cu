@@ -1,0 +1,411 @@
+// Host driver of the 3D update: the reference's Sim3D step sequence in
+// throughput mode (two phi pools, two aggregate slots; reference
+// src/pf3d/sim.cu:1460-1651):
+//
+//   snapshot accepted cells -> measure (tumble on, surface on full-moment
+//   steps) -> motion -> clear next S -> update -> repair if fatal ->
+//   finalize origins -> restore if fatal -> advance step counter.
+//
+// A fresh start seeds tanh spheres with the calibrated radius, builds S from
+// them and measures once without a tumble (src/pf3d/sim.cu:1100-1180).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "pfb3d_common.cuh"
+#include "pfb_internal.h"
+
+using namespace pfb;
+using namespace pfb::p3;
+
+#define PFB3_CU(expr, what)                                                               \
+    do {                                                                                  \
+        const cudaError_t e_ = (expr);                                                    \
+        if (e_ != cudaSuccess) return set_error(PFB_E_CUDA, "%s: %s", what, cudaGetErrorString(e_)); \
+    } while (0)
+#define PFB3_RC(expr)          \
+    do {                       \
+        const int r_ = (expr); \
+        if (r_) return r_;     \
+    } while (0)
+
+struct pfb_sim3d {
+    pfb_params3d p{};
+    int device = 0;
+    int B = 0, N = 0;
+    pfb_layout3d L{};
+    size_t s_words = 0, cell_words = 0;
+    float* d_phi[2] = {nullptr, nullptr};
+    uint32_t* d_S[2] = {nullptr, nullptr};
+    pfb_cell3d* d_cells = nullptr;
+    pfb_cell3d* d_accepted = nullptr;
+    uint32_t* d_flags = nullptr;
+    uint64_t* d_step = nullptr;
+    float* d_wall = nullptr;
+    pfb_vec3* d_centres = nullptr;
+    cudaStream_t stream = nullptr;
+    int cur_phi = 0, cur_S = 0;
+    long long steps_done = 0;
+    double V0 = 0.0;
+
+    ~pfb_sim3d() {
+        if (stream) cudaStreamDestroy(stream);
+        cudaFree(d_phi[0]);
+        cudaFree(d_phi[1]);
+        cudaFree(d_S[0]);
+        cudaFree(d_S[1]);
+        cudaFree(d_cells);
+        cudaFree(d_accepted);
+        cudaFree(d_flags);
+        cudaFree(d_step);
+        cudaFree(d_wall);
+        cudaFree(d_centres);
+    }
+};
+
+namespace pfb {
+namespace p3 {
+int geometry_ok3(int B, const pfb_layout3d& L);
+}
+}  // namespace pfb
+
+namespace {
+
+double volume0(const pfb_params3d& p) {
+    const double sphere = 4.0 * kPi * p.target_radius * p.target_radius * p.target_radius / 3.0;
+    return substrate_slab(p.boundary_flags) ? 0.5 * sphere : sphere;
+}
+
+uint64_t polarity_stream(const pfb_params3d& p) { return p.polarity_seed ? p.polarity_seed : p.seed; }
+
+int validate3(const pfb_params3d& p) {
+    const uint32_t b = p.boundary_flags;
+    if (periodic_xyz(b)) {
+        if (p.Nx <= 0 || p.Nx != p.Ny || p.Nx != p.Nz)
+            return set_error(PFB_E_ARG, "the periodic domain must be a positive cube");
+    } else if (substrate_slab(b) || hard_wall_channel(b)) {
+        if (p.Nx <= 0 || p.Ny != p.Nx || p.Nz <= 0)
+            return set_error(PFB_E_ARG, "bounded-z geometry must have positive Nx=Ny and Nz");
+    } else {
+        return set_error(PFB_E_ARG, "unknown boundary flags");
+    }
+    if (hard_wall_channel(b)) {
+        if (p.channel_height <= 0 || p.channel_padding <= 0 || !(p.wall_width > 0.0) ||
+            !(p.wall_kappa > 0.0) || !(p.kappa > 0.0))
+            return set_error(PFB_E_ARG, "channel wall parameters must be positive");
+        if (p.channel_height + 2 * p.channel_padding != p.Nz)
+            return set_error(PFB_E_ARG, "channel Nz must equal H + 2*padding");
+    }
+    if (p.num_cells <= 0) return set_error(PFB_E_ARG, "num_cells must be positive");
+    if (!(p.dt > 0.0) || !(p.lambda > 0.0) || !(p.target_radius > 0.0) || !(p.xi > 0.0) ||
+        !(p.tau > 0.0) || p.kappa < 0.0 || p.mu < 0.0 || p.v_A < 0.0 || !(p.gamma > 0.0))
+        return set_error(PFB_E_ARG, "invalid model parameters");
+    if (p.dt * p.gamma * (256.0 / 30.0) >= 1.0)
+        return set_error(PFB_E_ARG, "explicit-Euler Laplacian stability bound is violated");
+    return PFB_OK;
+}
+
+int upload_wall(pfb_sim3d* s) {
+    const pfb_params3d& p = s->p;
+    std::vector<float> w((size_t)p.Nz);
+    const float ratio = (float)(p.wall_kappa / p.kappa);
+    const double k = 2.7386127875258306 / p.wall_width;
+    const double lo = (double)p.channel_padding, hi = lo + p.channel_height;
+    for (int z = 0; z < p.Nz; ++z) {
+        const double c = (double)z + 0.5;
+        const double fluid = 0.25 * (1.0 + std::tanh(k * (c - lo))) * (1.0 - std::tanh(k * (c - hi)));
+        const double wall = 1.0 - fluid;
+        w[(size_t)z] = ratio * (float)(wall * wall);
+    }
+    PFB3_CU(cudaMalloc(&s->d_wall, w.size() * sizeof(float)), "cudaMalloc(wall)");
+    PFB3_CU(cudaMemcpyAsync(s->d_wall, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice,
+                            s->stream),
+            "upload wall field");
+    return PFB_OK;
+}
+
+pfb_measure_args3d measure_args(pfb_sim3d* s, bool tumble, bool surface) {
+    pfb_measure_args3d m{};
+    m.phi = s->d_phi[s->cur_phi];
+    m.S = s->d_S[s->cur_S];
+    m.wall.values = s->d_wall;
+    m.wall.planes = s->d_wall ? s->L.nz : 0;
+    m.cells = s->d_cells;
+    m.global_flags = s->d_flags;
+    m.step = s->d_step;
+    m.layout = s->L;
+    m.N = s->N;
+    m.B = s->B;
+    m.shards = 1;
+    m.polarity_stream = polarity_stream(s->p);
+    const double aging = s->p.aging_time / s->p.dt + 0.5;
+    m.aging_steps = (uint64_t)(aging > 0.0 ? aging : 0.0);
+    m.p_tumble = -std::expm1(-s->p.dt / s->p.tau);
+    m.motility_coeff = (float)(coeff_interaction(s->p.kappa, s->p.lambda) / s->p.xi);
+    m.max_shift = kMaxShift3;
+    m.support_margin = (int)kSafetyMargin;
+    m.apply_tumble = tumble ? 1 : 0;
+    m.compute_surface = surface ? 1 : 0;
+    return m;
+}
+
+pfb_update_args3d update_args(pfb_sim3d* s) {
+    pfb_update_args3d u{};
+    u.phi_in = s->d_phi[s->cur_phi];
+    u.phi_out = s->d_phi[1 - s->cur_phi];
+    u.S_in = s->d_S[s->cur_S];
+    u.S_out = s->d_S[1 - s->cur_S];
+    u.wall.values = s->d_wall;
+    u.wall.planes = s->d_wall ? s->L.nz : 0;
+    u.cells = s->d_cells;
+    u.global_flags = s->d_flags;
+    u.layout = s->L;
+    u.N = s->N;
+    u.B = s->B;
+    u.dt = (float)s->p.dt;
+    u.V0 = s->V0;
+    u.volume_scale = coeff_volume(s->p.mu, s->V0);
+    u.bulk_scale = (float)coeff_bulk(s->p.lambda);
+    u.interaction_coeff = (float)coeff_interaction(s->p.kappa, s->p.lambda);
+    u.tile_pass = PFB3D_TILE_PASS_ALL;
+    return u;
+}
+
+int one_step(pfb_sim3d* s) {
+    const bool full = s->p.full_moment_every > 0 && s->steps_done % s->p.full_moment_every == 0;
+    PFB3_CU(cudaMemcpyAsync(s->d_accepted, s->d_cells, (size_t)s->N * sizeof(pfb_cell3d),
+                            cudaMemcpyDeviceToDevice, s->stream),
+            "snapshot accepted cells");
+    const pfb_measure_args3d m = measure_args(s, true, full);
+    PFB3_RC(measure3d_launch(&m, s->stream));
+    PFB3_RC(motion3d_launch(&m, s->stream));
+    PFB3_RC(clear3d_launch(s->d_S[1 - s->cur_S], &s->L, nullptr, s->stream));
+    const pfb_update_args3d u = update_args(s);
+    PFB3_RC(update3d_launch(&u, s->stream));
+    PFB3_RC(repair3d_launch(&u, s->stream));
+    PFB3_RC(pfb3d_finalize_origins(s->d_cells, s->N, s->d_flags, s->stream));
+    PFB3_RC(pfb3d_restore_cells_after_fatal(s->d_cells, s->d_accepted, s->N, s->d_flags, nullptr,
+                                            s->stream));
+    PFB3_RC(pfb3d_advance_step(s->d_step, s->d_flags, s->stream));
+    s->cur_phi = 1 - s->cur_phi;
+    s->cur_S = 1 - s->cur_S;
+    ++s->steps_done;
+    return PFB_OK;
+}
+
+int create_impl(pfb_sim3d* s, const pfb_params3d* pp, const pfb_vec3* centres, int device) {
+    s->p = *pp;
+    const pfb_params3d& p = s->p;
+    PFB3_RC(validate3(p));
+    s->device = device;
+    PFB3_CU(cudaSetDevice(device), "cudaSetDevice");
+    s->B = p.B > 0 ? p.B : pfb3d_automatic_brick_edge(p.target_radius, p.lambda);
+    if (s->B <= 0 || s->B % kBrickAlign != 0)
+        return set_error(PFB_E_CONFIG, "brick edge must be a positive multiple of 8");
+    s->N = p.num_cells;
+    s->L.nx = p.Nx;
+    s->L.ny = p.Ny;
+    s->L.nz = p.Nz;
+    s->L.pitch_x = (p.Nx + 31) / 32 * 32;
+    s->L.boundary_flags = p.boundary_flags;
+    if (!geometry_ok3(s->B, s->L)) return set_error(PFB_E_ARG, "the brick must fit inside the domain");
+    s->V0 = volume0(p);
+    s->s_words = (size_t)s->L.pitch_x * s->L.ny * s->L.nz;
+    s->cell_words = (size_t)s->B * s->B * s->B;
+    PFB3_CU(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream");
+    for (int i = 0; i < 2; ++i) {
+        PFB3_CU(cudaMalloc(&s->d_phi[i], (size_t)s->N * s->cell_words * sizeof(float)), "cudaMalloc(phi)");
+        PFB3_CU(cudaMalloc(&s->d_S[i], s->s_words * sizeof(uint32_t)), "cudaMalloc(S)");
+    }
+    PFB3_CU(cudaMalloc(&s->d_cells, (size_t)s->N * sizeof(pfb_cell3d)), "cudaMalloc(cells)");
+    PFB3_CU(cudaMalloc(&s->d_accepted, (size_t)s->N * sizeof(pfb_cell3d)), "cudaMalloc(cells)");
+    PFB3_CU(cudaMalloc(&s->d_flags, PFB3D_FLAG_COUNT * sizeof(uint32_t)), "cudaMalloc(flags)");
+    PFB3_CU(cudaMalloc(&s->d_step, sizeof(uint64_t)), "cudaMalloc(step)");
+    PFB3_CU(cudaMalloc(&s->d_centres, (size_t)s->N * sizeof(pfb_vec3)), "cudaMalloc(centres)");
+    PFB3_CU(cudaMemsetAsync(s->d_flags, 0, PFB3D_FLAG_COUNT * sizeof(uint32_t), s->stream), "memset");
+    PFB3_CU(cudaMemsetAsync(s->d_step, 0, sizeof(uint64_t), s->stream), "memset");
+    if (hard_wall_channel(p.boundary_flags)) PFB3_RC(upload_wall(s));
+
+    // per-cell records (reference src/pf3d/sim.cu:1100-1130), soft fraction 0
+    std::vector<pfb_cell3d> cells((size_t)s->N);
+    std::vector<pfb_vec3> ctr((size_t)s->N);
+    const bool slab = substrate_slab(p.boundary_flags);
+    for (int i = 0; i < s->N; ++i) {
+        pfb_cell3d c;
+        std::memset(&c, 0, sizeof(c));
+        c.global_id = i;
+        c.gamma = (float)p.gamma;
+        c.v_A = (float)initial_speed3(i, p.seed, p.v_A, p.v_A_sigma);
+        c.R_tgt = (float)p.target_radius;
+        const Dir3 d = initial_polarity3(i, polarity_stream(p), slab);
+        c.polarity_x = (float)d.x;
+        c.polarity_y = (float)d.y;
+        c.polarity_z = (float)d.z;
+        cells[(size_t)i] = c;
+        pfb_vec3 v = centres[i];
+        // channel centres are given in slit coordinates; stored z adds the
+        // padding minus half a plane (reference src/pf3d/sim.cu:1121-1124)
+        if (hard_wall_channel(p.boundary_flags))
+            v.z = (double)((float)v.z + (float)p.channel_padding - 0.5f);
+        ctr[(size_t)i] = v;
+    }
+    PFB3_CU(cudaMemcpyAsync(s->d_cells, cells.data(), cells.size() * sizeof(pfb_cell3d),
+                            cudaMemcpyHostToDevice, s->stream),
+            "upload cells");
+    PFB3_CU(cudaMemcpyAsync(s->d_centres, ctr.data(), ctr.size() * sizeof(pfb_vec3),
+                            cudaMemcpyHostToDevice, s->stream),
+            "upload centres");
+    double seed = 0.0;
+    PFB3_RC(pfb3d_calibrate_seed_radius(p.target_radius, p.lambda, s->B, &seed, nullptr));
+    pfb_init_args3d ia{};
+    ia.phi_even = s->d_phi[0];
+    ia.phi_odd = s->d_phi[1];
+    ia.cells = s->d_cells;
+    ia.centres = s->d_centres;
+    ia.N = s->N;
+    ia.B = s->B;
+    ia.layout = s->L;
+    ia.lambda = (float)p.lambda;
+    ia.seed_radius = (float)seed;
+    PFB3_RC(init3d_launch(&ia, s->stream));
+    PFB3_RC(clear3d_launch(s->d_S[0], &s->L, nullptr, s->stream));
+    pfb_scatter_args3d sa{};
+    sa.phi = s->d_phi[0];
+    sa.cells = s->d_cells;
+    sa.S = s->d_S[0];
+    sa.global_flags = s->d_flags;
+    sa.layout = s->L;
+    sa.N = s->N;
+    sa.B = s->B;
+    PFB3_RC(scatter3d_launch(&sa, s->stream));
+    const pfb_measure_args3d m = measure_args(s, false, true);
+    PFB3_RC(measure3d_launch(&m, s->stream));
+    PFB3_RC(motion3d_launch(&m, s->stream));
+    PFB3_CU(cudaStreamSynchronize(s->stream), "fresh initialisation");
+    return PFB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+pfb_sim3d* pfb_sim3d_create(const pfb_params3d* p, const pfb_vec3* centres, int device) {
+    clear_error();
+    if (!p || !centres) {
+        set_error(PFB_E_ARG, "null params or centres");
+        return nullptr;
+    }
+    pfb_sim3d* s = new (std::nothrow) pfb_sim3d();
+    if (!s) {
+        set_error(PFB_E_NOMEM, "host allocation failed");
+        return nullptr;
+    }
+    if (create_impl(s, p, centres, device) != PFB_OK) {
+        delete s;
+        return nullptr;
+    }
+    return s;
+}
+
+void pfb_sim3d_destroy(pfb_sim3d* s) { delete s; }
+
+int pfb_sim3d_advance(pfb_sim3d* s, int steps) {
+    if (!s || steps < 0) return set_error(PFB_E_ARG, "invalid advance arguments");
+    PFB3_CU(cudaSetDevice(s->device), "cudaSetDevice");
+    for (int i = 0; i < steps; ++i) PFB3_RC(one_step(s));
+    return PFB_OK;
+}
+
+int pfb_sim3d_sync(pfb_sim3d* s) {
+    if (!s) return set_error(PFB_E_ARG, "null sim");
+    PFB3_CU(cudaStreamSynchronize(s->stream), "sync");
+    return PFB_OK;
+}
+
+int pfb_sim3d_brick(const pfb_sim3d* s) { return s ? s->B : -1; }
+
+long long pfb_sim3d_step(const pfb_sim3d* s) {
+    if (!s) return -1;
+    uint64_t v = 0;
+    if (cudaMemcpy(&v, s->d_step, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+    return (long long)v;
+}
+
+int pfb_sim3d_get_cells(pfb_sim3d* s, pfb_cell3d* out) {
+    if (!s || !out) return set_error(PFB_E_ARG, "null argument");
+    PFB3_CU(cudaStreamSynchronize(s->stream), "sync");
+    PFB3_CU(cudaMemcpy(out, s->d_cells, (size_t)s->N * sizeof(pfb_cell3d), cudaMemcpyDeviceToHost),
+            "copy cells");
+    return PFB_OK;
+}
+
+int pfb_sim3d_get_phi(pfb_sim3d* s, float* out) {
+    if (!s || !out) return set_error(PFB_E_ARG, "null argument");
+    PFB3_CU(cudaStreamSynchronize(s->stream), "sync");
+    PFB3_CU(cudaMemcpy(out, s->d_phi[s->cur_phi], (size_t)s->N * s->cell_words * sizeof(float),
+                       cudaMemcpyDeviceToHost),
+            "copy phi");
+    return PFB_OK;
+}
+
+int pfb_sim3d_get_S(pfb_sim3d* s, uint32_t* out) {
+    if (!s || !out) return set_error(PFB_E_ARG, "null argument");
+    PFB3_CU(cudaStreamSynchronize(s->stream), "sync");
+    PFB3_CU(cudaMemcpy(out, s->d_S[s->cur_S], s->s_words * sizeof(uint32_t), cudaMemcpyDeviceToHost),
+            "copy S");
+    return PFB_OK;
+}
+
+int pfb_sim3d_get_flags(pfb_sim3d* s, uint32_t* out10) {
+    if (!s || !out10) return set_error(PFB_E_ARG, "null argument");
+    PFB3_CU(cudaStreamSynchronize(s->stream), "sync");
+    PFB3_CU(cudaMemcpy(out10, s->d_flags, PFB3D_FLAG_COUNT * sizeof(uint32_t), cudaMemcpyDeviceToHost),
+            "copy flags");
+    return PFB_OK;
+}
+
+int pfb_sim3d_layout(const pfb_sim3d* s, pfb_layout3d* out) {
+    if (!s || !out) return set_error(PFB_E_ARG, "null argument");
+    *out = s->L;
+    return PFB_OK;
+}
+
+int pfb_sim3d_update_args(pfb_sim3d* s, pfb_update_args3d* out) {
+    if (!s || !out) return set_error(PFB_E_ARG, "null argument");
+    *out = update_args(s);
+    return PFB_OK;
+}
+
+int pfb_sim3d_measure_args(pfb_sim3d* s, pfb_measure_args3d* out) {
+    if (!s || !out) return set_error(PFB_E_ARG, "null argument");
+    const bool full = s->p.full_moment_every > 0 && s->steps_done % s->p.full_moment_every == 0;
+    *out = measure_args(s, true, full);
+    return PFB_OK;
+}
+
+void* pfb_sim3d_stream(const pfb_sim3d* s) { return s ? (void*)s->stream : nullptr; }
+
+int pfb_sim3d_bench(pfb_sim3d* s, int warmup, int steps, double* ms) {
+    if (!s || warmup < 0 || steps <= 0 || !ms) return set_error(PFB_E_ARG, "invalid bench arguments");
+    PFB3_CU(cudaSetDevice(s->device), "cudaSetDevice");
+    for (int i = 0; i < warmup; ++i) PFB3_RC(one_step(s));
+    cudaEvent_t e0, e1;
+    PFB3_CU(cudaEventCreate(&e0), "event");
+    PFB3_CU(cudaEventCreate(&e1), "event");
+    PFB3_CU(cudaStreamSynchronize(s->stream), "sync");
+    PFB3_CU(cudaEventRecord(e0, s->stream), "record");
+    for (int i = 0; i < steps; ++i) PFB3_RC(one_step(s));
+    PFB3_CU(cudaEventRecord(e1, s->stream), "record");
+    PFB3_CU(cudaEventSynchronize(e1), "sync");
+    float t = 0.0f;
+    PFB3_CU(cudaEventElapsedTime(&t, e0, e1), "elapsed");
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = (double)t;
+    return PFB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,201 @@
+"""Python face of the 3D host driver (the reference's ``Sim3D`` step
+sequence, reference src/pf3d/sim.cu:1460-1651) over the C ABI of
+``include/pfb200_3d.h``. Parameter defaults are the reference's
+``SimParams3D`` defaults (reference include/pf3d/params.cuh:257-300)."""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, fields
+
+import numpy as np
+
+from ._abi import check, lib, ptr
+from ._abi3d import (BOUNDARY_HARD_WALL_CHANNEL, BOUNDARY_PERIODIC_XYZ,
+                     BOUNDARY_SUBSTRATE_SLAB, CELL3D_DTYPE, FLAG3D_COUNT, FLAG3D_NAMES, Layout3D,
+                     MeasureArgs3D, Params3D, UpdateArgs3D)
+
+GEOMETRIES = {"periodic": BOUNDARY_PERIODIC_XYZ, "slab": BOUNDARY_SUBSTRATE_SLAB,
+              "channel": BOUNDARY_HARD_WALL_CHANNEL}
+
+
+@dataclass
+class SimParams3D:
+    """Model and run parameters of the 3D driver (reference SimParams3D)."""
+
+    Nx: int = 0
+    Ny: int = 0
+    Nz: int = 0
+    geometry: str = "periodic"
+    num_cells: int = 288
+    B: int = 0  # 0: automatic brick edge
+    dt: float = 0.01
+    lambda_: float = 7.0
+    target_radius: float = 49.0
+    kappa: float = 10.0
+    mu: float = 1.0
+    xi: float = 1500.0
+    tau: float = 1.0e4
+    v_A: float = 1.0e-2
+    gamma: float = 1.0
+    v_A_sigma: float = 0.0
+    aging_time: float = 0.0
+    wall_kappa: float = 0.0
+    wall_width: float = 0.0
+    channel_height: int = 0
+    channel_padding: int = 0
+    seed: int = 1234
+    polarity_seed: int = 0
+    full_moment_every: int = 100
+
+    def to_c(self) -> Params3D:
+        p = Params3D()
+        for f in fields(self):
+            if f.name == "geometry":
+                p.boundary_flags = GEOMETRIES[self.geometry]
+            else:
+                setattr(p, f.name, getattr(self, f.name))
+        return p
+
+    @property
+    def boundary_flags(self) -> int:
+        return GEOMETRIES[self.geometry]
+
+    @property
+    def volume0(self) -> float:
+        v = 4.0 * math.pi * self.target_radius ** 3 / 3.0
+        return 0.5 * v if self.geometry == "slab" else v
+
+    def brick(self) -> int:
+        return self.B or automatic_brick_edge(self.target_radius, self.lambda_)
+
+
+def automatic_brick_edge(radius: float, lam: float) -> int:
+    return int(lib().pfb3d_automatic_brick_edge(radius, lam))
+
+
+def calibrate_seed_radius(radius: float, lam: float, edge: int) -> tuple[float, float]:
+    s, v = C.c_double(), C.c_double()
+    check(lib().pfb3d_calibrate_seed_radius(radius, lam, edge, C.byref(s), C.byref(v)),
+          "calibrate_seed_radius")
+    return s.value, v.value
+
+
+def domain_side_for(n: int, radius: float, rho: float) -> int:
+    """Periodic cube side holding n spheres at volume fraction rho
+    (reference include/pf3d/params.cuh:214-223)."""
+    return int(math.ceil(((n * 4.0 * math.pi * radius ** 3 / 3.0) / rho) ** (1.0 / 3.0)))
+
+
+def sequential_centres(n: int, side: float, min_sep: float, seed: int, *, height: float = 0.0,
+                       z_margin: float = 0.0, planar_z: float | None = None,
+                       max_tries: int = 1_000_000) -> np.ndarray:
+    """Seeded random sequential placement with a minimum periodic separation
+    (periodic in x, y; in z too unless `height` bounds it). Returns (n, 3)."""
+    rng = np.random.default_rng(seed)
+    out = np.zeros((n, 3))
+    k = 0
+    tries = 0
+    while k < n:
+        tries += 1
+        if tries > max_tries:
+            raise RuntimeError(f"placed only {k} of {n} centres")
+        c = rng.random(3) * side
+        if planar_z is not None:
+            c[2] = planar_z
+        elif height > 0.0:
+            c[2] = z_margin + rng.random() * (height - 2.0 * z_margin)
+        if k:
+            d = out[:k] - c
+            d[:, :2] -= side * np.round(d[:, :2] / side)
+            if planar_z is None and height <= 0.0:
+                d[:, 2] -= side * np.round(d[:, 2] / side)
+            if np.min(np.einsum("ij,ij->i", d, d)) < min_sep * min_sep:
+                continue
+        out[k] = c
+        k += 1
+    return out
+
+
+def flags_report3(flags: np.ndarray) -> dict[str, int]:
+    return {FLAG3D_NAMES[i]: int(flags[i]) for i in range(FLAG3D_COUNT) if flags[i]}
+
+
+class Sim3D:
+    """Device-resident 3D simulation driven through the C ABI."""
+
+    def __init__(self, params: SimParams3D, centres: np.ndarray, *, device: int = 0):
+        self.params = params
+        self._pc = params.to_c()
+        c = np.ascontiguousarray(centres, dtype=np.float64)
+        assert c.shape == (params.num_cells, 3)
+        h = lib().pfb_sim3d_create(C.byref(self._pc), ptr(c), device)
+        if not h:
+            raise RuntimeError("pfb_sim3d_create failed: " + lib().pfb_last_error().decode())
+        self._h = h
+        lay = Layout3D()
+        check(lib().pfb_sim3d_layout(h, C.byref(lay)), "layout")
+        self.layout = lay
+        self.B = int(lib().pfb_sim3d_brick(h))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().pfb_sim3d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover - interpreter teardown order
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def advance(self, steps: int) -> None:
+        check(lib().pfb_sim3d_advance(self._h, steps), "advance")
+
+    def sync(self) -> None:
+        check(lib().pfb_sim3d_sync(self._h), "sync")
+
+    def bench(self, warmup: int, steps: int) -> float:
+        ms = C.c_double()
+        check(lib().pfb_sim3d_bench(self._h, warmup, steps, C.byref(ms)), "bench")
+        return ms.value
+
+    @property
+    def step(self) -> int:
+        return int(lib().pfb_sim3d_step(self._h))
+
+    @property
+    def stream(self) -> int:
+        return int(lib().pfb_sim3d_stream(self._h) or 0)
+
+    def cells(self) -> np.ndarray:
+        out = np.zeros(self.params.num_cells, CELL3D_DTYPE)
+        check(lib().pfb_sim3d_get_cells(self._h, ptr(out)), "get_cells")
+        return out
+
+    def phi(self) -> np.ndarray:
+        B = self.B
+        out = np.zeros((self.params.num_cells, B, B, B), np.float32)
+        check(lib().pfb_sim3d_get_phi(self._h, ptr(out)), "get_phi")
+        return out
+
+    def S(self) -> np.ndarray:
+        L = self.layout
+        out = np.zeros((L.nz, L.ny, L.pitch_x), np.uint32)
+        check(lib().pfb_sim3d_get_S(self._h, ptr(out)), "get_S")
+        return out
+
+    def flags(self) -> np.ndarray:
+        out = np.zeros(FLAG3D_COUNT, np.uint32)
+        check(lib().pfb_sim3d_get_flags(self._h, ptr(out)), "get_flags")
+        return out
+
+    def update_args(self) -> UpdateArgs3D:
+        a = UpdateArgs3D()
+        check(lib().pfb_sim3d_update_args(self._h, C.byref(a)), "update_args")
+        return a
+
+    def measure_args(self) -> MeasureArgs3D:
+        a = MeasureArgs3D()
+        check(lib().pfb_sim3d_measure_args(self._h, C.byref(a)), "measure_args")
+        return a

@@ -10,19 +10,23 @@ import numpy as np
 import pfb200
 from pfb200._abi import CELL_DTYPE, Cell2D, Params2D, StepArgs2D, TrajCell2D
 
-HEADER = Path(__file__).resolve().parent.parent / "include" / "pfb200.h"
+INCLUDE = Path(__file__).resolve().parent.parent / "include"
+HEADERS = sorted(INCLUDE.glob("*.h"))
 
 
-def declared_functions(path=HEADER):
-    text = re.sub(r"/\*.*?\*/", "", path.read_text(), flags=re.S)
-    names = re.findall(r"\b(pfb_[a-z0-9_]+)\s*\(", text)
-    return sorted(set(names))
+def declared_functions(paths=HEADERS):
+    names = set()
+    for path in paths:
+        text = re.sub(r"/\*.*?\*/", "", path.read_text(), flags=re.S)
+        names.update(re.findall(r"\b(pfb[0-9a-z_]*_[a-z0-9_]+)\s*\(", text))
+    return sorted(names)
 
 
 def test_header_declares_entry_points():
     names = declared_functions()
     assert "pfb_step2d_launch" in names and "pfb_sim2d_create" in names
-    assert len(names) >= 40
+    assert "pfb3d_update" in names and "pfb_sim3d_create" in names
+    assert len(names) >= 70
 
 
 def test_library_exports_every_declared_symbol():
@@ -84,3 +88,37 @@ def test_coefficients_match_reference_defaults():
     assert a.mot_coeff == np.float32((600.0 / 49.0) / 1500.0)
     assert a.p_tumble == -np.expm1(-0.01 / 1e4)
     assert a.polarity_seed == 1234
+
+
+def test_3d_record_layouts():
+    # reference include/pf3d/kernels.cuh:132-137 static_asserts and the
+    # measured offsets of MeasureArgs3D / UpdateArgs3D
+    from pfb200._abi3d import (Cell3D, InitArgs3D, MeasureArgs3D, ScatterArgs3D,
+                               UpdateArgs3D)
+    assert C.sizeof(Cell3D) == 256 and Cell3D.storage_edge.offset == 192
+    assert Cell3D.V.offset == 128 and Cell3D.pending_shift_x.offset == 112
+    assert C.sizeof(MeasureArgs3D) == 168 and MeasureArgs3D.apply_tumble.offset == 140
+    assert MeasureArgs3D.selection.offset == 144 and MeasureArgs3D.storage.offset == 160
+    assert C.sizeof(UpdateArgs3D) == 208 and UpdateArgs3D.tile_pass.offset == 152
+    assert UpdateArgs3D.exchange_region.offset == 156 and UpdateArgs3D.storage.offset == 200
+    assert C.sizeof(InitArgs3D) == 72 and C.sizeof(ScatterArgs3D) == 88
+
+
+def test_3d_launchers_reject_bad_arguments_without_touching_a_device():
+    from pfb200._abi3d import MeasureArgs3D, UpdateArgs3D
+    L = pfb200.lib()
+    assert L.pfb3d_update(None, None) == -1
+    u = UpdateArgs3D()
+    assert L.pfb3d_update(C.byref(u), None) < 0
+    u.B, u.N = 64, 4
+    u.layout.nx = u.layout.ny = u.layout.nz = 256
+    u.layout.pitch_x = 256
+    u.layout.boundary_flags = 0x7
+    assert L.pfb3d_update(C.byref(u), None) == -1  # null buffers
+    u.tile_pass = 1
+    assert L.pfb3d_update(C.byref(u), None) == -3  # boundary-first pass unsupported
+    m = MeasureArgs3D()
+    m.B, m.N = 64, 4
+    m.layout = u.layout
+    m.storage.z_cap = 8
+    assert L.pfb3d_measure_cells_only(C.byref(m), None) == -3  # compact storage
