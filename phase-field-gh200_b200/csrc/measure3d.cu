@@ -112,8 +112,15 @@ __global__ void __launch_bounds__(kThreads3, 2) k_measure3d(const __grid_constan
         ring.issue(k, field, src);
     };
     const int nreq = PB + 2;
-    for (int k = 0; k < kMeasureRing && k < nreq; ++k) issue(k);
+    int issued = 0;
+    for (int k = 0; k < kMeasureRing && k < nreq; ++k, ++issued) issue(k);
     __syncthreads();
+    // the first two planes are read from iteration 0 on; later ones are
+    // waited for one iteration before their first read
+    if (!ring.wait(0) || !ring.wait(1)) {
+        H.abort = 1;
+        atomicOr(&g_measure3d_status, 1u);
+    }
 
     Acc3 acc;
     acc.lox = acc.loy = acc.loz = B;
@@ -206,8 +213,17 @@ __global__ void __launch_bounds__(kThreads3, 2) k_measure3d(const __grid_constan
             }
         }
         __syncthreads();
-        if (i + kMeasureRing < nreq) issue(i + kMeasureRing);
+        // after a timed-out wait nothing more is issued into the ring
+        if (!H.abort && i + kMeasureRing < nreq) {
+            issue(i + kMeasureRing);
+            ++issued;
+        }
     }
+
+    // no bulk copy may still target this CTA's shared memory at exit
+    if (H.abort)
+        for (int k = issued > kMeasureRing ? issued - kMeasureRing : 0; k < issued; ++k)
+            ring.wait(k);
 
     // ---- flags: one counted raise per CTA and flag
     c_nonfinite = __reduce_add_sync(0xFFFFFFFFu, c_nonfinite);

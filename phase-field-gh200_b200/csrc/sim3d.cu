@@ -330,6 +330,8 @@ int pfb_sim3d_brick(const pfb_sim3d* s) { return s ? s->B : -1; }
 long long pfb_sim3d_step(const pfb_sim3d* s) {
     if (!s) return -1;
     uint64_t v = 0;
+    // the driver's stream does not order with the legacy stream: finish it first
+    if (cudaStreamSynchronize(s->stream) != cudaSuccess) return -1;
     if (cudaMemcpy(&v, s->d_step, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
     return (long long)v;
 }

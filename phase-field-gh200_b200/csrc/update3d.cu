@@ -189,8 +189,15 @@ __global__ void __launch_bounds__(kUThreads, 2) k_update3d(const __grid_constant
         ring.issue(kq, src, s);
     };
     const int nreq = PB + 2;
-    for (int kq = 0; kq < kURing && kq < nreq; ++kq) issue(kq);
+    int issued = 0;
+    for (int kq = 0; kq < kURing && kq < nreq; ++kq, ++issued) issue(kq);
     __syncthreads();
+    // the first two planes are read from iteration 0 on; later ones are
+    // waited for one iteration before their first read
+    if (!ring.wait(0) || !ring.wait(1)) {
+        H.abort = 1;
+        atomicOr(&g_update3d_status, 1u);
+    }
 
     unsigned cnt_nf = 0, cnt_neg = 0, cnt_top = 0, cnt_clamp = 0, cnt_ovf = 0;
     const int strips = B / 4;
@@ -312,8 +319,16 @@ __global__ void __launch_bounds__(kUThreads, 2) k_update3d(const __grid_constant
             for (int j = 0; j < 4; ++j) cnt_ovf += old_prev[j] > 0xFFFFFFFFu - q_prev[j] ? 1u : 0u;
         }
         __syncthreads();
-        if (i + kURing < nreq) issue(i + kURing);
+        // after a timed-out wait nothing more is issued into the ring
+        if (!H.abort && i + kURing < nreq) {
+            issue(i + kURing);
+            ++issued;
+        }
     }
+
+    // no bulk copy may still target this CTA's shared memory at exit
+    if (H.abort)
+        for (int kq = issued > kURing ? issued - kURing : 0; kq < issued; ++kq) ring.wait(kq);
 
     // ---- source voxels whose destination falls outside the brick: no write,
     // but a supported value is a DESTINATION_CLIP (rank 0 of the cell walks

@@ -89,12 +89,19 @@ def domain_side_for(n: int, radius: float, rho: float) -> int:
 
 def sequential_centres(n: int, side: float, min_sep: float, seed: int, *, height: float = 0.0,
                        z_margin: float = 0.0, planar_z: float | None = None,
+                       first_at_centre: bool = False,
                        max_tries: int = 1_000_000) -> np.ndarray:
     """Seeded random sequential placement with a minimum periodic separation
-    (periodic in x, y; in z too unless `height` bounds it). Returns (n, 3)."""
+    (periodic in x, y; in z too unless `height` bounds it). Returns (n, 3).
+    first_at_centre puts cell 0 at the box centre, the convention of the
+    reference's periodic initialiser and centre tables
+    (reference include/pf3d/palmieri_initializer.hpp:149-154)."""
     rng = np.random.default_rng(seed)
     out = np.zeros((n, 3))
     k = 0
+    if first_at_centre and n:
+        out[0] = 0.5 * side
+        k = 1
     tries = 0
     while k < n:
         tries += 1
