@@ -148,7 +148,17 @@ __global__ void __launch_bounds__(kThreads3, 2) k_measure3d(const __grid_constan
                 float rs[6], rc[6], rn[6];
                 load_row6(pc, B, y0 - 1, x0, rs);
                 load_row6(pc, B, y0, x0, rc);
-                const int wx0 = wrap_offset(ox, x0, L.nx);
+                int wxj[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) wxj[j] = wrap_offset(ox, x0 + j, L.nx);
+                // aggregate words of a row, fetched one row ahead
+                auto load_agg = [&](int y, uint32_t* out) {
+                    const size_t srow = s_index(L, 0, wrap_offset(oy, y, L.ny), wz);
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) out[j] = __ldg(A.S + srow + wxj[j]);
+                };
+                uint32_t agg_next[4];
+                load_agg(y0, agg_next);
 #pragma unroll 1
                 for (int r = 0; r < 4; ++r) {
                     const int y = y0 + r;
@@ -157,44 +167,36 @@ __global__ void __launch_bounds__(kThreads3, 2) k_measure3d(const __grid_constan
                     const float4 zp = *reinterpret_cast<const float4*>(pp + y * B + x0);
                     const float zmv[4] = {zm.x, zm.y, zm.z, zm.w};
                     const float zpv[4] = {zp.x, zp.y, zp.z, zp.w};
-                    const int wy = wrap_offset(oy, y, L.ny);
-                    const size_t srow = s_index(L, 0, wy, wz);
+                    uint32_t agg[4];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) agg[j] = agg_next[j];
+                    if (r < 3) load_agg(y + 1, agg_next);
+                    double rV = 0.0, rX = 0.0;
 #pragma unroll
                     for (int j = 0; j < 4; ++j) {
                         const float c = rc[j + 1];
-                        if (!isfinite(c)) {
-                            ++c_nonfinite;
-                            continue;
-                        }
-                        const int x = x0 + j;
+                        const bool cfin = isfinite(c);
+                        c_nonfinite += cfin ? 0u : 1u;
                         const float gx = 0.5f * (rc[j + 2] - rc[j]);
                         const float gy = 0.5f * (rn[j + 1] - rs[j + 1]);
                         const float gz = 0.5f * (zpv[j] - zmv[j]);
-                        float other = 0.0f;
-                        if (c != 0.0f) {
-                            int wx = wx0 + j;
-                            if (wx >= L.nx) wx -= L.nx;
-                            const uint32_t agg = __ldg(A.S + srow + wx);
-                            const uint32_t own = q_of3(c);
-                            if (agg >= own) {
-                                other = (float)(agg - own) * kQInv;
-                            } else {
-                                ++c_negative;
-                            }
-                        }
+                        const uint32_t own = q_of3(c);
+                        const bool nz = cfin && c != 0.0f;
+                        const bool neg = nz && agg[j] < own;
+                        c_negative += neg ? 1u : 0u;
+                        float other = (nz && !neg) ? (float)(agg[j] - own) * kQInv : 0.0f;
                         if (wall) other += wallv;
-                        const double sq = (double)c * (double)c;
-                        acc.V += sq;
-                        acc.Cx += sq * (double)x;
-                        acc.Cy += sq * (double)y;
-                        acc.Cz += sq * (double)z;
-                        if (A.compute_surface)
+                        const double sq = cfin ? (double)c * (double)c : 0.0;
+                        rV += sq;
+                        rX += sq * (double)j;
+                        if (A.compute_surface && cfin)
                             acc.Sf += sqrt((double)gx * gx + (double)gy * gy + (double)gz * gz);
-                        acc.Ix += (double)(c * gx * other);
-                        acc.Iy += (double)(c * gy * other);
-                        acc.Iz += (double)(c * gz * other);
-                        acc.pmax = max(acc.pmax, __float_as_uint(fabsf(c)));
-                        if (fabsf(c) > kSupportEps3) {
+                        acc.Ix += cfin ? (double)(c * gx * other) : 0.0;
+                        acc.Iy += cfin ? (double)(c * gy * other) : 0.0;
+                        acc.Iz += cfin ? (double)(c * gz * other) : 0.0;
+                        if (cfin) acc.pmax = max(acc.pmax, __float_as_uint(fabsf(c)));
+                        const int x = x0 + j;
+                        if (cfin && fabsf(c) > kSupportEps3) {
                             if (top_plane) ++c_top;
                             acc.lox = min(acc.lox, x);
                             acc.hix = max(acc.hix, x);
@@ -204,6 +206,10 @@ __global__ void __launch_bounds__(kThreads3, 2) k_measure3d(const __grid_constan
                             acc.hiz = max(acc.hiz, z);
                         }
                     }
+                    acc.V += rV;
+                    acc.Cx += rV * (double)x0 + rX;
+                    acc.Cy += rV * (double)y;
+                    acc.Cz += rV * (double)z;
 #pragma unroll
                     for (int c = 0; c < 6; ++c) {
                         rs[c] = rc[c];

@@ -106,6 +106,55 @@ __device__ __forceinline__ void stencil27w(const float (&w)[3][3][6], int j, flo
     gz = 0.5f * (w[2][1][j + 1] - w[0][1][j + 1]);
 }
 
+// row6 with the alignment decision taken once per strip
+__device__ __forceinline__ void row6v(const float* plane, int B, int ys, int xs0, bool vec_ok,
+                                      float* v) {
+    if ((unsigned)ys >= (unsigned)B) {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) v[c] = 0.0f;
+        return;
+    }
+    const float* row = plane + ys * B;
+    if (vec_ok) {
+        const float4 m = *reinterpret_cast<const float4*>(row + xs0);
+        v[0] = xs0 > 0 ? row[xs0 - 1] : 0.0f;
+        v[1] = m.x;
+        v[2] = m.y;
+        v[3] = m.z;
+        v[4] = m.w;
+        v[5] = xs0 + 4 < B ? row[xs0 + 4] : 0.0f;
+    } else {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            const int x = xs0 - 1 + c;
+            v[c] = (unsigned)x < (unsigned)B ? row[x] : 0.0f;
+        }
+    }
+}
+
+// stencil27w over a window whose rows rotate through slots: row offset -1,
+// 0, +1 of every plane live in slots s0, s1, s2.
+__device__ __forceinline__ void stencil27r(const float (&w)[3][3][6], int s0, int s1, int s2,
+                                           int j, float& lap, float& gx, float& gy, float& gz) {
+    const int sl[3] = {s0, s1, s2};
+    float acc = (float)kWCentre * w[1][s1][j + 1];
+#pragma unroll
+    for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+        for (int dy = 0; dy < 3; ++dy)
+#pragma unroll
+            for (int dx = 0; dx < 3; ++dx) {
+                const int d = (dz != 1) + (dy != 1) + (dx != 1);
+                if (d == 0) continue;
+                const int wgt = d == 1 ? kWFace : d == 2 ? kWEdge : kWCorner;
+                acc += (float)wgt * w[dz][sl[dy]][j + dx];
+            }
+    lap = acc * (float)(1.0 / 30.0);
+    gx = 0.5f * (w[1][s1][j + 2] - w[1][s1][j]);
+    gy = 0.5f * (w[1][s2][j + 1] - w[1][s0][j + 1]);
+    gz = 0.5f * (w[2][s1][j + 1] - w[0][s1][j + 1]);
+}
+
 struct CellCoef {
     float gamma, bulk, volume, inter, vx, vy, vz, dt;
 };
@@ -229,11 +278,12 @@ __global__ void __launch_bounds__(kUThreads, 2) k_update3d(const __grid_constant
                 continue;
             }
             const int xs0 = x0 + sx;
+            const bool vec_ok = (xs0 & 3) == 0 && xs0 >= 0 && xs0 + 4 <= B;
             float w[3][3][6];
 #pragma unroll
             for (int p = 0; p < 3; ++p) {
-                row6(pl[p], B, y0 + sy - 1, xs0, w[p][0]);
-                row6(pl[p], B, y0 + sy, xs0, w[p][1]);
+                row6v(pl[p], B, y0 + sy - 1, xs0, vec_ok, w[p][0]);
+                row6v(pl[p], B, y0 + sy, xs0, vec_ok, w[p][1]);
             }
             // world x of the four source columns (wrapped), or -1 outside
             int wxj[4];
@@ -252,11 +302,11 @@ __global__ void __launch_bounds__(kUThreads, 2) k_update3d(const __grid_constant
             };
             load_agg(y0 + sy, agg_next);
             uint32_t old_prev[4] = {0u, 0u, 0u, 0u}, q_prev[4] = {0u, 0u, 0u, 0u};
-#pragma unroll 1
+#pragma unroll
             for (int r = 0; r < 4; ++r) {
                 const int ys = y0 + r + sy;
 #pragma unroll
-                for (int p = 0; p < 3; ++p) row6(pl[p], B, ys + 1, xs0, w[p][2]);
+                for (int p = 0; p < 3; ++p) row6v(pl[p], B, ys + 1, xs0, vec_ok, w[p][(r + 2) % 3]);
                 uint32_t agg[4];
 #pragma unroll
                 for (int j = 0; j < 4; ++j) agg[j] = agg_next[j];
@@ -265,55 +315,42 @@ __global__ void __launch_bounds__(kUThreads, 2) k_update3d(const __grid_constant
                 const size_t srow = yin ? s_index(L, 0, wrap_offset(oy, ys, L.ny), wz) : 0;
 #pragma unroll
                 for (int j = 0; j < 4; ++j) cnt_ovf += old_prev[j] > 0xFFFFFFFFu - q_prev[j] ? 1u : 0u;
+                // rows r-1, r, r+1 of the window sit in slots (r+0..2) % 3
+                const int s0 = r % 3, s1 = (r + 1) % 3, s2 = (r + 2) % 3;
+                // the four stencils are independent chains: computed without
+                // branches so the scheduler can interleave them
+                float lap[4], gx[4], gy[4], gz[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) stencil27r(w, s0, s1, s2, j, lap[j], gx[j], gy[j], gz[j]);
                 float out[4];
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
-                    out[j] = 0.0f;
+                    const bool present = yin && wxj[j] >= 0;
+                    const float c = w[1][s1][j + 1];
+                    const bool cfin = isfinite(c);
+                    const uint32_t own = q_of3(c);
+                    const bool neg = agg[j] < own;
+                    float other = neg ? 0.0f : (float)(agg[j] - own) * kQInv;
+                    if (GEO == 2) other += wallv;
+                    const float next = c + k.dt * rhs3(k, c, lap[j], gx[j], gy[j], gz[j], other);
+                    const bool nfin = isfinite(next);
+                    const bool top = GEO == 1 && top_plane && fabsf(next) > kSupportEps3;
+                    cnt_nf += (present && (!cfin || !nfin)) ? 1u : 0u;
+                    cnt_neg += (present && cfin && neg) ? 1u : 0u;
+                    cnt_top += (present && cfin && nfin && top) ? 1u : 0u;
+                    const bool keep = present && cfin && nfin && !top;
+                    out[j] = keep ? next : 0.0f;
                     q_prev[j] = 0u;
                     old_prev[j] = 0u;
-                    if (!yin || wxj[j] < 0) continue;  // source voxel absent
-                    const float c = w[1][1][j + 1];
-                    if (!isfinite(c)) {
-                        ++cnt_nf;
-                        continue;
-                    }
-                    float lap, gx, gy, gz;
-                    stencil27w(w, j, lap, gx, gy, gz);
-                    const uint32_t own = q_of3(c);
-                    float other;
-                    if (agg[j] >= own) {
-                        other = (float)(agg[j] - own) * kQInv;
-                    } else {
-                        other = 0.0f;
-                        ++cnt_neg;
-                    }
-                    if (GEO == 2) other += wallv;
-                    const float next = c + k.dt * rhs3(k, c, lap, gx, gy, gz, other);
-                    if (!isfinite(next)) {
-                        ++cnt_nf;
-                        continue;
-                    }
-                    if (GEO == 1 && top_plane && fabsf(next) > kSupportEps3) {
-                        ++cnt_top;
-                        continue;
-                    }
-                    out[j] = next;
                     if (has_out) {
-                        if (next * next > kQClamp3) ++cnt_clamp;
-                        const uint32_t qv = q_of3(next);
+                        cnt_clamp += (keep && next * next > kQClamp3) ? 1u : 0u;
+                        const uint32_t qv = keep ? q_of3(next) : 0u;
                         q_prev[j] = qv;
-                        old_prev[j] = dev::atom_add_nonzero(A.S_out + srow + wxj[j], qv);
+                        old_prev[j] = dev::atom_add_nonzero(A.S_out + srow + (keep ? wxj[j] : 0), qv);
                     }
                 }
                 __stcs(reinterpret_cast<float4*>(orow + r * B),
                        make_float4(out[0], out[1], out[2], out[3]));
-#pragma unroll
-                for (int p = 0; p < 3; ++p)
-#pragma unroll
-                    for (int c = 0; c < 6; ++c) {
-                        w[p][0][c] = w[p][1][c];
-                        w[p][1][c] = w[p][2][c];
-                    }
             }
 #pragma unroll
             for (int j = 0; j < 4; ++j) cnt_ovf += old_prev[j] > 0xFFFFFFFFu - q_prev[j] ? 1u : 0u;
@@ -331,18 +368,20 @@ __global__ void __launch_bounds__(kUThreads, 2) k_update3d(const __grid_constant
         for (int kq = issued > kURing ? issued - kURing : 0; kq < issued; ++kq) ring.wait(kq);
 
     // ---- source voxels whose destination falls outside the brick: no write,
-    // but a supported value is a DESTINATION_CLIP (rank 0 of the cell walks
-    // the clipped set from global memory; shifts are rare).
+    // but a supported value is a DESTINATION_CLIP. Every CTA of the cell
+    // checks the source planes of its own z range (from global memory;
+    // shifts are rare).
     unsigned cnt_clip = 0;
-    if (part == 0 && (sx | sy | sz) != 0 && !H.abort) {
+    if ((sx | sy | sz) != 0 && !H.abort) {
         auto f = [&](int x, int y, int z) -> float {
             if ((unsigned)x >= (unsigned)B || (unsigned)y >= (unsigned)B) return 0.0f;
             int s;
             if (!fetch_plane(L, oz, z, B, &s)) return 0.0f;
             return src[((size_t)s * B + y) * B + x];
         };
-        for (size_t q = tid; q < words; q += kUThreads) {
-            const int x = (int)(q % B), y = (int)((q / B) % B), z = (int)(q / ((size_t)B * B));
+        const size_t plane = (size_t)B * B;
+        for (size_t q = (size_t)d0 * plane + tid; q < (size_t)d1 * plane; q += kUThreads) {
+            const int x = (int)(q % B), y = (int)((q / B) % B), z = (int)(q / plane);
             if ((unsigned)(x - sx) < (unsigned)B && (unsigned)(y - sy) < (unsigned)B &&
                 (unsigned)(z - sz) < (unsigned)B)
                 continue;
