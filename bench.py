@@ -256,6 +256,147 @@ def _fresh_cells(p):
     return cells
 
 
+# ---------------------------------------------------------------------------
+# 3D workload (--workload c3): periodic 256^3, 512 cells R = 10, B = 64
+# ---------------------------------------------------------------------------
+WORKLOAD3D = ("3D periodic 256^3, 512 cells R=10 (V0=4/3 pi R^3), lambda=7, brick B=64 "
+              "(the automatic edge; B=48 is rejected at lambda=7), min-separation 2R sequential "
+              "centres (cell 0 at the box centre), tanh spheres with the calibrated seed radius, "
+              "default coefficients, f32 phi, Q5.27 aggregate")
+
+
+def workload3d(seed: int):
+    import pfb200
+    p = pfb200.SimParams3D(Nx=256, Ny=256, Nz=256, num_cells=512, target_radius=10.0,
+                           lambda_=7.0, B=64, seed=seed)
+    c = pfb200.sequential_centres(512, 256.0, 20.0, seed, first_at_centre=True)
+    return p, c.astype(np.float32).astype(np.float64)
+
+
+def read_ncu_traffic3d():
+    f = REPO / "profiles" / "k_step3d_c3.md"
+    if not f.exists():
+        return None
+    for ln in f.read_text().splitlines():
+        if ln.startswith("dram_bytes_per_step:"):
+            try:
+                return int(float(ln.split(":", 1)[1].split()[0]))
+            except ValueError:
+                return None
+    return None
+
+
+def run_3d(a):
+    """One step = the reference Sim3D sequence (measure, motion, clear,
+    update, repair/finalize/restore/advance); throughput counts the B^3
+    brick of every cell (the reference's window)."""
+    import torch
+    import pfb200
+    rank, world, local = rank_env()
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    p, c = workload3d(1234 + rank)
+    sim = pfb200.Sim3D(p, c, device=local)
+    B, N = sim.B, p.num_cells
+    sites = N * B ** 3
+    alg = sites * 8 + p.Nx * p.Ny * p.Nz * 8
+    ext = torch.cuda.ExternalStream(sim.stream, device=local)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(local)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    sim.advance(a.warmup)
+    sim.sync()
+    barrier()
+    m0 = clocks.mark()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    sim.advance(a.steps)
+    e1.record(ext)
+    sim.sync()
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1), dist, f"cuda:{local}")
+    time.sleep(0.15)
+    m1 = clocks.mark()
+    e2e = None
+    if not a.no_e2e:
+        from pfb200._abi import check, lib
+        cells_out = torch.empty((N, 256), dtype=torch.uint8).pin_memory()
+        barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(ext)
+        for _ in range(a.steps):
+            check(lib().pfb_sim3d_advance(sim._h, 1), "advance")
+            check(lib().pfb_sim3d_get_cells(sim._h, cells_out.data_ptr()), "get_cells")
+        f1.record(ext)
+        sim.sync()
+        barrier()
+        el = max_over_ranks(f0.elapsed_time(f1) / 1000.0, dist, f"cuda:{local}")
+        e2e = {"value": world * sites * a.steps / el, "unit": "site-cell updates/s",
+               "h2d_bytes_per_step": 0, "d2h_bytes_per_step": cells_out.numel(),
+               "steps": a.steps,
+               "note": "state built on the device from host centres at creation; every step "
+                       "reads the 512 cell records back through pfb_sim3d_get_cells"}
+    clocks.stop()
+    flags = sim.flags()
+    if rank == 0:
+        ms_step = ms / a.steps
+        peak, peak_src = read_peak_hbm()
+        achieved = alg / (ms_step / 1000.0) / 1e9
+        cpu = None
+        if world == 1 and a.cpu_steps > 0:
+            cpu = cpu_sample3d(p, sim, threads=0)
+        line = {
+            "metric": "site-cell updates/s", "value": world * sites * a.steps / (ms / 1000.0),
+            "unit": "site-cell updates/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD3D, "L": 256, "cells": N, "radius": 10.0, "B": B,
+                       "sites_per_step": sites,
+                       "l2": "inputs larger than L2: two 537 MB phi pools and two 67 MB "
+                             "aggregate slots; no flush between steps",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": read_ncu_traffic3d(),
+                         "kernel": "pfb::p3::k_measure3d<4> + k_update3d<0> (one step)",
+                         "algorithmic_bytes_per_launch": alg, "peak_source": peak_src,
+                         "duration_source": "CUDA events over the timed region / steps"},
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks.summary(m0, m1),
+            "gpu_launches": a.steps * 10,
+            "flags": pfb200.flags_report3(flags),
+        }
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def cpu_sample3d(p, sim, threads: int):
+    """One full step of the 3D workload on the OpenMP restatement (oracle/)."""
+    sys.path.insert(0, str(REPO / "oracle"))
+    import oracle3d
+    st = oracle3d.OracleState3D(p, sim.layout, sim.B, sim.cells(), sim.phi(), sim.S())
+    n = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    st.advance(1, threads)
+    dt = time.perf_counter() - t0
+    return {"value": p.num_cells * sim.B ** 3 / dt, "unit": "site-cell updates/s", "cores": n,
+            "kind": "port", "sample": f"one full time step of the same 3D workload ({dt:.1f} s) "
+                                      "on the OpenMP restatement of the update"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -267,11 +408,15 @@ def main():
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=int(os.environ.get("PFB_CPU_STEPS", "6")))
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3"],
+                    help="c2: 2D 2048^2 / 1024 cells (default); c3: 3D 256^3 / 512 cells")
     a = ap.parse_args()
     if a.warmup < 3:
         a.warmup = 3
     if a.impl == "reference":
         return run_reference_arm(a)
+    if a.workload == "c3":
+        return run_3d(a)
 
     import torch
     import pfb200
