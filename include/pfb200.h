@@ -324,6 +324,35 @@ int pfb_sim2d_bench(pfb_sim2d* s, int warmup, int steps, double* ms_per_step);
 int pfb_sim2d_step_args(pfb_sim2d* s, pfb_step_args2d* out);
 void* pfb_sim2d_stream(pfb_sim2d* s);
 
+/* ---- batched ensemble (no reference counterpart) --------------------------
+ * R independent 2D systems, each with its own lattice side, cell count,
+ * seeds and buffers, advanced together by ONE kernel launch per step
+ * (k_step2d_batch: system r is served by its own contiguous range of
+ * clusters), six steps per CUDA graph. Each system evolves exactly as it
+ * would alone: the per-cell code is the same kernel body. */
+typedef struct pfb_ens2d pfb_ens2d;
+
+/* params[r], cx[r], cy[r] (params[r].num_cells centres each) describe
+ * system r; every system gets a fresh start as pfb_sim2d_create. */
+pfb_ens2d* pfb_ens2d_create(int R, const pfb_params2d* params, const float* const* cx,
+                            const float* const* cy, int device);
+void pfb_ens2d_destroy(pfb_ens2d* e);
+int pfb_ens2d_num_systems(const pfb_ens2d* e);
+int pfb_ens2d_set_cluster(pfb_ens2d* e, int cluster);
+/* Times `steps` steps with clusters of 2, 4 and 8 CTAs per cell and keeps the
+ * fastest (the ensemble's autotuner; the timed steps advance the systems). */
+int pfb_ens2d_autotune(pfb_ens2d* e, int steps, int* chosen);
+int pfb_ens2d_advance(pfb_ens2d* e, int steps);
+/* The same steps launched one system at a time (the baseline the batched
+ * launch is measured against). */
+int pfb_ens2d_advance_serial(pfb_ens2d* e, int steps);
+int pfb_ens2d_sync(pfb_ens2d* e);
+long long pfb_ens2d_step(const pfb_ens2d* e);
+/* System r as a pfb_sim2d handle owned by the ensemble (after finishing the
+ * ensemble's queued work): use pfb_sim2d_get_* on it; do not destroy it. */
+pfb_sim2d* pfb_ens2d_system(pfb_ens2d* e, int r);
+int pfb_ens2d_bench(pfb_ens2d* e, int warmup, int steps, int serial, double* ms_per_step);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif

@@ -8,6 +8,7 @@
 // CUDA graph of six steps that covers every (parity, slot) pair.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -474,5 +475,268 @@ int pfb_sim2d_step_args(pfb_sim2d* s, pfb_step_args2d* out) {
 }
 
 void* pfb_sim2d_stream(pfb_sim2d* s) { return s ? (void*)s->stream : nullptr; }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched ensemble: R independent 2D systems of any size advanced by one
+// launch per step (k_step2d_batch), six steps per CUDA graph. Each system
+// keeps its own buffers, slots and device step counters (a pfb_sim2d); the
+// ensemble owns the batch argument tables and its stream.
+// ---------------------------------------------------------------------------
+struct pfb_ens2d {
+    std::vector<pfb_sim2d*> sims;
+    std::vector<int> order;  // launch order of the systems (largest first)
+    int device = 0;
+    int cluster = kDefaultCluster;
+    long long steps_done = 0;
+    cudaStream_t stream = nullptr;
+    pfb_step_args2d* d_args = nullptr;  // 6 slots x R records
+    int* d_start = nullptr;             // R + 1 block offsets
+    int total_blocks = 0;
+    bool tables_ready = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+
+    ~pfb_ens2d() {
+        drop_graph();
+        if (stream) cudaStreamDestroy(stream);
+        cudaFree(d_args);
+        cudaFree(d_start);
+        for (pfb_sim2d* s : sims) delete s;
+    }
+
+    int R() const { return (int)sims.size(); }
+
+    void drop_graph() {
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        if (graph) cudaGraphDestroy(graph);
+        graph_exec = nullptr;
+        graph = nullptr;
+    }
+
+    // Argument tables for the six slots and the CTA offsets for `cluster`.
+    int build_tables() {
+        drop_graph();
+        const int R_ = R();
+        std::vector<pfb_step_args2d> h((size_t)6 * R_);
+        std::vector<int> start((size_t)R_ + 1, 0);
+        for (int i = 0; i < R_; ++i) {
+            const pfb_sim2d* s = sims[(size_t)order[(size_t)i]];
+            for (int slot = 0; slot < 6; ++slot) h[(size_t)slot * R_ + i] = s->args_for_slot(slot);
+            start[(size_t)i + 1] = start[(size_t)i] + s->N * cluster;
+        }
+        total_blocks = start[(size_t)R_];
+        if (!d_args) PFB_CU(cudaMalloc(&d_args, h.size() * sizeof(pfb_step_args2d)), "alloc args");
+        if (!d_start) PFB_CU(cudaMalloc(&d_start, start.size() * sizeof(int)), "alloc offsets");
+        PFB_CU(cudaMemcpyAsync(d_args, h.data(), h.size() * sizeof(pfb_step_args2d),
+                               cudaMemcpyHostToDevice, stream), "upload args");
+        PFB_CU(cudaMemcpyAsync(d_start, start.data(), start.size() * sizeof(int),
+                               cudaMemcpyHostToDevice, stream), "upload offsets");
+        PFB_CU(cudaStreamSynchronize(stream), "tables");
+        tables_ready = true;
+        return PFB_OK;
+    }
+
+    int launch_slot(int slot) {
+        return step2d_launch_batch(d_args + (size_t)slot * R(), d_start, R(), total_blocks, cluster,
+                                   stream);
+    }
+
+    int build_graph() {
+        drop_graph();
+        PFB_CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        int rc = PFB_OK;
+        for (int s = 0; s < 6 && rc == PFB_OK; ++s) rc = launch_slot(s);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(stream, &g);
+        if (rc != PFB_OK) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        PFB_CU(e, "end capture");
+        graph = g;
+        PFB_CU(cudaGraphInstantiateWithFlags(&graph_exec, graph, 0), "graph instantiate");
+        return PFB_OK;
+    }
+
+    int advance(long long steps) {
+        if (!tables_ready) {
+            const int rc = build_tables();
+            if (rc) return rc;
+        }
+        while (steps > 0) {
+            if (steps_done % 6 == 0 && steps >= 6) {
+                if (!graph_exec) {
+                    const int rc = build_graph();
+                    if (rc) return rc;
+                }
+                PFB_CU(cudaGraphLaunch(graph_exec, stream), "graph launch");
+                steps_done += 6;
+                steps -= 6;
+            } else {
+                const int rc = launch_slot((int)(steps_done % 6));
+                if (rc) return rc;
+                steps_done += 1;
+                steps -= 1;
+            }
+        }
+        for (pfb_sim2d* s : sims) s->steps_done = steps_done;
+        return PFB_OK;
+    }
+
+    // The same steps with one launch per system (the replicas-one-at-a-time
+    // baseline the batch is measured against).
+    int advance_serial(long long steps) {
+        for (long long k = 0; k < steps; ++k) {
+            const int slot = (int)(steps_done % 6);
+            for (pfb_sim2d* s : sims) {
+                const pfb_step_args2d a = s->args_for_slot(slot);
+                const int rc = step2d_launch_variant(&a, cluster, 0, stream);
+                if (rc) return rc;
+            }
+            ++steps_done;
+        }
+        for (pfb_sim2d* s : sims) s->steps_done = steps_done;
+        return PFB_OK;
+    }
+};
+
+extern "C" {
+
+pfb_ens2d* pfb_ens2d_create(int R, const pfb_params2d* params, const float* const* cx,
+                            const float* const* cy, int device) {
+    clear_error();
+    if (R <= 0 || !params || !cx || !cy) {
+        set_error(PFB_E_ARG, "ensemble needs R > 0 systems with parameters and centres");
+        return nullptr;
+    }
+    pfb_ens2d* e = new (std::nothrow) pfb_ens2d();
+    if (!e) {
+        set_error(PFB_E_NOMEM, "host allocation failed");
+        return nullptr;
+    }
+    e->device = device;
+    for (int r = 0; r < R; ++r) {
+        pfb_sim2d* s = pfb_sim2d_create(&params[r], cx[r], cy[r], device);
+        if (!s) {
+            delete e;
+            return nullptr;
+        }
+        s->use_graph = false;
+        e->sims.push_back(s);
+    }
+    e->order.resize((size_t)R);
+    for (int r = 0; r < R; ++r) e->order[(size_t)r] = r;
+    // largest systems first: their CTAs start in the first wave
+    std::stable_sort(e->order.begin(), e->order.end(),
+                     [e](int a, int b) { return e->sims[(size_t)a]->N > e->sims[(size_t)b]->N; });
+    if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        set_error(PFB_E_CUDA, "stream creation failed");
+        delete e;
+        return nullptr;
+    }
+    return e;
+}
+
+void pfb_ens2d_destroy(pfb_ens2d* e) { delete e; }
+
+int pfb_ens2d_num_systems(const pfb_ens2d* e) { return e ? e->R() : -1; }
+
+int pfb_ens2d_set_cluster(pfb_ens2d* e, int cluster) {
+    if (!e) return set_error(PFB_E_ARG, "null ensemble");
+    if (cluster == 0) cluster = kDefaultCluster;
+    if (cluster != 2 && cluster != 4 && cluster != 8)
+        return set_error(PFB_E_CONFIG, "cluster must be 2, 4 or 8");
+    if (cluster != e->cluster) {
+        e->cluster = cluster;
+        e->tables_ready = false;
+        e->drop_graph();
+    }
+    return PFB_OK;
+}
+
+int pfb_ens2d_advance(pfb_ens2d* e, int steps) {
+    if (!e || steps < 0) return set_error(PFB_E_ARG, "advance: bad argument");
+    PFB_CU(cudaSetDevice(e->device), "cudaSetDevice");
+    return e->advance(steps);
+}
+
+int pfb_ens2d_advance_serial(pfb_ens2d* e, int steps) {
+    if (!e || steps < 0) return set_error(PFB_E_ARG, "advance: bad argument");
+    PFB_CU(cudaSetDevice(e->device), "cudaSetDevice");
+    return e->advance_serial(steps);
+}
+
+int pfb_ens2d_sync(pfb_ens2d* e) {
+    if (!e) return set_error(PFB_E_ARG, "null ensemble");
+    PFB_CU(cudaStreamSynchronize(e->stream), "sync");
+    return PFB_OK;
+}
+
+long long pfb_ens2d_step(const pfb_ens2d* e) { return e ? e->steps_done : -1; }
+
+pfb_sim2d* pfb_ens2d_system(pfb_ens2d* e, int r) {
+    if (!e || r < 0 || r >= e->R()) {
+        set_error(PFB_E_ARG, "system index out of range");
+        return nullptr;
+    }
+    if (cudaStreamSynchronize(e->stream) != cudaSuccess) {
+        set_error(PFB_E_CUDA, "sync");
+        return nullptr;
+    }
+    return e->sims[(size_t)r];
+}
+
+// Device time of `steps` steps after `warmup`, in ms per step; serial != 0
+// launches the systems one at a time instead of in one batch.
+int pfb_ens2d_bench(pfb_ens2d* e, int warmup, int steps, int serial, double* ms_per_step) {
+    if (!e || warmup < 0 || steps < 1 || !ms_per_step) return set_error(PFB_E_ARG, "bench: bad argument");
+    PFB_CU(cudaSetDevice(e->device), "cudaSetDevice");
+    int rc = serial ? e->advance_serial(warmup) : e->advance(warmup);
+    if (rc) return rc;
+    if (!serial) {
+        rc = e->advance((6 - e->steps_done % 6) % 6);
+        if (rc) return rc;
+    }
+    PFB_CU(cudaStreamSynchronize(e->stream), "sync");
+    cudaEvent_t e0, e1;
+    PFB_CU(cudaEventCreate(&e0), "event");
+    PFB_CU(cudaEventCreate(&e1), "event");
+    cudaEventRecord(e0, e->stream);
+    rc = serial ? e->advance_serial(steps) : e->advance(steps);
+    cudaEventRecord(e1, e->stream);
+    const cudaError_t err = cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    PFB_CU(err, "bench sync");
+    *ms_per_step = (double)ms / (double)steps;
+    return PFB_OK;
+}
+
+// Time a few steps with each cluster size and keep the fastest (the
+// ensemble's autotuner); writes the chosen size.
+int pfb_ens2d_autotune(pfb_ens2d* e, int steps, int* chosen) {
+    if (!e || steps < 1) return set_error(PFB_E_ARG, "autotune: bad argument");
+    double best = 0.0;
+    int best_k = e->cluster;
+    const int ks[3] = {2, 4, 8};
+    for (int k : ks) {
+        int rc = pfb_ens2d_set_cluster(e, k);
+        if (rc) return rc;
+        double ms = 0.0;
+        rc = pfb_ens2d_bench(e, 6, steps, 0, &ms);
+        if (rc) return rc;
+        if (best == 0.0 || ms < best) {
+            best = ms;
+            best_k = k;
+        }
+    }
+    if (chosen) *chosen = best_k;
+    return pfb_ens2d_set_cluster(e, best_k);
+}
 
 }  // extern "C"

@@ -570,10 +570,9 @@ __device__ __forceinline__ void global_cell_v1(const pfb_step_args2d& A, int n, 
     global_cell<CLS, K, kWarps>(A, sh.plan, rank, sh.red, fm, &g_step2d_status);
 }
 
+// One system's step for CTA `lb` of the `nb` CTAs that serve it.
 template <int K>
-__global__ void __launch_bounds__(kThreads, PFB_STEP2D_MINB)
-    k_step2d(const __grid_constant__ pfb_step_args2d A) {
-    extern __shared__ __align__(128) char smem[];
+__device__ __forceinline__ void step_body(const pfb_step_args2d& A, int lb, int nb, char* smem) {
     const int tid = threadIdx.x;
 
     // Clear the S slot two steps ahead with streaming stores (the kernel does
@@ -581,13 +580,12 @@ __global__ void __launch_bounds__(kThreads, PFB_STEP2D_MINB)
     if (A.clear_ahead_words) {
         uint4* dst = reinterpret_cast<uint4*>(A.S_cl);
         const size_t nvec = (size_t)(A.clear_ahead_words >> 2);
-        const size_t stride = (size_t)gridDim.x * kThreads;
+        const size_t stride = (size_t)nb * kThreads;
         const uint4 z = make_uint4(0u, 0u, 0u, 0u);
-        for (size_t i = (size_t)blockIdx.x * kThreads + tid; i < nvec; i += stride)
-            __stcs(dst + i, z);
+        for (size_t i = (size_t)lb * kThreads + tid; i < nvec; i += stride) __stcs(dst + i, z);
     }
     const unsigned long long step = *A.step_rd;
-    if (blockIdx.x == 0 && tid == 0) {
+    if (lb == 0 && tid == 0) {
         if (A.cursor_clear) *A.cursor_clear = 0ull;
         *A.step_wr = step + 1ull;
     }
@@ -597,7 +595,7 @@ __global__ void __launch_bounds__(kThreads, PFB_STEP2D_MINB)
     StepShared<K>& sh = *reinterpret_cast<StepShared<K>*>(smem);
     if (tid == 0) red_init<kWarps, K>(sh.red, rank);
     dev::cluster_arrive_relaxed();  // matched by the wait in reduce_force
-    const int slot = (int)(blockIdx.x / K);
+    const int slot = lb / K;
     const int n = A.perm ? (int)A.perm[slot] : slot;
     const int cls = (int)A.cell_cls[n];
     switch (cls) {
@@ -614,6 +612,41 @@ __global__ void __launch_bounds__(kThreads, PFB_STEP2D_MINB)
     }
 }
 
+template <int K>
+__global__ void __launch_bounds__(kThreads, PFB_STEP2D_MINB)
+    k_step2d(const __grid_constant__ pfb_step_args2d A) {
+    extern __shared__ __align__(128) char smem[];
+    step_body<K>(A, (int)blockIdx.x, (int)gridDim.x, smem);
+}
+
+// Many independent systems in one launch: system r is served by CTAs
+// [block_start[r], block_start[r+1]) (multiples of K, so clusters never
+// straddle systems); its arguments are copied into shared memory.
+template <int K>
+__global__ void __launch_bounds__(kThreads, PFB_STEP2D_MINB)
+    k_step2d_batch(const pfb_step_args2d* __restrict__ args, const int* __restrict__ block_start,
+                   int R) {
+    extern __shared__ __align__(128) char smem[];
+    __shared__ __align__(16) pfb_step_args2d sA;
+    const int b = (int)blockIdx.x;
+    int lo = 0, hi = R - 1;  // last r with block_start[r] <= b
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(block_start + mid) <= b)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const int r = lo;
+    static_assert(sizeof(pfb_step_args2d) % 8 == 0, "argument record copy");
+    const uint64_t* srcw = reinterpret_cast<const uint64_t*>(args + r);
+    uint64_t* dstw = reinterpret_cast<uint64_t*>(&sA);
+    if (threadIdx.x < sizeof(pfb_step_args2d) / 8) dstw[threadIdx.x] = __ldg(srcw + threadIdx.x);
+    __syncthreads();
+    const int b0 = __ldg(block_start + r);
+    step_body<K>(sA, b - b0, __ldg(block_start + r + 1) - b0, smem);
+}
+
 // ---------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------
@@ -622,7 +655,13 @@ static cudaError_t configure_one() {
     cudaError_t e = cudaFuncSetAttribute(k_step2d<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          step_smem_bytes(K));
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_step2d<K>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    e = cudaFuncSetAttribute(k_step2d<K>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_step2d_batch<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             step_smem_bytes(K));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_step2d_batch<K>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                100);
 }
 
 int step2d_configure_device() {
@@ -685,6 +724,42 @@ int step2d_launch_variant(const pfb_step_args2d* a, int cluster, int variant,
                     : cluster == 4 ? launch_k<4>(A, stream)
                                    : launch_k<8>(A, stream);
     if (e != cudaSuccess) return set_error(PFB_E_CUDA, "step launch: %s", cudaGetErrorString(e));
+    return PFB_OK;
+}
+
+template <int K>
+static cudaError_t launch_batch_k(const pfb_step_args2d* args, const int* block_start, int R,
+                                  int total_blocks, cudaStream_t stream) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)total_blocks, 1, 1);
+    cfg.blockDim = dim3(kThreads, 1, 1);
+    cfg.dynamicSmemBytes = (size_t)step_smem_bytes(K);
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = K;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_step2d_batch<K>, args, block_start, R);
+}
+
+int step2d_launch_batch(const pfb_step_args2d* d_args, const int* d_block_start, int R,
+                        int total_blocks, int cluster, cudaStream_t stream) {
+    if (!d_args || !d_block_start || R <= 0 || total_blocks < 0)
+        return set_error(PFB_E_ARG, "invalid batch arguments");
+    if (cluster == 0) cluster = kDefaultCluster;
+    if (cluster != 2 && cluster != 4 && cluster != 8)
+        return set_error(PFB_E_CONFIG, "cluster must be 2, 4 or 8");
+    if (total_blocks % cluster) return set_error(PFB_E_ARG, "block count must be a multiple of K");
+    if (total_blocks == 0) return PFB_OK;
+    int rc = step2d_configure_device();
+    if (rc) return rc;
+    cudaError_t e = cluster == 2   ? launch_batch_k<2>(d_args, d_block_start, R, total_blocks, stream)
+                    : cluster == 4 ? launch_batch_k<4>(d_args, d_block_start, R, total_blocks, stream)
+                                   : launch_batch_k<8>(d_args, d_block_start, R, total_blocks, stream);
+    if (e != cudaSuccess) return set_error(PFB_E_CUDA, "batch launch: %s", cudaGetErrorString(e));
     return PFB_OK;
 }
 

@@ -14,6 +14,7 @@ from ._abi3d import (CELL3D_DTYPE, FLAG3D_COUNT, FLAG3D_NAMES, Cell3D, Layout3D,
 from .sim2d import (Sim2D, SimParams2D, domain_side_for, fatal, flags_report,
                     grid_jitter_centres, palmieri_centres, step_coefficients, window_view,
                     world_field)
+from .ensemble import Ensemble2D
 from .sim3d import (Sim3D, SimParams3D, automatic_brick_edge, calibrate_seed_radius,
                     flags_report3, sequential_centres)
 
@@ -24,5 +25,5 @@ __all__ = [
     "flags_report", "grid_jitter_centres", "palmieri_centres", "step_coefficients",
     "window_view", "world_field", "CELL3D_DTYPE", "FLAG3D_COUNT", "FLAG3D_NAMES", "Cell3D",
     "Layout3D", "MeasureArgs3D", "UpdateArgs3D", "Sim3D", "SimParams3D", "automatic_brick_edge",
-    "calibrate_seed_radius", "flags_report3", "sequential_centres",
+    "calibrate_seed_radius", "flags_report3", "sequential_centres", "Ensemble2D",
 ]

@@ -173,6 +173,17 @@ _SIGS = {
     "pfb_sim2d_bench": (I, [P, I, I, C.POINTER(C.c_double)]),
     "pfb_sim2d_step_args": (I, [P, C.POINTER(StepArgs2D)]),
     "pfb_sim2d_stream": (P, [P]),
+    "pfb_ens2d_create": (P, [I, C.POINTER(Params2D), P, P, I]),
+    "pfb_ens2d_destroy": (None, [P]),
+    "pfb_ens2d_num_systems": (I, [P]),
+    "pfb_ens2d_set_cluster": (I, [P, I]),
+    "pfb_ens2d_autotune": (I, [P, I, C.POINTER(C.c_int)]),
+    "pfb_ens2d_advance": (I, [P, I]),
+    "pfb_ens2d_advance_serial": (I, [P, I]),
+    "pfb_ens2d_sync": (I, [P]),
+    "pfb_ens2d_step": (C.c_longlong, [P]),
+    "pfb_ens2d_system": (P, [P, I]),
+    "pfb_ens2d_bench": (I, [P, I, I, I, C.POINTER(C.c_double)]),
 }
 
 _LIB = None

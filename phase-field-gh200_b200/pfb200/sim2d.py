@@ -138,8 +138,19 @@ class Sim2D:
     # ------------------------------------------------------------------ control
     def close(self) -> None:
         if getattr(self, "_h", None):
-            lib().pfb_sim2d_destroy(self._h)
+            if getattr(self, "_owned", True):
+                lib().pfb_sim2d_destroy(self._h)
             self._h = None
+
+    @classmethod
+    def _view(cls, handle: int, params: "SimParams2D") -> "Sim2D":
+        """A non-owning Sim2D over a handle that another object owns."""
+        v = cls.__new__(cls)
+        v.params = params
+        v._pc = params.to_c()
+        v._h = handle
+        v._owned = False
+        return v
 
     def __del__(self):  # pragma: no cover - interpreter teardown order
         try:
