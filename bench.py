@@ -81,12 +81,13 @@ def sites_per_step(cells) -> int:
     return int(sum(pfb200.CLASSES[0][0] * pfb200.CLASSES[0][1] for _ in range(len(cells))))
 
 
-def algorithmic_bytes(cells, L: int) -> int:
-    """sum_n A_n * 2 * 4 B (read phi^n + write phi^{n+1} over the processed
-    window) + L^2 * 8 B (one read and one write of the u32 aggregate)."""
+def algorithmic_bytes(cells, L: int, phi_bytes: int = 4) -> int:
+    """sum_n A_n * 2 * phi_bytes (read phi^n + write phi^{n+1} over the
+    processed window) + L^2 * 8 B (one read and one write of the u32
+    aggregate)."""
     import pfb200
     area = sum(pfb200.CLASSES[int(c)][0] * pfb200.CLASSES[int(c)][1] for c in cells["cls"])
-    return int(area * 8 + L * L * 8)
+    return int(area * 2 * phi_bytes + L * L * 8)
 
 
 class ClockSampler:
@@ -354,7 +355,7 @@ def run_3d(a):
         peak, peak_src = read_peak_hbm()
         achieved = alg / (ms_step / 1000.0) / 1e9
         cpu = None
-        if world == 1 and a.cpu_steps > 0:
+        if world == 1 and a.cpu_steps > 0 and a.phi_storage == 0:
             cpu = cpu_sample3d(p, sim, threads=0)
         line = {
             "metric": "site-cell updates/s", "value": world * sites * a.steps / (ms / 1000.0),
@@ -495,6 +496,8 @@ def main():
     ap.add_argument("--cluster", type=int, default=2, help="CTAs per cell (2, 4 or 8)")
     ap.add_argument("--variant", type=int, default=0, help="kernel variant (0 = default)")
     ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--phi-storage", type=int, default=0, choices=[0, 1, 2],
+                    help="2D phi pools: 0 binary32 (reference layout), 1 binary16, 2 bfloat16")
     ap.add_argument("--cpu-steps", type=int, default=int(os.environ.get("PFB_CPU_STEPS", "6")))
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "ce"],
@@ -524,12 +527,13 @@ def main():
     torch.cuda.set_device(device)
 
     p = workload_params(1234 + rank)
+    p.phi_storage = a.phi_storage
     cx, cy = workload_centres(p)
     sim = pfb200.Sim2D(p, cx, cy, device=device, cluster=a.cluster, use_graph=not a.no_graph,
                        variant=a.variant)
     init_cells = sim.cells()
     init_phi = sim.phi() if (rank == 0 and world == 1) or not a.no_e2e else None
-    alg = algorithmic_bytes(init_cells, p.L)
+    alg = algorithmic_bytes(init_cells, p.L, 2 if a.phi_storage else 4)
     sites = sites_per_step(init_cells)
 
     def barrier():
@@ -599,7 +603,7 @@ def main():
     if rank == 0:
         peak, peak_src = read_peak_hbm()
         achieved = alg / (ms_step / 1000.0) / 1e9
-        traffic = read_ncu_traffic()
+        traffic = read_ncu_traffic() if a.phi_storage == 0 else None
         cpu = None
         if world == 1 and a.cpu_steps > 0:
             v, dt, thr = cpu_sample(init_cells, init_phi, p, a.cpu_steps, 0)
@@ -609,19 +613,24 @@ def main():
         line = {
             "metric": "site-cell updates/s", "value": value, "unit": "site-cell updates/s",
             "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_step,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": ("f32", "f32 arithmetic, f16 phi storage",
+                      "f32 arithmetic, bf16 phi storage")[a.phi_storage],
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "L": L_SIDE, "cells": N_CELLS, "radius": RADIUS,
                        "sites_per_step": sites, "window": "reference class-0 window 144^2",
                        "cluster_ctas_per_cell": a.cluster, "kernel_variant": a.variant,
                        "cuda_graph": not a.no_graph,
+                       "phi_storage": ("binary32", "binary16", "bfloat16")[a.phi_storage],
                        "l2": "inputs larger than L2: two 340 MB phi pools; per-step working "
                              "set 85 MB phi read + 85 MB phi written + 3 x 16.8 MB aggregate "
                              "slots; no flush between steps",
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": f"pfb::k_step2d<{a.cluster}>", "algorithmic_bytes_per_launch": alg,
+                         "kernel": "pfb::k_step2d<%d%s>" % (
+                             a.cluster, ("", ", __half", ", __nv_bfloat16")[a.phi_storage]),
+                         "algorithmic_bytes_per_launch": alg,
                          "peak_source": peak_src,
                          "duration_source": "CUDA events over the timed region / steps"},
             "cpu_baseline": cpu,

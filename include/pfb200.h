@@ -149,6 +149,10 @@ typedef struct pfb_params2d {
     unsigned long long seed;
     unsigned long long polarity_seed; /* 0 follows seed                  */
     int full_moment_every;
+    /* phi pool storage of the host driver: 0 binary32 (the reference's),
+     * 1 binary16, 2 bfloat16 (binary32 arithmetic, stochastic rounding on
+     * store; classes 0-3 only) -- no reference counterpart */
+    int phi_storage;
 } pfb_params2d;
 
 /* Compact trajectory record (reference include/kernels.cuh:60-70). */

@@ -37,7 +37,7 @@ COMMON = [
 SOURCES = ["step2d.cu", "init2d.cu", "sim2d.cu", "host2d.cpp", "measure3d.cu", "update3d.cu",
            "misc3d.cu", "sim3d.cu", "host3d.cpp"]
 HEADERS = ["pfb_common.cuh", "device_util.cuh", "pfb_internal.h", "step2d_common.cuh",
-           "pfb3d_common.cuh", "ring3d.cuh"]
+           "pfb3d_common.cuh", "ring3d.cuh", "storage2d.cuh"]
 
 
 def _newer(target: Path, deps: list[Path]) -> bool:

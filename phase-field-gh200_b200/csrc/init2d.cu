@@ -8,6 +8,9 @@
 #include "device_util.cuh"
 #include "pfb_common.cuh"
 #include "pfb_internal.h"
+#include "storage2d.cuh"
+
+#include <algorithm>
 
 namespace pfb {
 
@@ -301,6 +304,43 @@ int pack_traj2d(const pfb_cell2d* cell, const uint8_t* cls, pfb_traj_cell2d* out
     if (N == 0) return PFB_OK;
     k_pack_traj2d<<<(N + 127) / 128, 128, 0, s>>>(cell, cls, out, N, L);
     return launch_status("pack_traj2d");
+}
+
+}  // namespace pfb
+
+// ---- 16-bit phi pools: conversions at the host boundary -------------------
+namespace pfb {
+
+__global__ void k_narrow_pool(const float* __restrict__ in, uint16_t* __restrict__ out, size_t n,
+                              int storage) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        out[i] = storage == kStoreF16 ? __half_as_ushort(__float2half_rn(in[i]))
+                                      : __bfloat16_as_ushort(__float2bfloat16_rn(in[i]));
+}
+
+__global__ void k_widen_pool(const uint16_t* __restrict__ in, float* __restrict__ out, size_t n,
+                             int storage) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        out[i] = storage == kStoreF16 ? Store<__half>::value(in[i])
+                                      : Store<__nv_bfloat16>::value(in[i]);
+}
+
+int narrow_pool(const float* in, void* out, size_t n, int storage, cudaStream_t s) {
+    if (!in || !out) return set_error(PFB_E_ARG, "narrow_pool: null");
+    const int blocks = (int)std::min<size_t>(148 * 8, (n + 255) / 256 + 1);
+    k_narrow_pool<<<blocks, 256, 0, s>>>(in, static_cast<uint16_t*>(out), n, storage);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? PFB_OK : set_error(PFB_E_CUDA, "narrow_pool: %s", cudaGetErrorString(e));
+}
+
+int widen_pool(const void* in, float* out, size_t n, int storage, cudaStream_t s) {
+    if (!in || !out) return set_error(PFB_E_ARG, "widen_pool: null");
+    const int blocks = (int)std::min<size_t>(148 * 8, (n + 255) / 256 + 1);
+    k_widen_pool<<<blocks, 256, 0, s>>>(static_cast<const uint16_t*>(in), out, n, storage);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? PFB_OK : set_error(PFB_E_CUDA, "widen_pool: %s", cudaGetErrorString(e));
 }
 
 }  // namespace pfb

@@ -28,6 +28,10 @@ int step2d_read_status(unsigned* out, int clear);
 // variant: 0 = default, 1 = one thread-block cluster per cell
 int step2d_launch_variant(const pfb_step_args2d* a, int cluster, int variant,
                           cudaStream_t stream);
+// storage: 0 binary32 pools, 1 binary16, 2 bfloat16 (16-bit pools hold 2-byte
+// values at the same tile positions; clusters of 2 or 4)
+int step2d_launch_storage(const pfb_step_args2d* a, int cluster, int variant, int storage,
+                          cudaStream_t stream);
 
 // init2d.cu
 int init_tiles2d(float* phi_a, float* phi_b, pfb_cell2d* cell, const uint8_t* cls, int N, int L,
@@ -38,6 +42,9 @@ int init_moments2d(pfb_cell2d* cell, const uint8_t* cls, const float* phi, int N
 int scatter_all2d(const float* phi, const pfb_cell2d* cell, const uint8_t* cls, uint32_t* S,
                   int N, int L, int P, uint32_t* flags, cudaStream_t s);
 int zero_u32(uint32_t* p, size_t n, cudaStream_t s);
+// binary32 <-> 16-bit pool conversion (round to nearest), storage 1 or 2
+int narrow_pool(const float* in, void* out, size_t n, int storage, cudaStream_t s);
+int widen_pool(const void* in, float* out, size_t n, int storage, cudaStream_t s);
 int verify_cells2d(const float* phi, const pfb_cell2d* cell, const uint8_t* cls, int N,
                    double* out_V, float* out_outside, cudaStream_t s);
 int verify_S(const uint32_t* S, size_t n, uint32_t* out_max, cudaStream_t s);

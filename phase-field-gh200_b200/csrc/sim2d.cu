@@ -92,7 +92,16 @@ struct pfb_sim2d {
 
     int launch_one(int slot) {
         const pfb_step_args2d a = args_for_slot(slot);
-        return step2d_launch_variant(&a, cluster, variant, stream);
+        return step2d_launch_storage(&a, cluster, variant, p.phi_storage, stream);
+    }
+
+    size_t pool_bytes() const {
+        return (size_t)N * kTileArea * (p.phi_storage ? sizeof(uint16_t) : sizeof(float));
+    }
+
+    // Field of a 16-bit pool in binary32 (a temporary of N tiles).
+    int widen(int pool, float* out) {
+        return widen_pool(d_phi[pool], out, (size_t)N * kTileArea, p.phi_storage, stream);
     }
 
     void drop_graph() {
@@ -149,10 +158,12 @@ struct pfb_sim2d {
         L = p.L;
         if (N < 1) return set_error(PFB_E_ARG, "num_cells must be positive");
         if (L <= 286) return set_error(PFB_E_ARG, "domain side %d must exceed 286", L);
+        if (p.phi_storage < 0 || p.phi_storage > 2)
+            return set_error(PFB_E_ARG, "phi_storage must be 0, 1 or 2");
         P = 32 * ((L + 31) / 32);
         s_words = (size_t)P * (size_t)L;
         PFB_CU(cudaSetDevice(device), "cudaSetDevice");
-        const size_t pool = (size_t)N * kTileArea * sizeof(float);
+        const size_t pool = pool_bytes();
         PFB_CU(cudaMalloc(&d_phi[0], pool), "alloc phi");
         PFB_CU(cudaMalloc(&d_phi[1], pool), "alloc phi");
         PFB_CU(cudaMalloc(&d_S, 3 * s_words * sizeof(uint32_t)), "alloc S");
@@ -184,12 +195,27 @@ struct pfb_sim2d {
             h[(size_t)i].cls_written[1] = cells[i].cls;
             hc[(size_t)i] = cells[i].cls;
         }
-        const size_t pool = (size_t)N * kTileArea * sizeof(float);
+        const size_t pool = pool_bytes();
+        const size_t fwords = (size_t)N * kTileArea;
         PFB_CU(cudaMemcpyAsync(d_cell, h.data(), h.size() * sizeof(pfb_cell2d),
                                cudaMemcpyHostToDevice, stream), "upload cells");
         PFB_CU(cudaMemcpyAsync(d_cls, hc.data(), hc.size(), cudaMemcpyHostToDevice, stream),
                "upload classes");
-        PFB_CU(cudaMemcpyAsync(d_phi[pin], phi, pool, cudaMemcpyHostToDevice, stream), "upload phi");
+        float* scan = nullptr;  // binary32 field the aggregate is built from
+        if (p.phi_storage) {
+            PFB_CU(cudaMalloc(&scan, fwords * sizeof(float)), "alloc staging field");
+            PFB_CU(cudaMemcpyAsync(scan, phi, fwords * sizeof(float), cudaMemcpyHostToDevice, stream),
+                   "upload phi");
+            int rc = narrow_pool(scan, d_phi[pin], fwords, p.phi_storage, stream);
+            if (!rc) rc = widen(pin, scan);
+            if (rc) {
+                cudaFree(scan);
+                return rc;
+            }
+        } else {
+            PFB_CU(cudaMemcpyAsync(d_phi[pin], phi, pool, cudaMemcpyHostToDevice, stream),
+                   "upload phi");
+        }
         PFB_CU(cudaMemsetAsync(d_phi[1 - pin], 0, pool, stream), "clear phi");
         const unsigned long long hs[2] = {
             (unsigned long long)(pin == 0 ? step : step + 1),
@@ -197,10 +223,12 @@ struct pfb_sim2d {
         PFB_CU(cudaMemcpyAsync(d_step, hs, sizeof(hs), cudaMemcpyHostToDevice, stream), "upload step");
         PFB_CU(cudaMemsetAsync(d_cursor, 0, 2 * sizeof(unsigned long long), stream), "memset");
         PFB_CU(cudaMemsetAsync(d_S, 0, 3 * s_words * sizeof(uint32_t), stream), "memset S");
-        int rc = scatter_all2d(d_phi[pin], d_cell, d_cls, d_S + (size_t)rot * s_words, N, L, P,
-                               d_flags, stream);
+        int rc = scatter_all2d(scan ? scan : (const float*)d_phi[pin], d_cell, d_cls,
+                               d_S + (size_t)rot * s_words, N, L, P, d_flags, stream);
+        const cudaError_t e = cudaStreamSynchronize(stream);
+        cudaFree(scan);
         if (rc) return rc;
-        PFB_CU(cudaStreamSynchronize(stream), "set_state sync");
+        PFB_CU(e, "set_state sync");
         return PFB_OK;
     }
 
@@ -235,14 +263,31 @@ struct pfb_sim2d {
                "upload centres");
         PFB_CU(cudaMemcpyAsync(d_cy, cy, (size_t)N * sizeof(float), cudaMemcpyHostToDevice, stream),
                "upload centres");
-        int rc = init_tiles2d(d_phi[0], d_phi[1], d_cell, d_cls, N, L, d_cx, d_cy,
+        // 16-bit pools: seed binary32 tiles in temporaries, round them to
+        // nearest into the pool and measure / scatter the stored values
+        float* f0 = nullptr;
+        float* f1 = nullptr;
+        if (p.phi_storage) {
+            PFB_CU(cudaMalloc(&f0, (size_t)N * kTileArea * sizeof(float)), "alloc staging field");
+            PFB_CU(cudaMalloc(&f1, (size_t)N * kTileArea * sizeof(float)), "alloc staging field");
+        }
+        float* a0 = p.phi_storage ? f0 : (float*)d_phi[0];
+        float* a1 = p.phi_storage ? f1 : (float*)d_phi[1];
+        int rc = init_tiles2d(a0, a1, d_cell, d_cls, N, L, d_cx, d_cy,
                               (float)seed_radius(p.target_radius, p.lambda),
                               (float)iface_k(p.lambda), stream);
-        if (!rc) rc = init_moments2d(d_cell, d_cls, d_phi[0], N, stream);
-        if (!rc) rc = scatter_all2d(d_phi[0], d_cell, d_cls, d_S, N, L, P, d_flags, stream);
+        if (!rc && p.phi_storage) {
+            rc = narrow_pool(f0, d_phi[0], (size_t)N * kTileArea, p.phi_storage, stream);
+            if (!rc) rc = narrow_pool(f1, d_phi[1], (size_t)N * kTileArea, p.phi_storage, stream);
+            if (!rc) rc = widen(0, f0);
+        }
+        if (!rc) rc = init_moments2d(d_cell, d_cls, a0, N, stream);
+        if (!rc) rc = scatter_all2d(a0, d_cell, d_cls, d_S, N, L, P, d_flags, stream);
         const cudaError_t e = cudaStreamSynchronize(stream);
         cudaFree(d_cx);
         cudaFree(d_cy);
+        cudaFree(f0);
+        cudaFree(f1);
         if (rc) return rc;
         PFB_CU(e, "init sync");
         steps_done = 0;
@@ -354,6 +399,8 @@ void pfb_sim2d_destroy(pfb_sim2d* s) {
 int pfb_sim2d_set_cluster(pfb_sim2d* s, int cluster) {
     if (!s) return set_error(PFB_E_ARG, "null sim");
     if (cluster != 2 && cluster != 4 && cluster != 8) return set_error(PFB_E_CONFIG, "cluster must be 2, 4 or 8");
+    if (cluster == 8 && s->p.phi_storage)
+        return set_error(PFB_E_CONFIG, "16-bit phi pools run with clusters of 2 or 4");
     if (cluster != s->cluster) s->drop_graph();
     s->cluster = cluster;
     return PFB_OK;
@@ -402,8 +449,22 @@ int pfb_sim2d_get_cells(pfb_sim2d* s, pfb_cell2d* out) {
 int pfb_sim2d_get_phi(pfb_sim2d* s, float* out) {
     if (!s || !out) return set_error(PFB_E_ARG, "get_phi: null");
     const int pin = (int)(s->steps_done % 2);
-    PFB_CU(cudaMemcpyAsync(out, s->d_phi[pin], (size_t)s->N * kTileArea * sizeof(float),
-                           cudaMemcpyDeviceToHost, s->stream), "download phi");
+    const size_t bytes = (size_t)s->N * kTileArea * sizeof(float);
+    if (s->p.phi_storage) {
+        float* tmp = nullptr;
+        PFB_CU(cudaMalloc(&tmp, bytes), "alloc staging field");
+        int rc = s->widen(pin, tmp);
+        const cudaError_t e = rc ? cudaSuccess
+                                 : cudaMemcpyAsync(out, tmp, bytes, cudaMemcpyDeviceToHost, s->stream);
+        const cudaError_t e2 = cudaStreamSynchronize(s->stream);
+        cudaFree(tmp);
+        if (rc) return rc;
+        PFB_CU(e, "download phi");
+        PFB_CU(e2, "sync");
+        return PFB_OK;
+    }
+    PFB_CU(cudaMemcpyAsync(out, s->d_phi[pin], bytes, cudaMemcpyDeviceToHost, s->stream),
+           "download phi");
     PFB_CU(cudaStreamSynchronize(s->stream), "sync");
     return PFB_OK;
 }
@@ -618,6 +679,11 @@ pfb_ens2d* pfb_ens2d_create(int R, const pfb_params2d* params, const float* cons
     }
     e->device = device;
     for (int r = 0; r < R; ++r) {
+        if (params[r].phi_storage != 0) {
+            set_error(PFB_E_CONFIG, "the batched ensemble uses binary32 pools");
+            delete e;
+            return nullptr;
+        }
         pfb_sim2d* s = pfb_sim2d_create(&params[r], cx[r], cy[r], device);
         if (!s) {
             delete e;

@@ -32,6 +32,7 @@
 #include "pfb_common.cuh"
 #include "pfb_internal.h"
 #include "step2d_common.cuh"
+#include "storage2d.cuh"
 
 namespace pfb {
 
@@ -44,8 +45,7 @@ namespace pfb {
 #define PFB_STEP2D_MINB 3
 #endif
 // L2 eviction priorities (bit 0: the staged phi_in and S_rd rows are read
-// evict-first; bit 1: phi_out rows are stored evict-last so the next step's
-// staging finds them in L2).
+// evict-first).
 #ifndef PFB_STEP2D_L2HINTS
 #define PFB_STEP2D_L2HINTS 1
 #endif
@@ -132,6 +132,56 @@ __host__ __device__ constexpr int step_smem_bytes(int k) {
     return m;
 }
 
+// ---- phi pool stores -------------------------------------------------------
+// float pools store as is; 16-bit pools round stochastically (storage2d.cuh)
+// and report the stored value back so that moments and the scatter see it.
+template <typename T>
+__device__ __forceinline__ void store4(T* o, float (&v)[4], uint32_t seed, uint32_t pix) {
+    if constexpr (!Store<T>::kHalf) {
+        __stcs(reinterpret_cast<float4*>(o), make_float4(v[0], v[1], v[2], v[3]));
+    } else {
+        uint16_t b[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            b[j] = Store<T>::bits(v[j], mix32(seed ^ ((pix + j) * 0x9E3779B9u)));
+            v[j] = Store<T>::value(b[j]);
+        }
+        __stcs(reinterpret_cast<uint2*>(o),
+               make_uint2((uint32_t)b[0] | ((uint32_t)b[1] << 16),
+                          (uint32_t)b[2] | ((uint32_t)b[3] << 16)));
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ float store1(T* o, float v, uint32_t seed, uint32_t pix) {
+    if constexpr (!Store<T>::kHalf) {
+        __stcs(o, v);
+        return v;
+    } else {
+        const uint16_t b = Store<T>::bits(v, mix32(seed ^ (pix * 0x9E3779B9u)));
+        __stcs(reinterpret_cast<unsigned short*>(o), b);
+        return Store<T>::value(b);
+    }
+}
+
+// value a store of v at tile pixel pix will hold
+template <typename T>
+__device__ __forceinline__ float rounded(float v, uint32_t seed, uint32_t pix) {
+    if constexpr (!Store<T>::kHalf) {
+        return v;
+    } else {
+        return Store<T>::value(Store<T>::bits(v, mix32(seed ^ (pix * 0x9E3779B9u))));
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void store_zero(T* o) {
+    if constexpr (!Store<T>::kHalf)
+        *o = 0.0f;
+    else
+        *reinterpret_cast<unsigned short*>(o) = 0;
+}
+
 // ---------------------------------------------------------------------------
 // Staged path: classes 0-3.
 // Shared layout after the header (row pitch PX = WX + 8 words):
@@ -143,7 +193,7 @@ __host__ __device__ constexpr int step_smem_bytes(int k) {
 //                          (f32 bits); on full-moment steps phi^{n+1} is
 //                          written over it.
 // ---------------------------------------------------------------------------
-template <int CLS, int K>
+template <int CLS, int K, typename T>
 __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int rank,
                                             char* smem, unsigned long long step, bool fm) {
     constexpr Window W = window_of(CLS);
@@ -162,9 +212,14 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int y0 = rank * RB;
     const int y1 = y0 + RB;
-    const float* tile_in = A.phi_in + (size_t)n * kTileArea;
+    const T* tile_in = reinterpret_cast<const T*>(A.phi_in) + (size_t)n * kTileArea;
     const int L = A.L, Pp = A.P;
     const bool s_tma = (L & 3) == 0;
+    constexpr bool kHalf = Store<T>::kHalf;
+    // 16-bit rows are copied into the back of their binary32 row and widened
+    // in place after the copy completes
+    constexpr int HOFF = WX / 2 + 8;
+    static_assert(!kHalf || (HOFF % 4 == 0 && HOFF + WX / 2 <= PX), "16-bit staging offset");
 
     if (tid == 0) {
         sh.abort = 0;
@@ -186,7 +241,7 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
         const int n1 = wrap ? L - gxa : min((soff + WX + 3) & ~3, Pp - gxa);
         const int n2 = wrap ? ((gx0 + WX - L + 3) & ~3) : 0;
         uint32_t bytes = 0;
-        for (int y = ra + lane; y < rb; y += 32) bytes += (uint32_t)(WX * 4);
+        for (int y = ra + lane; y < rb; y += 32) bytes += (uint32_t)(WX * sizeof(T));
         if (s_tma)
             for (int y = sa + lane; y < sb; y += 32) bytes += (uint32_t)((n1 + n2) * 4);
         bytes = __reduce_add_sync(0xFFFFFFFFu, bytes);
@@ -199,8 +254,9 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
 #define PFB_G2S(d, s, n, b) dev::bulk_g2s(d, s, n, b)
 #endif
         for (int y = ra + lane; y < rb; y += 32)
-            PFB_G2S(phi_s + (y - y0 + 2) * PX + 4, tile_in + (size_t)(TY0 + y) * kTilePitch + TX0,
-                    (uint32_t)(WX * 4), &sh.bar);
+            PFB_G2S(phi_s + (y - y0 + 2) * PX + (kHalf ? HOFF : 4),
+                    tile_in + (size_t)(TY0 + y) * kTilePitch + TX0, (uint32_t)(WX * sizeof(T)),
+                    &sh.bar);
         if (s_tma) {
             for (int y = sa + lane; y < sb; y += 32) {
                 int gy = gy0 + y;
@@ -230,14 +286,16 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
                 ps_s[(y - y0 + 1) * PX + x] = __ldg(A.S_rd + (size_t)gy * Pp + gx);
             }
         }
-        // Zero ring columns of in-window rows; whole rows outside the window.
-        for (int k = t; k < PHI_ROWS; k += NT) {
-            const int y = y0 - 2 + k;
-            if (y >= 0 && y < WY) {
-                phi_s[k * PX + 3] = 0.0f;
-                phi_s[k * PX + 4 + WX] = 0.0f;
+        // Zero ring columns of in-window rows (16-bit rows: after widening);
+        // whole rows outside the window.
+        if (!kHalf)
+            for (int k = t; k < PHI_ROWS; k += NT) {
+                const int y = y0 - 2 + k;
+                if (y >= 0 && y < WY) {
+                    phi_s[k * PX + 3] = 0.0f;
+                    phi_s[k * PX + 4 + WX] = 0.0f;
+                }
             }
-        }
         if (rank == 0 || rank == K - 1) {
             const int kb = rank == 0 ? 0 : RB + 2;
             for (int i = t; i < 2 * PX; i += NT) phi_s[kb * PX + i] = 0.0f;
@@ -249,6 +307,36 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
     }
     __syncthreads();
     const bool abort = sh.abort != 0;
+    if constexpr (kHalf) {
+        // widen each staged 16-bit row into its binary32 slots, one warp per
+        // row: all lanes read the row before any lane writes
+        if (!abort) {
+            constexpr int PER = (WX + 31) / 32;
+            for (int k = warp; k < PHI_ROWS; k += kWarps) {
+                const int y = y0 - 2 + k;
+                if (y < 0 || y >= WY) continue;
+                float* row = phi_s + k * PX;
+                const uint16_t* hrow = reinterpret_cast<const uint16_t*>(row + HOFF);
+                float v[PER];
+#pragma unroll
+                for (int i = 0; i < PER; ++i) {
+                    const int x = lane + 32 * i;
+                    v[i] = x < WX ? Store<T>::value(hrow[x]) : 0.0f;
+                }
+                __syncwarp();
+#pragma unroll
+                for (int i = 0; i < PER; ++i) {
+                    const int x = lane + 32 * i;
+                    if (x < WX) row[4 + x] = v[i];
+                }
+                if (lane == 0) {
+                    row[3] = 0.0f;
+                    row[4 + WX] = 0.0f;
+                }
+            }
+        }
+        __syncthreads();
+    }
 
     // ---- pass 1: S_other of the thread's strip (stored over q_S) and the
     // interaction integral. A thread owns a strip four pixels wide and up to
@@ -310,7 +398,12 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
     const int sx = P.sx, sy = P.sy;
     const int dwx = P.dwx, dwy = P.dwy, dtx0 = P.dtx0, dty0 = P.dty0;
     const int gx0n = P.gx0n, gy0n = P.gy0n;
-    float* tile_out = A.phi_out + (size_t)n * kTileArea;
+    T* tile_out = reinterpret_cast<T*>(A.phi_out) + (size_t)n * kTileArea;
+    // stochastic-rounding stream of this cell and step (16-bit pools)
+    const uint32_t sr_seed = kHalf ? mix32((uint32_t)step * 0x85EBCA6Bu ^
+                                           (uint32_t)A.cell[n].global_id * 0xC2B2AE35u ^
+                                           (uint32_t)A.seed)
+                                   : 0u;
     // Destination row b reads source row j = b + sy; rows above the window
     // belong to rank 0, rows below it to rank K-1.
     const int jlo = (rank == 0) ? -(1 << 20) : y0;
@@ -319,14 +412,14 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
     if (!abort && P.zero_tile) {
         // the destination tile last held another class: clear outside the window
         for (int b = b_lo + warp; b < b_hi; b += kWarps) {
-            float* trow = tile_out + (size_t)(dty0 + b) * kTilePitch;
+            T* trow = tile_out + (size_t)(dty0 + b) * kTilePitch;
             for (int c = lane; c < kTilePitch; c += 32)
-                if (c < dtx0 || c >= dtx0 + dwx) trow[c] = 0.0f;
+                if (c < dtx0 || c >= dtx0 + dwx) store_zero(trow + c);
         }
         for (int t = rank + K * warp; t < kTilePitch; t += K * kWarps) {
             if (t >= dty0 && t < dty0 + dwy) continue;
-            float* trow = tile_out + (size_t)t * kTilePitch;
-            for (int c = lane; c < kTilePitch; c += 32) trow[c] = 0.0f;
+            T* trow = tile_out + (size_t)t * kTilePitch;
+            for (int c = lane; c < kTilePitch; c += 32) store_zero(trow + c);
         }
     }
 
@@ -343,9 +436,7 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
             load_row(r0, wc, vc, ec);
             const uint32_t* qrow = ps_s + (r0 + 1) * PX + soff + x0;
             if (ident) {
-#if PFB_STEP2D_L2HINTS & 2
-                const uint64_t pol_out = dev::l2_policy_evict_last();
-#endif
+
                 uint32_t pmaxb = 0u;
                 unsigned colmask = 0u;
                 int gy = gy0 + y0 + r0;
@@ -356,7 +447,7 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
                 int gxj[4];
 #pragma unroll
                 for (int j = 0; j < 4; ++j) gxj[j] = gx + j < L ? gx + j : gx + j - L;
-                float* o = tile_out + (size_t)(TY0 + y0 + r0) * kTilePitch + TX0 + x0;
+                T* o = tile_out + (size_t)(TY0 + y0 + r0) * kTilePitch + TX0 + x0;
                 // overflow checks of a row's atomics run one row later, so the
                 // atomic round trip overlaps the next row's arithmetic
                 uint32_t old_prev[4] = {0u, 0u, 0u, 0u}, q_prev[4] = {0u, 0u, 0u, 0u};
@@ -370,12 +461,8 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
                     float pn[4];
                     stencil4(ws, vs, es, wc, vc, ec, wn, vn, en, so, gam, dwC, volC, repC, vx,
                              vy, mrel, dtf, pn);
-#if PFB_STEP2D_L2HINTS & 2
-                    dev::st_global_v4_hint(reinterpret_cast<float4*>(o),
-                                           make_float4(pn[0], pn[1], pn[2], pn[3]), pol_out);
-#else
-                    __stcs(reinterpret_cast<float4*>(o), make_float4(pn[0], pn[1], pn[2], pn[3]));
-#endif
+                    // pn becomes the stored value (16-bit pools round here)
+                    store4<T>(o, pn, sr_seed, (uint32_t)(o - tile_out));
                     uint32_t* srow = A.S_sc + (size_t)gy * Pp;
                     bool ovf = false;
 #pragma unroll
@@ -453,13 +540,14 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
                         int gyn = gy0n + b;
                         if (gyn >= L) gyn -= L;
                         uint32_t* srow = A.S_sc + (size_t)gyn * Pp;
-                        float* orow = tile_out + (size_t)(dty0 + b) * kTilePitch + dtx0;
+                        T* orow = tile_out + (size_t)(dty0 + b) * kTilePitch + dtx0;
 #pragma unroll
                         for (int j = 0; j < 4; ++j) {
                             const int a = x0 + j - sx;
                             if ((unsigned)a < (unsigned)dwx) {
-                                __stcs(orow + a, pn[j]);
-                                dest_pixel(A, acc, pn[j], a, b, srow, gx0n, L);
+                                const float v = store1<T>(orow + a, pn[j], sr_seed,
+                                                          (uint32_t)(orow + a - tile_out));
+                                dest_pixel(A, acc, v, a, b, srow, gx0n, L);
                             }
                         }
                     }
@@ -478,10 +566,10 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
             for (int b = b_lo + warp; b < b_hi; b += kWarps) {
                 const int j = b + sy;
                 const bool jin = (unsigned)j < (unsigned)WY;
-                float* orow = tile_out + (size_t)(dty0 + b) * kTilePitch + dtx0;
+                T* orow = tile_out + (size_t)(dty0 + b) * kTilePitch + dtx0;
                 for (int a = lane; a < dwx; a += 32) {
                     const int i = a + sx;
-                    if (!(jin && (unsigned)i < (unsigned)WX)) __stcs(orow + a, 0.0f);
+                    if (!(jin && (unsigned)i < (unsigned)WX)) store_zero(orow + a);
                 }
             }
         }
@@ -513,7 +601,9 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
                     const float So = own ? __uint_as_float(*q) : s_other_n(*q, cC, A.flags, 0u);
                     const float rhs =
                         rhs_pixel(lap, cC, So, gx, gy, gam, dwC, volC, repC, vx, vy, mrel);
-                    *q = __float_as_uint(cC + dtf * rhs);
+                    // the value the destination store will hold (pixel (x-sx, y-sy))
+                    const uint32_t pix = (uint32_t)((dty0 + y - sy) * kTilePitch + dtx0 + x - sx);
+                    *q = __float_as_uint(rounded<T>(cC + dtf * rhs, sr_seed, pix));
                     sW = cW;
                     sC = cC;
                     sE = cE;
@@ -533,14 +623,15 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
                 const int jr = j - y0 + 1;  // ps_s row of source row j
                 int gy = gy0n + b;
                 if (gy >= L) gy -= L;
-                float* orow = tile_out + (size_t)(dty0 + b) * kTilePitch + dtx0;
+                T* orow = tile_out + (size_t)(dty0 + b) * kTilePitch + dtx0;
                 uint32_t* srow = A.S_sc + (size_t)gy * Pp;
                 const uint32_t* row = ps_s + jr * PX + soff;
                 for (int a = lane; a < dwx; a += 32) {
                     const int i = a + sx;
                     const bool iin = (unsigned)i < (unsigned)WX;
                     const float pn = (jin && iin) ? __uint_as_float(row[i]) : 0.0f;
-                    __stcs(orow + a, pn);
+                    // already rounded when computed: the store keeps it exactly
+                    store1<T>(orow + a, pn, sr_seed, (uint32_t)(orow + a - tile_out));
                     dest_pixel(A, acc, pn, a, b, srow, gx0n, L);
                     float e = 0.0f, w = 0.0f, nn = 0.0f, ss = 0.0f;
                     if (jin) {
@@ -571,7 +662,7 @@ __device__ __forceinline__ void global_cell_v1(const pfb_step_args2d& A, int n, 
 }
 
 // One system's step for CTA `lb` of the `nb` CTAs that serve it.
-template <int K>
+template <int K, typename T>
 __device__ __forceinline__ void step_body(const pfb_step_args2d& A, int lb, int nb, char* smem) {
     const int tid = threadIdx.x;
 
@@ -599,12 +690,27 @@ __device__ __forceinline__ void step_body(const pfb_step_args2d& A, int lb, int 
     const int n = A.perm ? (int)A.perm[slot] : slot;
     const int cls = (int)A.cell_cls[n];
     switch (cls) {
-        case 0: staged_cell<0, K>(A, n, rank, smem, step, fm); break;
-        case 1: staged_cell<1, K>(A, n, rank, smem, step, fm); break;
-        case 2: staged_cell<2, K>(A, n, rank, smem, step, fm); break;
-        case 3: staged_cell<3, K>(A, n, rank, smem, step, fm); break;
-        case 4: global_cell_v1<4, K>(A, n, rank, smem, step, fm); break;
-        case 5: global_cell_v1<5, K>(A, n, rank, smem, step, fm); break;
+        case 0: staged_cell<0, K, T>(A, n, rank, smem, step, fm); break;
+        case 1: staged_cell<1, K, T>(A, n, rank, smem, step, fm); break;
+        case 2: staged_cell<2, K, T>(A, n, rank, smem, step, fm); break;
+        case 3: staged_cell<3, K, T>(A, n, rank, smem, step, fm); break;
+        case 4:
+            if constexpr (Store<T>::kHalf) {
+                // 16-bit pools: the global-memory classes are not provided
+                if (rank == 0 && tid == 0) atomicAdd(A.flags + PFB_FLAG_CLASS_UNSUPPORTED, 1u);
+                dev::cluster_wait();
+            } else {
+                global_cell_v1<4, K>(A, n, rank, smem, step, fm);
+            }
+            break;
+        case 5:
+            if constexpr (Store<T>::kHalf) {
+                if (rank == 0 && tid == 0) atomicAdd(A.flags + PFB_FLAG_CLASS_UNSUPPORTED, 1u);
+                dev::cluster_wait();
+            } else {
+                global_cell_v1<5, K>(A, n, rank, smem, step, fm);
+            }
+            break;
         default:
             if (rank == 0 && tid == 0) atomicAdd(A.flags + PFB_FLAG_CLASS_UNSUPPORTED, 1u);
             dev::cluster_wait();  // uniform over the cluster
@@ -612,11 +718,11 @@ __device__ __forceinline__ void step_body(const pfb_step_args2d& A, int lb, int 
     }
 }
 
-template <int K>
+template <int K, typename T = float>
 __global__ void __launch_bounds__(kThreads, PFB_STEP2D_MINB)
     k_step2d(const __grid_constant__ pfb_step_args2d A) {
     extern __shared__ __align__(128) char smem[];
-    step_body<K>(A, (int)blockIdx.x, (int)gridDim.x, smem);
+    step_body<K, T>(A, (int)blockIdx.x, (int)gridDim.x, smem);
 }
 
 // Many independent systems in one launch: system r is served by CTAs
@@ -644,19 +750,29 @@ __global__ void __launch_bounds__(kThreads, PFB_STEP2D_MINB)
     if (threadIdx.x < sizeof(pfb_step_args2d) / 8) dstw[threadIdx.x] = __ldg(srcw + threadIdx.x);
     __syncthreads();
     const int b0 = __ldg(block_start + r);
-    step_body<K>(sA, b - b0, __ldg(block_start + r + 1) - b0, smem);
+    step_body<K, float>(sA, b - b0, __ldg(block_start + r + 1) - b0, smem);
 }
 
 // ---------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------
-template <int K>
-static cudaError_t configure_one() {
-    cudaError_t e = cudaFuncSetAttribute(k_step2d<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+template <int K, typename T>
+static cudaError_t configure_pool() {
+    cudaError_t e = cudaFuncSetAttribute(k_step2d<K, T>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          step_smem_bytes(K));
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_step2d<K>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    return cudaFuncSetAttribute(k_step2d<K, T>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+}
+
+template <int K>
+static cudaError_t configure_one() {
+    cudaError_t e = configure_pool<K, float>();
     if (e != cudaSuccess) return e;
+    if constexpr (K != 8) {
+        if ((e = configure_pool<K, __half>()) != cudaSuccess) return e;
+        if ((e = configure_pool<K, __nv_bfloat16>()) != cudaSuccess) return e;
+    }
     e = cudaFuncSetAttribute(k_step2d_batch<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              step_smem_bytes(K));
     if (e != cudaSuccess) return e;
@@ -679,7 +795,7 @@ int step2d_configure_device() {
 
 int step2d_smem_bytes(int k) { return step_smem_bytes(k); }
 
-template <int K>
+template <int K, typename T = float>
 static cudaError_t launch_k(const pfb_step_args2d& A, cudaStream_t stream) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(A.N * K), 1, 1);
@@ -693,10 +809,10 @@ static cudaError_t launch_k(const pfb_step_args2d& A, cudaStream_t stream) {
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k_step2d<K>, A);
+    return cudaLaunchKernelEx(&cfg, k_step2d<K, T>, A);
 }
 
-int step2d_launch_variant(const pfb_step_args2d* a, int cluster, int variant,
+int step2d_launch_storage(const pfb_step_args2d* a, int cluster, int variant, int storage,
                           cudaStream_t stream) {
     if (!a) return set_error(PFB_E_ARG, "null step arguments");
     const pfb_step_args2d& A = *a;
@@ -720,11 +836,27 @@ int step2d_launch_variant(const pfb_step_args2d* a, int cluster, int variant,
     if (A.N == 0) return PFB_OK;
     int rc = step2d_configure_device();
     if (rc) return rc;
-    cudaError_t e = cluster == 2   ? launch_k<2>(A, stream)
-                    : cluster == 4 ? launch_k<4>(A, stream)
-                                   : launch_k<8>(A, stream);
+    if (storage != kStoreF32 && storage != kStoreF16 && storage != kStoreBF16)
+        return set_error(PFB_E_ARG, "unknown phi storage %d", storage);
+    if (storage != kStoreF32 && cluster == 8)
+        return set_error(PFB_E_CONFIG, "16-bit phi pools use clusters of 2 or 4");
+    cudaError_t e;
+    if (storage == kStoreF16)
+        e = cluster == 2 ? launch_k<2, __half>(A, stream) : launch_k<4, __half>(A, stream);
+    else if (storage == kStoreBF16)
+        e = cluster == 2 ? launch_k<2, __nv_bfloat16>(A, stream)
+                         : launch_k<4, __nv_bfloat16>(A, stream);
+    else
+        e = cluster == 2   ? launch_k<2>(A, stream)
+            : cluster == 4 ? launch_k<4>(A, stream)
+                           : launch_k<8>(A, stream);
     if (e != cudaSuccess) return set_error(PFB_E_CUDA, "step launch: %s", cudaGetErrorString(e));
     return PFB_OK;
+}
+
+int step2d_launch_variant(const pfb_step_args2d* a, int cluster, int variant,
+                          cudaStream_t stream) {
+    return step2d_launch_storage(a, cluster, variant, kStoreF32, stream);
 }
 
 template <int K>

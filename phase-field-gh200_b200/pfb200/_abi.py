@@ -109,7 +109,7 @@ class Params2D(C.Structure):
         ("cancer_fraction", C.c_double), ("v_A_sigma", C.c_double),
         ("phase_field_mobility", C.c_double),
         ("seed", C.c_ulonglong), ("polarity_seed", C.c_ulonglong),
-        ("full_moment_every", C.c_int),
+        ("full_moment_every", C.c_int), ("phi_storage", C.c_int),
     ]
 
 

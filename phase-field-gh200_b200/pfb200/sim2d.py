@@ -39,6 +39,7 @@ class SimParams2D:
     seed: int = 1234
     polarity_seed: int = 0
     full_moment_every: int = 100
+    phi_storage: int = 0  # 0 binary32, 1 binary16, 2 bfloat16 pools
 
     def to_c(self) -> Params2D:
         p = Params2D()
