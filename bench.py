@@ -408,12 +408,12 @@ WORKLOAD_CE = ("64 independent 2D periodic replicas, lattice side drawn from {38
                "default coefficients, f32 phi; one launch per step for all replicas")
 
 
-def ensemble_systems(base_seed: int):
+def ensemble_systems(base_seed: int, count: int = 64):
     import math
     import pfb200
     rng = np.random.default_rng(base_seed)
     ps, cs = [], []
-    for r in range(64):
+    for r in range(count):
         L = int(rng.choice([384, 512, 768, 1024]))
         rho = float(rng.uniform(0.5, 0.9))
         N = int(min(400, max(16, round(rho * L * L / (math.pi * RADIUS ** 2)))))
@@ -434,11 +434,14 @@ def run_ensemble(a):
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     torch.cuda.set_device(local)
-    ps, cs = ensemble_systems(1234 + 64 * rank)
+    ps, cs = ensemble_systems(1234 + 64 * rank, a.replicas)
+    for p in ps:
+        p.phi_storage = a.phi_storage
     ens = pfb200.Ensemble2D(ps, cs, device=local)
     chosen = ens.autotune(12)
     sites = sum(p.num_cells for p in ps) * 144 * 144
-    alg = sum(p.num_cells * 144 * 144 * 8 + p.L * p.L * 8 for p in ps)
+    phi_b = 2 if a.phi_storage else 4
+    alg = sum(p.num_cells * 144 * 144 * 2 * phi_b + p.L * p.L * 8 for p in ps)
 
     def barrier():
         if dist is not None:
@@ -464,14 +467,19 @@ def run_ensemble(a):
             "metric": "site-cell updates/s", "value": world * sites / (ms_step / 1000.0),
             "unit": "site-cell updates/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "vs_baseline": None,
+            "dtype": ("f32", "f32 arithmetic, f16 phi storage",
+                      "f32 arithmetic, bf16 phi storage")[a.phi_storage],
+            "data": "synthetic",
             "config": {"workload": WORKLOAD_CE, "replicas": len(ps),
+                       "phi_storage": ("binary32", "binary16", "bfloat16")[a.phi_storage],
                        "cells_total": sum(p.num_cells for p in ps), "sites_per_step": sites,
                        "sides": sorted({p.L for p in ps}), "cluster_ctas_per_cell": chosen,
                        "autotuned": True, "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,
-                         "kernel": f"pfb::k_step2d_batch<{chosen}>",
+                         "kernel": "pfb::k_step2d_batch<%d%s>" % (
+                             chosen, ("", ", __half", ", __nv_bfloat16")[a.phi_storage]),
                          "algorithmic_bytes_per_launch": alg, "peak_source": peak_src,
                          "duration_source": "CUDA events over the timed region / steps"},
             "replicas_one_at_a_time": {"ms_per_step": ms_serial,
@@ -496,6 +504,8 @@ def main():
     ap.add_argument("--cluster", type=int, default=2, help="CTAs per cell (2, 4 or 8)")
     ap.add_argument("--variant", type=int, default=0, help="kernel variant (0 = default)")
     ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--replicas", type=int, default=64,
+                    help="ensemble workload: the first R of its 64 replicas (profiling cases)")
     ap.add_argument("--phi-storage", type=int, default=0, choices=[0, 1, 2],
                     help="2D phi pools: 0 binary32 (reference layout), 1 binary16, 2 bfloat16")
     ap.add_argument("--cpu-steps", type=int, default=int(os.environ.get("PFB_CPU_STEPS", "6")))

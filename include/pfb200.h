@@ -337,14 +337,17 @@ void* pfb_sim2d_stream(pfb_sim2d* s);
 typedef struct pfb_ens2d pfb_ens2d;
 
 /* params[r], cx[r], cy[r] (params[r].num_cells centres each) describe
- * system r; every system gets a fresh start as pfb_sim2d_create. */
+ * system r; every system gets a fresh start as pfb_sim2d_create. All systems
+ * must share one phi_storage (one launch serves them all); 16-bit pools
+ * limit the cluster to 2 or 4 CTAs per cell. */
 pfb_ens2d* pfb_ens2d_create(int R, const pfb_params2d* params, const float* const* cx,
                             const float* const* cy, int device);
 void pfb_ens2d_destroy(pfb_ens2d* e);
 int pfb_ens2d_num_systems(const pfb_ens2d* e);
 int pfb_ens2d_set_cluster(pfb_ens2d* e, int cluster);
-/* Times `steps` steps with clusters of 2, 4 and 8 CTAs per cell and keeps the
- * fastest (the ensemble's autotuner; the timed steps advance the systems). */
+/* Times `steps` steps with clusters of 2, 4 and 8 CTAs per cell (2 and 4 with
+ * 16-bit pools) and keeps the fastest (the ensemble's autotuner; the timed
+ * steps advance the systems). */
 int pfb_ens2d_autotune(pfb_ens2d* e, int steps, int* chosen);
 int pfb_ens2d_advance(pfb_ens2d* e, int steps);
 /* The same steps launched one system at a time (the baseline the batched

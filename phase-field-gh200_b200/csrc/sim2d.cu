@@ -550,6 +550,7 @@ struct pfb_ens2d {
     std::vector<int> order;  // launch order of the systems (largest first)
     int device = 0;
     int cluster = kDefaultCluster;
+    int storage = 0;  // phi pool type shared by every system
     long long steps_done = 0;
     cudaStream_t stream = nullptr;
     pfb_step_args2d* d_args = nullptr;  // 6 slots x R records
@@ -601,7 +602,7 @@ struct pfb_ens2d {
 
     int launch_slot(int slot) {
         return step2d_launch_batch(d_args + (size_t)slot * R(), d_start, R(), total_blocks, cluster,
-                                   stream);
+                                   storage, stream);
     }
 
     int build_graph() {
@@ -653,7 +654,7 @@ struct pfb_ens2d {
             const int slot = (int)(steps_done % 6);
             for (pfb_sim2d* s : sims) {
                 const pfb_step_args2d a = s->args_for_slot(slot);
-                const int rc = step2d_launch_variant(&a, cluster, 0, stream);
+                const int rc = step2d_launch_storage(&a, cluster, 0, storage, stream);
                 if (rc) return rc;
             }
             ++steps_done;
@@ -678,9 +679,10 @@ pfb_ens2d* pfb_ens2d_create(int R, const pfb_params2d* params, const float* cons
         return nullptr;
     }
     e->device = device;
+    e->storage = params[0].phi_storage;
     for (int r = 0; r < R; ++r) {
-        if (params[r].phi_storage != 0) {
-            set_error(PFB_E_CONFIG, "the batched ensemble uses binary32 pools");
+        if (params[r].phi_storage != e->storage) {
+            set_error(PFB_E_CONFIG, "every system of an ensemble needs the same phi_storage");
             delete e;
             return nullptr;
         }
@@ -714,6 +716,8 @@ int pfb_ens2d_set_cluster(pfb_ens2d* e, int cluster) {
     if (cluster == 0) cluster = kDefaultCluster;
     if (cluster != 2 && cluster != 4 && cluster != 8)
         return set_error(PFB_E_CONFIG, "cluster must be 2, 4 or 8");
+    if (cluster == 8 && e->storage)
+        return set_error(PFB_E_CONFIG, "16-bit phi pools run with clusters of 2 or 4");
     if (cluster != e->cluster) {
         e->cluster = cluster;
         e->tables_ready = false;
@@ -791,6 +795,7 @@ int pfb_ens2d_autotune(pfb_ens2d* e, int steps, int* chosen) {
     int best_k = e->cluster;
     const int ks[3] = {2, 4, 8};
     for (int k : ks) {
+        if (k == 8 && e->storage) continue;
         int rc = pfb_ens2d_set_cluster(e, k);
         if (rc) return rc;
         double ms = 0.0;

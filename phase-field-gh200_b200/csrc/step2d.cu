@@ -727,8 +727,9 @@ __global__ void __launch_bounds__(kThreads, PFB_STEP2D_MINB)
 
 // Many independent systems in one launch: system r is served by CTAs
 // [block_start[r], block_start[r+1]) (multiples of K, so clusters never
-// straddle systems); its arguments are copied into shared memory.
-template <int K>
+// straddle systems); its arguments are copied into shared memory. All
+// systems of one launch share the pool storage type T.
+template <int K, typename T = float>
 __global__ void __launch_bounds__(kThreads, PFB_STEP2D_MINB)
     k_step2d_batch(const pfb_step_args2d* __restrict__ args, const int* __restrict__ block_start,
                    int R) {
@@ -750,7 +751,7 @@ __global__ void __launch_bounds__(kThreads, PFB_STEP2D_MINB)
     if (threadIdx.x < sizeof(pfb_step_args2d) / 8) dstw[threadIdx.x] = __ldg(srcw + threadIdx.x);
     __syncthreads();
     const int b0 = __ldg(block_start + r);
-    step_body<K, float>(sA, b - b0, __ldg(block_start + r + 1) - b0, smem);
+    step_body<K, T>(sA, b - b0, __ldg(block_start + r + 1) - b0, smem);
 }
 
 // ---------------------------------------------------------------------------
@@ -762,7 +763,13 @@ static cudaError_t configure_pool() {
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          step_smem_bytes(K));
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_step2d<K, T>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    e = cudaFuncSetAttribute(k_step2d<K, T>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_step2d_batch<K, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             step_smem_bytes(K));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_step2d_batch<K, T>,
+                                cudaFuncAttributePreferredSharedMemoryCarveout, 100);
 }
 
 template <int K>
@@ -773,11 +780,7 @@ static cudaError_t configure_one() {
         if ((e = configure_pool<K, __half>()) != cudaSuccess) return e;
         if ((e = configure_pool<K, __nv_bfloat16>()) != cudaSuccess) return e;
     }
-    e = cudaFuncSetAttribute(k_step2d_batch<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             step_smem_bytes(K));
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_step2d_batch<K>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                100);
+    return cudaSuccess;
 }
 
 int step2d_configure_device() {
@@ -859,7 +862,7 @@ int step2d_launch_variant(const pfb_step_args2d* a, int cluster, int variant,
     return step2d_launch_storage(a, cluster, variant, kStoreF32, stream);
 }
 
-template <int K>
+template <int K, typename T = float>
 static cudaError_t launch_batch_k(const pfb_step_args2d* args, const int* block_start, int R,
                                   int total_blocks, cudaStream_t stream) {
     cudaLaunchConfig_t cfg = {};
@@ -874,23 +877,35 @@ static cudaError_t launch_batch_k(const pfb_step_args2d* args, const int* block_
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k_step2d_batch<K>, args, block_start, R);
+    return cudaLaunchKernelEx(&cfg, k_step2d_batch<K, T>, args, block_start, R);
 }
 
 int step2d_launch_batch(const pfb_step_args2d* d_args, const int* d_block_start, int R,
-                        int total_blocks, int cluster, cudaStream_t stream) {
+                        int total_blocks, int cluster, int storage, cudaStream_t stream) {
     if (!d_args || !d_block_start || R <= 0 || total_blocks < 0)
         return set_error(PFB_E_ARG, "invalid batch arguments");
     if (cluster == 0) cluster = kDefaultCluster;
     if (cluster != 2 && cluster != 4 && cluster != 8)
         return set_error(PFB_E_CONFIG, "cluster must be 2, 4 or 8");
+    if (storage < 0 || storage > 2) return set_error(PFB_E_ARG, "storage must be 0, 1 or 2");
+    if (storage && cluster == 8)
+        return set_error(PFB_E_CONFIG, "16-bit phi pools run with clusters of 2 or 4");
     if (total_blocks % cluster) return set_error(PFB_E_ARG, "block count must be a multiple of K");
     if (total_blocks == 0) return PFB_OK;
     int rc = step2d_configure_device();
     if (rc) return rc;
-    cudaError_t e = cluster == 2   ? launch_batch_k<2>(d_args, d_block_start, R, total_blocks, stream)
-                    : cluster == 4 ? launch_batch_k<4>(d_args, d_block_start, R, total_blocks, stream)
-                                   : launch_batch_k<8>(d_args, d_block_start, R, total_blocks, stream);
+    cudaError_t e;
+    if (storage == kStoreF16)
+        e = cluster == 2 ? launch_batch_k<2, __half>(d_args, d_block_start, R, total_blocks, stream)
+                         : launch_batch_k<4, __half>(d_args, d_block_start, R, total_blocks, stream);
+    else if (storage == kStoreBF16)
+        e = cluster == 2
+                ? launch_batch_k<2, __nv_bfloat16>(d_args, d_block_start, R, total_blocks, stream)
+                : launch_batch_k<4, __nv_bfloat16>(d_args, d_block_start, R, total_blocks, stream);
+    else
+        e = cluster == 2   ? launch_batch_k<2>(d_args, d_block_start, R, total_blocks, stream)
+            : cluster == 4 ? launch_batch_k<4>(d_args, d_block_start, R, total_blocks, stream)
+                           : launch_batch_k<8>(d_args, d_block_start, R, total_blocks, stream);
     if (e != cudaSuccess) return set_error(PFB_E_CUDA, "batch launch: %s", cudaGetErrorString(e));
     return PFB_OK;
 }

@@ -153,7 +153,9 @@ def test_storage_cluster_limits():
     s.close()
 
 
-def test_ensemble_rejects_16bit_pools():
+def test_ensemble_rejects_mixed_storage():
     p = params(320, 12, R=12.0, seed=5, phi_storage=1)
+    q = params(320, 12, R=12.0, seed=6, phi_storage=0)
+    c = pfb200.palmieri_centres(12, 320, 24.0, 5)
     with pytest.raises(RuntimeError):
-        pfb200.Ensemble2D([p], [pfb200.palmieri_centres(12, 320, 24.0, 5)])
+        pfb200.Ensemble2D([p, q], [c, c])
