@@ -1,0 +1,74 @@
+/* pfb200_surrogate.h -- learned relaxation surrogate of the 2D update.
+ *
+ * No counterpart in the reference: the reference relaxes every system with
+ * the explicit Euler step only. This interface adds (1) 3x3 "same"
+ * convolutions on bfloat16 activations with binary32 accumulation on the
+ * tcgen05 tensor cores (forward, data gradient, weight gradient), (2) a small
+ * U-Net built from them that maps a 64 x 64 crop around one cell (its phi and
+ * the sum of the other cells' phi^2) to the cell's phi after a fixed number of
+ * passive relaxation steps, with its training step, and (3) the jump of a
+ * pfb_sim2d system by that network, after which the plain step resumes and
+ * judges the result by its residual.
+ *
+ * Activation layout ("padded NHWC"): image b of H x W pixels and C channels
+ * occupies (H + 2) * (W + 2) * C bfloat16 values, position
+ * q = (y + 1) * (W + 2) + (x + 1) for pixel (y, x), channels innermost, with a
+ * zero border one pixel wide. Kernels never write the top and bottom border
+ * rows, so buffers start zeroed. All buffers 16-byte aligned.
+ *
+ * Return values: PFB_OK (0) or a negative PFB_E_* code (pfb200.h), with the
+ * text in pfb_last_error(). */
+#ifndef PFB200_SURROGATE_H
+#define PFB200_SURROGATE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "pfb200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- convolutions ---------------------------------------------------------- */
+
+/* out = conv3x3(x, W) (+ bias[co]) (ReLU if relu) (* (gate > 0) if gate),
+ * computed for `batch` images of H x W; x has cin channels, the output cout.
+ * y receives bfloat16 (round to nearest), y_f32 binary32; either may be null
+ * but not both. w_packed comes from pfb_conv3x3_pack. Built channel pairs
+ * (cin, cout): (16, 16), (16, 32), (32, 16), (32, 32). The border columns of
+ * the output rows are written as zero. */
+int pfb_conv3x3_forward(const void* x, void* y, float* y_f32, const void* w_packed,
+                        const float* bias, const void* gate, int batch, int H, int W, int cin,
+                        int cout, int relu, void* stream);
+
+/* Pack binary32 weights w_oihw[cout][cin][3][3] into the bfloat16 operand
+ * layout of pfb_conv3x3_forward (9 * cin * cout values). transpose != 0 packs
+ * the flipped, transposed weights of the data gradient: running
+ * pfb_conv3x3_forward with them on dY (cout channels) gives dX (cin
+ * channels). */
+int pfb_conv3x3_pack(const float* w_oihw, void* w_packed, int cin, int cout, int transpose,
+                     void* stream);
+
+/* Bytes of the workspace pfb_conv3x3_wgrad needs for these sizes: binary32
+ * partial sums, one block per CTA, added afterwards in a fixed order. */
+size_t pfb_conv3x3_wgrad_workspace(int batch, int H, int W, int cx, int cy);
+
+/* dw_oihw[cy][cx][3][3] = sum over images and pixels of dY[q][co] *
+ * x[q + tap][ci], and db[co] = sum dY[q][co] (db may be null); x has cx
+ * channels, dy cy (its border must be zero). Overwrites dw and db.
+ * Deterministic. Built pairs (cx, cy) as for the forward pass. */
+int pfb_conv3x3_wgrad(const void* x, const void* dy, float* workspace, size_t workspace_bytes,
+                      float* dw_oihw, float* db, int batch, int H, int W, int cx, int cy,
+                      void* stream);
+
+/* Sticky device status of the convolution kernels: bit 0 = a wait for the
+ * tensor-core MMAs gave up (the kernel skipped its output). clear != 0
+ * resets it. */
+int pfb_conv_status(unsigned* out, int clear);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PFB200_SURROGATE_H */

@@ -35,9 +35,10 @@ COMMON = [
     "-I", str(INCLUDE),
 ]
 SOURCES = ["step2d.cu", "init2d.cu", "sim2d.cu", "host2d.cpp", "measure3d.cu", "update3d.cu",
-           "misc3d.cu", "sim3d.cu", "host3d.cpp"]
+           "misc3d.cu", "sim3d.cu", "host3d.cpp", "conv2d_tc.cu"]
 HEADERS = ["pfb_common.cuh", "device_util.cuh", "pfb_internal.h", "step2d_common.cuh",
-           "pfb3d_common.cuh", "ring3d.cuh", "storage2d.cuh"]
+           "pfb3d_common.cuh", "ring3d.cuh", "storage2d.cuh",
+           "tc_util.cuh"]
 
 
 def _newer(target: Path, deps: list[Path]) -> bool:
@@ -71,7 +72,8 @@ def build(force: bool = False, verbose: bool = False, ptxas_report: bool = False
         force = True
     lib_path.parent.mkdir(parents=True, exist_ok=True)
     obj_dir.mkdir(parents=True, exist_ok=True)
-    headers = [CSRC / h for h in HEADERS] + [INCLUDE / "pfb200.h", INCLUDE / "pfb200_3d.h"]
+    headers = [CSRC / h for h in HEADERS] + [INCLUDE / "pfb200.h", INCLUDE / "pfb200_3d.h",
+                                                 INCLUDE / "pfb200_surrogate.h"]
     objs = []
     relink = force or not lib_path.exists()
     for src in SOURCES:

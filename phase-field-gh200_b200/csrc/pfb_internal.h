@@ -51,6 +51,16 @@ int verify_S(const uint32_t* S, size_t n, uint32_t* out_max, cudaStream_t s);
 int pack_traj2d(const pfb_cell2d* cell, const uint8_t* cls, pfb_traj_cell2d* out, int N, int L,
                 cudaStream_t s);
 
+// conv2d_tc.cu: 3x3 same convolutions on padded-NHWC bfloat16 activations
+int conv3x3_fwd(const void* x, void* y, float* yf, const void* wp, const float* bias,
+                const void* gate, int B, int H, int W, int cin, int cout, int relu,
+                cudaStream_t s);
+size_t conv3x3_wgrad_workspace(int B, int H, int W, int cx, int cy);
+int conv3x3_wgrad(const void* x, const void* dy, float* workspace, size_t workspace_bytes,
+                  float* dw, float* db, int B, int H, int W, int cx, int cy, cudaStream_t s);
+int conv3x3_pack(const float* w, void* packed, int cin, int cout, int transpose, cudaStream_t s);
+int conv_read_status(unsigned* out, int clear);
+
 namespace p3 {
 // measure3d.cu / update3d.cu / misc3d.cu (pfb200_3d.h records)
 int measure3d_launch(const pfb_measure_args3d* a, cudaStream_t stream);

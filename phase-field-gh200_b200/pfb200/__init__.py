@@ -9,6 +9,7 @@ from ._abi import (CELL_DTYPE, CLASSES, FLAG_COUNT, FLAG_NAMES, LIB_PATH, TILE_A
                    TILE_PITCH, TRAJ_DTYPE, Cell2D, Params2D, PfbError, StepArgs2D, TrajCell2D,
                    check, exported_symbols, lib, ptr)
 from . import _abi3d  # registers the 3D entry points before the library loads
+from . import _abi_sur  # registers the surrogate entry points
 from ._abi3d import (CELL3D_DTYPE, FLAG3D_COUNT, FLAG3D_NAMES, Cell3D, Layout3D, MeasureArgs3D,
                      UpdateArgs3D)
 from .sim2d import (Sim2D, SimParams2D, domain_side_for, fatal, flags_report,
