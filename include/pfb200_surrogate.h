@@ -62,6 +62,24 @@ int pfb_conv3x3_wgrad(const void* x, const void* dy, float* workspace, size_t wo
                       float* dw_oihw, float* db, int batch, int H, int W, int cx, int cy,
                       void* stream);
 
+/* pfb_conv3x3_wgrad without a caller workspace. No counterpart in the
+ * reference. For callers that cannot allocate device memory for this
+ * library: hosts whose device memory belongs to their own pool allocator (a
+ * training framework's caching allocator, a serving engine's preallocated
+ * arena) and that forbid a raw cudaMalloc, which would take memory outside
+ * their budget and, being synchronizing, stall their streams. The partial
+ * sums live in a fixed 4 MiB array of the library that every GPU loading it
+ * holds until exit; sizes needing more (pfb_conv3x3_wgrad_workspace above
+ * 4 MiB, e.g. more than 56 images of 64 x 64 with 32 -> 32 channels) are
+ * rejected with PFB_E_ARG. Nothing in the array has to start at zero (each
+ * call overwrites what it reads). The first call on a device looks up the
+ * array's device address with that device current; make that first call
+ * before any stream capture. Calls that overlap on the GPU share the array
+ * and race: serialise them. Allocates nothing; same results as
+ * pfb_conv3x3_wgrad. */
+int pfb_conv3x3_wgrad_noalloc(const void* x, const void* dy, float* dw_oihw, float* db,
+                              int batch, int H, int W, int cx, int cy, void* stream);
+
 /* Sticky device status of the convolution kernels: bit 0 = a wait for the
  * tensor-core MMAs gave up (the kernel skipped its output). clear != 0
  * resets it. */

@@ -32,6 +32,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 
 #include "pfb_internal.h"
 #include "tc_util.cuh"
@@ -565,3 +566,72 @@ int pfb_conv3x3_wgrad(const void* x, const void* dy, float* workspace, size_t wo
 int pfb_conv_status(unsigned* out, int clear) { return pfb::conv_read_status(out, clear); }
 
 }  // extern "C"
+
+// ---- weight gradient without caller workspace -----------------------------------
+//
+// Some callers cannot hand this library device memory for scratch: hosts
+// whose device memory is owned by their own pool allocator (a training
+// framework's caching allocator, a serving engine's preallocated arena) and
+// that forbid a raw cudaMalloc, which would take memory outside their budget
+// and, being synchronizing, stall their streams. For them the weight gradient
+// keeps its partial sums in this fixed array instead, which every GPU that
+// loads the library holds until the process exits. Calls that overlap on the
+// GPU (two streams, or two host threads) share the array and race.
+
+using namespace pfb;
+
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = (size_t)4 << 20;  // 4 MiB per device
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) float g_wgrad_scratch[kNoAllocScratchBytes / sizeof(float)];
+
+std::mutex g_scratch_mutex;
+float* g_scratch_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of g_wgrad_scratch on the current device, looked up once per
+// device (the host-side name of the array is not a device address).
+int scratch_on_current_device(float** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return set_error(PFB_E_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
+    if (dev < 0 || dev >= kNoAllocMaxDevices)
+        return set_error(PFB_E_CONFIG, "device %d beyond the %d supported", dev, kNoAllocMaxDevices);
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_ptr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_wgrad_scratch);
+        if (e != cudaSuccess || !p)
+            return set_error(PFB_E_CUDA, "scratch address: %s", cudaGetErrorString(e));
+        g_scratch_ptr[dev] = static_cast<float*>(p);
+    }
+    *out = g_scratch_ptr[dev];
+    return PFB_OK;
+}
+
+}  // namespace
+
+extern "C" int pfb_conv3x3_wgrad_noalloc(const void* x, const void* dy, float* dw_oihw, float* db,
+                                         int batch, int H, int W, int cx, int cy, void* stream) {
+    clear_error();
+    if (!x || !dy || !dw_oihw) return set_error(PFB_E_ARG, "conv3x3_wgrad_noalloc: null buffer");
+    if (!shape_ok(batch, H, W))
+        return set_error(PFB_E_ARG, "conv3x3_wgrad_noalloc: bad shape %dx%dx%d", batch, H, W);
+    if (cx <= 0 || cy <= 0 || cx > 64 || cy > 64)
+        return set_error(PFB_E_CONFIG, "conv3x3_wgrad_noalloc: channels %d, %d not built", cx, cy);
+    const size_t need = conv3x3_wgrad_workspace(batch, H, W, cx, cy);
+    if (need > kNoAllocScratchBytes)
+        return set_error(PFB_E_ARG,
+                         "conv3x3_wgrad_noalloc: %d images of %dx%d with %d -> %d channels need "
+                         "%zu bytes of scratch, above its fixed %zu bytes (split the batch, or "
+                         "use pfb_conv3x3_wgrad with a workspace)",
+                         batch, H, W, cx, cy, need, kNoAllocScratchBytes);
+    float* scratch = nullptr;
+    const int rc = scratch_on_current_device(&scratch);
+    if (rc) return rc;
+    // every CTA overwrites its whole block of partial sums before the reduction
+    // reads it, so nothing in the shared array has to start at zero
+    return conv3x3_wgrad(x, dy, scratch, kNoAllocScratchBytes, dw_oihw, db, batch, H, W, cx, cy,
+                         static_cast<cudaStream_t>(stream));
+}

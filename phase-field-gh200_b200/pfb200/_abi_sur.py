@@ -13,5 +13,6 @@ _abi._SIGS.update({
     "pfb_conv3x3_pack": (I, [P, P, I, I, I, P]),
     "pfb_conv3x3_wgrad_workspace": (C.c_size_t, [I, I, I, I, I]),
     "pfb_conv3x3_wgrad": (I, [P, P, P, C.c_size_t, P, P, I, I, I, I, I, P]),
+    "pfb_conv3x3_wgrad_noalloc": (I, [P, P, P, P, I, I, I, I, I, P]),
     "pfb_conv_status": (I, [C.POINTER(C.c_uint), I]),
 })
