@@ -85,6 +85,73 @@ int pfb_conv3x3_wgrad_noalloc(const void* x, const void* dy, float* dw_oihw, flo
  * resets it. */
 int pfb_conv_status(unsigned* out, int clear);
 
+/* ---- relaxation measurements and crops of a pfb_sim2d system ---------------
+ * (binary32 pools only; PFB_E_CONFIG otherwise) */
+
+/* Advance `s` by one step and measure that step's residual over every cell:
+ * linf = max |phi_n^{k+1} - phi_n^k| / dt over the lattice sites of the
+ * cell's old and new windows (world coordinates), rms = the root mean square
+ * of the same quantity over those sites. Either output may be null. */
+int pfb_sim2d_residual_step(pfb_sim2d* s, double* linf, double* rms);
+
+/* Network input of every cell of `s` (num_cells padded 66 x 66 images of 16
+ * bfloat16 channels: phi_n and the sum over the other cells of
+ * min(phi_m^2, 4), on the 64 x 64 lattice crop centred at the cell's
+ * rounded centroid), the binary32 phi_n crops (num_cells x 64 x 64, may be
+ * null) and the crop origins (num_cells x 2 ints, x then y). Device
+ * buffers; runs on the system's stream. */
+int pfb_sur2d_extract(pfb_sim2d* s, void* x0, float* phi_crop, int* origins);
+
+/* out = phi_n on the 64 x 64 crops at `origins` (binary32), minus `minus`
+ * when it is not null (e.g. the crops of an earlier step: the increment). */
+int pfb_sur2d_crop_phi(pfb_sim2d* s, const int* origins, const float* minus, float* out);
+
+/* phi_n += dphi (num_cells x 64 x 64) at the crop sites inside each cell's
+ * window, then the cells' moments and the current aggregate are rebuilt from
+ * the edited field. */
+int pfb_sur2d_insert(pfb_sim2d* s, const int* origins, const float* dphi);
+
+/* ---- the surrogate network -------------------------------------------------
+ * A U-Net of eight 3x3 convolutions of width 32 (ReLU; 2x2 average pool and
+ * nearest upsampling with a skip connection between 64^2 and 32^2) mapping a
+ * crop from pfb_sur2d_extract to the increment of phi_n over the relaxation
+ * interval it was trained on. bfloat16 activations, binary32 accumulation,
+ * master weights, gradients and Adam moments. */
+typedef struct pfb_sur2d pfb_sur2d;
+
+/* Buffers for batches of up to max_batch crops; weights He-normal from
+ * `seed` (the last layer zero: the untrained network predicts no change). */
+pfb_sur2d* pfb_sur2d_create(int max_batch, unsigned long long seed, int device);
+void pfb_sur2d_destroy(pfb_sur2d* n);
+/* Number of binary32 parameters (weights [cout][cin][3][3] then bias, per
+ * layer in order; padded channels included). */
+long long pfb_sur2d_num_params(const pfb_sur2d* n);
+int pfb_sur2d_get_params(pfb_sur2d* n, float* out);     /* host buffer */
+int pfb_sur2d_set_params(pfb_sur2d* n, const float* in); /* resets Adam */
+int pfb_sur2d_get_grads(pfb_sur2d* n, float* out);      /* host buffer */
+
+/* dphi (batch x 64 x 64, binary32) = network(x0) for `batch` device crops. */
+int pfb_sur2d_predict(pfb_sur2d* n, const void* x0, float* dphi, int batch);
+
+/* Gather crops idx[0..batch) of a device training set (x_all: inputs as
+ * pfb_sur2d_extract writes them, t_all: target increments, 64 x 64 each),
+ * compute the mean-squared error of channel 0 and every parameter's
+ * gradient (no update). loss may be null (no host synchronisation). */
+int pfb_sur2d_loss_grad(pfb_sur2d* n, const void* x_all, const float* t_all, const int* idx,
+                        int batch, double* loss);
+/* pfb_sur2d_loss_grad followed by one Adam step (beta 0.9, 0.999, eps 1e-8)
+ * with learning rate lr. */
+int pfb_sur2d_train_step(pfb_sur2d* n, const void* x_all, const float* t_all, const int* idx,
+                         int batch, float lr, double* loss);
+int pfb_sur2d_sync(pfb_sur2d* n);
+
+/* Jump every cell of `s` by the network (extract, predict, insert, rebuild)
+ * on the system's stream; returns after it completed. */
+int pfb_sur2d_jump(pfb_sur2d* n, pfb_sim2d* s);
+
+/* Device milliseconds per forward pass over `batch` crops (CUDA events). */
+int pfb_sur2d_bench_forward(pfb_sur2d* n, int batch, int iters, double* ms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -51,6 +51,29 @@ int verify_S(const uint32_t* S, size_t n, uint32_t* out_max, cudaStream_t s);
 int pack_traj2d(const pfb_cell2d* cell, const uint8_t* cls, pfb_traj_cell2d* out, int N, int L,
                 cudaStream_t s);
 
+// sim2d.cu: device-side view of a pfb_sim2d for the relaxation tools
+struct Sim2DView {
+    float* phi_cur;            // pool of the current step (binary32 pools)
+    float* phi_prev;           // the other pool (the previous step after a step)
+    pfb_cell2d* cells;
+    const pfb_cell2d* cells_prev;  // records saved by sim2d_step_keep_prev
+    uint8_t* cls;
+    uint32_t* S_cur;           // aggregate of the current step
+    int N, L, P;
+    double dt;
+    int storage;
+    cudaStream_t stream;
+    long long step;
+    int device;
+};
+int sim2d_view(pfb_sim2d* s, Sim2DView* v);
+int sim2d_rebuild(pfb_sim2d* s);
+int sim2d_step_keep_prev(pfb_sim2d* s);
+// relax2d.cu: crops of the current state (network input, origins) and the
+// insertion of predicted increments (followed by a rebuild)
+int relax_extract(pfb_sim2d* s, void* x0, float* phi_crop, int* origins);
+int relax_insert(pfb_sim2d* s, const int* origins, const float* dphi);
+
 // conv2d_tc.cu: 3x3 same convolutions on padded-NHWC bfloat16 activations
 int conv3x3_fwd(const void* x, void* y, float* yf, const void* wp, const float* bias,
                 const void* gate, int B, int H, int W, int cin, int cout, int relu,

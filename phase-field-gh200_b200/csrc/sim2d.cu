@@ -34,6 +34,7 @@ struct pfb_sim2d {
     float* d_phi[2] = {nullptr, nullptr};
     uint32_t* d_S = nullptr;
     pfb_cell2d* d_cell = nullptr;
+    pfb_cell2d* d_cell_prev = nullptr;  // records before the last residual step
     uint8_t* d_cls = nullptr;
     unsigned long long* d_cursor = nullptr;
     unsigned long long* d_step = nullptr;
@@ -61,6 +62,7 @@ struct pfb_sim2d {
         cudaFree(d_step);
         cudaFree(d_flags);
         cudaFree(d_traj);
+        cudaFree(d_cell_prev);
     }
 
     pfb_step_args2d args_for_slot(int slot) const {
@@ -173,6 +175,7 @@ struct pfb_sim2d {
         PFB_CU(cudaMalloc(&d_step, 2 * sizeof(unsigned long long)), "alloc step");
         PFB_CU(cudaMalloc(&d_flags, PFB_FLAG_COUNT * sizeof(uint32_t)), "alloc flags");
         PFB_CU(cudaMalloc(&d_traj, (size_t)N * sizeof(pfb_traj_cell2d)), "alloc traj");
+        PFB_CU(cudaMalloc(&d_cell_prev, (size_t)N * sizeof(pfb_cell2d)), "alloc cells");
         PFB_CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
         PFB_CU(cudaMemsetAsync(d_cursor, 0, 2 * sizeof(unsigned long long), stream), "memset");
         PFB_CU(cudaMemsetAsync(d_step, 0, 2 * sizeof(unsigned long long), stream), "memset");
@@ -811,3 +814,63 @@ int pfb_ens2d_autotune(pfb_ens2d* e, int steps, int* chosen) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Device-side access for the relaxation tools (residual, surrogate jump):
+// the current pool, the previous one, the cell records and the aggregate.
+// ---------------------------------------------------------------------------
+namespace pfb {
+
+int sim2d_view(pfb_sim2d* s, Sim2DView* v) {
+    if (!s || !v) return set_error(PFB_E_ARG, "sim2d_view: null argument");
+    const int pin = (int)(s->steps_done % 2), rot = (int)(s->steps_done % 3);
+    v->phi_cur = s->d_phi[pin];
+    v->phi_prev = s->d_phi[1 - pin];
+    v->cells = s->d_cell;
+    v->cells_prev = s->d_cell_prev;
+    v->cls = s->d_cls;
+    v->S_cur = s->d_S + (size_t)rot * s->s_words;
+    v->N = s->N;
+    v->L = s->L;
+    v->P = s->P;
+    v->dt = s->p.dt;
+    v->storage = s->p.phi_storage;
+    v->stream = s->stream;
+    v->step = s->steps_done;
+    v->device = s->device;
+    return PFB_OK;
+}
+
+// After the current binary32 pool was edited on the device: recompute the
+// cells' moments and support from it and rebuild the current aggregate slot
+// (the next slot, the following step's scatter target, is cleared too).
+int sim2d_rebuild(pfb_sim2d* s) {
+    if (!s) return set_error(PFB_E_ARG, "sim2d_rebuild: null system");
+    if (s->p.phi_storage) return set_error(PFB_E_CONFIG, "rebuild needs binary32 pools");
+    PFB_CU(cudaSetDevice(s->device), "cudaSetDevice");
+    s->drop_graph();
+    const int pin = (int)(s->steps_done % 2), rot = (int)(s->steps_done % 3);
+    int rc = init_moments2d(s->d_cell, s->d_cls, s->d_phi[pin], s->N, s->stream);
+    if (rc) return rc;
+    PFB_CU(cudaMemsetAsync(s->d_S + (size_t)rot * s->s_words, 0, s->s_words * sizeof(uint32_t),
+                           s->stream), "clear S");
+    PFB_CU(cudaMemsetAsync(s->d_S + (size_t)((rot + 1) % 3) * s->s_words, 0,
+                           s->s_words * sizeof(uint32_t), s->stream), "clear S");
+    return scatter_all2d(s->d_phi[pin], s->d_cell, s->d_cls, s->d_S + (size_t)rot * s->s_words, s->N,
+                         s->L, s->P, s->d_flags, s->stream);
+}
+
+// One step with the cell records saved first (for a residual between the two
+// pools).
+int sim2d_step_keep_prev(pfb_sim2d* s) {
+    if (!s) return set_error(PFB_E_ARG, "sim2d_step_keep_prev: null system");
+    PFB_CU(cudaSetDevice(s->device), "cudaSetDevice");
+    PFB_CU(cudaMemcpyAsync(s->d_cell_prev, s->d_cell, (size_t)s->N * sizeof(pfb_cell2d),
+                           cudaMemcpyDeviceToDevice, s->stream), "save cells");
+    const int rc = s->launch_one((int)(s->steps_done % 6));
+    if (rc) return rc;
+    s->steps_done += 1;
+    return PFB_OK;
+}
+
+}  // namespace pfb

@@ -15,4 +15,20 @@ _abi._SIGS.update({
     "pfb_conv3x3_wgrad": (I, [P, P, P, C.c_size_t, P, P, I, I, I, I, I, P]),
     "pfb_conv3x3_wgrad_noalloc": (I, [P, P, P, P, I, I, I, I, I, P]),
     "pfb_conv_status": (I, [C.POINTER(C.c_uint), I]),
+    "pfb_sim2d_residual_step": (I, [P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "pfb_sur2d_extract": (I, [P, P, P, P]),
+    "pfb_sur2d_crop_phi": (I, [P, P, P, P]),
+    "pfb_sur2d_insert": (I, [P, P, P]),
+    "pfb_sur2d_create": (P, [I, C.c_ulonglong, I]),
+    "pfb_sur2d_destroy": (None, [P]),
+    "pfb_sur2d_num_params": (C.c_longlong, [P]),
+    "pfb_sur2d_get_params": (I, [P, P]),
+    "pfb_sur2d_set_params": (I, [P, P]),
+    "pfb_sur2d_get_grads": (I, [P, P]),
+    "pfb_sur2d_predict": (I, [P, P, P, I]),
+    "pfb_sur2d_loss_grad": (I, [P, P, P, P, I, C.POINTER(C.c_double)]),
+    "pfb_sur2d_train_step": (I, [P, P, P, P, I, C.c_float, C.POINTER(C.c_double)]),
+    "pfb_sur2d_sync": (I, [P]),
+    "pfb_sur2d_jump": (I, [P, P]),
+    "pfb_sur2d_bench_forward": (I, [P, I, I, C.POINTER(C.c_double)]),
 })

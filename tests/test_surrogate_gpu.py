@@ -1,0 +1,243 @@
+"""Learned relaxation surrogate on the GPU: the whole U-Net's loss and
+gradients against the FP64 oracle (oracle/unet_oracle.py), training, the
+crops that connect it to a pfb_sim2d system, the jump, and the residual.
+
+Tolerances: the network keeps activations and activation gradients in
+bfloat16 (8-bit significand) while the oracle runs in float64 from the same
+bfloat16 weights and inputs, so the loss is compared to 0.5 % and each
+layer's gradient to 2 % in relative L2 norm (with a cosine above 0.9995);
+measured: 4e-4 and at most 5e-3."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import conv_oracle as co
+import pfb200
+import unet_oracle as uo
+from helpers2d import params
+from pfb200 import check, lib
+
+pytestmark = pytest.mark.gpu
+
+H = 64
+
+
+def torch():
+    import torch as t
+    return t
+
+
+def bf16_round(a):
+    t = torch()
+    return t.from_numpy(np.ascontiguousarray(a, np.float32)).to(t.bfloat16).float().numpy()
+
+
+def make_net(max_batch=8, seed=3):
+    h = lib().pfb_sur2d_create(max_batch, seed, 0)
+    assert h, lib().pfb_last_error()
+    return h
+
+
+def get_params(h):
+    out = np.zeros(lib().pfb_sur2d_num_params(h), np.float32)
+    check(lib().pfb_sur2d_get_params(h, out.ctypes.data), "get_params")
+    return out
+
+
+def set_params(h, flat):
+    flat = np.ascontiguousarray(flat, np.float32)
+    check(lib().pfb_sur2d_set_params(h, flat.ctypes.data), "set_params")
+
+
+def layer_slices():
+    offs = np.cumsum([0] + [9 * a * b + b for a, b, _ in uo.LAYERS])
+    return [slice(offs[i], offs[i + 1]) for i in range(8)]
+
+
+def rounded_weights(flat):
+    """The weights as the kernels see them (bfloat16), biases binary32."""
+    out = flat.astype(np.float64).copy()
+    for (ci, co_, _), sl in zip(uo.LAYERS, layer_slices()):
+        nw = 9 * ci * co_
+        out[sl.start:sl.start + nw] = bf16_round(flat[sl.start:sl.start + nw])
+    return out
+
+
+def synthetic_set(n, seed):
+    rng = np.random.default_rng(seed)
+    yy, xx = np.mgrid[0:H, 0:H]
+    x = np.zeros((n, H, H, 16), np.float32)
+    t = np.zeros((n, H, H), np.float32)
+    for k in range(n):
+        cx, cy, r = 32 + rng.uniform(-4, 4), 32 + rng.uniform(-4, 4), rng.uniform(8, 14)
+        d = np.hypot(xx - cx, yy - cy)
+        x[k, ..., 0] = 0.5 * (1 - np.tanh((d - r) / 3.0))
+        ox, oy = cx + rng.choice([-1, 1]) * 24, cy + rng.uniform(-6, 6)
+        x[k, ..., 1] = (0.5 * (1 - np.tanh((np.hypot(xx - ox, yy - oy) - 12) / 3.0))) ** 2
+        # target: the disc relaxes towards radius 12 and away from the neighbour
+        d2 = np.hypot(xx - cx + 0.02 * (ox - cx), yy - cy)
+        t[k] = 0.5 * (1 - np.tanh((d2 - 12.0) / 3.0)) - x[k, ..., 0]
+    x = bf16_round(x)
+    return x, t
+
+
+def dev_inputs(x, t):
+    tt = torch()
+    xp = co.to_padded(x)
+    xd = tt.from_numpy(np.ascontiguousarray(xp, np.float32)).to(tt.bfloat16).cuda().contiguous()
+    td = tt.from_numpy(np.ascontiguousarray(t, np.float32)).cuda().contiguous()
+    return xd, td
+
+
+def test_loss_and_gradients_vs_fp64_oracle():
+    tt = torch()
+    h = make_net()
+    rng = np.random.default_rng(8)
+    flat = get_params(h)
+    sl = layer_slices()[7]
+    flat[sl] = 0.0
+    flat[sl.start:sl.start + 9 * 32] = rng.standard_normal(9 * 32) * 0.05  # output channel 0
+    flat[sl.stop - 16] = 0.01
+    for s in layer_slices()[:7]:  # small nonzero biases
+        flat[s.stop - 32:s.stop] = rng.standard_normal(32) * 0.01
+    set_params(h, flat)
+    x, t = synthetic_set(4, 2)
+    xd, td = dev_inputs(x, t)
+    idx = tt.arange(4, dtype=tt.int32, device="cuda")
+    loss = C.c_double()
+    check(lib().pfb_sur2d_loss_grad(h, xd.data_ptr(), td.data_ptr(), idx.data_ptr(), 4,
+                                    C.byref(loss)), "loss_grad")
+    g = np.zeros_like(flat)
+    check(lib().pfb_sur2d_get_grads(h, g.ctypes.data), "get_grads")
+    ref_loss, ref_g = uo.loss_and_grad(rounded_weights(flat), x.astype(np.float64), t)
+    print(f"loss {loss.value:.6e} vs FP64 {ref_loss:.6e}")
+    assert abs(loss.value - ref_loss) <= 0.005 * ref_loss
+    for l, s in enumerate(layer_slices()):
+        a, b = g[s].astype(np.float64), ref_g[s]
+        rel = np.linalg.norm(a - b) / np.linalg.norm(b)
+        cos = float(a @ b / (np.linalg.norm(a) * np.linalg.norm(b)))
+        print(f"layer {l + 1}: relative L2 error {rel:.3e}, cosine {cos:.6f}")
+        assert rel < 0.02 and cos > 0.9995, l
+    lib().pfb_sur2d_destroy(h)
+
+
+def test_training_reduces_the_loss():
+    tt = torch()
+    h = make_net(max_batch=16, seed=4)
+    x, t = synthetic_set(64, 7)
+    xd, td = dev_inputs(x, t)
+    rng = np.random.default_rng(0)
+    losses = []
+    for step in range(400):
+        idx = tt.from_numpy(rng.choice(64, 16, replace=False).astype(np.int32)).cuda()
+        loss = C.c_double()
+        check(lib().pfb_sur2d_train_step(h, xd.data_ptr(), td.data_ptr(), idx.data_ptr(), 16,
+                                         2e-3, C.byref(loss)), "train_step")
+        losses.append(loss.value)
+    first, last = np.mean(losses[:5]), np.mean(losses[-5:])
+    print(f"training loss {first:.3e} -> {last:.3e}")
+    assert last < 0.5 * first
+    status = C.c_uint()
+    check(lib().pfb_conv_status(C.byref(status), 1), "status")
+    assert status.value == 0
+    lib().pfb_sur2d_destroy(h)
+
+
+def small_sim(steps=20, seed=12):
+    p = params(320, 12, R=12.0, seed=seed, v_A=0.0)
+    cx, cy = pfb200.palmieri_centres(12, 320, 24.0, seed)
+    s = pfb200.Sim2D(p, cx, cy)
+    s.advance(steps)
+    return p, s
+
+
+def test_extract_and_crop_phi_match_world_fields():
+    tt = torch()
+    p, s = small_sim()
+    N, L = p.num_cells, p.L
+    x0 = tt.zeros((N, 66 * 66, 16), dtype=tt.bfloat16, device="cuda")
+    pc = tt.zeros((N, 64, 64), dtype=tt.float32, device="cuda")
+    org = tt.zeros((N, 2), dtype=tt.int32, device="cuda")
+    check(lib().pfb_sur2d_extract(s._h, x0.data_ptr(), pc.data_ptr(), org.data_ptr()), "extract")
+    s.sync()
+    cells, phi, S = s.cells(), s.phi(), s.S()
+    origins = org.cpu().numpy()
+    crops = pc.cpu().numpy()
+    xin = co.from_padded(x0.float().cpu().numpy(), 64, 64)
+    worlds = np.stack([pfb200.world_field(phi, cells, n, L) for n in range(N)])
+    sq = np.minimum(worlds ** 2, 4.0)
+    for n in range(N):
+        V = cells["V"][n]
+        cxn = int(np.floor(cells["gx0"][n] + cells["Cx"][n] / V + 0.5))
+        cyn = int(np.floor(cells["gy0"][n] + cells["Cy"][n] / V + 0.5))
+        assert tuple(origins[n]) == ((cxn - 32) % L, (cyn - 32) % L)
+        ys = (origins[n][1] + np.arange(64)) % L
+        xs = (origins[n][0] + np.arange(64)) % L
+        want = worlds[n][np.ix_(ys, xs)]
+        np.testing.assert_array_equal(crops[n], want.astype(np.float32))
+        np.testing.assert_array_equal(xin[n, ..., 0], bf16_round(want))
+        other = (sq.sum(0) - sq[n])[np.ix_(ys, xs)]
+        np.testing.assert_allclose(xin[n, ..., 1], other, rtol=8e-3, atol=1e-6)
+        assert not xin[n, ..., 2:].any()
+    s.close()
+
+
+def test_insert_rebuilds_moments_and_aggregate():
+    tt = torch()
+    p, s = small_sim()
+    N, L = p.num_cells, p.L
+    x0 = tt.zeros((N, 66 * 66, 16), dtype=tt.bfloat16, device="cuda")
+    pc = tt.zeros((N, 64, 64), dtype=tt.float32, device="cuda")
+    org = tt.zeros((N, 2), dtype=tt.int32, device="cuda")
+    check(lib().pfb_sur2d_extract(s._h, x0.data_ptr(), pc.data_ptr(), org.data_ptr()), "extract")
+    half = (-0.5 * pc).contiguous()
+    check(lib().pfb_sur2d_insert(s._h, org.data_ptr(), half.data_ptr()), "insert")
+    s.sync()
+    cells, phi, S = s.cells(), s.phi(), s.S()
+    from helpers2d import s_from_phi
+    np.testing.assert_array_equal(S, s_from_phi(phi, cells, L))
+    for n in range(N):
+        w = pfb200.window_view(phi, cells, n).astype(np.float64)
+        np.testing.assert_allclose(cells["V"][n], (w * w).sum(), rtol=1e-9)
+    # the cell bodies (inside the crops) were halved
+    assert cells["phi_max"].max() < 0.6
+    s.advance(3)
+    assert not pfb200.fatal(s.flags())
+    s.close()
+
+
+def test_untrained_jump_leaves_the_state_unchanged():
+    p, s = small_sim()
+    h = make_net(max_batch=8)  # zero last layer: predicts no change; 12 cells in 2 batches
+    before_phi, before_cells = s.phi(), s.cells()
+    check(lib().pfb_sur2d_jump(h, s._h), "jump")
+    np.testing.assert_array_equal(s.phi(), before_phi)
+    after = s.cells()
+    np.testing.assert_allclose(after["V"], before_cells["V"], rtol=1e-12)
+    np.testing.assert_allclose(after["Cx"], before_cells["Cx"], rtol=1e-12)
+    s.advance(2)
+    assert not pfb200.fatal(s.flags())
+    lib().pfb_sur2d_destroy(h)
+    s.close()
+
+
+def test_residual_step_matches_world_difference():
+    p, s = small_sim(steps=7)
+    a_phi, a_c = s.phi(), s.cells()
+    linf, rms = C.c_double(), C.c_double()
+    check(lib().pfb_sim2d_residual_step(s._h, C.byref(linf), C.byref(rms)), "residual")
+    b_phi, b_c = s.phi(), s.cells()
+    assert s.step == 8
+    mx, s2, area = 0.0, 0.0, 0
+    for n in range(p.num_cells):
+        wa = pfb200.world_field(a_phi, a_c, n, p.L)
+        wb = pfb200.world_field(b_phi, b_c, n, p.L)
+        d = (wb - wa) / p.dt
+        mx = max(mx, float(np.abs(d).max()))
+        s2 += float((d * d).sum())
+        cw = pfb200.CLASSES[int(b_c["cls"][n])]
+        area += cw[0] * cw[1]
+    assert linf.value == pytest.approx(mx, rel=1e-12)
+    assert rms.value == pytest.approx(np.sqrt(s2 / area), rel=1e-9)
+    s.close()
