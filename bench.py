@@ -495,6 +495,126 @@ def run_ensemble(a):
     return 0
 
 
+WORKLOAD_CS = ("passive relaxation (v_A = 0) of a 1024^2 periodic lattice with 400 cells of "
+               "radius 12 (rho 0.17, min separation 2R, seed 999): time until the step residual "
+               "max |dphi/dt| reaches the target, plain explicit steps against steps with jumps "
+               "of the learned surrogate judged by the plain solver")
+
+
+def run_surrogate(a):
+    """The surrogate workload: training data from plain-solver pairs (10 runs x
+    5 pairs x 400 cells = 20,000 crops, increments over 8,000 steps, inputs
+    with the rate over the previous 100 steps), Adam training of the U-Net,
+    then time-to-relaxed of a fresh system, plain against
+    surrogate-accelerated (median wall time of three runs each). One GPU
+    (other ranks exit)."""
+    import torch
+    import pfb200
+    from pfb200 import surrogate as sg
+    rank, world, local = rank_env()
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    if a.profile_forward:
+        net = sg.Surrogate2D(max_batch=512, seed=1, device=local)
+        ms = net.bench_forward(512, 3)
+        x = torch.zeros((512, sg.PADDED, sg.IN_CH), dtype=torch.bfloat16, device=f"cuda:{local}")
+        t = torch.zeros((512, sg.CROP, sg.CROP), dtype=torch.float32, device=f"cuda:{local}")
+        idx = torch.arange(512, dtype=torch.int32, device=f"cuda:{local}")
+        for _ in range(2):
+            net.train_step(x, t, idx, 1e-4)
+        net.sync()
+        print(json.dumps({"profile_forward_ms": ms, "batch": 512}), flush=True)
+        net.close()
+        return 0
+    interval, history, heal = 8000, 100, 100
+    p = sg.relaxation_params()
+    data = sg.make_dataset(p, runs=10, pairs_per_run=5, interval=interval, device=local,
+                           history=history)
+    net = sg.Surrogate2D(max_batch=512, seed=1, device=local)
+    for _ in range(3):
+        net.bench_forward(512, 5)  # warm-up
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    m0 = clocks.mark()
+    fwd_ms = net.bench_forward(512, 50)
+    m1 = clocks.mark()
+    t0 = time.perf_counter()
+    hist = sg.train(net, data, steps=a.train_steps, batch=256, log_every=1000)
+    train_s = time.perf_counter() - t0
+
+    def run(use_net):
+        t1 = time.perf_counter()
+        q = sg.relaxation_params(seed=999)
+        cx, cy = pfb200.palmieri_centres(q.num_cells, q.L, 2 * q.target_radius, q.seed)
+        sim = pfb200.Sim2D(q, cx, cy, device=local)
+        r = sg.relax(sim, a.target, 150000, net=net if use_net else None, interval=interval,
+                     heal=heal, history=history)
+        phi = sim.phi()  # final state back to the host
+        total = time.perf_counter() - t1
+        flags = sim.flags()
+        sim.close()
+        return r, total, phi.nbytes, flags
+
+    def median_of(use_net, k=3):
+        runs = sorted((run(use_net) for _ in range(k)), key=lambda x: x[0].seconds)
+        return runs[k // 2], [x[0].seconds for x in runs]
+
+    (plain, plain_total, _, _), plain_all = median_of(False)
+    (sur, sur_total, phi_bytes, flags), sur_all = median_of(True)
+    clocks.stop()
+    peaks = json.loads((REPO / "MEASURED_PEAKS.json").read_text()) \
+        if (REPO / "MEASURED_PEAKS.json").exists() else {}
+    peak = float(peaks.get("bf16_tflops", 1590.0))
+    achieved = sg.forward_flops(512) / (fwd_ms / 1000.0) / 1e12
+    # kernels of one jump: extract, 8 convolutions, pool, upsample, take, insert, moments, scatter
+    launches = sur.solver_steps + len(sur.history) + 15 * (sur.jumps_accepted + sur.jumps_rejected)
+    line = {
+        "metric": "time-to-relaxed", "value": sur.seconds, "unit": "s", "n_gpus": 1,
+        "steps": sur.solver_steps, "warmup": 0, "ms_per_step": 1000.0 * sur.seconds / sur.solver_steps,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 solver; bf16 network with f32 accumulation", "data": "synthetic",
+        "config": {"workload": WORKLOAD_CS, "L": p.L, "cells": p.num_cells, "radius": p.target_radius,
+                   "target_residual": a.target, "residual": "max over cells and sites of "
+                   "|phi^{k+1} - phi^k| / dt, checked every 500 steps",
+                   "jump_interval_steps": interval, "rate_history_steps": history,
+                   "heal_steps": heal, "repeats": "median of 3 wall times",
+                   "dataset": f"{data.x.shape[0]} crops from 10 fresh runs x 5 pairs ({data.seconds:.1f} s)",
+                   "train_steps": a.train_steps, "batch": 256,
+                   "l2": "solver inputs larger than L2 (two 133 MB phi pools)"},
+        "reached": sur.reached, "residual": sur.residual,
+        "plain": {"seconds": plain.seconds, "reached": plain.reached, "residual": plain.residual,
+                  "solver_steps": plain.solver_steps, "all_seconds": plain_all},
+        "surrogate": {"seconds": sur.seconds, "reached": sur.reached, "residual": sur.residual,
+                      "solver_steps": sur.solver_steps, "jumps_accepted": sur.jumps_accepted,
+                      "jumps_rejected": sur.jumps_rejected,
+                      "equivalent_steps": sur.equivalent_steps, "all_seconds": sur_all},
+        "speedup_vs_plain": plain.seconds / sur.seconds,
+        "solver_step_ratio": plain.solver_steps / sur.solver_steps,
+        "training": {"seconds": train_s, "crops_per_s": a.train_steps * 256 / train_s,
+                     "dataset_seconds": data.seconds,
+                     "loss_first": hist[0][1], "loss_last": hist[-1][1]},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "kernel": "pfb::k_conv3x3_fwd (U-Net forward, 512 crops, 8 layers)",
+                     "flops_per_launch": sg.forward_flops(512),
+                     "peak_source": "measured (MEASURED_PEAKS.json bf16_tflops, burst)",
+                     "duration_source": "CUDA events, 50 forward passes"},
+        "cpu_baseline": None,
+        "e2e": {"value": sur_total, "unit": "s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": phi_bytes / max(1, sur.solver_steps),
+                "plain_seconds": plain_total,
+                "note": "fresh system from host centres to the relaxed phi pool back on the host"},
+        "clocks": clocks.summary(m0, m1),
+        "gpu_launches": launches,
+        "flags": pfb200.flags_report(flags),
+    }
+    print(json.dumps(line), flush=True)
+    net.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -510,9 +630,16 @@ def main():
                     help="2D phi pools: 0 binary32 (reference layout), 1 binary16, 2 bfloat16")
     ap.add_argument("--cpu-steps", type=int, default=int(os.environ.get("PFB_CPU_STEPS", "6")))
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "ce"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "ce", "cs"],
                     help="c2: 2D 2048^2 / 1024 cells (default); c3: 3D 256^3 / 512 cells; "
-                         "ce: batched ensemble of 64 mixed-size 2D replicas")
+                         "ce: batched ensemble of 64 mixed-size 2D replicas; cs: passive "
+                         "relaxation of 1024^2 / 400 cells, plain against the learned surrogate")
+    ap.add_argument("--target", type=float, default=1e-3,
+                    help="cs: residual max |dphi/dt| that counts as relaxed")
+    ap.add_argument("--train-steps", type=int, default=8000, help="cs: Adam steps")
+    ap.add_argument("--profile-forward", action="store_true",
+                    help="cs: only 3 forward passes and 2 training steps of the U-Net on 512 "
+                         "zero crops (a short command for ncu)")
     a = ap.parse_args()
     if a.warmup < 3:
         a.warmup = 3
@@ -522,6 +649,8 @@ def main():
         return run_3d(a)
     if a.workload == "ce":
         return run_ensemble(a)
+    if a.workload == "cs":
+        return run_surrogate(a)
 
     import torch
     import pfb200

@@ -320,6 +320,12 @@ int pfb_sim2d_set_state(pfb_sim2d* s, const pfb_cell2d* cells,
                         const float* phi, long long step);
 /* Pack the per-cell trajectory record into host memory `out` (N records). */
 int pfb_sim2d_pack_traj(pfb_sim2d* s, pfb_traj_cell2d* out);
+/* In-memory device checkpoint (no reference counterpart): save copies the
+ * current pool, cells, aggregate and flags into buffers of the system
+ * (allocated on the first save); restore returns to that step exactly as a
+ * set_state of the saved state would. */
+int pfb_sim2d_save(pfb_sim2d* s);
+int pfb_sim2d_restore(pfb_sim2d* s);
 /* Timed benchmark in the manner of Sim::bench (reference src/sim.cu:1006):
  * `warmup` untimed steps, then `steps` steps timed with CUDA events on the
  * simulator's stream. Writes ms per step. */

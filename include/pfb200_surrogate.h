@@ -97,10 +97,17 @@ int pfb_sim2d_residual_step(pfb_sim2d* s, double* linf, double* rms);
 /* Network input of every cell of `s` (num_cells padded 66 x 66 images of 16
  * bfloat16 channels: phi_n and the sum over the other cells of
  * min(phi_m^2, 4), on the 64 x 64 lattice crop centred at the cell's
- * rounded centroid), the binary32 phi_n crops (num_cells x 64 x 64, may be
- * null) and the crop origins (num_cells x 2 ints, x then y). Device
- * buffers; runs on the system's stream. */
+ * rounded centroid; channel 2 zero), the binary32 phi_n crops (num_cells x
+ * 64 x 64, may be null) and the crop origins (num_cells x 2 ints, x then
+ * y). Device buffers; runs on the system's stream. */
 int pfb_sur2d_extract(pfb_sim2d* s, void* x0, float* phi_crop, int* origins);
+
+/* As pfb_sur2d_extract on crops at the given origins, with channel 2 =
+ * (phi_n - prev) * hist_scale when prev (num_cells x 64 x 64 crops of an
+ * earlier step at the same origins) is not null: the recent rate of change
+ * when hist_scale = 1 / (steps between them x dt). */
+int pfb_sur2d_extract_at(pfb_sim2d* s, const int* origins, const float* prev, float hist_scale,
+                         void* x0, float* phi_crop);
 
 /* out = phi_n on the 64 x 64 crops at `origins` (binary32), minus `minus`
  * when it is not null (e.g. the crops of an earlier step: the increment). */
@@ -112,6 +119,7 @@ int pfb_sur2d_crop_phi(pfb_sim2d* s, const int* origins, const float* minus, flo
 int pfb_sur2d_insert(pfb_sim2d* s, const int* origins, const float* dphi);
 
 /* ---- the surrogate network -------------------------------------------------
+ * Input channels: phi_n, the others' sum of phi^2, phi_n's recent rate.
  * A U-Net of eight 3x3 convolutions of width 32 (ReLU; 2x2 average pool and
  * nearest upsampling with a skip connection between 64^2 and 32^2) mapping a
  * crop from pfb_sur2d_extract to the increment of phi_n over the relaxation
@@ -148,6 +156,10 @@ int pfb_sur2d_sync(pfb_sur2d* n);
 /* Jump every cell of `s` by the network (extract, predict, insert, rebuild)
  * on the system's stream; returns after it completed. */
 int pfb_sur2d_jump(pfb_sur2d* n, pfb_sim2d* s);
+/* The same with the rate input: crops now, history_steps plain steps,
+ * crops again with channel 2 = their difference * hist_scale, then the
+ * jump. */
+int pfb_sur2d_jump_history(pfb_sur2d* n, pfb_sim2d* s, int history_steps, float hist_scale);
 
 /* Device milliseconds per forward pass over `batch` crops (CUDA events). */
 int pfb_sur2d_bench_forward(pfb_sur2d* n, int batch, int iters, double* ms);

@@ -71,7 +71,8 @@ int sim2d_rebuild(pfb_sim2d* s);
 int sim2d_step_keep_prev(pfb_sim2d* s);
 // relax2d.cu: crops of the current state (network input, origins) and the
 // insertion of predicted increments (followed by a rebuild)
-int relax_extract(pfb_sim2d* s, void* x0, float* phi_crop, int* origins);
+int relax_extract(pfb_sim2d* s, void* x0, float* phi_crop, int* origins, const int* origins_in,
+                  const float* prev, float hist_scale);
 int relax_insert(pfb_sim2d* s, const int* origins, const float* dphi);
 
 // conv2d_tc.cu: 3x3 same convolutions on padded-NHWC bfloat16 activations

@@ -104,27 +104,36 @@ __device__ __forceinline__ void crop_origin(const pfb_cell2d& c, int L, int* ox,
 
 // Network input of every cell: a padded 66 x 66 image of 16 bfloat16
 // channels, channel 0 = phi_n, channel 1 = sum over the other cells of
-// min(phi_m^2, 4) from the exact aggregate (S - q(phi_n)) 2^-27; the ring
-// and channels 2..15 are zero. Also the binary32 phi_n crop (optional) and
-// the crop origins.
+// min(phi_m^2, 4) from the exact aggregate (S - q(phi_n)) 2^-27, channel 2 =
+// (phi_n - prev) * hist_scale when an earlier crop `prev` at the same origins
+// is given (the recent rate of change), else 0; the ring and channels 3..15
+// are zero. Origins: the cell's rounded centroid minus half the crop, written
+// to `origins`, or read from `origins_in` when given. Also the binary32 phi_n
+// crop (optional).
 __global__ void __launch_bounds__(kRelaxThreads) k_extract_crops(
     const float* __restrict__ phi, const pfb_cell2d* __restrict__ cells,
     const uint32_t* __restrict__ S, int L, int P, __nv_bfloat16* __restrict__ x0,
-    float* __restrict__ phi_crop, int* __restrict__ origins) {
+    float* __restrict__ phi_crop, int* __restrict__ origins, const int* __restrict__ origins_in,
+    const float* __restrict__ prev, float hist_scale) {
     const int n = (int)blockIdx.x;
     const pfb_cell2d c = cells[n];
     const Window w = window_of(c.cls);
     int ox, oy;
-    crop_origin(c, L, &ox, &oy);
-    if (threadIdx.x == 0) {
-        origins[2 * n] = ox;
-        origins[2 * n + 1] = oy;
+    if (origins_in) {
+        ox = origins_in[2 * n];
+        oy = origins_in[2 * n + 1];
+    } else {
+        crop_origin(c, L, &ox, &oy);
+        if (threadIdx.x == 0) {
+            origins[2 * n] = ox;
+            origins[2 * n + 1] = oy;
+        }
     }
     const float* tile = phi + (size_t)n * kTileArea;
     uint4* img = reinterpret_cast<uint4*>(x0 + (size_t)n * kCropPad * kCropPad * kInCh);
     for (int k = (int)threadIdx.x; k < kCropPad * kCropPad; k += kRelaxThreads) {
         const int u = k % kCropPad - 1, v = k / kCropPad - 1;
-        float f = 0.0f, so = 0.0f;
+        float f = 0.0f, so = 0.0f, rate = 0.0f;
         if (u >= 0 && u < kCrop && v >= 0 && v < kCrop) {
             const int x = wrap(ox + u, L), y = wrap(oy + v, L);
             f = cell_phi_at(tile, w, c.gx0, c.gy0, x, y, L);
@@ -132,9 +141,12 @@ __global__ void __launch_bounds__(kRelaxThreads) k_extract_crops(
             const uint32_t q = q_encode(f);
             so = s >= q ? (float)(s - q) * kQInv : 0.0f;
             if (phi_crop) phi_crop[(size_t)n * kCrop * kCrop + v * kCrop + u] = f;
+            if (prev) rate = (f - prev[(size_t)n * kCrop * kCrop + v * kCrop + u]) * hist_scale;
         }
         __nv_bfloat162 h01 = __floats2bfloat162_rn(f, so);
-        uint4 first = make_uint4(*reinterpret_cast<uint32_t*>(&h01), 0u, 0u, 0u);
+        __nv_bfloat162 h23 = __floats2bfloat162_rn(rate, 0.0f);
+        uint4 first = make_uint4(*reinterpret_cast<uint32_t*>(&h01), *reinterpret_cast<uint32_t*>(&h23),
+                                 0u, 0u);
         img[2 * k] = first;
         img[2 * k + 1] = make_uint4(0u, 0u, 0u, 0u);
     }
@@ -182,15 +194,16 @@ int need_f32(const Sim2DView& v) {
 
 }  // namespace
 
-int relax_extract(pfb_sim2d* s, void* x0, float* phi_crop, int* origins) {
+int relax_extract(pfb_sim2d* s, void* x0, float* phi_crop, int* origins, const int* origins_in,
+                  const float* prev, float hist_scale) {
     Sim2DView v;
     int rc = sim2d_view(s, &v);
     if (rc || (rc = need_f32(v))) return rc;
-    if (!x0 || !origins) return set_error(PFB_E_ARG, "extract: null buffer");
+    if (!x0 || (!origins && !origins_in)) return set_error(PFB_E_ARG, "extract: null buffer");
     cudaSetDevice(v.device);
     k_extract_crops<<<v.N, kRelaxThreads, 0, v.stream>>>(v.phi_cur, v.cells, v.S_cur, v.L, v.P,
                                                         static_cast<__nv_bfloat16*>(x0), phi_crop,
-                                                        origins);
+                                                        origins, origins_in, prev, hist_scale);
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? PFB_OK : set_error(PFB_E_CUDA, "extract: %s", cudaGetErrorString(e));
 }
@@ -251,7 +264,14 @@ int pfb_sim2d_residual_step(pfb_sim2d* s, double* linf, double* rms) {
 
 int pfb_sur2d_extract(pfb_sim2d* s, void* x0, float* phi_crop, int* origins) {
     clear_error();
-    return relax_extract(s, x0, phi_crop, origins);
+    return relax_extract(s, x0, phi_crop, origins, nullptr, nullptr, 0.0f);
+}
+
+int pfb_sur2d_extract_at(pfb_sim2d* s, const int* origins, const float* prev, float hist_scale,
+                         void* x0, float* phi_crop) {
+    clear_error();
+    if (!origins) return set_error(PFB_E_ARG, "extract_at: null origins");
+    return relax_extract(s, x0, phi_crop, nullptr, origins, prev, hist_scale);
 }
 
 int pfb_sur2d_crop_phi(pfb_sim2d* s, const int* origins, const float* minus, float* out) {

@@ -35,6 +35,13 @@ struct pfb_sim2d {
     uint32_t* d_S = nullptr;
     pfb_cell2d* d_cell = nullptr;
     pfb_cell2d* d_cell_prev = nullptr;  // records before the last residual step
+    // in-memory device checkpoint (pfb_sim2d_save / pfb_sim2d_restore)
+    void* b_phi = nullptr;
+    pfb_cell2d* b_cell = nullptr;
+    uint8_t* b_cls = nullptr;
+    uint32_t* b_S = nullptr;
+    uint32_t* b_flags = nullptr;
+    long long b_step = -1;
     uint8_t* d_cls = nullptr;
     unsigned long long* d_cursor = nullptr;
     unsigned long long* d_step = nullptr;
@@ -63,6 +70,61 @@ struct pfb_sim2d {
         cudaFree(d_flags);
         cudaFree(d_traj);
         cudaFree(d_cell_prev);
+        cudaFree(b_phi);
+        cudaFree(b_cell);
+        cudaFree(b_cls);
+        cudaFree(b_S);
+        cudaFree(b_flags);
+    }
+
+    int save() {
+        PFB_CU(cudaSetDevice(device), "cudaSetDevice");
+        if (!b_phi) {
+            PFB_CU(cudaMalloc(&b_phi, pool_bytes()), "alloc checkpoint");
+            PFB_CU(cudaMalloc(&b_cell, (size_t)N * sizeof(pfb_cell2d)), "alloc checkpoint");
+            PFB_CU(cudaMalloc(&b_cls, (size_t)N), "alloc checkpoint");
+            PFB_CU(cudaMalloc(&b_S, s_words * sizeof(uint32_t)), "alloc checkpoint");
+            PFB_CU(cudaMalloc(&b_flags, PFB_FLAG_COUNT * sizeof(uint32_t)), "alloc checkpoint");
+        }
+        const int pin = (int)(steps_done % 2), rot = (int)(steps_done % 3);
+        PFB_CU(cudaMemcpyAsync(b_phi, d_phi[pin], pool_bytes(), cudaMemcpyDeviceToDevice, stream), "save");
+        PFB_CU(cudaMemcpyAsync(b_cell, d_cell, (size_t)N * sizeof(pfb_cell2d), cudaMemcpyDeviceToDevice,
+                               stream), "save");
+        PFB_CU(cudaMemcpyAsync(b_cls, d_cls, (size_t)N, cudaMemcpyDeviceToDevice, stream), "save");
+        PFB_CU(cudaMemcpyAsync(b_S, d_S + (size_t)rot * s_words, s_words * sizeof(uint32_t),
+                               cudaMemcpyDeviceToDevice, stream), "save");
+        PFB_CU(cudaMemcpyAsync(b_flags, d_flags, PFB_FLAG_COUNT * sizeof(uint32_t),
+                               cudaMemcpyDeviceToDevice, stream), "save");
+        b_step = steps_done;
+        return PFB_OK;
+    }
+
+    // Back to the saved state: pool, cells, the aggregate slot and flags, with
+    // the step counters, cursors and the other aggregate slots as a fresh
+    // set_state leaves them.
+    int restore() {
+        if (b_step < 0) return set_error(PFB_E_STATE, "restore: nothing saved");
+        PFB_CU(cudaSetDevice(device), "cudaSetDevice");
+        drop_graph();
+        steps_done = b_step;
+        const int pin = (int)(steps_done % 2), rot = (int)(steps_done % 3);
+        PFB_CU(cudaMemcpyAsync(d_phi[pin], b_phi, pool_bytes(), cudaMemcpyDeviceToDevice, stream),
+               "restore");
+        PFB_CU(cudaMemcpyAsync(d_cell, b_cell, (size_t)N * sizeof(pfb_cell2d), cudaMemcpyDeviceToDevice,
+                               stream), "restore");
+        PFB_CU(cudaMemcpyAsync(d_cls, b_cls, (size_t)N, cudaMemcpyDeviceToDevice, stream), "restore");
+        PFB_CU(cudaMemsetAsync(d_S, 0, 3 * s_words * sizeof(uint32_t), stream), "restore");
+        PFB_CU(cudaMemcpyAsync(d_S + (size_t)rot * s_words, b_S, s_words * sizeof(uint32_t),
+                               cudaMemcpyDeviceToDevice, stream), "restore");
+        PFB_CU(cudaMemcpyAsync(d_flags, b_flags, PFB_FLAG_COUNT * sizeof(uint32_t),
+                               cudaMemcpyDeviceToDevice, stream), "restore");
+        const unsigned long long hs[2] = {
+            (unsigned long long)(pin == 0 ? steps_done : steps_done + 1),
+            (unsigned long long)(pin == 1 ? steps_done : steps_done + 1)};
+        PFB_CU(cudaMemcpyAsync(d_step, hs, sizeof(hs), cudaMemcpyHostToDevice, stream), "restore");
+        PFB_CU(cudaMemsetAsync(d_cursor, 0, 2 * sizeof(unsigned long long), stream), "restore");
+        PFB_CU(cudaStreamSynchronize(stream), "restore");
+        return PFB_OK;
     }
 
     pfb_step_args2d args_for_slot(int slot) const {
@@ -487,6 +549,16 @@ int pfb_sim2d_get_flags(pfb_sim2d* s, uint32_t* out) {
                            cudaMemcpyDeviceToHost, s->stream), "download flags");
     PFB_CU(cudaStreamSynchronize(s->stream), "sync");
     return PFB_OK;
+}
+
+int pfb_sim2d_save(pfb_sim2d* s) {
+    if (!s) return set_error(PFB_E_ARG, "null system");
+    return s->save();
+}
+
+int pfb_sim2d_restore(pfb_sim2d* s) {
+    if (!s) return set_error(PFB_E_ARG, "null system");
+    return s->restore();
 }
 
 int pfb_sim2d_set_state(pfb_sim2d* s, const pfb_cell2d* cells, const float* phi, long long step) {

@@ -3,7 +3,8 @@
 // (mean-squared error, Adam) and the jump of a pfb_sim2d system. No
 // counterpart in the reference.
 //
-// Input: 2 channels (phi_n and the other cells' sum of phi^2, padded to 16).
+// Input: 3 channels (phi_n, the other cells' sum of phi^2 and phi_n's recent
+// rate of change, padded to 16).
 // Output: the increment of phi_n over a fixed number of passive relaxation
 // steps (channel 0 of 16). Layers (3x3, width 32, ReLU except the last):
 //   c1 16->32 @64, c2 32->32 @64 (skip), 2x2 average pool,
@@ -38,7 +39,7 @@ constexpr int kEwThreads = 256;
 struct LayerSpec {
     int cin, cout, res, relu, cin_real, cout_real;
 };
-constexpr LayerSpec kLayers[8] = {{16, 32, 64, 1, 2, 32},  {32, 32, 64, 1, 32, 32},
+constexpr LayerSpec kLayers[8] = {{16, 32, 64, 1, 3, 32},  {32, 32, 64, 1, 32, 32},
                                   {32, 32, 32, 1, 32, 32}, {32, 32, 32, 1, 32, 32},
                                   {32, 32, 64, 1, 32, 32}, {32, 32, 64, 1, 32, 32},
                                   {32, 32, 64, 1, 32, 32}, {32, 16, 64, 0, 32, 1}};
@@ -527,12 +528,13 @@ int pfb_sur2d_sync(pfb_sur2d* n) {
     return PFB_OK;
 }
 
-// Jump every cell of `s` by the network: crops of the current state, the
-// predicted increments added back into the cells' tiles, then moments and
-// aggregate rebuilt. Runs on the system's stream.
-int pfb_sur2d_jump(pfb_sur2d* n, pfb_sim2d* s) {
+// Jump every cell of `s` by the network: crops of the current state (with
+// the rate over the last history_steps plain steps, taken here, when
+// history_steps > 0), the predicted increments added back into the cells'
+// tiles, then moments and aggregate rebuilt. Runs on the system's stream.
+int pfb_sur2d_jump_history(pfb_sur2d* n, pfb_sim2d* s, int history_steps, float hist_scale) {
     clear_error();
-    if (!n || !s) return set_error(PFB_E_ARG, "jump: null argument");
+    if (!n || !s || history_steps < 0) return set_error(PFB_E_ARG, "jump: bad argument");
     Sim2DView v;
     int rc = sim2d_view(s, &v);
     if (rc) return rc;
@@ -545,7 +547,15 @@ int pfb_sur2d_jump(pfb_sur2d* n, pfb_sim2d* s) {
     SUR_CU(cudaMallocAsync(&xin, (size_t)N * kP64 * 16 * sizeof(bf16), v.stream), "jump alloc");
     SUR_CU(cudaMallocAsync(&d, (size_t)N * kImg * kImg * sizeof(float), v.stream), "jump alloc");
     SUR_CU(cudaMallocAsync(&org, (size_t)N * 2 * sizeof(int), v.stream), "jump alloc");
-    rc = relax_extract(s, xin, nullptr, org);
+    float* prev = nullptr;
+    if (history_steps > 0) {
+        SUR_CU(cudaMallocAsync(&prev, (size_t)N * kImg * kImg * sizeof(float), v.stream), "jump alloc");
+        rc = relax_extract(s, xin, prev, org, nullptr, nullptr, 0.0f);
+        if (!rc) rc = pfb_sim2d_advance(s, history_steps);
+        if (!rc) rc = relax_extract(s, xin, nullptr, nullptr, org, prev, hist_scale);
+    } else {
+        rc = relax_extract(s, xin, nullptr, org, nullptr, nullptr, 0.0f);
+    }
     for (int b0 = 0; !rc && b0 < N; b0 += n->max_batch) {
         const int B = N - b0 < n->max_batch ? N - b0 : n->max_batch;
         rc = n->forward(xin + (size_t)b0 * kP64 * 16, B, v.stream);
@@ -557,11 +567,14 @@ int pfb_sur2d_jump(pfb_sur2d* n, pfb_sim2d* s) {
     cudaFreeAsync(xin, v.stream);
     cudaFreeAsync(d, v.stream);
     cudaFreeAsync(org, v.stream);
+    if (prev) cudaFreeAsync(prev, v.stream);
     const cudaError_t e = cudaStreamSynchronize(v.stream);
     if (rc) return rc;
     SUR_CU(e, "jump sync");
     return PFB_OK;
 }
+
+int pfb_sur2d_jump(pfb_sur2d* n, pfb_sim2d* s) { return pfb_sur2d_jump_history(n, s, 0, 0.0f); }
 
 // Device time of `iters` forward passes over `batch` images (inputs as they
 // are in the network's buffer), ms per pass.

@@ -16,6 +16,7 @@ from .sim2d import (Sim2D, SimParams2D, domain_side_for, fatal, flags_report,
                     grid_jitter_centres, palmieri_centres, step_coefficients, window_view,
                     world_field)
 from .ensemble import Ensemble2D
+from .surrogate import Surrogate2D
 from .sim3d import (Sim3D, SimParams3D, automatic_brick_edge, calibrate_seed_radius,
                     flags_report3, sequential_centres)
 
@@ -27,4 +28,5 @@ __all__ = [
     "window_view", "world_field", "CELL3D_DTYPE", "FLAG3D_COUNT", "FLAG3D_NAMES", "Cell3D",
     "Layout3D", "MeasureArgs3D", "UpdateArgs3D", "Sim3D", "SimParams3D", "automatic_brick_edge",
     "calibrate_seed_radius", "flags_report3", "sequential_centres", "Ensemble2D",
+    "Surrogate2D",
 ]

@@ -170,6 +170,8 @@ _SIGS = {
     "pfb_sim2d_get_flags": (I, [P, P]),
     "pfb_sim2d_set_state": (I, [P, P, P, C.c_longlong]),
     "pfb_sim2d_pack_traj": (I, [P, P]),
+    "pfb_sim2d_save": (I, [P]),
+    "pfb_sim2d_restore": (I, [P]),
     "pfb_sim2d_bench": (I, [P, I, I, C.POINTER(C.c_double)]),
     "pfb_sim2d_step_args": (I, [P, C.POINTER(StepArgs2D)]),
     "pfb_sim2d_stream": (P, [P]),

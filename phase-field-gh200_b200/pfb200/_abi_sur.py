@@ -17,6 +17,8 @@ _abi._SIGS.update({
     "pfb_conv_status": (I, [C.POINTER(C.c_uint), I]),
     "pfb_sim2d_residual_step": (I, [P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "pfb_sur2d_extract": (I, [P, P, P, P]),
+    "pfb_sur2d_extract_at": (I, [P, P, P, C.c_float, P, P]),
+    "pfb_sur2d_jump_history": (I, [P, P, I, C.c_float]),
     "pfb_sur2d_crop_phi": (I, [P, P, P, P]),
     "pfb_sur2d_insert": (I, [P, P, P]),
     "pfb_sur2d_create": (P, [I, C.c_ulonglong, I]),

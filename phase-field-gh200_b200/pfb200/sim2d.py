@@ -224,6 +224,19 @@ class Sim2D:
         phi = np.ascontiguousarray(phi, dtype=np.float32)
         check(lib().pfb_sim2d_set_state(self._h, ptr(cells), ptr(phi), step), "set_state")
 
+    def save(self) -> None:
+        """In-memory device checkpoint of the current step."""
+        check(lib().pfb_sim2d_save(self._h), "save")
+
+    def restore(self) -> None:
+        check(lib().pfb_sim2d_restore(self._h), "restore")
+
+    def residual_step(self) -> tuple[float, float]:
+        """Advance one step; (max, rms) of |dphi / dt| over that step."""
+        linf, rms = C.c_double(), C.c_double()
+        check(lib().pfb_sim2d_residual_step(self._h, C.byref(linf), C.byref(rms)), "residual")
+        return linf.value, rms.value
+
     def step_args(self) -> StepArgs2D:
         a = StepArgs2D()
         check(lib().pfb_sim2d_step_args(self._h, C.byref(a)), "step_args")

@@ -241,3 +241,19 @@ def test_residual_step_matches_world_difference():
     assert linf.value == pytest.approx(mx, rel=1e-12)
     assert rms.value == pytest.approx(np.sqrt(s2 / area), rel=1e-9)
     s.close()
+
+
+def test_save_restore_returns_to_the_saved_step():
+    p, a = small_sim(steps=5)
+    _, b = small_sim(steps=5)
+    a.save()
+    a.advance(9)
+    a.restore()
+    assert a.step == 5
+    a.advance(7)
+    b.advance(7)
+    assert a.phi().tobytes() == b.phi().tobytes()
+    assert a.cells().tobytes() == b.cells().tobytes()
+    assert a.S().tobytes() == b.S().tobytes()
+    a.close()
+    b.close()
