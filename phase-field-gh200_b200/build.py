@@ -36,7 +36,7 @@ COMMON = [
 ]
 SOURCES = ["step2d.cu", "init2d.cu", "sim2d.cu", "host2d.cpp", "measure3d.cu", "update3d.cu",
            "misc3d.cu", "sim3d.cu", "host3d.cpp", "conv2d_tc.cu",
-           "relax2d.cu", "unet2d.cu"]
+           "relax2d.cu", "unet2d.cu", "ckpt2d.cpp"]
 HEADERS = ["pfb_common.cuh", "device_util.cuh", "pfb_internal.h", "step2d_common.cuh",
            "pfb3d_common.cuh", "ring3d.cuh", "storage2d.cuh",
            "tc_util.cuh"]
@@ -74,7 +74,8 @@ def build(force: bool = False, verbose: bool = False, ptxas_report: bool = False
     lib_path.parent.mkdir(parents=True, exist_ok=True)
     obj_dir.mkdir(parents=True, exist_ok=True)
     headers = [CSRC / h for h in HEADERS] + [INCLUDE / "pfb200.h", INCLUDE / "pfb200_3d.h",
-                                                 INCLUDE / "pfb200_surrogate.h"]
+                                                 INCLUDE / "pfb200_surrogate.h",
+                                                 INCLUDE / "pfb200_ckpt.h"]
     objs = []
     relink = force or not lib_path.exists()
     for src in SOURCES:

@@ -17,6 +17,7 @@ from .sim2d import (Sim2D, SimParams2D, domain_side_for, fatal, flags_report,
                     world_field)
 from .ensemble import Ensemble2D
 from .surrogate import Surrogate2D
+from . import checkpoint
 from .sim3d import (Sim3D, SimParams3D, automatic_brick_edge, calibrate_seed_radius,
                     flags_report3, sequential_centres)
 
