@@ -308,7 +308,19 @@ typedef struct pfb_sim3d pfb_sim3d;
 /* Fresh start from cell centres (world coordinates, substrate centres at
  * z = -0.5 as in the reference); N = p->num_cells entries. */
 pfb_sim3d* pfb_sim3d_create(const pfb_params3d* p, const pfb_vec3* centres, int device);
+/* Restart from cell records and base B^3 bricks (x fastest) of step `step`,
+ * as the reference's Sim3D::init_checkpoint does (src/pf3d/sim.cu:794-885):
+ * the records and bricks become the current state, the aggregate is rebuilt
+ * and the cells are measured once (surface included, no tumble). Ids must be
+ * 0..N-1 and every cell on the base brick. */
+pfb_sim3d* pfb_sim3d_create_from_state(const pfb_params3d* p, const pfb_cell3d* cells,
+                                       const float* phi, long long step, int device);
 void pfb_sim3d_destroy(pfb_sim3d* s);
+/* Measure the current state (moments, surface, support, recentring plan)
+ * and set velocities without a tumble, as the reference does before output
+ * and before writing a checkpoint (Sim3D::ensure_measurements ->
+ * refresh_measurements(false, true), src/pf3d/sim.cu:1301-1377, 2045-2047). */
+int pfb_sim3d_measure_current(pfb_sim3d* s);
 /* Advance `steps` accepted-or-rejected steps (the reference's
  * begin_step/finish_step sequence per step). */
 int pfb_sim3d_advance(pfb_sim3d* s, int steps);

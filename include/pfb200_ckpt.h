@@ -25,6 +25,7 @@
 #include <stdint.h>
 
 #include "pfb200.h"
+#include "pfb200_3d.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -111,6 +112,86 @@ int pfb_sim2d_write_checkpoint(pfb_sim2d* s, const char* path, const pfb_ckpt2d_
  * and step from its cells and tiles (the aggregate is rebuilt by the scatter,
  * the moments are taken from the file). device as pfb_sim2d_create. */
 pfb_sim2d* pfb_sim2d_create_from_checkpoint(const char* path, int device);
+
+/* ======================================================================
+ * 3D checkpoint file (PF3D schema 1) -- replaces pf3d::checkpoint_probe_3d /
+ * checkpoint_load_3d / checkpoint_write_3d (common/checkpoint_format_3d.h,
+ * src/pf3d/checkpoint.cu:116-420, 599-1235). A 96-byte header (magic
+ * "PF3D", schema 1, record sizes, endian marker, 3 dimensions, binary32,
+ * flags CRC + variable storage, step, time, cell count, B, x-fastest order,
+ * B^3 values and bytes per cell, the file's CRC-64/ECMA-182 computed with
+ * this field zero, base measurement CTAs per cell), the 288-byte parameter
+ * record below, then per cell a 256-byte record and its storage_edge^3
+ * binary32 brick. This library writes and reads base bricks only
+ * (storage_edge = B); files with promoted (larger) bricks are rejected with
+ * PFB_E_CONFIG.
+ * ==================================================================== */
+#pragma pack(push, 1)
+/* The reference's ParamsRecord3D (common/checkpoint_format_3d.h:167-227). */
+typedef struct pfb_ckpt3d_params {
+    int64_t Nx, Ny, Nz;                /*   0 */
+    double dx, dy, dz;                 /*  24 */
+    uint32_t brick_edge;               /*  48 */
+    uint32_t boundary_flags;           /*  52 */
+    double dt, t_end, lambda;          /*  56 */
+    double gamma_normal, gamma_soft, soft_fraction;
+    double kappa, target_radius, mu, v_A, v_A_sigma, xi, tau;
+    double volume_fraction;            /* rho_V; rho_A for a slab          */
+    uint64_t seed;                     /* 168 */
+    uint64_t polarity_seed;            /* 176 resolved                      */
+    int64_t print_interval, full_moment_every, verify_every;
+    uint32_t integrator_id;            /* 208: 1 explicit Euler             */
+    uint32_t stencil_id;               /* 2: 27-point                       */
+    uint32_t rng_id;                   /* 1: Philox4x32-10                  */
+    uint32_t trajectory_interval;      /* 220 */
+    uint64_t initialization_hash;      /* 224 */
+    double aging_time;                 /* 232 */
+    uint64_t promoted_measure_policy;  /* 240: 0 one CTA, 1..64, ~0 auto  */
+    uint64_t promoted_measure_auto_wave_ctas;
+    int64_t channel_height, channel_padding;
+    double wall_kappa, wall_width;     /* 272 */
+} pfb_ckpt3d_params;
+#pragma pack(pop)
+
+typedef struct pfb_ckpt3d_info {
+    long long step;
+    double time;
+    int num_cells;
+    int brick_edge;
+    int base_measure_shards; /* stored CTAs per cell of the base measurement */
+    uint64_t crc64;
+} pfb_ckpt3d_info;
+
+/* CRC-64/ECMA-182 (polynomial 0x42F0E1EBA9EA3693, MSB first, initial value
+ * and final xor 0) of n bytes, continuing from crc (0 to start). */
+uint64_t pfb_crc64_ecma(uint64_t crc, const void* data, size_t n);
+
+/* Record of a run with parameters p and brick edge B (0: the automatic
+ * edge): volume fraction realised from the cell count and the domain
+ * (areal coverage for a slab, the accessible slit for a channel), t_end 100,
+ * print interval 100, verify every 4096, the reference's integrator, stencil
+ * and RNG ids, one-CTA promoted-measurement policy. */
+int pfb_ckpt3d_params_from(const pfb_params3d* p, int brick, pfb_ckpt3d_params* out);
+int pfb_ckpt3d_params_to(const pfb_ckpt3d_params* rec, int num_cells, pfb_params3d* out);
+
+/* Read and validate (header, parameters, file size, every record, CRC) as
+ * the reference does. With cells and phi null only info and rec are filled
+ * (the CRC is still verified over the whole file); otherwise cells[N]
+ * (storage_edge 0, derived wall fields zero) and phi[N * B^3]. */
+int pfb_ckpt3d_read(const char* path, pfb_ckpt3d_info* info, pfb_ckpt3d_params* rec,
+                    pfb_cell3d* cells, float* phi);
+
+/* Write cells and base bricks at `step` (time = step * dt) through path.tmp
+ * and a rename; base_measure_shards in 1..64 is stored as the measurement
+ * grouping the continuation should use. Refuses records the reader would
+ * reject. */
+int pfb_ckpt3d_write(const char* path, const pfb_ckpt3d_params* rec, long long step, int num_cells,
+                     const pfb_cell3d* cells, const float* phi, int base_measure_shards);
+
+/* The current state of `s` (its brick edge, 4 measurement CTAs per cell),
+ * measured first (pfb_sim3d_measure_current) as the reference does. */
+int pfb_sim3d_write_checkpoint(pfb_sim3d* s, const char* path, const pfb_ckpt3d_params* rec);
+pfb_sim3d* pfb_sim3d_create_from_checkpoint(const char* path, int device);
 
 #ifdef __cplusplus
 }

@@ -36,7 +36,8 @@ COMMON = [
 ]
 SOURCES = ["step2d.cu", "init2d.cu", "sim2d.cu", "host2d.cpp", "measure3d.cu", "update3d.cu",
            "misc3d.cu", "sim3d.cu", "host3d.cpp", "conv2d_tc.cu",
-           "relax2d.cu", "unet2d.cu", "ckpt2d.cpp"]
+           "relax2d.cu", "unet2d.cu", "ckpt2d.cpp",
+           "ckpt3d.cpp"]
 HEADERS = ["pfb_common.cuh", "device_util.cuh", "pfb_internal.h", "step2d_common.cuh",
            "pfb3d_common.cuh", "ring3d.cuh", "storage2d.cuh",
            "tc_util.cuh"]

@@ -196,7 +196,8 @@ int one_step(pfb_sim3d* s) {
     return PFB_OK;
 }
 
-int create_impl(pfb_sim3d* s, const pfb_params3d* pp, const pfb_vec3* centres, int device) {
+// Buffers, layout and wall field of a system with parameters *pp.
+int alloc_impl(pfb_sim3d* s, const pfb_params3d* pp, int device) {
     s->p = *pp;
     const pfb_params3d& p = s->p;
     PFB3_RC(validate3(p));
@@ -228,6 +229,33 @@ int create_impl(pfb_sim3d* s, const pfb_params3d* pp, const pfb_vec3* centres, i
     PFB3_CU(cudaMemsetAsync(s->d_flags, 0, PFB3D_FLAG_COUNT * sizeof(uint32_t), s->stream), "memset");
     PFB3_CU(cudaMemsetAsync(s->d_step, 0, sizeof(uint64_t), s->stream), "memset");
     if (hard_wall_channel(p.boundary_flags)) PFB3_RC(upload_wall(s));
+    return PFB_OK;
+}
+
+// The measurement that follows a fresh seeding or a restore (reference
+// Sim3D::refresh_measurements(false, true) after reconstruct_current_S,
+// src/pf3d/sim.cu:877, 1175): aggregate from the current bricks, then
+// moments, surface, recentring plan and velocities without a tumble.
+int remeasure_impl(pfb_sim3d* s) {
+    PFB3_RC(clear3d_launch(s->d_S[0], &s->L, nullptr, s->stream));
+    pfb_scatter_args3d sa{};
+    sa.phi = s->d_phi[0];
+    sa.cells = s->d_cells;
+    sa.S = s->d_S[0];
+    sa.global_flags = s->d_flags;
+    sa.layout = s->L;
+    sa.N = s->N;
+    sa.B = s->B;
+    PFB3_RC(scatter3d_launch(&sa, s->stream));
+    const pfb_measure_args3d m = measure_args(s, false, true);
+    PFB3_RC(measure3d_launch(&m, s->stream));
+    PFB3_RC(motion3d_launch(&m, s->stream));
+    return PFB_OK;
+}
+
+int create_impl(pfb_sim3d* s, const pfb_params3d* pp, const pfb_vec3* centres, int device) {
+    PFB3_RC(alloc_impl(s, pp, device));
+    const pfb_params3d& p = s->p;
 
     // per-cell records (reference src/pf3d/sim.cu:1100-1130), soft fraction 0
     std::vector<pfb_cell3d> cells((size_t)s->N);
@@ -271,20 +299,34 @@ int create_impl(pfb_sim3d* s, const pfb_params3d* pp, const pfb_vec3* centres, i
     ia.lambda = (float)p.lambda;
     ia.seed_radius = (float)seed;
     PFB3_RC(init3d_launch(&ia, s->stream));
-    PFB3_RC(clear3d_launch(s->d_S[0], &s->L, nullptr, s->stream));
-    pfb_scatter_args3d sa{};
-    sa.phi = s->d_phi[0];
-    sa.cells = s->d_cells;
-    sa.S = s->d_S[0];
-    sa.global_flags = s->d_flags;
-    sa.layout = s->L;
-    sa.N = s->N;
-    sa.B = s->B;
-    PFB3_RC(scatter3d_launch(&sa, s->stream));
-    const pfb_measure_args3d m = measure_args(s, false, true);
-    PFB3_RC(measure3d_launch(&m, s->stream));
-    PFB3_RC(motion3d_launch(&m, s->stream));
+    PFB3_RC(remeasure_impl(s));
     PFB3_CU(cudaStreamSynchronize(s->stream), "fresh initialisation");
+    return PFB_OK;
+}
+
+// Restore (reference Sim3D::init_checkpoint, src/pf3d/sim.cu:794-885): cell
+// records and base bricks of step `step` into the current buffers, the step
+// counter, then the aggregate and one measurement.
+int restore_impl(pfb_sim3d* s, const pfb_params3d* pp, const pfb_cell3d* cells, const float* phi,
+                 long long step, int device) {
+    if (!cells || !phi || step < 0) return set_error(PFB_E_ARG, "restore: bad argument");
+    PFB3_RC(alloc_impl(s, pp, device));
+    for (int i = 0; i < s->N; ++i)
+        if (cells[i].global_id != i || (cells[i].storage_edge != 0 && (int)cells[i].storage_edge != s->B))
+            return set_error(PFB_E_ARG, "restore: cell %d is not a canonical base-brick record", i);
+    PFB3_CU(cudaMemcpyAsync(s->d_cells, cells, (size_t)s->N * sizeof(pfb_cell3d), cudaMemcpyHostToDevice,
+                            s->stream), "upload cells");
+    PFB3_CU(cudaMemcpyAsync(s->d_phi[0], phi, (size_t)s->N * s->cell_words * sizeof(float),
+                            cudaMemcpyHostToDevice, s->stream), "upload phi");
+    PFB3_CU(cudaMemsetAsync(s->d_phi[1], 0, (size_t)s->N * s->cell_words * sizeof(float), s->stream),
+            "clear phi");
+    const uint64_t st = (uint64_t)step;
+    PFB3_CU(cudaMemcpyAsync(s->d_step, &st, sizeof(st), cudaMemcpyHostToDevice, s->stream), "step");
+    s->steps_done = step;
+    s->cur_phi = 0;
+    s->cur_S = 0;
+    PFB3_RC(remeasure_impl(s));
+    PFB3_CU(cudaStreamSynchronize(s->stream), "restore");
     return PFB_OK;
 }
 
@@ -310,7 +352,36 @@ pfb_sim3d* pfb_sim3d_create(const pfb_params3d* p, const pfb_vec3* centres, int 
     return s;
 }
 
+pfb_sim3d* pfb_sim3d_create_from_state(const pfb_params3d* p, const pfb_cell3d* cells,
+                                       const float* phi, long long step, int device) {
+    clear_error();
+    if (!p || !cells || !phi) {
+        set_error(PFB_E_ARG, "null params, cells or phi");
+        return nullptr;
+    }
+    pfb_sim3d* s = new (std::nothrow) pfb_sim3d();
+    if (!s) {
+        set_error(PFB_E_NOMEM, "host allocation failed");
+        return nullptr;
+    }
+    if (restore_impl(s, p, cells, phi, step, device) != PFB_OK) {
+        delete s;
+        return nullptr;
+    }
+    return s;
+}
+
 void pfb_sim3d_destroy(pfb_sim3d* s) { delete s; }
+
+int pfb_sim3d_measure_current(pfb_sim3d* s) {
+    if (!s) return set_error(PFB_E_ARG, "null sim");
+    PFB3_CU(cudaSetDevice(s->device), "cudaSetDevice");
+    const pfb_measure_args3d m = measure_args(s, false, true);
+    PFB3_RC(measure3d_launch(&m, s->stream));
+    PFB3_RC(motion3d_launch(&m, s->stream));
+    PFB3_CU(cudaStreamSynchronize(s->stream), "measure_current");
+    return PFB_OK;
+}
 
 int pfb_sim3d_advance(pfb_sim3d* s, int steps) {
     if (!s || steps < 0) return set_error(PFB_E_ARG, "invalid advance arguments");

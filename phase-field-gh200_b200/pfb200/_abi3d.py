@@ -161,6 +161,8 @@ _abi._SIGS.update({
     "pfb3d_tumble": (I, [C.c_uint64, C.c_int64, C.c_uint64, C.c_double, I,
                          C.POINTER(C.c_double)]),
     "pfb_sim3d_create": (P, [C.POINTER(Params3D), P, I]),
+    "pfb_sim3d_create_from_state": (P, [C.POINTER(Params3D), P, P, C.c_longlong, I]),
+    "pfb_sim3d_measure_current": (I, [P]),
     "pfb_sim3d_destroy": (None, [P]),
     "pfb_sim3d_advance": (I, [P, I]),
     "pfb_sim3d_sync": (I, [P]),

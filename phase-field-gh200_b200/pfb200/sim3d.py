@@ -131,12 +131,23 @@ def flags_report3(flags: np.ndarray) -> dict[str, int]:
 class Sim3D:
     """Device-resident 3D simulation driven through the C ABI."""
 
-    def __init__(self, params: SimParams3D, centres: np.ndarray, *, device: int = 0):
+    def __init__(self, params: SimParams3D, centres: np.ndarray | None = None, *, device: int = 0,
+                 cells: np.ndarray | None = None, phi: np.ndarray | None = None, step: int = 0):
+        """Fresh start from centres, or a restart from cell records and base
+        bricks (cells, phi) of step `step`."""
         self.params = params
         self._pc = params.to_c()
-        c = np.ascontiguousarray(centres, dtype=np.float64)
-        assert c.shape == (params.num_cells, 3)
-        h = lib().pfb_sim3d_create(C.byref(self._pc), ptr(c), device)
+        if cells is not None:
+            self._cells0 = np.ascontiguousarray(cells, dtype=CELL3D_DTYPE)
+            self._phi0 = np.ascontiguousarray(phi, dtype=np.float32)
+            assert self._cells0.shape == (params.num_cells,)
+            h = lib().pfb_sim3d_create_from_state(C.byref(self._pc), ptr(self._cells0),
+                                                  ptr(self._phi0), step, device)
+            del self._cells0, self._phi0
+        else:
+            c = np.ascontiguousarray(centres, dtype=np.float64)
+            assert c.shape == (params.num_cells, 3)
+            h = lib().pfb_sim3d_create(C.byref(self._pc), ptr(c), device)
         if not h:
             raise RuntimeError("pfb_sim3d_create failed: " + lib().pfb_last_error().decode())
         self._h = h
@@ -161,6 +172,11 @@ class Sim3D:
 
     def sync(self) -> None:
         check(lib().pfb_sim3d_sync(self._h), "sync")
+
+    def measure_current(self) -> None:
+        """Measure the current state and set velocities without a tumble (as
+        the reference does before output and checkpoints)."""
+        check(lib().pfb_sim3d_measure_current(self._h), "measure_current")
 
     def bench(self, warmup: int, steps: int) -> float:
         ms = C.c_double()
