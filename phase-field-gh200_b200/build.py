@@ -38,6 +38,9 @@ SOURCES = ["step2d.cu", "init2d.cu", "sim2d.cu", "host2d.cpp", "measure3d.cu", "
            "misc3d.cu", "sim3d.cu", "host3d.cpp", "conv2d_tc.cu",
            "relax2d.cu", "unet2d.cu", "ckpt2d.cpp",
            "ckpt3d.cpp"]
+# command-line programs over the C ABI, linked against the library
+CLI_SOURCES = {"pfb_cell": "cli2d.cpp"}
+CXX = os.environ.get("CXX", "g++")
 HEADERS = ["pfb_common.cuh", "device_util.cuh", "pfb_internal.h", "step2d_common.cuh",
            "pfb3d_common.cuh", "ring3d.cuh", "storage2d.cuh",
            "tc_util.cuh"]
@@ -96,6 +99,14 @@ def build(force: bool = False, verbose: bool = False, ptxas_report: bool = False
         _run([NVCC, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-cudart", "static"],
              verbose)
         os.replace(tmp, lib_path)
+    if out is None:
+        for exe, src in CLI_SOURCES.items():
+            target = lib_path.parent / exe
+            s_path = CSRC / src
+            if force or _newer(target, [s_path, lib_path, *headers]):
+                _run([CXX, "-std=c++17", "-O2", "-Wall", "-I", str(INCLUDE), str(s_path),
+                      "-L", str(lib_path.parent), "-lpfb200", "-Wl,-rpath,$ORIGIN",
+                      "-o", str(target)], verbose)
     return lib_path
 
 

@@ -1,0 +1,565 @@
+// pfb_cell: the command line of the 2D run, with the reference's options,
+// files and cadences (reference src/main.cu:22-720, src/sim.cu:95-135 fresh
+// centres, 851-1004 run loop, 1095-1140 trajectory rows; src/trajectory.cpp
+// metadata and append rules). Everything goes through the library's C ABI.
+//
+// Supported: the model and run options, resume from a CELL checkpoint (-c),
+// rolling / tagged / final checkpoints, the plain-text trajectory (--out),
+// --bench. Not part of this build (they exit with status 2 and a message):
+// the velocity-moment and boundary recorders, --initial-centres, the mobility
+// map, --morton, --no-l2, --strict and --self-test, and, on resume, overrides
+// of model parameters other than the output cadences and t_end.
+#include <algorithm>
+#include <cerrno>
+#include <cmath>
+#include <csignal>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <sys/stat.h>
+#include <vector>
+
+#include "pfb200.h"
+#include "pfb200_ckpt.h"
+
+namespace {
+
+volatile std::sig_atomic_t g_stop = 0;
+void on_signal(int) { g_stop = 1; }
+
+struct Options {
+    pfb_params2d p{};
+    double rho = 0.90, t_end = 100.0;
+    int print_interval = 100, verify_every = 4096;
+    std::string ckpt_in, ckpt_dir, out_path;
+    long long ckpt_interval = 0, save_interval = 0;
+    bool final_ckpt = true;
+    int traj_samples = 100;
+    long long traj_interval = 0;
+    bool traj_samples_set = false, traj_interval_set = false;
+    bool t_end_set = false, print_set = false, verify_set = false;
+    int device = 0;
+    long long bench = 0;
+    bool graph = true;
+    bool model_override = false;  // a model option given on the command line
+    bool n_or_rho = false;
+};
+
+constexpr double kPi = 3.14159265358979323846;
+
+void usage() {
+    std::printf(
+        "usage: pfb_cell [options]\n"
+        "  --N <int> --radius <f> --rho <f> --lambda <f> --kappa <f> --mu <f> --xi <f>\n"
+        "  --tau <f> --v-A <f> --v-A-sigma <f> --gamma <f> --gamma-cancer <f>\n"
+        "  --cancer-fraction <f> --phase-field-mobility <f> --dt <f> --t-end <f>\n"
+        "  --seed <u64> --polarity-seed <u64> --full-moment <int> --verify-every <int>\n"
+        "  --print-interval <int>  -c|--checkpoint <path>  --checkpoint-interval <n>\n"
+        "  --save-interval <n>  --checkpoint-dir <path>  --no-final-checkpoint\n"
+        "  --trajectory-samples <n>  --trajectory-interval <n>  --out <path>\n"
+        "  --device <int>  --bench <steps>  --no-graph\n");
+}
+
+bool num(const char* s, double* v) {
+    char* e = nullptr;
+    errno = 0;
+    *v = std::strtod(s, &e);
+    return e != s && *e == '\0' && errno == 0 && std::isfinite(*v);
+}
+bool num(const char* s, long long* v) {
+    char* e = nullptr;
+    errno = 0;
+    *v = std::strtoll(s, &e, 10);
+    return e != s && *e == '\0' && errno == 0;
+}
+bool num(const char* s, unsigned long long* v) {
+    char* e = nullptr;
+    errno = 0;
+    *v = std::strtoull(s, &e, 10);
+    return e != s && *e == '\0' && errno == 0;
+}
+
+// FNV-1a 64 over the little-endian bytes of x0, y0, x1, y1, ... (binary32),
+// the reference's centre-table fingerprint (include/palmieri_initializer.hpp:104-121).
+uint64_t table_fnv1a64(const std::vector<float>& x, const std::vector<float>& y) {
+    uint64_t h = 0xcbf29ce484222325ull;
+    for (size_t i = 0; i < x.size(); ++i)
+        for (float f : {x[i], y[i]}) {
+            uint32_t b;
+            std::memcpy(&b, &f, 4);
+            for (int k = 0; k < 4; ++k) {
+                h ^= (b >> (8 * k)) & 0xffu;
+                h *= 0x00000100000001b3ull;
+            }
+        }
+    return h;
+}
+
+long long next_boundary(long long cur, long long every) {
+    if (cur < 0 || every <= 0) return (1LL << 62);
+    const long long r = cur % every;
+    return cur + (r == 0 ? every : every - r);
+}
+
+bool mkdirs(const std::string& dir) {
+    std::string acc;
+    for (size_t i = 0; i <= dir.size(); ++i) {
+        if (i == dir.size() || dir[i] == '/') {
+            if (!acc.empty() && ::mkdir(acc.c_str(), 0777) != 0 && errno != EEXIST) return false;
+        }
+        if (i < dir.size()) acc.push_back(dir[i]);
+    }
+    return true;
+}
+
+// ---- trajectory text (reference src/trajectory.cpp, src/sim.cu:1104-1140) ----
+std::string metadata(const pfb_params2d& p, double rho, uint64_t hash, long long every) {
+    char line[2048];
+    const double area0 = kPi * p.target_radius * p.target_radius;
+    const double realized = (double)p.num_cells * area0 / ((double)p.L * p.L);
+    const unsigned long long pstream = p.polarity_seed ? p.polarity_seed : p.seed;
+    std::snprintf(line, sizeof(line),
+                  "# trajectory_schema=1 dim=2 model=run_tumble N=%d Lx=%d Ly=%d "
+                  "dx=%.17g dy=%.17g dt=%.17g rho_target=%.17g "
+                  "rho_realized=%.17g lambda=%.17g R=%.17g kappa=%.17g mu=%.17g "
+                  "xi=%.17g tau=%.17g v_A=%.17g v_A_sigma=%.17g "
+                  "gamma_normal=%.17g gamma_soft=%.17g soft_fraction=%.17g "
+                  "soft_assignment=lowest_global_ids seed=%llu polarity_seed=%llu "
+                  "initialization_hash=%016llx full_moment=%d perim_offset=%.17g "
+                  "trajectory_interval=%lld",
+                  p.num_cells, p.L, p.L, 1.0, 1.0, p.dt, rho, realized, p.lambda, p.target_radius,
+                  p.kappa, p.mu, p.xi, p.tau, p.v_A, p.v_A_sigma, p.gamma_normal, p.gamma_cancer,
+                  p.cancer_fraction, (unsigned long long)p.seed, pstream, (unsigned long long)hash,
+                  p.full_moment_every, kPi / (2.7386127875258306 / p.lambda), every);
+    return line;
+}
+const char* kTitle = "# Trajectory data";
+const char* kColumns = "# Format: time cell_id x y vx vy px py theta v_A_i L_n volume";
+
+// Open for append: an empty file gets the three header lines; a non-empty one
+// must carry this run's header and whole frames, in canonical id order, with
+// strictly increasing times that end at or before the current step.
+std::FILE* open_trajectory(const std::string& path, const std::string& meta, int N, double dt, long long step) {
+    const size_t slash = path.rfind('/');
+    if (slash != std::string::npos && !mkdirs(path.substr(0, slash))) return nullptr;
+    std::FILE* f = std::fopen(path.c_str(), "a+");
+    if (!f) return nullptr;
+    std::rewind(f);
+    const int c0 = std::fgetc(f);
+    if (c0 == EOF) {
+        std::clearerr(f);
+        std::fseek(f, 0, SEEK_END);
+        std::fprintf(f, "%s\n%s\n%s\n", kTitle, kColumns, meta.c_str());
+        std::fflush(f);
+        return f;
+    }
+    std::rewind(f);
+    std::vector<char> line(1 << 16);
+    auto next = [&]() -> bool {
+        if (!std::fgets(line.data(), (int)line.size(), f)) return false;
+        size_t n = std::strlen(line.data());
+        if (n && line[n - 1] == '\n') line[--n] = '\0';
+        if (n && line[n - 1] == '\r') line[--n] = '\0';
+        return true;
+    };
+    for (const std::string& want : {std::string(kTitle), std::string(kColumns), meta}) {
+        if (!next() || want != line.data()) {
+            std::fprintf(stderr, "[error] refusing to append: trajectory metadata does not match this run\n");
+            std::fclose(f);
+            return nullptr;
+        }
+    }
+    unsigned long long rows = 0;
+    double frame_t = 0.0, prev_t = -1.0;
+    while (next()) {
+        double v[11];
+        long long id = 0;
+        char extra = 0;
+        const int got = std::sscanf(line.data(), "%lf %lld %lf %lf %lf %lf %lf %lf %lf %lf %lf %lf %c", &v[0], &id,
+                                    &v[1], &v[2], &v[3], &v[4], &v[5], &v[6], &v[7], &v[8], &v[9], &v[10], &extra);
+        bool ok = got == 12;
+        for (double x : v) ok = ok && std::isfinite(x);
+        const long long within = (long long)(rows % (unsigned long long)N);
+        if (ok && within == 0) {
+            frame_t = v[0];
+            ok = rows == 0 || frame_t > prev_t;
+        } else if (ok) {
+            ok = v[0] == frame_t;
+        }
+        ok = ok && id == within;
+        if (!ok) {
+            std::fprintf(stderr, "[error] trajectory row %llu is malformed or out of order\n", rows + 1);
+            std::fclose(f);
+            return nullptr;
+        }
+        ++rows;
+        if (rows % (unsigned long long)N == 0) prev_t = frame_t;
+    }
+    if (rows % (unsigned long long)N != 0) {
+        std::fprintf(stderr, "[error] refusing to append to a partial trajectory frame\n");
+        std::fclose(f);
+        return nullptr;
+    }
+    if (rows > 0) {
+        const long long last = std::llround(prev_t / dt);
+        if (std::fabs((double)last * dt - prev_t) > 1e-10 * std::max(1.0, std::fabs(prev_t)) || last > step) {
+            std::fprintf(stderr, "[error] trajectory extends beyond the initialized state\n");
+            std::fclose(f);
+            return nullptr;
+        }
+    }
+    std::clearerr(f);
+    std::fseek(f, 0, SEEK_END);
+    return f;
+}
+
+bool write_frame(std::FILE* f, pfb_sim2d* s, const pfb_params2d& p, long long step,
+                 std::vector<pfb_traj_cell2d>& t) {
+    if (pfb_sim2d_pack_traj(s, t.data()) != PFB_OK) return false;
+    const double Lw = (double)p.L;
+    auto wrap = [Lw](double v) {
+        double m = std::fmod(v, Lw);
+        return m < 0.0 ? m + Lw : m;
+    };
+    for (const pfb_traj_cell2d& c : t) {
+        const double th = (double)c.theta;
+        if (std::fprintf(f, "%.17g %d %.6f %.6f %.6f %.6f %.6f %.6f %.6f %.6f %.6f %.6f\n", (double)step * p.dt,
+                         c.global_id, wrap((double)c.cx), wrap((double)c.cy), (double)c.vx, (double)c.vy,
+                         std::cos(th), std::sin(th), th, (double)c.v_A,
+                         (double)c.perim / (2.0 * kPi * p.target_radius), (double)c.volume) < 0)
+            return false;
+    }
+    return std::fflush(f) == 0;
+}
+
+bool fatal(const uint32_t* flags) {
+    for (int i = 0; i < PFB_FLAG_COUNT; ++i)
+        if (i != PFB_FLAG_SUPPORT_CLIP && flags[i]) return true;
+    return false;
+}
+
+int parse(int argc, char** argv, Options* o) {
+    pfb_params2d& p = o->p;
+    p.num_cells = 288;
+    p.dt = 0.01;
+    p.lambda = 7.0;
+    p.target_radius = 49.0;
+    p.kappa = 10.0;
+    p.mu = 1.0;
+    p.xi = 1500.0;
+    p.tau = 1.0e4;
+    p.v_A = 1.0e-2;
+    p.gamma_normal = 1.0;
+    p.gamma_cancer = 0.35;
+    p.cancer_fraction = 0.0;
+    p.v_A_sigma = 0.0;
+    p.phase_field_mobility = 0.5;
+    p.seed = 1234;
+    p.polarity_seed = 0;
+    p.full_moment_every = 100;
+    for (int i = 1; i < argc; ++i) {
+        const std::string a = argv[i];
+        auto val = [&](void) -> const char* {
+            if (i + 1 >= argc) return nullptr;
+            return argv[++i];
+        };
+        double d;
+        long long n;
+        unsigned long long u;
+        const char* v = nullptr;
+        auto need_d = [&](double* dst, bool model) {
+            v = val();
+            if (!v || !num(v, &d)) return false;
+            *dst = d;
+            o->model_override = o->model_override || model;
+            return true;
+        };
+        if (a == "-h" || a == "--help") {
+            usage();
+            std::exit(0);
+        } else if (a == "--N") {
+            if (!(v = val()) || !num(v, &n) || n <= 0 || n > 4000000) return 2;
+            p.num_cells = (int)n;
+            o->n_or_rho = true;
+        } else if (a == "--radius") {
+            if (!need_d(&p.target_radius, true)) return 2;
+        } else if (a == "--rho") {
+            if (!need_d(&o->rho, false)) return 2;
+            o->n_or_rho = true;
+        } else if (a == "--lambda") {
+            if (!need_d(&p.lambda, true)) return 2;
+        } else if (a == "--kappa") {
+            if (!need_d(&p.kappa, true)) return 2;
+        } else if (a == "--mu") {
+            if (!need_d(&p.mu, true)) return 2;
+        } else if (a == "--xi") {
+            if (!need_d(&p.xi, true)) return 2;
+        } else if (a == "--tau") {
+            if (!need_d(&p.tau, true)) return 2;
+        } else if (a == "--v-A") {
+            if (!need_d(&p.v_A, true)) return 2;
+        } else if (a == "--v-A-sigma") {
+            if (!need_d(&p.v_A_sigma, true)) return 2;
+        } else if (a == "--gamma") {
+            if (!need_d(&p.gamma_normal, true)) return 2;
+        } else if (a == "--gamma-cancer") {
+            if (!need_d(&p.gamma_cancer, true)) return 2;
+        } else if (a == "--cancer-fraction") {
+            if (!need_d(&p.cancer_fraction, true)) return 2;
+        } else if (a == "--phase-field-mobility") {
+            if (!need_d(&p.phase_field_mobility, true)) return 2;
+        } else if (a == "--dt") {
+            if (!need_d(&p.dt, true)) return 2;
+        } else if (a == "--t-end") {
+            if (!need_d(&o->t_end, false)) return 2;
+            o->t_end_set = true;
+        } else if (a == "--seed") {
+            if (!(v = val()) || !num(v, &u)) return 2;
+            p.seed = u;
+            o->model_override = true;
+        } else if (a == "--polarity-seed") {
+            if (!(v = val()) || !num(v, &u)) return 2;
+            p.polarity_seed = u;
+            o->model_override = true;
+        } else if (a == "--full-moment") {
+            if (!(v = val()) || !num(v, &n) || n < 0) return 2;
+            p.full_moment_every = (int)n;
+        } else if (a == "--verify-every") {
+            if (!(v = val()) || !num(v, &n) || n < 0) return 2;
+            o->verify_every = (int)n;
+            o->verify_set = true;
+        } else if (a == "--print-interval") {
+            if (!(v = val()) || !num(v, &n) || n < 0) return 2;
+            o->print_interval = (int)n;
+            o->print_set = true;
+        } else if (a == "-c" || a == "--checkpoint") {
+            if (!(v = val())) return 2;
+            o->ckpt_in = v;
+        } else if (a == "--checkpoint-interval") {
+            if (!(v = val()) || !num(v, &n) || n < 0) return 2;
+            o->ckpt_interval = n;
+        } else if (a == "--save-interval") {
+            if (!(v = val()) || !num(v, &n) || n < 0) return 2;
+            o->save_interval = n;
+        } else if (a == "--checkpoint-dir") {
+            if (!(v = val())) return 2;
+            o->ckpt_dir = v;
+        } else if (a == "--no-final-checkpoint") {
+            o->final_ckpt = false;
+        } else if (a == "--trajectory-samples") {
+            if (!(v = val()) || !num(v, &n) || n <= 0) return 2;
+            o->traj_samples = (int)n;
+            o->traj_samples_set = true;
+        } else if (a == "--trajectory-interval") {
+            if (!(v = val()) || !num(v, &n) || n < 0) return 2;
+            o->traj_interval = n;
+            o->traj_interval_set = true;
+        } else if (a == "--out") {
+            if (!(v = val())) return 2;
+            o->out_path = v;
+        } else if (a == "--device") {
+            if (!(v = val()) || !num(v, &n) || n < 0) return 2;
+            o->device = (int)n;
+        } else if (a == "--bench") {
+            if (!(v = val()) || !num(v, &n) || n <= 0) return 2;
+            o->bench = n;
+        } else if (a == "--no-graph") {
+            o->graph = false;
+        } else if (a == "--velocity-moments" || a == "--velocity-spatial-stride" ||
+                   a == "--velocity-dense-start" || a == "--velocity-moments-reference" ||
+                   a == "--boundary-out" || a == "--boundary-interval" || a == "--boundary-compression" ||
+                   a == "--initial-centres" || a == "--phase-field-mobility-map" || a == "--morton" ||
+                   a == "--no-l2" || a == "--strict" || a == "--self-test") {
+            std::fprintf(stderr, "[fatal] option '%s' is not part of this build\n", a.c_str());
+            return 2;
+        } else {
+            std::fprintf(stderr, "[fatal] unknown option '%s' (try --help)\n", a.c_str());
+            return 2;
+        }
+    }
+    return 0;
+}
+
+long long total_steps(double t_end, double dt) {
+    const double n = t_end / dt + 0.5;
+    return (n >= 0.0 && n <= 9.0e18) ? (long long)n : -1;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    Options o;
+    if (parse(argc, argv, &o)) {
+        std::fprintf(stderr, "[fatal] invalid or missing option value (try --help)\n");
+        return 2;
+    }
+    pfb_params2d p = o.p;
+    uint64_t hash = 0;
+    pfb_sim2d* s = nullptr;
+    pfb_ckpt2d_params rec{};
+    if (!o.ckpt_in.empty()) {
+        if (o.n_or_rho) {
+            std::fprintf(stderr, "[fatal] --N and --rho cannot be overridden on resume\n");
+            return 2;
+        }
+        if (o.model_override) {
+            std::fprintf(stderr, "[fatal] this build resumes with the checkpoint's model parameters; "
+                                 "drop the model options\n");
+            return 2;
+        }
+        pfb_ckpt2d_info info{};
+        if (pfb_ckpt2d_read(o.ckpt_in.c_str(), &info, &rec, nullptr, nullptr) != PFB_OK) {
+            std::fprintf(stderr, "[ckpt] %s\n", pfb_last_error());
+            return 8;
+        }
+        if (pfb_ckpt2d_params_to(&rec, info.num_cells, &p) != PFB_OK) return 8;
+        hash = rec.initialization_hash;
+        o.rho = rec.rho;
+        if (!o.traj_samples_set && !o.traj_interval_set) {
+            o.traj_samples = rec.trajectory_samples;
+            o.traj_interval = rec.trajectory_interval;
+        }
+        if (!o.t_end_set) o.t_end = rec.t_end;
+        if (!o.print_set) o.print_interval = rec.print_interval;
+        if (!o.verify_set) o.verify_every = rec.verify_every;
+        s = pfb_sim2d_create_from_checkpoint(o.ckpt_in.c_str(), o.device);
+    } else {
+        p.L = pfb_domain_side_for(p.num_cells, p.target_radius, o.rho);
+        if (p.L <= 286) {
+            std::fprintf(stderr, "[fatal] domain side %d must exceed 286\n", p.L);
+            return 3;
+        }
+        std::vector<float> x((size_t)p.num_cells), y((size_t)p.num_cells);
+        if (pfb_grid_jitter_centres(p.num_cells, p.L, p.seed, x.data(), y.data()) != PFB_OK) return 3;
+        hash = table_fnv1a64(x, y);
+        s = pfb_sim2d_create(&p, x.data(), y.data(), o.device);
+    }
+    if (!s) {
+        std::fprintf(stderr, "[fatal] initialisation failed: %s\n", pfb_last_error());
+        return 5;
+    }
+    pfb_sim2d_set_graph(s, o.graph ? 1 : 0);
+    const long long total = total_steps(o.t_end, p.dt);
+    if (total < pfb_sim2d_step(s)) {
+        std::fprintf(stderr, "[fatal] t_end ends at step %lld, before the state's step %lld\n", total,
+                     pfb_sim2d_step(s));
+        pfb_sim2d_destroy(s);
+        return 3;
+    }
+    std::printf("pfb_cell: N %d  L %d  dt %g  steps %lld -> %lld  centre table %016llx\n", p.num_cells, p.L, p.dt,
+                pfb_sim2d_step(s), total, (unsigned long long)hash);
+
+    if (o.bench > 0) {
+        double ms = 0.0;
+        if (pfb_sim2d_bench(s, 30, (int)o.bench, &ms) != PFB_OK) {
+            std::fprintf(stderr, "[fatal] bench failed: %s\n", pfb_last_error());
+            pfb_sim2d_destroy(s);
+            return 6;
+        }
+        std::printf("bench: %lld steps -> %.6f ms/step\n", o.bench, ms);
+        pfb_sim2d_destroy(s);
+        return 0;
+    }
+
+    // checkpoint record of this run
+    pfb_ckpt2d_params_from(&p, &rec);
+    rec.t_end = o.t_end;
+    rec.rho = o.rho;
+    rec.initialization_hash = hash;
+    rec.print_interval = o.print_interval;
+    rec.verify_every = o.verify_every;
+    rec.save_interval = (int32_t)o.save_interval;
+    rec.trajectory_samples = o.traj_samples;
+    const long long traj_every = o.traj_interval > 0 ? o.traj_interval
+                                                     : std::max<long long>(1, total / std::max(1, o.traj_samples));
+    rec.trajectory_interval = traj_every;
+    const bool ckpt_on = !o.ckpt_dir.empty() || o.ckpt_interval > 0 || o.save_interval > 0 || !o.ckpt_in.empty();
+    std::string dir = o.ckpt_dir;
+    if (ckpt_on && dir.empty()) {
+        const std::string src = !o.out_path.empty() ? o.out_path : o.ckpt_in;
+        const size_t slash = src.rfind('/');
+        dir = slash == std::string::npos ? "." : src.substr(0, slash);
+    }
+    if (ckpt_on && !mkdirs(dir)) {
+        std::fprintf(stderr, "[fatal] cannot create checkpoint directory %s\n", dir.c_str());
+        pfb_sim2d_destroy(s);
+        return 2;
+    }
+    std::FILE* traj = nullptr;
+    std::vector<pfb_traj_cell2d> rows((size_t)p.num_cells);
+    if (!o.out_path.empty()) {
+        traj = open_trajectory(o.out_path, metadata(p, o.rho, hash, traj_every), p.num_cells, p.dt,
+                               pfb_sim2d_step(s));
+        if (!traj) {
+            pfb_sim2d_destroy(s);
+            return 9;
+        }
+    }
+    std::signal(SIGINT, on_signal);
+    std::signal(SIGTERM, on_signal);
+
+    auto save = [&](const std::string& path) {
+        if (pfb_sim2d_write_checkpoint(s, path.c_str(), &rec) != PFB_OK) {
+            std::fprintf(stderr, "[ckpt] %s\n", pfb_last_error());
+            return false;
+        }
+        std::printf("[ckpt] saved step %lld -> %s\n", pfb_sim2d_step(s), path.c_str());
+        return true;
+    };
+    const long long pi = o.print_interval > 0 ? o.print_interval : total;
+    long long step = pfb_sim2d_step(s);
+    long long next_traj = traj ? next_boundary(step, traj_every) : total + 1;
+    long long next_ckpt = ckpt_on && o.ckpt_interval > 0 ? step + o.ckpt_interval : total + 1;
+    long long next_save = ckpt_on && o.save_interval > 0 ? step + o.save_interval : total + 1;
+    constexpr long long kFatalPoll = 1000;
+    long long next_poll = step + kFatalPoll;
+    bool failed = false;
+    uint32_t flags[PFB_FLAG_COUNT];
+    while (step < total && !failed) {
+        const long long stop = std::min({total, (step / pi + 1) * pi, next_traj, next_ckpt, next_save, next_poll});
+        if (pfb_sim2d_advance(s, stop - step) != PFB_OK) {
+            std::fprintf(stderr, "[fatal] %s\n", pfb_last_error());
+            failed = true;
+            break;
+        }
+        step = stop;
+        if (pfb_sim2d_get_flags(s, flags) != PFB_OK || fatal(flags)) {
+            std::fprintf(stderr, "[fatal] a fatal flag was raised by step %lld\n", step);
+            failed = true;
+            break;
+        }
+        if (step >= next_poll) next_poll = step + kFatalPoll;
+        if (step % pi == 0 || step >= total)
+            std::printf("step %8lld  t %10.3f\n", step, (double)step * p.dt);
+        if (traj && step >= next_traj) {
+            if (!write_frame(traj, s, p, step, rows)) {
+                std::fprintf(stderr, "[error] trajectory write failed at step %lld\n", step);
+                failed = true;
+                break;
+            }
+            next_traj = next_boundary(step, traj_every);
+        }
+        if (step >= next_ckpt) {
+            if (!save(dir + "/checkpoint.bin")) failed = true;
+            next_ckpt = step + o.ckpt_interval;
+        }
+        if (step >= next_save) {
+            char name[64];
+            std::snprintf(name, sizeof(name), "/checkpoint_%08lld.bin", step);
+            if (!save(dir + name)) failed = true;
+            next_save = step + o.save_interval;
+        }
+        if (g_stop) {
+            std::printf("[signal] termination requested at step %lld\n", step);
+            break;
+        }
+    }
+    if (traj) std::fclose(traj);
+    if (ckpt_on && (o.final_ckpt || failed)) {
+        if (!save(dir + (failed ? "/checkpoint_failed.bin" : "/checkpoint.bin"))) failed = true;
+    }
+    pfb_sim2d_destroy(s);
+    return failed ? 9 : 0;
+}

@@ -1,0 +1,73 @@
+"""pfb_cell against the reference's own cell_gh200 (oracle/_ref) on the same
+command line: identical trajectory header (metadata, centre-table hash),
+trajectory rows, and final checkpoints with bit-identical phi; a run resumed
+by one from the other's checkpoint appends to the other's trajectory."""
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from pfb200 import checkpoint as ck
+
+pytestmark = pytest.mark.gpu
+
+ROOT = Path(__file__).resolve().parents[1]
+EXE = ROOT / "phase-field-gh200_b200" / "pfb200" / "_lib" / "pfb_cell"
+REF = ROOT / "oracle" / "_ref" / "cell_gh200"
+ARGS = ("--N", 8, "--radius", 12, "--rho", 0.03, "--seed", 5, "--trajectory-interval", 5,
+        "--print-interval", 0)
+
+
+def run(exe, *args):
+    r = subprocess.run([str(exe), *map(str, args)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    return r
+
+
+def rows(path):
+    lines = Path(path).read_text().splitlines()
+    head = lines[:3]
+    data = np.array([[float(v) for v in ln.split()] for ln in lines[3:]])
+    return head, data
+
+
+def same_rows(a, b):
+    assert a.shape == b.shape
+    np.testing.assert_array_equal(a[:, :2], b[:, :2])        # time, cell id
+    np.testing.assert_allclose(a[:, 2:], b[:, 2:], rtol=0, atol=2e-6)
+
+
+@pytest.mark.skipif(not REF.exists(), reason="reference CLI not built")
+def test_same_command_line_same_outputs(tmp_path):
+    ours, theirs = tmp_path / "ours", tmp_path / "theirs"
+    run(EXE, *ARGS, "--t-end", 0.2, "--out", ours / "traj.txt", "--checkpoint-dir", ours)
+    run(REF, *ARGS, "--t-end", 0.2, "--out", theirs / "traj.txt", "--checkpoint-dir", theirs)
+    ha, ra = rows(ours / "traj.txt")
+    hb, rb = rows(theirs / "traj.txt")
+    assert ha == hb
+    assert ra.shape[0] == 8 * 4
+    same_rows(ra, rb)
+    a, b = ck.read(ours / "checkpoint.bin"), ck.read(theirs / "checkpoint.bin")
+    assert a.step == b.step == 20
+    np.testing.assert_array_equal(a.phi, b.phi)
+    assert bytes(a.params) == bytes(b.params)
+    # each continues the other's run, appending to the other's trajectory
+    run(EXE, "-c", theirs / "checkpoint.bin", "--t-end", 0.3, "--out", theirs / "traj.txt",
+        "--checkpoint-dir", theirs / "next")
+    run(REF, "-c", ours / "checkpoint.bin", "--t-end", 0.3, "--out", ours / "traj.txt",
+        "--checkpoint-dir", ours / "next")
+    ha, ra = rows(ours / "traj.txt")
+    hb, rb = rows(theirs / "traj.txt")
+    assert ha == hb and ra.shape[0] == 8 * 6
+    same_rows(ra, rb)
+    a, b = ck.read(ours / "next" / "checkpoint.bin"), ck.read(theirs / "next" / "checkpoint.bin")
+    np.testing.assert_array_equal(a.phi, b.phi)
+
+
+def test_append_refuses_another_run(tmp_path):
+    run(EXE, *ARGS, "--t-end", 0.1, "--out", tmp_path / "traj.txt")
+    args = ("--N", 8, "--radius", 12, "--rho", 0.03, "--seed", 6, "--t-end", 0.1,
+            "--out", tmp_path / "traj.txt")
+    r = subprocess.run([str(EXE), *map(str, args)], capture_output=True, text=True, timeout=300)
+    assert r.returncode != 0 and "does not match" in r.stderr
