@@ -105,6 +105,15 @@ def rclib() -> C.CDLL:
         L.ref3d_cpu_initial_speed.restype = D
         L.ref3d_cpu_tumble.argtypes = [C.c_uint64, C.c_int64, C.c_uint64, D, I, C.POINTER(D)]
         L.ref3d_cpu_tumble.restype = I
+        F = C.POINTER(C.c_float)
+        L.ref3d_cpu_palmieri2d.argtypes = [I, D, D, C.c_uint64, F, F]
+        L.ref3d_cpu_palmieri2d.restype = I
+        L.ref3d_cpu_palmieri3d.argtypes = [I, D, D, C.c_uint64, F, F, F]
+        L.ref3d_cpu_palmieri3d.restype = I
+        L.ref3d_cpu_channel3d.argtypes = [I, D, I, D, C.c_uint64, F, F, F]
+        L.ref3d_cpu_channel3d.restype = I
+        L.ref3d_cpu_table_hash.argtypes = [I, F, F, F]
+        L.ref3d_cpu_table_hash.restype = C.c_uint64
         _RC = L
     return _RC
 

@@ -1,12 +1,16 @@
 // ORACLE -- test infrastructure only. C entry points over the reference's
 // dense FP64 one-step evaluation and seed-radius calibration
 // (include/pf3d/reference.hpp, header-only; compiled in place by
-// oracle/Makefile into oracle/_ref/libref3d_cpu.so). The tests pin the 3D
-// oracle against it.
+// oracle/Makefile into oracle/_ref/libref3d_cpu.so), and the reference's
+// fresh-start placements and centre-table hash (include/palmieri_initializer.hpp,
+// include/pf3d/palmieri_initializer.hpp, include/pf3d/initializer.hpp). The
+// tests pin the 3D oracle and the placement restatement against it.
 #include <cstdint>
 #include <cstring>
 #include <exception>
 
+#include "palmieri_initializer.hpp"
+#include "pf3d/palmieri_initializer.hpp"
 #include "pf3d/reference.hpp"
 #include "pf3d/rng.cuh"
 
@@ -90,6 +94,55 @@ int ref3d_cpu_tumble(uint64_t step, int64_t gid, uint64_t stream, double p, int 
     out[1] = t.polarity.y;
     out[2] = t.polarity.z;
     return t.tumbled ? 1 : 0;
+}
+
+// Sequential placements: x, y (and z) receive n binary32 centres; 0, or -1
+// when the reference throws.
+static void put(const std::vector<float>& v, float* out) { std::memcpy(out, v.data(), v.size() * 4); }
+
+int ref3d_cpu_palmieri2d(int n, double side, double radius, uint64_t seed, float* x, float* y) {
+    try {
+        std::vector<float> a, b;
+        pf::palmieri_sequential_centres(n, side, radius, seed, &a, &b, nullptr);
+        put(a, x);
+        put(b, y);
+        return 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+int ref3d_cpu_palmieri3d(int n, double side, double radius, uint64_t seed, float* x, float* y,
+                         float* z) {
+    try {
+        std::vector<float> a, b, c;
+        pf3d::palmieri3d_sequential_centres(n, side, radius, seed, &a, &b, &c, nullptr);
+        put(a, x);
+        put(b, y);
+        put(c, z);
+        return 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+int ref3d_cpu_channel3d(int n, double side, int height, double radius, uint64_t seed, float* x,
+                        float* y, float* z) {
+    try {
+        std::vector<float> a, b, c;
+        pf3d::channel3d_sequential_centres(n, side, height, radius, seed, &a, &b, &c, nullptr);
+        put(a, x);
+        put(b, y);
+        put(c, z);
+        return 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+uint64_t ref3d_cpu_table_hash(int n, const float* x, const float* y, const float* z) {
+    const std::vector<float> a(x, x + n), b(y, y + n), c(z, z + n);
+    return pf3d::centre_table_fnv1a64(pf3d::ordered_global_ids((std::size_t)n), a, b, c);
 }
 
 }  // extern "C"

@@ -39,7 +39,7 @@ SOURCES = ["step2d.cu", "init2d.cu", "sim2d.cu", "host2d.cpp", "measure3d.cu", "
            "relax2d.cu", "unet2d.cu", "ckpt2d.cpp",
            "ckpt3d.cpp"]
 # command-line programs over the C ABI, linked against the library
-CLI_SOURCES = {"pfb_cell": "cli2d.cpp"}
+CLI_SOURCES = {"pfb_cell": "cli2d.cpp", "pfb_cell_3d": "cli3d.cpp"}
 CXX = os.environ.get("CXX", "g++")
 HEADERS = ["pfb_common.cuh", "device_util.cuh", "pfb_internal.h", "step2d_common.cuh",
            "pfb3d_common.cuh", "ring3d.cuh", "storage2d.cuh",
@@ -90,9 +90,9 @@ def build(force: bool = False, verbose: bool = False, ptxas_report: bool = False
             cmd = [NVCC, *ARCH, *COMMON, *(f"-D{d}" for d in defines), "-c", str(s), "-o", str(o)]
             if ptxas_report and src.endswith(".cu"):
                 cmd += ["-Xptxas", "-v"]
-            out = _run(cmd, verbose)
-            if ptxas_report and out:
-                print(out)
+            report = _run(cmd, verbose)
+            if ptxas_report and report:
+                print(report)
             relink = True
     if relink or _newer(lib_path, objs):
         tmp = lib_path.with_suffix(".so.tmp")
@@ -104,7 +104,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_report: bool = False
             target = lib_path.parent / exe
             s_path = CSRC / src
             if force or _newer(target, [s_path, lib_path, *headers]):
-                _run([CXX, "-std=c++17", "-O2", "-Wall", "-I", str(INCLUDE), str(s_path),
+                _run([CXX, "-std=c++17", "-O2", "-Wall", "-ffp-contract=off", "-I", str(INCLUDE), str(s_path),
                       "-L", str(lib_path.parent), "-lpfb200", "-Wl,-rpath,$ORIGIN",
                       "-o", str(target)], verbose)
     return lib_path
