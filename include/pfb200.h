@@ -55,12 +55,37 @@ extern "C" {
 #define PFB_NUM_CLASSES 6
 
 /* Runtime velocity-observer accumulator carried inside the cell record
- * (reference common/velocity_moments.h:24-27). Unused by the disabled
- * observation path; kept for layout identity. */
+ * (reference common/velocity_moments.h:24-27): time integrals of the active
+ * velocity (q[0..1]), the interaction velocity (q[2..3]) and the rounding of
+ * the stored binary32 velocity (q[4..5]), and the observed step count.
+ * Updated by the observed steps only. */
 typedef struct pfb_advection_accum {
     double q[6];
     unsigned long long count;
 } pfb_advection_accum;
+
+/* Per-cell spatial-observer state, 240 B (reference
+ * common/velocity_moments.h:29-40, pf::velocity::MomentAccum): q[12] are
+ * the PFVMOM4 integral channels (active, interaction, interfacial,
+ * overlap, area, advection correction; x/y pairs), held[] the interfacial
+ * and overlap rates of the last spatial sample then the normalised
+ * same-cell neighbour overlaps, and the sampling bookkeeping. */
+typedef struct pfb_moment_accum2d {
+    double q[12];
+    unsigned long long count;
+    double held[6];
+    unsigned long long spatial_count;
+    unsigned long long last_sample;
+    unsigned long long last_interval;
+    double last_totals[4];
+    double correction[4];
+} pfb_moment_accum2d;
+
+/* Velocity observation of a step (reference include/kernels.cuh:216,
+ * pf::VelocityStep). */
+#define PFB_VELOCITY_DISABLED 0
+#define PFB_VELOCITY_ADVECTION 1 /* advection accumulators in the cells   */
+#define PFB_VELOCITY_SPATIAL 2   /* + spatial rates into args->moments    */
 
 /* Per-cell state, 192 B, 64-B aligned (reference include/kernels.cuh:27-57). */
 typedef struct pfb_cell2d {
@@ -93,8 +118,9 @@ pfb_cell2d;
 
 /* Arguments of one 2D step launch (reference include/kernels.cuh:74-116).
  * Step counters and cursors are device-resident so a captured CUDA graph can
- * be replayed; `perm` may be null (identity order); `moments` must be null
- * (the spatial observer specialisations are not part of this library). */
+ * be replayed; `perm` may be null (identity order); `moments` (an array of
+ * N pfb_moment_accum2d) is read only by pfb_step2d_launch_observed with
+ * PFB_VELOCITY_SPATIAL and must be null otherwise. */
 typedef struct pfb_step_args2d {
     const float* phi_in;
     float* phi_out;
@@ -206,6 +232,25 @@ int pfb_step2d_launch(const pfb_step_args2d* args, int cluster, void* stream);
  * thread-block cluster per cell, the only variant of this version). */
 int pfb_step2d_launch_ex(const pfb_step_args2d* args, int cluster, int variant,
                          void* stream);
+
+/* The step with a velocity observer fused in (reference launch_step's
+ * VelocityStep argument, include/kernels.cuh:216-225, and the observer
+ * specialisations of include/fused_moments.cuh): PFB_VELOCITY_ADVECTION
+ * integrates the active, interaction and rounding velocities into each
+ * cell's `advection` record; PFB_VELOCITY_SPATIAL additionally closes the
+ * held-rate interval of args->moments and measures new interfacial and
+ * overlap rates (FP64) from the same pass over phi^n. The field and every
+ * other cell field come out bit-identical to the unobserved step. binary32
+ * pools only. */
+int pfb_step2d_launch_observed(const pfb_step_args2d* args, int cluster, int observation,
+                               void* stream);
+
+/* Independent dense observer (reference src/velocity_moments.cu,
+ * launch_velocity_moments): adds physical_dt times the twelve velocity
+ * channels of the field args->phi_in to out[n].q and counts the step. One
+ * CTA per cell; shares no reduction with the step. */
+int pfb_velocity_moments2d(const pfb_step_args2d* args, pfb_moment_accum2d* out,
+                           double physical_dt, void* stream);
 
 /* Library status word kept in device memory: bit 0 is set when a CTA gave up
  * waiting for its staged band (a bounded wait that is never expected to run
@@ -332,6 +377,23 @@ int pfb_sim2d_restore(pfb_sim2d* s);
 int pfb_sim2d_bench(pfb_sim2d* s, int warmup, int steps, double* ms_per_step);
 /* Device pointers for callers that drive kernels themselves. */
 int pfb_sim2d_step_args(pfb_sim2d* s, pfb_step_args2d* out);
+
+/* PFVMOM4 velocity-component recorder (reference src/velocity_output.cu,
+ * include/velocity_sampling.hpp; file layout common/velocity_format.h):
+ * opens a NEW file at `path` (an existing one is refused) and writes the
+ * 56-byte header and the frame of the current step. While open, every step
+ * taken by pfb_sim2d_advance is observed: spatially on the first step, on
+ * the `dense_start` steps that follow the open and on steps that are
+ * multiples of `spatial_stride` (1..1000), by advection otherwise; with
+ * `reference` != 0 the dense independent observer runs before every step
+ * instead. Steps are launched one by one while a recorder is open. */
+int pfb_sim2d_velocity_open(pfb_sim2d* s, const char* path, int spatial_stride,
+                            long long dense_start, int reference);
+/* Append the frame of the current step (int64 step, N x 26 float64). */
+int pfb_sim2d_velocity_capture(pfb_sim2d* s);
+/* Step of the last frame written, -1 when none is open. */
+long long pfb_sim2d_velocity_last_frame(const pfb_sim2d* s);
+int pfb_sim2d_velocity_close(pfb_sim2d* s);
 void* pfb_sim2d_stream(pfb_sim2d* s);
 
 /* ---- batched ensemble (no reference counterpart) --------------------------

@@ -5,10 +5,12 @@
 //
 // Supported: the model and run options, resume from a CELL checkpoint (-c),
 // rolling / tagged / final checkpoints, the plain-text trajectory (--out),
-// --bench. Not part of this build (they exit with status 2 and a message):
-// the velocity-moment and boundary recorders, --initial-centres, the mobility
-// map, --morton, --no-l2, --strict and --self-test, and, on resume, overrides
-// of model parameters other than the output cadences and t_end.
+// the PFVMOM4 velocity-moment recorder (--velocity-moments; reference
+// src/velocity_output.cu), --bench. Not part of this build (they exit with
+// status 2 and a message): the boundary recorder, --initial-centres, the
+// mobility map, --morton, --no-l2, --strict and --self-test, velocity
+// observation under --bench, and, on resume, overrides of model parameters
+// other than the output cadences and t_end.
 #include <algorithm>
 #include <cerrno>
 #include <cmath>
@@ -45,6 +47,10 @@ struct Options {
     bool graph = true;
     bool model_override = false;  // a model option given on the command line
     bool n_or_rho = false;
+    std::string vel_path;
+    int vel_stride = 100;
+    long long vel_dense = 10000;
+    bool vel_reference = false, vel_given = false;
 };
 
 constexpr double kPi = 3.14159265358979323846;
@@ -59,7 +65,9 @@ void usage() {
         "  --print-interval <int>  -c|--checkpoint <path>  --checkpoint-interval <n>\n"
         "  --save-interval <n>  --checkpoint-dir <path>  --no-final-checkpoint\n"
         "  --trajectory-samples <n>  --trajectory-interval <n>  --out <path>\n"
-        "  --device <int>  --bench <steps>  --no-graph\n");
+        "  --device <int>  --bench <steps>  --no-graph\n"
+        "  --velocity-moments <path>  --velocity-spatial-stride <1..1000>\n"
+        "  --velocity-dense-start <int>  --velocity-moments-reference\n");
 }
 
 bool num(const char* s, double* v) {
@@ -367,9 +375,22 @@ int parse(int argc, char** argv, Options* o) {
             o->bench = n;
         } else if (a == "--no-graph") {
             o->graph = false;
-        } else if (a == "--velocity-moments" || a == "--velocity-spatial-stride" ||
-                   a == "--velocity-dense-start" || a == "--velocity-moments-reference" ||
-                   a == "--boundary-out" || a == "--boundary-interval" || a == "--boundary-compression" ||
+        } else if (a == "--velocity-moments") {
+            if (!(v = val())) return 2;
+            o->vel_path = v;
+            o->vel_given = true;
+        } else if (a == "--velocity-spatial-stride") {
+            if (!(v = val()) || !num(v, &n) || n < 1 || n > 1000) return 2;
+            o->vel_stride = (int)n;
+            o->vel_given = true;
+        } else if (a == "--velocity-dense-start") {
+            if (!(v = val()) || !num(v, &n) || n < 0 || n > 1000000000) return 2;
+            o->vel_dense = n;
+            o->vel_given = true;
+        } else if (a == "--velocity-moments-reference") {
+            o->vel_reference = true;
+            o->vel_given = true;
+        } else if (a == "--boundary-out" || a == "--boundary-interval" || a == "--boundary-compression" ||
                    a == "--initial-centres" || a == "--phase-field-mobility-map" || a == "--morton" ||
                    a == "--no-l2" || a == "--strict" || a == "--self-test") {
             std::fprintf(stderr, "[fatal] option '%s' is not part of this build\n", a.c_str());
@@ -393,6 +414,18 @@ int main(int argc, char** argv) {
     Options o;
     if (parse(argc, argv, &o)) {
         std::fprintf(stderr, "[fatal] invalid or missing option value (try --help)\n");
+        return 2;
+    }
+    if (o.vel_given && (o.vel_path.empty() || (o.out_path.empty() && o.bench == 0))) {
+        std::fprintf(stderr, "[fatal] velocity recording requires --velocity-moments and --out\n");
+        return 2;
+    }
+    if (o.vel_given && o.bench > 0) {
+        std::fprintf(stderr, "[fatal] velocity observation under --bench is not part of this build\n");
+        return 2;
+    }
+    if (!o.vel_path.empty() && o.vel_path == o.out_path) {
+        std::fprintf(stderr, "[fatal] output files must use distinct paths\n");
         return 2;
     }
     pfb_params2d p = o.p;
@@ -497,6 +530,14 @@ int main(int argc, char** argv) {
             return 9;
         }
     }
+    if (!o.vel_path.empty() &&
+        pfb_sim2d_velocity_open(s, o.vel_path.c_str(), o.vel_stride, o.vel_dense, o.vel_reference ? 1 : 0) !=
+            PFB_OK) {
+        std::fprintf(stderr, "[velocity] %s\n", pfb_last_error());
+        if (traj) std::fclose(traj);
+        pfb_sim2d_destroy(s);
+        return 9;
+    }
     std::signal(SIGINT, on_signal);
     std::signal(SIGTERM, on_signal);
 
@@ -540,6 +581,12 @@ int main(int argc, char** argv) {
                 break;
             }
             next_traj = next_boundary(step, traj_every);
+            // a velocity frame rides with every trajectory frame
+            if (!o.vel_path.empty() && pfb_sim2d_velocity_capture(s) != PFB_OK) {
+                std::fprintf(stderr, "[velocity] %s\n", pfb_last_error());
+                failed = true;
+                break;
+            }
         }
         if (step >= next_ckpt) {
             if (!save(dir + "/checkpoint.bin")) failed = true;
@@ -557,6 +604,14 @@ int main(int argc, char** argv) {
         }
     }
     if (traj) std::fclose(traj);
+    if (!o.vel_path.empty()) {
+        // a closing frame of a valid state, then close the file
+        if (!failed && pfb_sim2d_velocity_last_frame(s) != step && pfb_sim2d_velocity_capture(s) != PFB_OK) {
+            std::fprintf(stderr, "[velocity] %s\n", pfb_last_error());
+            failed = true;
+        }
+        if (pfb_sim2d_velocity_close(s) != PFB_OK) failed = true;
+    }
     if (ckpt_on && (o.final_ckpt || failed)) {
         if (!save(dir + (failed ? "/checkpoint_failed.bin" : "/checkpoint.bin"))) failed = true;
     }

@@ -32,6 +32,27 @@ int step2d_launch_variant(const pfb_step_args2d* a, int cluster, int variant,
 // values at the same tile positions; clusters of 2 or 4)
 int step2d_launch_storage(const pfb_step_args2d* a, int cluster, int variant, int storage,
                           cudaStream_t stream);
+// The step with a velocity observer (PFB_VELOCITY_*), binary32 pools.
+int step2d_launch_observed(const pfb_step_args2d* a, int cluster, int observation,
+                           cudaStream_t stream);
+
+// Velocity observation (velocity2d.cu): the dense observer and the PFVMOM4
+// recorder a pfb_sim2d drives.
+int velocity2d_observe(const pfb_step_args2d& A, pfb_moment_accum2d* out, double dt,
+                       cudaStream_t stream);
+struct Velocity2D;
+Velocity2D* velocity2d_create(const char* path, int N, double dt, int stride, long long dense,
+                              int reference);
+void velocity2d_destroy(Velocity2D* v);
+int velocity2d_open(Velocity2D* v, const pfb_step_args2d& A, long long step, cudaStream_t stream);
+// Observation of the step about to run from `step`: sets *observation and
+// A->moments (and runs the dense observer first in the reference mode).
+int velocity2d_prepare(Velocity2D* v, pfb_step_args2d* A, long long step, cudaStream_t stream,
+                       int* observation);
+void velocity2d_advanced(Velocity2D* v);
+int velocity2d_capture(Velocity2D* v, const pfb_step_args2d& A, long long step, cudaStream_t stream);
+long long velocity2d_last_frame(const Velocity2D* v);
+int velocity2d_close(Velocity2D* v);
 
 // init2d.cu
 int init_tiles2d(float* phi_a, float* phi_b, pfb_cell2d* cell, const uint8_t* cls, int N, int L,

@@ -55,8 +55,10 @@ struct pfb_sim2d {
     bool graph_ready = false;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
+    Velocity2D* vel = nullptr;  // open PFVMOM4 recorder
 
     ~pfb_sim2d() {
+        if (vel) velocity2d_destroy(vel);
         if (graph_exec) cudaGraphExecDestroy(graph_exec);
         if (graph) cudaGraphDestroy(graph);
         if (stream) cudaStreamDestroy(stream);
@@ -194,7 +196,25 @@ struct pfb_sim2d {
         return PFB_OK;
     }
 
+    // One observed step while a velocity recorder is open.
+    int launch_observed() {
+        pfb_step_args2d a = args_for_slot((int)(steps_done % 6));
+        int obs = PFB_VELOCITY_DISABLED;
+        int rc = velocity2d_prepare(vel, &a, steps_done, stream, &obs);
+        if (rc) return rc;
+        if ((rc = step2d_launch_observed(&a, cluster, obs, stream))) return rc;
+        velocity2d_advanced(vel);
+        return PFB_OK;
+    }
+
     int advance(long long steps) {
+        if (vel) {
+            for (; steps > 0; --steps, ++steps_done) {
+                const int rc = launch_observed();
+                if (rc) return rc;
+            }
+            return PFB_OK;
+        }
         while (steps > 0) {
             if (use_graph && !graph_ready) {
                 const int rc = build_graph();
@@ -380,6 +400,56 @@ int pfb_step2d_launch(const pfb_step_args2d* args, int cluster, void* stream) {
 
 int pfb_step2d_launch_ex(const pfb_step_args2d* args, int cluster, int variant, void* stream) {
     return step2d_launch_variant(args, cluster, variant, as_stream(stream));
+}
+
+int pfb_step2d_launch_observed(const pfb_step_args2d* args, int cluster, int observation,
+                               void* stream) {
+    return step2d_launch_observed(args, cluster, observation, as_stream(stream));
+}
+
+int pfb_velocity_moments2d(const pfb_step_args2d* args, pfb_moment_accum2d* out,
+                           double physical_dt, void* stream) {
+    if (!args) return set_error(PFB_E_ARG, "null step arguments");
+    if (!(physical_dt > 0.0)) return set_error(PFB_E_ARG, "physical_dt must be positive");
+    return velocity2d_observe(*args, out, physical_dt, as_stream(stream));
+}
+
+int pfb_sim2d_velocity_open(pfb_sim2d* s, const char* path, int spatial_stride,
+                            long long dense_start, int reference) {
+    if (!s) return set_error(PFB_E_ARG, "null system");
+    if (s->vel) return set_error(PFB_E_STATE, "a velocity recorder is already open");
+    if (s->p.phi_storage != 0)
+        return set_error(PFB_E_CONFIG, "velocity observation needs binary32 phi pools");
+    PFB_CU(cudaSetDevice(s->device), "cudaSetDevice");
+    Velocity2D* v = velocity2d_create(path, s->N, s->p.dt, spatial_stride, dense_start, reference);
+    if (!v) return PFB_E_ARG;
+    const pfb_step_args2d a = s->args_for_slot((int)(s->steps_done % 6));
+    const int rc = velocity2d_open(v, a, s->steps_done, s->stream);
+    if (rc) {
+        velocity2d_destroy(v);
+        return rc;
+    }
+    s->vel = v;
+    return PFB_OK;
+}
+
+int pfb_sim2d_velocity_capture(pfb_sim2d* s) {
+    if (!s || !s->vel) return set_error(PFB_E_STATE, "no velocity recorder is open");
+    PFB_CU(cudaSetDevice(s->device), "cudaSetDevice");
+    const pfb_step_args2d a = s->args_for_slot((int)(s->steps_done % 6));
+    return velocity2d_capture(s->vel, a, s->steps_done, s->stream);
+}
+
+long long pfb_sim2d_velocity_last_frame(const pfb_sim2d* s) {
+    return s && s->vel ? velocity2d_last_frame(s->vel) : -1;
+}
+
+int pfb_sim2d_velocity_close(pfb_sim2d* s) {
+    if (!s || !s->vel) return set_error(PFB_E_STATE, "no velocity recorder is open");
+    const int rc = velocity2d_close(s->vel);
+    velocity2d_destroy(s->vel);
+    s->vel = nullptr;
+    return rc;
 }
 
 int pfb_init_tiles2d(float* phi_a, float* phi_b, pfb_cell2d* cell, const uint8_t* cls, int N,

@@ -52,20 +52,26 @@ namespace pfb {
 constexpr int kThreads = PFB_STEP2D_THREADS;
 constexpr int kWarps = kThreads / 32;
 constexpr int kHeaderBytes = 2048;
+// the spatial velocity observer's kernels: room for its reduction arrays
+constexpr int kHeaderBytesObs = 2560;
+template <int OBS>
+constexpr int kHeader = OBS == PFB_VELOCITY_SPATIAL ? kHeaderBytesObs : kHeaderBytes;
 
 // Status word of this kernel family in device memory: bit 0 = a CTA gave up
 // waiting for its staged band. Read with pfb_device_status().
 __device__ unsigned int g_step2d_status = 0u;
 
-template <int K>
+template <int K, int OBS = PFB_VELOCITY_DISABLED>
 struct __align__(16) StepShared {
     uint64_t bar;
     int abort;
     int gx0, gy0;
     CellPlan plan;
-    RedScratch<kWarps, K> red;
+    RedScratch<kWarps, K, kObsVals<OBS>> red;
 };
 static_assert(sizeof(StepShared<8>) <= kHeaderBytes, "shared header too large");
+static_assert(sizeof(StepShared<8, PFB_VELOCITY_SPATIAL>) <= kHeaderBytesObs,
+              "observer shared header too large");
 
 __host__ __device__ constexpr int band_rows(int wy, int k) { return (wy + k - 1) / k; }
 
@@ -122,13 +128,14 @@ __device__ __forceinline__ void stencil4(float ws, float4 vs, float es, float wc
 }
 
 // Both staged arrays use the row pitch WX + 8 words.
-__host__ __device__ constexpr int staged_bytes(int cls, int k) {
-    return kHeaderBytes + (2 * band_rows(window_of(cls).wy, k) + 6) * (window_of(cls).wx + 8) * 4;
+__host__ __device__ constexpr int staged_bytes(int cls, int k, int header = kHeaderBytes) {
+    return header + (2 * band_rows(window_of(cls).wy, k) + 6) * (window_of(cls).wx + 8) * 4;
 }
 
-__host__ __device__ constexpr int step_smem_bytes(int k) {
+__host__ __device__ constexpr int step_smem_bytes(int k, int header = kHeaderBytes) {
     int m = 0;
-    for (int c = 0; c <= 3; ++c) m = staged_bytes(c, k) > m ? staged_bytes(c, k) : m;
+    for (int c = 0; c <= 3; ++c)
+        m = staged_bytes(c, k, header) > m ? staged_bytes(c, k, header) : m;
     return m;
 }
 
@@ -193,7 +200,7 @@ __device__ __forceinline__ void store_zero(T* o) {
 //                          (f32 bits); on full-moment steps phi^{n+1} is
 //                          written over it.
 // ---------------------------------------------------------------------------
-template <int CLS, int K, typename T>
+template <int CLS, int K, typename T, int OBS>
 __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int rank,
                                             char* smem, unsigned long long step, bool fm) {
     constexpr Window W = window_of(CLS);
@@ -204,10 +211,10 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
     static_assert(WY % K == 0, "staged classes split into equal bands");
     static_assert((WX * 4) % 16 == 0 && (TX0 * 4) % 16 == 0, "bulk copies need 16-B rows");
 
-    StepShared<K>& sh = *reinterpret_cast<StepShared<K>*>(smem);
+    StepShared<K, OBS>& sh = *reinterpret_cast<StepShared<K, OBS>*>(smem);
     const CellPlan& P = sh.plan;
-    float* phi_s = reinterpret_cast<float*>(smem + kHeaderBytes);
-    uint32_t* ps_s = reinterpret_cast<uint32_t*>(smem + kHeaderBytes + PHI_ROWS * PX * 4);
+    float* phi_s = reinterpret_cast<float*>(smem + kHeader<OBS>);
+    uint32_t* ps_s = reinterpret_cast<uint32_t*>(smem + kHeader<OBS> + PHI_ROWS * PX * 4);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int y0 = rank * RB;
@@ -268,7 +275,8 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
             }
         }
 #undef PFB_G2S
-        if (lane == 0) plan_cell(A, n, CLS, step, sh.plan, rank == 0);
+        if (lane == 0)
+            plan_cell<OBS == PFB_VELOCITY_SPATIAL>(A, n, CLS, step, sh.plan, rank == 0);
     } else {
         const int t = tid - 32;
         constexpr int NT = kThreads - 32;
@@ -354,6 +362,7 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
         e = row[4];
     };
     double aIx = 0.0, aIy = 0.0;
+    ObsAcc<OBS> ob;
     if (active) {
         float ws, es, wc, ec;
         float4 vs, vc;
@@ -378,6 +387,12 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
                 const float gy = 0.5f * (Nv[j] - Sv[j]);
                 aIx += (double)(cC * gx * So);
                 aIy += (double)(cC * gy * So);
+                if constexpr (OBS == PFB_VELOCITY_SPATIAL) {
+                    const float S6[6] = {ws, vs.x, vs.y, vs.z, vs.w, es};
+                    const float N6[6] = {wn, vn.x, vn.y, vn.z, vn.w, en};
+                    ob.pixel(P, A.rep_coeff, x0 + j, y0 + r0 + r, cC, C[j + 2], C[j], Nv[j], Sv[j],
+                             N6[j + 2], N6[j], S6[j + 2], S6[j], So);
+                }
             }
             qrow += PX;
             ws = wc;
@@ -390,7 +405,7 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
         // counted twice: the reference evaluates S_other in both passes
         if (neg) atomicAdd(A.flags + PFB_FLAG_S_NEGATIVE, 2u * neg);
     }
-    reduce_force<K, kWarps>(A, P, rank, sh.red, aIx, aIy, &g_step2d_status);
+    reduce_force<K, kWarps, OBS>(A, P, rank, sh.red, aIx, aIy, ob, &g_step2d_status);
 
     const float gam = P.gam, dwC = P.dwC, volC = P.volC;
     const float vx = sh.red.vx, vy = sh.red.vy, mrel = P.mrel;
@@ -652,17 +667,18 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
     reduce_moments<K, kWarps>(A, P, rank, sh.red, fm, acc, &g_step2d_status);
 }
 
-template <int CLS, int K>
+template <int CLS, int K, int OBS>
 __device__ __forceinline__ void global_cell_v1(const pfb_step_args2d& A, int n, int rank,
                                                char* smem, unsigned long long step, bool fm) {
-    StepShared<K>& sh = *reinterpret_cast<StepShared<K>*>(smem);
-    if (threadIdx.x == 0) plan_cell(A, n, CLS, step, sh.plan, rank == 0);
+    StepShared<K, OBS>& sh = *reinterpret_cast<StepShared<K, OBS>*>(smem);
+    if (threadIdx.x == 0)
+        plan_cell<OBS == PFB_VELOCITY_SPATIAL>(A, n, CLS, step, sh.plan, rank == 0);
     __syncthreads();
-    global_cell<CLS, K, kWarps>(A, sh.plan, rank, sh.red, fm, &g_step2d_status);
+    global_cell<CLS, K, kWarps, OBS>(A, sh.plan, rank, sh.red, fm, &g_step2d_status);
 }
 
 // One system's step for CTA `lb` of the `nb` CTAs that serve it.
-template <int K, typename T>
+template <int K, typename T, int OBS = PFB_VELOCITY_DISABLED>
 __device__ __forceinline__ void step_body(const pfb_step_args2d& A, int lb, int nb, char* smem) {
     const int tid = threadIdx.x;
 
@@ -683,24 +699,24 @@ __device__ __forceinline__ void step_body(const pfb_step_args2d& A, int lb, int 
     const bool fm = full_moment_step(A, step);
 
     const int rank = (int)dev::cluster_rank();
-    StepShared<K>& sh = *reinterpret_cast<StepShared<K>*>(smem);
-    if (tid == 0) red_init<kWarps, K>(sh.red, rank);
+    StepShared<K, OBS>& sh = *reinterpret_cast<StepShared<K, OBS>*>(smem);
+    if (tid == 0) red_init(sh.red, rank);
     dev::cluster_arrive_relaxed();  // matched by the wait in reduce_force
     const int slot = lb / K;
     const int n = A.perm ? (int)A.perm[slot] : slot;
     const int cls = (int)A.cell_cls[n];
     switch (cls) {
-        case 0: staged_cell<0, K, T>(A, n, rank, smem, step, fm); break;
-        case 1: staged_cell<1, K, T>(A, n, rank, smem, step, fm); break;
-        case 2: staged_cell<2, K, T>(A, n, rank, smem, step, fm); break;
-        case 3: staged_cell<3, K, T>(A, n, rank, smem, step, fm); break;
+        case 0: staged_cell<0, K, T, OBS>(A, n, rank, smem, step, fm); break;
+        case 1: staged_cell<1, K, T, OBS>(A, n, rank, smem, step, fm); break;
+        case 2: staged_cell<2, K, T, OBS>(A, n, rank, smem, step, fm); break;
+        case 3: staged_cell<3, K, T, OBS>(A, n, rank, smem, step, fm); break;
         case 4:
             if constexpr (Store<T>::kHalf) {
                 // 16-bit pools: the global-memory classes are not provided
                 if (rank == 0 && tid == 0) atomicAdd(A.flags + PFB_FLAG_CLASS_UNSUPPORTED, 1u);
                 dev::cluster_wait();
             } else {
-                global_cell_v1<4, K>(A, n, rank, smem, step, fm);
+                global_cell_v1<4, K, OBS>(A, n, rank, smem, step, fm);
             }
             break;
         case 5:
@@ -708,7 +724,7 @@ __device__ __forceinline__ void step_body(const pfb_step_args2d& A, int lb, int 
                 if (rank == 0 && tid == 0) atomicAdd(A.flags + PFB_FLAG_CLASS_UNSUPPORTED, 1u);
                 dev::cluster_wait();
             } else {
-                global_cell_v1<5, K>(A, n, rank, smem, step, fm);
+                global_cell_v1<5, K, OBS>(A, n, rank, smem, step, fm);
             }
             break;
         default:
@@ -718,11 +734,11 @@ __device__ __forceinline__ void step_body(const pfb_step_args2d& A, int lb, int 
     }
 }
 
-template <int K, typename T = float>
+template <int K, typename T = float, int OBS = PFB_VELOCITY_DISABLED>
 __global__ void __launch_bounds__(kThreads, PFB_STEP2D_MINB)
     k_step2d(const __grid_constant__ pfb_step_args2d A) {
     extern __shared__ __align__(128) char smem[];
-    step_body<K, T>(A, (int)blockIdx.x, (int)gridDim.x, smem);
+    step_body<K, T, OBS>(A, (int)blockIdx.x, (int)gridDim.x, smem);
 }
 
 // Many independent systems in one launch: system r is served by CTAs
@@ -772,10 +788,22 @@ static cudaError_t configure_pool() {
                                 cudaFuncAttributePreferredSharedMemoryCarveout, 100);
 }
 
+template <int K, int OBS>
+static cudaError_t configure_observed() {
+    cudaError_t e = cudaFuncSetAttribute(k_step2d<K, float, OBS>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         step_smem_bytes(K, kHeader<OBS>));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_step2d<K, float, OBS>,
+                                cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+}
+
 template <int K>
 static cudaError_t configure_one() {
     cudaError_t e = configure_pool<K, float>();
     if (e != cudaSuccess) return e;
+    if ((e = configure_observed<K, PFB_VELOCITY_ADVECTION>()) != cudaSuccess) return e;
+    if ((e = configure_observed<K, PFB_VELOCITY_SPATIAL>()) != cudaSuccess) return e;
     if constexpr (K != 8) {
         if ((e = configure_pool<K, __half>()) != cudaSuccess) return e;
         if ((e = configure_pool<K, __nv_bfloat16>()) != cudaSuccess) return e;
@@ -798,12 +826,12 @@ int step2d_configure_device() {
 
 int step2d_smem_bytes(int k) { return step_smem_bytes(k); }
 
-template <int K, typename T = float>
+template <int K, typename T = float, int OBS = PFB_VELOCITY_DISABLED>
 static cudaError_t launch_k(const pfb_step_args2d& A, cudaStream_t stream) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(A.N * K), 1, 1);
     cfg.blockDim = dim3(kThreads, 1, 1);
-    cfg.dynamicSmemBytes = (size_t)step_smem_bytes(K);
+    cfg.dynamicSmemBytes = (size_t)step_smem_bytes(K, kHeader<OBS>);
     cfg.stream = stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -812,11 +840,11 @@ static cudaError_t launch_k(const pfb_step_args2d& A, cudaStream_t stream) {
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k_step2d<K, T>, A);
+    return cudaLaunchKernelEx(&cfg, k_step2d<K, T, OBS>, A);
 }
 
-int step2d_launch_storage(const pfb_step_args2d* a, int cluster, int variant, int storage,
-                          cudaStream_t stream) {
+// Contract checks common to every single-system launch.
+static int check_step_args(const pfb_step_args2d* a) {
     if (!a) return set_error(PFB_E_ARG, "null step arguments");
     const pfb_step_args2d& A = *a;
     if (!A.phi_in || !A.phi_out || !A.S_rd || !A.S_sc || !A.cell || !A.cell_cls || !A.step_rd ||
@@ -826,18 +854,26 @@ int step2d_launch_storage(const pfb_step_args2d* a, int cluster, int variant, in
     if (((uintptr_t)A.phi_in & 15u) || ((uintptr_t)A.phi_out & 15u) ||
         ((uintptr_t)A.S_cl & 15u) || ((uintptr_t)A.S_rd & 15u))
         return set_error(PFB_E_ARG, "phi pools and S slots must be 16-byte aligned");
-    if (A.moments) return set_error(PFB_E_ARG, "velocity observation is not supported");
     if (A.N < 0) return set_error(PFB_E_ARG, "negative cell count");
     if (A.L <= 286 || A.P < A.L || (A.P & 3))
         return set_error(PFB_E_ARG, "domain side must exceed 286, P >= L and P % 4 == 0");
     if (A.parity_out != 0 && A.parity_out != 1) return set_error(PFB_E_ARG, "parity_out must be 0 or 1");
+    return PFB_OK;
+}
+
+int step2d_launch_storage(const pfb_step_args2d* a, int cluster, int variant, int storage,
+                          cudaStream_t stream) {
+    int rc = check_step_args(a);
+    if (rc) return rc;
+    const pfb_step_args2d& A = *a;
+    if (A.moments) return set_error(PFB_E_ARG, "moments are read by the observed launch only");
     if (cluster == 0) cluster = kDefaultCluster;
     if (cluster != 2 && cluster != 4 && cluster != 8)
         return set_error(PFB_E_CONFIG, "cluster must be 2, 4 or 8");
     if (variant == 0) variant = 1;
     if (variant != 1) return set_error(PFB_E_CONFIG, "unknown kernel variant");
     if (A.N == 0) return PFB_OK;
-    int rc = step2d_configure_device();
+    rc = step2d_configure_device();
     if (rc) return rc;
     if (storage != kStoreF32 && storage != kStoreF16 && storage != kStoreBF16)
         return set_error(PFB_E_ARG, "unknown phi storage %d", storage);
@@ -853,6 +889,40 @@ int step2d_launch_storage(const pfb_step_args2d* a, int cluster, int variant, in
         e = cluster == 2   ? launch_k<2>(A, stream)
             : cluster == 4 ? launch_k<4>(A, stream)
                            : launch_k<8>(A, stream);
+    if (e != cudaSuccess) return set_error(PFB_E_CUDA, "step launch: %s", cudaGetErrorString(e));
+    return PFB_OK;
+}
+
+int step2d_launch_observed(const pfb_step_args2d* a, int cluster, int observation,
+                           cudaStream_t stream) {
+    if (observation == PFB_VELOCITY_DISABLED) {
+        if (!a) return set_error(PFB_E_ARG, "null step arguments");
+        pfb_step_args2d b = *a;
+        b.moments = nullptr;
+        return step2d_launch_storage(&b, cluster, 0, kStoreF32, stream);
+    }
+    int rc = check_step_args(a);
+    if (rc) return rc;
+    const pfb_step_args2d& A = *a;
+    if (observation != PFB_VELOCITY_ADVECTION && observation != PFB_VELOCITY_SPATIAL)
+        return set_error(PFB_E_ARG, "unknown velocity observation %d", observation);
+    if (observation == PFB_VELOCITY_SPATIAL && !A.moments)
+        return set_error(PFB_E_ARG, "the spatial observer needs moment accumulators");
+    if (!(A.physical_dt > 0.0)) return set_error(PFB_E_ARG, "physical_dt must be positive");
+    if (cluster == 0) cluster = kDefaultCluster;
+    if (cluster != 2 && cluster != 4 && cluster != 8)
+        return set_error(PFB_E_CONFIG, "cluster must be 2, 4 or 8");
+    if (A.N == 0) return PFB_OK;
+    if ((rc = step2d_configure_device())) return rc;
+    cudaError_t e;
+    if (observation == PFB_VELOCITY_ADVECTION)
+        e = cluster == 2   ? launch_k<2, float, PFB_VELOCITY_ADVECTION>(A, stream)
+            : cluster == 4 ? launch_k<4, float, PFB_VELOCITY_ADVECTION>(A, stream)
+                           : launch_k<8, float, PFB_VELOCITY_ADVECTION>(A, stream);
+    else
+        e = cluster == 2   ? launch_k<2, float, PFB_VELOCITY_SPATIAL>(A, stream)
+            : cluster == 4 ? launch_k<4, float, PFB_VELOCITY_SPATIAL>(A, stream)
+                           : launch_k<8, float, PFB_VELOCITY_SPATIAL>(A, stream);
     if (e != cudaSuccess) return set_error(PFB_E_CUDA, "step launch: %s", cudaGetErrorString(e));
     return PFB_OK;
 }

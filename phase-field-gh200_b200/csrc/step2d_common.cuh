@@ -26,6 +26,7 @@ struct CellPlan {
     int pctr, tumbled, no_margin;
     int dwx, dwy, dtx0, dty0;
     float gam, dwC, volC, vA, pcos, psin, theta, mrel;
+    double ginv, gcx, gcy;  // spatial observer geometry: 2/V, Cx/V, Cy/V
 };
 
 // S_other = (q_S - q(phi)) 2^-27; a negative difference is counted, not
@@ -51,7 +52,9 @@ __device__ __forceinline__ float s_other_counted(uint32_t qS, float phi, uint32_
 // Tumble, class choice and recentring shift of cell n whose field is in class
 // `cls` (reference src/kernels.cu:93-191 and :624-711). Deterministic in its
 // inputs, so every CTA that runs it for the same cell decides the same thing;
-// only `leader` raises flags.
+// only `leader` raises flags. GEO also records the spatial observer's
+// geometry of the field about to be read.
+template <bool GEO = false>
 __device__ __forceinline__ void plan_cell(const pfb_step_args2d& A, int n, int cls,
                                           unsigned long long step, CellPlan& out, bool leader) {
     const Window W = window_of(cls);
@@ -153,6 +156,11 @@ __device__ __forceinline__ void plan_cell(const pfb_step_args2d& A, int n, int c
     out.psin = ps;
     out.theta = theta;
     out.mrel = mrel;
+    if constexpr (GEO) {
+        out.ginv = 2.0 / cs.V;
+        out.gcx = cs.Cx / cs.V;
+        out.gcy = cs.Cy / cs.V;
+    }
 }
 
 __device__ __forceinline__ bool full_moment_step(const pfb_step_args2d& A,
@@ -228,9 +236,20 @@ __device__ __forceinline__ void commit_cell(const pfb_step_args2d& A, const Cell
 // peer's mbarrier: no cluster barrier (and no release fence over the CTA's
 // outstanding global stores) sits on the path. Receive slots are indexed by
 // the sender's rank and summed in ascending rank order.
+// The spatial velocity observer's six sums (Bx, By, Gx, Gy, Kx, Ky) travel
+// with the force in their own arrays at the end of the scratch (NO = 6), so
+// the layout of every other kernel is unchanged.
+template <int NW, int K, int NO>
+struct ObsRed {
+    double d[NW][NO];
+    alignas(16) double recv[K][NO];
+};
 template <int NW, int K>
+struct ObsRed<NW, K, 0> {};
+
+template <int NW, int K, int NO = 0>
 struct RedScratch {
-    uint64_t barI;  // K force partials (16 B each) received, every CTA
+    uint64_t barI;  // K force partials (16 B, + 8 NO B) received, every CTA
     uint64_t barM;  // K moment partials (64 B each) received, rank 0
     double red_d[NW][4];
     int red_i[NW][5];
@@ -239,71 +258,232 @@ struct RedScratch {
     alignas(16) int recvB[K][4];
     alignas(16) int recvP[K][4];
     float vx, vy;
+    ObsRed<NW, K, NO> o;
 };
+
+// ---- velocity observers (reference include/fused_moments.cuh) -------------
+// OBS 0: none; 1: advection accumulators; 2: advection plus the spatial
+// rates. The spatial observer adds six sums to the force reduction: the
+// same-cell neighbour overlaps Bx, By, the interfacial moments Gx, Gy and the
+// overlap moments Kx, Ky.
+template <int OBS> constexpr int kObsVals = OBS == PFB_VELOCITY_SPATIAL ? 6 : 0;
+
+template <int OBS> struct ObsAcc {
+    __device__ __forceinline__ void pixel(const CellPlan&, float, int, int, float, float, float,
+                                          float, float, float, float, float, float, float) {}
+    __device__ __forceinline__ double val(int) const { return 0.0; }
+};
+
+template <> struct ObsAcc<PFB_VELOCITY_SPATIAL> {
+    double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // Bx, By, Gx, Gy, Kx, Ky
+    // One pixel of phi^n at window (x, y) with its eight neighbours and
+    // S_other, in FP64 from the binary32 inputs.
+    __device__ __forceinline__ void pixel(const CellPlan& P, float repC, int x, int y, float p,
+                                          float e, float w, float nn, float ss, float ne,
+                                          float nw, float se, float sw, float other) {
+        const double d = p;
+        v[0] += d * (double)e;
+        v[1] += d * (double)nn;
+        const double lap =
+            (4.0 * ((double)nn + ss + e + w) + (double)ne + nw + se + sw - 20.0 * d) / 6.0;
+        const double weight = P.ginv * d;
+        const double inter =
+            weight * ((double)P.gam * lap - (double)P.dwC * d * (1.0 - d) * (1.0 - 2.0 * d));
+        const double ox = (double)x - P.gcx, oy = (double)y - P.gcy;
+        v[2] += ox * inter;
+        v[3] += oy * inter;
+        const double over = -weight * (double)repC * d * (double)other;
+        v[4] += ox * over;
+        v[5] += oy * over;
+    }
+    __device__ __forceinline__ double val(int j) const { return v[j]; }
+};
+
+__device__ __forceinline__ double linear_corr(double dt, unsigned long long steps, double first,
+                                              double last) {
+    return steps ? dt * 0.5 * (double)(steps - 1) * (last - first) : 0.0;
+}
+
+// Observer commit of one cell by one thread once the cluster totals
+// t = {Ix, Iy, Bx, By, Gx, Gy, Kx, Ky} are known (reference
+// record_advection and RelaxMoments::finish): the spatial observer first
+// closes the interval held since its previous sample, then the advection
+// integrals advance, then the new rates replace the held ones.
+template <int OBS>
+__device__ __forceinline__ void observe_commit(const pfb_step_args2d& A, const CellPlan& P,
+                                               const double* t, float vxf, float vyf) {
+    if constexpr (OBS != PFB_VELOCITY_DISABLED) {
+        pfb_cell2d& c = A.cell[P.n];
+        pfb_advection_accum& a = c.advection;
+        const double dt = A.physical_dt;
+        const double ax = (double)P.vA * (double)P.pcos, ay = (double)P.vA * (double)P.psin;
+        const double ix = (double)A.mot_coeff * t[0], iy = (double)A.mot_coeff * t[1];
+        if constexpr (OBS == PFB_VELOCITY_SPATIAL) {
+            pfb_moment_accum2d& m = static_cast<pfb_moment_accum2d*>(A.moments)[P.n];
+            const double tot[4] = {a.q[0] + a.q[2], a.q[1] + a.q[3], a.q[4], a.q[5]};
+            const unsigned long long interval = a.count - m.last_sample;
+            if (m.spatial_count) {
+                for (int j = 0; j < 4; ++j) m.q[4 + j] += dt * (double)interval * m.held[j];
+                for (int xy = 0; xy < 2; ++xy) {
+                    const double beta = m.held[4 + xy];
+                    m.q[10 + xy] += (beta - 1.0) * (tot[xy] - m.last_totals[xy]) +
+                                    beta * (tot[2 + xy] - m.last_totals[2 + xy]);
+                }
+            }
+            for (int j = 0; j < 4; ++j) m.last_totals[j] = tot[j];
+            m.last_interval = interval;
+            m.last_sample = a.count;
+            ++m.spatial_count;
+            m.held[4] = t[2] / c.V;
+            m.held[5] = t[3] / c.V;
+        }
+        a.q[0] += dt * ax;
+        a.q[1] += dt * ay;
+        a.q[2] += dt * ix;
+        a.q[3] += dt * iy;
+        a.q[4] += dt * ((double)vxf - ax - ix);
+        a.q[5] += dt * ((double)vyf - ay - iy);
+        ++a.count;
+        if constexpr (OBS == PFB_VELOCITY_SPATIAL) {
+            pfb_moment_accum2d& m = static_cast<pfb_moment_accum2d*>(A.moments)[P.n];
+            const double mrel = (double)c.M_pf / kMobilityM0;
+            for (int j = 0; j < 4; ++j) {
+                double rate = t[4 + j];
+                if (mrel != 1.0) rate *= mrel;
+                if (m.spatial_count > 1)
+                    m.correction[j] += linear_corr(dt, m.last_interval, m.held[j], rate);
+                m.held[j] = rate;
+            }
+        }
+    }
+}
 
 // Receive barriers of one cluster reduction round; thread 0 of every CTA
 // calls it before the kernel's first (relaxed) cluster arrive.
-template <int NW, int K>
-__device__ __forceinline__ void red_init(RedScratch<NW, K>& R, int rank) {
+template <int NW, int K, int NO>
+__device__ __forceinline__ void red_init(RedScratch<NW, K, NO>& R, int rank) {
     dev::mbar_init(&R.barI, 1);
     dev::mbar_init(&R.barM, 1);
-    dev::mbar_arrive_expect_tx(&R.barI, (uint32_t)(K * 16));
+    dev::mbar_arrive_expect_tx(&R.barI, (uint32_t)(K * (16 + 8 * NO)));
     if (rank == 0) dev::mbar_arrive_expect_tx(&R.barM, (uint32_t)(K * 64));
 }
 
 // Interaction integral of this CTA -> cluster total -> velocity, identical
 // in every CTA. Sums run in ascending warp, then ascending rank order. Rank 0
-// stores v and I in the cell record. All threads call it; the caller has
-// issued the cluster arrive that follows red_init.
-template <int K, int NW>
+// stores v and I in the cell record and commits the velocity observer. All
+// threads call it; the caller has issued the cluster arrive that follows
+// red_init.
+template <int K, int NW, int OBS, int NO>
 __device__ __forceinline__ void reduce_force(const pfb_step_args2d& A, const CellPlan& P,
-                                             int rank, RedScratch<NW, K>& R, double aIx,
-                                             double aIy, unsigned int* status) {
+                                             int rank, RedScratch<NW, K, NO>& R, double aIx,
+                                             double aIy, const ObsAcc<OBS>& ob,
+                                             unsigned int* status) {
     static_assert(NW <= 32 && K <= 32, "one lane per warp and per rank");
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    aIx = dev::warp_sum_down(aIx);
-    aIy = dev::warp_sum_down(aIy);
-    if (lane == 0) {
-        R.red_d[warp][0] = aIx;
-        R.red_d[warp][1] = aIy;
-    }
-    __syncthreads();
-    dev::cluster_wait();  // every peer's receive barrier is initialised
-    if (warp == 0) {
-        const double px = lane < NW ? R.red_d[lane][0] : 0.0;
-        const double py = lane < NW ? R.red_d[lane][1] : 0.0;
-        const double s0 = dev::ordered_lane_sum(px, NW);
-        const double s1 = dev::ordered_lane_sum(py, NW);
-        if (lane < K)
-            dev::st_async_v2f64(dev::map_to_rank(dev::smem_addr(&R.recvI[rank][0]), lane), s0, s1,
-                                dev::map_to_rank(dev::smem_addr(&R.barI), lane));
-        if (!dev::mbar_wait_bounded(&R.barI, 0, kWaitPolls)) atomicOr(status, 2u);
-        const double2 v = lane < K ? make_double2(R.recvI[lane][0], R.recvI[lane][1])
-                                   : make_double2(0.0, 0.0);
-        const double sIx = dev::ordered_lane_sum(v.x, K);
-        const double sIy = dev::ordered_lane_sum(v.y, K);
+    if constexpr (OBS != PFB_VELOCITY_SPATIAL) {
+        aIx = dev::warp_sum_down(aIx);
+        aIy = dev::warp_sum_down(aIy);
         if (lane == 0) {
-            const double vxd = (double)P.vA * (double)P.pcos + (double)A.mot_coeff * sIx;
-            const double vyd = (double)P.vA * (double)P.psin + (double)A.mot_coeff * sIy;
-            R.vx = (float)vxd;
-            R.vy = (float)vyd;
-            if (rank == 0) {
-                pfb_cell2d& cs = A.cell[P.n];
-                cs.vx = (float)vxd;
-                cs.vy = (float)vyd;
-                cs.Ix = sIx;
-                cs.Iy = sIy;
+            R.red_d[warp][0] = aIx;
+            R.red_d[warp][1] = aIy;
+        }
+        __syncthreads();
+        dev::cluster_wait();  // every peer's receive barrier is initialised
+        if (warp == 0) {
+            const double px = lane < NW ? R.red_d[lane][0] : 0.0;
+            const double py = lane < NW ? R.red_d[lane][1] : 0.0;
+            const double s0 = dev::ordered_lane_sum(px, NW);
+            const double s1 = dev::ordered_lane_sum(py, NW);
+            if (lane < K)
+                dev::st_async_v2f64(dev::map_to_rank(dev::smem_addr(&R.recvI[rank][0]), lane), s0,
+                                    s1, dev::map_to_rank(dev::smem_addr(&R.barI), lane));
+            if (!dev::mbar_wait_bounded(&R.barI, 0, kWaitPolls)) atomicOr(status, 2u);
+            const double2 v = lane < K ? make_double2(R.recvI[lane][0], R.recvI[lane][1])
+                                       : make_double2(0.0, 0.0);
+            const double sIx = dev::ordered_lane_sum(v.x, K);
+            const double sIy = dev::ordered_lane_sum(v.y, K);
+            if (lane == 0) {
+                const double vxd = (double)P.vA * (double)P.pcos + (double)A.mot_coeff * sIx;
+                const double vyd = (double)P.vA * (double)P.psin + (double)A.mot_coeff * sIy;
+                R.vx = (float)vxd;
+                R.vy = (float)vyd;
+                if (rank == 0) {
+                    pfb_cell2d& cs = A.cell[P.n];
+                    cs.vx = (float)vxd;
+                    cs.vy = (float)vyd;
+                    cs.Ix = sIx;
+                    cs.Iy = sIy;
+                    if constexpr (OBS == PFB_VELOCITY_ADVECTION) {
+                        const double t[2] = {sIx, sIy};
+                        observe_commit<OBS>(A, P, t, (float)vxd, (float)vyd);
+                    }
+                }
             }
         }
+        __syncthreads();
+    } else {
+        // the spatial observer's six sums travel with the force
+        static_assert(NO == 6, "observer scratch");
+        const double fx = dev::warp_sum_down(aIx);
+        const double fy = dev::warp_sum_down(aIy);
+        double part[NO];
+#pragma unroll
+        for (int j = 0; j < NO; ++j) part[j] = dev::warp_sum_down(ob.val(j));
+        if (lane == 0) {
+            R.red_d[warp][0] = fx;
+            R.red_d[warp][1] = fy;
+#pragma unroll
+            for (int j = 0; j < NO; ++j) R.o.d[warp][j] = part[j];
+        }
+        __syncthreads();
+        dev::cluster_wait();
+        if (warp == 0) {
+            double s[2 + NO];
+            s[0] = dev::ordered_lane_sum(lane < NW ? R.red_d[lane][0] : 0.0, NW);
+            s[1] = dev::ordered_lane_sum(lane < NW ? R.red_d[lane][1] : 0.0, NW);
+#pragma unroll
+            for (int j = 0; j < NO; ++j)
+                s[2 + j] = dev::ordered_lane_sum(lane < NW ? R.o.d[lane][j] : 0.0, NW);
+            if (lane < K) {
+                const uint32_t bar = dev::map_to_rank(dev::smem_addr(&R.barI), lane);
+                dev::st_async_v2f64(dev::map_to_rank(dev::smem_addr(&R.recvI[rank][0]), lane), s[0],
+                                    s[1], bar);
+#pragma unroll
+                for (int j = 0; j < NO; j += 2)
+                    dev::st_async_v2f64(dev::map_to_rank(dev::smem_addr(&R.o.recv[rank][j]), lane),
+                                        s[2 + j], s[3 + j], bar);
+            }
+            if (!dev::mbar_wait_bounded(&R.barI, 0, kWaitPolls)) atomicOr(status, 2u);
+            double t[2 + NO];
+            t[0] = dev::ordered_lane_sum(lane < K ? R.recvI[lane][0] : 0.0, K);
+            t[1] = dev::ordered_lane_sum(lane < K ? R.recvI[lane][1] : 0.0, K);
+#pragma unroll
+            for (int j = 0; j < NO; ++j)
+                t[2 + j] = dev::ordered_lane_sum(lane < K ? R.o.recv[lane][j] : 0.0, K);
+            if (lane == 0) {
+                const double vxd = (double)P.vA * (double)P.pcos + (double)A.mot_coeff * t[0];
+                const double vyd = (double)P.vA * (double)P.psin + (double)A.mot_coeff * t[1];
+                R.vx = (float)vxd;
+                R.vy = (float)vyd;
+                if (rank == 0) {
+                    pfb_cell2d& cs = A.cell[P.n];
+                    cs.vx = (float)vxd;
+                    cs.vy = (float)vyd;
+                    cs.Ix = t[0];
+                    cs.Iy = t[1];
+                    observe_commit<OBS>(A, P, t, (float)vxd, (float)vyd);
+                }
+            }
+        }
+        __syncthreads();
     }
-    __syncthreads();
 }
 
 // Moments of this CTA -> pushed to rank 0 -> summed in rank order and
 // committed by rank 0 (reference src/kernels.cu:542-590).
-template <int K, int NW>
+template <int K, int NW, int NO>
 __device__ __forceinline__ void reduce_moments(const pfb_step_args2d& A, const CellPlan& P,
-                                               int rank, RedScratch<NW, K>& R, bool fm,
+                                               int rank, RedScratch<NW, K, NO>& R, bool fm,
                                                PixelAcc acc, unsigned int* status) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     acc.V = dev::warp_sum_down(acc.V);
@@ -363,9 +543,10 @@ __device__ __forceinline__ void reduce_moments(const pfb_step_args2d& A, const C
 // barrier each CTA re-reads its destination rows for scatter and moments
 // (reference src/kernels.cu:344-443 and :604-937). All NT threads of every CTA
 // of the cluster call it together.
-template <int CLS, int K, int NW>
+template <int CLS, int K, int NW, int OBS = PFB_VELOCITY_DISABLED>
 __device__ __noinline__ void global_cell(const pfb_step_args2d& A, const CellPlan& P, int rank,
-                                         RedScratch<NW, K>& R, bool fm, unsigned int* status) {
+                                         RedScratch<NW, K, kObsVals<OBS>>& R, bool fm,
+                                         unsigned int* status) {
     constexpr int NT = NW * 32;
     constexpr Window W = window_of(CLS);
     constexpr int WX = W.wx, WY = W.wy, TX0 = W.tx0, TY0 = W.ty0;
@@ -380,6 +561,7 @@ __device__ __noinline__ void global_cell(const pfb_step_args2d& A, const CellPla
     const int split = min(WX, L - gx0);
 
     double aIx = 0.0, aIy = 0.0;
+    ObsAcc<OBS> ob;
     const int cnt = (y1 - y0) * WX;
     for (int idx = tid; idx < cnt; idx += NT) {
         const int yy = idx / WX;
@@ -395,8 +577,12 @@ __device__ __noinline__ void global_cell(const pfb_step_args2d& A, const CellPla
         const float So = s_other_n(__ldg(A.S_rd + (size_t)gy * Pp + gxg), c, A.flags, 1u);
         aIx += (double)(c * gx * So);
         aIy += (double)(c * gyv * So);
+        if constexpr (OBS == PFB_VELOCITY_SPATIAL)
+            ob.pixel(P, A.rep_coeff, x, y, c, __ldg(p + 1), __ldg(p - 1), __ldg(p + kTilePitch),
+                     __ldg(p - kTilePitch), __ldg(p + kTilePitch + 1), __ldg(p + kTilePitch - 1),
+                     __ldg(p - kTilePitch + 1), __ldg(p - kTilePitch - 1), So);
     }
-    reduce_force<K, NW>(A, P, rank, R, aIx, aIy, status);
+    reduce_force<K, NW, OBS>(A, P, rank, R, aIx, aIy, ob, status);
 
     const int sx = P.sx, sy = P.sy;
     const int dwx = P.dwx, dwy = P.dwy, dtx0 = P.dtx0, dty0 = P.dty0;

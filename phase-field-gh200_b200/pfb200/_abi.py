@@ -172,6 +172,12 @@ _SIGS = {
     "pfb_sim2d_pack_traj": (I, [P, P]),
     "pfb_sim2d_save": (I, [P]),
     "pfb_sim2d_restore": (I, [P]),
+    "pfb_sim2d_velocity_open": (I, [P, C.c_char_p, I, C.c_longlong, I]),
+    "pfb_sim2d_velocity_capture": (I, [P]),
+    "pfb_sim2d_velocity_last_frame": (C.c_longlong, [P]),
+    "pfb_sim2d_velocity_close": (I, [P]),
+    "pfb_step2d_launch_observed": (I, [C.POINTER(StepArgs2D), I, I, P]),
+    "pfb_velocity_moments2d": (I, [C.POINTER(StepArgs2D), P, C.c_double, P]),
     "pfb_sim2d_bench": (I, [P, I, I, C.POINTER(C.c_double)]),
     "pfb_sim2d_step_args": (I, [P, C.POINTER(StepArgs2D)]),
     "pfb_sim2d_stream": (P, [P]),

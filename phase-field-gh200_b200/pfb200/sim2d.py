@@ -231,6 +231,19 @@ class Sim2D:
     def restore(self) -> None:
         check(lib().pfb_sim2d_restore(self._h), "restore")
 
+    def velocity_open(self, path, spatial_stride: int = 100, dense_start: int = 10000,
+                      reference: bool = False) -> None:
+        """Start a PFVMOM4 velocity-component recording in a new file
+        (writes the header and the frame of the current step)."""
+        check(lib().pfb_sim2d_velocity_open(self._h, str(path).encode(), spatial_stride,
+                                            dense_start, 1 if reference else 0), "velocity_open")
+
+    def velocity_capture(self) -> None:
+        check(lib().pfb_sim2d_velocity_capture(self._h), "velocity_capture")
+
+    def velocity_close(self) -> None:
+        check(lib().pfb_sim2d_velocity_close(self._h), "velocity_close")
+
     def residual_step(self) -> tuple[float, float]:
         """Advance one step; (max, rms) of |dphi / dt| over that step."""
         linf, rms = C.c_double(), C.c_double()

@@ -18,7 +18,9 @@ def test_help_lists_the_reference_options():
     r = run("--help")
     assert r.returncode == 0
     for opt in ("--N", "--radius", "--rho", "--v-A", "--t-end", "--checkpoint-dir",
-                "--trajectory-interval", "--out", "--bench"):
+                "--trajectory-interval", "--out", "--bench", "--velocity-moments",
+                "--velocity-spatial-stride", "--velocity-dense-start",
+                "--velocity-moments-reference"):
         assert opt in r.stdout
 
 
@@ -27,7 +29,13 @@ def test_help_lists_the_reference_options():
     (("--N",), 2),
     (("--N", "x"), 2),
     (("--dt", "nan"), 2),
-    (("--velocity-moments", "v.bin"), 2),
+    (("--velocity-moments", "v.bin"), 2),  # needs --out
+    (("--velocity-moments", "v.bin", "--out", "v.bin"), 2),  # distinct paths
+    (("--velocity-moments", "v.bin", "--out", "t.txt", "--velocity-spatial-stride", 0), 2),
+    (("--velocity-moments", "v.bin", "--out", "t.txt", "--velocity-spatial-stride", 1001), 2),
+    (("--velocity-moments", "v.bin", "--out", "t.txt", "--velocity-dense-start", -1), 2),
+    (("--velocity-moments-reference",), 2),
+    (("--velocity-moments", "v.bin", "--bench", 10), 2),
     (("--boundary-out", "b.bin"), 2),
     (("--initial-centres", "c.csv"), 2),
 ])
