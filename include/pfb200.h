@@ -394,6 +394,19 @@ int pfb_sim2d_velocity_capture(pfb_sim2d* s);
 /* Step of the last frame written, -1 when none is open. */
 long long pfb_sim2d_velocity_last_frame(const pfb_sim2d* s);
 int pfb_sim2d_velocity_close(pfb_sim2d* s);
+
+/* PFB boundary recorder (reference src/boundary.cu, common/boundary_format.h):
+ * creates a NEW file at `path` and writes its 72-byte header (level 1/2,
+ * the frame `interval` stored for readers). Each capture appends a frame of
+ * the current step: per cell a 40-byte record (id, tile origin, periodic
+ * centroid, gamma, mobility, active speed, target radius, square count) and
+ * the 2x2 squares of its tile that phi = 1/2 crosses, binary32 corners, in
+ * ascending tile order. Frames are written by a background thread; close
+ * writes the end record. `compress` (zstd) is refused: this build has no
+ * zstd. binary32 pools only. */
+int pfb_sim2d_boundary_open(pfb_sim2d* s, const char* path, long long interval, int compress);
+int pfb_sim2d_boundary_capture(pfb_sim2d* s);
+int pfb_sim2d_boundary_close(pfb_sim2d* s);
 void* pfb_sim2d_stream(pfb_sim2d* s);
 
 /* ---- batched ensemble (no reference counterpart) --------------------------

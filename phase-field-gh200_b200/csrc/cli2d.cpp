@@ -6,11 +6,12 @@
 // Supported: the model and run options, resume from a CELL checkpoint (-c),
 // rolling / tagged / final checkpoints, the plain-text trajectory (--out),
 // the PFVMOM4 velocity-moment recorder (--velocity-moments; reference
-// src/velocity_output.cu), --bench. Not part of this build (they exit with
-// status 2 and a message): the boundary recorder, --initial-centres, the
-// mobility map, --morton, --no-l2, --strict and --self-test, velocity
-// observation under --bench, and, on resume, overrides of model parameters
-// other than the output cadences and t_end.
+// src/velocity_output.cu), the PFB boundary recorder (--boundary-out;
+// src/boundary.cu), --bench. Not part of this build (they exit with status 2
+// and a message): --initial-centres, the mobility map, --morton, --no-l2,
+// --strict and --self-test, velocity observation under --bench, and, on
+// resume, overrides of model parameters other than the output cadences and
+// t_end. zstd boundary compression is refused at open (no zstd here).
 #include <algorithm>
 #include <cerrno>
 #include <cmath>
@@ -51,6 +52,9 @@ struct Options {
     int vel_stride = 100;
     long long vel_dense = 10000;
     bool vel_reference = false, vel_given = false;
+    std::string bnd_path;
+    long long bnd_interval = 0;
+    bool bnd_compress = false;
 };
 
 constexpr double kPi = 3.14159265358979323846;
@@ -67,7 +71,8 @@ void usage() {
         "  --trajectory-samples <n>  --trajectory-interval <n>  --out <path>\n"
         "  --device <int>  --bench <steps>  --no-graph\n"
         "  --velocity-moments <path>  --velocity-spatial-stride <1..1000>\n"
-        "  --velocity-dense-start <int>  --velocity-moments-reference\n");
+        "  --velocity-dense-start <int>  --velocity-moments-reference\n"
+        "  --boundary-out <path>  --boundary-interval <int>  --boundary-compression <none|zstd>\n");
 }
 
 bool num(const char* s, double* v) {
@@ -390,8 +395,21 @@ int parse(int argc, char** argv, Options* o) {
         } else if (a == "--velocity-moments-reference") {
             o->vel_reference = true;
             o->vel_given = true;
-        } else if (a == "--boundary-out" || a == "--boundary-interval" || a == "--boundary-compression" ||
-                   a == "--initial-centres" || a == "--phase-field-mobility-map" || a == "--morton" ||
+        } else if (a == "--boundary-out") {
+            if (!(v = val()) || !v[0]) return 2;
+            o->bnd_path = v;
+        } else if (a == "--boundary-interval") {
+            if (!(v = val()) || !num(v, &n) || n < 1 || n > 1000000000000LL) return 2;
+            o->bnd_interval = n;
+        } else if (a == "--boundary-compression") {
+            if (!(v = val())) return 2;
+            if (!std::strcmp(v, "none"))
+                o->bnd_compress = false;
+            else if (!std::strcmp(v, "zstd"))
+                o->bnd_compress = true;
+            else
+                return 2;
+        } else if (a == "--initial-centres" || a == "--phase-field-mobility-map" || a == "--morton" ||
                    a == "--no-l2" || a == "--strict" || a == "--self-test") {
             std::fprintf(stderr, "[fatal] option '%s' is not part of this build\n", a.c_str());
             return 2;
@@ -424,7 +442,14 @@ int main(int argc, char** argv) {
         std::fprintf(stderr, "[fatal] velocity observation under --bench is not part of this build\n");
         return 2;
     }
-    if (!o.vel_path.empty() && o.vel_path == o.out_path) {
+    if (o.bnd_path.empty() != (o.bnd_interval == 0) || (o.bnd_compress && o.bnd_path.empty()) ||
+        (!o.bnd_path.empty() && o.bench > 0)) {
+        std::fprintf(stderr, "[fatal] boundary output requires a path and interval, and cannot be used "
+                             "with --bench\n");
+        return 2;
+    }
+    if ((!o.bnd_path.empty() && (o.bnd_path == o.out_path || o.bnd_path == o.vel_path)) ||
+        (!o.vel_path.empty() && o.vel_path == o.out_path)) {
         std::fprintf(stderr, "[fatal] output files must use distinct paths\n");
         return 2;
     }
@@ -538,6 +563,17 @@ int main(int argc, char** argv) {
         pfb_sim2d_destroy(s);
         return 9;
     }
+    long long last_boundary = -1;
+    if (!o.bnd_path.empty()) {
+        if (pfb_sim2d_boundary_open(s, o.bnd_path.c_str(), o.bnd_interval, o.bnd_compress ? 1 : 0) != PFB_OK ||
+            pfb_sim2d_boundary_capture(s) != PFB_OK) {
+            std::fprintf(stderr, "[boundary] %s\n", pfb_last_error());
+            if (traj) std::fclose(traj);
+            pfb_sim2d_destroy(s);
+            return 9;
+        }
+        last_boundary = pfb_sim2d_step(s);
+    }
     std::signal(SIGINT, on_signal);
     std::signal(SIGTERM, on_signal);
 
@@ -556,10 +592,12 @@ int main(int argc, char** argv) {
     long long next_save = ckpt_on && o.save_interval > 0 ? step + o.save_interval : total + 1;
     constexpr long long kFatalPoll = 1000;
     long long next_poll = step + kFatalPoll;
+    long long next_bnd = o.bnd_path.empty() ? total + 1 : step + o.bnd_interval;
     bool failed = false;
     uint32_t flags[PFB_FLAG_COUNT];
     while (step < total && !failed) {
-        const long long stop = std::min({total, (step / pi + 1) * pi, next_traj, next_ckpt, next_save, next_poll});
+        const long long stop =
+            std::min({total, (step / pi + 1) * pi, next_traj, next_ckpt, next_save, next_poll, next_bnd});
         if (pfb_sim2d_advance(s, stop - step) != PFB_OK) {
             std::fprintf(stderr, "[fatal] %s\n", pfb_last_error());
             failed = true;
@@ -588,6 +626,15 @@ int main(int argc, char** argv) {
                 break;
             }
         }
+        if (step >= next_bnd) {
+            if (pfb_sim2d_boundary_capture(s) != PFB_OK) {
+                std::fprintf(stderr, "[boundary] %s\n", pfb_last_error());
+                failed = true;
+                break;
+            }
+            last_boundary = step;
+            next_bnd = step + o.bnd_interval;
+        }
         if (step >= next_ckpt) {
             if (!save(dir + "/checkpoint.bin")) failed = true;
             next_ckpt = step + o.ckpt_interval;
@@ -611,6 +658,16 @@ int main(int argc, char** argv) {
             failed = true;
         }
         if (pfb_sim2d_velocity_close(s) != PFB_OK) failed = true;
+    }
+    if (!o.bnd_path.empty()) {
+        if (!failed && last_boundary != step && pfb_sim2d_boundary_capture(s) != PFB_OK) {
+            std::fprintf(stderr, "[boundary] %s\n", pfb_last_error());
+            failed = true;
+        }
+        if (pfb_sim2d_boundary_close(s) != PFB_OK) {
+            std::fprintf(stderr, "[boundary] %s\n", pfb_last_error());
+            failed = true;
+        }
     }
     if (ckpt_on && (o.final_ckpt || failed)) {
         if (!save(dir + (failed ? "/checkpoint_failed.bin" : "/checkpoint.bin"))) failed = true;

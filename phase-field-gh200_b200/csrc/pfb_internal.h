@@ -54,6 +54,15 @@ int velocity2d_capture(Velocity2D* v, const pfb_step_args2d& A, long long step, 
 long long velocity2d_last_frame(const Velocity2D* v);
 int velocity2d_close(Velocity2D* v);
 
+// PFB boundary recorder (boundary2d.cu).
+struct Boundary2D;
+Boundary2D* boundary2d_open(const char* path, int N, int side, double dt, double tau,
+                            long long interval, int compress);
+int boundary2d_capture(Boundary2D* b, const float* phi, const pfb_cell2d* cells,
+                       cudaStream_t stream, long long step, double time);
+// Finish the file (end record) and free the recorder.
+int boundary2d_close(Boundary2D* b);
+
 // init2d.cu
 int init_tiles2d(float* phi_a, float* phi_b, pfb_cell2d* cell, const uint8_t* cls, int N, int L,
                  const float* cx, const float* cy, float radius_eff, float kappa_iface,

@@ -56,9 +56,11 @@ struct pfb_sim2d {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     Velocity2D* vel = nullptr;  // open PFVMOM4 recorder
+    Boundary2D* bnd = nullptr;  // open PFB recorder
 
     ~pfb_sim2d() {
         if (vel) velocity2d_destroy(vel);
+        if (bnd) (void)boundary2d_close(bnd);
         if (graph_exec) cudaGraphExecDestroy(graph_exec);
         if (graph) cudaGraphDestroy(graph);
         if (stream) cudaStreamDestroy(stream);
@@ -442,6 +444,30 @@ int pfb_sim2d_velocity_capture(pfb_sim2d* s) {
 
 long long pfb_sim2d_velocity_last_frame(const pfb_sim2d* s) {
     return s && s->vel ? velocity2d_last_frame(s->vel) : -1;
+}
+
+int pfb_sim2d_boundary_open(pfb_sim2d* s, const char* path, long long interval, int compress) {
+    if (!s) return set_error(PFB_E_ARG, "null system");
+    if (s->bnd) return set_error(PFB_E_STATE, "a boundary recorder is already open");
+    if (s->p.phi_storage != 0)
+        return set_error(PFB_E_CONFIG, "the boundary recorder needs binary32 phi pools");
+    PFB_CU(cudaSetDevice(s->device), "cudaSetDevice");
+    s->bnd = boundary2d_open(path, s->N, s->L, s->p.dt, s->p.tau, interval, compress);
+    return s->bnd ? PFB_OK : PFB_E_ARG;
+}
+
+int pfb_sim2d_boundary_capture(pfb_sim2d* s) {
+    if (!s || !s->bnd) return set_error(PFB_E_STATE, "no boundary recorder is open");
+    PFB_CU(cudaSetDevice(s->device), "cudaSetDevice");
+    return boundary2d_capture(s->bnd, s->d_phi[s->steps_done % 2], s->d_cell, s->stream,
+                              s->steps_done, (double)s->steps_done * s->p.dt);
+}
+
+int pfb_sim2d_boundary_close(pfb_sim2d* s) {
+    if (!s || !s->bnd) return set_error(PFB_E_STATE, "no boundary recorder is open");
+    const int rc = boundary2d_close(s->bnd);
+    s->bnd = nullptr;
+    return rc;
 }
 
 int pfb_sim2d_velocity_close(pfb_sim2d* s) {

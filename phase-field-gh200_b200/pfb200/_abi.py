@@ -176,6 +176,9 @@ _SIGS = {
     "pfb_sim2d_velocity_capture": (I, [P]),
     "pfb_sim2d_velocity_last_frame": (C.c_longlong, [P]),
     "pfb_sim2d_velocity_close": (I, [P]),
+    "pfb_sim2d_boundary_open": (I, [P, C.c_char_p, C.c_longlong, I]),
+    "pfb_sim2d_boundary_capture": (I, [P]),
+    "pfb_sim2d_boundary_close": (I, [P]),
     "pfb_step2d_launch_observed": (I, [C.POINTER(StepArgs2D), I, I, P]),
     "pfb_velocity_moments2d": (I, [C.POINTER(StepArgs2D), P, C.c_double, P]),
     "pfb_sim2d_bench": (I, [P, I, I, C.POINTER(C.c_double)]),

@@ -244,6 +244,17 @@ class Sim2D:
     def velocity_close(self) -> None:
         check(lib().pfb_sim2d_velocity_close(self._h), "velocity_close")
 
+    def boundary_open(self, path, interval: int, compress: bool = False) -> None:
+        """Start a PFB boundary recording in a new file (header only)."""
+        check(lib().pfb_sim2d_boundary_open(self._h, str(path).encode(), interval,
+                                            1 if compress else 0), "boundary_open")
+
+    def boundary_capture(self) -> None:
+        check(lib().pfb_sim2d_boundary_capture(self._h), "boundary_capture")
+
+    def boundary_close(self) -> None:
+        check(lib().pfb_sim2d_boundary_close(self._h), "boundary_close")
+
     def residual_step(self) -> tuple[float, float]:
         """Advance one step; (max, rms) of |dphi / dt| over that step."""
         linf, rms = C.c_double(), C.c_double()

@@ -20,7 +20,8 @@ def test_help_lists_the_reference_options():
     for opt in ("--N", "--radius", "--rho", "--v-A", "--t-end", "--checkpoint-dir",
                 "--trajectory-interval", "--out", "--bench", "--velocity-moments",
                 "--velocity-spatial-stride", "--velocity-dense-start",
-                "--velocity-moments-reference"):
+                "--velocity-moments-reference", "--boundary-out", "--boundary-interval",
+                "--boundary-compression"):
         assert opt in r.stdout
 
 
@@ -36,7 +37,13 @@ def test_help_lists_the_reference_options():
     (("--velocity-moments", "v.bin", "--out", "t.txt", "--velocity-dense-start", -1), 2),
     (("--velocity-moments-reference",), 2),
     (("--velocity-moments", "v.bin", "--bench", 10), 2),
-    (("--boundary-out", "b.bin"), 2),
+    (("--boundary-out", "b.bin"), 2),  # needs an interval
+    (("--boundary-interval", 5), 2),  # needs a path
+    (("--boundary-out", "b.bin", "--boundary-interval", 0), 2),
+    (("--boundary-out", "b.bin", "--boundary-interval", 5, "--boundary-compression", "gz"), 2),
+    (("--boundary-compression", "zstd"), 2),
+    (("--boundary-out", "b.bin", "--boundary-interval", 5, "--bench", 10), 2),
+    (("--boundary-out", "b.bin", "--boundary-interval", 5, "--out", "b.bin"), 2),
     (("--initial-centres", "c.csv"), 2),
 ])
 def test_bad_options_exit_2(args, code):
