@@ -342,6 +342,24 @@ void* pfb_sim3d_stream(const pfb_sim3d* s);
 /* Device time of `steps` steps after `warmup`, in ms (CUDA events). */
 int pfb_sim3d_bench(pfb_sim3d* s, int warmup, int steps, double* ms);
 
+/* PFB3D boundary recorder (reference src/pf3d/boundary_output.cu, file
+ * layout common/boundary_format_3d.h): creates a NEW file at `path` with its
+ * 128-byte header. Each capture appends a frame of the current step: per
+ * cell a 64-byte record and the 2x2 squares that phi = 1/2 crosses in the
+ * cell's (B+2)^2 projected plane (zero ring around the x/y faces), binary32
+ * corners in ascending plane order. The projection is the maximum over the
+ * brick's in-domain z planes (PFB3D_PROJECTION_MAXIMUM) or the plane on the
+ * substrate (PFB3D_PROJECTION_BASAL, substrate slab only). Close with
+ * `complete` != 0 writes the end record; a file closed otherwise (or by
+ * pfb_sim3d_destroy) stays unterminated, marking an incomplete run.
+ * `compress` (zstd) is refused: this build has no zstd. */
+#define PFB3D_PROJECTION_BASAL 1
+#define PFB3D_PROJECTION_MAXIMUM 2
+int pfb_sim3d_boundary_open(pfb_sim3d* s, const char* path, int projection, long long interval,
+                            int compress);
+int pfb_sim3d_boundary_capture(pfb_sim3d* s);
+int pfb_sim3d_boundary_close(pfb_sim3d* s, int complete);
+
 #ifdef __cplusplus
 }
 #endif

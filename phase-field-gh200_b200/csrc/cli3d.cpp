@@ -8,8 +8,11 @@
 // include/pf3d/trajectory_header.hpp metadata line). Everything goes through
 // the library's C ABI.
 //
-// Not part of this build (exit status 2 with a message): the boundary
-// recorder, --initial-centres, soft cells (--cancer-fraction > 0), --strict,
+// The PFB3D boundary recorder (--boundary-out; reference
+// src/pf3d/boundary_output.cu) writes its opening frame at initialisation,
+// frames on the grid of --boundary-interval and a closing frame after the
+// final checkpoint. Not part of this build (exit status 2 with a message):
+// --initial-centres, soft cells (--cancer-fraction > 0), --strict,
 // the memory modes, scratch slots, peer device and shard overrides, and a
 // trajectory for the channel geometry (its wall-overlap columns). The
 // trajectory header and checkpoints state this build's measurement grouping
@@ -55,6 +58,10 @@ struct Options {
          interval_given = false, ckpt_dir_given = false, schedule_given = false, slab_h_given = false,
          channel_h_given = false, wall_k_given = false, wall_w_given = false, pad_given = false;
     std::string ckpt_in, ckpt_dir, out_path;
+    std::string bnd_path;
+    long long bnd_interval = 0;
+    int bnd_projection = PFB3D_PROJECTION_MAXIMUM;
+    bool bnd_compress = false, bnd_given = false;
 };
 
 bool parse_real(const char* flag, const char* s, double lo, double hi, double* v) {
@@ -371,7 +378,9 @@ void usage() {
         "  run:      --t-end --brick-edge --device --bench --print-interval\n"
         "  output:   --out --trajectory-samples --trajectory-interval\n"
         "  restart:  -c|--checkpoint FILE --checkpoint-interval --save-interval\n"
-        "            --checkpoint-dir --no-final-checkpoint\n");
+        "            --checkpoint-dir --no-final-checkpoint\n"
+        "  boundary: --boundary-out FILE --boundary-interval N\n"
+        "            --boundary-projection maximum|basal --boundary-compression none|zstd\n");
 }
 
 struct RealOpt {
@@ -440,6 +449,7 @@ int parse(int argc, char** argv, Options* o) {
         {"--trajectory-interval", 1, 4294967295LL, &o->traj_interval, &o->interval_given},
         {"--checkpoint-interval", 1, 1000000000000LL, &o->ckpt_interval, &o->schedule_given},
         {"--save-interval", 1, 1000000000000LL, &o->save_interval, &o->schedule_given},
+        {"--boundary-interval", 1, 1000000000000LL, &o->bnd_interval, &o->bnd_given},
     };
     for (int i = 1; i < argc; ++i) {
         const char* a = argv[i];
@@ -501,6 +511,28 @@ int parse(int argc, char** argv, Options* o) {
             }
         } else if (!std::strcmp(a, "--no-final-checkpoint")) {
             o->final_ckpt = false;
+        } else if (!std::strcmp(a, "--boundary-out") || !std::strcmp(a, "--boundary-projection") ||
+                   !std::strcmp(a, "--boundary-compression")) {
+            const char* v = value();
+            if (!v) return 2;
+            o->bnd_given = true;
+            if (!std::strcmp(a, "--boundary-out")) {
+                o->bnd_path = v;
+            } else if (!std::strcmp(a, "--boundary-projection")) {
+                if (!std::strcmp(v, "maximum")) o->bnd_projection = PFB3D_PROJECTION_MAXIMUM;
+                else if (!std::strcmp(v, "basal")) o->bnd_projection = PFB3D_PROJECTION_BASAL;
+                else {
+                    std::fprintf(stderr, "[3d] --boundary-projection expects maximum or basal\n");
+                    return 2;
+                }
+            } else {
+                if (!std::strcmp(v, "none")) o->bnd_compress = false;
+                else if (!std::strcmp(v, "zstd")) o->bnd_compress = true;
+                else {
+                    std::fprintf(stderr, "[3d] --boundary-compression expects none or zstd\n");
+                    return 2;
+                }
+            }
         } else {
             std::fprintf(stderr, "[3d] unknown option '%s' or one this build does not provide (try --help)\n", a);
             return 2;
@@ -508,6 +540,14 @@ int parse(int argc, char** argv, Options* o) {
     }
     if (o->soft_fraction != 0.0) {
         std::fprintf(stderr, "[3d] soft cells (--cancer-fraction > 0) are not part of this build\n");
+        return 2;
+    }
+    if (o->bnd_given && (o->bnd_path.empty() || o->bnd_interval <= 0)) {
+        std::fprintf(stderr, "[3d] boundary output requires --boundary-out and --boundary-interval\n");
+        return 2;
+    }
+    if (o->bnd_given && o->bench > 0) {
+        std::fprintf(stderr, "[3d] boundary output cannot be combined with --bench\n");
         return 2;
     }
     p.num_cells = (int)n_cells;
@@ -670,6 +710,10 @@ int main(int argc, char** argv) {
         std::fprintf(stderr, "[3d] dt and t_end do not define a valid step count\n");
         return 2;
     }
+    if (!o.bnd_path.empty() && o.bnd_projection == PFB3D_PROJECTION_BASAL && o.geometry != kSlab) {
+        std::fprintf(stderr, "[3d] basal boundary output requires --geometry slab\n");
+        return 2;
+    }
     if (!o.out_path.empty() && o.geometry == kChannel) {
         std::fprintf(stderr, "[3d] the channel trajectory (wall-overlap columns) is not part of this build\n");
         return 2;
@@ -725,6 +769,30 @@ int main(int argc, char** argv) {
             last_frame = step;
         }
     }
+    long long last_bnd = -1;
+    if (ok && !o.bnd_path.empty()) {
+        // refuse a boundary file that would collide with the trajectory or a checkpoint
+        const size_t slash = o.bnd_path.rfind('/');
+        const std::string name = slash == std::string::npos ? o.bnd_path : o.bnd_path.substr(slash + 1);
+        const bool ckpt_name = name == "checkpoint.pf3d" ||
+                               (name.rfind("checkpoint_", 0) == 0 && name.size() > 5 &&
+                                name.compare(name.size() - 5, 5, ".pf3d") == 0);
+        if (o.bnd_path == o.out_path) {
+            std::fprintf(stderr, "[3d] boundary output and trajectory paths must differ\n");
+            ok = false;
+        } else if (!o.ckpt_dir.empty() && ckpt_name &&
+                   (parent_of(o.bnd_path).empty() ? std::string(".") : parent_of(o.bnd_path)) == o.ckpt_dir) {
+            std::fprintf(stderr, "[3d] boundary output must not use a checkpoint filename\n");
+            ok = false;
+        } else if (pfb_sim3d_boundary_open(s, o.bnd_path.c_str(), o.bnd_projection, o.bnd_interval,
+                                           o.bnd_compress ? 1 : 0) != PFB_OK ||
+                   pfb_sim3d_boundary_capture(s) != PFB_OK) {
+            std::fprintf(stderr, "[3d] %s\n", pfb_last_error());
+            ok = false;
+        } else {
+            last_bnd = step;
+        }
+    }
     const bool ckpt_on = !o.ckpt_dir.empty();
     if (ok && ckpt_on && !mkdirs(o.ckpt_dir)) {
         std::fprintf(stderr, "[3d] cannot create checkpoint directory %s\n", o.ckpt_dir.c_str());
@@ -741,10 +809,12 @@ int main(int argc, char** argv) {
     long long next_ckpt = ckpt_on ? after(step, o.ckpt_interval) : kNever;
     long long next_save = ckpt_on ? after(step, o.save_interval) : kNever;
     long long next_print = after(step, o.print_interval);
+    long long next_bnd = o.bnd_path.empty() ? kNever : grid_after(step, o.bnd_interval);
     constexpr long long kPollEvery = 256;
     uint32_t flags[PFB3D_FLAG_COUNT];
     while (ok && step < total && !g_stop) {
-        const long long stop = std::min({total, next_traj, next_ckpt, next_save, next_print, step + kPollEvery});
+        const long long stop =
+            std::min({total, next_traj, next_ckpt, next_save, next_print, next_bnd, step + kPollEvery});
         if (pfb_sim3d_advance(s, (int)(stop - step)) != PFB_OK || pfb_sim3d_get_flags(s, flags) != PFB_OK) {
             std::fprintf(stderr, "[3d] step failed: %s\n", pfb_last_error());
             ok = false;
@@ -768,6 +838,14 @@ int main(int argc, char** argv) {
             last_frame = step;
             next_traj = after(next_traj, traj_every);
         }
+        if (ok && step >= next_bnd) {
+            if (pfb_sim3d_boundary_capture(s) != PFB_OK) {
+                std::fprintf(stderr, "[3d] %s\n", pfb_last_error());
+                ok = false;
+            }
+            last_bnd = step;
+            next_bnd = after(next_bnd, o.bnd_interval);
+        }
         if (ok && step >= next_ckpt) {
             ok = save(o.ckpt_dir + "/checkpoint.pf3d");
             next_ckpt = after(next_ckpt, o.ckpt_interval);
@@ -782,6 +860,11 @@ int main(int argc, char** argv) {
     if (ok && traj && last_frame != step) ok = write_frame(traj, s, p);
     if (traj) std::fclose(traj);
     if (ok && ckpt_on && o.final_ckpt) ok = save(o.ckpt_dir + "/checkpoint.pf3d");
+    if (ok && !o.bnd_path.empty()) {
+        if (last_bnd != step && pfb_sim3d_boundary_capture(s) != PFB_OK) ok = false;
+        if (pfb_sim3d_boundary_close(s, ok ? 1 : 0) != PFB_OK) ok = false;
+        if (!ok) std::fprintf(stderr, "[3d] %s\n", pfb_last_error());
+    }
     if (ok && g_stop) std::printf("[3d] termination requested; stopped at accepted step %lld\n", step);
     pfb_sim3d_destroy(s);
     return ok ? 0 : 1;

@@ -63,6 +63,15 @@ int boundary2d_capture(Boundary2D* b, const float* phi, const pfb_cell2d* cells,
 // Finish the file (end record) and free the recorder.
 int boundary2d_close(Boundary2D* b);
 
+// PFB3D boundary recorder (boundary3d.cu); projection 1 basal, 2 maximum.
+struct Boundary3D;
+Boundary3D* boundary3d_open(const char* path, const pfb_params3d& p, int projection,
+                            long long interval, int compress);
+int boundary3d_capture(Boundary3D* b, const float* phi, const pfb_cell3d* cells, int B,
+                       cudaStream_t stream, long long step, double time);
+// complete != 0 writes the end record; the recorder is freed either way.
+int boundary3d_close(Boundary3D* b, int complete);
+
 // init2d.cu
 int init_tiles2d(float* phi_a, float* phi_b, pfb_cell2d* cell, const uint8_t* cls, int N, int L,
                  const float* cx, const float* cy, float radius_eff, float kappa_iface,

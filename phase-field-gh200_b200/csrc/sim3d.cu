@@ -50,8 +50,10 @@ struct pfb_sim3d {
     int cur_phi = 0, cur_S = 0;
     long long steps_done = 0;
     double V0 = 0.0;
+    pfb::Boundary3D* bnd = nullptr;  // open PFB3D recorder
 
     ~pfb_sim3d() {
+        if (bnd) (void)pfb::boundary3d_close(bnd, 0);  // unterminated: not a completed run
         if (stream) cudaStreamDestroy(stream);
         cudaFree(d_phi[0]);
         cudaFree(d_phi[1]);
@@ -372,6 +374,29 @@ pfb_sim3d* pfb_sim3d_create_from_state(const pfb_params3d* p, const pfb_cell3d* 
 }
 
 void pfb_sim3d_destroy(pfb_sim3d* s) { delete s; }
+
+int pfb_sim3d_boundary_open(pfb_sim3d* s, const char* path, int projection, long long interval,
+                            int compress) {
+    if (!s) return set_error(PFB_E_ARG, "null sim");
+    if (s->bnd) return set_error(PFB_E_STATE, "a boundary recorder is already open");
+    PFB3_CU(cudaSetDevice(s->device), "cudaSetDevice");
+    s->bnd = pfb::boundary3d_open(path, s->p, projection, interval, compress);
+    return s->bnd ? PFB_OK : PFB_E_ARG;
+}
+
+int pfb_sim3d_boundary_capture(pfb_sim3d* s) {
+    if (!s || !s->bnd) return set_error(PFB_E_STATE, "no boundary recorder is open");
+    PFB3_CU(cudaSetDevice(s->device), "cudaSetDevice");
+    return pfb::boundary3d_capture(s->bnd, s->d_phi[s->cur_phi], s->d_cells, s->B, s->stream,
+                              s->steps_done, (double)s->steps_done * s->p.dt);
+}
+
+int pfb_sim3d_boundary_close(pfb_sim3d* s, int complete) {
+    if (!s || !s->bnd) return set_error(PFB_E_STATE, "no boundary recorder is open");
+    const int rc = pfb::boundary3d_close(s->bnd, complete);
+    s->bnd = nullptr;
+    return rc;
+}
 
 int pfb_sim3d_measure_current(pfb_sim3d* s) {
     if (!s) return set_error(PFB_E_ARG, "null sim");

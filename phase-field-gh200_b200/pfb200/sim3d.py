@@ -178,6 +178,20 @@ class Sim3D:
         the reference does before output and checkpoints)."""
         check(lib().pfb_sim3d_measure_current(self._h), "measure_current")
 
+    def boundary_open(self, path, interval: int, projection: str = "maximum",
+                      compress: bool = False) -> None:
+        """Start a PFB3D boundary recording in a new file (header only);
+        projection "maximum" or "basal" (substrate slab)."""
+        proj = {"basal": 1, "maximum": 2}[projection]
+        check(lib().pfb_sim3d_boundary_open(self._h, str(path).encode(), proj, interval,
+                                            1 if compress else 0), "boundary_open")
+
+    def boundary_capture(self) -> None:
+        check(lib().pfb_sim3d_boundary_capture(self._h), "boundary_capture")
+
+    def boundary_close(self, complete: bool = True) -> None:
+        check(lib().pfb_sim3d_boundary_close(self._h, 1 if complete else 0), "boundary_close")
+
     def bench(self, warmup: int, steps: int) -> float:
         ms = C.c_double()
         check(lib().pfb_sim3d_bench(self._h, warmup, steps, C.byref(ms)), "bench")

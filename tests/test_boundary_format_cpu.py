@@ -69,3 +69,24 @@ def test_refusals(tmp_path):
     (tmp_path / "e.pfb").write_bytes(file_bytes([good], end=False))
     with pytest.raises(ValueError):
         bf.read(tmp_path / "e.pfb")
+
+
+def test_pfb3d_layout_and_reader(tmp_path):
+    assert bf.HEADER3D.size == 128 and bf.CELL3D_DTYPE.itemsize == 64
+    head = bf.HEADER3D.pack(b"PFB3D1\0\0", 1, 128, 2, 2, 3, 0, 40, 40, 56, 1.0, 1.0, 1.0, 0.01,
+                            1e4, 0.5, 2, 20, 64, 0)
+    cells = np.zeros(2, bf.CELL3D_DTYPE)
+    cells["id"] = [0, 1]
+    cells["squares"] = [1, 2]
+    sq = np.zeros(3, bf.SQUARE_DTYPE)
+    sq["xy"] = [5, 7, 9]
+    payload = cells.tobytes() + sq.tobytes()
+    frame = struct.pack("<8sQdQQQ", b"P3BFRM1\0", 4, 0.04, len(payload), len(payload),
+                        bf.fnv1a64(payload)) + payload
+    end = struct.pack("<8sQdQQQ", b"P3BEND1\0", 4, 0.04, 0, 0, 0)
+    (tmp_path / "b").write_bytes(head + frame + end)
+    b = bf.read3d(tmp_path / "b")
+    assert b.complete and b.projection == 2 and b.shape == (40, 40, 56) and b.end_step == 4
+    assert [list(s["xy"]) for s in b.frames[0].squares] == [[5], [7, 9]]
+    (tmp_path / "u").write_bytes(head + frame)  # unterminated: an incomplete run
+    assert not bf.read3d(tmp_path / "u").complete

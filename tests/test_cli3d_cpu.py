@@ -83,10 +83,19 @@ def test_help():
     (("--geometry", "slab", "--radius", 8, "--lambda", 3, "--slab-height", 3), "must exceed"),
     (("--cancer-fraction", 0.25), "soft cells"),
     (("--strict",), "unknown option"),
-    (("--boundary-out", "x"), "unknown option"),
+    (("--boundary-out", "x", "--boundary-interval", 2, "--memory-mode", "auto"), "unknown option"),
     (("--trajectory-interval", 0), "--trajectory-interval expects"),
     (("--seed", -4), "unsigned"),
     (("--out",), "requires a value"),
+    (("--boundary-out", "b.pfb3d"), "requires --boundary-out and --boundary-interval"),
+    (("--boundary-interval", 5), "requires --boundary-out and --boundary-interval"),
+    (("--boundary-out", "b", "--boundary-interval", 5, "--boundary-projection", "flat"),
+     "expects maximum or basal"),
+    (("--boundary-out", "b", "--boundary-interval", 5, "--boundary-compression", "gz"),
+     "expects none or zstd"),
+    (("--boundary-out", "b", "--boundary-interval", 5, "--bench", 3), "cannot be combined"),
+    (("--boundary-out", "b", "--boundary-interval", 5, "--boundary-projection", "basal"),
+     "requires --geometry slab"),
 ])
 def test_usage_errors(args, msg):
     r = run(*args)
