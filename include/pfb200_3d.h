@@ -306,7 +306,9 @@ typedef struct pfb_params3d {
 typedef struct pfb_sim3d pfb_sim3d;
 
 /* Fresh start from cell centres (world coordinates, substrate centres at
- * z = -0.5 as in the reference); N = p->num_cells entries. */
+ * z = -0.5 as in the reference; channel centres in slit coordinates, moved
+ * to array coordinates as z + padding - 1/2 in binary32 as the reference
+ * does); N = p->num_cells entries. */
 pfb_sim3d* pfb_sim3d_create(const pfb_params3d* p, const pfb_vec3* centres, int device);
 /* Restart from cell records and base B^3 bricks (x fastest) of step `step`,
  * as the reference's Sim3D::init_checkpoint does (src/pf3d/sim.cu:794-885):
@@ -341,6 +343,13 @@ int pfb_sim3d_measure_args(pfb_sim3d* s, pfb_measure_args3d* out);
 void* pfb_sim3d_stream(const pfb_sim3d* s);
 /* Device time of `steps` steps after `warmup`, in ms (CUDA events). */
 int pfb_sim3d_bench(pfb_sim3d* s, int warmup, int steps, double* ms);
+
+/* Channel wall diagnostics of the current field (reference
+ * k_measure_wall_diagnostics, src/pf3d/kernels.cu): sets each cell's
+ * wall_overlap = sum of phi^2 psi_w^2(z) and outside_slit_volume = sum of
+ * phi^2 outside the slit over its in-domain voxels, psi_w^2 the binary32
+ * wall profile. Hard-wall channel only. */
+int pfb_sim3d_measure_wall(pfb_sim3d* s);
 
 /* PFB3D boundary recorder (reference src/pf3d/boundary_output.cu, file
  * layout common/boundary_format_3d.h): creates a NEW file at `path` with its

@@ -13,8 +13,7 @@
 // frames on the grid of --boundary-interval and a closing frame after the
 // final checkpoint. Not part of this build (exit status 2 with a message):
 // --initial-centres, soft cells (--cancer-fraction > 0), --strict,
-// the memory modes, scratch slots, peer device and shard overrides, and a
-// trajectory for the channel geometry (its wall-overlap columns). The
+// the memory modes, scratch slots, peer device and shard overrides. The
 // trajectory header and checkpoints state this build's measurement grouping
 // (4 CTAs per base cell, one-CTA promoted policy).
 #include <algorithm>
@@ -207,7 +206,22 @@ std::string header(const pfb_params3d& p, const Options& o, int B, uint64_t hash
         "soft_fraction=%a seed=%llu polarity_stream=%llu init_hash=%016llx "
         "promoted_measure_reduction=one-cta promoted_measure_policy=0 "
         "promoted_measure_auto_wave_ctas=0 base_measure_shards=%d trajectory_interval=%llu";
-    if (p.boundary_flags == PFB3D_BOUNDARY_SUBSTRATE_SLAB) {
+    if (p.boundary_flags == PFB3D_BOUNDARY_HARD_WALL_CHANNEL) {
+        const std::string fmt =
+            "# phase_field_gh200 trajectory schema=1 dim=3 geometry=resolved-wall-channel "
+            "boundary=periodic-xy outer_array_boundary=homogeneous-neumann-z N=%d "
+            "Nx=%d Ny=%d allocated_Nz=%d H=%d padding=%d B=%d "
+            "z_coordinate=height-above-lower-wall lower_wall_z=0 upper_wall_z=%d "
+            "wall_profile=tanh-union kappa_w=%a lambda_w=%a translation=three-dimensional "
+            "dx=%a dt=%a aging_time=%a rho_V_target=%a rho_V_realized=%a "
+            "R=%a lambda=%a kappa=%a mu=%a xi=%a " + tail;
+        std::snprintf(t, sizeof(t), fmt.c_str(), p.num_cells, p.Nx, p.Ny, p.Nz, p.channel_height,
+                      p.channel_padding, B, p.channel_height, p.wall_kappa, p.wall_width, 1.0, p.dt,
+                      p.aging_time, o.rho, realized_rho(p), p.target_radius, p.lambda, p.kappa, p.mu, p.xi,
+                      p.tau, p.v_A, p.v_A_sigma, p.gamma, o.gamma_soft, o.soft_fraction,
+                      (unsigned long long)p.seed, ps, (unsigned long long)hash, kMeasureShards,
+                      (unsigned long long)every);
+    } else if (p.boundary_flags == PFB3D_BOUNDARY_SUBSTRATE_SLAB) {
         const std::string fmt =
             "# phase_field_gh200 trajectory schema=1 dim=3 geometry=substrate-slab "
             "boundary=periodic-xy N=%d Nx=%d Ny=%d Nz=%d B=%d "
@@ -237,13 +251,17 @@ const char* kColsPeriodic =
 const char* kColsSlab =
     "# columns: time cell_id x y height vx vy vz px py pz gamma v_A "
     "free_interface_proxy hemisphere_normalized_free_surface_compactness volume phi_max";
+const char* kColsChannel =
+    "# columns: time cell_id x y height vx vy vz px py pz gamma v_A "
+    "interface_measure sphericity_proxy volume phi_max wall_overlap wall_overlap_fraction "
+    "outside_slit_volume physical_penetration_fraction";
 
 // Open for append. A new (empty) file gets the two header lines and
 // *last_step = -1; an existing one must carry this run's header and whole
 // frames of canonically ordered rows with strictly increasing times, the
 // last of which lies at a step not beyond `step` (returned in *last_step).
 bool open_traj(const std::string& path, const std::string& head, const char* cols, int N, double dt,
-               long long step, std::FILE** out, long long* last_step) {
+               long long step, bool channel, std::FILE** out, long long* last_step) {
     const std::string dir = parent_of(path);
     if (!dir.empty() && !mkdirs(dir)) {
         std::fprintf(stderr, "[3d] cannot create trajectory directory\n");
@@ -293,15 +311,19 @@ bool open_traj(const std::string& path, const std::string& head, const char* col
     double frame_t = 0.0, prev_t = -1.0;
     while (next()) {
         if (line[0] == '\0') return fail("blank line in trajectory payload");
-        double v[16];
+        double v[20];
         long long id = 0;
         char extra = 0;
+        // 16 values after the id, 20 with the channel's wall columns
         const int got = std::sscanf(line.data(),
-                                    "%lf %lld %lf %lf %lf %lf %lf %lf %lf %lf %lf %lf %lf %lf %lf %lf %lf %c",
+                                    "%lf %lld %lf %lf %lf %lf %lf %lf %lf %lf %lf %lf %lf %lf %lf %lf %lf "
+                                    "%lf %lf %lf %lf %c",
                                     &v[0], &id, &v[1], &v[2], &v[3], &v[4], &v[5], &v[6], &v[7], &v[8], &v[9],
-                                    &v[10], &v[11], &v[12], &v[13], &v[14], &v[15], &extra);
-        bool finite = got == 17;
-        for (int k = 0; finite && k < 16; ++k) finite = std::isfinite(v[k]);
+                                    &v[10], &v[11], &v[12], &v[13], &v[14], &v[15], &v[16], &v[17], &v[18],
+                                    &v[19], &extra);
+        const int values = channel ? 20 : 16;
+        bool finite = got == values + 1;
+        for (int k = 0; finite && k < values; ++k) finite = std::isfinite(v[k]);
         if (!finite) {
             std::fprintf(stderr, "[3d] malformed trajectory row %llu\n", rows + 1);
             std::fclose(f);
@@ -338,7 +360,9 @@ bool open_traj(const std::string& path, const std::string& head, const char* col
 // device forms it, one fused multiply-add), heights above the lower face for
 // the slab, then the shape measure of the geometry.
 bool write_frame(std::FILE* f, pfb_sim3d* s, const pfb_params3d& p) {
+    const bool channel = p.boundary_flags == PFB3D_BOUNDARY_HARD_WALL_CHANNEL;
     if (pfb_sim3d_measure_current(s) != PFB_OK) return false;
+    if (channel && pfb_sim3d_measure_wall(s) != PFB_OK) return false;
     std::vector<pfb_cell3d> c((size_t)p.num_cells);
     if (pfb_sim3d_get_cells(s, c.data()) != PFB_OK) return false;
     const double t = (double)pfb_sim3d_step(s) * p.dt;
@@ -350,16 +374,21 @@ bool write_frame(std::FILE* f, pfb_sim3d* s, const pfb_params3d& p) {
         const double y = std::fma(k.Cy, inv, (double)k.origin_y);
         double z = std::fma(k.Cz, inv, (double)k.origin_z);
         if (slab) z += 0.5;
+        if (channel) z += 0.5 - (double)p.channel_padding;
         double shape = 0.0;
         if (k.V > 0.0 && k.surface > 0.0)
             shape = slab ? hemi * std::pow(k.V, 2.0 / 3.0) / k.surface
                          : std::cbrt(kPi) * std::pow(6.0 * k.V, 2.0 / 3.0) / k.surface;
         if (std::fprintf(f,
                          "%.17g %lld %.17g %.17g %.17g %.9g %.9g %.9g %.9g %.9g %.9g %.9g %.9g %.17g %.17g %.17g "
-                         "%.9g\n",
+                         "%.9g",
                          t, (long long)k.global_id, x, y, z, (double)k.velocity_x, (double)k.velocity_y,
                          (double)k.velocity_z, (double)k.polarity_x, (double)k.polarity_y, (double)k.polarity_z,
-                         (double)k.gamma, (double)k.v_A, k.surface, shape, k.V, (double)k.phi_max) < 0) {
+                         (double)k.gamma, (double)k.v_A, k.surface, shape, k.V, (double)k.phi_max) < 0 ||
+            (channel ? std::fprintf(f, " %.17g %.17g %.17g %.17g\n", k.wall_overlap,
+                                    k.V > 0.0 ? k.wall_overlap / k.V : 0.0, k.outside_slit_volume,
+                                    k.V > 0.0 ? k.outside_slit_volume / k.V : 0.0)
+                     : std::fputc('\n', f)) < 0) {
             std::fprintf(stderr, "[3d] failed to write trajectory frame\n");
             return false;
         }
@@ -694,11 +723,9 @@ int main(int argc, char** argv) {
         hash = table_hash(x, y, z);
         std::printf("  centres: %d placed, table hash %016llx\n", p.num_cells, (unsigned long long)hash);
         std::fflush(stdout);
-        for (size_t i = 0; i < x.size(); ++i) {
-            // channel centres move from slit to array coordinates in binary32
-            const float zs = o.geometry == kChannel ? z[i] + (float)p.channel_padding - 0.5f : z[i];
-            centres.push_back(pfb_vec3{x[i], y[i], zs});
-        }
+        // channel centres stay in slit coordinates: pfb_sim3d_create moves
+        // them to array coordinates (z + padding - 1/2 in binary32)
+        for (size_t i = 0; i < x.size(); ++i) centres.push_back(pfb_vec3{x[i], y[i], z[i]});
     }
     if (!o.ckpt_dir_given && o.schedule_given) {
         o.ckpt_dir = parent_of(o.out_path);
@@ -712,10 +739,6 @@ int main(int argc, char** argv) {
     }
     if (!o.bnd_path.empty() && o.bnd_projection == PFB3D_PROJECTION_BASAL && o.geometry != kSlab) {
         std::fprintf(stderr, "[3d] basal boundary output requires --geometry slab\n");
-        return 2;
-    }
-    if (!o.out_path.empty() && o.geometry == kChannel) {
-        std::fprintf(stderr, "[3d] the channel trajectory (wall-overlap columns) is not part of this build\n");
         return 2;
     }
 
@@ -760,9 +783,9 @@ int main(int argc, char** argv) {
     std::FILE* traj = nullptr;
     long long step = pfb_sim3d_step(s), last_frame = -1;
     if (!o.out_path.empty()) {
-        const char* cols = o.geometry == kSlab ? kColsSlab : kColsPeriodic;
-        ok = open_traj(o.out_path, header(p, o, B, hash, traj_every), cols, p.num_cells, p.dt, step, &traj,
-                       &last_frame);
+        const char* cols = o.geometry == kSlab ? kColsSlab : o.geometry == kChannel ? kColsChannel : kColsPeriodic;
+        ok = open_traj(o.out_path, header(p, o, B, hash, traj_every), cols, p.num_cells, p.dt, step,
+                       o.geometry == kChannel, &traj, &last_frame);
         // a new file starts at the initialized state
         if (ok && last_frame < 0) {
             ok = write_frame(traj, s, p);

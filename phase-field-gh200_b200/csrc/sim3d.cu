@@ -45,6 +45,7 @@ struct pfb_sim3d {
     uint32_t* d_flags = nullptr;
     uint64_t* d_step = nullptr;
     float* d_wall = nullptr;
+    float* d_wall_psi = nullptr;  // channel: psi_w^2 per plane (diagnostics)
     pfb_vec3* d_centres = nullptr;
     cudaStream_t stream = nullptr;
     int cur_phi = 0, cur_S = 0;
@@ -64,6 +65,7 @@ struct pfb_sim3d {
         cudaFree(d_flags);
         cudaFree(d_step);
         cudaFree(d_wall);
+        cudaFree(d_wall_psi);
         cudaFree(d_centres);
     }
 };
@@ -75,6 +77,48 @@ int geometry_ok3(int B, const pfb_layout3d& L);
 }  // namespace pfb
 
 namespace {
+
+// Channel wall diagnostics of each cell (reference src/pf3d/kernels.cu,
+// k_measure_wall_diagnostics): FP64 sums over the brick's in-domain voxels
+// of phi^2 psi_w^2(z) (wall overlap) and of phi^2 outside the slit. One CTA
+// per cell; warp sums, then ascending warps.
+constexpr int kWallThreads = 256;
+__global__ void __launch_bounds__(kWallThreads)
+    k_wall_diag3d(const float* phi, pfb_cell3d* cells, int B, int nz, int pad, int H,
+                  const float* psi) {
+    const int n = blockIdx.x;
+    const size_t words = (size_t)B * B * B, plane = (size_t)B * B;
+    const float* brick = phi + (size_t)n * words;
+    const int64_t oz = cells[n].origin_z;
+    double overlap = 0.0, outside = 0.0;
+    for (size_t q = threadIdx.x; q < words; q += kWallThreads) {
+        const int64_t z = oz + (int64_t)(q / plane);
+        if (z < 0 || z >= nz) continue;
+        const double v = (double)brick[q];
+        const double sq = v * v;
+        overlap += sq * (double)psi[z];
+        if (z < pad || z >= pad + H) outside += sq;
+    }
+    __shared__ double wo[kWallThreads / 32], wt[kWallThreads / 32];
+    for (int d = 16; d; d >>= 1) {
+        overlap += __shfl_down_sync(0xFFFFFFFFu, overlap, d);
+        outside += __shfl_down_sync(0xFFFFFFFFu, outside, d);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        wo[threadIdx.x >> 5] = overlap;
+        wt[threadIdx.x >> 5] = outside;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int w = 0; w < kWallThreads / 32; ++w) {
+            a += wo[w];
+            b += wt[w];
+        }
+        cells[n].wall_overlap = a;
+        cells[n].outside_slit_volume = b;
+    }
+}
 
 double volume0(const pfb_params3d& p) {
     const double sphere = 4.0 * kPi * p.target_radius * p.target_radius * p.target_radius / 3.0;
@@ -112,7 +156,7 @@ int validate3(const pfb_params3d& p) {
 
 int upload_wall(pfb_sim3d* s) {
     const pfb_params3d& p = s->p;
-    std::vector<float> w((size_t)p.Nz);
+    std::vector<float> w((size_t)p.Nz), psi((size_t)p.Nz);
     const float ratio = (float)(p.wall_kappa / p.kappa);
     const double k = 2.7386127875258306 / p.wall_width;
     const double lo = (double)p.channel_padding, hi = lo + p.channel_height;
@@ -120,8 +164,13 @@ int upload_wall(pfb_sim3d* s) {
         const double c = (double)z + 0.5;
         const double fluid = 0.25 * (1.0 + std::tanh(k * (c - lo))) * (1.0 - std::tanh(k * (c - hi)));
         const double wall = 1.0 - fluid;
-        w[(size_t)z] = ratio * (float)(wall * wall);
+        psi[(size_t)z] = (float)(wall * wall);
+        w[(size_t)z] = ratio * psi[(size_t)z];
     }
+    PFB3_CU(cudaMalloc(&s->d_wall_psi, psi.size() * sizeof(float)), "cudaMalloc(wall psi)");
+    PFB3_CU(cudaMemcpyAsync(s->d_wall_psi, psi.data(), psi.size() * sizeof(float),
+                            cudaMemcpyHostToDevice, s->stream),
+            "upload wall psi");
     PFB3_CU(cudaMalloc(&s->d_wall, w.size() * sizeof(float)), "cudaMalloc(wall)");
     PFB3_CU(cudaMemcpyAsync(s->d_wall, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice,
                             s->stream),
@@ -374,6 +423,19 @@ pfb_sim3d* pfb_sim3d_create_from_state(const pfb_params3d* p, const pfb_cell3d* 
 }
 
 void pfb_sim3d_destroy(pfb_sim3d* s) { delete s; }
+
+int pfb_sim3d_measure_wall(pfb_sim3d* s) {
+    if (!s) return set_error(PFB_E_ARG, "null sim");
+    if (!hard_wall_channel(s->p.boundary_flags) || !s->d_wall_psi)
+        return set_error(PFB_E_CONFIG, "wall diagnostics need the hard-wall channel");
+    PFB3_CU(cudaSetDevice(s->device), "cudaSetDevice");
+    k_wall_diag3d<<<s->N, kWallThreads, 0, s->stream>>>(s->d_phi[s->cur_phi], s->d_cells, s->B,
+                                                       s->p.Nz, s->p.channel_padding,
+                                                       s->p.channel_height, s->d_wall_psi);
+    PFB3_CU(cudaGetLastError(), "wall diagnostics");
+    PFB3_CU(cudaStreamSynchronize(s->stream), "wall diagnostics");
+    return PFB_OK;
+}
 
 int pfb_sim3d_boundary_open(pfb_sim3d* s, const char* path, int projection, long long interval,
                             int compress) {

@@ -163,6 +163,7 @@ _abi._SIGS.update({
     "pfb_sim3d_create": (P, [C.POINTER(Params3D), P, I]),
     "pfb_sim3d_create_from_state": (P, [C.POINTER(Params3D), P, P, C.c_longlong, I]),
     "pfb_sim3d_measure_current": (I, [P]),
+    "pfb_sim3d_measure_wall": (I, [P]),
     "pfb_sim3d_boundary_open": (I, [P, C.c_char_p, I, C.c_longlong, I]),
     "pfb_sim3d_boundary_capture": (I, [P]),
     "pfb_sim3d_boundary_close": (I, [P, I]),

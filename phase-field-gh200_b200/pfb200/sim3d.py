@@ -178,6 +178,11 @@ class Sim3D:
         the reference does before output and checkpoints)."""
         check(lib().pfb_sim3d_measure_current(self._h), "measure_current")
 
+    def measure_wall(self) -> None:
+        """Channel wall diagnostics of the current field into the cell
+        records (wall_overlap, outside_slit_volume)."""
+        check(lib().pfb_sim3d_measure_wall(self._h), "measure_wall")
+
     def boundary_open(self, path, interval: int, projection: str = "maximum",
                       compress: bool = False) -> None:
         """Start a PFB3D boundary recording in a new file (header only);

@@ -19,7 +19,7 @@ EXE = ROOT / "phase-field-gh200_b200" / "pfb200" / "_lib" / "pfb_cell_3d"
 REF = ROOT / "oracle" / "_ref" / "cell_gh200_3d"
 ARGS = ("--N", 3, "--radius", 4, "--lambda", 3, "--v-A", 0.05, "--seed", 11,
         "--trajectory-interval", 2, "--print-interval", 0)
-GEOMETRIES = [("periodic", 0.007), ("slab", 0.05)]
+GEOMETRIES = [("periodic", 0.007), ("slab", 0.05), ("channel", 0.05)]
 
 
 def run(exe, *args):
