@@ -114,6 +114,15 @@ def rclib() -> C.CDLL:
         L.ref3d_cpu_channel3d.restype = I
         L.ref3d_cpu_table_hash.argtypes = [I, F, F, F]
         L.ref3d_cpu_table_hash.restype = C.c_uint64
+        U = C.POINTER(C.c_uint64)
+        L.ref_read_table2.argtypes = [C.c_char_p, I, D, D, F, F, U]
+        L.ref_read_table2.restype = I
+        L.ref_read_relaxed2.argtypes = [C.c_char_p, I, D, I, F, F]
+        L.ref_read_relaxed2.restype = I
+        L.ref_read_table3.argtypes = [C.c_char_p, I, D, D, F, F, F, U]
+        L.ref_read_table3.restype = I
+        L.ref_read_channel3.argtypes = [C.c_char_p, I, D, I, D, F, F, F, U]
+        L.ref_read_channel3.restype = I
         _RC = L
     return _RC
 

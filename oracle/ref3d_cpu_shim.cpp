@@ -2,14 +2,17 @@
 // dense FP64 one-step evaluation and seed-radius calibration
 // (include/pf3d/reference.hpp, header-only; compiled in place by
 // oracle/Makefile into oracle/_ref/libref3d_cpu.so), and the reference's
-// fresh-start placements and centre-table hash (include/palmieri_initializer.hpp,
+// fresh-start placements, centre-table readers and centre-table hash
+// (include/palmieri_initializer.hpp, include/relaxed_centres.hpp,
 // include/pf3d/palmieri_initializer.hpp, include/pf3d/initializer.hpp). The
-// tests pin the 3D oracle and the placement restatement against it.
+// tests pin the 3D oracle, the placement restatement and the command lines'
+// table readers against it.
 #include <cstdint>
 #include <cstring>
 #include <exception>
 
 #include "palmieri_initializer.hpp"
+#include "relaxed_centres.hpp"
 #include "pf3d/palmieri_initializer.hpp"
 #include "pf3d/reference.hpp"
 #include "pf3d/rng.cuh"
@@ -143,6 +146,59 @@ int ref3d_cpu_channel3d(int n, double side, int height, double radius, uint64_t 
 uint64_t ref3d_cpu_table_hash(int n, const float* x, const float* y, const float* z) {
     const std::vector<float> a(x, x + n), b(y, y + n), c(z, z + n);
     return pf3d::centre_table_fnv1a64(pf3d::ordered_global_ids((std::size_t)n), a, b, c);
+}
+
+// The reference's --initial-centres readers: 0 and the table's hash (and
+// its centres) when accepted, -1 when refused.
+int ref_read_table2(const char* path, int n, double side, double radius, float* x, float* y,
+                    uint64_t* hash) {
+    std::vector<float> a, b;
+    pf::PalmieriCentresCsvDiagnostics d{};
+    std::string err;
+    if (!pf::palmieri_read_centres_csv(path, n, side, radius, &a, &b, &d, &err)) return -1;
+    put(a, x);
+    put(b, y);
+    *hash = d.table_fnv1a64;
+    return 0;
+}
+
+int ref_read_relaxed2(const char* path, int n, double side, int need_source_side, float* x, float* y) {
+    std::vector<std::int64_t> ids;
+    std::vector<float> a, b;
+    pf::RelaxedCentresCsvDiagnostics d{};
+    std::string err;
+    if (!pf::relaxed_read_centres_csv(path, n, side, &ids, &a, &b, &d, &err, need_source_side != 0))
+        return -1;
+    put(a, x);
+    put(b, y);
+    return 0;
+}
+
+int ref_read_table3(const char* path, int n, double side, double radius, float* x, float* y,
+                    float* z, uint64_t* hash) {
+    std::vector<float> a, b, c;
+    pf3d::PalmieriCentres3DCsvDiagnostics d{};
+    std::string err;
+    if (!pf3d::palmieri3d_read_centres_csv(path, n, side, radius, &a, &b, &c, &d, &err)) return -1;
+    put(a, x);
+    put(b, y);
+    put(c, z);
+    *hash = d.table_fnv1a64;
+    return 0;
+}
+
+int ref_read_channel3(const char* path, int n, double side, int height, double radius, float* x,
+                      float* y, float* z, uint64_t* hash) {
+    std::vector<float> a, b, c;
+    pf3d::PalmieriCentres3DCsvDiagnostics d{};
+    std::string err;
+    if (!pf3d::channel3d_read_centres_csv(path, n, side, height, radius, &a, &b, &c, &d, &err))
+        return -1;
+    put(a, x);
+    put(b, y);
+    put(c, z);
+    *hash = d.table_fnv1a64;
+    return 0;
 }
 
 }  // extern "C"

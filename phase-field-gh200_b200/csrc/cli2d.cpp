@@ -8,7 +8,7 @@
 // the PFVMOM4 velocity-moment recorder (--velocity-moments; reference
 // src/velocity_output.cu), the PFB boundary recorder (--boundary-out;
 // src/boundary.cu), --bench. Not part of this build (they exit with status 2
-// and a message): --initial-centres, the mobility map, --morton, --no-l2,
+// and a message): the mobility map, --morton, --no-l2,
 // --strict and --self-test, velocity observation under --bench, and, on
 // resume, overrides of model parameters other than the output cadences and
 // t_end. zstd boundary compression is refused at open (no zstd here).
@@ -24,6 +24,7 @@
 #include <sys/stat.h>
 #include <vector>
 
+#include "centres_csv.hpp"
 #include "pfb200.h"
 #include "pfb200_ckpt.h"
 
@@ -55,6 +56,7 @@ struct Options {
     std::string bnd_path;
     long long bnd_interval = 0;
     bool bnd_compress = false;
+    std::string centres_path;  // --initial-centres
 };
 
 constexpr double kPi = 3.14159265358979323846;
@@ -66,7 +68,8 @@ void usage() {
         "  --tau <f> --v-A <f> --v-A-sigma <f> --gamma <f> --gamma-cancer <f>\n"
         "  --cancer-fraction <f> --phase-field-mobility <f> --dt <f> --t-end <f>\n"
         "  --seed <u64> --polarity-seed <u64> --full-moment <int> --verify-every <int>\n"
-        "  --print-interval <int>  -c|--checkpoint <path>  --checkpoint-interval <n>\n"
+        "  --print-interval <int>  --initial-centres <csv>  -c|--checkpoint <path>\n"
+        "  --checkpoint-interval <n>\n"
         "  --save-interval <n>  --checkpoint-dir <path>  --no-final-checkpoint\n"
         "  --trajectory-samples <n>  --trajectory-interval <n>  --out <path>\n"
         "  --device <int>  --bench <steps>  --no-graph\n"
@@ -409,7 +412,14 @@ int parse(int argc, char** argv, Options* o) {
                 o->bnd_compress = true;
             else
                 return 2;
-        } else if (a == "--initial-centres" || a == "--phase-field-mobility-map" || a == "--morton" ||
+        } else if (a == "--initial-centres") {
+            if (!(v = val())) return 2;
+            if (!v[0]) {
+                std::fprintf(stderr, "[fatal] --initial-centres requires a non-empty path\n");
+                return 2;
+            }
+            o->centres_path = v;
+        } else if (a == "--phase-field-mobility-map" || a == "--morton" ||
                    a == "--no-l2" || a == "--strict" || a == "--self-test") {
             std::fprintf(stderr, "[fatal] option '%s' is not part of this build\n", a.c_str());
             return 2;
@@ -458,6 +468,11 @@ int main(int argc, char** argv) {
     pfb_sim2d* s = nullptr;
     pfb_ckpt2d_params rec{};
     if (!o.ckpt_in.empty()) {
+        if (!o.centres_path.empty()) {
+            std::fprintf(stderr, "[fatal] --initial-centres is valid only for a fresh start; a checkpoint "
+                                 "already holds the initialised state\n");
+            return 2;
+        }
         if (o.n_or_rho) {
             std::fprintf(stderr, "[fatal] --N and --rho cannot be overridden on resume\n");
             return 2;
@@ -490,8 +505,20 @@ int main(int argc, char** argv) {
             return 3;
         }
         std::vector<float> x((size_t)p.num_cells), y((size_t)p.num_cells);
-        if (pfb_grid_jitter_centres(p.num_cells, p.L, p.seed, x.data(), y.data()) != PFB_OK) return 3;
+        if (!o.centres_path.empty()) {
+            // a validated table (reference src/sim.cu:90-106)
+            std::string err;
+            if (!pfb_csv::read_table2(o.centres_path, p.num_cells, (double)p.L, p.target_radius, x, y, &err)) {
+                std::fprintf(stderr, "[fatal] invalid --initial-centres '%s': %s\n", o.centres_path.c_str(),
+                             err.c_str());
+                return 5;
+            }
+        } else if (pfb_grid_jitter_centres(p.num_cells, p.L, p.seed, x.data(), y.data()) != PFB_OK) {
+            return 3;
+        }
         hash = table_fnv1a64(x, y);
+        std::printf("  centres: %d, table hash %016llx\n", p.num_cells, (unsigned long long)hash);
+        std::fflush(stdout);
         s = pfb_sim2d_create(&p, x.data(), y.data(), o.device);
     }
     if (!s) {

@@ -11,8 +11,10 @@
 // The PFB3D boundary recorder (--boundary-out; reference
 // src/pf3d/boundary_output.cu) writes its opening frame at initialisation,
 // frames on the grid of --boundary-interval and a closing frame after the
-// final checkpoint. Not part of this build (exit status 2 with a message):
-// --initial-centres, soft cells (--cancer-fraction > 0), --strict,
+// final checkpoint. --initial-centres reads the reference's centre tables
+// (periodic x,y,z; relaxed x,y for the slab and the one-layer channel;
+// channel x,y,z). Not part of this build (exit status 2 with a message):
+// soft cells (--cancer-fraction > 0), --strict,
 // the memory modes, scratch slots, peer device and shard overrides. The
 // trajectory header and checkpoints state this build's measurement grouping
 // (4 CTAs per base cell, one-CTA promoted policy).
@@ -30,6 +32,7 @@
 #include <sys/stat.h>
 #include <vector>
 
+#include "centres_csv.hpp"
 #include "pfb200.h"
 #include "pfb200_3d.h"
 #include "pfb200_ckpt.h"
@@ -61,6 +64,7 @@ struct Options {
     long long bnd_interval = 0;
     int bnd_projection = PFB3D_PROJECTION_MAXIMUM;
     bool bnd_compress = false, bnd_given = false;
+    std::string centres_path;  // --initial-centres
 };
 
 bool parse_real(const char* flag, const char* s, double lo, double hi, double* v) {
@@ -404,7 +408,7 @@ void usage() {
         "  model:    --N --radius --rho --lambda --kappa --mu --xi --tau --v-A --v-A-sigma\n"
         "            --gamma --gamma-cancer --cancer-fraction (0 only) --dt --aging-time\n"
         "            --seed --polarity-seed --full-moment --verify-every\n"
-        "  run:      --t-end --brick-edge --device --bench --print-interval\n"
+        "  run:      --t-end --brick-edge --device --bench --print-interval --initial-centres CSV\n"
         "  output:   --out --trajectory-samples --trajectory-interval\n"
         "  restart:  -c|--checkpoint FILE --checkpoint-interval --save-interval\n"
         "            --checkpoint-dir --no-final-checkpoint\n"
@@ -540,6 +544,10 @@ int parse(int argc, char** argv, Options* o) {
             }
         } else if (!std::strcmp(a, "--no-final-checkpoint")) {
             o->final_ckpt = false;
+        } else if (!std::strcmp(a, "--initial-centres")) {
+            const char* v = value();
+            if (!v || !v[0]) return 2;
+            o->centres_path = v;
         } else if (!std::strcmp(a, "--boundary-out") || !std::strcmp(a, "--boundary-projection") ||
                    !std::strcmp(a, "--boundary-compression")) {
             const char* v = value();
@@ -672,7 +680,7 @@ int main(int argc, char** argv) {
     pfb_ckpt3d_params rec{};
     std::vector<pfb_vec3> centres;
     if (resumed) {
-        if (o.model_given) {
+        if (o.model_given || !o.centres_path.empty()) {
             std::fprintf(stderr, "[3d] checkpoint continuation preserves its model and initialized state; only "
                                  "--t-end and run/output options may change\n");
             return 2;
@@ -707,7 +715,34 @@ int main(int argc, char** argv) {
         p.B = (int)o.brick;
         const double R = p.target_radius;
         std::vector<float> x, y, z;
-        if (o.geometry == kSlab) {
+        std::string err;
+        bool read_ok = true;
+        if (!o.centres_path.empty()) {
+            // the reference's tables (src/pf3d/sim.cu:900-1096)
+            std::vector<int64_t> ids;
+            if (o.geometry == kSlab) {
+                read_ok = pfb_csv::read_relaxed2(o.centres_path, p.num_cells, (double)p.Nx, false, ids, x, y, &err);
+                z.assign(x.size(), -0.5f);
+            } else if (o.geometry == kChannel && pfb_csv::first_line(o.centres_path) == "global_id,x,y") {
+                const int one_layer = (int)std::ceil(2.0 * R);
+                if (p.channel_height != one_layer) {
+                    std::fprintf(stderr, "[3d] a 2D relaxed x/y table is accepted only for the one-layer "
+                                         "channel H=ceil(2R)=%d\n", one_layer);
+                    return 1;
+                }
+                read_ok = pfb_csv::read_relaxed2(o.centres_path, p.num_cells, (double)p.Nx, true, ids, x, y, &err);
+                z.assign(x.size(), (float)(0.5 * one_layer));
+            } else if (o.geometry == kChannel) {
+                read_ok = pfb_csv::read_channel3(o.centres_path, p.num_cells, (double)p.Nx, p.channel_height, R,
+                                                 x, y, z, &err);
+            } else {
+                read_ok = pfb_csv::read_table3(o.centres_path, p.num_cells, (double)p.Nx, R, x, y, z, &err);
+            }
+            if (!read_ok) {
+                std::fprintf(stderr, "[3d] %s\n", err.c_str());
+                return 1;
+            }
+        } else if (o.geometry == kSlab) {
             x.resize((size_t)p.num_cells);
             y.resize((size_t)p.num_cells);
             if (pfb_palmieri_centres(p.num_cells, (double)p.Nx, R, p.seed, x.data(), y.data()) != PFB_OK) {

@@ -71,3 +71,23 @@ def test_append_refuses_another_run(tmp_path):
             "--out", tmp_path / "traj.txt")
     r = subprocess.run([str(EXE), *map(str, args)], capture_output=True, text=True, timeout=300)
     assert r.returncode != 0 and "does not match" in r.stderr
+
+
+@pytest.mark.skipif(not REF.exists(), reason="reference CLI not built")
+def test_initial_centres_table_same_run(tmp_path):
+    """A validated x,y centre table: both programs start from it and write the
+    same trajectory header (its hash) and rows."""
+    import pfb200
+    L = pfb200.domain_side_for(8, 12, 0.03)
+    c = L / 2
+    pts = [(c, c), (20.5, 30.0), (100.0, 40.0), (150.25, 200.0), (30.0, 150.0), (260.0, 260.0),
+           (200.0, 100.0), (80.0, 250.0)]
+    table = tmp_path / "c.csv"
+    table.write_text("global_id,x,y\n" + "".join(f"{i},{x!r},{y!r}\n" for i, (x, y) in enumerate(pts)))
+    ours, theirs = tmp_path / "ours", tmp_path / "theirs"
+    run(EXE, *ARGS, "--t-end", 0.2, "--initial-centres", table, "--out", ours / "traj.txt")
+    run(REF, *ARGS, "--t-end", 0.2, "--initial-centres", table, "--out", theirs / "traj.txt")
+    ha, ra = rows(ours / "traj.txt")
+    hb, rb = rows(theirs / "traj.txt")
+    assert ha == hb
+    same_rows(ra, rb)

@@ -109,3 +109,19 @@ def test_resume_continues_the_sampling_grid(tmp_path):
     run(EXE, "-c", d / "checkpoint.pf3d", "--t-end", 0.08, "--out", d / "traj.txt")
     _, r2 = rows(d / "traj.txt")
     np.testing.assert_allclose(np.unique(r2[:, 0]), [0.0, 0.02, 0.04, 0.05, 0.06, 0.08])
+
+
+@pytest.mark.skipif(not REF.exists(), reason="reference CLI not built")
+def test_initial_centres_table_same_run(tmp_path):
+    """A periodic x,y,z centre table (side 49 for N=3, R=4, rho=0.007): both
+    programs start from it and write the same header (its hash) and rows."""
+    table = tmp_path / "c.csv"
+    table.write_text("global_id,x,y,z\n0,24.5,24.5,24.5\n1,5.5,6.25,7\n2,40,40.5,10\n")
+    ours, theirs = tmp_path / "ours", tmp_path / "theirs"
+    args = (*ARGS, "--rho", 0.007, "--t-end", 0.04, "--initial-centres", table)
+    run(EXE, *args, "--out", ours / "traj.txt")
+    run(REF, *args, "--out", theirs / "traj.txt")
+    ha, ra = rows(ours / "traj.txt")
+    hb, rb = rows(theirs / "traj.txt")
+    assert ha == hb
+    same_rows(ra, rb)
