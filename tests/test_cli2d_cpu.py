@@ -44,7 +44,7 @@ def test_help_lists_the_reference_options():
     (("--boundary-compression", "zstd"), 2),
     (("--boundary-out", "b.bin", "--boundary-interval", 5, "--bench", 10), 2),
     (("--boundary-out", "b.bin", "--boundary-interval", 5, "--out", "b.bin"), 2),
-    (("--initial-centres", "c.csv"), 2),
+    (("--initial-centres", ""), 2),
 ])
 def test_bad_options_exit_2(args, code):
     assert run(*args).returncode == code
