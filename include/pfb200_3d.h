@@ -269,6 +269,11 @@ void pfb3d_initial_polarity(int64_t global_id, uint64_t stream, int planar, doub
 /* Lognormal active speed from the VALO domain (rng.cuh:65-78). */
 double pfb3d_initial_active_speed(int64_t global_id, uint64_t seed, double median,
                                   double sigma);
+/* Soft identities (reference include/pf3d/initializer.hpp:17-95,
+ * soft_id_membership): out[i] = 1 for the round(fraction n) ids a
+ * Philox-driven Fisher-Yates shuffle of 0..n-1 puts first (domain "SFT3",
+ * bounded draws by rejection), 0 otherwise. Independent of placement. */
+int pfb3d_soft_membership(int n, double fraction, uint64_t seed, uint8_t* out);
 /* Tumble draw of step `step` (rng.cuh:80-150): returns 1 on an event and
  * writes the new polarity, else 0. */
 int pfb3d_tumble(uint64_t step, int64_t global_id, uint64_t stream, double probability,
@@ -301,6 +306,10 @@ typedef struct pfb_params3d {
     uint64_t seed;
     uint64_t polarity_seed;
     int full_moment_every;
+    /* soft cells (reference gamma_cancer / cancer_fraction): round(
+     * soft_fraction N) identities drawn without replacement take gamma_soft */
+    double gamma_soft;
+    double soft_fraction;
 } pfb_params3d;
 
 typedef struct pfb_sim3d pfb_sim3d;

@@ -115,6 +115,8 @@ def rclib() -> C.CDLL:
         L.ref3d_cpu_table_hash.argtypes = [I, F, F, F]
         L.ref3d_cpu_table_hash.restype = C.c_uint64
         U = C.POINTER(C.c_uint64)
+        L.ref_soft_membership.argtypes = [I, D, C.c_uint64, P]
+        L.ref_soft_membership.restype = I
         L.ref_read_table2.argtypes = [C.c_char_p, I, D, D, F, F, U]
         L.ref_read_table2.restype = I
         L.ref_read_relaxed2.argtypes = [C.c_char_p, I, D, I, F, F]

@@ -148,6 +148,17 @@ uint64_t ref3d_cpu_table_hash(int n, const float* x, const float* y, const float
     return pf3d::centre_table_fnv1a64(pf3d::ordered_global_ids((std::size_t)n), a, b, c);
 }
 
+// The reference's soft identities (include/pf3d/initializer.hpp:81-95).
+int ref_soft_membership(int n, double fraction, uint64_t seed, uint8_t* out) {
+    try {
+        const std::vector<std::uint8_t> m = pf3d::soft_id_membership(n, fraction, seed);
+        std::memcpy(out, m.data(), m.size());
+        return 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
 // The reference's --initial-centres readers: 0 and the table's hash (and
 // its centres) when accepted, -1 when refused.
 int ref_read_table2(const char* path, int n, double side, double radius, float* x, float* y,

@@ -457,8 +457,8 @@ int pfb_ckpt3d_params_from(const pfb_params3d* p, int brick, pfb_ckpt3d_params* 
     out->t_end = 100.0;
     out->lambda = p->lambda;
     out->gamma_normal = p->gamma;
-    out->gamma_soft = p->gamma;
-    out->soft_fraction = 0.0;
+    out->gamma_soft = p->gamma_soft > 0.0 ? p->gamma_soft : p->gamma;
+    out->soft_fraction = p->soft_fraction;
     out->kappa = p->kappa;
     out->target_radius = p->target_radius;
     out->mu = p->mu;
@@ -494,8 +494,6 @@ int pfb_ckpt3d_params_from(const pfb_params3d* p, int brick, pfb_ckpt3d_params* 
 int pfb_ckpt3d_params_to(const pfb_ckpt3d_params* r, int num_cells, pfb_params3d* out) {
     clear_error();
     if (!r || !out || num_cells <= 0) return set_error(PFB_E_ARG, "params_to: bad argument");
-    if (r->soft_fraction > 0.0 && r->gamma_soft != r->gamma_normal)
-        return set_error(PFB_E_CONFIG, "PF3D record with a soft fraction: the 3D driver runs one gamma");
     std::memset(out, 0, sizeof(*out));
     out->Nx = (int)r->Nx;
     out->Ny = (int)r->Ny;
@@ -512,6 +510,8 @@ int pfb_ckpt3d_params_to(const pfb_ckpt3d_params* r, int num_cells, pfb_params3d
     out->tau = r->tau;
     out->v_A = r->v_A;
     out->gamma = r->gamma_normal;
+    out->gamma_soft = r->gamma_soft;
+    out->soft_fraction = r->soft_fraction;
     out->v_A_sigma = r->v_A_sigma;
     out->aging_time = r->aging_time;
     out->wall_kappa = r->wall_kappa;

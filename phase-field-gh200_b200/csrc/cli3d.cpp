@@ -13,8 +13,9 @@
 // frames on the grid of --boundary-interval and a closing frame after the
 // final checkpoint. --initial-centres reads the reference's centre tables
 // (periodic x,y,z; relaxed x,y for the slab and the one-layer channel;
-// channel x,y,z). Not part of this build (exit status 2 with a message):
-// soft cells (--cancer-fraction > 0), --strict,
+// channel x,y,z). Soft cells (--cancer-fraction, --gamma-cancer) take
+// their identities from the reference's Philox shuffle. Not part of this
+// build (exit status 2 with a message): --strict,
 // the memory modes, scratch slots, peer device and shard overrides. The
 // trajectory header and checkpoints state this build's measurement grouping
 // (4 CTAs per base cell, one-CTA promoted policy).
@@ -406,7 +407,7 @@ void usage() {
         "  geometry: --geometry periodic|slab|channel, --slab-height, --channel-height,\n"
         "            --wall-kappa, --wall-width, --wall-padding\n"
         "  model:    --N --radius --rho --lambda --kappa --mu --xi --tau --v-A --v-A-sigma\n"
-        "            --gamma --gamma-cancer --cancer-fraction (0 only) --dt --aging-time\n"
+        "            --gamma --gamma-cancer --cancer-fraction --dt --aging-time\n"
         "            --seed --polarity-seed --full-moment --verify-every\n"
         "  run:      --t-end --brick-edge --device --bench --print-interval --initial-centres CSV\n"
         "  output:   --out --trajectory-samples --trajectory-interval\n"
@@ -575,10 +576,6 @@ int parse(int argc, char** argv, Options* o) {
             return 2;
         }
     }
-    if (o->soft_fraction != 0.0) {
-        std::fprintf(stderr, "[3d] soft cells (--cancer-fraction > 0) are not part of this build\n");
-        return 2;
-    }
     if (o->bnd_given && (o->bnd_path.empty() || o->bnd_interval <= 0)) {
         std::fprintf(stderr, "[3d] boundary output requires --boundary-out and --boundary-interval\n");
         return 2;
@@ -691,11 +688,8 @@ int main(int argc, char** argv) {
             std::fprintf(stderr, "[3d] %s\n", pfb_last_error());
             return 1;
         }
-        if (rec.soft_fraction != 0.0) {
-            std::fprintf(stderr, "[3d] soft cells are not part of this build\n");
-            return 2;
-        }
         hash = rec.initialization_hash;
+        o.soft_fraction = rec.soft_fraction;
         o.rho = rec.volume_fraction;
         o.gamma_soft = rec.gamma_soft;
         o.verify_every = rec.verify_every;
@@ -713,6 +707,8 @@ int main(int argc, char** argv) {
     } else {
         if (!resolve_geometry(&o)) return 2;
         p.B = (int)o.brick;
+        p.gamma_soft = o.gamma_soft;
+        p.soft_fraction = o.soft_fraction;
         const double R = p.target_radius;
         std::vector<float> x, y, z;
         std::string err;

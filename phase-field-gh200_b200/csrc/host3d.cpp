@@ -2,7 +2,10 @@
 // per-cell Philox draws (reference include/pf3d/reference.hpp:601-745,
 // include/pf3d/params.cuh:112-166, include/pf3d/rng.cuh:35-150).
 #include <cmath>
+#include <cstdint>
 #include <limits>
+#include <utility>
+#include <vector>
 
 #include "pfb3d_common.cuh"
 #include "pfb_internal.h"
@@ -83,6 +86,34 @@ void pfb3d_initial_polarity(int64_t gid, uint64_t stream, int planar, double* ou
 
 double pfb3d_initial_active_speed(int64_t gid, uint64_t seed, double median, double sigma) {
     return pfb::p3::initial_speed3(gid, seed, median, sigma);
+}
+
+int pfb3d_soft_membership(int n, double fraction, uint64_t seed, uint8_t* out) {
+    if (n < 1 || !out || !std::isfinite(fraction) || fraction < 0.0 || fraction > 1.0)
+        return pfb::set_error(PFB_E_ARG, "invalid soft-cell selection parameters");
+    constexpr uint32_t kDomainSoft = 0x33544653u;  // "SFT3"
+    const int count = (int)std::llround(fraction * (double)n);
+    std::vector<int> ids((size_t)n);
+    for (int i = 0; i < n; ++i) ids[(size_t)i] = i;
+    for (int i = 0; i < count; ++i) {
+        // uniform in [0, n - i): reject words below 2^64 mod bound
+        const uint64_t bound = (uint64_t)(n - i);
+        const uint64_t threshold = (0ull - bound) % bound;
+        uint64_t pick = 0;
+        for (uint32_t attempt = 0;; ++attempt) {
+            const pfb::Words4 r = pfb::p3::draw3((uint64_t)i, kDomainSoft, attempt, seed);
+            const uint64_t word = ((uint64_t)r.w[0] << 32) | r.w[1];
+            if (word >= threshold) {
+                pick = word % bound;
+                break;
+            }
+            if (attempt == 0xFFFFFFFFu) return pfb::set_error(PFB_E_STATE, "soft-cell draw did not converge");
+        }
+        std::swap(ids[(size_t)i], ids[(size_t)i + (size_t)pick]);
+    }
+    for (int i = 0; i < n; ++i) out[i] = 0;
+    for (int i = 0; i < count; ++i) out[ids[(size_t)i]] = 1;
+    return PFB_OK;
 }
 
 int pfb3d_tumble(uint64_t step, int64_t gid, uint64_t stream, double p, int planar, double* out3) {

@@ -10,6 +10,7 @@
 // them and measures once without a tumble (src/pf3d/sim.cu:1100-1180).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -149,7 +150,11 @@ int validate3(const pfb_params3d& p) {
     if (!(p.dt > 0.0) || !(p.lambda > 0.0) || !(p.target_radius > 0.0) || !(p.xi > 0.0) ||
         !(p.tau > 0.0) || p.kappa < 0.0 || p.mu < 0.0 || p.v_A < 0.0 || !(p.gamma > 0.0))
         return set_error(PFB_E_ARG, "invalid model parameters");
-    if (p.dt * p.gamma * (256.0 / 30.0) >= 1.0)
+    if (!(p.soft_fraction >= 0.0 && p.soft_fraction <= 1.0) ||
+        (p.soft_fraction > 0.0 && !(p.gamma_soft > 0.0)))
+        return set_error(PFB_E_ARG, "soft fraction must lie in [0, 1] with a positive gamma_soft");
+    const double gmax = p.soft_fraction > 0.0 ? std::max(p.gamma, p.gamma_soft) : p.gamma;
+    if (p.dt * gmax * (256.0 / 30.0) >= 1.0)
         return set_error(PFB_E_ARG, "explicit-Euler Laplacian stability bound is violated");
     return PFB_OK;
 }
@@ -308,7 +313,9 @@ int create_impl(pfb_sim3d* s, const pfb_params3d* pp, const pfb_vec3* centres, i
     PFB3_RC(alloc_impl(s, pp, device));
     const pfb_params3d& p = s->p;
 
-    // per-cell records (reference src/pf3d/sim.cu:1100-1130), soft fraction 0
+    // per-cell records (reference src/pf3d/sim.cu:1100-1130)
+    std::vector<uint8_t> soft((size_t)s->N, 0);
+    if (p.soft_fraction > 0.0) PFB3_RC(pfb3d_soft_membership(s->N, p.soft_fraction, p.seed, soft.data()));
     std::vector<pfb_cell3d> cells((size_t)s->N);
     std::vector<pfb_vec3> ctr((size_t)s->N);
     const bool slab = substrate_slab(p.boundary_flags);
@@ -316,7 +323,7 @@ int create_impl(pfb_sim3d* s, const pfb_params3d* pp, const pfb_vec3* centres, i
         pfb_cell3d c;
         std::memset(&c, 0, sizeof(c));
         c.global_id = i;
-        c.gamma = (float)p.gamma;
+        c.gamma = (float)(soft[(size_t)i] ? p.gamma_soft : p.gamma);
         c.v_A = (float)initial_speed3(i, p.seed, p.v_A, p.v_A_sigma);
         c.R_tgt = (float)p.target_radius;
         const Dir3 d = initial_polarity3(i, polarity_stream(p), slab);

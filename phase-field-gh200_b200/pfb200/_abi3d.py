@@ -131,6 +131,7 @@ class Params3D(C.Structure):
         ("aging_time", C.c_double), ("wall_kappa", C.c_double), ("wall_width", C.c_double),
         ("channel_height", C.c_int), ("channel_padding", C.c_int),
         ("seed", C.c_uint64), ("polarity_seed", C.c_uint64), ("full_moment_every", C.c_int),
+        ("gamma_soft", C.c_double), ("soft_fraction", C.c_double),
     ]
 
 
@@ -158,6 +159,7 @@ _abi._SIGS.update({
     "pfb3d_automatic_brick_edge": (I, [C.c_double, C.c_double]),
     "pfb3d_initial_polarity": (None, [C.c_int64, C.c_uint64, I, C.POINTER(C.c_double)]),
     "pfb3d_initial_active_speed": (C.c_double, [C.c_int64, C.c_uint64, C.c_double, C.c_double]),
+    "pfb3d_soft_membership": (I, [I, C.c_double, C.c_uint64, C.c_void_p]),
     "pfb3d_tumble": (I, [C.c_uint64, C.c_int64, C.c_uint64, C.c_double, I,
                          C.POINTER(C.c_double)]),
     "pfb_sim3d_create": (P, [C.POINTER(Params3D), P, I]),

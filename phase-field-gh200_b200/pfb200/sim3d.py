@@ -47,6 +47,8 @@ class SimParams3D:
     seed: int = 1234
     polarity_seed: int = 0
     full_moment_every: int = 100
+    gamma_soft: float = 0.35     # soft cells' stiffness (reference gamma_cancer)
+    soft_fraction: float = 0.0   # share of soft identities (reference cancer_fraction)
 
     def to_c(self) -> Params3D:
         p = Params3D()

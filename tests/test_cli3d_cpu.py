@@ -81,7 +81,7 @@ def test_help():
     (("--geometry", "channel", "--radius", 8, "--channel-height", 10), "one-diameter minimum"),
     (("--geometry", "channel", "--lambda", 3, "--wall-padding", 5), "smaller than the minimum"),
     (("--geometry", "slab", "--radius", 8, "--lambda", 3, "--slab-height", 3), "must exceed"),
-    (("--cancer-fraction", 0.25), "soft cells"),
+    (("--cancer-fraction", 1.5), "--cancer-fraction expects"),
     (("--strict",), "unknown option"),
     (("--boundary-out", "x", "--boundary-interval", 2, "--memory-mode", "auto"), "unknown option"),
     (("--trajectory-interval", 0), "--trajectory-interval expects"),
@@ -144,3 +144,19 @@ def test_channel_placement_hash():
     x, y, z = pl.channel3d(c["N"], float(side), H, c["radius"], c["seed"])
     assert np.all((z >= c["radius"]) & (z <= H - c["radius"]))
     assert printed_hash("channel") == pl.table_hash(x, y, z)
+
+
+@pytest.mark.skipif(not (ROOT / "oracle" / "_ref" / "libref3d_cpu.so").exists(),
+                    reason="reference host build absent")
+@pytest.mark.parametrize("n,fraction,seed", [(3, 0.34, 11), (10, 0.5, 1234), (288, 0.1, 7),
+                                             (97, 1.0, 3), (50, 0.0, 5), (1, 0.6, 9)])
+def test_soft_identities_match_reference(n, fraction, seed):
+    import ctypes as C
+    import oracle3d as o3
+    from pfb200._abi import lib
+    theirs = np.zeros(n, np.uint8)
+    ours = np.zeros(n, np.uint8)
+    assert o3.rclib().ref_soft_membership(n, fraction, seed, theirs.ctypes.data) == 0
+    assert lib().pfb3d_soft_membership(n, fraction, seed, ours.ctypes.data) == 0
+    np.testing.assert_array_equal(ours, theirs)
+    assert ours.sum() == round(fraction * n)

@@ -125,3 +125,27 @@ def test_initial_centres_table_same_run(tmp_path):
     hb, rb = rows(theirs / "traj.txt")
     assert ha == hb
     same_rows(ra, rb)
+
+
+@pytest.mark.skipif(not REF.exists(), reason="reference CLI not built")
+def test_soft_cells_same_run(tmp_path):
+    """One soft cell of three (gamma 0.5): the same header (gamma_soft,
+    soft_fraction), the same per-cell gamma column and rows, and identical
+    checkpoint records; each continues the other's run."""
+    ours, theirs = tmp_path / "ours", tmp_path / "theirs"
+    args = (*ARGS, "--rho", 0.007, "--t-end", 0.04, "--cancer-fraction", 0.34, "--gamma-cancer", 0.5)
+    run(EXE, *args, "--out", ours / "traj.txt", "--checkpoint-dir", ours)
+    run(REF, *args, "--out", theirs / "traj.txt", "--checkpoint-dir", theirs)
+    ha, ra = rows(ours / "traj.txt")
+    hb, rb = rows(theirs / "traj.txt")
+    assert ha == hb and "soft_fraction=" in ha[0]
+    np.testing.assert_array_equal(ra[:, 11], rb[:, 11])  # gamma per cell
+    assert sorted(set(ra[:, 11])) == [0.5, 1.0]
+    same_rows(ra, rb)
+    same_checkpoint(ours / "checkpoint.pf3d", theirs / "checkpoint.pf3d")
+    run(EXE, "-c", theirs / "checkpoint.pf3d", "--t-end", 0.06, "--out", theirs / "traj.txt")
+    run(REF, "-c", ours / "checkpoint.pf3d", "--t-end", 0.06, "--out", ours / "traj.txt")
+    ha, ra = rows(ours / "traj.txt")
+    hb, rb = rows(theirs / "traj.txt")
+    assert ha == hb
+    same_rows(ra, rb)
