@@ -395,6 +395,13 @@ int pfb_sim2d_velocity_capture(pfb_sim2d* s);
 long long pfb_sim2d_velocity_last_frame(const pfb_sim2d* s);
 int pfb_sim2d_velocity_close(pfb_sim2d* s);
 
+/* Invariant check of the current state (reference Sim::verify,
+ * src/sim.cu:817-850, the --strict cadence): *max_rel_V = max over cells of
+ * |V recomputed from phi - V of the record| / max(1e-12, |V|), *max_outside =
+ * max |phi| of a tile outside its class window, *max_S = the largest word of
+ * the current aggregate. binary32 pools only. */
+int pfb_sim2d_verify(pfb_sim2d* s, double* max_rel_V, float* max_outside, uint32_t* max_S);
+
 /* PFB boundary recorder (reference src/boundary.cu, common/boundary_format.h):
  * creates a NEW file at `path` and writes its 72-byte header (level 1/2,
  * the frame `interval` stored for readers). Each capture appends a frame of

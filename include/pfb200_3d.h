@@ -360,6 +360,16 @@ int pfb_sim3d_bench(pfb_sim3d* s, int warmup, int steps, double* ms);
  * wall profile. Hard-wall channel only. */
 int pfb_sim3d_measure_wall(pfb_sim3d* s);
 
+/* Invariant check (reference Sim3D::verify, src/pf3d/sim.cu:2078-2137, the
+ * --strict cadence): measures the current state, then per cell recomputes
+ * V from the in-domain voxels and counts support voxels (|phi| > 1e-5) on a
+ * brick face, outside the domain or on the slab's top plane.
+ * *max_rel_V = max |V recomputed - V of the record| / max(1, V recomputed),
+ * *edge_voxels = their total, *max_S = the largest aggregate word.
+ * Returns PFB_E_STATE for a non-finite sample. */
+int pfb_sim3d_verify(pfb_sim3d* s, double* max_rel_V, uint32_t* max_S,
+                     unsigned long long* edge_voxels);
+
 /* PFB3D boundary recorder (reference src/pf3d/boundary_output.cu, file
  * layout common/boundary_format_3d.h): creates a NEW file at `path` with its
  * 128-byte header. Each capture appends a frame of the current step: per

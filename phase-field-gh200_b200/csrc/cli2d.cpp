@@ -7,9 +7,10 @@
 // rolling / tagged / final checkpoints, the plain-text trajectory (--out),
 // the PFVMOM4 velocity-moment recorder (--velocity-moments; reference
 // src/velocity_output.cu), the PFB boundary recorder (--boundary-out;
-// src/boundary.cu), --bench. Not part of this build (they exit with status 2
-// and a message): the mobility map, --morton, --no-l2,
-// --strict and --self-test, velocity observation under --bench, and, on
+// src/boundary.cu), --strict (the reference's invariant report on the
+// verify cadence), --bench. Not part of this build (they exit with status 2
+// and a message): the mobility map, --morton, --no-l2 and --self-test,
+// velocity observation under --bench, and, on
 // resume, overrides of model parameters other than the output cadences and
 // t_end. zstd boundary compression is refused at open (no zstd here).
 #include <algorithm>
@@ -57,6 +58,7 @@ struct Options {
     long long bnd_interval = 0;
     bool bnd_compress = false;
     std::string centres_path;  // --initial-centres
+    bool strict = false;
 };
 
 constexpr double kPi = 3.14159265358979323846;
@@ -69,7 +71,7 @@ void usage() {
         "  --cancer-fraction <f> --phase-field-mobility <f> --dt <f> --t-end <f>\n"
         "  --seed <u64> --polarity-seed <u64> --full-moment <int> --verify-every <int>\n"
         "  --print-interval <int>  --initial-centres <csv>  -c|--checkpoint <path>\n"
-        "  --checkpoint-interval <n>\n"
+        "  --checkpoint-interval <n>  --strict\n"
         "  --save-interval <n>  --checkpoint-dir <path>  --no-final-checkpoint\n"
         "  --trajectory-samples <n>  --trajectory-interval <n>  --out <path>\n"
         "  --device <int>  --bench <steps>  --no-graph\n"
@@ -419,8 +421,10 @@ int parse(int argc, char** argv, Options* o) {
                 return 2;
             }
             o->centres_path = v;
-        } else if (a == "--phase-field-mobility-map" || a == "--morton" ||
-                   a == "--no-l2" || a == "--strict" || a == "--self-test") {
+        } else if (a == "--strict") {
+            o->strict = true;
+        } else if (a == "--phase-field-mobility-map" || a == "--morton" || a == "--no-l2" ||
+                   a == "--self-test") {
             std::fprintf(stderr, "[fatal] option '%s' is not part of this build\n", a.c_str());
             return 2;
         } else {
@@ -620,11 +624,14 @@ int main(int argc, char** argv) {
     constexpr long long kFatalPoll = 1000;
     long long next_poll = step + kFatalPoll;
     long long next_bnd = o.bnd_path.empty() ? total + 1 : step + o.bnd_interval;
+    // --strict: invariant report at multiples of verify_every (reference src/sim.cu:860-973)
+    long long next_verify = o.strict && o.verify_every > 0 ? next_boundary(step, o.verify_every) : total + 1;
     bool failed = false;
     uint32_t flags[PFB_FLAG_COUNT];
     while (step < total && !failed) {
         const long long stop =
-            std::min({total, (step / pi + 1) * pi, next_traj, next_ckpt, next_save, next_poll, next_bnd});
+            std::min({total, (step / pi + 1) * pi, next_traj, next_ckpt, next_save, next_poll, next_bnd,
+                      next_verify});
         if (pfb_sim2d_advance(s, stop - step) != PFB_OK) {
             std::fprintf(stderr, "[fatal] %s\n", pfb_last_error());
             failed = true;
@@ -671,6 +678,16 @@ int main(int argc, char** argv) {
             std::snprintf(name, sizeof(name), "/checkpoint_%08lld.bin", step);
             if (!save(dir + name)) failed = true;
             next_save = step + o.save_interval;
+        }
+        if (step >= next_verify) {
+            double mr = 0.0;
+            float mo = 0.0f;
+            uint32_t ms = 0;
+            if (pfb_sim2d_verify(s, &mr, &mo, &ms) == PFB_OK)
+                std::printf("  [verify] step %lld  max rel V error %.3e   max|phi| outside window %.3e   "
+                            "max S %.6f\n",
+                            step, mr, (double)mo, (double)ms * 7.45058059692382812e-09);
+            next_verify = step + o.verify_every;
         }
         if (g_stop) {
             std::printf("[signal] termination requested at step %lld\n", step);

@@ -15,7 +15,7 @@
 // (periodic x,y,z; relaxed x,y for the slab and the one-layer channel;
 // channel x,y,z). Soft cells (--cancer-fraction, --gamma-cancer) take
 // their identities from the reference's Philox shuffle. Not part of this
-// build (exit status 2 with a message): --strict,
+// build (exit status 2 with a message):
 // the memory modes, scratch slots, peer device and shard overrides. The
 // trajectory header and checkpoints state this build's measurement grouping
 // (4 CTAs per base cell, one-CTA promoted policy).
@@ -66,6 +66,7 @@ struct Options {
     int bnd_projection = PFB3D_PROJECTION_MAXIMUM;
     bool bnd_compress = false, bnd_given = false;
     std::string centres_path;  // --initial-centres
+    bool strict = false;
 };
 
 bool parse_real(const char* flag, const char* s, double lo, double hi, double* v) {
@@ -410,6 +411,7 @@ void usage() {
         "            --gamma --gamma-cancer --cancer-fraction --dt --aging-time\n"
         "            --seed --polarity-seed --full-moment --verify-every\n"
         "  run:      --t-end --brick-edge --device --bench --print-interval --initial-centres CSV\n"
+        "            --strict (invariants every --verify-every steps)\n"
         "  output:   --out --trajectory-samples --trajectory-interval\n"
         "  restart:  -c|--checkpoint FILE --checkpoint-interval --save-interval\n"
         "            --checkpoint-dir --no-final-checkpoint\n"
@@ -545,6 +547,8 @@ int parse(int argc, char** argv, Options* o) {
             }
         } else if (!std::strcmp(a, "--no-final-checkpoint")) {
             o->final_ckpt = false;
+        } else if (!std::strcmp(a, "--strict")) {
+            o->strict = true;
         } else if (!std::strcmp(a, "--initial-centres")) {
             const char* v = value();
             if (!v || !v[0]) return 2;
@@ -864,11 +868,15 @@ int main(int argc, char** argv) {
     long long next_save = ckpt_on ? after(step, o.save_interval) : kNever;
     long long next_print = after(step, o.print_interval);
     long long next_bnd = o.bnd_path.empty() ? kNever : grid_after(step, o.bnd_interval);
+    // --strict: invariants at multiples of verify_every (reference src/pf3d/sim.cu:2167-2214)
+    const long long verify_every = o.strict ? o.verify_every : 0;
+    long long next_verify = verify_every > 0 ? after(step, verify_every - step % verify_every) : kNever;
     constexpr long long kPollEvery = 256;
     uint32_t flags[PFB3D_FLAG_COUNT];
     while (ok && step < total && !g_stop) {
         const long long stop =
-            std::min({total, next_traj, next_ckpt, next_save, next_print, next_bnd, step + kPollEvery});
+            std::min({total, next_traj, next_ckpt, next_save, next_print, next_bnd, next_verify,
+                      step + kPollEvery});
         if (pfb_sim3d_advance(s, (int)(stop - step)) != PFB_OK || pfb_sim3d_get_flags(s, flags) != PFB_OK) {
             std::fprintf(stderr, "[3d] step failed: %s\n", pfb_last_error());
             ok = false;
@@ -891,6 +899,16 @@ int main(int argc, char** argv) {
             ok = write_frame(traj, s, p);
             last_frame = step;
             next_traj = after(next_traj, traj_every);
+        }
+        if (ok && step >= next_verify) {
+            double rel = 0.0;
+            uint32_t maxS = 0;
+            unsigned long long edges = 0;
+            if (pfb_sim3d_verify(s, &rel, &maxS, &edges) != PFB_OK || rel > 1.0e-12 || edges != 0) {
+                std::fprintf(stderr, "[3d] strict verification failed: relV %.3e, edge voxels %llu\n", rel, edges);
+                ok = false;
+            }
+            next_verify = after(next_verify, verify_every);
         }
         if (ok && step >= next_bnd) {
             if (pfb_sim3d_boundary_capture(s) != PFB_OK) {

@@ -470,6 +470,51 @@ int pfb_sim2d_boundary_close(pfb_sim2d* s) {
     return rc;
 }
 
+int pfb_sim2d_verify(pfb_sim2d* s, double* max_rel_V, float* max_outside, uint32_t* max_S) {
+    if (!s || !max_rel_V || !max_outside || !max_S) return set_error(PFB_E_ARG, "verify: null argument");
+    if (s->p.phi_storage != 0) return set_error(PFB_E_CONFIG, "verify needs binary32 phi pools");
+    PFB_CU(cudaSetDevice(s->device), "cudaSetDevice");
+    double* d_v = nullptr;
+    float* d_o = nullptr;
+    uint32_t* d_m = nullptr;
+    const size_t N = (size_t)s->N;
+    int rc = PFB_OK;
+    std::vector<double> v(N);
+    std::vector<float> o(N);
+    std::vector<pfb_cell2d> c(N);
+    if (cudaMalloc(&d_v, N * sizeof(double)) != cudaSuccess || cudaMalloc(&d_o, N * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&d_m, sizeof(uint32_t)) != cudaSuccess || cudaMemsetAsync(d_m, 0, 4, s->stream) != cudaSuccess) {
+        rc = set_error(PFB_E_CUDA, "verify: allocation failed");
+    } else {
+        const int pin = (int)(s->steps_done % 2), rot = (int)(s->steps_done % 3);
+        rc = verify_cells2d(s->d_phi[pin], s->d_cell, s->d_cls, s->N, d_v, d_o, s->stream);
+        if (!rc) rc = verify_S(s->d_S + (size_t)rot * s->s_words, s->s_words, d_m, s->stream);
+        if (!rc && (cudaMemcpyAsync(v.data(), d_v, N * sizeof(double), cudaMemcpyDeviceToHost, s->stream) !=
+                        cudaSuccess ||
+                    cudaMemcpyAsync(o.data(), d_o, N * sizeof(float), cudaMemcpyDeviceToHost, s->stream) !=
+                        cudaSuccess ||
+                    cudaMemcpyAsync(c.data(), s->d_cell, N * sizeof(pfb_cell2d), cudaMemcpyDeviceToHost,
+                                    s->stream) != cudaSuccess ||
+                    cudaMemcpyAsync(max_S, d_m, 4, cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
+                    cudaStreamSynchronize(s->stream) != cudaSuccess))
+            rc = set_error(PFB_E_CUDA, "verify: readback failed");
+    }
+    cudaFree(d_v);
+    cudaFree(d_o);
+    cudaFree(d_m);
+    if (rc) return rc;
+    double mr = 0.0;
+    float mo = 0.0f;
+    for (size_t i = 0; i < N; ++i) {
+        const double den = std::max(1e-12, std::fabs(c[i].V));
+        mr = std::max(mr, std::fabs(v[i] - c[i].V) / den);
+        mo = std::max(mo, o[i]);
+    }
+    *max_rel_V = mr;
+    *max_outside = mo;
+    return PFB_OK;
+}
+
 int pfb_sim2d_velocity_close(pfb_sim2d* s) {
     if (!s || !s->vel) return set_error(PFB_E_STATE, "no velocity recorder is open");
     const int rc = velocity2d_close(s->vel);

@@ -121,6 +121,76 @@ __global__ void __launch_bounds__(kWallThreads)
     }
 }
 
+// Invariant check of each cell (reference src/pf3d/kernels.cu verify_one_cell):
+// FP64 volume of the in-domain voxels, non-finite samples, and support
+// voxels (|phi| > eps) on a brick face, outside the domain or on the slab's
+// top plane. One CTA per cell.
+struct Verify3 {
+    double V;
+    unsigned int nonfinite, edge;
+};
+__global__ void __launch_bounds__(kWallThreads)
+    k_verify3d(const float* phi, const pfb_cell3d* cells, int B, int nz, int periodic, int slab,
+               Verify3* out) {
+    const int n = blockIdx.x;
+    const size_t words = (size_t)B * B * B, plane = (size_t)B * B;
+    const float* brick = phi + (size_t)n * words;
+    const int64_t oz = cells[n].origin_z;
+    double vol = 0.0;
+    unsigned bad = 0, edge = 0;
+    for (size_t q = threadIdx.x; q < words; q += kWallThreads) {
+        const float v = brick[q];
+        if (!isfinite(v)) {
+            ++bad;
+            continue;
+        }
+        const int z = (int)(q / plane);
+        const int64_t wz = oz + z;
+        const bool in = periodic || (wz >= 0 && wz < nz);
+        const bool support = fabsf(v) > kSupportEps3;
+        if (!in) {
+            edge += support ? 1u : 0u;
+            continue;
+        }
+        vol += (double)v * (double)v;
+        if (support) {
+            const int x = (int)(q % B), y = (int)((q / B) % B);
+            edge += (x == 0 || x == B - 1 || y == 0 || y == B - 1 || z == 0 || z == B - 1 ||
+                     (slab && wz == nz - 1))
+                        ? 1u
+                        : 0u;
+        }
+    }
+    __shared__ double sv[kWallThreads / 32];
+    __shared__ unsigned sb[kWallThreads / 32], se[kWallThreads / 32];
+    for (int d = 16; d; d >>= 1) vol += __shfl_down_sync(0xFFFFFFFFu, vol, d);
+    bad = __reduce_add_sync(0xFFFFFFFFu, bad);
+    edge = __reduce_add_sync(0xFFFFFFFFu, edge);
+    if ((threadIdx.x & 31) == 0) {
+        sv[threadIdx.x >> 5] = vol;
+        sb[threadIdx.x >> 5] = bad;
+        se[threadIdx.x >> 5] = edge;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        Verify3 r{0.0, 0u, 0u};
+        for (int w = 0; w < kWallThreads / 32; ++w) {
+            r.V += sv[w];
+            r.nonfinite += sb[w];
+            r.edge += se[w];
+        }
+        out[n] = r;
+    }
+}
+
+__global__ void k_max_u32(const uint32_t* a, size_t n, uint32_t* out) {
+    uint32_t m = 0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        m = max(m, a[i]);
+    m = __reduce_max_sync(0xFFFFFFFFu, m);
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
 double volume0(const pfb_params3d& p) {
     const double sphere = 4.0 * kPi * p.target_radius * p.target_radius * p.target_radius / 3.0;
     return substrate_slab(p.boundary_flags) ? 0.5 * sphere : sphere;
@@ -441,6 +511,48 @@ int pfb_sim3d_measure_wall(pfb_sim3d* s) {
                                                        s->p.channel_height, s->d_wall_psi);
     PFB3_CU(cudaGetLastError(), "wall diagnostics");
     PFB3_CU(cudaStreamSynchronize(s->stream), "wall diagnostics");
+    return PFB_OK;
+}
+
+int pfb_sim3d_verify(pfb_sim3d* s, double* max_rel_V, uint32_t* max_S,
+                     unsigned long long* edge_voxels) {
+    if (!s || !max_rel_V || !max_S || !edge_voxels) return set_error(PFB_E_ARG, "verify: null argument");
+    PFB3_RC(pfb_sim3d_measure_current(s));
+    const size_t N = (size_t)s->N;
+    Verify3* d_r = nullptr;
+    uint32_t* d_m = nullptr;
+    std::vector<Verify3> r(N);
+    std::vector<pfb_cell3d> c(N);
+    int rc = PFB_OK;
+    const bool periodic = !substrate_slab(s->p.boundary_flags) && !hard_wall_channel(s->p.boundary_flags);
+    if (cudaMalloc(&d_r, N * sizeof(Verify3)) != cudaSuccess || cudaMalloc(&d_m, sizeof(uint32_t)) != cudaSuccess ||
+        cudaMemsetAsync(d_m, 0, 4, s->stream) != cudaSuccess) {
+        rc = set_error(PFB_E_CUDA, "verify: allocation failed");
+    } else {
+        k_verify3d<<<s->N, kWallThreads, 0, s->stream>>>(s->d_phi[s->cur_phi], s->d_cells, s->B, s->p.Nz,
+                                                         periodic ? 1 : 0,
+                                                         substrate_slab(s->p.boundary_flags) ? 1 : 0, d_r);
+        k_max_u32<<<148, 256, 0, s->stream>>>(s->d_S[s->cur_S], s->s_words, d_m);
+        if (cudaGetLastError() != cudaSuccess ||
+            cudaMemcpyAsync(r.data(), d_r, N * sizeof(Verify3), cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
+            cudaMemcpyAsync(c.data(), s->d_cells, N * sizeof(pfb_cell3d), cudaMemcpyDeviceToHost, s->stream) !=
+                cudaSuccess ||
+            cudaMemcpyAsync(max_S, d_m, 4, cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
+            cudaStreamSynchronize(s->stream) != cudaSuccess)
+            rc = set_error(PFB_E_CUDA, "verify: kernels or readback failed");
+    }
+    cudaFree(d_r);
+    cudaFree(d_m);
+    if (rc) return rc;
+    double mr = 0.0;
+    unsigned long long edges = 0;
+    for (size_t i = 0; i < N; ++i) {
+        if (r[i].nonfinite) return set_error(PFB_E_STATE, "verify: non-finite sample in cell slot %zu", i);
+        mr = std::max(mr, std::fabs(r[i].V - c[i].V) / std::max(1.0, std::fabs(r[i].V)));
+        edges += r[i].edge;
+    }
+    *max_rel_V = mr;
+    *edge_voxels = edges;
     return PFB_OK;
 }
 

@@ -176,6 +176,7 @@ _SIGS = {
     "pfb_sim2d_velocity_capture": (I, [P]),
     "pfb_sim2d_velocity_last_frame": (C.c_longlong, [P]),
     "pfb_sim2d_velocity_close": (I, [P]),
+    "pfb_sim2d_verify": (I, [P, C.POINTER(C.c_double), C.POINTER(C.c_float), C.POINTER(C.c_uint32)]),
     "pfb_sim2d_boundary_open": (I, [P, C.c_char_p, C.c_longlong, I]),
     "pfb_sim2d_boundary_capture": (I, [P]),
     "pfb_sim2d_boundary_close": (I, [P]),

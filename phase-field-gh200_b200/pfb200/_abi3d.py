@@ -166,6 +166,8 @@ _abi._SIGS.update({
     "pfb_sim3d_create_from_state": (P, [C.POINTER(Params3D), P, P, C.c_longlong, I]),
     "pfb_sim3d_measure_current": (I, [P]),
     "pfb_sim3d_measure_wall": (I, [P]),
+    "pfb_sim3d_verify": (I, [P, C.POINTER(C.c_double), C.POINTER(C.c_uint32),
+                             C.POINTER(C.c_ulonglong)]),
     "pfb_sim3d_boundary_open": (I, [P, C.c_char_p, I, C.c_longlong, I]),
     "pfb_sim3d_boundary_capture": (I, [P]),
     "pfb_sim3d_boundary_close": (I, [P, I]),

@@ -244,6 +244,13 @@ class Sim2D:
     def velocity_close(self) -> None:
         check(lib().pfb_sim2d_velocity_close(self._h), "velocity_close")
 
+    def verify(self) -> tuple[float, float, int]:
+        """(max relative volume error, max |phi| outside the windows, max
+        aggregate word) of the current state."""
+        rel, out, smax = C.c_double(), C.c_float(), C.c_uint32()
+        check(lib().pfb_sim2d_verify(self._h, C.byref(rel), C.byref(out), C.byref(smax)), "verify")
+        return rel.value, out.value, smax.value
+
     def boundary_open(self, path, interval: int, compress: bool = False) -> None:
         """Start a PFB boundary recording in a new file (header only)."""
         check(lib().pfb_sim2d_boundary_open(self._h, str(path).encode(), interval,

@@ -180,6 +180,13 @@ class Sim3D:
         the reference does before output and checkpoints)."""
         check(lib().pfb_sim3d_measure_current(self._h), "measure_current")
 
+    def verify(self) -> tuple[float, int, int]:
+        """(max relative volume error, max aggregate word, support voxels on a
+        brick face or outside the domain) after measuring the current state."""
+        rel, smax, edges = C.c_double(), C.c_uint32(), C.c_ulonglong()
+        check(lib().pfb_sim3d_verify(self._h, C.byref(rel), C.byref(smax), C.byref(edges)), "verify")
+        return rel.value, smax.value, edges.value
+
     def measure_wall(self) -> None:
         """Channel wall diagnostics of the current field into the cell
         records (wall_overlap, outside_slit_volume)."""

@@ -91,3 +91,14 @@ def test_initial_centres_table_same_run(tmp_path):
     hb, rb = rows(theirs / "traj.txt")
     assert ha == hb
     same_rows(ra, rb)
+
+
+def test_strict_reports_invariants(tmp_path):
+    args = (*ARGS, "--t-end", 0.2, "--strict", "--verify-every", 5)
+    r = subprocess.run([str(EXE), *map(str, args)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    lines = [ln for ln in r.stdout.splitlines() if "[verify]" in ln]
+    assert len(lines) == 4  # steps 5, 10, 15, 20
+    for ln in lines:
+        rel = float(ln.split("max rel V error")[1].split()[0])
+        assert rel < 1e-12

@@ -82,7 +82,7 @@ def test_help():
     (("--geometry", "channel", "--lambda", 3, "--wall-padding", 5), "smaller than the minimum"),
     (("--geometry", "slab", "--radius", 8, "--lambda", 3, "--slab-height", 3), "must exceed"),
     (("--cancer-fraction", 1.5), "--cancer-fraction expects"),
-    (("--strict",), "unknown option"),
+    (("--memory-mode", "compact"), "unknown option"),
     (("--boundary-out", "x", "--boundary-interval", 2, "--memory-mode", "auto"), "unknown option"),
     (("--trajectory-interval", 0), "--trajectory-interval expects"),
     (("--seed", -4), "unsigned"),

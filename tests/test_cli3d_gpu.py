@@ -149,3 +149,15 @@ def test_soft_cells_same_run(tmp_path):
     hb, rb = rows(theirs / "traj.txt")
     assert ha == hb
     same_rows(ra, rb)
+
+
+@pytest.mark.parametrize("geometry,rho", GEOMETRIES)
+def test_strict_verification_passes(tmp_path, geometry, rho):
+    """--strict re-measures every 2 steps and requires the recorded volumes to
+    hold to 1e-12 and no support on a brick face; a healthy run exits 0, as
+    the reference's does."""
+    args = (*ARGS, "--geometry", geometry, "--rho", rho, "--t-end", 0.06, "--strict",
+            "--verify-every", 2)
+    run(EXE, *args)
+    if REF.exists():
+        run(REF, *args)
