@@ -8,12 +8,16 @@
 // the PFVMOM4 velocity-moment recorder (--velocity-moments; reference
 // src/velocity_output.cu), the PFB boundary recorder (--boundary-out;
 // src/boundary.cu), --strict (the reference's invariant report on the
-// verify cadence), --bench. Not part of this build (they exit with status 2
-// and a message): the mobility map, --morton, --no-l2 and --self-test,
+// verify cadence), the per-cell mobility map (--phase-field-mobility-map;
+// reference src/checkpoint.cu:663-820: uniform mobility then listed
+// overrides on a fresh start, listed overrides of the stored values on
+// resume), --bench. Not part of this build (they exit with status 2 and a
+// message): --morton, --no-l2 and --self-test,
 // velocity observation under --bench, and, on
 // resume, overrides of model parameters other than the output cadences and
 // t_end. zstd boundary compression is refused at open (no zstd here).
 #include <algorithm>
+#include <cctype>
 #include <cerrno>
 #include <cmath>
 #include <csignal>
@@ -23,6 +27,7 @@
 #include <cstring>
 #include <string>
 #include <sys/stat.h>
+#include <utility>
 #include <vector>
 
 #include "centres_csv.hpp"
@@ -59,7 +64,99 @@ struct Options {
     bool bnd_compress = false;
     std::string centres_path;  // --initial-centres
     bool strict = false;
+    std::string mobility_map;  // --phase-field-mobility-map
 };
+
+// Read a mobility map: one "global_id value" pair per line, blank lines and
+// '#' comments skipped; ids in int32, unique; values finite and positive as
+// binary32 (reference src/checkpoint.cu:663-728).
+bool read_mobility_map(const std::string& path, std::vector<std::pair<int32_t, float>>* out, std::string* err) {
+    out->clear();
+    std::FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) return *err = "cannot open " + path + ": " + std::strerror(errno), false;
+    char line[256];
+    int lineno = 0;
+    std::vector<int32_t> seen;
+    bool ok = true;
+    auto fail = [&](const char* what) {
+        *err = path + ":" + std::to_string(lineno) + ": " + what;
+        ok = false;
+    };
+    while (ok && std::fgets(line, sizeof(line), f)) {
+        ++lineno;
+        const size_t len = std::strlen(line);
+        if (len + 1 == sizeof(line) && line[len - 1] != '\n') {
+            fail("line exceeds 254 characters");
+            break;
+        }
+        const char* s = line;
+        while (*s && std::isspace((unsigned char)*s)) ++s;
+        if (*s == '\0' || *s == '#') continue;
+        char* end = nullptr;
+        errno = 0;
+        const long long id = std::strtoll(s, &end, 10);
+        if (end == s || !std::isspace((unsigned char)*end)) {
+            fail("malformed global id");
+            break;
+        }
+        if (errno == ERANGE || id < 0 || id > 2147483647LL) {
+            fail("global id out of the int32 range or negative");
+            break;
+        }
+        s = end;
+        while (*s && std::isspace((unsigned char)*s)) ++s;
+        const double v = std::strtod(s, &end);
+        if (end == s) {
+            fail("malformed mobility value");
+            break;
+        }
+        s = end;
+        while (*s && std::isspace((unsigned char)*s)) ++s;
+        if (*s != '\0') {
+            fail("trailing characters after the value");
+            break;
+        }
+        const float mv = (float)v;
+        if (!std::isfinite(v) || !std::isfinite(mv) || !(mv > 0.0f)) {
+            fail("mobility must be finite and positive as binary32");
+            break;
+        }
+        if (std::find(seen.begin(), seen.end(), (int32_t)id) != seen.end()) {
+            fail("duplicate global id");
+            break;
+        }
+        seen.push_back((int32_t)id);
+        out->emplace_back((int32_t)id, mv);
+    }
+    const bool read_error = std::ferror(f) != 0;
+    std::fclose(f);
+    if (!ok) return false;
+    if (read_error) return *err = "read error on " + path, false;
+    if (out->empty()) return *err = path + ": contains no 'global_id value' entries", false;
+    return true;
+}
+
+// Overlay the map on the system's cell records (every listed id must exist).
+bool apply_mobility_map(pfb_sim2d* s, const std::vector<std::pair<int32_t, float>>& map, std::string* err) {
+    const int N = pfb_sim2d_num_cells(s);
+    std::vector<pfb_cell2d> cells((size_t)N);
+    std::vector<float> phi((size_t)N * PFB_TILE_AREA);
+    if (pfb_sim2d_get_cells(s, cells.data()) != PFB_OK || pfb_sim2d_get_phi(s, phi.data()) != PFB_OK)
+        return *err = pfb_last_error(), false;
+    for (const auto& e : map) {
+        int hit = -1;
+        for (int i = 0; i < N; ++i)
+            if (cells[(size_t)i].global_id == e.first) hit = i;
+        if (hit < 0)
+            return *err = "map id " + std::to_string(e.first) + " does not exist among the " + std::to_string(N) +
+                          " simulated global cell ids",
+                   false;
+        cells[(size_t)hit].M_pf = e.second;
+    }
+    if (pfb_sim2d_set_state(s, cells.data(), phi.data(), pfb_sim2d_step(s)) != PFB_OK)
+        return *err = pfb_last_error(), false;
+    return true;
+}
 
 constexpr double kPi = 3.14159265358979323846;
 
@@ -423,8 +520,13 @@ int parse(int argc, char** argv, Options* o) {
             o->centres_path = v;
         } else if (a == "--strict") {
             o->strict = true;
-        } else if (a == "--phase-field-mobility-map" || a == "--morton" || a == "--no-l2" ||
-                   a == "--self-test") {
+        } else if (a == "--phase-field-mobility-map") {
+            if (!(v = val()) || !v[0]) {
+                std::fprintf(stderr, "[fatal] --phase-field-mobility-map requires a non-empty path\n");
+                return 2;
+            }
+            o->mobility_map = v;
+        } else if (a == "--morton" || a == "--no-l2" || a == "--self-test") {
             std::fprintf(stderr, "[fatal] option '%s' is not part of this build\n", a.c_str());
             return 2;
         } else {
@@ -466,6 +568,14 @@ int main(int argc, char** argv) {
         (!o.vel_path.empty() && o.vel_path == o.out_path)) {
         std::fprintf(stderr, "[fatal] output files must use distinct paths\n");
         return 2;
+    }
+    std::vector<std::pair<int32_t, float>> mobility;
+    if (!o.mobility_map.empty()) {
+        std::string err;
+        if (!read_mobility_map(o.mobility_map, &mobility, &err)) {
+            std::fprintf(stderr, "[fatal] phase-field mobility map: %s\n", err.c_str());
+            return 2;
+        }
     }
     pfb_params2d p = o.p;
     uint64_t hash = 0;
@@ -528,6 +638,14 @@ int main(int argc, char** argv) {
     if (!s) {
         std::fprintf(stderr, "[fatal] initialisation failed: %s\n", pfb_last_error());
         return 5;
+    }
+    if (!mobility.empty()) {
+        std::string err;
+        if (!apply_mobility_map(s, mobility, &err)) {
+            std::fprintf(stderr, "[fatal] phase-field mobility: %s\n", err.c_str());
+            pfb_sim2d_destroy(s);
+            return 5;
+        }
     }
     pfb_sim2d_set_graph(s, o.graph ? 1 : 0);
     const long long total = total_steps(o.t_end, p.dt);

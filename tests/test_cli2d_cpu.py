@@ -56,3 +56,28 @@ def test_resume_refuses_domain_and_model_overrides(tmp_path):
     assert run("-c", missing, "--kappa", 3).returncode == 2
     r = run("-c", missing)
     assert r.returncode == 8 and "cannot open" in r.stderr
+
+
+@pytest.mark.parametrize("text,ok", [
+    ("1 0.25\n3 1.0\n", True),
+    ("# comment\n\n  2\t0.75  \n", True),
+    ("x 0.5\n", False),           # malformed id
+    ("-1 0.5\n", False),          # negative id
+    ("1 0.5 extra\n", False),     # trailing characters
+    ("1 0\n", False),             # not positive
+    ("1 1e39\n", False),          # not finite as binary32
+    ("1 0.5\n1 0.6\n", False),    # duplicate id
+    ("# only a comment\n", False),
+    ("1\n", False),               # no value
+])
+def test_mobility_map_rules(tmp_path, text, ok):
+    """Map files the reference refuses exit with status 2 before any device
+    work; accepted ones get past reading (and then stop here, without a GPU,
+    at initialisation)."""
+    path = tmp_path / "m.txt"
+    path.write_text(text)
+    r = run("--N", 8, "--radius", 12, "--rho", 0.03, "--t-end", 0.01, "--phase-field-mobility-map", path)
+    if ok:
+        assert r.returncode != 2, r.stderr
+    else:
+        assert r.returncode == 2 and "mobility map" in r.stderr, r.stderr

@@ -102,3 +102,33 @@ def test_strict_reports_invariants(tmp_path):
     for ln in lines:
         rel = float(ln.split("max rel V error")[1].split()[0])
         assert rel < 1e-12
+
+
+@pytest.mark.skipif(not REF.exists(), reason="reference CLI not built")
+def test_mobility_map_same_run(tmp_path):
+    """Per-cell mobilities from a map: the same trajectory and bit-identical
+    checkpoints (fields and stored mobilities) as cell_gh200; on resume the
+    map overrides only its listed cells in both programs."""
+    m = tmp_path / "m.txt"
+    m.write_text("1 0.25\n3 1.0\n")
+    m2 = tmp_path / "m2.txt"
+    m2.write_text("5 0.125\n")
+    ours, theirs = tmp_path / "ours", tmp_path / "theirs"
+    for exe, d in ((EXE, ours), (REF, theirs)):
+        run(exe, *ARGS, "--t-end", 0.2, "--phase-field-mobility-map", m, "--out", d / "traj.txt",
+            "--checkpoint-dir", d)
+    ha, ra = rows(ours / "traj.txt")
+    hb, rb = rows(theirs / "traj.txt")
+    assert ha == hb
+    same_rows(ra, rb)
+    a, b = ck.read(ours / "checkpoint.bin"), ck.read(theirs / "checkpoint.bin")
+    np.testing.assert_array_equal(a.phi, b.phi)
+    np.testing.assert_array_equal(a.cells["M_pf"], b.cells["M_pf"])
+    assert sorted(set(a.cells["M_pf"])) == [0.25, 0.5, 1.0]
+    for exe, d in ((EXE, ours), (REF, theirs)):
+        run(exe, "-c", d / "checkpoint.bin", "--t-end", 0.3, "--phase-field-mobility-map", m2,
+            "--checkpoint-dir", d / "next")
+    a, b = ck.read(ours / "next" / "checkpoint.bin"), ck.read(theirs / "next" / "checkpoint.bin")
+    np.testing.assert_array_equal(a.phi, b.phi)
+    np.testing.assert_array_equal(a.cells["M_pf"], b.cells["M_pf"])
+    assert sorted(set(a.cells["M_pf"])) == [0.125, 0.25, 0.5, 1.0]
