@@ -346,6 +346,16 @@ void pfb_sim2d_destroy(pfb_sim2d* s);
 int pfb_sim2d_set_cluster(pfb_sim2d* s, int cluster);
 int pfb_sim2d_set_variant(pfb_sim2d* s, int variant);
 int pfb_sim2d_set_graph(pfb_sim2d* s, int use_graph);
+/* Cell visit order (reference src/main.cu:491-492 --morton, src/sim.cu:
+ * 284-296, 649-653). PFB_VISIT_MORTON orders the clusters by the Z-order
+ * index of each cell's centroid pixel, re-sorted on the device every sixth
+ * step; it changes no result. One CTA sorts the keys in shared memory, so
+ * N is limited (PFB_E_CONFIG above it; the order is then left unchanged).
+ * pfb_sim2d_visit_order copies the current order (N indices) to `out`. */
+#define PFB_VISIT_LAUNCH 0
+#define PFB_VISIT_MORTON 1
+int pfb_sim2d_set_visit_order(pfb_sim2d* s, int order);
+int pfb_sim2d_visit_order(pfb_sim2d* s, uint32_t* out);
 /* Advance `steps` steps on the simulator's stream (asynchronous). */
 int pfb_sim2d_advance(pfb_sim2d* s, long long steps);
 /* Wait for the simulator's stream. */

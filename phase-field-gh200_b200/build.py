@@ -37,7 +37,8 @@ COMMON = [
 SOURCES = ["step2d.cu", "init2d.cu", "sim2d.cu", "host2d.cpp", "measure3d.cu", "update3d.cu",
            "misc3d.cu", "sim3d.cu", "host3d.cpp", "conv2d_tc.cu",
            "relax2d.cu", "unet2d.cu", "ckpt2d.cpp",
-           "ckpt3d.cpp", "velocity2d.cu", "boundary2d.cu", "boundary3d.cu"]
+           "ckpt3d.cpp", "velocity2d.cu", "boundary2d.cu", "boundary3d.cu",
+           "order2d.cu"]
 # command-line programs over the C ABI, linked against the library
 CLI_SOURCES = {"pfb_cell": "cli2d.cpp", "pfb_cell_3d": "cli3d.cpp"}
 CXX = os.environ.get("CXX", "g++")

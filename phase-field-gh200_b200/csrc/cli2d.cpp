@@ -11,9 +11,10 @@
 // verify cadence), the per-cell mobility map (--phase-field-mobility-map;
 // reference src/checkpoint.cu:663-820: uniform mobility then listed
 // overrides on a fresh start, listed overrides of the stored values on
-// resume), --bench. Not part of this build (they exit with status 2 and a
-// message): --morton, --no-l2 and --self-test,
-// velocity observation under --bench, and, on
+// resume), --bench, --morton (the Morton visit order, re-sorted every sixth
+// step) and --no-l2 (accepted: this build sets no L2 persistence window for
+// S). Not part of this build (they exit with status 2 and a message):
+// --self-test, velocity observation under --bench, and, on
 // resume, overrides of model parameters other than the output cadences and
 // t_end. zstd boundary compression is refused at open (no zstd here).
 #include <algorithm>
@@ -64,6 +65,7 @@ struct Options {
     bool bnd_compress = false;
     std::string centres_path;  // --initial-centres
     bool strict = false;
+    bool morton = false;
     std::string mobility_map;  // --phase-field-mobility-map
 };
 
@@ -171,7 +173,7 @@ void usage() {
         "  --checkpoint-interval <n>  --strict\n"
         "  --save-interval <n>  --checkpoint-dir <path>  --no-final-checkpoint\n"
         "  --trajectory-samples <n>  --trajectory-interval <n>  --out <path>\n"
-        "  --device <int>  --bench <steps>  --no-graph\n"
+        "  --device <int>  --bench <steps>  --no-graph  --morton  --no-l2\n"
         "  --velocity-moments <path>  --velocity-spatial-stride <1..1000>\n"
         "  --velocity-dense-start <int>  --velocity-moments-reference\n"
         "  --boundary-out <path>  --boundary-interval <int>  --boundary-compression <none|zstd>\n");
@@ -526,7 +528,11 @@ int parse(int argc, char** argv, Options* o) {
                 return 2;
             }
             o->mobility_map = v;
-        } else if (a == "--morton" || a == "--no-l2" || a == "--self-test") {
+        } else if (a == "--morton") {
+            o->morton = true;
+        } else if (a == "--no-l2") {
+            // S is never pinned in an L2 persisting carve-out here
+        } else if (a == "--self-test") {
             std::fprintf(stderr, "[fatal] option '%s' is not part of this build\n", a.c_str());
             return 2;
         } else {
@@ -648,6 +654,18 @@ int main(int argc, char** argv) {
         }
     }
     pfb_sim2d_set_graph(s, o.graph ? 1 : 0);
+    if (o.morton) {
+        const int rc = pfb_sim2d_set_visit_order(s, PFB_VISIT_MORTON);
+        if (rc == PFB_E_CONFIG) {
+            std::fprintf(stderr, "[warn] %s. Falling back to launch order.\n", pfb_last_error());
+        } else if (rc) {
+            std::fprintf(stderr, "[fatal] visit order: %s\n", pfb_last_error());
+            pfb_sim2d_destroy(s);
+            return 5;
+        } else {
+            std::printf("  visit order: Morton, re-sorted every six steps\n");
+        }
+    }
     const long long total = total_steps(o.t_end, p.dt);
     if (total < pfb_sim2d_step(s)) {
         std::fprintf(stderr, "[fatal] t_end ends at step %lld, before the state's step %lld\n", total,

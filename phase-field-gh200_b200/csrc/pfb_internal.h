@@ -63,6 +63,12 @@ int boundary2d_capture(Boundary2D* b, const float* phi, const pfb_cell2d* cells,
 // Finish the file (end record) and free the recorder.
 int boundary2d_close(Boundary2D* b);
 
+// Morton visit order of the 2D cells (order2d.cu): the largest N one sorting
+// CTA holds, the shared-memory opt-in (outside stream capture), the sort.
+int visit_order2d_capacity();
+cudaError_t visit_order2d_prepare(int N);
+cudaError_t visit_order2d_launch(const pfb_cell2d* cell, uint32_t* perm, int N, int L, cudaStream_t stream);
+
 // PFB3D boundary recorder (boundary3d.cu); projection 1 basal, 2 maximum.
 struct Boundary3D;
 Boundary3D* boundary3d_open(const char* path, const pfb_params3d& p, int projection,

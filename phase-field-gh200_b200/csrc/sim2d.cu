@@ -57,6 +57,7 @@ struct pfb_sim2d {
     cudaGraphExec_t graph_exec = nullptr;
     Velocity2D* vel = nullptr;  // open PFVMOM4 recorder
     Boundary2D* bnd = nullptr;  // open PFB recorder
+    uint32_t* d_perm = nullptr;  // Morton visit order (null: launch order)
 
     ~pfb_sim2d() {
         if (vel) velocity2d_destroy(vel);
@@ -73,6 +74,7 @@ struct pfb_sim2d {
         cudaFree(d_step);
         cudaFree(d_flags);
         cudaFree(d_traj);
+        cudaFree(d_perm);
         cudaFree(d_cell_prev);
         cudaFree(b_phi);
         cudaFree(b_cell);
@@ -143,7 +145,7 @@ struct pfb_sim2d {
         a.S_cl = d_S + (size_t)((rs + 2) % 3) * s_words;
         a.cell = d_cell;
         a.cell_cls = d_cls;
-        a.perm = nullptr;
+        a.perm = d_perm;
         a.cursor_use = d_cursor + pin;
         a.cursor_clear = d_cursor + pout;
         a.step_rd = d_step + pin;
@@ -158,7 +160,15 @@ struct pfb_sim2d {
         return a;
     }
 
+    // Re-sort the visit order on the first slot of every six (reference
+    // src/sim.cu:649-653).
+    int sort_visit_order(int slot) {
+        if (d_perm && slot % 6 == 0) PFB_CU(visit_order2d_launch(d_cell, d_perm, N, L, stream), "visit order");
+        return PFB_OK;
+    }
+
     int launch_one(int slot) {
+        if (const int rc = sort_visit_order(slot)) return rc;
         const pfb_step_args2d a = args_for_slot(slot);
         return step2d_launch_storage(&a, cluster, variant, p.phi_storage, stream);
     }
@@ -200,6 +210,7 @@ struct pfb_sim2d {
 
     // One observed step while a velocity recorder is open.
     int launch_observed() {
+        if (const int rc = sort_visit_order((int)(steps_done % 6))) return rc;
         pfb_step_args2d a = args_for_slot((int)(steps_done % 6));
         int obs = PFB_VELOCITY_DISABLED;
         int rc = velocity2d_prepare(vel, &a, steps_done, stream, &obs);
@@ -624,6 +635,53 @@ int pfb_sim2d_set_graph(pfb_sim2d* s, int use_graph) {
     if (!s) return set_error(PFB_E_ARG, "null sim");
     s->use_graph = use_graph != 0;
     if (!s->use_graph) s->drop_graph();
+    return PFB_OK;
+}
+
+int pfb_sim2d_set_visit_order(pfb_sim2d* s, int order) {
+    if (!s) return set_error(PFB_E_ARG, "null sim");
+    if (order != PFB_VISIT_LAUNCH && order != PFB_VISIT_MORTON) return set_error(PFB_E_ARG, "unknown visit order");
+    PFB_CU(cudaSetDevice(s->device), "cudaSetDevice");
+    if (order == PFB_VISIT_LAUNCH) {
+        if (s->d_perm) {
+            s->drop_graph();
+            PFB_CU(cudaStreamSynchronize(s->stream), "sync");
+            cudaFree(s->d_perm);
+            s->d_perm = nullptr;
+        }
+        return PFB_OK;
+    }
+    if (s->d_perm) return PFB_OK;
+    const int cap = visit_order2d_capacity();
+    if (s->N > cap) {
+        size_t m = 1;
+        while (m < (size_t)s->N) m <<= 1;
+        return set_error(PFB_E_CONFIG,
+                         "Morton order needs %.1f KB of shared memory for N=%d; the sort holds at most %d cells",
+                         (double)(m * sizeof(unsigned long long)) / 1024.0, s->N, cap);
+    }
+    PFB_CU(visit_order2d_prepare(s->N), "visit order attribute");
+    PFB_CU(cudaMalloc(&s->d_perm, (size_t)s->N * sizeof(uint32_t)), "alloc visit order");
+    // sorted now, so that a start at any step finds a valid order
+    if (cudaError_t e = visit_order2d_launch(s->d_cell, s->d_perm, s->N, s->L, s->stream)) {
+        cudaFree(s->d_perm);
+        s->d_perm = nullptr;
+        PFB_CU(e, "visit order");
+    }
+    s->drop_graph();
+    return PFB_OK;
+}
+
+int pfb_sim2d_visit_order(pfb_sim2d* s, uint32_t* out) {
+    if (!s || !out) return set_error(PFB_E_ARG, "visit_order: bad argument");
+    if (!s->d_perm) {
+        for (int i = 0; i < s->N; ++i) out[i] = (uint32_t)i;
+        return PFB_OK;
+    }
+    PFB_CU(cudaSetDevice(s->device), "cudaSetDevice");
+    PFB_CU(cudaMemcpyAsync(out, s->d_perm, (size_t)s->N * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream),
+           "visit order copy");
+    PFB_CU(cudaStreamSynchronize(s->stream), "sync");
     return PFB_OK;
 }
 

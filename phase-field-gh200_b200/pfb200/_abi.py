@@ -158,6 +158,8 @@ _SIGS = {
     "pfb_sim2d_set_cluster": (I, [P, I]),
     "pfb_sim2d_set_graph": (I, [P, I]),
     "pfb_sim2d_set_variant": (I, [P, I]),
+    "pfb_sim2d_set_visit_order": (I, [P, I]),
+    "pfb_sim2d_visit_order": (I, [P, P]),
     "pfb_sim2d_advance": (I, [P, C.c_longlong]),
     "pfb_sim2d_sync": (I, [P]),
     "pfb_sim2d_step": (C.c_longlong, [P]),

@@ -162,6 +162,16 @@ class Sim2D:
     def set_cluster(self, k: int) -> None:
         check(lib().pfb_sim2d_set_cluster(self._h, k), "set_cluster")
 
+    def set_visit_order(self, morton: bool) -> None:
+        """Visit the cells in Morton order of their centroids, re-sorted every
+        sixth step (reference --morton); results do not change."""
+        check(lib().pfb_sim2d_set_visit_order(self._h, 1 if morton else 0), "set_visit_order")
+
+    def visit_order(self) -> np.ndarray:
+        out = np.zeros(self.params.num_cells, np.uint32)
+        check(lib().pfb_sim2d_visit_order(self._h, out.ctypes.data), "visit_order")
+        return out
+
     def advance(self, steps: int) -> None:
         check(lib().pfb_sim2d_advance(self._h, steps), "advance")
 
