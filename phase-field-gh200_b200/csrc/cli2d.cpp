@@ -13,8 +13,10 @@
 // overrides on a fresh start, listed overrides of the stored values on
 // resume), --bench, --morton (the Morton visit order, re-sorted every sixth
 // step) and --no-l2 (accepted: this build sets no L2 persistence window for
-// S). Not part of this build (they exit with status 2 and a message):
-// --self-test, velocity observation under --bench, and, on
+// S) and --self-test (host checks of this build's stencil, coefficients,
+// force sign, tumble draws and windows; exit status 4 when one fails). Not
+// part of this build (they exit with status 2 and a message): velocity
+// observation under --bench, and, on
 // resume, overrides of model parameters other than the output cadences and
 // t_end. zstd boundary compression is refused at open (no zstd here).
 #include <algorithm>
@@ -27,6 +29,9 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <vector>
+
+#include "pfb_common.cuh"
 #include <sys/stat.h>
 #include <utility>
 #include <vector>
@@ -66,6 +71,7 @@ struct Options {
     std::string centres_path;  // --initial-centres
     bool strict = false;
     bool morton = false;
+    bool self_test = false;
     std::string mobility_map;  // --phase-field-mobility-map
 };
 
@@ -533,8 +539,7 @@ int parse(int argc, char** argv, Options* o) {
         } else if (a == "--no-l2") {
             // S is never pinned in an L2 persisting carve-out here
         } else if (a == "--self-test") {
-            std::fprintf(stderr, "[fatal] option '%s' is not part of this build\n", a.c_str());
-            return 2;
+            o->self_test = true;
         } else {
             std::fprintf(stderr, "[fatal] unknown option '%s' (try --help)\n", a.c_str());
             return 2;
@@ -549,6 +554,95 @@ long long total_steps(double t_end, double dt) {
 }
 
 }  // namespace
+
+// --self-test (reference src/main.cu:144-321): host checks of the nine-point
+// stencil, the model coefficients the library derives, the sign of the
+// repulsive velocity between two overlapping disks, the tumble probability
+// and the uniformity of the Philox stream, and the class windows against the
+// interface width. Returns the number of failed checks.
+static int self_test(const pfb_params2d& p) {
+    std::printf("--- self-test checks ---\n");
+    int bad = 0;
+    auto mark = [&](bool ok) {
+        bad += ok ? 0 : 1;
+        return ok ? "PASS" : "FAIL";
+    };
+    {
+        const float lap = pfb::lap9(1, 0, 1, 1, 0, 1, 1, 0, 1);  // f = x^2 around x = 0
+        const float flat = pfb::lap9(1, 1, 1, 1, 1, 1, 1, 1, 1);
+        std::printf("  [%s] Laplacian stencil: lap(x^2) = %.9g (expected 2), lap(1) = %.9g\n",
+                    mark(lap == 2.0f && flat == 0.0f), lap, flat);
+    }
+    pfb_step_args2d a;
+    std::memset(&a, 0, sizeof(a));
+    pfb_fill_coefficients2d(&p, &a);
+    {
+        const double bulk = pfb::coeff_bulk(p.lambda), rep = pfb::coeff_interaction(p.kappa, p.lambda);
+        const double ratio = (double)a.rep_coeff / (double)a.mot_coeff;
+        const bool ok = std::fabs(rep - 2.0 * p.kappa * bulk) <= 1e-12 * rep &&
+                        std::fabs((double)a.rep_coeff - rep) <= 1e-6 * rep &&
+                        std::fabs(ratio - p.xi) <= 1e-6 * p.xi;
+        std::printf("  [%s] coefficients: 30/l^2 = %.9g  60k/l^2 = %.9g (library %.9g)  "
+                    "60k/(xi l^2) = %.9g  ratio = %.9g (want xi = %.9g)\n",
+                    mark(ok), bulk, rep, (double)a.rep_coeff, (double)a.mot_coeff, ratio, p.xi);
+    }
+    {
+        // cell n left of cell m: phi_n falls to the right inside their overlap,
+        // so the interaction integral, and n's velocity, point away from m
+        const int L = 192;
+        const double R = 20.0, k = pfb::iface_k(p.lambda);
+        std::vector<double> pn((size_t)L * L), pm((size_t)L * L);
+        for (int sep = 26; sep <= 38; sep += 4) {
+            const double xn = 0.5 * (L - sep), xm = 0.5 * (L + sep);
+            for (int y = 0; y < L; ++y)
+                for (int x = 0; x < L; ++x) {
+                    const double dy = y - 0.5 * L;
+                    pn[(size_t)y * L + x] = 0.5 * (1.0 - std::tanh(k * (std::hypot(x - xn, dy) - R)));
+                    pm[(size_t)y * L + x] = 0.5 * (1.0 - std::tanh(k * (std::hypot(x - xm, dy) - R)));
+                }
+            double Ix = 0.0;
+            for (int y = 0; y < L; ++y)
+                for (int x = 1; x < L - 1; ++x) {
+                    const size_t i = (size_t)y * L + x;
+                    Ix += pn[i] * 0.5 * (pn[i + 1] - pn[i - 1]) * pm[i] * pm[i];
+                }
+            std::printf("  [%s] repulsive sign at separation %d: Ix = %+.6e  vx = %+.6e (n moves away from m)\n",
+                        mark(Ix < 0.0), sep, Ix, (double)a.mot_coeff * Ix);
+        }
+    }
+    {
+        const double tau_eff = -p.dt / std::log1p(-a.p_tumble);
+        std::printf("  [%s] tumble probability %.9e per step -> tau_eff = %.6f (tau %.6f)\n",
+                    mark(std::fabs(tau_eff - p.tau) <= 1e-9 * p.tau), a.p_tumble, tau_eff, p.tau);
+        const double tau_s = 10.0, ps = -std::expm1(-p.dt / tau_s);
+        const long long trials = 5000000;
+        long long hits = 0;
+        for (long long i = 0; i < trials; ++i) {
+            const pfb::Words4 r = pfb::philox10((uint32_t)i, (uint32_t)(i >> 32), 7u, 0xA5A5A5A5u,
+                                                (uint32_t)p.seed, 0u);
+            hits += pfb::u53(r.w[0], r.w[1]) < ps;
+        }
+        const double ph = (double)hits / (double)trials, tau_m = -p.dt / std::log1p(-ph);
+        const double sigma = std::sqrt(ps * (1.0 - ps) / (double)trials) / ps;
+        std::printf("  [%s] Philox draws: %lld at p = %.6e, tau_eff = %.3f (want %.1f +- %.3f at 5 sigma)\n",
+                    mark(std::fabs(tau_m - tau_s) <= 5.0 * sigma * tau_s), trials, ps, tau_m, tau_s,
+                    5.0 * sigma * tau_s);
+    }
+    {
+        // a relaxed hexagon's circumradius plus the distance at which phi^2
+        // falls below half a Q5.27 quantum, plus one pixel, on each axis
+        const double k = pfb::iface_k(p.lambda), A0 = kPi * p.target_radius * p.target_radius;
+        const double need = std::sqrt(A0 / (1.5 * std::sqrt(3.0))) + std::log(2.0 / pfb::kQInvD) / (4.0 * k) + 1.0;
+        for (int c = 0; c < pfb::kNumClasses; ++c) {
+            const pfb::Window w = pfb::window_of(c);
+            const int half = std::min(w.wx, w.wy) / 2;
+            std::printf("  [%s] class %d window %d x %d: half-width %d, required %.2f\n",
+                        mark((double)half >= need), c, w.wx, w.wy, half, need);
+        }
+    }
+    std::printf("--- %s ---\n", bad ? "SELF-TEST FAILED" : "self-test passed");
+    return bad;
+}
 
 int main(int argc, char** argv) {
     Options o;
@@ -617,6 +711,7 @@ int main(int argc, char** argv) {
         if (!o.t_end_set) o.t_end = rec.t_end;
         if (!o.print_set) o.print_interval = rec.print_interval;
         if (!o.verify_set) o.verify_every = rec.verify_every;
+        if (o.self_test && self_test(p)) return 4;
         s = pfb_sim2d_create_from_checkpoint(o.ckpt_in.c_str(), o.device);
     } else {
         p.L = pfb_domain_side_for(p.num_cells, p.target_radius, o.rho);
@@ -639,6 +734,7 @@ int main(int argc, char** argv) {
         hash = table_fnv1a64(x, y);
         std::printf("  centres: %d, table hash %016llx\n", p.num_cells, (unsigned long long)hash);
         std::fflush(stdout);
+        if (o.self_test && self_test(p)) return 4;
         s = pfb_sim2d_create(&p, x.data(), y.data(), o.device);
     }
     if (!s) {

@@ -1,5 +1,6 @@
 """pfb_cell (the 2D command line) without a GPU: options, refusals and exit
 codes (reference src/main.cu:340-560)."""
+import re
 import subprocess
 from pathlib import Path
 
@@ -81,3 +82,32 @@ def test_mobility_map_rules(tmp_path, text, ok):
         assert r.returncode != 2, r.stderr
     else:
         assert r.returncode == 2 and "mobility map" in r.stderr, r.stderr
+
+
+SELF_TEST_ARGS = ("--self-test", "--N", 16, "--rho", 0.02, "--t-end", 0.01)
+
+
+def self_test_numbers(text):
+    """Ix of each separation and the Philox tau_eff printed by a self-test."""
+    ix = [float(v) for v in re.findall(r"repulsive sign at separation \d+: Ix = (\S+)", text)]
+    tau = re.search(r"Philox \w+: 5000000 (?:draws )?at p = \S+, tau_eff = (\S+)", text)
+    return ix, float(tau.group(1)) if tau else None
+
+
+def test_self_test_passes_and_matches_reference():
+    r = subprocess.run([str(EXE), *map(str, SELF_TEST_ARGS)], capture_output=True, text=True, timeout=120)
+    assert "--- self-test passed ---" in r.stdout and "[FAIL]" not in r.stdout, r.stdout
+    ix, tau = self_test_numbers(r.stdout)
+    assert len(ix) == 4 and all(v < 0 for v in ix) and tau is not None
+    ref = EXE.parents[3] / "oracle" / "_ref" / "cell_gh200"
+    if ref.exists():  # the reference prints its checks before it needs a device
+        t = subprocess.run([str(ref), *map(str, SELF_TEST_ARGS)], capture_output=True, text=True, timeout=120)
+        rix, rtau = self_test_numbers(t.stdout)
+        assert rix == ix and rtau == tau
+
+
+def test_self_test_failure_exits_4():
+    # windows too small for the interface of a radius-110 cell
+    r = subprocess.run([str(EXE), *map(str, SELF_TEST_ARGS), "--radius", "110"], capture_output=True,
+                       text=True, timeout=120)
+    assert r.returncode == 4 and "SELF-TEST FAILED" in r.stdout
