@@ -67,8 +67,8 @@ def whole_job_rate(sites_per_rank_step: int, steps: int, world: int, max_ms: flo
 
 
 def workload_params(seed: int):
-    import pfb200
-    return pfb200.SimParams2D(L=L_SIDE, num_cells=N_CELLS, target_radius=RADIUS, seed=seed)
+    from pfb200.sim2d import SimParams2D
+    return SimParams2D(L=L_SIDE, num_cells=N_CELLS, target_radius=RADIUS, seed=seed)
 
 
 def workload_centres(p):
@@ -77,8 +77,8 @@ def workload_centres(p):
 
 
 def sites_per_step(cells) -> int:
-    import pfb200
-    return int(sum(pfb200.CLASSES[0][0] * pfb200.CLASSES[0][1] for _ in range(len(cells))))
+    """Reference window of every cell: 144^2 sites per class-0 cell."""
+    return int(len(cells)) * 144 * 144
 
 
 def algorithmic_bytes(cells, L: int, phi_bytes: int = 4) -> int:
@@ -172,15 +172,27 @@ def read_ncu_traffic():
     return None
 
 
-def cpu_sample(cells, phi, p, steps: int, threads: int):
-    """Time the oracle's OpenMP restatement on a bounded sample of the same
-    workload; returns (site-cell updates/s, seconds, threads)."""
+def oracle_workload_state(seed: int):
+    """The c2 workload's initial state built by the oracle alone (placement,
+    fresh-start draws and tanh seeds restated from the reference's host code
+    and k_init_tiles), so the CPU legs load no library of this package."""
     sys.path.insert(0, str(REPO / "oracle"))
     import oracle2d
-    if threads <= 0:
-        threads = os.cpu_count() or 1
+    p = workload_params(seed)
+    cx, cy = oracle2d.palmieri_centres(p.num_cells, p.L, 2.0 * p.target_radius, p.seed)
+    cells, phi = oracle2d.init_state(p.to_c(), cx, cy, oracle2d.fresh_cells(p.to_c()))
+    return p, cells, phi
+
+
+def cpu_time_steps(p, cells, phi, warmup: int, steps: int):
+    """Time `steps` consecutive time steps of the whole workload on the
+    oracle's OpenMP restatement (all host threads), as one timed region after
+    `warmup` untimed steps; returns (site-cell updates/s, seconds, threads)."""
+    sys.path.insert(0, str(REPO / "oracle"))
+    import oracle2d
+    threads = os.cpu_count() or 1
     o = oracle2d.OracleSim(p.to_c(), cells, phi, step=0)
-    o.advance(1, threads)  # warm the caches and the thread pool
+    o.advance(max(1, warmup), threads)  # warms the caches and the thread pool
     t0 = time.perf_counter()
     o.advance(steps, threads)
     dt = time.perf_counter() - t0
@@ -188,50 +200,38 @@ def cpu_sample(cells, phi, p, steps: int, threads: int):
     return sites_per_step(cells) * steps / dt, dt, threads
 
 
+def c2_config(a, sites: int) -> dict:
+    """The workload description both arms print (identical by construction)."""
+    return {"workload": WORKLOAD, "L": L_SIDE, "cells": N_CELLS, "radius": RADIUS,
+            "sites_per_step": sites, "window": "reference class-0 window 144^2",
+            "l2": "inputs larger than L2: two 340 MB phi pools; per-step working set 85 MB "
+                  "phi read + 85 MB phi written + 3 x 16.8 MB aggregate slots; no flush "
+                  "between steps",
+            "parallelism": f"replicas x{a.gpus}"}
+
+
 def run_reference_arm(a):
     """Reference arm: the reference's update on the host cores. The reference
     has no CPU solver, so this is the OpenMP restatement of its update in
-    oracle/. Each bench step is one time step of a subset of the workload's
-    cells (same lattice), sized so the whole run stays within about a minute;
-    throughput is per site-cell, so the subset does not change the rate."""
+    oracle/ (pinned to the reference's own kernel and host code), over the
+    whole c2 workload: W untimed steps, then K steps timed as one region on
+    every host thread. The state comes from the oracle's own restatement of
+    the reference's initialiser; nothing of this package is loaded."""
     rank, world, _ = rank_env()
     if rank != 0:
         return 0
-    p = workload_params(1234)
-    cx, cy = workload_centres(p)
-    sys.path.insert(0, str(REPO / "oracle"))
-    import oracle2d
-    cells, phi = oracle2d.init_state(p.to_c(), cx, cy, _fresh_cells(p))
-    threads = os.cpu_count() or 1
-    full = oracle2d.OracleSim(p.to_c(), cells, phi, step=0)
-    t0 = time.perf_counter()
-    full.advance(1, threads)
-    t_full = time.perf_counter() - t0
-    full.close()
-    budget = float(os.environ.get("PFB_REF_BUDGET_S", "60"))
-    m = int(max(1, min(p.num_cells, p.num_cells * budget / (max(1, a.steps) * t_full))))
-    ps = workload_params(1234)
-    ps.num_cells = m
-    sub = oracle2d.OracleSim(ps.to_c(), cells[:m].copy(), phi[:m].copy(), step=0)
-    for _ in range(min(a.warmup, 3)):
-        sub.advance(1, threads)
-    times = []
-    for _ in range(a.steps):
-        t0 = time.perf_counter()
-        sub.advance(1, threads)
-        times.append(time.perf_counter() - t0)
-    sub.close()
-    tot = sum(times)
-    value = sites_per_step(cells[:m]) * a.steps / tot
-    sample = (f"one time step of {m} of the {p.num_cells} cells (same 2048^2 lattice) per "
-              f"bench step; a full step took {t_full:.2f} s on {threads} threads")
+    p, cells, phi = oracle_workload_state(1234)
+    value, secs, threads = cpu_time_steps(p, cells, phi, a.warmup, a.steps)
+    sites = sites_per_step(cells)
+    sample = (f"{a.steps} consecutive time steps of the whole workload after {max(1, a.warmup)} "
+              f"untimed ones ({secs:.2f} s on {threads} threads)")
     line = {
         "impl": "reference", "metric": "site-cell updates/s", "value": value,
         "unit": "site-cell updates/s", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
-        "ms_per_step": 1000.0 * tot / a.steps, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": 1000.0 * secs / a.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "L": L_SIDE, "cells": N_CELLS,
-                   "implementation": "CPU OpenMP restatement of the reference update (oracle/)"},
+        "config": c2_config(a, sites),
+        "implementation": "CPU OpenMP restatement of the reference update (oracle/)",
         "cpu_baseline": {"value": value, "unit": "site-cell updates/s", "cores": threads,
                          "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "site-cell updates/s", "h2d_bytes_per_step": 0,
@@ -239,22 +239,6 @@ def run_reference_arm(a):
     }
     print(json.dumps(line), flush=True)
     return 0
-
-
-def _fresh_cells(p):
-    import pfb200
-    from pfb200 import CELL_DTYPE
-    L = pfb200.lib()
-    cells = np.zeros(p.num_cells, CELL_DTYPE)
-    pstream = p.polarity_seed or p.seed
-    for i in range(p.num_cells):
-        cells[i]["global_id"] = i
-        cells[i]["gamma"] = p.gamma_normal
-        cells[i]["v_A"] = L.pfb_ic_v_A(i, p.seed, p.v_A, p.v_A_sigma)
-        cells[i]["M_pf"] = p.phase_field_mobility
-        cells[i]["R_tgt"] = p.target_radius
-        cells[i]["theta"] = L.pfb_ic_theta(i, pstream)
-    return cells
 
 
 # ---------------------------------------------------------------------------
@@ -628,7 +612,8 @@ def main():
                     help="ensemble workload: the first R of its 64 replicas (profiling cases)")
     ap.add_argument("--phi-storage", type=int, default=0, choices=[0, 1, 2],
                     help="2D phi pools: 0 binary32 (reference layout), 1 binary16, 2 bfloat16")
-    ap.add_argument("--cpu-steps", type=int, default=int(os.environ.get("PFB_CPU_STEPS", "6")))
+    ap.add_argument("--cpu-steps", type=int, default=int(os.environ.get("PFB_CPU_STEPS", "20")),
+                    help="time steps of the CPU baseline leg (one timed region)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "ce", "cs"],
                     help="c2: 2D 2048^2 / 1024 cells (default); c3: 3D 256^3 / 512 cells; "
@@ -745,10 +730,11 @@ def main():
         traffic = read_ncu_traffic() if a.phi_storage == 0 else None
         cpu = None
         if world == 1 and a.cpu_steps > 0:
-            v, dt, thr = cpu_sample(init_cells, init_phi, p, a.cpu_steps, 0)
+            v, dt, thr = cpu_time_steps(p, init_cells, init_phi, 1, a.cpu_steps)
             cpu = {"value": v, "unit": "site-cell updates/s", "cores": thr, "kind": "port",
-                   "sample": f"{a.cpu_steps} full time steps of the same workload "
-                             f"({dt:.1f} s) on the OpenMP restatement of the update"}
+                   "sample": f"{a.cpu_steps} consecutive time steps of the whole workload "
+                             f"after 1 untimed one ({dt:.2f} s on {thr} threads), the same "
+                             "measurement as --impl reference"}
         line = {
             "metric": "site-cell updates/s", "value": value, "unit": "site-cell updates/s",
             "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_step,
@@ -756,15 +742,11 @@ def main():
             "dtype": ("f32", "f32 arithmetic, f16 phi storage",
                       "f32 arithmetic, bf16 phi storage")[a.phi_storage],
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "L": L_SIDE, "cells": N_CELLS, "radius": RADIUS,
-                       "sites_per_step": sites, "window": "reference class-0 window 144^2",
-                       "cluster_ctas_per_cell": a.cluster, "kernel_variant": a.variant,
-                       "cuda_graph": not a.no_graph,
-                       "phi_storage": ("binary32", "binary16", "bfloat16")[a.phi_storage],
-                       "l2": "inputs larger than L2: two 340 MB phi pools; per-step working "
-                             "set 85 MB phi read + 85 MB phi written + 3 x 16.8 MB aggregate "
-                             "slots; no flush between steps",
-                       "parallelism": f"replicas x{world}"},
+            "config": c2_config(a, sites),
+            "implementation": {"cluster_ctas_per_cell": a.cluster, "kernel_variant": a.variant,
+                               "cuda_graph": not a.no_graph,
+                               "phi_storage": ("binary32", "binary16",
+                                               "bfloat16")[a.phi_storage]},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": "pfb::k_step2d<%d%s>" % (

@@ -76,6 +76,15 @@ def olib() -> C.CDLL:
         L.oracle_init_state2d.restype = None
         L.oracle_scatter_all2d.argtypes = [P, P, C.c_int, C.c_int, C.c_int, P, P]
         L.oracle_scatter_all2d.restype = None
+        L.oracle_palmieri_centres.argtypes = [C.c_int, C.c_double, C.c_double, C.c_ulonglong,
+                                              P, P]
+        L.oracle_palmieri_centres.restype = C.c_int
+        L.oracle_ic_theta.argtypes = [C.c_int32, C.c_ulonglong]
+        L.oracle_ic_theta.restype = C.c_float
+        L.oracle_ic_v_A.argtypes = [C.c_int32, C.c_ulonglong, C.c_double, C.c_double]
+        L.oracle_ic_v_A.restype = C.c_double
+        L.oracle_fresh_cells2d.argtypes = [C.POINTER(Params2D), P]
+        L.oracle_fresh_cells2d.restype = None
         _O = L
     return _O
 
@@ -99,6 +108,15 @@ def rlib() -> C.CDLL:
         L.ref2d_configure.restype = C.c_int
         L.ref2d_scatter_all.argtypes = [P, P, P, P, C.c_int, C.c_int, C.c_int, P, P]
         L.ref2d_scatter_all.restype = C.c_int
+        L.ref2d_ic_theta.argtypes = [C.c_int32, C.c_ulonglong]
+        L.ref2d_ic_theta.restype = C.c_float
+        L.ref2d_ic_v_A.argtypes = [C.c_int32, C.c_ulonglong, C.c_double, C.c_double]
+        L.ref2d_ic_v_A.restype = C.c_double
+        L.ref2d_init_tiles.argtypes = [P, P, P, P, C.c_int, C.c_int, P, P, C.c_float, C.c_float,
+                                       P]
+        L.ref2d_init_tiles.restype = C.c_int
+        L.ref2d_init_moments.argtypes = [P, P, P, C.c_int, P]
+        L.ref2d_init_moments.restype = C.c_int
         _R = L
     return _R
 
@@ -121,6 +139,23 @@ def coefficients(lam, kappa, xi, mu, target, f64: bool):
         out = (C.c_float * 6)()
         olib().oracle_coefficients_f32(lam, kappa, xi, mu, target, out)
     return list(out)
+
+
+def palmieri_centres(n: int, side: float, min_sep: float, seed: int):
+    """Sequential periodic placement (reference include/palmieri_initializer.hpp:66-103)."""
+    x = np.zeros(n, np.float32)
+    y = np.zeros(n, np.float32)
+    rc = olib().oracle_palmieri_centres(n, float(side), float(min_sep), seed, _p(x), _p(y))
+    if rc:
+        raise RuntimeError("oracle placement did not terminate")
+    return x, y
+
+
+def fresh_cells(params_c: Params2D) -> np.ndarray:
+    """Cell records of a fresh start (reference src/sim.cu:136-143, 324-340)."""
+    cells = np.zeros(params_c.num_cells, CELL_DTYPE)
+    olib().oracle_fresh_cells2d(C.byref(params_c), _p(cells))
+    return cells
 
 
 def init_state(params_c: Params2D, cx: np.ndarray, cy: np.ndarray, cells: np.ndarray):

@@ -25,7 +25,9 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
+#include <random>
 #include <vector>
 
 #ifdef _OPENMP
@@ -786,6 +788,75 @@ void oracle_scatter_all2d(const float* phi, const pfb_cell2d* cells, int N, int 
                 if (v * v > 4.0f) flags[PFB_FLAG_Q_CLAMP] |= 1u;
                 t += q;
             }
+    }
+}
+
+// ---- fresh-start draws (host code of the reference) -------------------------
+// Sequential periodic placement: cell 0 at the box centre, candidates from
+// std::mt19937_64 (top 53 bits times 2^-53), accepted centres rounded to
+// binary32 before later distance tests, minimum-image separation test
+// (include/palmieri_initializer.hpp:48-103). Returns 0, or -1 when the
+// placement does not terminate.
+int oracle_palmieri_centres(int n, double side, double min_sep, unsigned long long seed,
+                            float* x, float* y) {
+    if (n < 1 || !(side > 0.0) || !(min_sep > 0.0)) return -1;
+    std::mt19937_64 eng(seed);
+    auto image = [side](double d) { return d - side * std::floor(d / side + 0.5); };
+    x[0] = (float)(0.5 * side);
+    y[0] = (float)(0.5 * side);
+    int placed = 1;
+    for (unsigned long long tries = 0; placed < n; ++tries) {
+        if (tries >= 1000000000ull) return -1;
+        const double px = side * ((double)(eng() >> 11) * 0x1.0p-53);
+        const double py = side * ((double)(eng() >> 11) * 0x1.0p-53);
+        int j = 0;
+        for (; j < placed; ++j) {
+            const double dx = image(px - (double)x[j]), dy = image(py - (double)y[j]);
+            if (dx * dx + dy * dy < min_sep * min_sep) break;
+        }
+        if (j < placed) continue;
+        x[placed] = (float)px;
+        y[placed] = (float)py;
+        ++placed;
+    }
+    return 0;
+}
+
+// Initial polarity angle: Philox4x32-10 on (gid, 2, 0, 0) keyed by the
+// polarity stream, theta = (float)(2 pi u53(w0, w1)) (include/kernels.cuh:146-158).
+float oracle_ic_theta(int32_t gid, unsigned long long stream) {
+    uint32_t w[4];
+    philox((uint32_t)gid, 2u, 0u, 0u, (uint32_t)stream, (uint32_t)(stream >> 32), w);
+    return (float)(2.0 * kPi * u53(w[0], w[1]));
+}
+
+// Initial active speed: lognormal with median v_A from a Box-Muller normal on
+// Philox (gid, 3, 0, 0) keyed by the seed (include/kernels.cuh:160-172).
+double oracle_ic_v_A(int32_t gid, unsigned long long seed, double v_A, double sigma) {
+    if (!(sigma > 0.0)) return v_A;
+    uint32_t w[4];
+    philox((uint32_t)gid, 3u, 0u, 0u, (uint32_t)seed, (uint32_t)(seed >> 32), w);
+    const double u1 = std::max(1e-300, u53(w[0], w[1]));
+    const double u2 = u53(w[2], w[3]);
+    const double z = std::sqrt(-2.0 * std::log(u1)) * std::cos(2.0 * kPi * u2);
+    return v_A * std::exp(sigma * z);
+}
+
+// Cell records of a fresh start: ids, stiffness (the first round(f N) ids
+// soft), speed, mobility, target radius and angle (src/sim.cu:136-145, 324-340).
+void oracle_fresh_cells2d(const pfb_params2d* p, pfb_cell2d* cells) {
+    const int N = p->num_cells;
+    const int soft = (int)std::lround(p->cancer_fraction * N);
+    const unsigned long long stream = p->polarity_seed ? p->polarity_seed : p->seed;
+    std::memset(cells, 0, sizeof(pfb_cell2d) * (size_t)N);
+    for (int i = 0; i < N; ++i) {
+        pfb_cell2d& c = cells[i];
+        c.global_id = i;
+        c.gamma = (float)(i < soft ? p->gamma_cancer : p->gamma_normal);
+        c.v_A = (float)oracle_ic_v_A(i, p->seed, p->v_A, p->v_A_sigma);
+        c.M_pf = (float)p->phase_field_mobility;
+        c.R_tgt = (float)p->target_radius;
+        c.theta = oracle_ic_theta(i, stream);
     }
 }
 

@@ -6,7 +6,9 @@
 //
 // Binds (reference include/kernels.cuh:185-225):
 //   pf::configure_k_step_smem, pf::k_step_grid, pf::launch_step,
-//   pf::k_init_tiles, pf::k_init_moments, pf::k_scatter_all.
+//   pf::k_init_tiles, pf::k_init_moments, pf::k_scatter_all;
+// and the host-side fresh-start draws pf::ic_theta, pf::ic_v_A (:146-172),
+// which pin the oracle's restatement of them (no device needed).
 #include <cstdio>
 
 #include "kernels.cuh"
@@ -59,6 +61,12 @@ int ref2d_scatter_all(const float* phi, const void* cell, const uint8_t* cls, ui
     pf::k_scatter_all<<<N, 256, 0, static_cast<cudaStream_t>(stream)>>>(
         phi, static_cast<const pf::CellState*>(cell), cls, S, N, L, P, flags);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+float ref2d_ic_theta(int32_t gid, unsigned long long stream) { return pf::ic_theta(gid, stream); }
+
+double ref2d_ic_v_A(int32_t gid, unsigned long long seed, double v_A, double sigma) {
+    return pf::ic_v_A(gid, seed, v_A, sigma);
 }
 
 }  // extern "C"

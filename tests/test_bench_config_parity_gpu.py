@@ -1,0 +1,308 @@
+"""Parity at the configurations bench.py times, on a B200.
+
+2D, the bench workload (2048^2 lattice, 1024 cells of radius 12, centres
+from the sequential initialiser with minimum separation 2R, state built by
+the library's own initialiser exactly as bench.py builds it):
+
+* 101 steps of this library's step kernel (cluster of 2, the bench's launch)
+  and of the reference's own kernel (oracle/_ref/libref2d.so) on
+  byte-identical buffers. Step 99 is a full-moment step (perimeter pass).
+  phi pools bit-identical, aggregate slots exact, integer cell fields exact,
+  FP64 moments within 1e-9 relative (the sums are grouped differently),
+  flags identical.
+* one step against the binary32 CPU oracle: max |dphi| <= 2e-6 (the
+  reference's own GPU-vs-FP64 Euler bound), aggregate exact given the
+  stored field.
+* 20,000 steps (the configuration's run length) through the driver: no
+  fatal flag; the class histogram is reported.
+
+3D, the bench workloads with lambda = 7, R = 10 and B = 64 (the automatic
+brick edge at lambda = 7):
+
+* periodic 256^3 with 512 cells and the slab 256 x 256 x 128 with
+  187 cells (rho_A ~ 0.9): for three steps each, both implementations
+  measure the same state (moments within 1e-12 relative, integer fields and
+  shifts exact), then update the same measured records (phi and the
+  aggregate bit for bit). One of the steps carries a recentring shift on
+  every cell.
+* 1000 steps of the periodic geometry at 128^3 with 64 cells (the same
+  density and brick) through the whole step sequence of each
+  implementation: phi within 1e-5, origins and counters exact.
+* 100 steps against the binary64 CPU oracle at the same configuration:
+  the error of each observable (phi, V, centroid, velocity) is printed and
+  bounded.
+"""
+import ctypes as C
+import math
+
+import numpy as np
+import pytest
+
+import oracle2d
+import oracle3d
+import pfb200
+from helpers2d import DeviceState2D, s_from_phi
+from helpers3d import DeviceState3D
+
+pytestmark = pytest.mark.gpu
+needs_ref2 = pytest.mark.skipif(not oracle2d.ref_available(), reason="reference build absent")
+needs_ref3 = pytest.mark.skipif(not oracle3d.ref_available(), reason="reference build absent")
+
+PHI_TOL_1 = 2e-6
+MOMENT_RTOL_GPU = 1e-9
+MOMENT_RTOL_3D = 1e-12
+PHI_TOL_3D_1000 = 1e-5
+
+INT_FIELDS_2D = ("gx0", "gy0", "cls", "bb_lo_x", "bb_hi_x", "bb_lo_y", "bb_hi_y", "promote_ctr",
+                 "shift_ctr", "tumble_ctr", "global_id")
+
+
+# ---------------------------------------------------------------------------
+# 2D: 2048^2, 1024 cells
+# ---------------------------------------------------------------------------
+def c2_state():
+    """The bench workload's initial state, built by the library's initialiser."""
+    p = pfb200.SimParams2D(L=2048, num_cells=1024, target_radius=12.0, seed=1234)
+    cx, cy = pfb200.palmieri_centres(p.num_cells, p.L, 2.0 * p.target_radius, p.seed)
+    sim = pfb200.Sim2D(p, cx, cy)
+    cells, phi = sim.cells(), sim.phi()
+    sim.close()
+    return p, cells, phi
+
+
+@pytest.fixture(scope="module")
+def c2():
+    return c2_state()
+
+
+def launch_pfb2(a):
+    return pfb200.lib().pfb_step2d_launch_ex(C.byref(a), 2, 1, None)
+
+
+def launch_ref2(a):
+    return oracle2d.rlib().ref2d_launch_step(C.byref(a), oracle2d.rlib().ref2d_grid(0), None)
+
+
+def assert_cells_2d(a, b, moment_rtol):
+    for k in INT_FIELDS_2D:
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+    np.testing.assert_array_equal(a["theta"], b["theta"], err_msg="theta")
+    np.testing.assert_array_equal(a["phi_max"], b["phi_max"], err_msg="phi_max")
+    for k in ("V", "Cx", "Cy", "perim"):
+        np.testing.assert_allclose(a[k], b[k], rtol=moment_rtol, err_msg=k)
+    for k in ("vx", "vy"):
+        np.testing.assert_allclose(a[k], b[k], rtol=1e-6, atol=1e-12, err_msg=k)
+
+
+@needs_ref2
+def test_c2_101_steps_bit_identical_to_reference_kernel(c2):
+    p, cells, phi = c2
+    a = DeviceState2D(p, cells, phi, step=0)
+    b = DeviceState2D(p, cells, phi, step=0)
+    for n in range(1, 102):
+        a.step_with(launch_pfb2)
+        b.step_with(launch_ref2)
+        if n in (1, 100, 101):
+            ca, cb = a.get_cells(), b.get_cells()
+            assert_cells_2d(ca, cb, MOMENT_RTOL_GPU)
+            assert np.array_equal(a.get_phi(), b.get_phi()), f"phi differs after {n} steps"
+            np.testing.assert_array_equal(a.get_S(), b.get_S())
+            np.testing.assert_array_equal(a.get_flags(), b.get_flags())
+    ca = a.get_cells()
+    # the full-moment step (step index 99) wrote a perimeter into every cell
+    assert (ca["perim"] > 0).all()
+    assert not pfb200.fatal(a.get_flags())
+    np.testing.assert_array_equal(a.get_S()[:, :p.L], s_from_phi(a.get_phi(), ca, p.L)[:, :p.L])
+    print(f"C2 101 steps: bit-identical to the reference kernel; classes "
+          f"{np.bincount(ca['cls'], minlength=6).tolist()}, shifts {int(ca['shift_ctr'].sum())}, "
+          f"tumbles {int(ca['tumble_ctr'].sum())}")
+
+
+def test_c2_one_step_vs_f32_oracle(c2):
+    p, cells, phi = c2
+    a = DeviceState2D(p, cells, phi, step=0)
+    a.step_with(launch_pfb2)
+    ca, pa = a.get_cells(), a.get_phi()
+    o = oracle2d.OracleSim(p.to_c(), cells, phi, step=0)
+    o.advance(1)
+    oc, op = o.cells(), o.phi()
+    o.close()
+    for k in INT_FIELDS_2D:
+        np.testing.assert_array_equal(ca[k], oc[k], err_msg=k)
+    np.testing.assert_array_equal(ca["theta"], oc["theta"])
+    np.testing.assert_allclose(ca["V"], oc["V"], rtol=1e-7)
+    # same origins and classes: the tiles compare directly
+    d = float(np.max(np.abs(pa.astype(np.float64) - op)))
+    assert d <= PHI_TOL_1, d
+    np.testing.assert_array_equal(a.get_S()[:, :p.L], s_from_phi(pa, ca, p.L)[:, :p.L])
+    print(f"C2 one step vs the f32 oracle: max|dphi| = {d:.3e}")
+
+
+def test_c2_20000_steps_stay_valid(c2):
+    p, cells, phi = c2
+    sim = pfb200.Sim2D(p, cells=cells, phi=phi, step=0)
+    sim.advance(20000)
+    flags = sim.flags()
+    cs = sim.cells()
+    hist = np.bincount(cs["cls"], minlength=6).tolist()
+    sim.close()
+    assert not pfb200.fatal(flags), pfb200.flags_report(flags)
+    assert np.isfinite(cs["V"]).all() and (cs["V"] > 0).all()
+    print(f"C2 after 20000 steps: classes {hist}, flags {pfb200.flags_report(flags)}, "
+          f"V/A0 in [{cs['V'].min() / p.area0:.4f}, {cs['V'].max() / p.area0:.4f}]")
+
+
+# ---------------------------------------------------------------------------
+# 3D: lambda 7, R 10, B 64
+# ---------------------------------------------------------------------------
+def c3_params(geometry: str, N: int, side: int, Nz: int):
+    return pfb200.SimParams3D(Nx=side, Ny=side, Nz=Nz, geometry=geometry, num_cells=N,
+                              target_radius=10.0, lambda_=7.0, B=64, seed=1234)
+
+
+def c3_centres(p):
+    if p.geometry == "slab":
+        # rho_A ~ 0.9 cannot be packed at separation 2R; the dense reference
+        # runs use separation R
+        return pfb200.sequential_centres(p.num_cells, p.Nx, p.target_radius, p.seed,
+                                         planar_z=-0.5)
+    c = pfb200.sequential_centres(p.num_cells, p.Nx, 2.0 * p.target_radius, p.seed,
+                                  first_at_centre=True)
+    return c.astype(np.float32).astype(np.float64)
+
+
+def set_cells(s: DeviceState3D, cells: np.ndarray) -> None:
+    s.cells.copy_(s.torch.from_numpy(np.ascontiguousarray(cells).view(np.uint8).copy())
+                  .to(s.cells.device))
+
+
+EXACT_3D = ("origin_x", "origin_y", "origin_z", "pending_shift_x", "pending_shift_y",
+            "pending_shift_z", "bb_lo_x", "bb_hi_x", "bb_lo_y", "bb_hi_y", "bb_lo_z", "bb_hi_z",
+            "phi_max", "flags", "shift_ctr", "tumble_ctr")
+
+
+def assert_measure_3d(a, b):
+    for f in EXACT_3D:
+        np.testing.assert_array_equal(a[f], b[f], err_msg=f)
+    for f in ("V", "Cx", "Cy", "Cz", "surface"):
+        np.testing.assert_allclose(a[f], b[f], rtol=MOMENT_RTOL_3D, err_msg=f)
+    scale = max(np.max(np.abs(b[f])) for f in ("Ix", "Iy", "Iz")) + 1e-300
+    for f in ("Ix", "Iy", "Iz"):
+        assert np.max(np.abs(a[f] - b[f])) <= 1e-10 * scale, f
+
+
+def lockstep_3d(p, steps=3, forced_shift_step=1):
+    """Per step: both measure the same state; then both update from the
+    reference's measured records (identical update inputs)."""
+    c = c3_centres(p)
+    a = DeviceState3D(p, c, "pfb")
+    b = DeviceState3D(p, c, "ref")
+    np.testing.assert_array_equal(a.get_phi(0), b.get_phi(0))
+    np.testing.assert_array_equal(a.get_S(0), b.get_S(0))
+    assert_measure_3d(a.get_cells(), b.get_cells())
+    shifted = 0
+    for k in range(steps):
+        a.clone_from(b)
+        for s in (a, b):
+            s.accepted.copy_(s.cells)
+            m = s.measure_args(tumble=True, surface=(k == 0))
+            s._call("measure_cells_only", m)
+            s._call("apply_cell_motion", m)
+        ca, cb = a.get_cells(), b.get_cells()
+        assert_measure_3d(ca, cb)
+        for f in ("velocity_x", "velocity_y", "velocity_z", "polarity_x", "polarity_y",
+                  "polarity_z"):
+            np.testing.assert_allclose(ca[f], cb[f], rtol=1e-6, atol=1e-12, err_msg=f)
+        if k == forced_shift_step:
+            # a recentring shift on every cell (within the reference's clamp)
+            sx = 2 * (np.arange(p.num_cells) % 2) - 1
+            cb["pending_shift_x"], cb["pending_shift_y"] = sx, -sx
+            cb["pending_shift_z"] = 1 if p.geometry == "periodic" else 0
+        shifted += int(np.count_nonzero(cb["pending_shift_x"] | cb["pending_shift_y"]
+                                        | cb["pending_shift_z"]))
+        for s in (a, b):
+            set_cells(s, cb)
+            s.S[1 - s.cur].zero_()
+            u = s.update_args()
+            s.update(u)
+            s._call("repair_after_fatal", u)
+            s._call("finalize_origins", s.cells.data_ptr(), s.N, s.flags.data_ptr())
+            s._call("restore_cells_after_fatal", s.cells.data_ptr(), s.accepted.data_ptr(),
+                    s.N, s.flags.data_ptr(), *([None] if s.impl == "pfb" else []))
+            s._call("advance_step", s.step.data_ptr(), s.flags.data_ptr())
+            s.cur = 1 - s.cur
+            s.steps_done += 1
+        s.torch.cuda.synchronize()
+        assert np.array_equal(a.get_phi(), b.get_phi()), f"phi differs after update {k}"
+        np.testing.assert_array_equal(a.get_S(), b.get_S())
+        np.testing.assert_array_equal(a.get_flags(), b.get_flags())
+        ca, cb = a.get_cells(), b.get_cells()
+        for f in ("origin_x", "origin_y", "origin_z", "shift_ctr", "tumble_ctr", "flags"):
+            np.testing.assert_array_equal(ca[f], cb[f], err_msg=f)
+    assert shifted >= p.num_cells
+    assert int(a.get_flags().sum()) == 0
+    return a, b
+
+
+@needs_ref3
+def test_c3_periodic_256_lockstep_with_reference():
+    p = c3_params("periodic", 512, 256, 256)
+    assert p.brick() == 64
+    lockstep_3d(p)
+
+
+@needs_ref3
+def test_c3_slab_256x256x128_lockstep_with_reference():
+    N = int(0.9 * 256 * 256 / (math.pi * 100.0))
+    assert N == 187
+    p = c3_params("slab", N, 256, 128)
+    lockstep_3d(p)
+
+
+@needs_ref3
+@pytest.mark.slow
+def test_c3_periodic_1000_steps_vs_reference():
+    p = c3_params("periodic", 64, 128, 128)
+    c = c3_centres(p)
+    a = DeviceState3D(p, c, "pfb")
+    b = DeviceState3D(p, c, "ref")
+    worst = {}
+    for n in range(1, 1001):
+        a.step_once()
+        b.step_once()
+        if n in (1, 10, 100, 1000):
+            worst[n] = float(np.max(np.abs(a.get_phi() - b.get_phi())))
+            ca, cb = a.get_cells(), b.get_cells()
+            for f in ("origin_x", "origin_y", "origin_z", "shift_ctr", "tumble_ctr", "flags"):
+                np.testing.assert_array_equal(ca[f], cb[f], err_msg=f"{f} after {n} steps")
+            np.testing.assert_allclose(ca["V"], cb["V"], rtol=1e-7)
+    np.testing.assert_array_equal(a.get_flags(), b.get_flags())
+    assert int(a.get_flags().sum()) == 0
+    print("C3 (128^3, 64 cells, B=64) max|dphi| vs the reference after 1/10/100/1000 steps:",
+          worst, "shifts", int(a.get_cells()["shift_ctr"].sum()))
+    assert worst[1000] <= PHI_TOL_3D_1000
+
+
+@pytest.mark.slow
+def test_c3_periodic_errors_vs_fp64_oracle():
+    p = c3_params("periodic", 64, 128, 128)
+    c = c3_centres(p)
+    a = DeviceState3D(p, c, "pfb")
+    o64 = oracle3d.OracleState3D(p, a.layout, a.B, a.get_cells(), a.get_phi(), a.get_S(),
+                                 f64=True)
+    steps = 100
+    for _ in range(steps):
+        a.step_once()
+    assert o64.advance(steps) == [0] * steps
+    ca, co = a.get_cells(), o64.cells
+    for f in ("origin_x", "origin_y", "origin_z"):
+        np.testing.assert_array_equal(ca[f], co[f], err_msg=f)
+    e_phi = float(np.max(np.abs(a.get_phi().astype(np.float64) - o64.phi)))
+    e_V = float(np.max(np.abs(ca["V"] - co["V"]) / co["V"]))
+    cen = lambda x, k: x["C" + k] / x["V"]  # noqa: E731
+    e_C = max(float(np.max(np.abs(cen(ca, k) - cen(co, k)))) for k in "xyz")
+    vel = lambda x: np.stack([x["velocity_" + k] for k in "xyz"], 1).astype(np.float64)  # noqa: E731
+    e_v = float(np.max(np.abs(vel(ca) - vel(co)))) / p.v_A
+    print(f"C3 (128^3, 64 cells, B=64) after {steps} steps vs the FP64 oracle: "
+          f"max|dphi|={e_phi:.2e} max rel dV={e_V:.2e} max|dC|={e_C:.2e} max|dv|/v_A={e_v:.2e}")
+    assert e_phi <= 1e-4 and e_V <= 1e-5 and e_C <= 1e-4 and e_v <= 1e-3

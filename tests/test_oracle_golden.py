@@ -136,3 +136,40 @@ def test_q_of_encoding():
         want = int(np.rint(np.float64(F(sq * F(2**27)))))
         assert L.oracle_q_of(v) == want
         assert lib.pfb_q_of(v) == want
+
+
+# ---- fresh-start draws: the oracle against the reference's own host code ----
+@pytest.mark.skipif(not oracle2d.ref_available(), reason="reference build absent")
+def test_oracle_ic_draws_equal_reference():
+    r = oracle2d.rlib()
+    o = oracle2d.olib()
+    for gid in (0, 1, 7, 1023, 123456, 2**31 - 1):
+        for stream in (1234, 0xDEADBEEFCAFEF00D, 1):
+            assert o.oracle_ic_theta(gid, stream) == r.ref2d_ic_theta(gid, stream)
+            for sigma in (0.0, 0.3, 1.2):
+                assert o.oracle_ic_v_A(gid, stream, 0.01, sigma) == \
+                    r.ref2d_ic_v_A(gid, stream, 0.01, sigma)
+
+
+@pytest.mark.skipif(not __import__("oracle3d").ref_cpu_available(),
+                    reason="reference host build absent")
+@pytest.mark.parametrize("n,side,sep,seed", [(64, 512.0, 24.0, 1234), (1024, 2048.0, 24.0, 1234),
+                                             (187, 256.0, 10.0, 99)])
+def test_oracle_placement_equals_reference(n, side, sep, seed):
+    import ctypes as C
+    import oracle3d
+    x, y = oracle2d.palmieri_centres(n, side, sep, seed)
+    rx, ry = np.zeros(n, np.float32), np.zeros(n, np.float32)
+    fp = C.POINTER(C.c_float)
+    assert oracle3d.rclib().ref3d_cpu_palmieri2d(n, side, sep, seed, rx.ctypes.data_as(fp),
+                                                 ry.ctypes.data_as(fp)) == 0
+    np.testing.assert_array_equal(x, rx)
+    np.testing.assert_array_equal(y, ry)
+
+
+def test_oracle_fresh_cells_equal_library():
+    from helpers2d import fresh_cells, params
+    p = params(512, 64, R=12.0, seed=77, v_A_sigma=0.4, cancer_fraction=0.25)
+    a = oracle2d.fresh_cells(p.to_c())
+    b = fresh_cells(p)
+    assert a.tobytes() == b.tobytes()
