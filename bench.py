@@ -221,10 +221,11 @@ def run_reference_arm(a):
     if rank != 0:
         return 0
     p, cells, phi = oracle_workload_state(1234)
-    value, secs, threads = cpu_time_steps(p, cells, phi, a.warmup, a.steps)
+    warm = min(a.warmup, 5)
+    value, secs, threads = cpu_time_steps(p, cells, phi, warm, a.steps)
     sites = sites_per_step(cells)
-    sample = (f"{a.steps} consecutive time steps of the whole workload after {max(1, a.warmup)} "
-              f"untimed ones ({secs:.2f} s on {threads} threads)")
+    sample = (f"{a.steps} consecutive time steps of the whole workload after {warm} untimed "
+              f"ones ({secs:.2f} s on {threads} threads)")
     line = {
         "impl": "reference", "metric": "site-cell updates/s", "value": value,
         "unit": "site-cell updates/s", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
@@ -612,8 +613,8 @@ def main():
                     help="ensemble workload: the first R of its 64 replicas (profiling cases)")
     ap.add_argument("--phi-storage", type=int, default=0, choices=[0, 1, 2],
                     help="2D phi pools: 0 binary32 (reference layout), 1 binary16, 2 bfloat16")
-    ap.add_argument("--cpu-steps", type=int, default=int(os.environ.get("PFB_CPU_STEPS", "20")),
-                    help="time steps of the CPU baseline leg (one timed region)")
+    ap.add_argument("--cpu-steps", type=int, default=int(os.environ.get("PFB_CPU_STEPS", "40")),
+                    help="most time steps of the CPU baseline leg (one timed region)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "ce", "cs"],
                     help="c2: 2D 2048^2 / 1024 cells (default); c3: 3D 256^3 / 512 cells; "
@@ -730,11 +731,14 @@ def main():
         traffic = read_ncu_traffic() if a.phi_storage == 0 else None
         cpu = None
         if world == 1 and a.cpu_steps > 0:
-            v, dt, thr = cpu_time_steps(p, init_cells, init_phi, 1, a.cpu_steps)
+            # the procedure of --impl reference with this run's warm-up and step
+            # count, the steps capped to keep the default run short
+            cw, cs = min(a.warmup, 5), min(a.steps, a.cpu_steps)
+            v, dt, thr = cpu_time_steps(p, init_cells, init_phi, cw, cs)
             cpu = {"value": v, "unit": "site-cell updates/s", "cores": thr, "kind": "port",
-                   "sample": f"{a.cpu_steps} consecutive time steps of the whole workload "
-                             f"after 1 untimed one ({dt:.2f} s on {thr} threads), the same "
-                             "measurement as --impl reference"}
+                   "sample": f"{cs} consecutive time steps of the whole workload after {cw} "
+                             f"untimed ones ({dt:.2f} s on {thr} threads), the measurement "
+                             "of --impl reference"}
         line = {
             "metric": "site-cell updates/s", "value": value, "unit": "site-cell updates/s",
             "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_step,

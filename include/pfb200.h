@@ -252,9 +252,11 @@ int pfb_step2d_launch_observed(const pfb_step_args2d* args, int cluster, int obs
 int pfb_velocity_moments2d(const pfb_step_args2d* args, pfb_moment_accum2d* out,
                            double physical_dt, void* stream);
 
-/* Library status word kept in device memory: bit 0 is set when a CTA gave up
- * waiting for its staged band (a bounded wait that is never expected to run
- * out). `clear` != 0 resets it after reading. */
+/* Library status word kept in device memory: bit 0 is set when a CTA of the
+ * step gave up waiting for its staged band, bit 1 when a step cluster gave up
+ * waiting for a reduction, bit 2 when a set-up pass (initial moments,
+ * invariant check) gave up waiting for its cluster fold (bounded waits that
+ * are never expected to run out). `clear` != 0 resets it after reading. */
 int pfb_device_status(unsigned* out, int clear);
 
 /* ======================================================================

@@ -150,6 +150,13 @@ class OracleState3D:
         self.step = np.array([step], np.uint64)
         self.steps_done = 0
         self.wall = None if wall is None else np.ascontiguousarray(wall, dtype=np.float32)
+        if f64:
+            # the aggregate of the binary64 field: q(phi) of a widened binary32
+            # value can differ from the binary32 q by one unit, which the step
+            # would count as a negative S_other
+            self.S[...] = 0
+            olib().oracle3d_scatter(1, _p(self.phi), _p(self.cells), _p(self.S), _p(self.flags),
+                                    C.byref(self.L), len(self.cells), B)
 
     def advance(self, n: int = 1, threads: int = 0) -> list[int]:
         p = self.p

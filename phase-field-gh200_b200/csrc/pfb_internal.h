@@ -25,6 +25,7 @@ int step2d_smem_bytes(int cluster);
 int step2d_launch_batch(const pfb_step_args2d* d_args, const int* d_block_start, int R,
                         int total_blocks, int cluster, int storage, cudaStream_t stream);
 int step2d_read_status(unsigned* out, int clear);
+int init2d_read_status(unsigned* out, int clear);
 // variant: 0 = default, 1 = one thread-block cluster per cell
 int step2d_launch_variant(const pfb_step_args2d* a, int cluster, int variant,
                           cudaStream_t stream);

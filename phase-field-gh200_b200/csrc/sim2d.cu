@@ -567,7 +567,13 @@ int pfb_pack_traj2d(const pfb_cell2d* cell, const uint8_t* cls, pfb_traj_cell2d*
     return pack_traj2d(cell, cls, out, N, L, as_stream(stream));
 }
 
-int pfb_device_status(unsigned* out, int clear) { return step2d_read_status(out, clear); }
+int pfb_device_status(unsigned* out, int clear) {
+    unsigned a = 0, b = 0;
+    int rc = step2d_read_status(&a, clear);
+    if (!rc) rc = init2d_read_status(&b, clear);
+    if (out) *out = a | (b << 2);
+    return rc;
+}
 
 pfb_sim2d* pfb_sim2d_create(const pfb_params2d* p, const float* cx, const float* cy, int device) {
     clear_error();

@@ -28,126 +28,216 @@
 namespace pfb {
 namespace {
 
-constexpr int kObsThreads = 256;
-constexpr int kObsWarps = kObsThreads / 32;
 constexpr int kColumns = 26;        // PFVMOM4 columns per cell
 constexpr int kIntegralColumn = 9;  // q[0..11]
 constexpr int kSpatialCountColumn = 21;
 constexpr int kEndpointColumn = 22;
 
-__device__ __forceinline__ float tile_at(const float* tile, const Window& w, int x, int y) {
-    if ((unsigned)x >= (unsigned)w.wx || (unsigned)y >= (unsigned)w.wy) return 0.0f;
-    return tile[(w.ty0 + y) * kTilePitch + w.tx0 + x];
+// ---- the dense observer -------------------------------------------------------
+// One thread-block cluster of kObsBands CTAs per cell. CTA r walks tile rows
+// [72 r, 72 r + 72) as four-pixel chunks (288 threads: 4 rows x 72 chunks per
+// sweep); samples outside the cell's class window read as zero. Two passes:
+//   1. the interaction integral of phi^n, pushed by every CTA into every
+//      CTA's shared memory (st.async) and summed there in rank order, so all
+//      CTAs derive the same velocity;
+//   2. the eight centroid-moment channels, pushed into rank 0, which adds them
+//      in rank order and commits the rates times dt.
+constexpr int kObsBands = 4;
+constexpr int kObsThreads = 288;
+constexpr int kObsWarps = kObsThreads / 32;
+constexpr int kObsChunks = kTilePitch / 4;
+constexpr int kObsBandRows = kTilePitch / kObsBands;
+constexpr int kObsSweep = kObsThreads / kObsChunks;
+static_assert(kObsBandRows % kObsSweep == 0, "band walk");
+
+struct ObsShared {
+    uint64_t barF;  // kObsBands force partials (16 B each), every CTA
+    uint64_t barM;  // kObsBands channel partials (64 B each), rank 0
+    double wf[kObsWarps][2];
+    double wm[kObsWarps][8];
+    alignas(16) double rf[kObsBands][2];
+    alignas(16) double rm[kObsBands][8];
+    double vel[4];
+};
+
+// Three rows (y-1, y, y+1) of a four-pixel chunk with its left and right
+// neighbours, window-masked: v[r][k] is tile column 4c - 1 + k of row y - 1 + r.
+struct Chunk3 {
+    float v[3][6];
+};
+
+__device__ __forceinline__ Chunk3 load_chunk(const float* tile, const Window& w, int y, int c) {
+    Chunk3 q;
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        const int yy = y - 1 + r;
+        const bool row_in = (unsigned)(yy - w.ty0) < (unsigned)w.wy;
+        const float* row = tile + (size_t)yy * kTilePitch;
+        const float4 mid = row_in ? __ldg(reinterpret_cast<const float4*>(row) + c)
+                                  : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        const float m4[4] = {mid.x, mid.y, mid.z, mid.w};
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const int x = 4 * c - 1 + k;
+            const bool in = row_in && (unsigned)(x - w.tx0) < (unsigned)w.wx;
+            q.v[r][k] = !in ? 0.0f : (k >= 1 && k <= 4) ? m4[k - 1] : __ldg(row + x);
+        }
+    }
+    return q;
 }
 
-// S_other at window pixel (x, y); an aggregate below the cell's own share is
-// returned as NaN so that a frame built from it is refused.
-__device__ __forceinline__ float other_at(const pfb_step_args2d& A, const pfb_cell2d& c, int x,
-                                          int y, float p) {
-    const int gx = (c.gx0 + x) % A.L, gy = (c.gy0 + y) % A.L;
+// S_other at window pixel (a, b) of a cell holding p there; an aggregate below
+// the cell's own share reads as NaN, so that a frame built from it is refused.
+__device__ __forceinline__ float other_share(const pfb_step_args2d& A, const pfb_cell2d& c, int a,
+                                             int b, float p) {
+    const int gx = (c.gx0 + a) % A.L, gy = (c.gy0 + b) % A.L;
     const uint32_t all = A.S_rd[(size_t)gy * A.P + gx], self = q_encode(p);
     return all >= self ? (float)(all - self) * kQInv : __int_as_float(0x7fc00000);
 }
 
-// Block sum of NV doubles: warp shuffles, then ascending warps by thread 0;
-// the totals land in red[j][0].
+// Warp butterflies, then this CTA's warps in order, into lane 0 of warp 0.
 template <int NV>
-__device__ __forceinline__ void block_sum(double (&v)[NV], double (*red)[kObsWarps]) {
+__device__ __forceinline__ void cta_fold(double (&v)[NV], double (*slots)[NV]) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-    for (int j = 0; j < NV; ++j) {
-        const double s = dev::warp_sum_down(v[j]);
-        if (lane == 0) red[j][warp] = s;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
+    for (int j = 0; j < NV; ++j) v[j] = dev::warp_sum_down(v[j]);
+    if (lane == 0)
 #pragma unroll
-        for (int j = 0; j < NV; ++j) {
-            double s = 0.0;
-            for (int w = 0; w < kObsWarps; ++w) s += red[j][w];
-            red[j][0] = s;
-        }
-    }
+        for (int j = 0; j < NV; ++j) slots[warp][j] = v[j];
     __syncthreads();
+    if (warp == 0)
+#pragma unroll
+        for (int j = 0; j < NV; ++j)
+            v[j] = dev::ordered_lane_sum(lane < kObsWarps ? slots[lane][j] : 0.0, kObsWarps);
 }
 
-// One CTA per cell: the velocity the step would take (tumble included) and
-// the twelve centroid-moment channels of phi^n, each rate times dt added to
-// out[n] (reference src/velocity_moments.cu:47-123).
+// Adds the velocity the step would take (tumble included) and the twelve
+// centroid-moment channels of phi^n, each rate times dt, to out[n]
+// (the reference's dense observer, src/velocity_moments.cu:43-123).
 __global__ void __launch_bounds__(kObsThreads)
     k_observe2d(const __grid_constant__ pfb_step_args2d A, pfb_moment_accum2d* out, double dt) {
-    const int n = blockIdx.x, tid = threadIdx.x;
+    __shared__ ObsShared sh;
+    const int n = blockIdx.x / kObsBands;
+    const int rank = (int)dev::cluster_rank();
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) {
+        dev::mbar_init(&sh.barF, 1);
+        dev::mbar_init(&sh.barM, 1);
+        dev::mbar_arrive_expect_tx(&sh.barF, kObsBands * 16u);
+        if (rank == 0) dev::mbar_arrive_expect_tx(&sh.barM, kObsBands * 64u);
+    }
+    dev::cluster_arrive_relaxed();
     const pfb_cell2d& c = A.cell[n];
     const Window w = window_of(c.cls);
     const float* tile = A.phi_in + (size_t)n * kTileArea;
-    __shared__ double red[8][kObsWarps];
-    __shared__ double vel[4];
-    const int area = w.wx * w.wy;
+    const int ch = tid % kObsChunks;
+    const int y_lo = rank * kObsBandRows + tid / kObsChunks, y_hi = (rank + 1) * kObsBandRows;
 
+    // ---- pass 1: interaction integral (binary32 products, FP64 sums)
     double f[2] = {0.0, 0.0};
-    for (int k = tid; k < area; k += kObsThreads) {
-        const int x = k % w.wx, y = k / w.wx;
-        const float p = tile_at(tile, w, x, y);
-        const float gx = 0.5f * (tile_at(tile, w, x + 1, y) - tile_at(tile, w, x - 1, y));
-        const float gy = 0.5f * (tile_at(tile, w, x, y + 1) - tile_at(tile, w, x, y - 1));
-        const float so = other_at(A, c, x, y, p);
-        f[0] += (double)(p * gx * so);
-        f[1] += (double)(p * gy * so);
-    }
-    block_sum(f, red);
-    if (tid == 0) {
-        const unsigned long long step = *A.step_rd;
-        const Words4 r = philox10((uint32_t)(step & 0xFFFFFFFFull), (uint32_t)(step >> 32),
-                                  (uint32_t)c.global_id, kTumbleTag,
-                                  (uint32_t)(A.polarity_seed & 0xFFFFFFFFull),
-                                  (uint32_t)(A.polarity_seed >> 32));
-        float theta = c.theta;
-        if (u53(r.w[0], r.w[1]) < A.p_tumble) theta = (float)(2.0 * kPi * u53(r.w[2], r.w[3]));
-        float sn, co;
-        sincosf(theta, &sn, &co);
-        vel[0] = (double)c.v_A * (double)co;
-        vel[1] = (double)c.v_A * (double)sn;
-        vel[2] = (double)A.mot_coeff * red[0][0];
-        vel[3] = (double)A.mot_coeff * red[1][0];
-    }
-    __syncthreads();
-    const double cx = c.Cx / c.V, cy = c.Cy / c.V;
-    const double dw = (double)(A.bulk_scale * c.gamma);
-    const double vol = (double)(float)(A.vol_scale * (A.A0 - c.V));
-    const double mobility = (double)(c.M_pf / (float)kMobilityM0);
-    const double vx = (double)(float)(vel[0] + vel[2]);
-    const double vy = (double)(float)(vel[1] + vel[3]);
-    double m[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    for (int k = tid; k < area; k += kObsThreads) {
-        const int x = k % w.wx, y = k / w.wx;
-        const double p = tile_at(tile, w, x, y);
-        const double e = tile_at(tile, w, x + 1, y), ww = tile_at(tile, w, x - 1, y);
-        const double nn = tile_at(tile, w, x, y + 1), s = tile_at(tile, w, x, y - 1);
-        const double ne = tile_at(tile, w, x + 1, y + 1), nw = tile_at(tile, w, x - 1, y + 1);
-        const double se = tile_at(tile, w, x + 1, y - 1), sw = tile_at(tile, w, x - 1, y - 1);
-        const double lap = (4.0 * (nn + s + e + ww) + ne + nw + se + sw - 20.0 * p) / 6.0;
-        const double gx = 0.5 * (e - ww), gy = 0.5 * (nn - s);
-        const double so = (double)other_at(A, c, x, y, (float)p);
-        double src[4] = {(double)c.gamma * lap - dw * p * (1.0 - p) * (1.0 - 2.0 * p),
-                         -(double)A.rep_coeff * p * so, vol * p, -(vx * gx + vy * gy)};
-        // the mobility scales the passive terms, never advection
-        if (mobility != 1.0)
-            for (int j = 0; j < 3; ++j) src[j] *= mobility;
-        const double wx = 2.0 * ((double)x - cx) * p / c.V;
-        const double wy = 2.0 * ((double)y - cy) * p / c.V;
+    for (int y = y_lo; y < y_hi; y += kObsSweep) {
+        const int b = y - w.ty0;
+        if ((unsigned)b >= (unsigned)w.wy) continue;
+        const Chunk3 q = load_chunk(tile, w, y, ch);
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            m[2 * j] += wx * src[j];
-            m[2 * j + 1] += wy * src[j];
+        for (int k = 1; k <= 4; ++k) {
+            const int a = 4 * ch - 1 + k - w.tx0;
+            if ((unsigned)a >= (unsigned)w.wx) continue;
+            const float p = q.v[1][k];
+            const float gx = 0.5f * (q.v[1][k + 1] - q.v[1][k - 1]);
+            const float gy = 0.5f * (q.v[2][k] - q.v[0][k]);
+            const float so = other_share(A, c, a, b, p);
+            f[0] += (double)(p * gx * so);
+            f[1] += (double)(p * gy * so);
         }
     }
-    block_sum(m, red);
-    if (tid == 0) {
+    cta_fold(f, sh.wf);
+    dev::cluster_wait();  // every peer's barriers are initialised
+    if (warp == 0) {
+        if (lane < kObsBands)
+            dev::st_async_v2f64(dev::map_to_rank(dev::smem_addr(&sh.rf[rank][0]), lane), f[0],
+                                f[1], dev::map_to_rank(dev::smem_addr(&sh.barF), lane));
+        (void)dev::mbar_wait_bounded(&sh.barF, 0, 1u << 24);
+        const double Fx = dev::ordered_lane_sum(lane < kObsBands ? sh.rf[lane][0] : 0.0, kObsBands);
+        const double Fy = dev::ordered_lane_sum(lane < kObsBands ? sh.rf[lane][1] : 0.0, kObsBands);
+        if (lane == 0) {
+            const unsigned long long step = *A.step_rd;
+            const Words4 r = philox10((uint32_t)(step & 0xFFFFFFFFull), (uint32_t)(step >> 32),
+                                      (uint32_t)c.global_id, kTumbleTag,
+                                      (uint32_t)(A.polarity_seed & 0xFFFFFFFFull),
+                                      (uint32_t)(A.polarity_seed >> 32));
+            float theta = c.theta;
+            if (u53(r.w[0], r.w[1]) < A.p_tumble) theta = (float)(2.0 * kPi * u53(r.w[2], r.w[3]));
+            float sn, co;
+            sincosf(theta, &sn, &co);
+            sh.vel[0] = (double)c.v_A * (double)co;
+            sh.vel[1] = (double)c.v_A * (double)sn;
+            sh.vel[2] = (double)A.mot_coeff * Fx;
+            sh.vel[3] = (double)A.mot_coeff * Fy;
+        }
+    }
+    __syncthreads();
+
+    // ---- pass 2: centroid-moment channels (FP64 from the binary32 samples)
+    const double V = c.V, cx = c.Cx / V, cy = c.Cy / V;
+    const double gam = (double)c.gamma, dw = (double)(A.bulk_scale * c.gamma);
+    const double vol = (double)(float)(A.vol_scale * (A.A0 - V));
+    const double mob = (double)(c.M_pf / (float)kMobilityM0);
+    const double rep = (double)A.rep_coeff;
+    const double vx = (double)(float)(sh.vel[0] + sh.vel[2]);
+    const double vy = (double)(float)(sh.vel[1] + sh.vel[3]);
+    double m[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int y = y_lo; y < y_hi; y += kObsSweep) {
+        const int b = y - w.ty0;
+        if ((unsigned)b >= (unsigned)w.wy) continue;
+        const Chunk3 q = load_chunk(tile, w, y, ch);
+#pragma unroll
+        for (int k = 1; k <= 4; ++k) {
+            const int a = 4 * ch - 1 + k - w.tx0;
+            if ((unsigned)a >= (unsigned)w.wx) continue;
+            const double p = q.v[1][k];
+            const double e = q.v[1][k + 1], ww = q.v[1][k - 1];
+            const double nn = q.v[2][k], s = q.v[0][k];
+            const double ne = q.v[2][k + 1], nw = q.v[2][k - 1];
+            const double se = q.v[0][k + 1], sw = q.v[0][k - 1];
+            const double lap = (4.0 * (nn + s + e + ww) + ne + nw + se + sw - 20.0 * p) / 6.0;
+            const double gx = 0.5 * (e - ww), gy = 0.5 * (nn - s);
+            const double so = (double)other_share(A, c, a, b, q.v[1][k]);
+            double src[4] = {gam * lap - dw * p * (1.0 - p) * (1.0 - 2.0 * p), -rep * p * so,
+                             vol * p, -(vx * gx + vy * gy)};
+            if (mob != 1.0)  // passive channels only
+#pragma unroll
+                for (int j = 0; j < 3; ++j) src[j] *= mob;
+            const double wx = 2.0 * ((double)a - cx) * p / V;
+            const double wy = 2.0 * ((double)b - cy) * p / V;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                m[2 * j] += wx * src[j];
+                m[2 * j + 1] += wy * src[j];
+            }
+        }
+    }
+    cta_fold(m, sh.wm);
+    if (warp != 0) return;
+    if (lane == 0) {
+        const uint32_t bar = dev::map_to_rank(dev::smem_addr(&sh.barM), 0);
+#pragma unroll
+        for (int j = 0; j < 8; j += 2)
+            dev::st_async_v2f64(dev::map_to_rank(dev::smem_addr(&sh.rm[rank][j]), 0), m[j],
+                                m[j + 1], bar);
+    }
+    if (rank != 0) return;
+    if (!dev::mbar_wait_bounded(&sh.barM, 0, 1u << 24)) return;
+    double t[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+        t[j] = dev::ordered_lane_sum(lane < kObsBands ? sh.rm[lane][j] : 0.0, kObsBands);
+    if (lane == 0) {
         pfb_moment_accum2d& z = out[n];
-        for (int j = 0; j < 4; ++j) z.q[j] += dt * vel[j];
-        for (int j = 0; j < 6; ++j) z.q[4 + j] += dt * red[j][0];
-        z.q[10] += dt * (red[6][0] - vel[0] - vel[2]);
-        z.q[11] += dt * (red[7][0] - vel[1] - vel[3]);
+        for (int j = 0; j < 4; ++j) z.q[j] += dt * sh.vel[j];
+        for (int j = 0; j < 6; ++j) z.q[4 + j] += dt * t[j];
+        z.q[10] += dt * (t[6] - sh.vel[0] - sh.vel[2]);
+        z.q[11] += dt * (t[7] - sh.vel[1] - sh.vel[3]);
         ++z.count;
     }
 }
@@ -165,8 +255,20 @@ int velocity2d_observe(const pfb_step_args2d& A, pfb_moment_accum2d* out, double
                        cudaStream_t stream) {
     if (!out || !A.cell || !A.phi_in || !A.S_rd || !A.step_rd || A.N < 0 || A.L <= 0)
         return set_error(PFB_E_ARG, "velocity observer: bad arguments");
+    if (((uintptr_t)A.phi_in & 15u)) return set_error(PFB_E_ARG, "velocity observer: phi_in must be 16-byte aligned");
     if (A.N == 0) return PFB_OK;
-    k_observe2d<<<A.N, kObsThreads, 0, stream>>>(A, out, dt);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(A.N * kObsBands), 1, 1);
+    cfg.blockDim = dim3(kObsThreads, 1, 1);
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kObsBands;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_observe2d, A, out, dt);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return set_error(PFB_E_CUDA, "velocity observer: %s", cudaGetErrorString(e));
     return PFB_OK;

@@ -27,7 +27,16 @@ brick edge at lambda = 7):
   every cell.
 * 1000 steps of the periodic geometry at 128^3 with 64 cells (the same
   density and brick) through the whole step sequence of each
-  implementation: phi within 1e-5, origins and counters exact.
+  implementation: phi within 1e-5 at the same lattice voxel, tumble
+  counters and flags exact.
+
+Rounding ties. Cell 0 of these workloads is seeded at the box centre, an
+integer position, so in an even brick its centroid sits exactly half a voxel
+from the brick centre: its recentring shift rounds 1/2 plus or minus the
+last bits of the FP64 moment sums and follows their summation order. Such
+cells are exempt from the exact shift comparison, and in the free-running
+1000-step comparison only they may recentre at another step (their fields
+are then compared at the same lattice voxel).
 * 100 steps against the binary64 CPU oracle at the same configuration:
   the error of each observable (phi, V, centroid, velocity) is printed and
   bounded.
@@ -181,9 +190,41 @@ EXACT_3D = ("origin_x", "origin_y", "origin_z", "pending_shift_x", "pending_shif
             "phi_max", "flags", "shift_ctr", "tumble_ctr")
 
 
-def assert_measure_3d(a, b):
+def tie_cells(cells, B) -> np.ndarray:
+    """Cells whose centroid lies within 1e-9 of half a voxel from the brick
+    centre on some axis. Their recentring shift rounds a value that is 1/2 up
+    to the last bits of the FP64 moment sums, so it follows the summation
+    order (this library groups the sums by cluster band, the reference by its
+    tiles). A cell seeded at an integer position in an even brick is one."""
+    mid = 0.5 * (B - 1)
+    tie = np.zeros(len(cells), bool)
+    for k in "xyz":
+        off = cells["C" + k] / cells["V"] - mid
+        tie |= np.abs(np.abs(off - np.floor(off)) - 0.5) < 1e-9
+    return tie
+
+
+def world_diff3d(pa, ca, pb, cb) -> float:
+    """Largest |phi_a - phi_b| at the same lattice voxel: brick b is moved by
+    the difference of the origins (at most the shift clamp) before the
+    comparison; the voxels moved across the brick edge hold only the far
+    tail of the profile."""
+    worst = 0.0
+    for n in range(len(ca)):
+        delta = [int(ca["origin_" + k][n] - cb["origin_" + k][n]) for k in "zyx"]
+        assert max(abs(x) for x in delta) <= 4, (n, delta)
+        bb = np.roll(pb[n], [-x for x in delta], axis=(0, 1, 2)) if any(delta) else pb[n]
+        worst = max(worst, float(np.max(np.abs(pa[n] - bb))))
+    return worst
+
+
+def assert_measure_3d(a, b, B=64):
+    tie = tie_cells(b, B)
     for f in EXACT_3D:
-        np.testing.assert_array_equal(a[f], b[f], err_msg=f)
+        if f.startswith("pending_shift"):
+            np.testing.assert_array_equal(a[f][~tie], b[f][~tie], err_msg=f)
+        else:
+            np.testing.assert_array_equal(a[f], b[f], err_msg=f)
     for f in ("V", "Cx", "Cy", "Cz", "surface"):
         np.testing.assert_allclose(a[f], b[f], rtol=MOMENT_RTOL_3D, err_msg=f)
     scale = max(np.max(np.abs(b[f])) for f in ("Ix", "Iy", "Iz")) + 1e-300
@@ -266,20 +307,27 @@ def test_c3_periodic_1000_steps_vs_reference():
     c = c3_centres(p)
     a = DeviceState3D(p, c, "pfb")
     b = DeviceState3D(p, c, "ref")
-    worst = {}
+    tie0 = tie_cells(a.get_cells(), a.B)
+    worst, moved = {}, set()
     for n in range(1, 1001):
         a.step_once()
         b.step_once()
         if n in (1, 10, 100, 1000):
-            worst[n] = float(np.max(np.abs(a.get_phi() - b.get_phi())))
             ca, cb = a.get_cells(), b.get_cells()
-            for f in ("origin_x", "origin_y", "origin_z", "shift_ctr", "tumble_ctr", "flags"):
+            worst[n] = world_diff3d(a.get_phi(), ca, b.get_phi(), cb)
+            for f in ("tumble_ctr", "flags"):
                 np.testing.assert_array_equal(ca[f], cb[f], err_msg=f"{f} after {n} steps")
+            d = np.stack([ca["origin_" + k] - cb["origin_" + k] for k in "xyz"], 1)
+            moved |= set(np.nonzero(np.any(d != 0, 1))[0].tolist())
             np.testing.assert_allclose(ca["V"], cb["V"], rtol=1e-7)
     np.testing.assert_array_equal(a.get_flags(), b.get_flags())
     assert int(a.get_flags().sum()) == 0
-    print("C3 (128^3, 64 cells, B=64) max|dphi| vs the reference after 1/10/100/1000 steps:",
-          worst, "shifts", int(a.get_cells()["shift_ctr"].sum()))
+    print("C3 (128^3, 64 cells, B=64) world-frame max|dphi| vs the reference after "
+          f"1/10/100/1000 steps: {worst}; shifts {int(a.get_cells()['shift_ctr'].sum())}; "
+          f"cells at a rounding tie at the start {np.nonzero(tie0)[0].tolist()}, cells whose "
+          f"brick origin differed at a check {sorted(moved)}")
+    # only cells that started at a rounding tie may have recentred differently
+    assert moved <= set(np.nonzero(tie0)[0].tolist())
     assert worst[1000] <= PHI_TOL_3D_1000
 
 
