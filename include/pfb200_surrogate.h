@@ -72,11 +72,14 @@ int pfb_conv3x3_wgrad(const void* x, const void* dy, float* workspace, size_t wo
  * holds until exit; sizes needing more (pfb_conv3x3_wgrad_workspace above
  * 4 MiB, e.g. more than 56 images of 64 x 64 with 32 -> 32 channels) are
  * rejected with PFB_E_ARG. Nothing in the array has to start at zero (each
- * call overwrites what it reads). The first call on a device looks up the
- * array's device address with that device current; make that first call
- * before any stream capture. Calls that overlap on the GPU share the array
- * and race: serialise them. Allocates nothing; same results as
- * pfb_conv3x3_wgrad. */
+ * call overwrites what it reads; a CTA whose bounded MMA wait gave up writes
+ * NaN, so such a result is NaN, never stale data, and pfb_conv_status bit 0
+ * is set). The first call on a device looks up the array's device address
+ * with that device current and keeps it for the process; make that first
+ * call before any stream capture, and do not call it after a
+ * cudaDeviceReset of that device (the kept address would be stale). Calls
+ * that overlap on the GPU share the array and race: serialise them.
+ * Allocates nothing; same results as pfb_conv3x3_wgrad. */
 int pfb_conv3x3_wgrad_noalloc(const void* x, const void* dy, float* dw_oihw, float* db,
                               int batch, int H, int W, int cx, int cy, void* stream);
 

@@ -144,8 +144,89 @@ bool read_mobility_map(const std::string& path, std::vector<std::pair<int32_t, f
     return true;
 }
 
-// Overlay the map on the system's cell records (every listed id must exist).
-bool apply_mobility_map(pfb_sim2d* s, const std::vector<std::pair<int32_t, float>>& map, std::string* err) {
+// Explicit-Euler bound over the resolved per-cell pairs (gamma_i, M_i), the
+// reference's validate_effective_stiffness (include/params.cuh:729-775):
+// dt * max_i (M_i / M0) gamma_i * 40/6 must stay below 1 (fatal, with its
+// message), with warnings when a margin falls under 2x.
+bool effective_stiffness_ok(const pfb_params2d& p, const std::vector<pfb_cell2d>& cells) {
+    constexpr double kM0 = 0.5, kLapRowSum = 40.0 / 6.0;
+    double geff_max = 0.0, mrel_max = 0.0;
+    for (size_t i = 0; i < cells.size(); ++i) {
+        const double g = (double)cells[i].gamma, m = (double)cells[i].M_pf;
+        if (!(g > 0.0) || !std::isfinite(g) || !(m > 0.0) || !std::isfinite(m)) {
+            std::fprintf(stderr,
+                         "[fatal] cell %d has gamma = %.9g, phase-field mobility = %.9g; both must be "
+                         "positive and finite.\n",
+                         (int)i, g, m);
+            return false;
+        }
+        geff_max = std::fmax(geff_max, (m / kM0) * g);
+        mrel_max = std::fmax(mrel_max, m / kM0);
+    }
+    const double cfl = p.dt * geff_max * kLapRowSum;
+    if (cfl >= 1.0) {
+        std::fprintf(stderr,
+                     "[fatal] max_i[(M_i/M0)*gamma_i] = %.6g gives dt*coeff*laplacian_bound = %.4f; the "
+                     "configured safety limit is 1. Reduce dt below %.5g.\n",
+                     geff_max, cfl, 1.0 / (geff_max * kLapRowSum));
+        return false;
+    }
+    if (cfl > 0.5)
+        std::fprintf(stderr,
+                     "[warn] max_i[(M_i/M0)*gamma_i] = %.6g; dt*coeff*laplacian_bound = %.4f leaves under "
+                     "2x margin to the safety limit.\n",
+                     geff_max, cfl);
+    const double rep = 60.0 * p.kappa / (p.lambda * p.lambda);
+    const double rep_cfl = p.dt * mrel_max * rep;
+    if (rep_cfl > 0.5)
+        std::fprintf(stderr,
+                     "[warn] dt*max_i(M_i/M0)*rep_coeff = %.4f; the overlap-repulsion term has under 2x "
+                     "explicit-Euler margin at S_other ~ 1. Consider reducing dt (it is not changed "
+                     "automatically).\n",
+                     rep_cfl);
+    const double vol_cfl = p.dt * mrel_max * 2.0 * p.mu;
+    if (vol_cfl > 0.5)
+        std::fprintf(stderr,
+                     "[warn] dt*max_i(M_i/M0)*2*mu = %.4f; the area-constraint term has under 2x "
+                     "explicit-Euler margin.\n",
+                     vol_cfl);
+    return true;
+}
+
+// Host-side check of the resolved per-cell pairs before any device work, as
+// the reference validates the host initial condition before opening a GPU
+// context (src/sim.cu:308-317, :390-399): a fresh start resolves gamma from
+// the soft fraction and the mobility from the uniform value and the map; a
+// resume reads the checkpoint's records and overlays the map. Unknown map ids
+// are left to apply_mobility_map's message.
+bool precheck_stiffness(const pfb_params2d& p, const std::string& ckpt_in,
+                        const std::vector<std::pair<int32_t, float>>& map) {
+    std::vector<pfb_cell2d> cells((size_t)p.num_cells);
+    if (ckpt_in.empty()) {
+        const long long soft = std::llround(p.cancer_fraction * (double)p.num_cells);
+        for (int i = 0; i < p.num_cells; ++i) {
+            cells[(size_t)i].global_id = i;
+            cells[(size_t)i].gamma = (float)(i < soft ? p.gamma_cancer : p.gamma_normal);
+            cells[(size_t)i].M_pf = (float)p.phase_field_mobility;
+        }
+    } else {
+        std::vector<float> phi((size_t)p.num_cells * PFB_TILE_AREA);
+        pfb_ckpt2d_info info{};
+        pfb_ckpt2d_params rec{};
+        if (pfb_ckpt2d_read(ckpt_in.c_str(), &info, &rec, cells.data(), phi.data()) != PFB_OK)
+            return true;  // the resume path reports the reader's error
+    }
+    for (const auto& e : map)
+        for (auto& c : cells)
+            if (c.global_id == e.first) c.M_pf = e.second;
+    return effective_stiffness_ok(p, cells);
+}
+
+// Overlay the map on the system's cell records (every listed id must exist);
+// the resolved records must pass the explicit-Euler bound before the first
+// step, on a fresh start and on a resume alike.
+bool apply_mobility_map(pfb_sim2d* s, const pfb_params2d& p,
+                        const std::vector<std::pair<int32_t, float>>& map, std::string* err) {
     const int N = pfb_sim2d_num_cells(s);
     std::vector<pfb_cell2d> cells((size_t)N);
     std::vector<float> phi((size_t)N * PFB_TILE_AREA);
@@ -161,6 +242,8 @@ bool apply_mobility_map(pfb_sim2d* s, const std::vector<std::pair<int32_t, float
                    false;
         cells[(size_t)hit].M_pf = e.second;
     }
+    if (!effective_stiffness_ok(p, cells))
+        return *err = "the resolved per-cell mobilities break the explicit-Euler bound", false;
     if (pfb_sim2d_set_state(s, cells.data(), phi.data(), pfb_sim2d_step(s)) != PFB_OK)
         return *err = pfb_last_error(), false;
     return true;
@@ -712,6 +795,7 @@ int main(int argc, char** argv) {
         if (!o.print_set) o.print_interval = rec.print_interval;
         if (!o.verify_set) o.verify_every = rec.verify_every;
         if (o.self_test && self_test(p)) return 4;
+        if (!mobility.empty() && !precheck_stiffness(p, o.ckpt_in, mobility)) return 5;
         s = pfb_sim2d_create_from_checkpoint(o.ckpt_in.c_str(), o.device);
     } else {
         p.L = pfb_domain_side_for(p.num_cells, p.target_radius, o.rho);
@@ -735,6 +819,7 @@ int main(int argc, char** argv) {
         std::printf("  centres: %d, table hash %016llx\n", p.num_cells, (unsigned long long)hash);
         std::fflush(stdout);
         if (o.self_test && self_test(p)) return 4;
+        if (!mobility.empty() && !precheck_stiffness(p, "", mobility)) return 5;
         s = pfb_sim2d_create(&p, x.data(), y.data(), o.device);
     }
     if (!s) {
@@ -743,7 +828,7 @@ int main(int argc, char** argv) {
     }
     if (!mobility.empty()) {
         std::string err;
-        if (!apply_mobility_map(s, mobility, &err)) {
+        if (!apply_mobility_map(s, p, mobility, &err)) {
             std::fprintf(stderr, "[fatal] phase-field mobility: %s\n", err.c_str());
             pfb_sim2d_destroy(s);
             return 5;

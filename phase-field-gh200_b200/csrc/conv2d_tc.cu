@@ -330,7 +330,11 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3x3_wgrad(const __grid_con
     }
     float* out = A.partial + (size_t)blockIdx.x * (9 * CY * CX + CY);
     if (!ok) {
+        // the MMA wait gave up: poison this CTA's block so the reduction
+        // yields NaN instead of mixing in what the scratch held before
         if (tid == 0) atomicOr(&g_conv_status, 1u);
+        for (int i = tid; i < 9 * CY * CX + CY; i += (int)blockDim.x)
+            out[i] = __int_as_float(0x7fc00000);
     } else {
         const int r = warp * 32 + lane;
         for (int t = 0; t < NT; ++t) {
@@ -591,7 +595,10 @@ std::mutex g_scratch_mutex;
 float* g_scratch_ptr[kNoAllocMaxDevices] = {};
 
 // Device address of g_wgrad_scratch on the current device, looked up once per
-// device (the host-side name of the array is not a device address).
+// device (the host-side name of the array is not a device address). The
+// address belongs to the device's primary context: a cudaDeviceReset in the
+// same process makes the cached value stale, so such hosts must not call the
+// entry point after a reset.
 int scratch_on_current_device(float** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -631,7 +638,8 @@ extern "C" int pfb_conv3x3_wgrad_noalloc(const void* x, const void* dy, float* d
     const int rc = scratch_on_current_device(&scratch);
     if (rc) return rc;
     // every CTA overwrites its whole block of partial sums before the reduction
-    // reads it, so nothing in the shared array has to start at zero
+    // reads it (with NaN when its MMA wait gave up), so nothing in the shared
+    // array has to start at zero
     return conv3x3_wgrad(x, dy, scratch, kNoAllocScratchBytes, dw_oihw, db, batch, H, W, cx, cy,
                          static_cast<cudaStream_t>(stream));
 }

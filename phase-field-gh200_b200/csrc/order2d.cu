@@ -13,6 +13,8 @@
 // are all ones and sort last).
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include <cstdint>
 
 #include "pfb200.h"
@@ -86,12 +88,23 @@ int visit_order2d_capacity() {
     return m;
 }
 
-// Shared-memory opt-in for N cells; call outside stream capture.
+// Shared-memory opt-in for up to N cells; call outside stream capture. The
+// attribute belongs to the kernel on the whole device, so it only ever grows
+// (a smaller system created later must not shrink it under a larger one).
 cudaError_t visit_order2d_prepare(int N) {
+    static std::mutex mu;
+    static int granted[64] = {};
     int M = 1;
     while (M < N) M <<= 1;
-    return cudaFuncSetAttribute(k_visit_order2d, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(M * sizeof(unsigned long long)));
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const int bytes = (int)(M * sizeof(unsigned long long));
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev >= 0 && dev < 64 && granted[dev] >= bytes) return cudaSuccess;
+    e = cudaFuncSetAttribute(k_visit_order2d, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess && dev >= 0 && dev < 64) granted[dev] = bytes;
+    return e;
 }
 
 cudaError_t visit_order2d_launch(const pfb_cell2d* cell, uint32_t* perm, int N, int L, cudaStream_t stream) {

@@ -111,3 +111,27 @@ def test_self_test_failure_exits_4():
     r = subprocess.run([str(EXE), *map(str, SELF_TEST_ARGS), "--radius", "110"], capture_output=True,
                        text=True, timeout=120)
     assert r.returncode == 4 and "SELF-TEST FAILED" in r.stdout
+
+
+@pytest.mark.parametrize("resume", [False, True])
+def test_mobility_map_breaking_the_euler_bound_is_fatal(tmp_path, resume):
+    """A map whose resolved (M_i/M0) gamma_i breaks dt * . * 40/6 < 1 stops the
+    run before any device work, with the reference's message and its exit
+    code (the reference's Sim::init fails: src/sim.cu:316, src/main.cu:611-615)."""
+    import gzip
+    m = tmp_path / "mob.txt"
+    m.write_text("# one stiff cell\n0 100.0\n")
+    if resume:
+        ck = tmp_path / "ck.bin"
+        src = Path(__file__).resolve().parent / "golden" / "ckpt2d_ref_n2.bin.gz"
+        ck.write_bytes(gzip.decompress(src.read_bytes()))
+        r = run("-c", ck, "--phase-field-mobility-map", m)
+    else:
+        r = run("--N", 12, "--phase-field-mobility-map", m)
+    assert r.returncode == 5, r.stderr
+    assert "[fatal] max_i[(M_i/M0)*gamma_i] = 200 gives dt*coeff*laplacian_bound" in r.stderr
+    # an acceptable map passes the check (and then needs a device)
+    m.write_text("0 0.6\n")
+    r = run(*(("-c", tmp_path / "ck.bin") if resume else ("--N", 12)),
+            "--phase-field-mobility-map", m)
+    assert "laplacian_bound" not in r.stderr
