@@ -343,10 +343,17 @@ pfb_sim2d* pfb_sim2d_create_from_state(const pfb_params2d* p,
                                        const float* phi, long long step,
                                        int device);
 void pfb_sim2d_destroy(pfb_sim2d* s);
-/* Tuning knobs: cluster CTAs per cell (2/4/8), kernel variant (as in
- * pfb_step2d_launch_ex) and CUDA-graph use. */
+/* Tuning knobs: cluster CTAs per cell (2/4/8), kernel variant and CUDA-graph
+ * use. Variants: 0 (default) and 1 scatter the Q5.27 aggregate with
+ * non-returning adds on the common path and detect S_overflow exactly through
+ * per-bin bounds the driver keeps (recounting only a bin whose bound reaches
+ * 2^32); 2 uses returning adds that test every add (pfb_step2d_launch's
+ * scatter). Results, flags included, are identical. */
 int pfb_sim2d_set_cluster(pfb_sim2d* s, int cluster);
 int pfb_sim2d_set_variant(pfb_sim2d* s, int variant);
+/* Bins recounted exactly so far by variants 0/1 (bins whose bound reached
+ * 2^32; normally none). No reference counterpart: a diagnostic. */
+int pfb_sim2d_scatter_recounts(pfb_sim2d* s, unsigned int* out);
 int pfb_sim2d_set_graph(pfb_sim2d* s, int use_graph);
 /* Cell visit order (reference src/main.cu:491-492 --morton, src/sim.cu:
  * 284-296, 649-653). PFB_VISIT_MORTON orders the clusters by the Z-order

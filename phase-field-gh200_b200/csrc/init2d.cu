@@ -63,7 +63,9 @@ __device__ __forceinline__ float seed_value(int gx, int gy, float cx, float cy, 
     if (dx < -half) dx += L;
     if (dy > half) dy -= L;
     if (dy < -half) dy += L;
-    const float r = sqrtf(dx * dx + dy * dy);
+    // the reference's build contracts dx*dx + dy*dy into fma(dx, dx, dy*dy);
+    // written out so the seed stays bit-identical whatever the code around it
+    const float r = sqrtf(__fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
     return 0.5f * (1.0f - tanhf(kappa_iface * (r - radius_eff)));
 }
 

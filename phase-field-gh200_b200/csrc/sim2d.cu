@@ -58,6 +58,28 @@ struct pfb_sim2d {
     Velocity2D* vel = nullptr;  // open PFVMOM4 recorder
     Boundary2D* bnd = nullptr;  // open PFB recorder
     uint32_t* d_perm = nullptr;  // Morton visit order (null: launch order)
+    // exact overflow detection of the non-returning scatter (BinArgs)
+    unsigned long long* d_bins = nullptr;
+    unsigned int* d_binctl = nullptr;  // done, 2 list counts, recounts, 2 lists
+    int nbins_side = 0;
+
+    size_t bin_words() const { return 2 * (size_t)nbins_side * (size_t)nbins_side; }
+    static constexpr size_t kBinCtlWords = 4 + 2 * kMaxFlaggedBins;
+
+    BinArgs bin_args() const {
+        return BinArgs{d_bins, d_binctl, d_binctl + 1, d_binctl + 4, d_binctl + 3, nbins_side,
+                       nbins_side};
+    }
+
+    // Both bound sets, the counter and the lists back to zero: after any
+    // change of the step counter other than a launch.
+    int reset_bins() {
+        PFB_CU(cudaMemsetAsync(d_bins, 0, bin_words() * sizeof(unsigned long long), stream),
+               "clear bins");
+        PFB_CU(cudaMemsetAsync(d_binctl, 0, kBinCtlWords * sizeof(unsigned int), stream),
+               "clear bins");
+        return PFB_OK;
+    }
 
     ~pfb_sim2d() {
         if (vel) velocity2d_destroy(vel);
@@ -76,6 +98,8 @@ struct pfb_sim2d {
         cudaFree(d_traj);
         cudaFree(d_perm);
         cudaFree(d_cell_prev);
+        cudaFree(d_bins);
+        cudaFree(d_binctl);
         cudaFree(b_phi);
         cudaFree(b_cell);
         cudaFree(b_cls);
@@ -129,6 +153,7 @@ struct pfb_sim2d {
             (unsigned long long)(pin == 1 ? steps_done : steps_done + 1)};
         PFB_CU(cudaMemcpyAsync(d_step, hs, sizeof(hs), cudaMemcpyHostToDevice, stream), "restore");
         PFB_CU(cudaMemsetAsync(d_cursor, 0, 2 * sizeof(unsigned long long), stream), "restore");
+        if (const int rc = reset_bins()) return rc;
         PFB_CU(cudaStreamSynchronize(stream), "restore");
         return PFB_OK;
     }
@@ -170,7 +195,10 @@ struct pfb_sim2d {
     int launch_one(int slot) {
         if (const int rc = sort_visit_order(slot)) return rc;
         const pfb_step_args2d a = args_for_slot(slot);
-        return step2d_launch_storage(&a, cluster, variant, p.phi_storage, stream);
+        // the driver owns bin buffers: non-returning scatter, overflow exact
+        if (variant == 0 || variant == 1)
+            return step2d_launch_binned(&a, cluster, p.phi_storage, bin_args(), stream);
+        return step2d_launch_storage(&a, cluster, 1, p.phi_storage, stream);
     }
 
     size_t pool_bytes() const {
@@ -271,7 +299,11 @@ struct pfb_sim2d {
         PFB_CU(cudaMalloc(&d_flags, PFB_FLAG_COUNT * sizeof(uint32_t)), "alloc flags");
         PFB_CU(cudaMalloc(&d_traj, (size_t)N * sizeof(pfb_traj_cell2d)), "alloc traj");
         PFB_CU(cudaMalloc(&d_cell_prev, (size_t)N * sizeof(pfb_cell2d)), "alloc cells");
+        nbins_side = (L + (1 << kBinShift) - 1) >> kBinShift;
+        PFB_CU(cudaMalloc(&d_bins, bin_words() * sizeof(unsigned long long)), "alloc bins");
+        PFB_CU(cudaMalloc(&d_binctl, kBinCtlWords * sizeof(unsigned int)), "alloc bins");
         PFB_CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
+        if (const int rc = reset_bins()) return rc;
         PFB_CU(cudaMemsetAsync(d_cursor, 0, 2 * sizeof(unsigned long long), stream), "memset");
         PFB_CU(cudaMemsetAsync(d_step, 0, 2 * sizeof(unsigned long long), stream), "memset");
         PFB_CU(cudaMemsetAsync(d_flags, 0, PFB_FLAG_COUNT * sizeof(uint32_t), stream), "memset");
@@ -320,6 +352,7 @@ struct pfb_sim2d {
             (unsigned long long)(pin == 1 ? step : step + 1)};
         PFB_CU(cudaMemcpyAsync(d_step, hs, sizeof(hs), cudaMemcpyHostToDevice, stream), "upload step");
         PFB_CU(cudaMemsetAsync(d_cursor, 0, 2 * sizeof(unsigned long long), stream), "memset");
+        if (const int rc2 = reset_bins()) return rc2;
         PFB_CU(cudaMemsetAsync(d_S, 0, 3 * s_words * sizeof(uint32_t), stream), "memset S");
         int rc = scatter_all2d(scan ? scan : (const float*)d_phi[pin], d_cell, d_cls,
                                d_S + (size_t)rot * s_words, N, L, P, d_flags, stream);
@@ -631,9 +664,19 @@ int pfb_sim2d_set_cluster(pfb_sim2d* s, int cluster) {
 
 int pfb_sim2d_set_variant(pfb_sim2d* s, int variant) {
     if (!s) return set_error(PFB_E_ARG, "null sim");
-    if (variant < 0 || variant > 1) return set_error(PFB_E_CONFIG, "unknown kernel variant");
+    if (variant < 0 || variant > 2) return set_error(PFB_E_CONFIG, "unknown kernel variant");
     if (variant != s->variant) s->drop_graph();
     s->variant = variant;
+    return PFB_OK;
+}
+
+int pfb_sim2d_scatter_recounts(pfb_sim2d* s, unsigned int* out) {
+    if (!s || !out) return set_error(PFB_E_ARG, "scatter_recounts: null argument");
+    PFB_CU(cudaSetDevice(s->device), "cudaSetDevice");
+    PFB_CU(cudaMemcpyAsync(out, s->d_binctl + 3, sizeof(unsigned int), cudaMemcpyDeviceToHost,
+                           s->stream),
+           "read recounts");
+    PFB_CU(cudaStreamSynchronize(s->stream), "read recounts");
     return PFB_OK;
 }
 

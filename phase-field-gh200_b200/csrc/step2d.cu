@@ -200,9 +200,10 @@ __device__ __forceinline__ void store_zero(T* o) {
 //                          (f32 bits); on full-moment steps phi^{n+1} is
 //                          written over it.
 // ---------------------------------------------------------------------------
-template <int CLS, int K, typename T, int OBS>
+template <int CLS, int K, typename T, int OBS, bool BINS = false>
 __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int rank,
-                                            char* smem, unsigned long long step, bool fm) {
+                                            char* smem, unsigned long long step, bool fm,
+                                            const BinArgs* bins = nullptr) {
     constexpr Window W = window_of(CLS);
     constexpr int WX = W.wx, WY = W.wy, TX0 = W.tx0, TY0 = W.ty0;
     constexpr int RB = band_rows(WY, K);
@@ -479,10 +480,12 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
                     // pn becomes the stored value (16-bit pools round here)
                     store4<T>(o, pn, sr_seed, (uint32_t)(o - tile_out));
                     uint32_t* srow = A.S_sc + (size_t)gy * Pp;
-                    bool ovf = false;
+                    if constexpr (!BINS) {
+                        bool ovf = false;
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) ovf |= old_prev[j] > 0xFFFFFFFFu - q_prev[j];
-                    if (ovf) atomicOr(A.flags + PFB_FLAG_S_OVERFLOW, 1u);
+                        for (int j = 0; j < 4; ++j) ovf |= old_prev[j] > 0xFFFFFFFFu - q_prev[j];
+                        if (ovf) atomicOr(A.flags + PFB_FLAG_S_OVERFLOW, 1u);
+                    }
                     // |phi| bit patterns order like the values; NaN and inf
                     // sort above 2.0, so one compare guards the rare checks
                     const uint32_t rowb =
@@ -503,8 +506,13 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
                     for (int j = 0; j < 4; ++j) {
                         const float p = pn[j];
                         const uint32_t qv = q_encode(p);
-                        q_prev[j] = qv;
-                        old_prev[j] = dev::atom_add_nonzero(srow + gxj[j], qv);
+                        if constexpr (BINS) {
+                            // bounded per bin; checked by the launch's last CTA
+                            red_add_nonzero(srow + gxj[j], qv);
+                        } else {
+                            q_prev[j] = qv;
+                            old_prev[j] = dev::atom_add_nonzero(srow + gxj[j], qv);
+                        }
                         const double d = (double)p * (double)p;
                         rowV += d;
                         rowX += d * (double)j;
@@ -529,10 +537,16 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
                     vc = vn;
                     ec = en;
                 }
-                bool ovf = false;
+                if constexpr (BINS) {
+                    int gys = gy0 + y0 + r0;
+                    if (gys >= L) gys -= L;
+                    bin_block_add(*bins, gys, nr, gxj[0], 4, L, q_encode(__uint_as_float(pmaxb)));
+                } else {
+                    bool ovf = false;
 #pragma unroll
-                for (int j = 0; j < 4; ++j) ovf |= old_prev[j] > 0xFFFFFFFFu - q_prev[j];
-                if (ovf) atomicOr(A.flags + PFB_FLAG_S_OVERFLOW, 1u);
+                    for (int j = 0; j < 4; ++j) ovf |= old_prev[j] > 0xFFFFFFFFu - q_prev[j];
+                    if (ovf) atomicOr(A.flags + PFB_FLAG_S_OVERFLOW, 1u);
+                }
                 acc.pmaxb = max(acc.pmaxb, (int)pmaxb);
                 if (colmask) {
                     acc.blox = min(acc.blox, x0 + __ffs(colmask) - 1);
@@ -573,6 +587,16 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
                     wc = wn;
                     vc = vn;
                     ec = en;
+                }
+                if constexpr (BINS) {
+                    // the strip's destination block, clipped to the window
+                    const int ba = max(0, y0 + r0 - sy), bb = min(dwy, y0 + r0 + nr - sy);
+                    const int aa = max(0, x0 - sx), ab = min(dwx, x0 + 4 - sx);
+                    int gys = gy0n + ba, gxs = gx0n + aa;
+                    if (gys >= L) gys -= L;
+                    if (gxs >= L) gxs -= L;
+                    bin_block_add(*bins, gys, bb - ba, gxs, ab - aa, L,
+                                  q_encode(__uint_as_float((uint32_t)acc.pmaxb)));
                 }
             }
         }
@@ -669,17 +693,92 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
 
 template <int CLS, int K, int OBS>
 __device__ __forceinline__ void global_cell_v1(const pfb_step_args2d& A, int n, int rank,
-                                               char* smem, unsigned long long step, bool fm) {
+                                               char* smem, unsigned long long step, bool fm,
+                                               const BinArgs* bins = nullptr) {
     StepShared<K, OBS>& sh = *reinterpret_cast<StepShared<K, OBS>*>(smem);
     if (threadIdx.x == 0)
         plan_cell<OBS == PFB_VELOCITY_SPATIAL>(A, n, CLS, step, sh.plan, rank == 0);
     __syncthreads();
-    global_cell<CLS, K, kWarps, OBS>(A, sh.plan, rank, sh.red, fm, &g_step2d_status);
+    global_cell<CLS, K, kWarps, OBS>(A, sh.plan, rank, sh.red, fm, &g_step2d_status, bins,
+                                     &sh.abort);
 }
 
-// One system's step for CTA `lb` of the `nb` CTAs that serve it.
-template <int K, typename T, int OBS = PFB_VELOCITY_DISABLED>
-__device__ __forceinline__ void step_body(const pfb_step_args2d& A, int lb, int nb, char* smem) {
+// ---- end of a launch that scattered with non-returning adds ------------------
+// Every CTA counts itself done (after a CTA barrier and a gpu-scope fence, so
+// its scatters, bounds and commits are visible); the CTA that completes the
+// count resets it and recounts each listed bin exactly: 64-bit sums of q over the committed
+// windows of every cell (phi_out, cell records), S_overflow when one reaches
+// 2^32. A list that overflowed makes it scan every bound of the set.
+template <typename T>
+__device__ __noinline__ void bins_finish(const pfb_step_args2d& A, const BinArgs& Bc,
+                                         char* smem) {
+    __shared__ int last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned old = atomicAdd(Bc.done, 1u);
+        last = old + 1u == gridDim.x;
+        if (last) *Bc.done = 0u;  // every other CTA has counted itself
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    const unsigned listed = *reinterpret_cast<volatile unsigned*>(Bc.nflag);
+    if (listed == 0u) return;
+    unsigned long long* acc = reinterpret_cast<unsigned long long*>(smem);  // 256 pixels
+    const int L = A.L, nbins = Bc.nbx * Bc.nby;
+    const bool scan = listed > (unsigned)kMaxFlaggedBins;
+    const int items = scan ? nbins : (int)listed;
+    for (int it = 0; it < items; ++it) {
+        int bin;
+        if (scan) {
+            if (Bc.bound[it] < (1ull << 32)) continue;  // uniform: every thread reads it
+            bin = it;
+        } else {
+            bin = (int)Bc.flagged[it];
+        }
+        for (int k = threadIdx.x; k < 256; k += blockDim.x) acc[k] = 0ull;
+        __syncthreads();
+        const int px0 = (bin % Bc.nbx) << kBinShift, py0 = (bin / Bc.nbx) << kBinShift;
+        const int w = min(16, L - px0), h = min(16, L - py0);
+        for (int c = threadIdx.x; c < A.N; c += blockDim.x) {
+            const Window W = window_of((int)A.cell_cls[c]);
+            const int gx0 = A.cell[c].gx0, gy0 = A.cell[c].gy0;
+            const T* tile = reinterpret_cast<const T*>(A.phi_out) + (size_t)c * kTileArea;
+            for (int j = 0; j < h; ++j) {
+                int b = py0 + j - gy0;
+                if (b < 0) b += L;
+                if (b >= W.wy) continue;
+                for (int i = 0; i < w; ++i) {
+                    int a = px0 + i - gx0;
+                    if (a < 0) a += L;
+                    if (a >= W.wx) continue;
+                    const T raw = tile[(size_t)(W.ty0 + b) * kTilePitch + W.tx0 + a];
+                    float v;
+                    if constexpr (Store<T>::kHalf)
+                        v = Store<T>::value(*reinterpret_cast<const uint16_t*>(&raw));
+                    else
+                        v = raw;
+                    const uint32_t q = q_encode(v);
+                    if (q) atomicAdd(acc + j * 16 + i, (unsigned long long)q);
+                }
+            }
+        }
+        __syncthreads();
+        bool over = false;
+        for (int k = threadIdx.x; k < 256; k += blockDim.x) over |= acc[k] >= (1ull << 32);
+        if (__syncthreads_or(over) && threadIdx.x == 0) atomicOr(A.flags + PFB_FLAG_S_OVERFLOW, 1u);
+        if (threadIdx.x == 0) atomicAdd(Bc.recounts, 1u);
+    }
+    if (threadIdx.x == 0) *Bc.nflag = 0u;
+}
+
+// One system's step for CTA `lb` of the `nb` CTAs that serve it. BINS: the
+// identity path scatters without returns under per-bin bounds (B holds both
+// sets; this launch uses set step & 1 and clears the other).
+template <int K, typename T, int OBS = PFB_VELOCITY_DISABLED, bool BINS = false>
+__device__ __forceinline__ void step_body(const pfb_step_args2d& A, int lb, int nb, char* smem,
+                                          const BinArgs& B = BinArgs{}) {
     const int tid = threadIdx.x;
 
     // Clear the S slot two steps ahead with streaming stores (the kernel does
@@ -697,6 +796,18 @@ __device__ __forceinline__ void step_body(const pfb_step_args2d& A, int lb, int 
         *A.step_wr = step + 1ull;
     }
     const bool fm = full_moment_step(A, step);
+    BinArgs Bc{};
+    if constexpr (BINS) {
+        const int nbins = B.nbx * B.nby;
+        const int par = (int)(step & 1ull);
+        Bc = BinArgs{B.bound + (size_t)par * nbins, B.done, B.nflag + par,
+                     B.flagged + (size_t)par * kMaxFlaggedBins, B.recounts, B.nbx, B.nby};
+        unsigned long long* other = B.bound + (size_t)(1 - par) * nbins;
+        for (int i = lb * kThreads + tid; i < nbins; i += nb * kThreads) other[i] = 0ull;
+    }
+    // bounds are only needed where a non-returning scatter happens: the
+    // identity path, which full-moment steps never take
+    const BinArgs* bins = (BINS && !fm) ? &Bc : nullptr;
 
     const int rank = (int)dev::cluster_rank();
     StepShared<K, OBS>& sh = *reinterpret_cast<StepShared<K, OBS>*>(smem);
@@ -706,17 +817,17 @@ __device__ __forceinline__ void step_body(const pfb_step_args2d& A, int lb, int 
     const int n = A.perm ? (int)A.perm[slot] : slot;
     const int cls = (int)A.cell_cls[n];
     switch (cls) {
-        case 0: staged_cell<0, K, T, OBS>(A, n, rank, smem, step, fm); break;
-        case 1: staged_cell<1, K, T, OBS>(A, n, rank, smem, step, fm); break;
-        case 2: staged_cell<2, K, T, OBS>(A, n, rank, smem, step, fm); break;
-        case 3: staged_cell<3, K, T, OBS>(A, n, rank, smem, step, fm); break;
+        case 0: staged_cell<0, K, T, OBS, BINS>(A, n, rank, smem, step, fm, bins); break;
+        case 1: staged_cell<1, K, T, OBS, BINS>(A, n, rank, smem, step, fm, bins); break;
+        case 2: staged_cell<2, K, T, OBS, BINS>(A, n, rank, smem, step, fm, bins); break;
+        case 3: staged_cell<3, K, T, OBS, BINS>(A, n, rank, smem, step, fm, bins); break;
         case 4:
             if constexpr (Store<T>::kHalf) {
                 // 16-bit pools: the global-memory classes are not provided
                 if (rank == 0 && tid == 0) atomicAdd(A.flags + PFB_FLAG_CLASS_UNSUPPORTED, 1u);
                 dev::cluster_wait();
             } else {
-                global_cell_v1<4, K, OBS>(A, n, rank, smem, step, fm);
+                global_cell_v1<4, K, OBS>(A, n, rank, smem, step, fm, bins);
             }
             break;
         case 5:
@@ -724,7 +835,7 @@ __device__ __forceinline__ void step_body(const pfb_step_args2d& A, int lb, int 
                 if (rank == 0 && tid == 0) atomicAdd(A.flags + PFB_FLAG_CLASS_UNSUPPORTED, 1u);
                 dev::cluster_wait();
             } else {
-                global_cell_v1<5, K, OBS>(A, n, rank, smem, step, fm);
+                global_cell_v1<5, K, OBS>(A, n, rank, smem, step, fm, bins);
             }
             break;
         default:
@@ -732,13 +843,14 @@ __device__ __forceinline__ void step_body(const pfb_step_args2d& A, int lb, int 
             dev::cluster_wait();  // uniform over the cluster
             break;
     }
+    if constexpr (BINS) bins_finish<T>(A, Bc, smem);
 }
 
-template <int K, typename T = float, int OBS = PFB_VELOCITY_DISABLED>
+template <int K, typename T = float, int OBS = PFB_VELOCITY_DISABLED, bool BINS = false>
 __global__ void __launch_bounds__(kThreads, PFB_STEP2D_MINB)
-    k_step2d(const __grid_constant__ pfb_step_args2d A) {
+    k_step2d(const __grid_constant__ pfb_step_args2d A, const __grid_constant__ BinArgs B) {
     extern __shared__ __align__(128) char smem[];
-    step_body<K, T, OBS>(A, (int)blockIdx.x, (int)gridDim.x, smem);
+    step_body<K, T, OBS, BINS>(A, (int)blockIdx.x, (int)gridDim.x, smem, B);
 }
 
 // Many independent systems in one launch: system r is served by CTAs
@@ -780,6 +892,12 @@ static cudaError_t configure_pool() {
                                          step_smem_bytes(K));
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_step2d<K, T>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_step2d<K, T, PFB_VELOCITY_DISABLED, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, step_smem_bytes(K));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_step2d<K, T, PFB_VELOCITY_DISABLED, true>,
+                             cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_step2d_batch<K, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              step_smem_bytes(K));
@@ -826,8 +944,9 @@ int step2d_configure_device() {
 
 int step2d_smem_bytes(int k) { return step_smem_bytes(k); }
 
-template <int K, typename T = float, int OBS = PFB_VELOCITY_DISABLED>
-static cudaError_t launch_k(const pfb_step_args2d& A, cudaStream_t stream) {
+template <int K, typename T = float, int OBS = PFB_VELOCITY_DISABLED, bool BINS = false>
+static cudaError_t launch_k(const pfb_step_args2d& A, cudaStream_t stream,
+                            const BinArgs& B = BinArgs{}) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(A.N * K), 1, 1);
     cfg.blockDim = dim3(kThreads, 1, 1);
@@ -840,7 +959,7 @@ static cudaError_t launch_k(const pfb_step_args2d& A, cudaStream_t stream) {
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k_step2d<K, T, OBS>, A);
+    return cudaLaunchKernelEx(&cfg, k_step2d<K, T, OBS, BINS>, A, B);
 }
 
 // Contract checks common to every single-system launch.
@@ -889,6 +1008,41 @@ int step2d_launch_storage(const pfb_step_args2d* a, int cluster, int variant, in
         e = cluster == 2   ? launch_k<2>(A, stream)
             : cluster == 4 ? launch_k<4>(A, stream)
                            : launch_k<8>(A, stream);
+    if (e != cudaSuccess) return set_error(PFB_E_CUDA, "step launch: %s", cudaGetErrorString(e));
+    return PFB_OK;
+}
+
+int step2d_launch_binned(const pfb_step_args2d* a, int cluster, int storage,
+                         const BinArgs& B, cudaStream_t stream) {
+    int rc = check_step_args(a);
+    if (rc) return rc;
+    const pfb_step_args2d& A = *a;
+    if (A.moments) return set_error(PFB_E_ARG, "moments are read by the observed launch only");
+    if (!B.bound || !B.done || !B.nflag || !B.flagged)
+        return set_error(PFB_E_ARG, "binned launch without its bin buffers");
+    if (B.nbx != (A.L + (1 << kBinShift) - 1) >> kBinShift || B.nby != B.nbx)
+        return set_error(PFB_E_ARG, "bin grid does not match the lattice side");
+    if (cluster == 0) cluster = kDefaultCluster;
+    if (cluster != 2 && cluster != 4 && cluster != 8)
+        return set_error(PFB_E_CONFIG, "cluster must be 2, 4 or 8");
+    if (storage != kStoreF32 && storage != kStoreF16 && storage != kStoreBF16)
+        return set_error(PFB_E_ARG, "unknown phi storage %d", storage);
+    if (storage != kStoreF32 && cluster == 8)
+        return set_error(PFB_E_CONFIG, "16-bit phi pools use clusters of 2 or 4");
+    if (A.N == 0) return PFB_OK;
+    if ((rc = step2d_configure_device())) return rc;
+    constexpr int D = PFB_VELOCITY_DISABLED;
+    cudaError_t e;
+    if (storage == kStoreF16)
+        e = cluster == 2 ? launch_k<2, __half, D, true>(A, stream, B)
+                         : launch_k<4, __half, D, true>(A, stream, B);
+    else if (storage == kStoreBF16)
+        e = cluster == 2 ? launch_k<2, __nv_bfloat16, D, true>(A, stream, B)
+                         : launch_k<4, __nv_bfloat16, D, true>(A, stream, B);
+    else
+        e = cluster == 2   ? launch_k<2, float, D, true>(A, stream, B)
+            : cluster == 4 ? launch_k<4, float, D, true>(A, stream, B)
+                           : launch_k<8, float, D, true>(A, stream, B);
     if (e != cudaSuccess) return set_error(PFB_E_CUDA, "step launch: %s", cudaGetErrorString(e));
     return PFB_OK;
 }

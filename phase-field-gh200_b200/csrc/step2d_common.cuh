@@ -8,6 +8,7 @@
 
 #include "device_util.cuh"
 #include "pfb_common.cuh"
+#include "pfb_internal.h"
 
 namespace pfb {
 
@@ -167,6 +168,112 @@ __device__ __forceinline__ bool full_moment_step(const pfb_step_args2d& A,
                                                  unsigned long long step) {
     return A.full_moment_every > 0 &&
            ((step + 1ull) % (unsigned long long)A.full_moment_every) == 0ull;
+}
+
+// ---- exact overflow detection for non-returning scatters -------------------
+// The Q5.27 aggregate only ever receives non-negative addends, so the running
+// sum at a pixel crosses 2^32 - 1 (the reference's S_overflow test on each
+// returning atomicAdd, src/kernels.cu:496-497) exactly when the pixel's final
+// total T(p) does, whatever the order of the adds. A launch that scatters with
+// non-returning red.add keeps, per 16 x 16 lattice bin, an upper bound of
+// T(p) over the bin: every scatter adds the largest addend it put into the bin
+// (warp-aggregated). The last CTA of the launch scans the bins; only a bin whose
+// bound reaches 2^32 is recounted exactly (64-bit sums of q over the committed
+// windows of every cell), and S_overflow is raised iff some T(p) >= 2^32.
+// Two sets of bins alternate by step parity: a launch bounds into set
+// (step & 1) and clears the other set for the next launch, so nothing is ever
+// cleared on the host. A bound's first crossing of 2^32 appends its bin to the
+// set's short list, so the last CTA normally has nothing to scan.
+// (BinArgs, kBinShift and kMaxFlaggedBins: pfb_internal.h)
+
+__device__ __forceinline__ void red_add_nonzero(uint32_t* p, uint32_t v) {
+    asm volatile(
+        "{\n\t.reg .pred nz;\n\t"
+        "setp.ne.u32 nz, %1, 0;\n\t"
+        "@nz red.global.add.u32 [%0], %1;\n\t}" ::"l"(p),
+        "r"(v)
+        : "memory");
+}
+
+// Adds q to the bound of `bin` from the calling lanes, one atomic per distinct
+// bin among them (the largest q of the group); q == 0 adds nothing.
+__device__ __forceinline__ void bin_bound_add(const BinArgs& B, int bin, uint32_t q) {
+    const unsigned act = __activemask();
+    const unsigned key = q ? (unsigned)bin : 0xFFFFFFFFu;
+    const unsigned grp = __match_any_sync(act, key);
+    const uint32_t mx = __reduce_max_sync(grp, q);
+    if (q && (int)(__ffs(grp) - 1) == (int)(threadIdx.x & 31)) {
+        const unsigned long long old = atomicAdd(B.bound + bin, (unsigned long long)mx);
+        if (old < (1ull << 32) && old + mx >= (1ull << 32)) {
+            const unsigned k = atomicAdd(B.nflag, 1u);
+            if (k < (unsigned)kMaxFlaggedBins) B.flagged[k] = (unsigned)bin;
+        }
+    }
+}
+
+// Forward cyclic run of bins touched by lattice rows (or columns) g .. g+n-1
+// (0 <= g < L, 1 <= n < L): first bin and count. The last bin of a side that
+// is not a multiple of 16 is partial, so a short run can cross it.
+__device__ __forceinline__ int bin_run(int g, int n, int L, int nb, int* first) {
+    int g1 = g + n - 1;
+    if (g1 >= L) g1 -= L;
+    const int a = g >> kBinShift, b = g1 >> kBinShift;
+    *first = a;
+    return (b - a + nb) % nb + 1;
+}
+
+// A block of destination pixels (rows gy .. gy+nr-1, columns gx .. gx+nc-1 of
+// the periodic lattice, 1 <= nr, nc <= 16) whose largest addend is q: adds q to
+// every bin the block touches (at most 3 x 3). All lanes of a warp call it
+// together; nr or nc <= 0 adds nothing.
+__device__ __forceinline__ void bin_block_add(const BinArgs& B, int gy, int nr, int gx, int nc,
+                                              int L, uint32_t q) {
+    int r0 = 0, c0 = 0, nrb = 0, ncb = 0;
+    if (nr > 0 && nc > 0 && q) {
+        nrb = bin_run(gy, nr, L, B.nby, &r0);
+        ncb = bin_run(gx, nc, L, B.nbx, &c0);
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        int r = r0 + i;
+        if (r >= B.nby) r -= B.nby;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            int c = c0 + j;
+            if (c >= B.nbx) c -= B.nbx;
+            bin_bound_add(B, r * B.nbx + c, (i < nrb && j < ncb) ? q : 0u);
+        }
+    }
+}
+
+// The largest addend of a whole CTA (q_of the largest |phi| over its threads,
+// pmaxb) added to every bin of a box of destination rows [b0, b1) and window
+// columns [0, wx) at lattice origin (gx0, gy0). All threads of the CTA call it;
+// `slot` is a shared word.
+__device__ __forceinline__ void bin_box_add(const BinArgs& B, int pmaxb, int b0, int b1, int wx,
+                                            int gx0, int gy0, int L, int* slot) {
+    if (threadIdx.x == 0) *slot = 0;
+    __syncthreads();
+    const int m = __reduce_max_sync(0xFFFFFFFFu, pmaxb);
+    if ((threadIdx.x & 31) == 0) atomicMax(slot, m);
+    __syncthreads();
+    const uint32_t q = q_encode(__uint_as_float((uint32_t)*slot));
+    if (q == 0u || b1 <= b0) return;
+    int gy = gy0 + b0;
+    if (gy >= L) gy -= L;
+    int r0 = 0, c0 = 0;
+    const int nr = bin_run(gy, b1 - b0, L, B.nby, &r0);
+    const int nc = bin_run(gx0, wx, L, B.nbx, &c0);
+    for (int k = threadIdx.x; k < nr * nc; k += blockDim.x) {
+        int r = r0 + k / nc, c = c0 + k % nc;
+        if (r >= B.nby) r -= B.nby;
+        if (c >= B.nbx) c -= B.nbx;
+        const unsigned long long old = atomicAdd(B.bound + r * B.nbx + c, (unsigned long long)q);
+        if (old < (1ull << 32) && old + q >= (1ull << 32)) {
+            const unsigned f = atomicAdd(B.nflag, 1u);
+            if (f < (unsigned)kMaxFlaggedBins) B.flagged[f] = (unsigned)(r * B.nbx + c);
+        }
+    }
 }
 
 // Running per-thread moments of destination pixels.
@@ -507,7 +614,7 @@ __device__ __forceinline__ void reduce_moments(const pfb_step_args2d& A, const C
         R.red_i[warp][4] = acc.pmaxb;
     }
     __syncthreads();
-    if (warp != 0) return;
+    if (warp != 0) return;  // callers that need the whole CTA afterwards re-join it
     double m[4];
     for (int k = 0; k < 4; ++k) m[k] = dev::ordered_lane_sum(lane < NW ? R.red_d[lane][k] : 0.0, NW);
     const int b0 = __reduce_min_sync(0xFFFFFFFFu, lane < NW ? R.red_i[lane][0] : P.dwx);
@@ -546,7 +653,8 @@ __device__ __forceinline__ void reduce_moments(const pfb_step_args2d& A, const C
 template <int CLS, int K, int NW, int OBS = PFB_VELOCITY_DISABLED>
 __device__ __noinline__ void global_cell(const pfb_step_args2d& A, const CellPlan& P, int rank,
                                          RedScratch<NW, K, kObsVals<OBS>>& R, bool fm,
-                                         unsigned int* status) {
+                                         unsigned int* status, const BinArgs* bins = nullptr,
+                                         int* slot = nullptr) {
     constexpr int NT = NW * 32;
     constexpr Window W = window_of(CLS);
     constexpr int WX = W.wx, WY = W.wy, TX0 = W.tx0, TY0 = W.ty0;
@@ -656,6 +764,9 @@ __device__ __noinline__ void global_cell(const pfb_step_args2d& A, const CellPla
             }
         }
     }
+    // returning adds, but the launch also has non-returning ones elsewhere:
+    // bound this CTA's destination band (the whole CTA calls it)
+    if (bins) bin_box_add(*bins, acc.pmaxb, db0, db1, P.dwx, P.gx0n, P.gy0n, L, slot);
     reduce_moments<K, NW>(A, P, rank, R, fm, acc, status);
 }
 

@@ -158,6 +158,7 @@ _SIGS = {
     "pfb_sim2d_set_cluster": (I, [P, I]),
     "pfb_sim2d_set_graph": (I, [P, I]),
     "pfb_sim2d_set_variant": (I, [P, I]),
+    "pfb_sim2d_scatter_recounts": (I, [P, C.POINTER(C.c_uint)]),
     "pfb_sim2d_set_visit_order": (I, [P, I]),
     "pfb_sim2d_visit_order": (I, [P, P]),
     "pfb_sim2d_advance": (I, [P, C.c_longlong]),

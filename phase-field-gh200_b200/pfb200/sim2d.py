@@ -159,6 +159,17 @@ class Sim2D:
         except Exception:
             pass
 
+    def set_variant(self, variant: int) -> None:
+        """0/1: non-returning scatter with exact per-bin overflow detection;
+        2: returning scatter that tests every add. Results are identical."""
+        check(lib().pfb_sim2d_set_variant(self._h, variant), "set_variant")
+
+    def scatter_recounts(self) -> int:
+        """Bins recounted exactly so far (their bound reached 2^32)."""
+        out = C.c_uint(0)
+        check(lib().pfb_sim2d_scatter_recounts(self._h, C.byref(out)), "scatter_recounts")
+        return int(out.value)
+
     def set_cluster(self, k: int) -> None:
         check(lib().pfb_sim2d_set_cluster(self._h, k), "set_cluster")
 
