@@ -34,16 +34,13 @@ int step2d_launch_variant(const pfb_step_args2d* a, int cluster, int variant,
 int step2d_launch_storage(const pfb_step_args2d* a, int cluster, int variant, int storage,
                           cudaStream_t stream);
 // Device buffers of the 2D step's exact overflow detection for non-returning
-// scatters (two alternating sets of per-bin bounds over 16 x 16 lattice bins,
-// a completion counter, two short lists of bins whose bound reached 2^32).
-// All zero when first handed to a launch.
+// scatters: two alternating sets of per-bin bounds over 16 x 16 lattice bins
+// and two alternating sets of the cells' committed window geometry
+// (gx0, gy0, class, 0). All zero when first handed to a launch.
 constexpr int kBinShift = 4;
-constexpr int kMaxFlaggedBins = 256;
 struct BinArgs {
     unsigned long long* bound;  // 2 sets of nbx * nby bounds
-    unsigned int* done;         // CTAs of the running launch finished
-    unsigned int* nflag;        // 2 counts of listed bins
-    unsigned int* flagged;      // 2 lists of kMaxFlaggedBins bin indices
+    int4* geo;                  // 2 sets of N window geometries
     unsigned int* recounts;     // bins recounted exactly so far (diagnostic)
     int nbx, nby;               // bins per lattice row and column
 };
@@ -51,6 +48,11 @@ struct BinArgs {
 // through B (binary32 or 16-bit pools, no observer).
 int step2d_launch_binned(const pfb_step_args2d* a, int cluster, int storage, const BinArgs& B,
                          cudaStream_t stream);
+// Settles the bounds of the launch that ran at `step` (the last one issued):
+// recounts every bin whose bound reached 2^32 from the field it wrote (`phi`,
+// storage 0/1/2) and raises S_overflow when some pixel total reaches 2^32.
+int step2d_settle_bins(const BinArgs& B, const void* phi, int storage, int N, int L,
+                       unsigned long long step, uint32_t* flags, cudaStream_t stream);
 // The step with a velocity observer (PFB_VELOCITY_*), binary32 pools.
 int step2d_launch_observed(const pfb_step_args2d* a, int cluster, int observation,
                            cudaStream_t stream);

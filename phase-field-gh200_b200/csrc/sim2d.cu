@@ -60,25 +60,32 @@ struct pfb_sim2d {
     uint32_t* d_perm = nullptr;  // Morton visit order (null: launch order)
     // exact overflow detection of the non-returning scatter (BinArgs)
     unsigned long long* d_bins = nullptr;
-    unsigned int* d_binctl = nullptr;  // done, 2 list counts, recounts, 2 lists
+    int4* d_geo = nullptr;             // 2 x N committed window geometries
+    unsigned int* d_recounts = nullptr;
     int nbins_side = 0;
+    bool bins_pending = false;  // the last launch's bounds are not settled yet
 
     size_t bin_words() const { return 2 * (size_t)nbins_side * (size_t)nbins_side; }
-    static constexpr size_t kBinCtlWords = 4 + 2 * kMaxFlaggedBins;
 
     BinArgs bin_args() const {
-        return BinArgs{d_bins, d_binctl, d_binctl + 1, d_binctl + 4, d_binctl + 3, nbins_side,
-                       nbins_side};
+        return BinArgs{d_bins, d_geo, d_recounts, nbins_side, nbins_side};
     }
 
-    // Both bound sets, the counter and the lists back to zero: after any
-    // change of the step counter other than a launch.
+    // Both bound sets back to zero: after any change of the step counter
+    // other than a launch.
     int reset_bins() {
         PFB_CU(cudaMemsetAsync(d_bins, 0, bin_words() * sizeof(unsigned long long), stream),
                "clear bins");
-        PFB_CU(cudaMemsetAsync(d_binctl, 0, kBinCtlWords * sizeof(unsigned int), stream),
-               "clear bins");
+        bins_pending = false;
         return PFB_OK;
+    }
+
+    // Settle the bounds of the last launch (its field is the current pool).
+    int settle_bins() {
+        if (!bins_pending) return PFB_OK;
+        bins_pending = false;
+        return step2d_settle_bins(bin_args(), d_phi[steps_done % 2], p.phi_storage, N, L,
+                                  (unsigned long long)(steps_done - 1), d_flags, stream);
     }
 
     ~pfb_sim2d() {
@@ -99,7 +106,8 @@ struct pfb_sim2d {
         cudaFree(d_perm);
         cudaFree(d_cell_prev);
         cudaFree(d_bins);
-        cudaFree(d_binctl);
+        cudaFree(d_geo);
+        cudaFree(d_recounts);
         cudaFree(b_phi);
         cudaFree(b_cell);
         cudaFree(b_cls);
@@ -196,8 +204,12 @@ struct pfb_sim2d {
         if (const int rc = sort_visit_order(slot)) return rc;
         const pfb_step_args2d a = args_for_slot(slot);
         // the driver owns bin buffers: non-returning scatter, overflow exact
-        if (variant == 0 || variant == 1)
+        if (variant == 0 || variant == 1) {
+            bins_pending = true;
             return step2d_launch_binned(&a, cluster, p.phi_storage, bin_args(), stream);
+        }
+        // a returning-scatter step settles nothing: settle the last binned one first
+        if (const int rc = settle_bins()) return rc;
         return step2d_launch_storage(&a, cluster, 1, p.phi_storage, stream);
     }
 
@@ -220,9 +232,11 @@ struct pfb_sim2d {
 
     int build_graph() {
         drop_graph();
+        if (const int rc = settle_bins()) return rc;  // capture marks nothing as run
         PFB_CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
         int rc = PFB_OK;
         for (int s = 0; s < 6 && rc == PFB_OK; ++s) rc = launch_one(s);
+        bins_pending = false;
         cudaGraph_t g = nullptr;
         const cudaError_t e = cudaStreamEndCapture(stream, &g);
         if (rc != PFB_OK) {
@@ -263,6 +277,7 @@ struct pfb_sim2d {
             }
             if (use_graph && graph_ready && steps_done % 6 == 0 && steps >= 6) {
                 PFB_CU(cudaGraphLaunch(graph_exec, stream), "graph launch");
+                bins_pending = variant == 0 || variant == 1;
                 steps_done += 6;
                 steps -= 6;
             } else {
@@ -272,7 +287,9 @@ struct pfb_sim2d {
                 steps -= 1;
             }
         }
-        return PFB_OK;
+        // nothing stays pending across calls: the caller may read flags or
+        // change the field next
+        return settle_bins();
     }
 
     // Allocate every device buffer for p (reference src/sim.cu:159-232).
@@ -301,8 +318,11 @@ struct pfb_sim2d {
         PFB_CU(cudaMalloc(&d_cell_prev, (size_t)N * sizeof(pfb_cell2d)), "alloc cells");
         nbins_side = (L + (1 << kBinShift) - 1) >> kBinShift;
         PFB_CU(cudaMalloc(&d_bins, bin_words() * sizeof(unsigned long long)), "alloc bins");
-        PFB_CU(cudaMalloc(&d_binctl, kBinCtlWords * sizeof(unsigned int)), "alloc bins");
+        PFB_CU(cudaMalloc(&d_geo, 2 * (size_t)N * sizeof(int4)), "alloc bins");
+        PFB_CU(cudaMalloc(&d_recounts, sizeof(unsigned int)), "alloc bins");
         PFB_CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
+        PFB_CU(cudaMemsetAsync(d_recounts, 0, sizeof(unsigned int), stream), "clear bins");
+        PFB_CU(cudaMemsetAsync(d_geo, 0, 2 * (size_t)N * sizeof(int4), stream), "clear bins");
         if (const int rc = reset_bins()) return rc;
         PFB_CU(cudaMemsetAsync(d_cursor, 0, 2 * sizeof(unsigned long long), stream), "memset");
         PFB_CU(cudaMemsetAsync(d_step, 0, 2 * sizeof(unsigned long long), stream), "memset");
@@ -673,7 +693,7 @@ int pfb_sim2d_set_variant(pfb_sim2d* s, int variant) {
 int pfb_sim2d_scatter_recounts(pfb_sim2d* s, unsigned int* out) {
     if (!s || !out) return set_error(PFB_E_ARG, "scatter_recounts: null argument");
     PFB_CU(cudaSetDevice(s->device), "cudaSetDevice");
-    PFB_CU(cudaMemcpyAsync(out, s->d_binctl + 3, sizeof(unsigned int), cudaMemcpyDeviceToHost,
+    PFB_CU(cudaMemcpyAsync(out, s->d_recounts, sizeof(unsigned int), cudaMemcpyDeviceToHost,
                            s->stream),
            "read recounts");
     PFB_CU(cudaStreamSynchronize(s->stream), "read recounts");
@@ -1190,7 +1210,7 @@ int sim2d_step_keep_prev(pfb_sim2d* s) {
     const int rc = s->launch_one((int)(s->steps_done % 6));
     if (rc) return rc;
     s->steps_done += 1;
-    return PFB_OK;
+    return s->settle_bins();
 }
 
 }  // namespace pfb

@@ -26,6 +26,7 @@
 // The grid is N*K CTAs; a cell is owned by one cluster for the whole step.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "device_util.cuh"
@@ -203,7 +204,7 @@ __device__ __forceinline__ void store_zero(T* o) {
 template <int CLS, int K, typename T, int OBS, bool BINS = false>
 __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int rank,
                                             char* smem, unsigned long long step, bool fm,
-                                            const BinArgs* bins = nullptr) {
+                                            const BinArgs& B) {
     constexpr Window W = window_of(CLS);
     constexpr int WX = W.wx, WY = W.wy, TX0 = W.tx0, TY0 = W.ty0;
     constexpr int RB = band_rows(WY, K);
@@ -540,7 +541,8 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
                 if constexpr (BINS) {
                     int gys = gy0 + y0 + r0;
                     if (gys >= L) gys -= L;
-                    bin_block_add(*bins, gys, nr, gxj[0], 4, L, q_encode(__uint_as_float(pmaxb)));
+                    bin_block_add(gy0 >> kBinShift, gx0 >> kBinShift, B.nbx, B.nby, gys, nr,
+                                  gxj[0], 4, L, q_encode(__uint_as_float(pmaxb)));
                 } else {
                     bool ovf = false;
 #pragma unroll
@@ -595,7 +597,8 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
                     int gys = gy0n + ba, gxs = gx0n + aa;
                     if (gys >= L) gys -= L;
                     if (gxs >= L) gxs -= L;
-                    bin_block_add(*bins, gys, bb - ba, gxs, ab - aa, L,
+                    bin_block_add(gy0n >> kBinShift, gx0n >> kBinShift, B.nbx, B.nby, gys,
+                                  bb - ba, gxs, ab - aa, L,
                                   q_encode(__uint_as_float((uint32_t)acc.pmaxb)));
                 }
             }
@@ -694,88 +697,20 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
 template <int CLS, int K, int OBS>
 __device__ __forceinline__ void global_cell_v1(const pfb_step_args2d& A, int n, int rank,
                                                char* smem, unsigned long long step, bool fm,
-                                               const BinArgs* bins = nullptr) {
+                                               unsigned long long* bound = nullptr, int nbx = 0,
+                                               int nby = 0) {
     StepShared<K, OBS>& sh = *reinterpret_cast<StepShared<K, OBS>*>(smem);
     if (threadIdx.x == 0)
         plan_cell<OBS == PFB_VELOCITY_SPATIAL>(A, n, CLS, step, sh.plan, rank == 0);
     __syncthreads();
-    global_cell<CLS, K, kWarps, OBS>(A, sh.plan, rank, sh.red, fm, &g_step2d_status, bins,
-                                     &sh.abort);
-}
-
-// ---- end of a launch that scattered with non-returning adds ------------------
-// Every CTA counts itself done (after a CTA barrier and a gpu-scope fence, so
-// its scatters, bounds and commits are visible); the CTA that completes the
-// count resets it and recounts each listed bin exactly: 64-bit sums of q over the committed
-// windows of every cell (phi_out, cell records), S_overflow when one reaches
-// 2^32. A list that overflowed makes it scan every bound of the set.
-template <typename T>
-__device__ __noinline__ void bins_finish(const pfb_step_args2d& A, const BinArgs& Bc,
-                                         char* smem) {
-    __shared__ int last;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        const unsigned old = atomicAdd(Bc.done, 1u);
-        last = old + 1u == gridDim.x;
-        if (last) *Bc.done = 0u;  // every other CTA has counted itself
-    }
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    const unsigned listed = *reinterpret_cast<volatile unsigned*>(Bc.nflag);
-    if (listed == 0u) return;
-    unsigned long long* acc = reinterpret_cast<unsigned long long*>(smem);  // 256 pixels
-    const int L = A.L, nbins = Bc.nbx * Bc.nby;
-    const bool scan = listed > (unsigned)kMaxFlaggedBins;
-    const int items = scan ? nbins : (int)listed;
-    for (int it = 0; it < items; ++it) {
-        int bin;
-        if (scan) {
-            if (Bc.bound[it] < (1ull << 32)) continue;  // uniform: every thread reads it
-            bin = it;
-        } else {
-            bin = (int)Bc.flagged[it];
-        }
-        for (int k = threadIdx.x; k < 256; k += blockDim.x) acc[k] = 0ull;
-        __syncthreads();
-        const int px0 = (bin % Bc.nbx) << kBinShift, py0 = (bin / Bc.nbx) << kBinShift;
-        const int w = min(16, L - px0), h = min(16, L - py0);
-        for (int c = threadIdx.x; c < A.N; c += blockDim.x) {
-            const Window W = window_of((int)A.cell_cls[c]);
-            const int gx0 = A.cell[c].gx0, gy0 = A.cell[c].gy0;
-            const T* tile = reinterpret_cast<const T*>(A.phi_out) + (size_t)c * kTileArea;
-            for (int j = 0; j < h; ++j) {
-                int b = py0 + j - gy0;
-                if (b < 0) b += L;
-                if (b >= W.wy) continue;
-                for (int i = 0; i < w; ++i) {
-                    int a = px0 + i - gx0;
-                    if (a < 0) a += L;
-                    if (a >= W.wx) continue;
-                    const T raw = tile[(size_t)(W.ty0 + b) * kTilePitch + W.tx0 + a];
-                    float v;
-                    if constexpr (Store<T>::kHalf)
-                        v = Store<T>::value(*reinterpret_cast<const uint16_t*>(&raw));
-                    else
-                        v = raw;
-                    const uint32_t q = q_encode(v);
-                    if (q) atomicAdd(acc + j * 16 + i, (unsigned long long)q);
-                }
-            }
-        }
-        __syncthreads();
-        bool over = false;
-        for (int k = threadIdx.x; k < 256; k += blockDim.x) over |= acc[k] >= (1ull << 32);
-        if (__syncthreads_or(over) && threadIdx.x == 0) atomicOr(A.flags + PFB_FLAG_S_OVERFLOW, 1u);
-        if (threadIdx.x == 0) atomicAdd(Bc.recounts, 1u);
-    }
-    if (threadIdx.x == 0) *Bc.nflag = 0u;
+    global_cell<CLS, K, kWarps, OBS>(A, sh.plan, rank, sh.red, fm, &g_step2d_status, bound, nbx,
+                                     nby, &sh.abort);
 }
 
 // One system's step for CTA `lb` of the `nb` CTAs that serve it. BINS: the
 // identity path scatters without returns under per-bin bounds (B holds both
-// sets; this launch uses set step & 1 and clears the other).
+// sets; this launch bounds into set step & 1, and settles and clears the set
+// of the previous launch, which has finished).
 template <int K, typename T, int OBS = PFB_VELOCITY_DISABLED, bool BINS = false>
 __device__ __forceinline__ void step_body(const pfb_step_args2d& A, int lb, int nb, char* smem,
                                           const BinArgs& B = BinArgs{}) {
@@ -796,38 +731,38 @@ __device__ __forceinline__ void step_body(const pfb_step_args2d& A, int lb, int 
         *A.step_wr = step + 1ull;
     }
     const bool fm = full_moment_step(A, step);
-    BinArgs Bc{};
     if constexpr (BINS) {
         const int nbins = B.nbx * B.nby;
         const int par = (int)(step & 1ull);
-        Bc = BinArgs{B.bound + (size_t)par * nbins, B.done, B.nflag + par,
-                     B.flagged + (size_t)par * kMaxFlaggedBins, B.recounts, B.nbx, B.nby};
-        unsigned long long* other = B.bound + (size_t)(1 - par) * nbins;
-        for (int i = lb * kThreads + tid; i < nbins; i += nb * kThreads) other[i] = 0ull;
+        // the previous launch's bounds: check (recounting the rare bin at
+        // 2^32) and clear them for the next launch; its field is our phi_in
+        for (int first = lb * kThreads; first < nbins; first += nb * kThreads)
+            bin_settle_chunk<T>(B.bound + (size_t)(1 - par) * nbins, B.geo + (size_t)(1 - par) * A.N,
+                                reinterpret_cast<const T*>(A.phi_in), A.N, A.L, B.nbx, first,
+                                min(kThreads, nbins - first), A.flags, B.recounts, smem);
+        for (int k = tid; k < kBinTab * kBinTab; k += kThreads) g_bintab[k] = 0u;
     }
-    // bounds are only needed where a non-returning scatter happens: the
-    // identity path, which full-moment steps never take
-    const BinArgs* bins = (BINS && !fm) ? &Bc : nullptr;
 
     const int rank = (int)dev::cluster_rank();
     StepShared<K, OBS>& sh = *reinterpret_cast<StepShared<K, OBS>*>(smem);
     if (tid == 0) red_init(sh.red, rank);
+    if (BINS && tid == 0) sh.plan.n = -1;  // set when the cell's step is planned
     dev::cluster_arrive_relaxed();  // matched by the wait in reduce_force
     const int slot = lb / K;
     const int n = A.perm ? (int)A.perm[slot] : slot;
     const int cls = (int)A.cell_cls[n];
     switch (cls) {
-        case 0: staged_cell<0, K, T, OBS, BINS>(A, n, rank, smem, step, fm, bins); break;
-        case 1: staged_cell<1, K, T, OBS, BINS>(A, n, rank, smem, step, fm, bins); break;
-        case 2: staged_cell<2, K, T, OBS, BINS>(A, n, rank, smem, step, fm, bins); break;
-        case 3: staged_cell<3, K, T, OBS, BINS>(A, n, rank, smem, step, fm, bins); break;
+        case 0: staged_cell<0, K, T, OBS, BINS>(A, n, rank, smem, step, fm, B); break;
+        case 1: staged_cell<1, K, T, OBS, BINS>(A, n, rank, smem, step, fm, B); break;
+        case 2: staged_cell<2, K, T, OBS, BINS>(A, n, rank, smem, step, fm, B); break;
+        case 3: staged_cell<3, K, T, OBS, BINS>(A, n, rank, smem, step, fm, B); break;
         case 4:
             if constexpr (Store<T>::kHalf) {
                 // 16-bit pools: the global-memory classes are not provided
                 if (rank == 0 && tid == 0) atomicAdd(A.flags + PFB_FLAG_CLASS_UNSUPPORTED, 1u);
                 dev::cluster_wait();
             } else {
-                global_cell_v1<4, K, OBS>(A, n, rank, smem, step, fm, bins);
+                global_cell_v1<4, K, OBS>(A, n, rank, smem, step, fm, BINS && !fm ? B.bound + (size_t)(step & 1ull) * B.nbx * B.nby : nullptr, B.nbx, B.nby);
             }
             break;
         case 5:
@@ -835,7 +770,7 @@ __device__ __forceinline__ void step_body(const pfb_step_args2d& A, int lb, int 
                 if (rank == 0 && tid == 0) atomicAdd(A.flags + PFB_FLAG_CLASS_UNSUPPORTED, 1u);
                 dev::cluster_wait();
             } else {
-                global_cell_v1<5, K, OBS>(A, n, rank, smem, step, fm, bins);
+                global_cell_v1<5, K, OBS>(A, n, rank, smem, step, fm, BINS && !fm ? B.bound + (size_t)(step & 1ull) * B.nbx * B.nby : nullptr, B.nbx, B.nby);
             }
             break;
         default:
@@ -843,7 +778,21 @@ __device__ __forceinline__ void step_body(const pfb_step_args2d& A, int lb, int 
             dev::cluster_wait();  // uniform over the cluster
             break;
     }
-    if constexpr (BINS) bins_finish<T>(A, Bc, smem);
+    if constexpr (BINS) {
+        // the shared table into this launch's bounds; the committed window
+        // geometry for the launch that will settle them (everything read
+        // again here rather than kept live through the passes)
+        __syncthreads();
+        const CellPlan& P = reinterpret_cast<StepShared<K, OBS>*>(smem)->plan;
+        if (P.n >= 0) {
+            const unsigned long long st = *A.step_rd;
+            unsigned long long* set = B.bound + (size_t)(st & 1ull) * B.nbx * B.nby;
+            if (!full_moment_step(A, st))
+                bin_table_flush(set, P.gy0n >> kBinShift, P.gx0n >> kBinShift, B.nbx, B.nby);
+            if (dev::cluster_rank() == 0 && threadIdx.x == 0)
+                B.geo[(size_t)(st & 1ull) * A.N + P.n] = make_int4(P.gx0n, P.gy0n, P.dcls, 0);
+        }
+    }
 }
 
 template <int K, typename T = float, int OBS = PFB_VELOCITY_DISABLED, bool BINS = false>
@@ -1018,7 +967,7 @@ int step2d_launch_binned(const pfb_step_args2d* a, int cluster, int storage,
     if (rc) return rc;
     const pfb_step_args2d& A = *a;
     if (A.moments) return set_error(PFB_E_ARG, "moments are read by the observed launch only");
-    if (!B.bound || !B.done || !B.nflag || !B.flagged)
+    if (!B.bound || !B.geo || !B.recounts)
         return set_error(PFB_E_ARG, "binned launch without its bin buffers");
     if (B.nbx != (A.L + (1 << kBinShift) - 1) >> kBinShift || B.nby != B.nbx)
         return set_error(PFB_E_ARG, "bin grid does not match the lattice side");
@@ -1044,6 +993,39 @@ int step2d_launch_binned(const pfb_step_args2d* a, int cluster, int storage,
             : cluster == 4 ? launch_k<4, float, D, true>(A, stream, B)
                            : launch_k<8, float, D, true>(A, stream, B);
     if (e != cudaSuccess) return set_error(PFB_E_CUDA, "step launch: %s", cudaGetErrorString(e));
+    return PFB_OK;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+    k_settle_bins2d(const __grid_constant__ BinArgs B, const T* phi, int N, int L,
+                    unsigned long long step, uint32_t* flags) {
+    __shared__ __align__(16) char scratch[256 * sizeof(unsigned long long) + (kThreads + 1) * 4];
+    const int nbins = B.nbx * B.nby;
+    const int par = (int)(step & 1ull);
+    for (int first = blockIdx.x * kThreads; first < nbins; first += gridDim.x * kThreads)
+        bin_settle_chunk<T>(B.bound + (size_t)par * nbins, B.geo + (size_t)par * N, phi, N, L,
+                            B.nbx, first, min(kThreads, nbins - first), flags, B.recounts,
+                            scratch);
+}
+
+int step2d_settle_bins(const BinArgs& B, const void* phi, int storage, int N, int L,
+                       unsigned long long step, uint32_t* flags, cudaStream_t stream) {
+    if (!B.bound || !B.geo || !B.recounts || !phi || !flags || N <= 0)
+        return set_error(PFB_E_ARG, "settle_bins: bad arguments");
+    const int nbins = B.nbx * B.nby;
+    const int grid = std::min(148 * 2, (nbins + kThreads - 1) / kThreads);
+    if (storage == kStoreF16)
+        k_settle_bins2d<__half><<<grid, kThreads, 0, stream>>>(B, static_cast<const __half*>(phi), N,
+                                                              L, step, flags);
+    else if (storage == kStoreBF16)
+        k_settle_bins2d<__nv_bfloat16><<<grid, kThreads, 0, stream>>>(
+            B, static_cast<const __nv_bfloat16*>(phi), N, L, step, flags);
+    else
+        k_settle_bins2d<float><<<grid, kThreads, 0, stream>>>(B, static_cast<const float*>(phi), N,
+                                                             L, step, flags);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_error(PFB_E_CUDA, "settle_bins: %s", cudaGetErrorString(e));
     return PFB_OK;
 }
 

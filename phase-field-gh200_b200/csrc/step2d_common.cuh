@@ -9,6 +9,7 @@
 #include "device_util.cuh"
 #include "pfb_common.cuh"
 #include "pfb_internal.h"
+#include "storage2d.cuh"
 
 namespace pfb {
 
@@ -175,16 +176,16 @@ __device__ __forceinline__ bool full_moment_step(const pfb_step_args2d& A,
 // sum at a pixel crosses 2^32 - 1 (the reference's S_overflow test on each
 // returning atomicAdd, src/kernels.cu:496-497) exactly when the pixel's final
 // total T(p) does, whatever the order of the adds. A launch that scatters with
-// non-returning red.add keeps, per 16 x 16 lattice bin, an upper bound of
-// T(p) over the bin: every scatter adds the largest addend it put into the bin
-// (warp-aggregated). The last CTA of the launch scans the bins; only a bin whose
-// bound reaches 2^32 is recounted exactly (64-bit sums of q over the committed
-// windows of every cell), and S_overflow is raised iff some T(p) >= 2^32.
-// Two sets of bins alternate by step parity: a launch bounds into set
-// (step & 1) and clears the other set for the next launch, so nothing is ever
-// cleared on the host. A bound's first crossing of 2^32 appends its bin to the
-// set's short list, so the last CTA normally has nothing to scan.
-// (BinArgs, kBinShift and kMaxFlaggedBins: pfb_internal.h)
+// non-returning red.add keeps, per 16 x 16 lattice bin, an upper bound of T(p)
+// over the bin: each CTA gathers the largest addend of each strip into a
+// shared table over its destination window's bins (atomicMax) and adds the
+// table to the global bounds with non-returning adds at its end. The next
+// launch, which starts only when this one has finished, checks these bounds
+// while it clears them: a bin at or above 2^32 is recounted exactly (64-bit
+// sums of q of the field this launch wrote, over the windows this launch
+// committed, kept per step parity in `geo`) and S_overflow is raised iff some
+// T(p) >= 2^32. The driver settles the last launch of a run the same way.
+constexpr int kBinTab = 16;  // the shared table is kBinTab x kBinTab bins
 
 __device__ __forceinline__ void red_add_nonzero(uint32_t* p, uint32_t v) {
     asm volatile(
@@ -195,21 +196,10 @@ __device__ __forceinline__ void red_add_nonzero(uint32_t* p, uint32_t v) {
         : "memory");
 }
 
-// Adds q to the bound of `bin` from the calling lanes, one atomic per distinct
-// bin among them (the largest q of the group); q == 0 adds nothing.
-__device__ __forceinline__ void bin_bound_add(const BinArgs& B, int bin, uint32_t q) {
-    const unsigned act = __activemask();
-    const unsigned key = q ? (unsigned)bin : 0xFFFFFFFFu;
-    const unsigned grp = __match_any_sync(act, key);
-    const uint32_t mx = __reduce_max_sync(grp, q);
-    if (q && (int)(__ffs(grp) - 1) == (int)(threadIdx.x & 31)) {
-        const unsigned long long old = atomicAdd(B.bound + bin, (unsigned long long)mx);
-        if (old < (1ull << 32) && old + mx >= (1ull << 32)) {
-            const unsigned k = atomicAdd(B.nflag, 1u);
-            if (k < (unsigned)kMaxFlaggedBins) B.flagged[k] = (unsigned)bin;
-        }
-    }
-}
+// Per-CTA table of the largest addend per bin over the destination window
+// (kBinTab x kBinTab bins from the bin holding the window origin), filled with
+// shared atomicMax and added to the launch's bounds at the CTA's end.
+__shared__ unsigned int g_bintab[kBinTab * kBinTab];
 
 // Forward cyclic run of bins touched by lattice rows (or columns) g .. g+n-1
 // (0 <= g < L, 1 <= n < L): first bin and count. The last bin of a side that
@@ -219,39 +209,51 @@ __device__ __forceinline__ int bin_run(int g, int n, int L, int nb, int* first) 
     if (g1 >= L) g1 -= L;
     const int a = g >> kBinShift, b = g1 >> kBinShift;
     *first = a;
-    return (b - a + nb) % nb + 1;
+    return b >= a ? b - a + 1 : b - a + nb + 1;
 }
 
 // A block of destination pixels (rows gy .. gy+nr-1, columns gx .. gx+nc-1 of
-// the periodic lattice, 1 <= nr, nc <= 16) whose largest addend is q: adds q to
-// every bin the block touches (at most 3 x 3). All lanes of a warp call it
-// together; nr or nc <= 0 adds nothing.
-__device__ __forceinline__ void bin_block_add(const BinArgs& B, int gy, int nr, int gx, int nc,
-                                              int L, uint32_t q) {
-    int r0 = 0, c0 = 0, nrb = 0, ncb = 0;
-    if (nr > 0 && nc > 0 && q) {
-        nrb = bin_run(gy, nr, L, B.nby, &r0);
-        ncb = bin_run(gx, nc, L, B.nbx, &c0);
-    }
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        int r = r0 + i;
-        if (r >= B.nby) r -= B.nby;
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            int c = c0 + j;
-            if (c >= B.nbx) c -= B.nbx;
-            bin_bound_add(B, r * B.nbx + c, (i < nrb && j < ncb) ? q : 0u);
-        }
+// the periodic lattice, nr, nc <= 16) of a destination window whose origin
+// lies in bin (tr0, tc0), largest addend q: q raises every bin the block
+// touches (at most 3 x 3) in the shared table. A window of a staged class
+// (at most 176 pixels a side) spans at most 13 bins a side, so every bin has
+// a table entry.
+__device__ __forceinline__ void bin_block_add(int tr0, int tc0, int nbx, int nby, int gy, int nr,
+                                              int gx, int nc, int L, uint32_t q) {
+    if (nr <= 0 || nc <= 0 || q == 0u) return;
+    int r0 = 0, c0 = 0;
+    const int nrb = bin_run(gy, nr, L, nby, &r0);
+    const int ncb = bin_run(gx, nc, L, nbx, &c0);
+    int lr = r0 - tr0;
+    if (lr < 0) lr += nby;
+    int lc0 = c0 - tc0;
+    if (lc0 < 0) lc0 += nbx;
+    for (int i = 0; i < nrb; ++i, ++lr)
+        for (int j = 0, lc = lc0; j < ncb; ++j, ++lc)
+            if (lr < kBinTab && lc < kBinTab) atomicMax(g_bintab + lr * kBinTab + lc, q);
+}
+
+// The shared table added to the bounds `set` (non-returning adds). All
+// threads of the CTA call it after a CTA barrier.
+__device__ __forceinline__ void bin_table_flush(unsigned long long* set, int tr0, int tc0, int nbx,
+                                                int nby) {
+    for (int k = threadIdx.x; k < kBinTab * kBinTab; k += blockDim.x) {
+        const unsigned q = g_bintab[k];
+        if (!q) continue;
+        int r = tr0 + k / kBinTab, c = tc0 + k % kBinTab;
+        if (r >= nby) r -= nby;
+        if (c >= nbx) c -= nbx;
+        atomicAdd(set + r * nbx + c, (unsigned long long)q);
     }
 }
 
 // The largest addend of a whole CTA (q_of the largest |phi| over its threads,
 // pmaxb) added to every bin of a box of destination rows [b0, b1) and window
-// columns [0, wx) at lattice origin (gx0, gy0). All threads of the CTA call it;
-// `slot` is a shared word.
-__device__ __forceinline__ void bin_box_add(const BinArgs& B, int pmaxb, int b0, int b1, int wx,
-                                            int gx0, int gy0, int L, int* slot) {
+// columns [0, wx) at lattice origin (gx0, gy0), straight into the global
+// bounds. All threads of the CTA call it; `slot` is a shared word.
+__device__ __forceinline__ void bin_box_add(unsigned long long* bound, int nbx, int nby,
+                                            int pmaxb, int b0, int b1, int wx, int gx0, int gy0,
+                                            int L, int* slot) {
     if (threadIdx.x == 0) *slot = 0;
     __syncthreads();
     const int m = __reduce_max_sync(0xFFFFFFFFu, pmaxb);
@@ -262,17 +264,102 @@ __device__ __forceinline__ void bin_box_add(const BinArgs& B, int pmaxb, int b0,
     int gy = gy0 + b0;
     if (gy >= L) gy -= L;
     int r0 = 0, c0 = 0;
-    const int nr = bin_run(gy, b1 - b0, L, B.nby, &r0);
-    const int nc = bin_run(gx0, wx, L, B.nbx, &c0);
+    const int nr = bin_run(gy, b1 - b0, L, nby, &r0);
+    const int nc = bin_run(gx0, wx, L, nbx, &c0);
     for (int k = threadIdx.x; k < nr * nc; k += blockDim.x) {
         int r = r0 + k / nc, c = c0 + k % nc;
-        if (r >= B.nby) r -= B.nby;
-        if (c >= B.nbx) c -= B.nbx;
-        const unsigned long long old = atomicAdd(B.bound + r * B.nbx + c, (unsigned long long)q);
-        if (old < (1ull << 32) && old + q >= (1ull << 32)) {
-            const unsigned f = atomicAdd(B.nflag, 1u);
-            if (f < (unsigned)kMaxFlaggedBins) B.flagged[f] = (unsigned)(r * B.nbx + c);
+        if (r >= nby) r -= nby;
+        if (c >= nbx) c -= nbx;
+        atomicAdd(bound + r * nbx + c, (unsigned long long)q);
+    }
+}
+
+// Exact recount of bin `bin` of a launch's bounds: 64-bit totals of q over the
+// windows `geo` (that launch's commits) of the field `phi` it wrote; returns
+// true when some total reaches 2^32. All threads of the CTA call it; `acc` is
+// 256 shared 64-bit words.
+template <typename T>
+__device__ __noinline__ bool bin_recount(const T* phi, const int4* geo, int N, int L, int nbx,
+                                         int bin, unsigned long long* acc) {
+    for (int k = threadIdx.x; k < 256; k += blockDim.x) acc[k] = 0ull;
+    __syncthreads();
+    const int px0 = (bin % nbx) << kBinShift, py0 = (bin / nbx) << kBinShift;
+    const int w = min(16, L - px0), h = min(16, L - py0);
+    for (int c = threadIdx.x; c < N; c += blockDim.x) {
+        const int4 g = geo[c];
+        const Window W = window_of(g.z);
+        const T* tile = phi + (size_t)c * kTileArea;
+        for (int j = 0; j < h; ++j) {
+            int b = py0 + j - g.y;
+            if (b < 0) b += L;
+            if (b >= W.wy) continue;
+            for (int i = 0; i < w; ++i) {
+                int a = px0 + i - g.x;
+                if (a < 0) a += L;
+                if (a >= W.wx) continue;
+                const T raw = tile[(size_t)(W.ty0 + b) * kTilePitch + W.tx0 + a];
+                float v;
+                if constexpr (sizeof(T) == 2)
+                    v = Store<T>::value(*reinterpret_cast<const uint16_t*>(&raw));
+                else
+                    v = raw;
+                const uint32_t q = q_encode(v);
+                if (q) atomicAdd(acc + j * 16 + i, (unsigned long long)q);
+            }
         }
+    }
+    __syncthreads();
+    bool over = false;
+    for (int k = threadIdx.x; k < 256; k += blockDim.x) over |= acc[k] >= (1ull << 32);
+    return __syncthreads_or(over) != 0;
+}
+
+template <typename T>
+__device__ __noinline__ void bin_settle_hot(unsigned long long* bound, const int4* geo,
+                                            const T* phi, int N, int L, int nbx, int i, bool hot,
+                                            uint32_t* flags, unsigned int* recounts,
+                                            char* scratch);
+
+// Checks and clears bins [first, first + count) of a finished launch's bounds
+// (count <= blockDim.x), recounting those at or above 2^32. All threads of the
+// CTA call it; `scratch` holds 256 64-bit words and an int list of blockDim.x.
+template <typename T>
+__device__ void bin_settle_chunk(unsigned long long* bound, const int4* geo, const T* phi, int N,
+                                 int L, int nbx, int first, int count, uint32_t* flags,
+                                 unsigned int* recounts, char* scratch) {
+    const int i = first + (int)threadIdx.x;
+    bool hot = false;
+    if ((int)threadIdx.x < count) {
+        const unsigned long long v = bound[i];
+        if (v) {
+            hot = v >= (1ull << 32);
+            bound[i] = 0ull;
+        }
+    }
+    if (!__syncthreads_or(hot)) return;
+    bin_settle_hot<T>(bound, geo, phi, N, L, nbx, i, hot, flags, recounts, scratch);
+}
+
+// The rare part of bin_settle_chunk: recount the chunk's hot bins one by one.
+template <typename T>
+__device__ __noinline__ void bin_settle_hot(unsigned long long* bound, const int4* geo,
+                                            const T* phi, int N, int L, int nbx, int i, bool hot,
+                                            uint32_t* flags, unsigned int* recounts,
+                                            char* scratch) {
+    unsigned long long* acc = reinterpret_cast<unsigned long long*>(scratch);
+    int* list = reinterpret_cast<int*>(scratch + 256 * sizeof(unsigned long long));
+    int* nlist = list + blockDim.x;
+    if (threadIdx.x == 0) *nlist = 0;
+    __syncthreads();
+    if (hot) list[atomicAdd(nlist, 1)] = i;
+    __syncthreads();
+    const int n = *nlist;
+    for (int k = 0; k < n; ++k) {
+        const int bin = list[k];
+        if (bin_recount<T>(phi, geo, N, L, nbx, bin, acc) && threadIdx.x == 0)
+            atomicOr(flags + PFB_FLAG_S_OVERFLOW, 1u);
+        if (threadIdx.x == 0) atomicAdd(recounts, 1u);
+        __syncthreads();
     }
 }
 
@@ -653,8 +740,9 @@ __device__ __forceinline__ void reduce_moments(const pfb_step_args2d& A, const C
 template <int CLS, int K, int NW, int OBS = PFB_VELOCITY_DISABLED>
 __device__ __noinline__ void global_cell(const pfb_step_args2d& A, const CellPlan& P, int rank,
                                          RedScratch<NW, K, kObsVals<OBS>>& R, bool fm,
-                                         unsigned int* status, const BinArgs* bins = nullptr,
-                                         int* slot = nullptr) {
+                                         unsigned int* status,
+                                         unsigned long long* bound = nullptr, int nbx = 0,
+                                         int nby = 0, int* slot = nullptr) {
     constexpr int NT = NW * 32;
     constexpr Window W = window_of(CLS);
     constexpr int WX = W.wx, WY = W.wy, TX0 = W.tx0, TY0 = W.ty0;
@@ -766,7 +854,7 @@ __device__ __noinline__ void global_cell(const pfb_step_args2d& A, const CellPla
     }
     // returning adds, but the launch also has non-returning ones elsewhere:
     // bound this CTA's destination band (the whole CTA calls it)
-    if (bins) bin_box_add(*bins, acc.pmaxb, db0, db1, P.dwx, P.gx0n, P.gy0n, L, slot);
+    if (bound) bin_box_add(bound, nbx, nby, acc.pmaxb, db0, db1, P.dwx, P.gx0n, P.gy0n, L, slot);
     reduce_moments<K, NW>(A, P, rank, R, fm, acc, status);
 }
 
