@@ -42,6 +42,16 @@ WORKLOAD = ("2D periodic 2048x2048, 1024 cells R=12, min-separation 2R sequentia
             "tanh disks, default coefficients (dt=0.01, lambda=7, kappa=10, mu=1, xi=1500, "
             "tau=1e4, v_A=0.01, M=0.5), f32 phi, Q5.27 aggregate")
 FALLBACK_HBM_GBS = 6650.0
+# the 2D single-system workloads: side, cells, description, L2 statement
+WORKLOADS_2D = {
+    "c2": (L_SIDE, N_CELLS, WORKLOAD,
+           "inputs larger than L2: two 340 MB phi pools; per-step working set 85 MB phi read + "
+           "85 MB phi written + 3 x 16.8 MB aggregate slots; no flush between steps"),
+    "c1": (512, 64, WORKLOAD.replace("2048x2048, 1024 cells", "512x512, 64 cells"),
+           "the whole state (two 21 MB phi pools, three 1 MB aggregate slots) fits in the 126 MB "
+           "L2, so a 256 MiB buffer is written before every timed step and each step is timed "
+           "alone (CUDA events around it); the L2-resident graph replay is reported beside it"),
+}
 
 
 def rank_env():
@@ -66,9 +76,10 @@ def whole_job_rate(sites_per_rank_step: int, steps: int, world: int, max_ms: flo
     return world * sites_per_rank_step * steps / (max_ms / 1000.0)
 
 
-def workload_params(seed: int):
+def workload_params(seed: int, wl: str = "c2"):
     from pfb200.sim2d import SimParams2D
-    return SimParams2D(L=L_SIDE, num_cells=N_CELLS, target_radius=RADIUS, seed=seed)
+    L, N = WORKLOADS_2D[wl][:2]
+    return SimParams2D(L=L, num_cells=N, target_radius=RADIUS, seed=seed)
 
 
 def workload_centres(p):
@@ -157,10 +168,10 @@ def read_peak_hbm():
         return FALLBACK_HBM_GBS, "fallback 6.65 TB/s"
 
 
-def read_ncu_traffic():
+def read_ncu_traffic(wl: str = "c2"):
     """DRAM bytes per launch of the step kernel from the committed ncu summary
-    of the same workload (profiles/k_step2d_c2.md), or None."""
-    f = REPO / "profiles" / "k_step2d_c2.md"
+    of the same workload (profiles/k_step2d_<workload>.md), or None."""
+    f = REPO / "profiles" / f"k_step2d_{wl}.md"
     if not f.exists():
         return None
     for ln in f.read_text().splitlines():
@@ -172,13 +183,13 @@ def read_ncu_traffic():
     return None
 
 
-def oracle_workload_state(seed: int):
-    """The c2 workload's initial state built by the oracle alone (placement,
+def oracle_workload_state(seed: int, wl: str = "c2"):
+    """A 2D workload's initial state built by the oracle alone (placement,
     fresh-start draws and tanh seeds restated from the reference's host code
     and k_init_tiles), so the CPU legs load no library of this package."""
     sys.path.insert(0, str(REPO / "oracle"))
     import oracle2d
-    p = workload_params(seed)
+    p = workload_params(seed, wl)
     cx, cy = oracle2d.palmieri_centres(p.num_cells, p.L, 2.0 * p.target_radius, p.seed)
     cells, phi = oracle2d.init_state(p.to_c(), cx, cy, oracle2d.fresh_cells(p.to_c()))
     return p, cells, phi
@@ -202,12 +213,10 @@ def cpu_time_steps(p, cells, phi, warmup: int, steps: int):
 
 def c2_config(a, sites: int) -> dict:
     """The workload description both arms print (identical by construction)."""
-    return {"workload": WORKLOAD, "L": L_SIDE, "cells": N_CELLS, "radius": RADIUS,
+    L, N, text, l2 = WORKLOADS_2D[a.workload]
+    return {"workload": text, "L": L, "cells": N, "radius": RADIUS,
             "sites_per_step": sites, "window": "reference class-0 window 144^2",
-            "l2": "inputs larger than L2: two 340 MB phi pools; per-step working set 85 MB "
-                  "phi read + 85 MB phi written + 3 x 16.8 MB aggregate slots; no flush "
-                  "between steps",
-            "parallelism": f"replicas x{a.gpus}"}
+            "l2": l2, "parallelism": f"replicas x{a.gpus}"}
 
 
 def run_reference_arm(a):
@@ -220,7 +229,9 @@ def run_reference_arm(a):
     rank, world, _ = rank_env()
     if rank != 0:
         return 0
-    p, cells, phi = oracle_workload_state(1234)
+    wl = a.workload if a.workload in WORKLOADS_2D else "c2"
+    a.workload = wl
+    p, cells, phi = oracle_workload_state(1234, wl)
     warm = min(a.warmup, 5)
     value, secs, threads = cpu_time_steps(p, cells, phi, warm, a.steps)
     sites = sites_per_step(cells)
@@ -251,16 +262,29 @@ WORKLOAD3D = ("3D periodic 256^3, 512 cells R=10 (V0=4/3 pi R^3), lambda=7, bric
               "default coefficients, f32 phi, Q5.27 aggregate")
 
 
-def workload3d(seed: int):
+WORKLOAD3D_SLAB = ("3D substrate slab 256x256x128 (Nz = 2B, the reference default; Nz = 32 is "
+                   "rejected because the slab needs Nz > B), 187 cells R=10 (rho_A = N pi R^2 / "
+                   "256^2 = 0.90; the same cells per area as the periodic run would need "
+                   "rho_A = 2.45), hemispherical V0 = 2/3 pi R^3, lambda=7, B=64, centres on "
+                   "the substrate (z = -1/2) sequential with minimum separation R (2R cannot "
+                   "pack rho_A = 0.9), default coefficients, f32 phi, Q5.27 aggregate")
+
+
+def workload3d(seed: int, wl: str = "c3"):
     import pfb200
+    if wl == "c3s":
+        p = pfb200.SimParams3D(Nx=256, Ny=256, Nz=128, geometry="slab", num_cells=187,
+                               target_radius=10.0, lambda_=7.0, B=64, seed=seed)
+        c = pfb200.sequential_centres(187, 256.0, 10.0, seed, planar_z=-0.5)
+        return p, c
     p = pfb200.SimParams3D(Nx=256, Ny=256, Nz=256, num_cells=512, target_radius=10.0,
                            lambda_=7.0, B=64, seed=seed)
     c = pfb200.sequential_centres(512, 256.0, 20.0, seed, first_at_centre=True)
     return p, c.astype(np.float32).astype(np.float64)
 
 
-def read_ncu_traffic3d():
-    f = REPO / "profiles" / "k_step3d_c3.md"
+def read_ncu_traffic3d(wl: str = "c3"):
+    f = REPO / "profiles" / f"k_step3d_{wl}.md"
     if not f.exists():
         return None
     for ln in f.read_text().splitlines():
@@ -286,11 +310,14 @@ def run_3d(a):
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     torch.cuda.set_device(local)
-    p, c = workload3d(1234 + rank)
+    p, c = workload3d(1234 + rank, a.workload)
+    if a.brick_edge:
+        p.B = a.brick_edge
     sim = pfb200.Sim3D(p, c, device=local)
     B, N = sim.B, p.num_cells
     sites = N * B ** 3
     alg = sites * 8 + p.Nx * p.Ny * p.Nz * 8
+    slab = a.workload == "c3s"
     ext = torch.cuda.ExternalStream(sim.stream, device=local)
 
     def barrier():
@@ -347,14 +374,17 @@ def run_3d(a):
             "unit": "site-cell updates/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD3D, "L": 256, "cells": N, "radius": 10.0, "B": B,
-                       "sites_per_step": sites,
-                       "l2": "inputs larger than L2: two 537 MB phi pools and two 67 MB "
-                             "aggregate slots; no flush between steps",
+            "config": {"workload": WORKLOAD3D_SLAB if slab else WORKLOAD3D,
+                       "domain": [p.Nx, p.Ny, p.Nz], "geometry": p.geometry, "cells": N,
+                       "radius": 10.0, "B": B, "sites_per_step": sites,
+                       "l2": "inputs larger than L2: two %d MB phi pools and two %d MB "
+                             "aggregate slots; no flush between steps" % (
+                                 N * B ** 3 * 4 // 2 ** 20, p.Nx * p.Ny * p.Nz * 4 // 2 ** 20),
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": read_ncu_traffic3d(),
-                         "kernel": "pfb::p3::k_measure3d<4> + k_update3d<0> (one step)",
+                         "frac": achieved / peak, "traffic": read_ncu_traffic3d(a.workload),
+                         "kernel": "pfb::p3::k_measure3d<4> + k_update3d<%d> (one step)" % (
+                             1 if slab else 0),
                          "algorithmic_bytes_per_launch": alg, "peak_source": peak_src,
                          "duration_source": "CUDA events over the timed region / steps"},
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks.summary(m0, m1),
@@ -443,6 +473,59 @@ def run_ensemble(a):
     ms_serial = ens.bench(3, max(6, a.steps // 10), serial=True)
     barrier()
     ms_step = max_over_ranks(ms_step, dist, f"cuda:{local}")
+    # ---- end to end through the public API with host buffers (wall clock):
+    # every replica's state uploaded from pinned memory once, every step the
+    # trajectory records of all replicas read back, the final fields read back
+    e2e = None
+    if not a.no_e2e:
+        from pfb200._abi import check, lib
+        views = [ens.system(r) for r in range(len(ps))]
+        up = [(torch.from_numpy(v.cells().view(np.uint8).copy()).pin_memory(),
+               torch.from_numpy(np.ascontiguousarray(v.phi())).pin_memory()) for v in views]
+        trajs = [torch.empty((p.num_cells, 48), dtype=torch.uint8).pin_memory() for p in ps]
+        outs = [torch.empty_like(u[1]).pin_memory() for u in up]
+        step0 = ens.step
+        e2e_steps = max(6, min(a.steps, 60))
+        ens.sync()
+        barrier()
+        t0 = time.perf_counter()
+        for v, (c_h, p_h) in zip(views, up):
+            check(lib().pfb_sim2d_set_state(v._h, c_h.data_ptr(), p_h.data_ptr(), step0),
+                  "set_state")
+        for _ in range(e2e_steps):
+            ens.advance(1)
+            for v, t in zip(views, trajs):
+                check(lib().pfb_sim2d_pack_traj(v._h, t.data_ptr()), "pack_traj")
+        for v, o in zip(views, outs):
+            check(lib().pfb_sim2d_get_phi(v._h, o.data_ptr()), "get_phi")
+        ens.sync()
+        el = max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{local}")
+        h2d = sum(c.numel() + p_.numel() * p_.element_size() for c, p_ in up)
+        d2h = sum(t.numel() for t in trajs) * e2e_steps + sum(o.numel() * o.element_size() for o in outs)
+        e2e = {"value": world * sites * e2e_steps / el, "unit": "site-cell updates/s",
+               "h2d_bytes_per_step": h2d / e2e_steps, "d2h_bytes_per_step": d2h / e2e_steps,
+               "steps": e2e_steps,
+               "note": "host wall clock; states of all replicas uploaded from pinned memory, "
+                       "one batched launch per step, every replica's trajectory records read "
+                       "back every step, final fields read back"}
+    cpu = None
+    if world == 1 and a.cpu_steps > 0 and a.phi_storage == 0:
+        # one time step of every replica on the OpenMP restatement (oracle/)
+        sys.path.insert(0, str(REPO / "oracle"))
+        import oracle2d
+        tot, secs, thr = 0, 0.0, os.cpu_count() or 1
+        for r, p in enumerate(ps):
+            v = ens.system(r)
+            o = oracle2d.OracleSim(p.to_c(), v.cells(), v.phi(), step=ens.step)
+            o.advance(1, thr)
+            t1 = time.perf_counter()
+            o.advance(1, thr)
+            secs += time.perf_counter() - t1
+            o.close()
+            tot += p.num_cells * 144 * 144
+        cpu = {"value": tot / secs, "unit": "site-cell updates/s", "cores": thr, "kind": "port",
+               "sample": f"one time step of each of the {len(ps)} replicas after one untimed "
+                         f"({secs:.2f} s on {thr} threads) on the OpenMP restatement"}
     clocks.stop()
     flags = sum(int(ens.system(r).flags().sum()) for r in range(len(ps)))
     if rank == 0:
@@ -469,7 +552,7 @@ def run_ensemble(a):
                          "duration_source": "CUDA events over the timed region / steps"},
             "replicas_one_at_a_time": {"ms_per_step": ms_serial,
                                        "batched_speedup": ms_serial / ms_step},
-            "cpu_baseline": None, "e2e": None, "clocks": clocks.summary(m0, m1),
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks.summary(m0, m1),
             "gpu_launches": a.steps, "flags_total": flags,
         }
         print(json.dumps(line), flush=True)
@@ -606,7 +689,8 @@ def main():
     ap.add_argument("--steps", type=int, default=6000)
     ap.add_argument("--warmup", type=int, default=60)
     ap.add_argument("--impl", default="pfb", choices=["pfb", "reference"])
-    ap.add_argument("--cluster", type=int, default=2, help="CTAs per cell (2, 4 or 8)")
+    ap.add_argument("--cluster", type=int, default=0,
+                    help="CTAs per cell (2, 4 or 8; 0: 2 for c2, 4 for c1)")
     ap.add_argument("--variant", type=int, default=0, help="kernel variant (0 = default)")
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--replicas", type=int, default=64,
@@ -616,10 +700,13 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=int(os.environ.get("PFB_CPU_STEPS", "40")),
                     help="most time steps of the CPU baseline leg (one timed region)")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "ce", "cs"],
-                    help="c2: 2D 2048^2 / 1024 cells (default); c3: 3D 256^3 / 512 cells; "
-                         "ce: batched ensemble of 64 mixed-size 2D replicas; cs: passive "
+    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "c3s", "ce", "cs"],
+                    help="c2: 2D 2048^2 / 1024 cells (default); c1: 2D 512^2 / 64 cells; "
+                         "c3: 3D periodic 256^3 / 512 cells; c3s: 3D slab 256x256x128 / 187 "
+                         "cells; ce: batched ensemble of 64 mixed-size 2D replicas; cs: passive "
                          "relaxation of 1024^2 / 400 cells, plain against the learned surrogate")
+    ap.add_argument("--brick-edge", type=int, default=0,
+                    help="c3/c3s: brick edge B (0: the automatic edge, 64 at lambda 7, R 10)")
     ap.add_argument("--target", type=float, default=1e-3,
                     help="cs: residual max |dphi/dt| that counts as relaxed")
     ap.add_argument("--train-steps", type=int, default=8000, help="cs: Adam steps")
@@ -631,7 +718,7 @@ def main():
         a.warmup = 3
     if a.impl == "reference":
         return run_reference_arm(a)
-    if a.workload == "c3":
+    if a.workload in ("c3", "c3s"):
         return run_3d(a)
     if a.workload == "ce":
         return run_ensemble(a)
@@ -651,7 +738,9 @@ def main():
     device = local
     torch.cuda.set_device(device)
 
-    p = workload_params(1234 + rank)
+    if a.cluster == 0:  # measured best per workload: 2 for c2, 4 for c1
+        a.cluster = 4 if a.workload == "c1" else 2
+    p = workload_params(1234 + rank, a.workload)
     p.phi_storage = a.phi_storage
     cx, cy = workload_centres(p)
     sim = pfb200.Sim2D(p, cx, cy, device=device, cluster=a.cluster, use_graph=not a.no_graph,
@@ -675,14 +764,32 @@ def main():
     sim.sync()
     barrier()
     m0 = clocks.mark()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(ext)
-    sim.advance(a.steps)
-    e1.record(ext)
-    sim.sync()
-    barrier()
-    ms = e0.elapsed_time(e1)
+    graph_ms = None
+    if a.workload == "c1":
+        # L2-resident state: flush before every step, each step timed alone
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{device}")
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(a.steps)]
+        with torch.cuda.stream(ext):
+            for b0, b1 in evs:
+                flush.fill_(1)
+                b0.record(ext)
+                sim.advance(1)
+                b1.record(ext)
+        sim.sync()
+        barrier()
+        ms = sum(b0.elapsed_time(b1) for b0, b1 in evs)
+        graph_ms = sim.bench(12, max(600, a.steps))
+        del flush
+    else:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        sim.advance(a.steps)
+        e1.record(ext)
+        sim.sync()
+        barrier()
+        ms = e0.elapsed_time(e1)
     time.sleep(0.15)
     m1 = clocks.mark()
     ms = max_over_ranks(ms, dist, f"cuda:{device}")
@@ -728,7 +835,7 @@ def main():
     if rank == 0:
         peak, peak_src = read_peak_hbm()
         achieved = alg / (ms_step / 1000.0) / 1e9
-        traffic = read_ncu_traffic() if a.phi_storage == 0 else None
+        traffic = read_ncu_traffic(a.workload) if a.phi_storage == 0 else None
         cpu = None
         if world == 1 and a.cpu_steps > 0:
             # the procedure of --impl reference with this run's warm-up and step
@@ -753,18 +860,24 @@ def main():
                                                "bfloat16")[a.phi_storage]},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "pfb::k_step2d<%d%s>" % (
-                             a.cluster, ("", ", __half", ", __nv_bfloat16")[a.phi_storage]),
+                         "kernel": "pfb::k_step2d<%d, %s, 0, true>" % (
+                             a.cluster, ("float", "__half", "__nv_bfloat16")[a.phi_storage]),
                          "algorithmic_bytes_per_launch": alg,
                          "peak_source": peak_src,
                          "duration_source": "CUDA events over the timed region / steps"},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "clocks": clocks.summary(m0, m1),
-            "gpu_launches": a.steps,
+            # one step kernel per step, plus one bound-settling kernel per advance call
+            "gpu_launches": a.steps + (a.steps if a.workload == "c1" else 1),
             "flags": pfb200.flags_report(flags),
             "cells_class_histogram": np.bincount(final_cells["cls"], minlength=6).tolist(),
         }
+        if graph_ms is not None:
+            line["l2_resident_graph_replay"] = {
+                "ms_per_step": graph_ms, "value": sites / (graph_ms / 1000.0),
+                "note": "the same steps replayed as six-step CUDA graphs with the state held in L2 "
+                        "(no flush): the configuration's steady state in a long run"}
         print(json.dumps(line), flush=True)
     sim.close()
     if dist is not None:

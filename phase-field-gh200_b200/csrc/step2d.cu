@@ -52,6 +52,7 @@ namespace pfb {
 #endif
 constexpr int kThreads = PFB_STEP2D_THREADS;
 constexpr int kWarps = kThreads / 32;
+static_assert(kThreads % 32 == 0, "whole warps: the reductions index per-warp slots");
 constexpr int kHeaderBytes = 2048;
 // the spatial velocity observer's kernels: room for its reduction arrays
 constexpr int kHeaderBytesObs = 2560;
