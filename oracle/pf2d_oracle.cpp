@@ -53,11 +53,13 @@ Win win(int c) {
     return t[(c >= 0 && c < 6) ? c : 0];
 }
 
-// include/params.cuh:222-235
-int class_containing(int ex, int ey, int slack) {
+// include/params.cuh:222-235; on sides up to 286 (below the reference's
+// minimum) only the classes whose window fits the side L take part
+int class_containing(int ex, int ey, int slack, int L) {
     int best = -1, area = 0;
     for (int c = 0; c < 6; ++c) {
         const Win w = win(c);
+        if (w.wx > L || w.wy > L) continue;
         if (ex + slack <= w.wx && ey + slack <= w.wy && (best < 0 || w.wx * w.wy < area)) {
             best = c;
             area = w.wx * w.wy;
@@ -198,7 +200,7 @@ template <typename R> void step_cell(const Args<R>& A, int n, std::vector<R>& tm
     unsigned pctr = c.promote;
     if (ex > 0) {
         if (ex + 8 > W.wx || ey + 8 > W.wy) {
-            const int grow = class_containing(ex, ey, 8);
+            const int grow = class_containing(ex, ey, 8, A.L);
             if (grow >= 0)
                 dcls = grow;
             else if (fallback && ex <= W.wx && ey <= W.wy)
@@ -207,7 +209,7 @@ template <typename R> void step_cell(const Args<R>& A, int n, std::vector<R>& tm
                 flag_add(A.flags, PFB_FLAG_CLASS_EXHAUSTED, 1u);
             pctr = 0;
         } else {
-            const int small = class_containing(ex, ey, 20);
+            const int small = class_containing(ex, ey, 20, A.L);
             if (small >= 0 && small != CLS && win(small).wx * win(small).wy < W.wx * W.wy) {
                 if (++pctr >= 200u) {
                     dcls = small;

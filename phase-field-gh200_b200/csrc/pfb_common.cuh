@@ -162,12 +162,24 @@ constexpr int kDemoteSlack = 20;
 constexpr int kDemoteDwell = 200;
 constexpr int kMaxShift = 4;
 
-// Smallest-area class whose window holds (ex + slack, ey + slack); -1 if none.
-PFB_HD PFB_INLINE int smallest_class_holding(int ex, int ey, int slack) {
+// Smallest lattice side this build accepts: the class-0 window must fit.
+// Sides up to 286 (which the reference refuses: its largest window is 286)
+// use only the classes whose window fits the side (a window never overlaps
+// itself on the periodic lattice); above 286 every class is available and
+// the choice is the reference's.
+constexpr int kMinSide = 144;
+PFB_HD PFB_INLINE bool class_fits(int c, int L) {
+    const Window w = window_of(c);
+    return w.wx <= L && w.wy <= L;
+}
+
+// Smallest-area class fitting the side L whose window holds (ex + slack,
+// ey + slack); -1 if none.
+PFB_HD PFB_INLINE int smallest_class_holding(int ex, int ey, int slack, int L) {
     int best = -1, best_area = 0;
     for (int c = 0; c < kNumClasses; ++c) {
         const Window w = window_of(c);
-        if (ex + slack <= w.wx && ey + slack <= w.wy) {
+        if (ex + slack <= w.wx && ey + slack <= w.wy && w.wx <= L && w.wy <= L) {
             const int area = w.wx * w.wy;
             if (best < 0 || area < best_area) {
                 best = c;

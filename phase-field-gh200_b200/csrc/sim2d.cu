@@ -299,7 +299,7 @@ struct pfb_sim2d {
         N = p.num_cells;
         L = p.L;
         if (N < 1) return set_error(PFB_E_ARG, "num_cells must be positive");
-        if (L <= 286) return set_error(PFB_E_ARG, "domain side %d must exceed 286", L);
+        if (L < kMinSide) return set_error(PFB_E_ARG, "domain side %d is below %d", L, kMinSide);
         if (p.phi_storage < 0 || p.phi_storage > 2)
             return set_error(PFB_E_ARG, "phi_storage must be 0, 1 or 2");
         P = 32 * ((L + 31) / 32);

@@ -924,8 +924,9 @@ static int check_step_args(const pfb_step_args2d* a) {
         ((uintptr_t)A.S_cl & 15u) || ((uintptr_t)A.S_rd & 15u))
         return set_error(PFB_E_ARG, "phi pools and S slots must be 16-byte aligned");
     if (A.N < 0) return set_error(PFB_E_ARG, "negative cell count");
-    if (A.L <= 286 || A.P < A.L || (A.P & 3))
-        return set_error(PFB_E_ARG, "domain side must exceed 286, P >= L and P % 4 == 0");
+    if (A.L < kMinSide || A.P < A.L || (A.P & 3))
+        return set_error(PFB_E_ARG, "domain side must be at least %d, P >= L and P %% 4 == 0",
+                         kMinSide);
     if (A.parity_out != 0 && A.parity_out != 1) return set_error(PFB_E_ARG, "parity_out must be 0 or 1");
     return PFB_OK;
 }

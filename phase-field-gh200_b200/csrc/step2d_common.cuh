@@ -86,7 +86,7 @@ __device__ __forceinline__ void plan_cell(const pfb_step_args2d& A, int n, int c
     unsigned pctr = cs.promote_ctr;
     if (ex > 0) {
         if (ex + kPromoteSlack > W.wx || ey + kPromoteSlack > W.wy) {
-            const int grow = smallest_class_holding(ex, ey, kPromoteSlack);
+            const int grow = smallest_class_holding(ex, ey, kPromoteSlack, A.L);
             if (grow >= 0) {
                 dcls = grow;
             } else if (cls == kClassFallback && ex <= W.wx && ey <= W.wy) {
@@ -96,7 +96,7 @@ __device__ __forceinline__ void plan_cell(const pfb_step_args2d& A, int n, int c
             }
             pctr = 0u;
         } else {
-            const int small = smallest_class_holding(ex, ey, kDemoteSlack);
+            const int small = smallest_class_holding(ex, ey, kDemoteSlack, A.L);
             if (small >= 0 && small != cls &&
                 window_of(small).wx * window_of(small).wy < W.wx * W.wy) {
                 if (++pctr >= (unsigned)kDemoteDwell) {

@@ -54,8 +54,8 @@ class SimParams2D:
     def validate(self) -> None:
         """The checks of the reference's validate() that concern the update
         (reference include/params.cuh:596-722); raises ValueError."""
-        if self.L <= 286:
-            raise ValueError(f"domain side {self.L} must exceed the largest rect dimension 286")
+        if self.L < 144:
+            raise ValueError(f"domain side {self.L} is below the class-0 window 144")
         if self.num_cells <= 0:
             raise ValueError("num_cells must be positive")
         for name in ("lambda_", "target_radius", "dt", "xi", "tau"):

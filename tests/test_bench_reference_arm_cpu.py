@@ -32,4 +32,5 @@ def test_reference_arm_loads_only_the_oracle():
 
     class A:
         gpus = 1
+        workload = "c2"
     assert line["config"] == bench.c2_config(A, 1024 * 144 * 144)
