@@ -202,34 +202,39 @@ class OracleSim:
         except Exception:
             pass
 
+    def _handle(self):
+        if not self._h:
+            raise RuntimeError("the oracle simulation was closed")
+        return self._h
+
     def advance(self, steps: int, threads: int = 0):
-        olib().oracle_sim_advance(self._h, self.f64, steps, threads)
+        olib().oracle_sim_advance(self._handle(), self.f64, steps, threads)
 
     @property
     def step(self) -> int:
-        return int(olib().oracle_sim_step(self._h, self.f64))
+        return int(olib().oracle_sim_step(self._handle(), self.f64))
 
     def cells(self) -> np.ndarray:
         out = np.zeros(self.N, CELL_DTYPE)
-        olib().oracle_sim_get_cells(self._h, self.f64, _p(out))
+        olib().oracle_sim_get_cells(self._handle(), self.f64, _p(out))
         return out
 
     def velocity(self) -> np.ndarray:
         out = np.zeros((self.N, 2), np.float64)
-        olib().oracle_sim_get_velocity(self._h, self.f64, _p(out))
+        olib().oracle_sim_get_velocity(self._handle(), self.f64, _p(out))
         return out
 
     def phi(self) -> np.ndarray:
         out = np.zeros((self.N, 288, 288), np.float64)
-        olib().oracle_sim_get_phi(self._h, self.f64, _p(out))
+        olib().oracle_sim_get_phi(self._handle(), self.f64, _p(out))
         return out
 
     def S(self) -> np.ndarray:
         out = np.zeros((self.L, self.P), np.uint32)
-        olib().oracle_sim_get_S(self._h, self.f64, _p(out))
+        olib().oracle_sim_get_S(self._handle(), self.f64, _p(out))
         return out
 
     def flags(self) -> np.ndarray:
         out = np.zeros(8, np.uint32)
-        olib().oracle_sim_get_flags(self._h, self.f64, _p(out))
+        olib().oracle_sim_get_flags(self._handle(), self.f64, _p(out))
         return out
