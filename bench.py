@@ -320,6 +320,13 @@ def run_3d(a):
     if a.brick_edge:
         p.B = a.brick_edge
     sim = pfb200.Sim3D(p, c, device=local)
+    if a.fused3d == "off":
+        sim.set_fused(False)
+    elif a.fused3d == "on":
+        sim.set_fused(True)
+    if a.order3d == "slot":
+        sim.set_order(False)
+    fused = sim.fused
     B, N = sim.B, p.num_cells
     sites = N * B ** 3
     alg = sites * 8 + p.Nx * p.Ny * p.Nz * 8
@@ -383,18 +390,23 @@ def run_3d(a):
             "config": {"workload": WORKLOAD3D_SLAB if slab else WORKLOAD3D,
                        "domain": [p.Nx, p.Ny, p.Nz], "geometry": p.geometry, "cells": N,
                        "radius": 10.0, "B": B, "sites_per_step": sites,
+                       "step": "fused measure + motion + update launch" if fused else
+                               "separate measure, motion and update launches",
+                       "visit_order": a.order3d,
                        "l2": "inputs larger than L2: two %d MB phi pools and two %d MB "
                              "aggregate slots; no flush between steps" % (
                                  N * B ** 3 * 4 // 2 ** 20, p.Nx * p.Ny * p.Nz * 4 // 2 ** 20),
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": read_ncu_traffic3d(a.workload),
-                         "kernel": "pfb::p3::k_measure3d<4> + k_update3d<%d> (one step)" % (
-                             1 if slab else 0),
+                         "kernel": ("pfb::p3::k_step3d<%d, %d> (one step)" % (
+                             pfb200.lib().pfb3d_step_cluster(B), 1 if slab else 0)) if fused else
+                                   ("pfb::p3::k_measure3d<%d> + k_update3d<%d> (one step)" % (
+                                       pfb200.lib().pfb3d_step_cluster(B) or 4, 1 if slab else 0)),
                          "algorithmic_bytes_per_launch": alg, "peak_source": peak_src,
                          "duration_source": "CUDA events over the timed region / steps"},
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks.summary(m0, m1),
-            "gpu_launches": a.steps * 10,
+            "gpu_launches": a.steps * (8 if fused else 10),
             "flags": pfb200.flags_report3(flags),
         }
         print(json.dumps(line), flush=True)
@@ -713,6 +725,11 @@ def main():
                          "c3: 3D periodic 256^3 / 512 cells; c3s: 3D slab 256x256x128 / 187 "
                          "cells; ce: batched ensemble of 64 mixed-size 2D replicas; cs: passive "
                          "relaxation of 1024^2 / 400 cells, plain against the learned surrogate")
+    ap.add_argument("--fused3d", choices=("auto", "on", "off"), default="auto",
+                    help="3D: one fused measure + motion + update launch per step (auto: the "
+                         "driver's default, the separate launches)")
+    ap.add_argument("--order3d", choices=("morton", "slot"), default="morton",
+                    help="3D: visit cells in the Morton order of their bricks or in slot order")
     ap.add_argument("--brick-edge", type=int, default=0,
                     help="c3/c3s: brick edge B (0: the automatic edge, 64 at lambda 7, R 10)")
     ap.add_argument("--target", type=float, default=1e-3,

@@ -234,6 +234,30 @@ int pfb3d_measure_cells(const pfb_measure_args3d* args, void* stream);
  * S_in != S_out, compute_surface = 0 and tile_pass = ALL. */
 int pfb3d_update(const pfb_update_args3d* args, void* stream);
 
+/* The step's measurement, motion and update in one launch (one thread-block
+ * cluster per cell holds the brick in shared memory, so each brick is read
+ * from HBM once); replaces launch_measure_cells followed by the update
+ * launcher of the geometry (reference Sim3D::begin_step/finish_step,
+ * src/pf3d/sim.cu:1460-1651). The caller clears update->S_out first. Both
+ * records must describe the same system (phi == phi_in, S == S_in, cells,
+ * flags, layout, wall and selection). The committed records, phi and S of a
+ * step without fatal flags equal those of pfb3d_measure_cells +
+ * pfb3d_update; on a step that raises a fatal flag the cells updated before
+ * it was raised update normally, so after the repair and restore only the
+ * step's global flag counts can differ. PFB_E_CONFIG when the brick edge
+ * does not fit (pfb3d_step_cluster returns 0). */
+int pfb3d_step_fused(const pfb_measure_args3d* measure, const pfb_update_args3d* update,
+                     void* stream);
+/* Cluster size (CTAs per cell) of the fused step for brick edge B, 0 when
+ * the brick does not fit it. The measurement launchers use the same cluster
+ * size, so both paths sum the moments in the same grouping. */
+int pfb3d_step_cluster(int B);
+/* Status bits of the 3D kernels' bounded waits since the last clear: bit 0
+ * measurement plane wait, bit 1 measurement fold, bit 2 update plane wait,
+ * bit 4 fused-step plane wait, bit 5 fused-step fold, bit 6 fused-step
+ * broadcast. 0 on a healthy device. */
+int pfb3d_device_status(unsigned* out, int clear);
+
 /* launch_clear_S (kernels.cu:2704). */
 int pfb3d_clear_S(uint32_t* S, const pfb_layout3d* layout, void* stream);
 /* launch_repair_after_fatal: restores phi_out and rebuilds S_out from phi_in
@@ -335,6 +359,18 @@ int pfb_sim3d_measure_current(pfb_sim3d* s);
 /* Advance `steps` accepted-or-rejected steps (the reference's
  * begin_step/finish_step sequence per step). */
 int pfb_sim3d_advance(pfb_sim3d* s, int steps);
+/* 1: one fused launch per step (pfb3d_step_fused), 0 (default): the
+ * separate measurement, motion and update launches. */
+int pfb_sim3d_set_fused(pfb_sim3d* s, int fused);
+int pfb_sim3d_fused(const pfb_sim3d* s);
+/* Replay pairs of steps without a surface pass from a CUDA graph (default
+ * 1). */
+int pfb_sim3d_set_graph(pfb_sim3d* s, int use_graph);
+/* Visit order of the cells in every launch: 1 (default) the Morton order of
+ * the brick centres, refreshed every 4096 steps, so that clusters in flight
+ * share aggregate words in L2; 0 the slot order. Results do not depend on
+ * it. */
+int pfb_sim3d_set_order(pfb_sim3d* s, int morton);
 int pfb_sim3d_sync(pfb_sim3d* s);
 int pfb_sim3d_brick(const pfb_sim3d* s);
 long long pfb_sim3d_step(const pfb_sim3d* s);

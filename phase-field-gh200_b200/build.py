@@ -35,7 +35,7 @@ COMMON = [
     "-I", str(INCLUDE),
 ]
 SOURCES = ["step2d.cu", "init2d.cu", "sim2d.cu", "host2d.cpp", "measure3d.cu", "update3d.cu",
-           "misc3d.cu", "sim3d.cu", "host3d.cpp", "conv2d_tc.cu",
+           "step3d.cu", "misc3d.cu", "sim3d.cu", "host3d.cpp", "conv2d_tc.cu",
            "relax2d.cu", "unet2d.cu", "ckpt2d.cpp",
            "ckpt3d.cpp", "velocity2d.cu", "boundary2d.cu", "boundary3d.cu",
            "order2d.cu"]
@@ -43,7 +43,8 @@ SOURCES = ["step2d.cu", "init2d.cu", "sim2d.cu", "host2d.cpp", "measure3d.cu", "
 CLI_SOURCES = {"pfb_cell": "cli2d.cpp", "pfb_cell_3d": "cli3d.cpp"}
 CXX = os.environ.get("CXX", "g++")
 HEADERS = ["pfb_common.cuh", "device_util.cuh", "pfb_internal.h", "step2d_common.cuh",
-           "pfb3d_common.cuh", "ring3d.cuh", "storage2d.cuh",
+           "pfb3d_common.cuh", "ring3d.cuh", "storage2d.cuh", "measure3d_common.cuh",
+           "update3d_common.cuh",
            "tc_util.cuh"]
 
 

@@ -164,6 +164,16 @@ int init3d_launch(const pfb_init_args3d* a, cudaStream_t stream);
 int scatter3d_launch(const pfb_scatter_args3d* a, cudaStream_t stream);
 int measure3d_read_status(unsigned* out, int clear);
 int update3d_read_status(unsigned* out, int clear);
+int check_measure(const pfb_measure_args3d* a);
+int check_update(const pfb_update_args3d* a);
+// cluster size of the measurement (the fused step's where it applies)
+int measure3d_cluster(int B);
+// step3d.cu: fused measure + motion + update; cluster size 0 when the brick
+// does not fit the fused kernel's shared memory
+int step3d_cluster(int B);
+size_t step3d_smem(int B);
+int step3d_launch(const pfb_measure_args3d* m, const pfb_update_args3d* u, cudaStream_t stream);
+int step3d_read_status(unsigned* out, int clear);
 }  // namespace p3
 
 }  // namespace pfb

@@ -6,6 +6,17 @@
 //   steps) -> motion -> clear next S -> update -> repair if fatal ->
 //   finalize origins -> restore if fatal -> advance step counter.
 //
+// pfb_sim3d_set_fused(s, 1) runs the measurement, motion and update as one
+// fused launch (k_step3d) after the clear; the separate launches stay the
+// default, being faster on a B200. Pairs of steps without a surface pass are
+// replayed from one CUDA graph.
+//
+// Cells are visited in the Morton order of their brick centres (the launches'
+// selection list, refreshed every kOrderRefresh steps): clusters in flight at
+// the same time then touch neighbouring aggregate words, which stay in L2
+// across the eight-fold overlap of the bricks. Cells are independent within a
+// step, so the order changes no result.
+//
 // A fresh start seeds tanh spheres with the calibrated radius, builds S from
 // them and measures once without a tumble (src/pf3d/sim.cu:1100-1180).
 #include <cuda_runtime.h>
@@ -53,8 +64,23 @@ struct pfb_sim3d {
     long long steps_done = 0;
     double V0 = 0.0;
     pfb::Boundary3D* bnd = nullptr;  // open PFB3D recorder
+    int fused = 0;                   // 1: one fused launch per step
+    int* d_order = nullptr;          // visit order of the cells
+    bool use_order = true;
+    long long order_step = -1;       // step of the last order refresh
+    bool use_graph = true;
+    cudaGraph_t graph = nullptr;     // two steps from buffer parity 0
+    cudaGraphExec_t graph_exec = nullptr;
+
+    void drop_graph() {
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        if (graph) cudaGraphDestroy(graph);
+        graph_exec = nullptr;
+        graph = nullptr;
+    }
 
     ~pfb_sim3d() {
+        drop_graph();
         if (bnd) (void)pfb::boundary3d_close(bnd, 0);  // unterminated: not a completed run
         if (stream) cudaStreamDestroy(stream);
         cudaFree(d_phi[0]);
@@ -68,6 +94,7 @@ struct pfb_sim3d {
         cudaFree(d_wall);
         cudaFree(d_wall_psi);
         cudaFree(d_centres);
+        cudaFree(d_order);
     }
 };
 
@@ -198,6 +225,52 @@ double volume0(const pfb_params3d& p) {
 
 uint64_t polarity_stream(const pfb_params3d& p) { return p.polarity_seed ? p.polarity_seed : p.seed; }
 
+constexpr long long kOrderRefresh = 4096;
+
+// 21 bits of each coordinate interleaved (x lowest).
+uint64_t morton3(uint32_t x, uint32_t y, uint32_t z) {
+    auto spread = [](uint64_t v) {
+        v &= 0x1FFFFFull;
+        v = (v | (v << 32)) & 0x1F00000000FFFFull;
+        v = (v | (v << 16)) & 0x1F0000FF0000FFull;
+        v = (v | (v << 8)) & 0x100F00F00F00F00Full;
+        v = (v | (v << 4)) & 0x10C30C30C30C30C3ull;
+        v = (v | (v << 2)) & 0x1249249249249249ull;
+        return v;
+    };
+    return spread(x) | (spread(y) << 1) | (spread(z) << 2);
+}
+
+// Visit order: Morton order of the (wrapped) brick centres, or the identity.
+int refresh_order(pfb_sim3d* s) {
+    std::vector<int> order((size_t)s->N);
+    for (int i = 0; i < s->N; ++i) order[(size_t)i] = i;
+    if (s->use_order) {
+        std::vector<pfb_cell3d> c((size_t)s->N);
+        PFB3_CU(cudaStreamSynchronize(s->stream), "sync");
+        PFB3_CU(cudaMemcpy(c.data(), s->d_cells, c.size() * sizeof(pfb_cell3d), cudaMemcpyDeviceToHost),
+                "read cells");
+        const int h = s->B / 2;
+        std::vector<uint64_t> key((size_t)s->N);
+        for (int i = 0; i < s->N; ++i) {
+            const pfb_cell3d& r = c[(size_t)i];
+            const int x = wrap_origin(r.origin_x + h, s->L.nx);
+            const int y = wrap_origin(r.origin_y + h, s->L.ny);
+            const int64_t zz = r.origin_z + h;
+            const int z = periodic_xyz(s->L.boundary_flags) ? wrap_origin(zz, s->L.nz)
+                                                            : (int)std::max<int64_t>(0, zz);
+            key[(size_t)i] = morton3((uint32_t)x, (uint32_t)y, (uint32_t)z);
+        }
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int a, int b) { return key[(size_t)a] < key[(size_t)b]; });
+    }
+    PFB3_CU(cudaStreamSynchronize(s->stream), "sync");
+    PFB3_CU(cudaMemcpy(s->d_order, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice),
+            "upload order");
+    s->order_step = s->steps_done;
+    return PFB_OK;
+}
+
 int validate3(const pfb_params3d& p) {
     const uint32_t b = p.boundary_flags;
     if (periodic_xyz(b)) {
@@ -275,6 +348,8 @@ pfb_measure_args3d measure_args(pfb_sim3d* s, bool tumble, bool surface) {
     m.support_margin = (int)kSafetyMargin;
     m.apply_tumble = tumble ? 1 : 0;
     m.compute_surface = surface ? 1 : 0;
+    m.selection.ids = s->d_order;
+    m.selection.count = s->N;
     return m;
 }
 
@@ -297,28 +372,86 @@ pfb_update_args3d update_args(pfb_sim3d* s) {
     u.bulk_scale = (float)coeff_bulk(s->p.lambda);
     u.interaction_coeff = (float)coeff_interaction(s->p.kappa, s->p.lambda);
     u.tile_pass = PFB3D_TILE_PASS_ALL;
+    u.selection.ids = s->d_order;
+    u.selection.count = s->N;
     return u;
 }
 
-int one_step(pfb_sim3d* s) {
-    const bool full = s->p.full_moment_every > 0 && s->steps_done % s->p.full_moment_every == 0;
+bool full_step(const pfb_sim3d* s, long long step) {
+    return s->p.full_moment_every > 0 && step % s->p.full_moment_every == 0;
+}
+
+// The launches of one step on the current buffers (no host state changes).
+int launch_step(pfb_sim3d* s, bool full) {
     PFB3_CU(cudaMemcpyAsync(s->d_accepted, s->d_cells, (size_t)s->N * sizeof(pfb_cell3d),
                             cudaMemcpyDeviceToDevice, s->stream),
             "snapshot accepted cells");
     const pfb_measure_args3d m = measure_args(s, true, full);
-    PFB3_RC(measure3d_launch(&m, s->stream));
-    PFB3_RC(motion3d_launch(&m, s->stream));
-    PFB3_RC(clear3d_launch(s->d_S[1 - s->cur_S], &s->L, nullptr, s->stream));
     const pfb_update_args3d u = update_args(s);
-    PFB3_RC(update3d_launch(&u, s->stream));
+    if (s->fused) {
+        PFB3_RC(clear3d_launch(s->d_S[1 - s->cur_S], &s->L, nullptr, s->stream));
+        PFB3_RC(step3d_launch(&m, &u, s->stream));
+    } else {
+        PFB3_RC(measure3d_launch(&m, s->stream));
+        PFB3_RC(motion3d_launch(&m, s->stream));
+        PFB3_RC(clear3d_launch(s->d_S[1 - s->cur_S], &s->L, nullptr, s->stream));
+        PFB3_RC(update3d_launch(&u, s->stream));
+    }
     PFB3_RC(repair3d_launch(&u, s->stream));
     PFB3_RC(pfb3d_finalize_origins(s->d_cells, s->N, s->d_flags, s->stream));
     PFB3_RC(pfb3d_restore_cells_after_fatal(s->d_cells, s->d_accepted, s->N, s->d_flags, nullptr,
                                             s->stream));
     PFB3_RC(pfb3d_advance_step(s->d_step, s->d_flags, s->stream));
+    return PFB_OK;
+}
+
+void flip(pfb_sim3d* s) {
     s->cur_phi = 1 - s->cur_phi;
     s->cur_S = 1 - s->cur_S;
+}
+
+int one_step(pfb_sim3d* s) {
+    PFB3_RC(launch_step(s, full_step(s, s->steps_done)));
+    flip(s);
     ++s->steps_done;
+    return PFB_OK;
+}
+
+// Capture two steps without a surface pass, from buffer parity 0.
+int build_graph(pfb_sim3d* s) {
+    s->drop_graph();
+    PFB3_CU(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    int rc = launch_step(s, false);
+    flip(s);
+    if (rc == PFB_OK) rc = launch_step(s, false);
+    flip(s);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+    if (rc != PFB_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    PFB3_CU(e, "end capture");
+    s->graph = g;
+    PFB3_CU(cudaGraphInstantiateWithFlags(&s->graph_exec, s->graph, 0), "graph instantiate");
+    return PFB_OK;
+}
+
+int advance_impl(pfb_sim3d* s, long long steps) {
+    while (steps > 0) {
+        if (s->steps_done - s->order_step >= kOrderRefresh) PFB3_RC(refresh_order(s));
+        const bool pair = s->use_graph && s->cur_phi == 0 && steps >= 2 &&
+                          !full_step(s, s->steps_done) && !full_step(s, s->steps_done + 1);
+        if (pair) {
+            if (!s->graph_exec) PFB3_RC(build_graph(s));
+            PFB3_CU(cudaGraphLaunch(s->graph_exec, s->stream), "graph launch");
+            s->steps_done += 2;
+            steps -= 2;
+        } else {
+            PFB3_RC(one_step(s));
+            --steps;
+        }
+    }
     return PFB_OK;
 }
 
@@ -340,6 +473,7 @@ int alloc_impl(pfb_sim3d* s, const pfb_params3d* pp, int device) {
     s->L.boundary_flags = p.boundary_flags;
     if (!geometry_ok3(s->B, s->L)) return set_error(PFB_E_ARG, "the brick must fit inside the domain");
     s->V0 = volume0(p);
+    s->fused = 0;  // the separate launches measure faster (both are issue-bound)
     s->s_words = (size_t)s->L.pitch_x * s->L.ny * s->L.nz;
     s->cell_words = (size_t)s->B * s->B * s->B;
     PFB3_CU(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream");
@@ -352,6 +486,13 @@ int alloc_impl(pfb_sim3d* s, const pfb_params3d* pp, int device) {
     PFB3_CU(cudaMalloc(&s->d_flags, PFB3D_FLAG_COUNT * sizeof(uint32_t)), "cudaMalloc(flags)");
     PFB3_CU(cudaMalloc(&s->d_step, sizeof(uint64_t)), "cudaMalloc(step)");
     PFB3_CU(cudaMalloc(&s->d_centres, (size_t)s->N * sizeof(pfb_vec3)), "cudaMalloc(centres)");
+    PFB3_CU(cudaMalloc(&s->d_order, (size_t)s->N * sizeof(int)), "cudaMalloc(order)");
+    {
+        std::vector<int> id((size_t)s->N);
+        for (int i = 0; i < s->N; ++i) id[(size_t)i] = i;
+        PFB3_CU(cudaMemcpy(s->d_order, id.data(), id.size() * sizeof(int), cudaMemcpyHostToDevice),
+                "upload order");
+    }
     PFB3_CU(cudaMemsetAsync(s->d_flags, 0, PFB3D_FLAG_COUNT * sizeof(uint32_t), s->stream), "memset");
     PFB3_CU(cudaMemsetAsync(s->d_step, 0, sizeof(uint64_t), s->stream), "memset");
     if (hard_wall_channel(p.boundary_flags)) PFB3_RC(upload_wall(s));
@@ -429,7 +570,7 @@ int create_impl(pfb_sim3d* s, const pfb_params3d* pp, const pfb_vec3* centres, i
     PFB3_RC(init3d_launch(&ia, s->stream));
     PFB3_RC(remeasure_impl(s));
     PFB3_CU(cudaStreamSynchronize(s->stream), "fresh initialisation");
-    return PFB_OK;
+    return refresh_order(s);
 }
 
 // Restore (reference Sim3D::init_checkpoint, src/pf3d/sim.cu:794-885): cell
@@ -455,7 +596,7 @@ int restore_impl(pfb_sim3d* s, const pfb_params3d* pp, const pfb_cell3d* cells, 
     s->cur_S = 0;
     PFB3_RC(remeasure_impl(s));
     PFB3_CU(cudaStreamSynchronize(s->stream), "restore");
-    return PFB_OK;
+    return refresh_order(s);
 }
 
 }  // namespace
@@ -592,7 +733,36 @@ int pfb_sim3d_measure_current(pfb_sim3d* s) {
 int pfb_sim3d_advance(pfb_sim3d* s, int steps) {
     if (!s || steps < 0) return set_error(PFB_E_ARG, "invalid advance arguments");
     PFB3_CU(cudaSetDevice(s->device), "cudaSetDevice");
-    for (int i = 0; i < steps; ++i) PFB3_RC(one_step(s));
+    return advance_impl(s, steps);
+}
+
+int pfb_sim3d_set_fused(pfb_sim3d* s, int fused) {
+    if (!s) return set_error(PFB_E_ARG, "null sim");
+    if (fused && step3d_cluster(s->B) == 0)
+        return set_error(PFB_E_CONFIG, "brick edge %d does not fit the fused step", s->B);
+    const int f = fused ? 1 : 0;
+    if (f != s->fused) {
+        PFB3_CU(cudaStreamSynchronize(s->stream), "sync");
+        s->drop_graph();
+        s->fused = f;
+    }
+    return PFB_OK;
+}
+
+int pfb_sim3d_fused(const pfb_sim3d* s) { return s ? s->fused : -1; }
+
+int pfb_sim3d_set_order(pfb_sim3d* s, int morton) {
+    if (!s) return set_error(PFB_E_ARG, "null sim");
+    PFB3_CU(cudaSetDevice(s->device), "cudaSetDevice");
+    s->use_order = morton != 0;
+    return refresh_order(s);
+}
+
+int pfb_sim3d_set_graph(pfb_sim3d* s, int use_graph) {
+    if (!s) return set_error(PFB_E_ARG, "null sim");
+    PFB3_CU(cudaStreamSynchronize(s->stream), "sync");
+    s->drop_graph();
+    s->use_graph = use_graph != 0;
     return PFB_OK;
 }
 
@@ -670,13 +840,13 @@ void* pfb_sim3d_stream(const pfb_sim3d* s) { return s ? (void*)s->stream : nullp
 int pfb_sim3d_bench(pfb_sim3d* s, int warmup, int steps, double* ms) {
     if (!s || warmup < 0 || steps <= 0 || !ms) return set_error(PFB_E_ARG, "invalid bench arguments");
     PFB3_CU(cudaSetDevice(s->device), "cudaSetDevice");
-    for (int i = 0; i < warmup; ++i) PFB3_RC(one_step(s));
+    PFB3_RC(advance_impl(s, warmup));
     cudaEvent_t e0, e1;
     PFB3_CU(cudaEventCreate(&e0), "event");
     PFB3_CU(cudaEventCreate(&e1), "event");
     PFB3_CU(cudaStreamSynchronize(s->stream), "sync");
     PFB3_CU(cudaEventRecord(e0, s->stream), "record");
-    for (int i = 0; i < steps; ++i) PFB3_RC(one_step(s));
+    PFB3_RC(advance_impl(s, steps));
     PFB3_CU(cudaEventRecord(e1, s->stream), "record");
     PFB3_CU(cudaEventSynchronize(e1), "sync");
     float t = 0.0f;

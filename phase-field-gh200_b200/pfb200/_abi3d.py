@@ -147,6 +147,9 @@ _abi._SIGS.update({
     "pfb3d_apply_cell_motion": (I, [C.POINTER(MeasureArgs3D), P]),
     "pfb3d_measure_cells": (I, [C.POINTER(MeasureArgs3D), P]),
     "pfb3d_update": (I, [C.POINTER(UpdateArgs3D), P]),
+    "pfb3d_step_fused": (I, [C.POINTER(MeasureArgs3D), C.POINTER(UpdateArgs3D), P]),
+    "pfb3d_step_cluster": (I, [I]),
+    "pfb3d_device_status": (I, [C.POINTER(C.c_uint), I]),
     "pfb3d_clear_S": (I, [P, C.POINTER(Layout3D), P]),
     "pfb3d_repair_after_fatal": (I, [C.POINTER(UpdateArgs3D), P]),
     "pfb3d_finalize_origins": (I, [P, I, P, P]),
@@ -173,6 +176,10 @@ _abi._SIGS.update({
     "pfb_sim3d_boundary_close": (I, [P, I]),
     "pfb_sim3d_destroy": (None, [P]),
     "pfb_sim3d_advance": (I, [P, I]),
+    "pfb_sim3d_set_fused": (I, [P, I]),
+    "pfb_sim3d_fused": (I, [P]),
+    "pfb_sim3d_set_graph": (I, [P, I]),
+    "pfb_sim3d_set_order": (I, [P, I]),
     "pfb_sim3d_sync": (I, [P]),
     "pfb_sim3d_brick": (I, [P]),
     "pfb_sim3d_step": (C.c_longlong, [P]),

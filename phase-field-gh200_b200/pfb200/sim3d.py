@@ -175,6 +175,22 @@ class Sim3D:
     def sync(self) -> None:
         check(lib().pfb_sim3d_sync(self._h), "sync")
 
+    @property
+    def fused(self) -> bool:
+        """True when a step runs as one fused measure + motion + update launch."""
+        return bool(lib().pfb_sim3d_fused(self._h))
+
+    def set_fused(self, fused: bool) -> None:
+        check(lib().pfb_sim3d_set_fused(self._h, 1 if fused else 0), "set_fused")
+
+    def set_graph(self, use_graph: bool) -> None:
+        check(lib().pfb_sim3d_set_graph(self._h, 1 if use_graph else 0), "set_graph")
+
+    def set_order(self, morton: bool) -> None:
+        """Visit cells in the Morton order of their bricks (default) or in
+        slot order; results do not depend on it."""
+        check(lib().pfb_sim3d_set_order(self._h, 1 if morton else 0), "set_order")
+
     def measure_current(self) -> None:
         """Measure the current state and set velocities without a tumble (as
         the reference does before output and checkpoints)."""
