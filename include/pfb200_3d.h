@@ -248,6 +248,53 @@ int pfb3d_update(const pfb_update_args3d* args, void* stream);
  * does not fit (pfb3d_step_cluster returns 0). */
 int pfb3d_step_fused(const pfb_measure_args3d* measure, const pfb_update_args3d* update,
                      void* stream);
+
+/* ---- adaptive bricks (reference include/pf3d/brick_classes.hpp,
+ * src/pf3d/adaptive_storage.cu, launchers of src/pf3d/kernels.cu) ----------
+ * A promoted cell (storage_edge E > B, E a multiple of 8 and at most
+ * promoted_edge) lives in its own E^3 cube, promoted_phi[n] (promoted_phi_in
+ * and _out for the update); promoted_ids lists the promoted_count promoted
+ * cells. The base launchers skip such cells. Per-voxel arithmetic is the base
+ * kernels'. */
+
+/* Next tier of a cube of edge `current`: 32 more planes rounded up to a
+ * multiple of 16, at most the largest multiple of 8 below `maximum`; 0 when
+ * none is larger (reference next_brick_edge). */
+int pfb3d_next_brick_edge(int current, int maximum);
+/* Smallest centred crop of a cube of edge `current`, not below `minimum`,
+ * that keeps 16 spare planes beyond the support box lo3..hi3 on every face,
+ * rounded up to a multiple of 16; `current` when none (reference
+ * shrink_brick_edge). */
+int pfb3d_shrink_brick_edge(int current, int minimum, const int* lo3, const int* hi3);
+/* Measurement (moments, support box, recentring plan) of the promoted cubes;
+ * replaces launch_measure_promoted (kernels.cu:1413-1427). */
+int pfb3d_measure_promoted(const pfb_measure_args3d* args, float* const* promoted_phi,
+                           const int* promoted_ids, int promoted_count, int promoted_edge,
+                           void* stream);
+/* Update of the promoted cubes with their planned shifts and the Q5.27
+ * scatter into args->S_out; replaces launch_update_promoted and
+ * launch_update_promoted_sharded_fast (kernels.cu:1888-1925). The base pools
+ * of args are not used. */
+int pfb3d_update_promoted(const pfb_update_args3d* args, float* const* promoted_phi_in,
+                          float* const* promoted_phi_out, const int* promoted_ids,
+                          int promoted_count, int promoted_edge, void* stream);
+/* Q5.27 scatter of the promoted cubes into args->S (k_scatter_promoted). */
+int pfb3d_scatter_promoted(const pfb_scatter_args3d* args, float* const* promoted_phi,
+                           const int* promoted_ids, int promoted_count, int promoted_edge,
+                           void* stream);
+/* On a step holding a fatal counter: each promoted cube keeps its accepted
+ * field (copied into the output cube and scattered into args->S_out) and its
+ * planned shift is dropped (launch_repair_promoted_after_fatal). */
+int pfb3d_repair_promoted_after_fatal(const pfb_update_args3d* args,
+                                      float* const* promoted_phi_in,
+                                      float* const* promoted_phi_out, const int* promoted_ids,
+                                      int promoted_count, int promoted_edge, void* stream);
+/* rejected[n] |= 1 unless cube n may be cropped to candidate_edges[n]
+ * (0: no candidate): every voxel finite and every voxel outside the retained
+ * cube's inner 8-plane guard band an exact zero (k_check_promoted_crops). */
+int pfb3d_check_promoted_crops(float* const* promoted_phi, const pfb_cell3d* cells,
+                               const int* candidate_edges, uint32_t* rejected, int N,
+                               int base_edge, void* stream);
 /* Cluster size (CTAs per cell) of the fused step for brick edge B, 0 when
  * the brick does not fit it. The measurement launchers use the same cluster
  * size, so both paths sum the moments in the same grouping. */
@@ -343,11 +390,13 @@ typedef struct pfb_sim3d pfb_sim3d;
  * to array coordinates as z + padding - 1/2 in binary32 as the reference
  * does); N = p->num_cells entries. */
 pfb_sim3d* pfb_sim3d_create(const pfb_params3d* p, const pfb_vec3* centres, int device);
-/* Restart from cell records and base B^3 bricks (x fastest) of step `step`,
- * as the reference's Sim3D::init_checkpoint does (src/pf3d/sim.cu:794-885):
- * the records and bricks become the current state, the aggregate is rebuilt
- * and the cells are measured once (surface included, no tumble). Ids must be
- * 0..N-1 and every cell on the base brick. */
+/* Restart from cell records and fields (x fastest) of step `step`, as the
+ * reference's Sim3D::init_checkpoint does (src/pf3d/sim.cu:794-885): the
+ * records and fields become the current state, the aggregate is rebuilt and
+ * the cells are measured once (surface included, no tumble). Ids must be
+ * 0..N-1. phi packs each cell's field in cell order: B^3 values for a base
+ * cell (storage_edge 0 or B), E^3 for a cell on a promoted cube of edge
+ * E = storage_edge > B (N * B^3 when no cell is promoted). */
 pfb_sim3d* pfb_sim3d_create_from_state(const pfb_params3d* p, const pfb_cell3d* cells,
                                        const float* phi, long long step, int device);
 void pfb_sim3d_destroy(pfb_sim3d* s);
@@ -356,8 +405,15 @@ void pfb_sim3d_destroy(pfb_sim3d* s);
  * and before writing a checkpoint (Sim3D::ensure_measurements ->
  * refresh_measurements(false, true), src/pf3d/sim.cu:1301-1377, 2045-2047). */
 int pfb_sim3d_measure_current(pfb_sim3d* s);
-/* Advance `steps` accepted-or-rejected steps (the reference's
- * begin_step/finish_step sequence per step). */
+/* Advance by `steps` accepted steps (the reference's begin_step/finish_step
+ * sequence per step, synchronising at the end and at every multiple of 1024
+ * accepted steps). A step on which a cell's support reaches its brick is
+ * rolled back and the cell's brick grows to the next tier (reference
+ * Sim3D::recover_support_exhaustion, src/pf3d/sim.cu:1653-1727), then the
+ * step is retried; promoted cubes are cropped back where their support
+ * allows at every multiple of 1024 accepted steps
+ * (Sim3D::compact_promoted_fields). Returns early, with the flags set, at any
+ * other fatal flag or when no larger cube fits the domain. */
 int pfb_sim3d_advance(pfb_sim3d* s, int steps);
 /* 1: one fused launch per step (pfb3d_step_fused), 0 (default): the
  * separate measurement, motion and update launches. */
@@ -375,8 +431,18 @@ int pfb_sim3d_sync(pfb_sim3d* s);
 int pfb_sim3d_brick(const pfb_sim3d* s);
 long long pfb_sim3d_step(const pfb_sim3d* s);
 int pfb_sim3d_get_cells(pfb_sim3d* s, pfb_cell3d* out);
-/* N * B^3 floats of the current field. */
+/* N * B^3 floats of the base pool's current field (the slot of a promoted
+ * cell is not its field: pfb_sim3d_get_packed). */
 int pfb_sim3d_get_phi(pfb_sim3d* s, float* out);
+/* Length and values of the current fields packed in cell order, each cell on
+ * its own cube (B^3 or E^3 values), as the PF3D checkpoint stores them. */
+int pfb_sim3d_packed_words(pfb_sim3d* s, unsigned long long* words);
+int pfb_sim3d_get_packed(pfb_sim3d* s, float* out);
+/* Adaptive bricks: cells currently on promoted cubes, the largest cube edge
+ * the domain allows, and the support-exhaustion recoveries so far. */
+int pfb_sim3d_promoted_count(const pfb_sim3d* s);
+int pfb_sim3d_max_edge(const pfb_sim3d* s);
+long long pfb_sim3d_recoveries(const pfb_sim3d* s);
 /* nz * ny * pitch_x words of the current aggregate. */
 int pfb_sim3d_get_S(pfb_sim3d* s, uint32_t* out);
 int pfb_sim3d_get_flags(pfb_sim3d* s, uint32_t* out10);

@@ -177,12 +177,19 @@ int pfb_ckpt3d_params_to(const pfb_ckpt3d_params* rec, int num_cells, pfb_params
 /* Read and validate (header, parameters, file size, every record, CRC) as
  * the reference does. With cells and phi null only info and rec are filled
  * (the CRC is still verified over the whole file); otherwise cells[N]
- * (storage_edge 0, derived wall fields zero) and phi[N * B^3]. */
+ * (storage_edge 0 for a base cell, E for a cell stored on a promoted cube of
+ * edge E > B; derived wall fields zero) and phi: each cell's field packed in
+ * cell order, B^3 values for a base cell and E^3 for a promoted one
+ * (pfb_ckpt3d_payload_words gives the length; N * B^3 when no cell is
+ * promoted). */
 int pfb_ckpt3d_read(const char* path, pfb_ckpt3d_info* info, pfb_ckpt3d_params* rec,
                     pfb_cell3d* cells, float* phi);
+/* Packed field length (values) of the PF3D file at path, after the same
+ * validation as pfb_ckpt3d_read. */
+int pfb_ckpt3d_payload_words(const char* path, unsigned long long* words);
 
-/* Write cells and base bricks at `step` (time = step * dt) through path.tmp
- * and a rename; base_measure_shards in 1..64 is stored as the measurement
+/* Write cells and their packed fields (as pfb_ckpt3d_read returns them) at
+ * `step` (time = step * dt) through path.tmp and a rename; base_measure_shards in 1..64 is stored as the measurement
  * grouping the continuation should use. Refuses records the reader would
  * reject. */
 int pfb_ckpt3d_write(const char* path, const pfb_ckpt3d_params* rec, long long step, int num_cells,

@@ -35,7 +35,7 @@ COMMON = [
     "-I", str(INCLUDE),
 ]
 SOURCES = ["step2d.cu", "init2d.cu", "sim2d.cu", "host2d.cpp", "measure3d.cu", "update3d.cu",
-           "step3d.cu", "misc3d.cu", "sim3d.cu", "host3d.cpp", "conv2d_tc.cu",
+           "step3d.cu", "promote3d.cu", "misc3d.cu", "sim3d.cu", "host3d.cpp", "conv2d_tc.cu",
            "relax2d.cu", "unet2d.cu", "ckpt2d.cpp",
            "ckpt3d.cpp", "velocity2d.cu", "boundary2d.cu", "boundary3d.cu",
            "order2d.cu"]

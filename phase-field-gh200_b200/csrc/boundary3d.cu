@@ -89,24 +89,28 @@ __device__ __forceinline__ void z_range(int64_t oz, int B, int nz, bool periodic
     *z1 = (int)min((int64_t)B, (int64_t)nz - oz);
 }
 
-// grid (plane blocks, N): plane[n] of cell n; status[n] = 1 on a non-finite
-// sample.
+// grid (plane blocks, N): plane of cell n (edge pe[n] = E + 2 for its cube
+// of edge E, at slot n of stride PS^2); status[n] = 1 on a non-finite
+// sample. A cell's cube is cubes[n] when it has one, else its slot of the
+// base pool (edge B).
 __global__ void __launch_bounds__(kB3Threads)
-    k_b3_project(const float* phi, const pfb_cell3d* cells, int B, int nz, int periodic,
-                 int projection, float* plane, uint32_t* status) {
+    k_b3_project(const float* phi, float* const* cubes, const pfb_cell3d* cells, int B0,
+                 const int* pe, int PS, int nz, int periodic, int projection, float* plane,
+                 uint32_t* status) {
     const int n = blockIdx.y;
-    const int PE = B + 2;
+    const int PE = pe[n], B = PE - 2;
     const int q = blockIdx.x * kB3Threads + threadIdx.x;
     if (q >= PE * PE) return;
     const int x = q % PE, y = q / PE;
-    float* out = plane + (size_t)n * PE * PE;
+    float* out = plane + (size_t)n * PS * PS;
     out[q] = 0.0f;
     if (x == 0 || y == 0 || x == PE - 1 || y == PE - 1) return;
     int z0, z1;
     z_range(cells[n].origin_z, B, nz, periodic != 0, projection, &z0, &z1);
     if (z0 >= z1) return;
     const size_t slab = (size_t)B * B;
-    const float* src = phi + (size_t)n * slab * B + ((size_t)z0 * B + (y - 1)) * B + (x - 1);
+    const float* brick = (cubes && cubes[n]) ? cubes[n] : phi + (size_t)n * B0 * B0 * B0;
+    const float* src = brick + ((size_t)z0 * B + (y - 1)) * B + (x - 1);
     float v = src[0];
     bool bad = !isfinite(v);
     for (int z = z0 + 1; z < z1; ++z) {
@@ -132,9 +136,10 @@ __device__ __forceinline__ bool plane_square(const float* p, int PE, int q, B3Sq
 }
 
 __global__ void __launch_bounds__(kB3Threads)
-    k_b3_count(const float* plane, int PE, uint32_t* counts) {
+    k_b3_count(const float* plane, const int* pe, int PS, uint32_t* counts) {
     const int n = blockIdx.x;
-    const float* p = plane + (size_t)n * PE * PE;
+    const int PE = pe[n];
+    const float* p = plane + (size_t)n * PS * PS;
     const int squares = (PE - 1) * (PE - 1);
     unsigned c = 0;
     for (int q = threadIdx.x; q < squares; q += kB3Threads) {
@@ -154,9 +159,10 @@ __global__ void __launch_bounds__(kB3Threads)
 
 // Squares of cell n in ascending plane order from out[offsets[n]].
 __global__ void __launch_bounds__(kB3Threads)
-    k_b3_gather(const float* plane, int PE, const uint64_t* offsets, B3Square* out) {
+    k_b3_gather(const float* plane, const int* pe, int PS, const uint64_t* offsets, B3Square* out) {
     const int n = blockIdx.x, t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    const float* p = plane + (size_t)n * PE * PE;
+    const int PE = pe[n];
+    const float* p = plane + (size_t)n * PS * PS;
     const int squares = (PE - 1) * (PE - 1);
     __shared__ unsigned wsum[kB3Threads / 32];
     B3Square* dst = out + offsets[n];
@@ -202,11 +208,13 @@ struct Boundary3D {
     size_t plane_cap = 0;
     uint32_t* d_status = nullptr;  // N status words, then N counts
     uint64_t* d_off = nullptr;
+    int* d_pe = nullptr;  // plane edge of each cell
     B3Square* d_sq = nullptr;
     size_t sq_cap = 0;
     std::vector<pfb_cell3d> cells;
     std::vector<uint32_t> status;
     std::vector<uint64_t> off;
+    std::vector<int> pe;
     std::vector<unsigned char> payload;
 
     ~Boundary3D() {
@@ -214,6 +222,7 @@ struct Boundary3D {
         cudaFree(d_plane);
         cudaFree(d_status);
         cudaFree(d_off);
+        cudaFree(d_pe);
         cudaFree(d_sq);
     }
 
@@ -222,8 +231,8 @@ struct Boundary3D {
         return set_error(code, "boundary3d: %s", what);
     }
 
-    int capture(const float* phi, const pfb_cell3d* d_cells, int B, cudaStream_t stream,
-                long long step, double time) {
+    int capture(const float* phi, float* const* cubes, const pfb_cell3d* d_cells, int B,
+                cudaStream_t stream, long long step, double time) {
         if (failed || !f) return set_error(PFB_E_STATE, "boundary3d: no open file");
         if (B <= 0 || B > 65532 || !std::isfinite(time) || time < 0.0 ||
             (frames > 0 && ((uint64_t)step <= last_step || time < last_time)))
@@ -233,9 +242,17 @@ struct Boundary3D {
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) return fail(PFB_E_CUDA, cudaGetErrorString(e));
         std::unordered_set<int64_t> ids;
-        const int64_t hi = std::numeric_limits<int64_t>::max() - B;
-        for (const pfb_cell3d& c : cells) {
-            const bool ok = (c.storage_edge == 0 || c.storage_edge == (uint32_t)B) && c.global_id >= 0 &&
+        int PS = 0;
+        for (int i = 0; i < N; ++i) {
+            const pfb_cell3d& c = cells[(size_t)i];
+            // a cube edge per cell (reference cell_support_edge)
+            const int E = (cubes && c.storage_edge > (uint32_t)B) ? (int)c.storage_edge : B;
+            pe[(size_t)i] = E + 2;
+            PS = std::max(PS, E + 2);
+            const int64_t hi = std::numeric_limits<int64_t>::max() - E;
+            const bool ok = (c.storage_edge == 0 || c.storage_edge == (uint32_t)B ||
+                             (cubes && c.storage_edge > (uint32_t)B && c.storage_edge <= 65532u)) &&
+                            c.global_id >= 0 &&
                             c.origin_x > std::numeric_limits<int64_t>::min() &&
                             c.origin_y > std::numeric_limits<int64_t>::min() && c.origin_x <= hi &&
                             c.origin_y <= hi && c.origin_z <= hi && finite_positive(c.gamma) &&
@@ -243,8 +260,7 @@ struct Boundary3D {
                             ids.insert(c.global_id).second;
             if (!ok) return fail(PFB_E_STATE, "invalid or duplicate cell metadata");
         }
-        const int PE = B + 2;
-        const size_t plane = (size_t)N * PE * PE;
+        const size_t plane = (size_t)N * PS * PS;
         if (plane > plane_cap) {
             cudaFree(d_plane);
             d_plane = nullptr;
@@ -252,12 +268,14 @@ struct Boundary3D {
                 return fail(PFB_E_CUDA, "plane allocation failed");
             plane_cap = plane;
         }
-        if ((e = cudaMemsetAsync(d_status, 0, (size_t)N * sizeof(uint32_t), stream)) != cudaSuccess)
+        if ((e = cudaMemsetAsync(d_status, 0, (size_t)N * sizeof(uint32_t), stream)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(d_pe, pe.data(), (size_t)N * sizeof(int), cudaMemcpyHostToDevice,
+                                 stream)) != cudaSuccess)
             return fail(PFB_E_CUDA, cudaGetErrorString(e));
-        const dim3 grid((unsigned)((PE * PE + kB3Threads - 1) / kB3Threads), (unsigned)N);
-        k_b3_project<<<grid, kB3Threads, 0, stream>>>(phi, d_cells, B, nz, periodic ? 1 : 0,
-                                                        projection, d_plane, d_status);
-        k_b3_count<<<N, kB3Threads, 0, stream>>>(d_plane, PE, d_status + N);
+        const dim3 grid((unsigned)((PS * PS + kB3Threads - 1) / kB3Threads), (unsigned)N);
+        k_b3_project<<<grid, kB3Threads, 0, stream>>>(phi, cubes, d_cells, B, d_pe, PS, nz,
+                                                        periodic ? 1 : 0, projection, d_plane, d_status);
+        k_b3_count<<<N, kB3Threads, 0, stream>>>(d_plane, d_pe, PS, d_status + N);
         if ((e = cudaGetLastError()) != cudaSuccess ||
             (e = cudaMemcpyAsync(status.data(), d_status, 2 * (size_t)N * sizeof(uint32_t),
                                  cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
@@ -278,8 +296,8 @@ struct Boundary3D {
             r.origin_x = c.origin_x - 1;
             r.origin_y = c.origin_y - 1;
             r.origin_z = c.origin_z;
-            r.brick_edge = (uint32_t)B;
-            r.plane_edge = (uint32_t)PE;
+            r.brick_edge = (uint32_t)(pe[(size_t)i] - 2);
+            r.plane_edge = (uint32_t)pe[(size_t)i];
             r.squares = status[(size_t)N + i];
             r.gamma = c.gamma;
             r.active_speed = c.v_A;
@@ -297,7 +315,7 @@ struct Boundary3D {
             if ((e = cudaMemcpyAsync(d_off, off.data(), (size_t)N * sizeof(uint64_t),
                                      cudaMemcpyHostToDevice, stream)) != cudaSuccess)
                 return fail(PFB_E_CUDA, cudaGetErrorString(e));
-            k_b3_gather<<<N, kB3Threads, 0, stream>>>(d_plane, PE, d_off, d_sq);
+            k_b3_gather<<<N, kB3Threads, 0, stream>>>(d_plane, d_pe, PS, d_off, d_sq);
             if ((e = cudaGetLastError()) != cudaSuccess ||
                 (e = cudaMemcpyAsync(payload.data() + prefix, d_sq, (size_t)total * sizeof(B3Square),
                                      cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
@@ -343,8 +361,10 @@ Boundary3D* boundary3d_open(const char* path, const pfb_params3d& p, int project
     b->cells.resize((size_t)b->N);
     b->status.resize(2 * (size_t)b->N);
     b->off.resize((size_t)b->N);
+    b->pe.resize((size_t)b->N);
     if (cudaMalloc(&b->d_status, 2 * (size_t)b->N * sizeof(uint32_t)) != cudaSuccess ||
-        cudaMalloc(&b->d_off, (size_t)b->N * sizeof(uint64_t)) != cudaSuccess) {
+        cudaMalloc(&b->d_off, (size_t)b->N * sizeof(uint64_t)) != cudaSuccess ||
+        cudaMalloc(&b->d_pe, (size_t)b->N * sizeof(int)) != cudaSuccess) {
         delete b;
         set_error(PFB_E_CUDA, "boundary3d: allocation failed");
         return nullptr;
@@ -381,9 +401,9 @@ Boundary3D* boundary3d_open(const char* path, const pfb_params3d& p, int project
     return b;
 }
 
-int boundary3d_capture(Boundary3D* b, const float* phi, const pfb_cell3d* cells, int B,
-                       cudaStream_t stream, long long step, double time) {
-    return b->capture(phi, cells, B, stream, step, time);
+int boundary3d_capture(Boundary3D* b, const float* phi, float* const* cubes, const pfb_cell3d* cells,
+                       int B, cudaStream_t stream, long long step, double time) {
+    return b->capture(phi, cubes, cells, B, stream, step, time);
 }
 
 int boundary3d_close(Boundary3D* b, int complete) {

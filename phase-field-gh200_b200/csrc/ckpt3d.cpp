@@ -4,8 +4,9 @@
 // records, 599-751 metadata and layout, 841-996 load with the CRC, 1009-1235
 // write; parameter checks of include/pf3d/params.cuh:373-473). The byte
 // layout has to be the reference's, so the records below keep its field order
-// and sizes; the code is this library's own. Cells are read and written on
-// their base B^3 bricks only.
+// and sizes; the code is this library's own. Each cell record is followed by
+// the cell's own cube: B^3 values on the base brick, E^3 on a promoted cube
+// of edge E = storage_edge (reference src/pf3d/checkpoint.cu:655-751).
 #include <algorithm>
 #include <cerrno>
 #include <cmath>
@@ -209,10 +210,8 @@ int check_record(const Record3& r, int index, int B, const pfb_ckpt3d_params& p)
     if (r.storage_edge < (uint32_t)B || r.storage_edge > 4096 || r.storage_edge % 8 != 0 ||
         (int64_t)r.storage_edge >= dom)
         return set_error(PFB_E_FORMAT, "PF3D cell %d has an invalid storage edge", index);
-    if (r.storage_edge != (uint32_t)B)
-        return set_error(PFB_E_CONFIG, "PF3D cell %d is stored on a promoted %u^3 brick (adaptive bricks "
-                         "are not supported here)", index, r.storage_edge);
-    const int e = B;
+    // the cell's own cube: the base brick or a promoted one
+    const int e = (int)r.storage_edge;
     bool ok = std::isfinite(r.vx) && std::isfinite(r.vy) && std::isfinite(r.vz);
     if (p.boundary_flags == kPeriodic || p.boundary_flags == kChannel) {
         const double n2 = (double)r.px * r.px + (double)r.py * r.py + (double)r.pz * r.pz;
@@ -237,6 +236,7 @@ int check_record(const Record3& r, int index, int B, const pfb_ckpt3d_params& p)
 }
 
 Record3 record_of(const pfb_cell3d& c, int B) {
+    // a base cell stores the base edge; a promoted one its cube's edge
     Record3 r;
     std::memset(&r, 0, sizeof(r));
     r.id = c.global_id;
@@ -269,11 +269,11 @@ Record3 record_of(const pfb_cell3d& c, int B) {
     r.shift[0] = c.pending_shift_x;
     r.shift[1] = c.pending_shift_y;
     r.shift[2] = c.pending_shift_z;
-    r.storage_edge = (uint32_t)B;
+    r.storage_edge = c.storage_edge > (uint32_t)B ? c.storage_edge : (uint32_t)B;
     return r;
 }
 
-void cell_of(const Record3& r, pfb_cell3d* c) {
+void cell_of(const Record3& r, int B, pfb_cell3d* c) {
     std::memset(c, 0, sizeof(*c));
     c->global_id = r.id;
     c->origin_x = r.ox;
@@ -309,10 +309,15 @@ void cell_of(const Record3& r, pfb_cell3d* c) {
     c->pending_shift_x = r.shift[0];
     c->pending_shift_y = r.shift[1];
     c->pending_shift_z = r.shift[2];
-    c->storage_edge = 0;  // base brick
+    c->storage_edge = r.storage_edge == (uint32_t)B ? 0u : r.storage_edge;  // 0: base brick
 }
 
-int read3(const char* path, pfb_ckpt3d_info* info, pfb_ckpt3d_params* rec_out, pfb_cell3d* cells, float* phi) {
+// Read (and verify) a PF3D file. phi receives each cell's field packed in cell
+// order (B^3 values for a base cell, E^3 for a cell stored on a promoted cube
+// of edge E); *words the packed length. With cells and phi null the file is
+// only verified.
+int read3(const char* path, pfb_ckpt3d_info* info, pfb_ckpt3d_params* rec_out, pfb_cell3d* cells, float* phi,
+          unsigned long long* words_out = nullptr) {
     File f(std::fopen(path, "rb"));
     if (!f) return set_error(PFB_E_IO, "cannot open %s: %s", path, std::strerror(errno));
     Header3 h;
@@ -328,29 +333,41 @@ int read3(const char* path, pfb_ckpt3d_info* info, pfb_ckpt3d_params* rec_out, p
     if (std::fseek(f.get(), 0, SEEK_END) != 0) return set_error(PFB_E_IO, "cannot seek %s", path);
     const long long size = std::ftell(f.get());
     const int N = (int)h.cells, B = (int)h.brick;
-    const unsigned long long per = sizeof(Record3) + h.bytes_per_cell;
-    const unsigned long long want = sizeof(Header3) + sizeof(pfb_ckpt3d_params) + per * (unsigned long long)N;
-    if (size < 0 || (unsigned long long)size != want)
-        return set_error(PFB_E_FORMAT, "PF3D file has %lld bytes; base-brick cell records require %llu", size, want);
-    if (std::fseek(f.get(), (long)(sizeof(Header3) + sizeof(pfb_ckpt3d_params)), SEEK_SET) != 0)
-        return set_error(PFB_E_IO, "cannot seek %s", path);
+    // every cell at least a record and a base brick
+    const unsigned long long prefix = sizeof(Header3) + sizeof(pfb_ckpt3d_params);
+    const unsigned long long least = prefix + (sizeof(Record3) + h.bytes_per_cell) * (unsigned long long)N;
+    if (size < 0 || (unsigned long long)size < least)
+        return set_error(PFB_E_FORMAT, "PF3D file has %lld bytes; its cell records need at least %llu", size,
+                         least);
+    if (std::fseek(f.get(), (long)prefix, SEEK_SET) != 0) return set_error(PFB_E_IO, "cannot seek %s", path);
     const Crc64& crc = crc_table();
     Header3 canon = h;
     canon.crc = 0;
     uint64_t c = crc.update(0, &canon, sizeof(canon));
     c = crc.update(c, &p, sizeof(p));
-    const size_t words = (size_t)h.values_per_cell;
-    std::vector<float> brick(phi ? 0 : words);
+    unsigned long long pos = prefix, packed = 0;
+    std::vector<float> tmp;
     for (int i = 0; i < N; ++i) {
         Record3 r;
+        if (pos + sizeof(r) > (unsigned long long)size) return bad("the file truncates a cell record");
         if (!get(f.get(), &r, sizeof(r))) return bad("short read of a cell record");
         if ((rc = check_record(r, i, B, p))) return rc;
         c = crc.update(c, &r, sizeof(r));
-        float* dst = phi ? phi + (size_t)i * words : brick.data();
-        if (!get(f.get(), dst, words * sizeof(float))) return bad("short read of a phase brick");
+        const size_t words = (size_t)r.storage_edge * r.storage_edge * r.storage_edge;
+        pos += sizeof(r) + words * sizeof(float);
+        if (pos > (unsigned long long)size) return bad("the file truncates a phase payload");
+        float* dst = phi ? phi + packed : nullptr;
+        if (!dst) {
+            tmp.resize(words);
+            dst = tmp.data();
+        }
+        if (!get(f.get(), dst, words * sizeof(float))) return bad("short read of a phase payload");
         c = crc.update(c, dst, words * sizeof(float));
-        if (cells) cell_of(r, cells + i);
+        packed += words;
+        if (cells) cell_of(r, B, cells + i);
     }
+    if (pos != (unsigned long long)size)
+        return set_error(PFB_E_FORMAT, "PF3D file has %lld bytes; its cell records require %llu", size, pos);
     if (c != h.crc) return bad("file CRC-64/ECMA mismatch");
     if (info) {
         info->step = h.step;
@@ -361,6 +378,7 @@ int read3(const char* path, pfb_ckpt3d_info* info, pfb_ckpt3d_params* rec_out, p
         info->crc64 = h.crc;
     }
     if (rec_out) *rec_out = p;
+    if (words_out) *words_out = packed;
     return PFB_OK;
 }
 
@@ -395,12 +413,12 @@ int write3(const char* path, const pfb_ckpt3d_params* rec, long long step, int N
         return set_error(PFB_E_ARG, "PF3D write refused: %s", why.c_str());
     }
     const int B = (int)h.brick;
-    const size_t words = (size_t)h.values_per_cell;
     std::vector<Record3> recs((size_t)N);
+    std::vector<size_t> offs((size_t)N + 1, 0);
     for (int i = 0; i < N; ++i) {
-        if (cells[i].storage_edge != 0 && (int)cells[i].storage_edge != B)
-            return set_error(PFB_E_ARG, "PF3D write: cell %d is not on a base brick", i);
         recs[(size_t)i] = record_of(cells[i], B);
+        const size_t e = recs[(size_t)i].storage_edge;
+        offs[(size_t)i + 1] = offs[(size_t)i] + e * e * e;
         if ((rc = check_record(recs[(size_t)i], i, B, *rec))) {
             const std::string why = pfb_last_error();
             return set_error(PFB_E_ARG, "PF3D write refused: %s", why.c_str());
@@ -412,16 +430,18 @@ int write3(const char* path, const pfb_ckpt3d_params* rec, long long step, int N
     c = crc.update(c, rec, sizeof(*rec));
     for (int i = 0; i < N; ++i) {
         c = crc.update(c, &recs[(size_t)i], sizeof(Record3));
-        c = crc.update(c, phi + (size_t)i * words, words * sizeof(float));
+        c = crc.update(c, phi + offs[(size_t)i], (offs[(size_t)i + 1] - offs[(size_t)i]) * sizeof(float));
     }
     h.crc = c;
     const std::string tmp = std::string(path) + ".tmp";
     std::FILE* f = std::fopen(tmp.c_str(), "wb");
     if (!f) return set_error(PFB_E_IO, "cannot open %s: %s", tmp.c_str(), std::strerror(errno));
     bool ok = std::fwrite(&h, sizeof(h), 1, f) == 1 && std::fwrite(rec, sizeof(*rec), 1, f) == 1;
-    for (int i = 0; ok && i < N; ++i)
+    for (int i = 0; ok && i < N; ++i) {
+        const size_t words = offs[(size_t)i + 1] - offs[(size_t)i];
         ok = std::fwrite(&recs[(size_t)i], sizeof(Record3), 1, f) == 1 &&
-             std::fwrite(phi + (size_t)i * words, sizeof(float), words, f) == words;
+             std::fwrite(phi + offs[(size_t)i], sizeof(float), words, f) == words;
+    }
     ok = (std::fclose(f) == 0) && ok;
     if (!ok) {
         std::remove(tmp.c_str());
@@ -538,6 +558,12 @@ int pfb_ckpt3d_write(const char* path, const pfb_ckpt3d_params* rec, long long s
     return write3(path, rec, step, num_cells, cells, phi, base_measure_shards);
 }
 
+int pfb_ckpt3d_payload_words(const char* path, unsigned long long* words) {
+    clear_error();
+    if (!path || !words) return set_error(PFB_E_ARG, "PF3D payload: null argument");
+    return read3(path, nullptr, nullptr, nullptr, nullptr, words);
+}
+
 int pfb_sim3d_write_checkpoint(pfb_sim3d* s, const char* path, const pfb_ckpt3d_params* rec) {
     clear_error();
     if (!s || !path || !rec) return set_error(PFB_E_ARG, "write_checkpoint: null argument");
@@ -559,10 +585,13 @@ int pfb_sim3d_write_checkpoint(pfb_sim3d* s, const char* path, const pfb_ckpt3d_
     // the reference measures the current state before it writes
     rc = pfb_sim3d_measure_current(s);
     if (rc) return rc;
+    unsigned long long words = 0;
+    rc = pfb_sim3d_packed_words(s, &words);
+    if (rc) return rc;
     std::vector<pfb_cell3d> cells((size_t)N);
-    std::vector<float> phi((size_t)N * B * B * B);
+    std::vector<float> phi((size_t)words);
     rc = pfb_sim3d_get_cells(s, cells.data());
-    if (!rc) rc = pfb_sim3d_get_phi(s, phi.data());
+    if (!rc) rc = pfb_sim3d_get_packed(s, phi.data());
     if (rc) return rc;
     // the base measurement here reduces each cell over a cluster of 4 CTAs
     return write3(path, rec, step, N, cells.data(), phi.data(), 4);
@@ -572,10 +601,10 @@ pfb_sim3d* pfb_sim3d_create_from_checkpoint(const char* path, int device) {
     clear_error();
     pfb_ckpt3d_info info;
     pfb_ckpt3d_params rec;
-    if (read3(path, &info, &rec, nullptr, nullptr)) return nullptr;
-    const size_t words = (size_t)info.brick_edge * info.brick_edge * info.brick_edge;
+    unsigned long long words = 0;
+    if (read3(path, &info, &rec, nullptr, nullptr, &words)) return nullptr;
     std::vector<pfb_cell3d> cells((size_t)info.num_cells);
-    std::vector<float> phi((size_t)info.num_cells * words);
+    std::vector<float> phi((size_t)words);
     if (read3(path, &info, &rec, cells.data(), phi.data())) return nullptr;
     pfb_params3d p;
     if (pfb_ckpt3d_params_to(&rec, info.num_cells, &p)) return nullptr;

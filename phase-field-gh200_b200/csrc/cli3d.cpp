@@ -14,11 +14,13 @@
 // final checkpoint. --initial-centres reads the reference's centre tables
 // (periodic x,y,z; relaxed x,y for the slab and the one-layer channel;
 // channel x,y,z). Soft cells (--cancer-fraction, --gamma-cancer) take
-// their identities from the reference's Philox shuffle. Not part of this
-// build (exit status 2 with a message):
-// the memory modes, scratch slots, peer device and shard overrides. The
-// trajectory header and checkpoints state this build's measurement grouping
-// (4 CTAs per base cell, one-CTA promoted policy).
+// their identities from the reference's Philox shuffle. Cells whose support
+// reaches their brick grow into larger cubes (adaptive bricks) as in the
+// reference. Not part of this build (exit status 2 with a message): the
+// in-place memory modes (balanced, compact), scratch slots, peer device, and
+// measurement groupings other than this build's (--measure-shards 4,
+// --promoted-measure-shards 0), which the trajectory header and checkpoints
+// state.
 #include <algorithm>
 #include <cerrno>
 #include <cmath>
@@ -553,6 +555,32 @@ int parse(int argc, char** argv, Options* o) {
             const char* v = value();
             if (!v || !v[0]) return 2;
             o->centres_path = v;
+        } else if (!std::strcmp(a, "--memory-mode")) {
+            // the two-pool throughput layout is the only storage here
+            const char* v = value();
+            if (!v) return 2;
+            if (std::strcmp(v, "auto") && std::strcmp(v, "throughput")) {
+                if (!std::strcmp(v, "balanced") || !std::strcmp(v, "compact")) {
+                    std::fprintf(stderr, "[3d] --memory-mode %s: the in-place storage modes are not "
+                                         "provided by this build (use throughput)\n", v);
+                } else {
+                    std::fprintf(stderr, "[3d] --memory-mode expects auto, throughput, balanced, or "
+                                         "compact\n");
+                }
+                return 2;
+            }
+        } else if (!std::strcmp(a, "--measure-shards") || !std::strcmp(a, "--promoted-measure-shards")) {
+            // the measurement groupings are fixed: 4 CTAs per base cell, the
+            // one-CTA promoted policy (as the trajectory header states)
+            const char* v = value();
+            long long k = 0;
+            if (!v || !parse_int(a, v, -1, 1024, &k)) return 2;
+            const bool base = !std::strcmp(a, "--measure-shards");
+            if (k != (base ? kMeasureShards : 0)) {
+                std::fprintf(stderr, "[3d] %s %lld: this build measures with %s only\n", a, k,
+                             base ? "--measure-shards 4" : "--promoted-measure-shards 0");
+                return 2;
+            }
         } else if (!std::strcmp(a, "--boundary-out") || !std::strcmp(a, "--boundary-projection") ||
                    !std::strcmp(a, "--boundary-compression")) {
             const char* v = value();

@@ -48,7 +48,7 @@ __global__ void __launch_bounds__(kThreads3, 2) k_measure3d(const __grid_constan
     const int n = A.selection.ids ? A.selection.ids[slot] : slot;
     pfb_cell3d* cell = &A.cells[n];
     // Promoted cells are uniform over the cluster: every CTA returns.
-    if (cell->storage_edge != 0u) return;
+    if (cell->storage_edge > (uint32_t)B) return;
 
     PlaneRing<kMeasureRing> ring{reinterpret_cast<float*>(smem + kHeader), H.bars, B * B};
     ring.init();
@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(kThreads3, 2) k_measure3d(const __grid_constan
             if (!fold_receive<K>(H.fold, B, kPlaneWaitPolls, r)) atomicOr(&g_measure3d_status, 2u);
             if (lane == 0) {
                 int sx, sy, sz;
-                (void)commit_measure(A, cell, r, &sx, &sy, &sz);
+                (void)commit_measure(A, A.B, cell, r, &sx, &sy, &sz);
             }
         }
     }

@@ -273,12 +273,12 @@ __device__ __forceinline__ uint32_t raise_counted(pfb_cell3d* cell, uint32_t* gf
 }
 
 // Commit of the measured record (one thread): moments, support box,
-// phi_max, the recentring plan and the support-margin check. Returns the
-// flag bits raised for the cell; *sx, *sy, *sz receive the planned shift.
-__device__ __forceinline__ uint32_t commit_measure(const pfb_measure_args3d& A, pfb_cell3d* cell,
-                                                   const MeasureTotals& r, int* psx, int* psy,
-                                                   int* psz) {
-    const int B = A.B;
+// phi_max, the recentring plan and the support-margin check of a brick of
+// edge B. Returns the flag bits raised for the cell; *sx, *sy, *sz receive
+// the planned shift.
+__device__ __forceinline__ uint32_t commit_measure(const pfb_measure_args3d& A, int B,
+                                                   pfb_cell3d* cell, const MeasureTotals& r,
+                                                   int* psx, int* psy, int* psz) {
     uint32_t raised = 0u;
     raised |= raise_counted(cell, A.global_flags, PFB3D_FLAG_NONFINITE, r.nonfinite);
     raised |= raise_counted(cell, A.global_flags, PFB3D_FLAG_S_NEGATIVE, r.negative);

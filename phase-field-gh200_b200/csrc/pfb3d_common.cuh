@@ -23,6 +23,15 @@ namespace pfb {
 namespace p3 {
 
 constexpr int kBrickAlign = 8;
+// Adaptive bricks: a grown cube adds kBrickGrowth planes, rounded up to a
+// multiple of kBrickTier; a crop keeps kBrickShrinkSpare spare planes beyond
+// the support on every face; compaction runs every kBrickCompactEvery
+// accepted steps. Promoted cubes are at most kMaxPromotedEdge voxels wide.
+constexpr int kBrickGrowth = 32;
+constexpr int kBrickTier = 16;
+constexpr int kBrickShrinkSpare = 16;
+constexpr long long kBrickCompactEvery = 1024;
+constexpr int kMaxPromotedEdge = 1024;
 constexpr float kSupportEps3 = 1.0e-5f;
 constexpr double kSafetyMargin = 8.0;
 constexpr int kMaxShift3 = 4;

@@ -94,8 +94,8 @@ cudaError_t visit_order2d_launch(const pfb_cell2d* cell, uint32_t* perm, int N, 
 struct Boundary3D;
 Boundary3D* boundary3d_open(const char* path, const pfb_params3d& p, int projection,
                             long long interval, int compress);
-int boundary3d_capture(Boundary3D* b, const float* phi, const pfb_cell3d* cells, int B,
-                       cudaStream_t stream, long long step, double time);
+int boundary3d_capture(Boundary3D* b, const float* phi, float* const* cubes, const pfb_cell3d* cells,
+                       int B, cudaStream_t stream, long long step, double time);
 // complete != 0 writes the end record; the recorder is freed either way.
 int boundary3d_close(Boundary3D* b, int complete);
 
@@ -165,7 +165,8 @@ int scatter3d_launch(const pfb_scatter_args3d* a, cudaStream_t stream);
 int measure3d_read_status(unsigned* out, int clear);
 int update3d_read_status(unsigned* out, int clear);
 int check_measure(const pfb_measure_args3d* a);
-int check_update(const pfb_update_args3d* a);
+// pools = false: the base phi pools are not needed (promoted-cube launches)
+int check_update(const pfb_update_args3d* a, bool pools = true);
 // cluster size of the measurement (the fused step's where it applies)
 int measure3d_cluster(int B);
 // step3d.cu: fused measure + motion + update; cluster size 0 when the brick
@@ -174,6 +175,21 @@ int step3d_cluster(int B);
 size_t step3d_smem(int B);
 int step3d_launch(const pfb_measure_args3d* m, const pfb_update_args3d* u, cudaStream_t stream);
 int step3d_read_status(unsigned* out, int clear);
+// promote3d.cu: cells in their own cubes (storage_edge > B)
+int next_brick_edge3(int current, int maximum);
+int shrink_brick_edge3(int current, int minimum, const int* lo, const int* hi);
+int measure3d_promoted_launch(const pfb_measure_args3d* a, float* const* cubes, const int* ids,
+                              int count, int max_edge, cudaStream_t stream);
+int update3d_promoted_launch(const pfb_update_args3d* a, float* const* in, float* const* out,
+                             const int* ids, int count, int max_edge, cudaStream_t stream);
+int scatter3d_promoted_launch(const pfb_scatter_args3d* a, float* const* cubes, const int* ids,
+                              int count, int max_edge, int guard_fatal, cudaStream_t stream);
+int repair3d_promoted_launch(const pfb_update_args3d* a, float* const* in, float* const* out,
+                             const int* ids, int count, int max_edge, cudaStream_t stream);
+int copy_centred3d_launch(const float* src, int Es, float* dst, int Ed, cudaStream_t stream);
+int check_crops3d_launch(float* const* cubes, const pfb_cell3d* cells, const int* candidate,
+                         uint32_t* rejected, int N, int B, cudaStream_t stream);
+int promote3d_read_status(unsigned* out, int clear);
 }  // namespace p3
 
 }  // namespace pfb

@@ -71,6 +71,18 @@ struct pfb_sim3d {
     bool use_graph = true;
     cudaGraph_t graph = nullptr;     // two steps from buffer parity 0
     cudaGraphExec_t graph_exec = nullptr;
+    // adaptive bricks: cells whose support outgrew B live in their own cubes
+    // of edge storage_edge > B; cube[cur_phi][n] holds the current field
+    int max_edge = 0;                   // largest cube the domain allows
+    std::vector<float*> h_cube[2];      // per cell; null for base cells
+    float** d_cube[2] = {nullptr, nullptr};
+    std::vector<int> prom_ids;          // promoted cells in id order
+    int* d_prom_ids = nullptr;
+    int prom_edge = 0;                  // largest promoted edge
+    uint32_t* d_requests = nullptr;     // support-exhaustion requests (restore pass)
+    long long accepted = 0;             // accepted steps at the last synchronisation
+    long long next_compact = 0;         // accepted step of the next compaction
+    long long recoveries = 0;
 
     void drop_graph() {
         if (graph_exec) cudaGraphExecDestroy(graph_exec);
@@ -95,7 +107,14 @@ struct pfb_sim3d {
         cudaFree(d_wall_psi);
         cudaFree(d_centres);
         cudaFree(d_order);
+        for (int b = 0; b < 2; ++b) {
+            for (float* c : h_cube[b]) cudaFree(c);
+            cudaFree(d_cube[b]);
+        }
+        cudaFree(d_prom_ids);
+        cudaFree(d_requests);
     }
+    int prom_count() const { return (int)prom_ids.size(); }
 };
 
 namespace pfb {
@@ -111,12 +130,25 @@ namespace {
 // of phi^2 psi_w^2(z) (wall overlap) and of phi^2 outside the slit. One CTA
 // per cell; warp sums, then ascending warps.
 constexpr int kWallThreads = 256;
+// Brick of cell n: its own cube (edge = storage edge) when it has one, else
+// its slot of the base pool.
+__device__ __forceinline__ const float* cell_brick(const float* phi, float* const* cubes,
+                                                  const pfb_cell3d* cells, int n, int B, int* E) {
+    if (cubes && cubes[n]) {
+        *E = (int)cells[n].storage_edge;
+        return cubes[n];
+    }
+    *E = B;
+    return phi + (size_t)n * B * B * B;
+}
+
 __global__ void __launch_bounds__(kWallThreads)
-    k_wall_diag3d(const float* phi, pfb_cell3d* cells, int B, int nz, int pad, int H,
-                  const float* psi) {
+    k_wall_diag3d(const float* phi, float* const* cubes, pfb_cell3d* cells, int B0, int nz, int pad,
+                  int H, const float* psi) {
     const int n = blockIdx.x;
+    int B;
+    const float* brick = cell_brick(phi, cubes, cells, n, B0, &B);
     const size_t words = (size_t)B * B * B, plane = (size_t)B * B;
-    const float* brick = phi + (size_t)n * words;
     const int64_t oz = cells[n].origin_z;
     double overlap = 0.0, outside = 0.0;
     for (size_t q = threadIdx.x; q < words; q += kWallThreads) {
@@ -157,11 +189,12 @@ struct Verify3 {
     unsigned int nonfinite, edge;
 };
 __global__ void __launch_bounds__(kWallThreads)
-    k_verify3d(const float* phi, const pfb_cell3d* cells, int B, int nz, int periodic, int slab,
-               Verify3* out) {
+    k_verify3d(const float* phi, float* const* cubes, const pfb_cell3d* cells, int B0, int nz,
+               int periodic, int slab, Verify3* out) {
     const int n = blockIdx.x;
+    int B;
+    const float* brick = cell_brick(phi, cubes, cells, n, B0, &B);
     const size_t words = (size_t)B * B * B, plane = (size_t)B * B;
-    const float* brick = phi + (size_t)n * words;
     const int64_t oz = cells[n].origin_z;
     double vol = 0.0;
     unsigned bad = 0, edge = 0;
@@ -388,19 +421,27 @@ int launch_step(pfb_sim3d* s, bool full) {
             "snapshot accepted cells");
     const pfb_measure_args3d m = measure_args(s, true, full);
     const pfb_update_args3d u = update_args(s);
-    if (s->fused) {
+    const int np = s->prom_count();
+    float* const* cur = s->d_cube[s->cur_phi];
+    float* const* nxt = s->d_cube[1 - s->cur_phi];
+    if (s->fused && np == 0) {
         PFB3_RC(clear3d_launch(s->d_S[1 - s->cur_S], &s->L, nullptr, s->stream));
         PFB3_RC(step3d_launch(&m, &u, s->stream));
     } else {
+        // base bricks, then the promoted cubes; motion after every measurement
         PFB3_RC(measure3d_launch(&m, s->stream));
+        if (np) PFB3_RC(measure3d_promoted_launch(&m, cur, s->d_prom_ids, np, s->max_edge, s->stream));
         PFB3_RC(motion3d_launch(&m, s->stream));
         PFB3_RC(clear3d_launch(s->d_S[1 - s->cur_S], &s->L, nullptr, s->stream));
         PFB3_RC(update3d_launch(&u, s->stream));
+        if (np)
+            PFB3_RC(update3d_promoted_launch(&u, cur, nxt, s->d_prom_ids, np, s->max_edge, s->stream));
     }
     PFB3_RC(repair3d_launch(&u, s->stream));
+    if (np) PFB3_RC(repair3d_promoted_launch(&u, cur, nxt, s->d_prom_ids, np, s->max_edge, s->stream));
     PFB3_RC(pfb3d_finalize_origins(s->d_cells, s->N, s->d_flags, s->stream));
-    PFB3_RC(pfb3d_restore_cells_after_fatal(s->d_cells, s->d_accepted, s->N, s->d_flags, nullptr,
-                                            s->stream));
+    PFB3_RC(pfb3d_restore_cells_after_fatal(s->d_cells, s->d_accepted, s->N, s->d_flags,
+                                            s->d_requests, s->stream));
     PFB3_RC(pfb3d_advance_step(s->d_step, s->d_flags, s->stream));
     return PFB_OK;
 }
@@ -414,6 +455,251 @@ int one_step(pfb_sim3d* s) {
     PFB3_RC(launch_step(s, full_step(s, s->steps_done)));
     flip(s);
     ++s->steps_done;
+    return PFB_OK;
+}
+
+// The current aggregate rebuilt from the current fields (reference
+// Sim3D::reconstruct_current_S).
+int reconstruct_S(pfb_sim3d* s) {
+    PFB3_RC(clear3d_launch(s->d_S[s->cur_S], &s->L, nullptr, s->stream));
+    pfb_scatter_args3d sa{};
+    sa.phi = s->d_phi[s->cur_phi];
+    sa.cells = s->d_cells;
+    sa.S = s->d_S[s->cur_S];
+    sa.global_flags = s->d_flags;
+    sa.layout = s->L;
+    sa.N = s->N;
+    sa.B = s->B;
+    PFB3_RC(scatter3d_launch(&sa, s->stream));
+    if (s->prom_count())
+        PFB3_RC(scatter3d_promoted_launch(&sa, s->d_cube[s->cur_phi], s->d_prom_ids, s->prom_count(),
+                                          s->max_edge, 0, s->stream));
+    return PFB_OK;
+}
+
+// Measurement of every cell on the current field (no tumble); the motion
+// only when asked (reference Sim3D::refresh_measurements).
+int refresh(pfb_sim3d* s, bool surface, bool motion) {
+    const pfb_measure_args3d m = measure_args(s, false, surface);
+    PFB3_RC(measure3d_launch(&m, s->stream));
+    if (s->prom_count())
+        PFB3_RC(measure3d_promoted_launch(&m, s->d_cube[s->cur_phi], s->d_prom_ids, s->prom_count(),
+                                          s->max_edge, s->stream));
+    if (motion) PFB3_RC(motion3d_launch(&m, s->stream));
+    return PFB_OK;
+}
+
+int edge_of(const pfb_sim3d* s, const pfb_cell3d& c) {
+    return c.storage_edge > (uint32_t)s->B ? (int)c.storage_edge : s->B;
+}
+
+// A cell record moved into a centred cube of edge En (reference
+// adaptive_storage.cu translate_state): the world field stays in place.
+bool translate_record(pfb_cell3d* c, int Eo, int En) {
+    const int off = (En - Eo) / 2;
+    int64_t* o[3] = {&c->origin_x, &c->origin_y, &c->origin_z};
+    for (int64_t* v : o) {
+        if ((off > 0 && *v < INT64_MIN + off) || (off < 0 && *v > INT64_MAX + off)) return false;
+        *v -= off;
+    }
+    c->Cx += (double)off * c->V;
+    c->Cy += (double)off * c->V;
+    c->Cz += (double)off * c->V;
+    if (!std::isfinite(c->Cx) || !std::isfinite(c->Cy) || !std::isfinite(c->Cz)) return false;
+    if (c->bb_hi_x >= c->bb_lo_x) {
+        c->bb_lo_x += off; c->bb_hi_x += off;
+        c->bb_lo_y += off; c->bb_hi_y += off;
+        c->bb_lo_z += off; c->bb_hi_z += off;
+    }
+    c->pending_shift_x = c->pending_shift_y = c->pending_shift_z = 0;
+    c->storage_edge = (uint32_t)En;
+    c->flags &= ~((1u << PFB3D_FLAG_SUPPORT_EXHAUSTED) | (1u << PFB3D_FLAG_SUPPORT_EDGE));
+    return true;
+}
+
+int upload_tables(pfb_sim3d* s) {
+    for (int b = 0; b < 2; ++b)
+        PFB3_CU(cudaMemcpy(s->d_cube[b], s->h_cube[b].data(), (size_t)s->N * sizeof(float*),
+                           cudaMemcpyHostToDevice),
+                "upload cube table");
+    if (!s->prom_ids.empty())
+        PFB3_CU(cudaMemcpy(s->d_prom_ids, s->prom_ids.data(), s->prom_ids.size() * sizeof(int),
+                           cudaMemcpyHostToDevice),
+                "upload promoted ids");
+    return PFB_OK;
+}
+
+// Move the requested cells (id, new edge) into centred cubes of the new edge
+// (a new edge equal to B returns the cell to its base slot), transactionally:
+// every new cube is allocated and filled before any table changes (reference
+// Sim3D::resize_cells). `cells` holds the current records on entry and the
+// installed ones on success.
+int resize_cells(pfb_sim3d* s, const std::vector<std::pair<int, int>>& req,
+                 std::vector<pfb_cell3d>* cells) {
+    PFB3_CU(cudaStreamSynchronize(s->stream), "sync");
+    std::vector<pfb_cell3d> next = *cells;
+    struct Move { int id, Eo, En; float* cube[2]; };
+    std::vector<Move> moves;
+    auto release = [&]() {
+        for (Move& m : moves)
+            for (float* c : m.cube) cudaFree(c);
+    };
+    for (const auto& r : req) {
+        const int n = r.first, En = r.second;
+        const int Eo = edge_of(s, (*cells)[(size_t)n]);
+        if (n < 0 || n >= s->N || En < s->B || En > s->max_edge || En % kBrickAlign != 0 || En == Eo ||
+            !translate_record(&next[(size_t)n], Eo, En)) {
+            release();
+            return set_error(PFB_E_STATE, "resize of cell %d from %d to %d refused", n, Eo, En);
+        }
+        Move m{n, Eo, En, {nullptr, nullptr}};
+        if (En > s->B)
+            for (float*& c : m.cube)
+                if (cudaMalloc(&c, (size_t)En * En * En * sizeof(float)) != cudaSuccess) {
+                    moves.push_back(m);
+                    release();
+                    return set_error(PFB_E_NOMEM, "no device memory for a %d^3 cube of cell %d", En, n);
+                }
+        moves.push_back(m);
+    }
+    const size_t bw = (size_t)s->B * s->B * s->B;
+    for (Move& m : moves) {
+        const float* src = m.Eo > s->B ? s->h_cube[s->cur_phi][(size_t)m.id]
+                                       : s->d_phi[s->cur_phi] + (size_t)m.id * bw;
+        for (int b = 0; b < 2; ++b) {
+            float* dst = m.En > s->B ? m.cube[b] : s->d_phi[b] + (size_t)m.id * bw;
+            const int rc = copy_centred3d_launch(src, m.Eo, dst, m.En, s->stream);
+            if (rc) {
+                release();
+                return rc;
+            }
+        }
+    }
+    if (cudaStreamSynchronize(s->stream) != cudaSuccess) {
+        release();
+        return set_error(PFB_E_CUDA, "cube copies failed");
+    }
+    // install: tables, id list, records; then free the replaced cubes
+    for (Move& m : moves)
+        for (int b = 0; b < 2; ++b) {
+            float* old = s->h_cube[b][(size_t)m.id];
+            s->h_cube[b][(size_t)m.id] = m.cube[b];
+            m.cube[b] = old;
+        }
+    s->prom_ids.clear();
+    for (int n = 0; n < s->N; ++n)
+        if (next[(size_t)n].storage_edge > (uint32_t)s->B) s->prom_ids.push_back(n);
+    PFB3_RC(upload_tables(s));
+    PFB3_CU(cudaMemcpy(s->d_cells, next.data(), next.size() * sizeof(pfb_cell3d), cudaMemcpyHostToDevice),
+            "install resized records");
+    s->prom_edge = 0;
+    for (int n : s->prom_ids) s->prom_edge = std::max(s->prom_edge, (int)next[(size_t)n].storage_edge);
+    release();  // the replaced cubes
+    cells->swap(next);
+    s->drop_graph();  // launch shapes changed
+    return PFB_OK;
+}
+
+int read_flags(pfb_sim3d* s, uint32_t* f) {
+    PFB3_CU(cudaStreamSynchronize(s->stream), "sync");
+    PFB3_CU(cudaMemcpy(f, s->d_flags, PFB3D_FLAG_COUNT * sizeof(uint32_t), cudaMemcpyDeviceToHost),
+            "read flags");
+    return PFB_OK;
+}
+
+bool fatal_in(const uint32_t* f) {
+    for (int i = 0; i < PFB3D_FLAG_COUNT; ++i)
+        if (((PFB3D_FATAL_MASK >> i) & 1u) && f[i]) return true;
+    return false;
+}
+
+// Support exhaustion as the only fatal flag: grow every requesting cell to the
+// next tier, rebuild the aggregate, remeasure without motion and check again
+// (reference Sim3D::recover_support_exhaustion). *ok false: not recoverable
+// (the state is left as the rolled-back step left it).
+int recover_support(pfb_sim3d* s, const uint32_t* flags, bool* ok) {
+    *ok = false;
+    if (!flags[PFB3D_FLAG_SUPPORT_EXHAUSTED]) return PFB_OK;
+    for (int f = 0; f < PFB3D_FLAG_COUNT; ++f)
+        if (f != PFB3D_FLAG_SUPPORT_EXHAUSTED && ((PFB3D_FATAL_MASK >> f) & 1u) && flags[f]) return PFB_OK;
+    std::vector<pfb_cell3d> cells((size_t)s->N);
+    std::vector<uint32_t> requests((size_t)s->N);
+    PFB3_CU(cudaMemcpy(cells.data(), s->d_cells, cells.size() * sizeof(pfb_cell3d), cudaMemcpyDeviceToHost),
+            "read cells");
+    PFB3_CU(cudaMemcpy(requests.data(), s->d_requests, requests.size() * sizeof(uint32_t),
+                       cudaMemcpyDeviceToHost),
+            "read support requests");
+    std::vector<std::pair<int, int>> req;
+    for (int n = 0; n < s->N; ++n) {
+        const pfb_cell3d& c = cells[(size_t)n];
+        if (!requests[(size_t)n] && !(c.flags & (1u << PFB3D_FLAG_SUPPORT_EXHAUSTED))) continue;
+        const int next = next_brick_edge3(edge_of(s, c), s->max_edge);
+        if (next == 0 || next > kMaxPromotedEdge) return PFB_OK;  // no larger cube fits the domain
+        req.emplace_back(n, next);
+    }
+    if (req.empty()) return PFB_OK;
+    PFB3_RC(resize_cells(s, req, &cells));
+    PFB3_CU(cudaMemsetAsync(s->d_flags + PFB3D_FLAG_SUPPORT_EXHAUSTED, 0, sizeof(uint32_t), s->stream),
+            "clear flag");
+    PFB3_CU(cudaMemsetAsync(s->d_flags + PFB3D_FLAG_SUPPORT_EDGE, 0, sizeof(uint32_t), s->stream),
+            "clear flag");
+    PFB3_CU(cudaMemsetAsync(s->d_requests, 0, (size_t)s->N * sizeof(uint32_t), s->stream), "clear requests");
+    PFB3_RC(reconstruct_S(s));
+    PFB3_RC(refresh(s, false, false));
+    ++s->recoveries;
+    uint32_t after[PFB3D_FLAG_COUNT];
+    PFB3_RC(read_flags(s, after));
+    if (after[PFB3D_FLAG_SUPPORT_EXHAUSTED]) return recover_support(s, after, ok);
+    *ok = !fatal_in(after);
+    return PFB_OK;
+}
+
+// Every kBrickCompactEvery accepted steps: crop promoted cubes whose support
+// leaves enough exactly-zero shell (reference Sim3D::compact_promoted_fields).
+int compact_cubes(pfb_sim3d* s) {
+    if (s->prom_ids.empty()) return PFB_OK;
+    PFB3_RC(refresh(s, false, false));  // support boxes of the accepted field
+    std::vector<pfb_cell3d> cells((size_t)s->N);
+    PFB3_CU(cudaStreamSynchronize(s->stream), "sync");
+    PFB3_CU(cudaMemcpy(cells.data(), s->d_cells, cells.size() * sizeof(pfb_cell3d), cudaMemcpyDeviceToHost),
+            "read cells");
+    std::vector<int> cand((size_t)s->N, 0);
+    bool any = false;
+    for (int n : s->prom_ids) {
+        const pfb_cell3d& c = cells[(size_t)n];
+        const int lo[3] = {c.bb_lo_x, c.bb_lo_y, c.bb_lo_z}, hi[3] = {c.bb_hi_x, c.bb_hi_y, c.bb_hi_z};
+        const int E = edge_of(s, c);
+        const int smaller = shrink_brick_edge3(E, s->B, lo, hi);
+        if (smaller < E) {
+            cand[(size_t)n] = smaller;
+            any = true;
+        }
+    }
+    if (!any) return PFB_OK;
+    int* d_cand = nullptr;
+    uint32_t* d_rej = nullptr;
+    std::vector<uint32_t> rej((size_t)s->N, 0u);
+    int rc = PFB_OK;
+    if (cudaMalloc(&d_cand, cand.size() * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&d_rej, rej.size() * sizeof(uint32_t)) != cudaSuccess ||
+        cudaMemcpy(d_cand, cand.data(), cand.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(d_rej, 0, rej.size() * sizeof(uint32_t)) != cudaSuccess)
+        rc = set_error(PFB_E_CUDA, "crop check buffers");
+    if (!rc) rc = check_crops3d_launch(s->d_cube[s->cur_phi], s->d_cells, d_cand, d_rej, s->N, s->B, s->stream);
+    if (!rc && (cudaStreamSynchronize(s->stream) != cudaSuccess ||
+                cudaMemcpy(rej.data(), d_rej, rej.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost) !=
+                    cudaSuccess))
+        rc = set_error(PFB_E_CUDA, "crop check");
+    cudaFree(d_cand);
+    cudaFree(d_rej);
+    if (rc) return rc;
+    std::vector<std::pair<int, int>> req;
+    for (int n : s->prom_ids)
+        if (cand[(size_t)n] && !rej[(size_t)n]) req.emplace_back(n, cand[(size_t)n]);
+    if (req.empty()) return PFB_OK;
+    PFB3_RC(resize_cells(s, req, &cells));
+    PFB3_RC(reconstruct_S(s));
+    PFB3_RC(refresh(s, false, false));
     return PFB_OK;
 }
 
@@ -437,7 +723,8 @@ int build_graph(pfb_sim3d* s) {
     return PFB_OK;
 }
 
-int advance_impl(pfb_sim3d* s, long long steps) {
+// Run `steps` step attempts (graph pairs where possible).
+int attempt_steps(pfb_sim3d* s, long long steps) {
     while (steps > 0) {
         if (s->steps_done - s->order_step >= kOrderRefresh) PFB3_RC(refresh_order(s));
         const bool pair = s->use_graph && s->cur_phi == 0 && steps >= 2 &&
@@ -450,6 +737,37 @@ int advance_impl(pfb_sim3d* s, long long steps) {
         } else {
             PFB3_RC(one_step(s));
             --steps;
+        }
+    }
+    return PFB_OK;
+}
+
+// Advance by `steps` accepted steps. A step that exhausts a cell's support is
+// rolled back; at the next synchronisation the cell's brick grows to the next
+// tier and the rolled-back steps are retried. Stops early, leaving the flags
+// for the caller, at any other fatal flag. Promoted cubes are compacted at
+// every multiple of kBrickCompactEvery accepted steps.
+int advance_impl(pfb_sim3d* s, long long steps) {
+    const long long target = s->accepted + steps;
+    while (s->accepted < target) {
+        // synchronisations land on the compaction multiples
+        const long long chunk = std::min(target, s->next_compact) - s->accepted;
+        PFB3_RC(attempt_steps(s, chunk));
+        uint32_t f[PFB3D_FLAG_COUNT];
+        PFB3_RC(read_flags(s, f));
+        uint64_t acc = 0;
+        PFB3_CU(cudaMemcpy(&acc, s->d_step, sizeof(acc), cudaMemcpyDeviceToHost), "read step");
+        s->accepted = (long long)acc;
+        s->steps_done = s->accepted;
+        if (fatal_in(f)) {
+            bool ok = false;
+            PFB3_RC(recover_support(s, f, &ok));
+            if (!ok) return PFB_OK;
+            continue;
+        }
+        if (s->accepted >= s->next_compact) {
+            PFB3_RC(compact_cubes(s));
+            s->next_compact = (s->accepted / kBrickCompactEvery + 1) * kBrickCompactEvery;
         }
     }
     return PFB_OK;
@@ -495,8 +813,27 @@ int alloc_impl(pfb_sim3d* s, const pfb_params3d* pp, int device) {
     }
     PFB3_CU(cudaMemsetAsync(s->d_flags, 0, PFB3D_FLAG_COUNT * sizeof(uint32_t), s->stream), "memset");
     PFB3_CU(cudaMemsetAsync(s->d_step, 0, sizeof(uint64_t), s->stream), "memset");
+    // adaptive bricks: the largest cube that fits the domain (reference
+    // src/pf3d/sim.cu:291-293), empty tables, no requests
+    const int dom = hard_wall_channel(p.boundary_flags) ? std::min(p.Nx, p.Ny)
+                                                        : std::min(std::min(p.Nx, p.Ny), p.Nz);
+    s->max_edge = std::min((dom - 1) / kBrickAlign * kBrickAlign, kMaxPromotedEdge);
+    for (int b = 0; b < 2; ++b) {
+        s->h_cube[b].assign((size_t)s->N, nullptr);
+        PFB3_CU(cudaMalloc(&s->d_cube[b], (size_t)s->N * sizeof(float*)), "cudaMalloc(cube table)");
+        PFB3_CU(cudaMemsetAsync(s->d_cube[b], 0, (size_t)s->N * sizeof(float*), s->stream), "memset");
+    }
+    PFB3_CU(cudaMalloc(&s->d_prom_ids, (size_t)s->N * sizeof(int)), "cudaMalloc(promoted ids)");
+    PFB3_CU(cudaMalloc(&s->d_requests, (size_t)s->N * sizeof(uint32_t)), "cudaMalloc(requests)");
+    PFB3_CU(cudaMemsetAsync(s->d_requests, 0, (size_t)s->N * sizeof(uint32_t), s->stream), "memset");
     if (hard_wall_channel(p.boundary_flags)) PFB3_RC(upload_wall(s));
     return PFB_OK;
+}
+
+void set_accepted(pfb_sim3d* s, long long step) {
+    s->accepted = step;
+    s->steps_done = step;
+    s->next_compact = (step / kBrickCompactEvery + 1) * kBrickCompactEvery;
 }
 
 // The measurement that follows a fresh seeding or a restore (reference
@@ -504,20 +841,8 @@ int alloc_impl(pfb_sim3d* s, const pfb_params3d* pp, int device) {
 // src/pf3d/sim.cu:877, 1175): aggregate from the current bricks, then
 // moments, surface, recentring plan and velocities without a tumble.
 int remeasure_impl(pfb_sim3d* s) {
-    PFB3_RC(clear3d_launch(s->d_S[0], &s->L, nullptr, s->stream));
-    pfb_scatter_args3d sa{};
-    sa.phi = s->d_phi[0];
-    sa.cells = s->d_cells;
-    sa.S = s->d_S[0];
-    sa.global_flags = s->d_flags;
-    sa.layout = s->L;
-    sa.N = s->N;
-    sa.B = s->B;
-    PFB3_RC(scatter3d_launch(&sa, s->stream));
-    const pfb_measure_args3d m = measure_args(s, false, true);
-    PFB3_RC(measure3d_launch(&m, s->stream));
-    PFB3_RC(motion3d_launch(&m, s->stream));
-    return PFB_OK;
+    PFB3_RC(reconstruct_S(s));
+    return refresh(s, true, true);
 }
 
 int create_impl(pfb_sim3d* s, const pfb_params3d* pp, const pfb_vec3* centres, int device) {
@@ -570,33 +895,73 @@ int create_impl(pfb_sim3d* s, const pfb_params3d* pp, const pfb_vec3* centres, i
     PFB3_RC(init3d_launch(&ia, s->stream));
     PFB3_RC(remeasure_impl(s));
     PFB3_CU(cudaStreamSynchronize(s->stream), "fresh initialisation");
+    set_accepted(s, 0);
     return refresh_order(s);
 }
 
-// Restore (reference Sim3D::init_checkpoint, src/pf3d/sim.cu:794-885): cell
-// records and base bricks of step `step` into the current buffers, the step
-// counter, then the aggregate and one measurement.
-int restore_impl(pfb_sim3d* s, const pfb_params3d* pp, const pfb_cell3d* cells, const float* phi,
+// Restore (reference Sim3D::init_checkpoint and install_checkpoint_promotions,
+// src/pf3d/sim.cu:794-885, adaptive_storage.cu:264-310): cell records and
+// fields of step `step` into the current buffers, the step counter, then the
+// aggregate and one measurement. `phi` packs each cell's field in cell order:
+// B^3 values for a base cell, E^3 for a cell whose storage edge E exceeds B.
+int restore_impl(pfb_sim3d* s, const pfb_params3d* pp, const pfb_cell3d* cells_in, const float* phi,
                  long long step, int device) {
-    if (!cells || !phi || step < 0) return set_error(PFB_E_ARG, "restore: bad argument");
+    if (!cells_in || !phi || step < 0) return set_error(PFB_E_ARG, "restore: bad argument");
     PFB3_RC(alloc_impl(s, pp, device));
-    for (int i = 0; i < s->N; ++i)
-        if (cells[i].global_id != i || (cells[i].storage_edge != 0 && (int)cells[i].storage_edge != s->B))
-            return set_error(PFB_E_ARG, "restore: cell %d is not a canonical base-brick record", i);
-    PFB3_CU(cudaMemcpyAsync(s->d_cells, cells, (size_t)s->N * sizeof(pfb_cell3d), cudaMemcpyHostToDevice,
+    std::vector<pfb_cell3d> cells(cells_in, cells_in + s->N);
+    for (int i = 0; i < s->N; ++i) {
+        pfb_cell3d& c = cells[(size_t)i];
+        if (c.storage_edge == (uint32_t)s->B) c.storage_edge = 0;  // a base record
+        const bool ok = c.global_id == i &&
+                        (c.storage_edge == 0 ||
+                         (c.storage_edge > (uint32_t)s->B && (int)c.storage_edge <= s->max_edge &&
+                          c.storage_edge % kBrickAlign == 0));
+        if (!ok) return set_error(PFB_E_ARG, "restore: cell %d has an invalid id or storage edge", i);
+    }
+    const size_t bw = s->cell_words;
+    size_t off = 0;
+    for (int i = 0; i < s->N; ++i) {
+        const int E = edge_of(s, cells[(size_t)i]);
+        const size_t words = (size_t)E * E * E;
+        if (E == s->B) {
+            PFB3_CU(cudaMemcpy(s->d_phi[0] + (size_t)i * bw, phi + off, words * sizeof(float),
+                               cudaMemcpyHostToDevice),
+                    "upload brick");
+        } else {
+            for (int b = 0; b < 2; ++b) {
+                PFB3_CU(cudaMalloc(&s->h_cube[b][(size_t)i], words * sizeof(float)), "cudaMalloc(cube)");
+                PFB3_CU(cudaMemcpy(s->h_cube[b][(size_t)i], phi + off, words * sizeof(float),
+                                   cudaMemcpyHostToDevice),
+                        "upload cube");
+            }
+            s->prom_ids.push_back(i);
+            s->prom_edge = std::max(s->prom_edge, E);
+        }
+        off += words;
+    }
+    PFB3_RC(upload_tables(s));
+    PFB3_CU(cudaMemcpyAsync(s->d_cells, cells.data(), (size_t)s->N * sizeof(pfb_cell3d), cudaMemcpyHostToDevice,
                             s->stream), "upload cells");
-    PFB3_CU(cudaMemcpyAsync(s->d_phi[0], phi, (size_t)s->N * s->cell_words * sizeof(float),
-                            cudaMemcpyHostToDevice, s->stream), "upload phi");
     PFB3_CU(cudaMemsetAsync(s->d_phi[1], 0, (size_t)s->N * s->cell_words * sizeof(float), s->stream),
             "clear phi");
     const uint64_t st = (uint64_t)step;
     PFB3_CU(cudaMemcpyAsync(s->d_step, &st, sizeof(st), cudaMemcpyHostToDevice, s->stream), "step");
-    s->steps_done = step;
+    set_accepted(s, step);
     s->cur_phi = 0;
     s->cur_S = 0;
     PFB3_RC(remeasure_impl(s));
     PFB3_CU(cudaStreamSynchronize(s->stream), "restore");
     return refresh_order(s);
+}
+
+// Values of the packed field of the current state (each cell's own edge).
+size_t packed_words(const pfb_sim3d* s, const std::vector<pfb_cell3d>& cells) {
+    size_t w = 0;
+    for (const pfb_cell3d& c : cells) {
+        const size_t E = (size_t)edge_of(s, c);
+        w += E * E * E;
+    }
+    return w;
 }
 
 }  // namespace
@@ -647,7 +1012,8 @@ int pfb_sim3d_measure_wall(pfb_sim3d* s) {
     if (!hard_wall_channel(s->p.boundary_flags) || !s->d_wall_psi)
         return set_error(PFB_E_CONFIG, "wall diagnostics need the hard-wall channel");
     PFB3_CU(cudaSetDevice(s->device), "cudaSetDevice");
-    k_wall_diag3d<<<s->N, kWallThreads, 0, s->stream>>>(s->d_phi[s->cur_phi], s->d_cells, s->B,
+    k_wall_diag3d<<<s->N, kWallThreads, 0, s->stream>>>(s->d_phi[s->cur_phi], s->d_cube[s->cur_phi],
+                                                       s->d_cells, s->B,
                                                        s->p.Nz, s->p.channel_padding,
                                                        s->p.channel_height, s->d_wall_psi);
     PFB3_CU(cudaGetLastError(), "wall diagnostics");
@@ -670,7 +1036,8 @@ int pfb_sim3d_verify(pfb_sim3d* s, double* max_rel_V, uint32_t* max_S,
         cudaMemsetAsync(d_m, 0, 4, s->stream) != cudaSuccess) {
         rc = set_error(PFB_E_CUDA, "verify: allocation failed");
     } else {
-        k_verify3d<<<s->N, kWallThreads, 0, s->stream>>>(s->d_phi[s->cur_phi], s->d_cells, s->B, s->p.Nz,
+        k_verify3d<<<s->N, kWallThreads, 0, s->stream>>>(s->d_phi[s->cur_phi], s->d_cube[s->cur_phi],
+                                                         s->d_cells, s->B, s->p.Nz,
                                                          periodic ? 1 : 0,
                                                          substrate_slab(s->p.boundary_flags) ? 1 : 0, d_r);
         k_max_u32<<<148, 256, 0, s->stream>>>(s->d_S[s->cur_S], s->s_words, d_m);
@@ -709,7 +1076,8 @@ int pfb_sim3d_boundary_open(pfb_sim3d* s, const char* path, int projection, long
 int pfb_sim3d_boundary_capture(pfb_sim3d* s) {
     if (!s || !s->bnd) return set_error(PFB_E_STATE, "no boundary recorder is open");
     PFB3_CU(cudaSetDevice(s->device), "cudaSetDevice");
-    return pfb::boundary3d_capture(s->bnd, s->d_phi[s->cur_phi], s->d_cells, s->B, s->stream,
+    return pfb::boundary3d_capture(s->bnd, s->d_phi[s->cur_phi], s->d_cube[s->cur_phi], s->d_cells, s->B,
+                                   s->stream,
                               s->steps_done, (double)s->steps_done * s->p.dt);
 }
 
@@ -723,9 +1091,7 @@ int pfb_sim3d_boundary_close(pfb_sim3d* s, int complete) {
 int pfb_sim3d_measure_current(pfb_sim3d* s) {
     if (!s) return set_error(PFB_E_ARG, "null sim");
     PFB3_CU(cudaSetDevice(s->device), "cudaSetDevice");
-    const pfb_measure_args3d m = measure_args(s, false, true);
-    PFB3_RC(measure3d_launch(&m, s->stream));
-    PFB3_RC(motion3d_launch(&m, s->stream));
+    PFB3_RC(refresh(s, true, true));
     PFB3_CU(cudaStreamSynchronize(s->stream), "measure_current");
     return PFB_OK;
 }
@@ -799,6 +1165,37 @@ int pfb_sim3d_get_phi(pfb_sim3d* s, float* out) {
             "copy phi");
     return PFB_OK;
 }
+
+int pfb_sim3d_packed_words(pfb_sim3d* s, unsigned long long* words) {
+    if (!s || !words) return set_error(PFB_E_ARG, "null argument");
+    std::vector<pfb_cell3d> c((size_t)s->N);
+    PFB3_RC(pfb_sim3d_get_cells(s, c.data()));
+    *words = packed_words(s, c);
+    return PFB_OK;
+}
+
+int pfb_sim3d_get_packed(pfb_sim3d* s, float* out) {
+    if (!s || !out) return set_error(PFB_E_ARG, "null argument");
+    std::vector<pfb_cell3d> c((size_t)s->N);
+    PFB3_RC(pfb_sim3d_get_cells(s, c.data()));
+    size_t off = 0;
+    for (int n = 0; n < s->N; ++n) {
+        const int E = edge_of(s, c[(size_t)n]);
+        const size_t words = (size_t)E * E * E;
+        const float* src = E > s->B ? s->h_cube[s->cur_phi][(size_t)n]
+                                    : s->d_phi[s->cur_phi] + (size_t)n * s->cell_words;
+        if (!src) return set_error(PFB_E_STATE, "cell %d has no cube of edge %d", n, E);
+        PFB3_CU(cudaMemcpy(out + off, src, words * sizeof(float), cudaMemcpyDeviceToHost), "copy field");
+        off += words;
+    }
+    return PFB_OK;
+}
+
+int pfb_sim3d_promoted_count(const pfb_sim3d* s) { return s ? s->prom_count() : -1; }
+
+int pfb_sim3d_max_edge(const pfb_sim3d* s) { return s ? s->max_edge : -1; }
+
+long long pfb_sim3d_recoveries(const pfb_sim3d* s) { return s ? s->recoveries : -1; }
 
 int pfb_sim3d_get_S(pfb_sim3d* s, uint32_t* out) {
     if (!s || !out) return set_error(PFB_E_ARG, "null argument");

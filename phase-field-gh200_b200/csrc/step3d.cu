@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(kThreads3, 2) k_step3d(const __grid_constant__
     const int n = A.selection.ids ? A.selection.ids[slot_cell] : slot_cell;
     pfb_cell3d* cell = &A.cells[n];
     // promoted cells are uniform over the cluster: every CTA returns
-    if (cell->storage_edge != 0u) return;
+    if (cell->storage_edge > (uint32_t)B) return;
     const uint32_t flags0 = cell->flags;
     const pfb_layout3d L = A.layout;
     const int64_t oz = cell->origin_z;
@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(kThreads3, 2) k_step3d(const __grid_constant__
             if (lane == 0) {
                 if (!rok) atomicOr(&g_step3d_status, 2u);
                 int sx = 0, sy = 0, sz = 0;
-                const uint32_t raised = rok ? commit_measure(A, cell, r, &sx, &sy, &sz) : 0u;
+                const uint32_t raised = rok ? commit_measure(A, A.B, cell, r, &sx, &sy, &sz) : 0u;
                 const bool fatal = !rok || ((flags0 | raised) & PFB3D_FATAL_MASK) != 0u ||
                                    fatal_counters(A.global_flags);
                 float v[3] = {0.0f, 0.0f, 0.0f};

@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(kUThreads, 2) k_update3d(const __grid_constant
     const int part = (int)(blockIdx.x % kUCtasPerCell);
     const int n = A.selection.ids ? A.selection.ids[slot_cell] : slot_cell;
     pfb_cell3d* cell = &A.cells[n];
-    if (cell->storage_edge != 0u) return;
+    if (cell->storage_edge > (uint32_t)B) return;
     const pfb_layout3d L = A.layout;
     const size_t words = (size_t)B * B * B;
     const float* src = A.phi_in + (size_t)n * words;
@@ -160,7 +160,7 @@ int geometry_ok3(int B, const pfb_layout3d& L);
 
 size_t update3d_smem(int B) { return (size_t)kUHeader + (size_t)kURing * (size_t)B * B * 4; }
 
-int check_update(const pfb_update_args3d* a) {
+int check_update(const pfb_update_args3d* a, bool pools) {
     if (!a) return set_error(PFB_E_ARG, "null update arguments");
     const pfb_update_args3d& A = *a;
     if (A.tile_pass != PFB3D_TILE_PASS_ALL)
@@ -176,9 +176,11 @@ int check_update(const pfb_update_args3d* a) {
     if (channel ? (A.wall.values == nullptr || A.wall.planes != A.layout.nz)
                 : (A.wall.values != nullptr || A.wall.planes != 0))
         return set_error(PFB_E_ARG, "wall field does not match the geometry");
-    if (!A.phi_in || !A.phi_out || A.phi_in == A.phi_out || !A.S_in || !A.cells ||
-        (A.S_out && A.S_out == A.S_in))
+    if (!A.S_in || !A.cells || (A.S_out && A.S_out == A.S_in))
         return set_error(PFB_E_ARG, "invalid buffers in update arguments");
+    if (!pools) return PFB_OK;
+    if (!A.phi_in || !A.phi_out || A.phi_in == A.phi_out)
+        return set_error(PFB_E_ARG, "invalid phi pools in update arguments");
     if (((uintptr_t)A.phi_in & 15u) || ((uintptr_t)A.phi_out & 15u))
         return set_error(PFB_E_ARG, "phi pools must be 16-byte aligned");
     return PFB_OK;

@@ -148,6 +148,13 @@ _abi._SIGS.update({
     "pfb3d_measure_cells": (I, [C.POINTER(MeasureArgs3D), P]),
     "pfb3d_update": (I, [C.POINTER(UpdateArgs3D), P]),
     "pfb3d_step_fused": (I, [C.POINTER(MeasureArgs3D), C.POINTER(UpdateArgs3D), P]),
+    "pfb3d_next_brick_edge": (I, [I, I]),
+    "pfb3d_shrink_brick_edge": (I, [I, I, P, P]),
+    "pfb3d_measure_promoted": (I, [C.POINTER(MeasureArgs3D), P, P, I, I, P]),
+    "pfb3d_update_promoted": (I, [C.POINTER(UpdateArgs3D), P, P, P, I, I, P]),
+    "pfb3d_scatter_promoted": (I, [C.POINTER(ScatterArgs3D), P, P, I, I, P]),
+    "pfb3d_repair_promoted_after_fatal": (I, [C.POINTER(UpdateArgs3D), P, P, P, I, I, P]),
+    "pfb3d_check_promoted_crops": (I, [P, P, P, P, I, I, P]),
     "pfb3d_step_cluster": (I, [I]),
     "pfb3d_device_status": (I, [C.POINTER(C.c_uint), I]),
     "pfb3d_clear_S": (I, [P, C.POINTER(Layout3D), P]),
@@ -180,6 +187,11 @@ _abi._SIGS.update({
     "pfb_sim3d_fused": (I, [P]),
     "pfb_sim3d_set_graph": (I, [P, I]),
     "pfb_sim3d_set_order": (I, [P, I]),
+    "pfb_sim3d_packed_words": (I, [P, C.POINTER(C.c_ulonglong)]),
+    "pfb_sim3d_get_packed": (I, [P, P]),
+    "pfb_sim3d_promoted_count": (I, [P]),
+    "pfb_sim3d_max_edge": (I, [P]),
+    "pfb_sim3d_recoveries": (C.c_longlong, [P]),
     "pfb_sim3d_sync": (I, [P]),
     "pfb_sim3d_brick": (I, [P]),
     "pfb_sim3d_step": (C.c_longlong, [P]),

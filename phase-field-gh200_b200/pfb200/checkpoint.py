@@ -77,6 +77,7 @@ _abi._SIGS.update({
     "pfb_ckpt3d_params_from": (I, [C.POINTER(Params3D), I, C.POINTER(CkptParams3D)]),
     "pfb_ckpt3d_params_to": (I, [C.POINTER(CkptParams3D), I, C.POINTER(Params3D)]),
     "pfb_ckpt3d_read": (I, [C.c_char_p, C.POINTER(CkptInfo3D), C.POINTER(CkptParams3D), P, P]),
+    "pfb_ckpt3d_payload_words": (I, [C.c_char_p, C.POINTER(C.c_ulonglong)]),
     "pfb_ckpt3d_write": (I, [C.c_char_p, C.POINTER(CkptParams3D), C.c_longlong, I, P, P, I]),
     "pfb_sim3d_write_checkpoint": (I, [P, C.c_char_p, C.POINTER(CkptParams3D)]),
     "pfb_sim3d_create_from_checkpoint": (P, [C.c_char_p, I]),
@@ -152,11 +153,33 @@ class Checkpoint3D:
     step: int
     time: float
     params: CkptParams3D
-    cells: np.ndarray   # CELL3D_DTYPE records (base bricks)
-    phi: np.ndarray     # (N, B, B, B) float32, x fastest
+    cells: np.ndarray   # CELL3D_DTYPE records (storage_edge 0: base brick)
+    packed: np.ndarray  # each cell's field in cell order, B^3 or E^3 values, x fastest
     brick_edge: int
     base_measure_shards: int
     crc64: int
+
+    def edges(self) -> np.ndarray:
+        """Cube edge of every cell (B for a base cell)."""
+        e = self.cells["storage_edge"].astype(np.int64)
+        return np.where(e > self.brick_edge, e, self.brick_edge)
+
+    def fields(self) -> list[np.ndarray]:
+        """Each cell's field as an (E, E, E) view (z, y, x)."""
+        out, off = [], 0
+        for e in self.edges():
+            n = int(e) ** 3
+            out.append(self.packed[off:off + n].reshape(int(e), int(e), int(e)))
+            off += n
+        return out
+
+    @property
+    def phi(self) -> np.ndarray:
+        """(N, B, B, B) fields; only when no cell is on a promoted cube."""
+        B = self.brick_edge
+        if (self.edges() != B).any():
+            raise ValueError("cells on promoted cubes: use fields() or packed")
+        return self.packed.reshape(self.cells.size, B, B, B)
 
 
 def params_record3d(sim_params, brick: int = 0) -> CkptParams3D:
@@ -168,14 +191,15 @@ def params_record3d(sim_params, brick: int = 0) -> CkptParams3D:
 
 def read3d(path) -> Checkpoint3D:
     info, rec = CkptInfo3D(), CkptParams3D()
+    words = C.c_ulonglong(0)
+    check(lib().pfb_ckpt3d_payload_words(_path(path), C.byref(words)), "read")
     check(lib().pfb_ckpt3d_read(_path(path), C.byref(info), C.byref(rec), None, None), "read")
-    B = info.brick_edge
     cells = np.zeros(info.num_cells, CELL3D_DTYPE)
-    phi = np.zeros((info.num_cells, B, B, B), np.float32)
+    packed = np.zeros(words.value, np.float32)
     check(lib().pfb_ckpt3d_read(_path(path), C.byref(info), C.byref(rec), cells.ctypes.data,
-                                phi.ctypes.data), "read")
-    return Checkpoint3D(info.step, info.time, rec, cells, phi, B, info.base_measure_shards,
-                        info.crc64)
+                                packed.ctypes.data), "read")
+    return Checkpoint3D(info.step, info.time, rec, cells, packed, info.brick_edge,
+                        info.base_measure_shards, info.crc64)
 
 
 def write3d(path, rec: CkptParams3D, step: int, cells: np.ndarray, phi: np.ndarray,
@@ -201,4 +225,4 @@ def restart3d(path, device: int = 0):
     from dataclasses import fields
     kw = {f.name: getattr(pc, f.name) for f in fields(SimParams3D) if f.name != "geometry"}
     p = SimParams3D(geometry=geometry, **kw)
-    return Sim3D(p, cells=ck3.cells, phi=ck3.phi, step=ck3.step, device=device)
+    return Sim3D(p, cells=ck3.cells, phi=ck3.packed, step=ck3.step, device=device)

@@ -135,8 +135,9 @@ class Sim3D:
 
     def __init__(self, params: SimParams3D, centres: np.ndarray | None = None, *, device: int = 0,
                  cells: np.ndarray | None = None, phi: np.ndarray | None = None, step: int = 0):
-        """Fresh start from centres, or a restart from cell records and base
-        bricks (cells, phi) of step `step`."""
+        """Fresh start from centres, or a restart from cell records and fields
+        (cells, phi) of step `step`: phi is (N, B, B, B) or each cell's field
+        packed in cell order (E^3 values for a cell on a promoted cube)."""
         self.params = params
         self._pc = params.to_c()
         if cells is not None:
@@ -185,6 +186,37 @@ class Sim3D:
 
     def set_graph(self, use_graph: bool) -> None:
         check(lib().pfb_sim3d_set_graph(self._h, 1 if use_graph else 0), "set_graph")
+
+    def packed(self) -> np.ndarray:
+        """Current fields of all cells packed in cell order, each on its own
+        cube (B^3 or E^3 values)."""
+        w = C.c_ulonglong(0)
+        check(lib().pfb_sim3d_packed_words(self._h, C.byref(w)), "packed_words")
+        out = np.zeros(w.value, np.float32)
+        check(lib().pfb_sim3d_get_packed(self._h, ptr(out)), "get_packed")
+        return out
+
+    def fields(self) -> list[np.ndarray]:
+        """Each cell's current field as an (E, E, E) array."""
+        cells, flat = self.cells(), self.packed()
+        out, off = [], 0
+        for e in cells["storage_edge"]:
+            e = int(e) if int(e) > self.B else self.B
+            out.append(flat[off:off + e ** 3].reshape(e, e, e))
+            off += e ** 3
+        return out
+
+    @property
+    def promoted_count(self) -> int:
+        return int(lib().pfb_sim3d_promoted_count(self._h))
+
+    @property
+    def max_edge(self) -> int:
+        return int(lib().pfb_sim3d_max_edge(self._h))
+
+    @property
+    def recoveries(self) -> int:
+        return int(lib().pfb_sim3d_recoveries(self._h))
 
     def set_order(self, morton: bool) -> None:
         """Visit cells in the Morton order of their bricks (default) or in

@@ -131,13 +131,58 @@ def test_rejections(tmp_path):
         (_put("<Q", c0 + 200, 1), "reserved"),
         (_put("<i", c0 + 172, B + 1), "invalid"),
         (_put("<i", c0 + 152, B), "invalid"),
-        (_put("<I", c0 + 184, 72), "promoted"),
+        # a 72^3 payload would run into the next record
+        (_put("<I", c0 + 184, 72), "carries id|storage edge|truncates"),
+        (_put("<I", c0 + 184, 100), "storage edge"),
         (_put("<f", c0 + 256 + 4 * 1000, 0.123), "CRC"),
         (lambda b: b[:-4], "bytes"),
         (lambda b: b + b"\0\0\0\0", "bytes"),
     ]
     for k, (fn, match) in enumerate(cases):
         _rejects(tmp_path, path, fn, match, f"m{k}.pf3d")
+
+
+def promote_cell(cells, phi, n, edge):
+    """Cell n moved into a centred cube of `edge` padded with exact zeros, its
+    world field unchanged (the reference's adaptive resize)."""
+    off = (edge - B) // 2
+    cube = np.zeros((edge, edge, edge), np.float32)
+    cube[off:off + B, off:off + B, off:off + B] = phi[n]
+    c = cells.copy()
+    for k in "xyz":
+        c["origin_" + k][n] -= off
+        c["C" + k][n] += off * c["V"][n]
+        c["bb_lo_" + k][n] += off
+        c["bb_hi_" + k][n] += off
+    c["storage_edge"][n] = edge
+    return c, cube
+
+
+def test_promoted_cube_round_trip(tmp_path):
+    """A cell on a promoted cube (storage_edge 80 > B = 64): its record stores
+    the cube's edge and is followed by 80^3 values (reference
+    src/pf3d/checkpoint.cu:655-751); the file reads back and re-writes byte for
+    byte, and a base record reads with storage_edge 0."""
+    p, cells, phi = make_state()
+    c, cube = promote_cell(cells, phi, 1, 80)
+    packed = np.concatenate([phi[0].ravel(), cube.ravel()])
+    path = tmp_path / "p.pf3d"
+    ck.write3d(path, ck.params_record3d(p, B), 5, c, packed, 4)
+    b = path.read_bytes()
+    assert len(b) == 96 + 288 + 2 * 256 + 4 * (B ** 3 + 80 ** 3)
+    assert struct.unpack_from("<I", b, 96 + 288 + 184)[0] == B
+    assert struct.unpack_from("<I", b, 96 + 288 + 256 + 4 * B ** 3 + 184)[0] == 80
+    got = ck.read3d(path)
+    assert list(got.cells["storage_edge"]) == [0, 80]
+    assert list(got.edges()) == [B, 80]
+    f = got.fields()
+    np.testing.assert_array_equal(f[0], phi[0])
+    np.testing.assert_array_equal(f[1], cube)
+    with pytest.raises(ValueError):
+        got.phi
+    again = tmp_path / "q.pf3d"
+    ck.write3d(again, got.params, got.step, got.cells, got.packed, got.base_measure_shards)
+    assert again.read_bytes() == b
 
 
 def test_writer_refusals(tmp_path):
