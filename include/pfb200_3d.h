@@ -390,6 +390,36 @@ typedef struct pfb_sim3d pfb_sim3d;
  * to array coordinates as z + padding - 1/2 in binary32 as the reference
  * does); N = p->num_cells entries. */
 pfb_sim3d* pfb_sim3d_create(const pfb_params3d* p, const pfb_vec3* centres, int device);
+
+/* Storage modes (reference StorageMode3D, --memory-mode): throughput keeps
+ * two phi pools and two aggregates; balanced one pool, two aggregates and
+ * scratch bricks the update writes before committing each healthy cell;
+ * compact one pool and one aggregate rebuilt after every update. Fields,
+ * aggregates and flags are the same in every mode. AUTO takes throughput when
+ * it fits in 90 % of the free device memory, else balanced, else compact. */
+enum {
+    PFB3D_MEMORY_AUTO = -1,
+    PFB3D_MEMORY_THROUGHPUT = 0,
+    PFB3D_MEMORY_BALANCED = 1,
+    PFB3D_MEMORY_COMPACT = 2
+};
+/* pfb_sim3d_create / _create_from_state with a storage mode and a number of
+ * scratch bricks (0: two per SM, at most N). The plain functions use AUTO. */
+pfb_sim3d* pfb_sim3d_create_ex(const pfb_params3d* p, const pfb_vec3* centres, int device,
+                               int memory_mode, int scratch_slots);
+pfb_sim3d* pfb_sim3d_create_from_state_ex(const pfb_params3d* p, const pfb_cell3d* cells,
+                                          const float* phi, long long step, int device,
+                                          int memory_mode, int scratch_slots);
+int pfb_sim3d_memory_mode(const pfb_sim3d* s);
+int pfb_sim3d_scratch_slots(const pfb_sim3d* s);
+/* The in-place update of the balanced and compact modes (reference
+ * launch_update_inplace / launch_update_inplace_fast): the selected cells,
+ * scratch_slots at a time, update from the single pool args->phi_in into the
+ * scratch bricks (scratch_slots * B^3 floats), then each cell without a fatal
+ * flag is copied back (with one, its field stays and its planned shift is
+ * dropped). args->phi_out is ignored; args->S_out may be null. */
+int pfb3d_update_inplace(const pfb_update_args3d* args, float* scratch, int scratch_slots,
+                         void* stream);
 /* Restart from cell records and fields (x fastest) of step `step`, as the
  * reference's Sim3D::init_checkpoint does (src/pf3d/sim.cu:794-885): the
  * records and fields become the current state, the aggregate is rebuilt and

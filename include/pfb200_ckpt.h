@@ -199,6 +199,9 @@ int pfb_ckpt3d_write(const char* path, const pfb_ckpt3d_params* rec, long long s
  * measured first (pfb_sim3d_measure_current) as the reference does. */
 int pfb_sim3d_write_checkpoint(pfb_sim3d* s, const char* path, const pfb_ckpt3d_params* rec);
 pfb_sim3d* pfb_sim3d_create_from_checkpoint(const char* path, int device);
+/* The same with a storage mode and scratch bricks (pfb_sim3d_create_ex). */
+pfb_sim3d* pfb_sim3d_create_from_checkpoint_ex(const char* path, int device, int memory_mode,
+                                               int scratch_slots);
 
 #ifdef __cplusplus
 }

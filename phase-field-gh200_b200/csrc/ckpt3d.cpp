@@ -598,6 +598,11 @@ int pfb_sim3d_write_checkpoint(pfb_sim3d* s, const char* path, const pfb_ckpt3d_
 }
 
 pfb_sim3d* pfb_sim3d_create_from_checkpoint(const char* path, int device) {
+    return pfb_sim3d_create_from_checkpoint_ex(path, device, PFB3D_MEMORY_AUTO, 0);
+}
+
+pfb_sim3d* pfb_sim3d_create_from_checkpoint_ex(const char* path, int device, int memory_mode,
+                                               int scratch_slots) {
     clear_error();
     pfb_ckpt3d_info info;
     pfb_ckpt3d_params rec;
@@ -608,7 +613,8 @@ pfb_sim3d* pfb_sim3d_create_from_checkpoint(const char* path, int device) {
     if (read3(path, &info, &rec, cells.data(), phi.data())) return nullptr;
     pfb_params3d p;
     if (pfb_ckpt3d_params_to(&rec, info.num_cells, &p)) return nullptr;
-    return pfb_sim3d_create_from_state(&p, cells.data(), phi.data(), info.step, device);
+    return pfb_sim3d_create_from_state_ex(&p, cells.data(), phi.data(), info.step, device, memory_mode,
+                                          scratch_slots);
 }
 
 }  // extern "C"

@@ -15,9 +15,9 @@
 // (periodic x,y,z; relaxed x,y for the slab and the one-layer channel;
 // channel x,y,z). Soft cells (--cancer-fraction, --gamma-cancer) take
 // their identities from the reference's Philox shuffle. Cells whose support
-// reaches their brick grow into larger cubes (adaptive bricks) as in the
-// reference. Not part of this build (exit status 2 with a message): the
-// in-place memory modes (balanced, compact), scratch slots, peer device, and
+// reaches their brick grow into larger cubes (adaptive bricks), and
+// --memory-mode / --scratch-slots select the storage, as in the reference.
+// Not part of this build (exit status 2 with a message): the peer device and
 // measurement groupings other than this build's (--measure-shards 4,
 // --promoted-measure-shards 0), which the trajectory header and checkpoints
 // state.
@@ -56,6 +56,7 @@ struct Options {
     double rho = 0.90, t_end = 100.0, gamma_soft = 0.35, soft_fraction = 0.0;
     int slab_height = 0, channel_height = 0, wall_padding = 0;
     long long brick = 0, device = 0, bench = 0, print_interval = 100, verify_every = 4096;
+    int mem_mode = PFB3D_MEMORY_AUTO, scratch_slots = 0;
     long long traj_samples = 100, traj_interval = 0, ckpt_interval = 0, save_interval = 0;
     bool final_ckpt = true;
     // which options the command line supplied
@@ -556,19 +557,21 @@ int parse(int argc, char** argv, Options* o) {
             if (!v || !v[0]) return 2;
             o->centres_path = v;
         } else if (!std::strcmp(a, "--memory-mode")) {
-            // the two-pool throughput layout is the only storage here
             const char* v = value();
             if (!v) return 2;
-            if (std::strcmp(v, "auto") && std::strcmp(v, "throughput")) {
-                if (!std::strcmp(v, "balanced") || !std::strcmp(v, "compact")) {
-                    std::fprintf(stderr, "[3d] --memory-mode %s: the in-place storage modes are not "
-                                         "provided by this build (use throughput)\n", v);
-                } else {
-                    std::fprintf(stderr, "[3d] --memory-mode expects auto, throughput, balanced, or "
-                                         "compact\n");
-                }
+            if (!std::strcmp(v, "auto")) o->mem_mode = PFB3D_MEMORY_AUTO;
+            else if (!std::strcmp(v, "throughput")) o->mem_mode = PFB3D_MEMORY_THROUGHPUT;
+            else if (!std::strcmp(v, "balanced")) o->mem_mode = PFB3D_MEMORY_BALANCED;
+            else if (!std::strcmp(v, "compact")) o->mem_mode = PFB3D_MEMORY_COMPACT;
+            else {
+                std::fprintf(stderr, "[3d] --memory-mode expects auto, throughput, balanced, or compact\n");
                 return 2;
             }
+        } else if (!std::strcmp(a, "--scratch-slots")) {
+            const char* v = value();
+            long long k = 0;
+            if (!v || !parse_int(a, v, 0, 1 << 20, &k)) return 2;
+            o->scratch_slots = (int)k;
         } else if (!std::strcmp(a, "--measure-shards") || !std::strcmp(a, "--promoted-measure-shards")) {
             // the measurement groupings are fixed: 4 CTAs per base cell, the
             // one-CTA promoted policy (as the trajectory header states)
@@ -805,8 +808,10 @@ int main(int argc, char** argv) {
         return 2;
     }
 
-    pfb_sim3d* s = resumed ? pfb_sim3d_create_from_checkpoint(o.ckpt_in.c_str(), (int)o.device)
-                           : pfb_sim3d_create(&p, centres.data(), (int)o.device);
+    pfb_sim3d* s = resumed ? pfb_sim3d_create_from_checkpoint_ex(o.ckpt_in.c_str(), (int)o.device, o.mem_mode,
+                                                                 o.scratch_slots)
+                           : pfb_sim3d_create_ex(&p, centres.data(), (int)o.device, o.mem_mode,
+                                                 o.scratch_slots);
     if (!s) {
         std::fprintf(stderr, "[3d] initialisation failed: %s\n", pfb_last_error());
         return 1;

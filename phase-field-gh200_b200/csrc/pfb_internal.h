@@ -156,6 +156,9 @@ namespace p3 {
 int measure3d_launch(const pfb_measure_args3d* a, cudaStream_t stream);
 int motion3d_launch(const pfb_measure_args3d* a, cudaStream_t stream);
 int update3d_launch(const pfb_update_args3d* a, cudaStream_t stream);
+// in-place modes: update into `slots` scratch bricks, then commit (reference
+// launch_update_inplace); a->phi_out is ignored
+int update3d_inplace_launch(const pfb_update_args3d* a, float* scratch, int slots, cudaStream_t stream);
 // clears S; with a non-null guard only when a fatal global flag is set
 int clear3d_launch(uint32_t* S, const pfb_layout3d* L, const uint32_t* guard,
                    cudaStream_t stream);

@@ -72,7 +72,7 @@ struct pfb_sim3d {
     cudaGraph_t graph = nullptr;     // two steps from buffer parity 0
     cudaGraphExec_t graph_exec = nullptr;
     // adaptive bricks: cells whose support outgrew B live in their own cubes
-    // of edge storage_edge > B; cube[cur_phi][n] holds the current field
+    // of edge storage_edge > B; cube[cur_cube][n] holds the current field
     int max_edge = 0;                   // largest cube the domain allows
     std::vector<float*> h_cube[2];      // per cell; null for base cells
     float** d_cube[2] = {nullptr, nullptr};
@@ -83,6 +83,14 @@ struct pfb_sim3d {
     long long accepted = 0;             // accepted steps at the last synchronisation
     long long next_compact = 0;         // accepted step of the next compaction
     long long recoveries = 0;
+    int cur_cube = 0;                   // current side of the promoted double buffers
+    // storage mode (reference StorageMode3D): 0 throughput (two phi pools,
+    // two aggregates), 1 balanced (one pool, two aggregates, scratch bricks),
+    // 2 compact (one pool, one aggregate rebuilt after every update)
+    int mem_mode = 0;
+    int mode_request = -1;              // as created: -1 auto
+    int slots = 0;                      // scratch bricks of the in-place modes
+    float* d_scratch = nullptr;
 
     void drop_graph() {
         if (graph_exec) cudaGraphExecDestroy(graph_exec);
@@ -113,6 +121,7 @@ struct pfb_sim3d {
         }
         cudaFree(d_prom_ids);
         cudaFree(d_requests);
+        cudaFree(d_scratch);
     }
     int prom_count() const { return (int)prom_ids.size(); }
 };
@@ -389,9 +398,9 @@ pfb_measure_args3d measure_args(pfb_sim3d* s, bool tumble, bool surface) {
 pfb_update_args3d update_args(pfb_sim3d* s) {
     pfb_update_args3d u{};
     u.phi_in = s->d_phi[s->cur_phi];
-    u.phi_out = s->d_phi[1 - s->cur_phi];
+    u.phi_out = s->mem_mode == 0 ? s->d_phi[1 - s->cur_phi] : nullptr;  // in place: none
     u.S_in = s->d_S[s->cur_S];
-    u.S_out = s->d_S[1 - s->cur_S];
+    u.S_out = s->mem_mode == 2 ? nullptr : s->d_S[1 - s->cur_S];       // compact: rebuilt
     u.wall.values = s->d_wall;
     u.wall.planes = s->d_wall ? s->L.nz : 0;
     u.cells = s->d_cells;
@@ -422,9 +431,9 @@ int launch_step(pfb_sim3d* s, bool full) {
     const pfb_measure_args3d m = measure_args(s, true, full);
     const pfb_update_args3d u = update_args(s);
     const int np = s->prom_count();
-    float* const* cur = s->d_cube[s->cur_phi];
-    float* const* nxt = s->d_cube[1 - s->cur_phi];
-    if (s->fused && np == 0) {
+    float* const* cur = s->d_cube[s->cur_cube];
+    float* const* nxt = s->d_cube[1 - s->cur_cube];
+    if (s->fused && np == 0 && s->mem_mode == 0) {
         PFB3_RC(clear3d_launch(s->d_S[1 - s->cur_S], &s->L, nullptr, s->stream));
         PFB3_RC(step3d_launch(&m, &u, s->stream));
     } else {
@@ -432,8 +441,11 @@ int launch_step(pfb_sim3d* s, bool full) {
         PFB3_RC(measure3d_launch(&m, s->stream));
         if (np) PFB3_RC(measure3d_promoted_launch(&m, cur, s->d_prom_ids, np, s->max_edge, s->stream));
         PFB3_RC(motion3d_launch(&m, s->stream));
-        PFB3_RC(clear3d_launch(s->d_S[1 - s->cur_S], &s->L, nullptr, s->stream));
-        PFB3_RC(update3d_launch(&u, s->stream));
+        if (u.S_out) PFB3_RC(clear3d_launch(u.S_out, &s->L, nullptr, s->stream));
+        if (s->mem_mode == 0)
+            PFB3_RC(update3d_launch(&u, s->stream));
+        else
+            PFB3_RC(update3d_inplace_launch(&u, s->d_scratch, s->slots, s->stream));
         if (np)
             PFB3_RC(update3d_promoted_launch(&u, cur, nxt, s->d_prom_ids, np, s->max_edge, s->stream));
     }
@@ -442,13 +454,29 @@ int launch_step(pfb_sim3d* s, bool full) {
     PFB3_RC(pfb3d_finalize_origins(s->d_cells, s->N, s->d_flags, s->stream));
     PFB3_RC(pfb3d_restore_cells_after_fatal(s->d_cells, s->d_accepted, s->N, s->d_flags,
                                             s->d_requests, s->stream));
+    if (s->mem_mode == 2) {
+        // compact: the single aggregate is rebuilt from the new fields
+        // (reference Sim3D::finish_step, src/pf3d/sim.cu:1636-1641)
+        PFB3_RC(clear3d_launch(s->d_S[0], &s->L, nullptr, s->stream));
+        pfb_scatter_args3d sa{};
+        sa.phi = s->d_phi[0];
+        sa.cells = s->d_cells;
+        sa.S = s->d_S[0];
+        sa.global_flags = s->d_flags;
+        sa.layout = s->L;
+        sa.N = s->N;
+        sa.B = s->B;
+        PFB3_RC(scatter3d_launch(&sa, s->stream));
+        if (np) PFB3_RC(scatter3d_promoted_launch(&sa, nxt, s->d_prom_ids, np, s->max_edge, 0, s->stream));
+    }
     PFB3_RC(pfb3d_advance_step(s->d_step, s->d_flags, s->stream));
     return PFB_OK;
 }
 
 void flip(pfb_sim3d* s) {
-    s->cur_phi = 1 - s->cur_phi;
-    s->cur_S = 1 - s->cur_S;
+    if (s->mem_mode == 0) s->cur_phi = 1 - s->cur_phi;
+    if (s->mem_mode != 2) s->cur_S = 1 - s->cur_S;
+    s->cur_cube = 1 - s->cur_cube;
 }
 
 int one_step(pfb_sim3d* s) {
@@ -472,7 +500,7 @@ int reconstruct_S(pfb_sim3d* s) {
     sa.B = s->B;
     PFB3_RC(scatter3d_launch(&sa, s->stream));
     if (s->prom_count())
-        PFB3_RC(scatter3d_promoted_launch(&sa, s->d_cube[s->cur_phi], s->d_prom_ids, s->prom_count(),
+        PFB3_RC(scatter3d_promoted_launch(&sa, s->d_cube[s->cur_cube], s->d_prom_ids, s->prom_count(),
                                           s->max_edge, 0, s->stream));
     return PFB_OK;
 }
@@ -483,7 +511,7 @@ int refresh(pfb_sim3d* s, bool surface, bool motion) {
     const pfb_measure_args3d m = measure_args(s, false, surface);
     PFB3_RC(measure3d_launch(&m, s->stream));
     if (s->prom_count())
-        PFB3_RC(measure3d_promoted_launch(&m, s->d_cube[s->cur_phi], s->d_prom_ids, s->prom_count(),
+        PFB3_RC(measure3d_promoted_launch(&m, s->d_cube[s->cur_cube], s->d_prom_ids, s->prom_count(),
                                           s->max_edge, s->stream));
     if (motion) PFB3_RC(motion3d_launch(&m, s->stream));
     return PFB_OK;
@@ -564,9 +592,10 @@ int resize_cells(pfb_sim3d* s, const std::vector<std::pair<int, int>>& req,
     }
     const size_t bw = (size_t)s->B * s->B * s->B;
     for (Move& m : moves) {
-        const float* src = m.Eo > s->B ? s->h_cube[s->cur_phi][(size_t)m.id]
+        const float* src = m.Eo > s->B ? s->h_cube[s->cur_cube][(size_t)m.id]
                                        : s->d_phi[s->cur_phi] + (size_t)m.id * bw;
         for (int b = 0; b < 2; ++b) {
+            if (m.En == s->B && !s->d_phi[b]) continue;  // one pool in place
             float* dst = m.En > s->B ? m.cube[b] : s->d_phi[b] + (size_t)m.id * bw;
             const int rc = copy_centred3d_launch(src, m.Eo, dst, m.En, s->stream);
             if (rc) {
@@ -685,7 +714,7 @@ int compact_cubes(pfb_sim3d* s) {
         cudaMemcpy(d_cand, cand.data(), cand.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemset(d_rej, 0, rej.size() * sizeof(uint32_t)) != cudaSuccess)
         rc = set_error(PFB_E_CUDA, "crop check buffers");
-    if (!rc) rc = check_crops3d_launch(s->d_cube[s->cur_phi], s->d_cells, d_cand, d_rej, s->N, s->B, s->stream);
+    if (!rc) rc = check_crops3d_launch(s->d_cube[s->cur_cube], s->d_cells, d_cand, d_rej, s->N, s->B, s->stream);
     if (!rc && (cudaStreamSynchronize(s->stream) != cudaSuccess ||
                 cudaMemcpy(rej.data(), d_rej, rej.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost) !=
                     cudaSuccess))
@@ -703,7 +732,8 @@ int compact_cubes(pfb_sim3d* s) {
     return PFB_OK;
 }
 
-// Capture two steps without a surface pass, from buffer parity 0.
+// Capture two steps without a surface pass, from buffer parity 0 (every
+// double buffer back on the same side after them).
 int build_graph(pfb_sim3d* s) {
     s->drop_graph();
     PFB3_CU(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
@@ -727,7 +757,7 @@ int build_graph(pfb_sim3d* s) {
 int attempt_steps(pfb_sim3d* s, long long steps) {
     while (steps > 0) {
         if (s->steps_done - s->order_step >= kOrderRefresh) PFB3_RC(refresh_order(s));
-        const bool pair = s->use_graph && s->cur_phi == 0 && steps >= 2 &&
+        const bool pair = s->use_graph && s->cur_cube == 0 && steps >= 2 &&
                           !full_step(s, s->steps_done) && !full_step(s, s->steps_done + 1);
         if (pair) {
             if (!s->graph_exec) PFB3_RC(build_graph(s));
@@ -773,6 +803,32 @@ int advance_impl(pfb_sim3d* s, long long steps) {
     return PFB_OK;
 }
 
+// Storage mode and scratch bricks (reference Sim3D::allocate storage
+// selection, src/pf3d/sim.cu:440-560): mem_mode -1 (auto) takes throughput
+// when two pools and two aggregates fit in 90 % of the free device memory,
+// else balanced when one pool, two aggregates and a scratch brick per
+// resident update cluster fit, else compact. slots 0: 2 per SM, at most N.
+int choose_storage(pfb_sim3d* s) {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int want = s->slots > 0 ? s->slots : std::min(s->N, 2 * sms);
+    if (s->mode_request < -1 || s->mode_request > 2)
+        return set_error(PFB_E_ARG, "unknown storage mode %d", s->mode_request);
+    if (s->slots < 0 || s->slots > s->N) return set_error(PFB_E_ARG, "scratch slots must be 0..N");
+    int mode = s->mode_request;
+    if (mode < 0) {
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = (size_t)-1;
+        const double budget = 0.9 * (double)free_b;
+        const double pool = (double)s->N * (double)s->cell_words * 4.0, agg = (double)s->s_words * 4.0;
+        const double brick = (double)s->cell_words * 4.0;
+        mode = 2 * pool + 2 * agg <= budget ? 0 : pool + 2 * agg + want * brick <= budget ? 1 : 2;
+    }
+    s->mem_mode = mode;
+    s->slots = mode == 0 ? 0 : want;
+    return PFB_OK;
+}
+
 // Buffers, layout and wall field of a system with parameters *pp.
 int alloc_impl(pfb_sim3d* s, const pfb_params3d* pp, int device) {
     s->p = *pp;
@@ -795,10 +851,16 @@ int alloc_impl(pfb_sim3d* s, const pfb_params3d* pp, int device) {
     s->s_words = (size_t)s->L.pitch_x * s->L.ny * s->L.nz;
     s->cell_words = (size_t)s->B * s->B * s->B;
     PFB3_CU(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream");
+    PFB3_RC(choose_storage(s));
     for (int i = 0; i < 2; ++i) {
-        PFB3_CU(cudaMalloc(&s->d_phi[i], (size_t)s->N * s->cell_words * sizeof(float)), "cudaMalloc(phi)");
-        PFB3_CU(cudaMalloc(&s->d_S[i], s->s_words * sizeof(uint32_t)), "cudaMalloc(S)");
+        if (i == 0 || s->mem_mode == 0)
+            PFB3_CU(cudaMalloc(&s->d_phi[i], (size_t)s->N * s->cell_words * sizeof(float)), "cudaMalloc(phi)");
+        if (i == 0 || s->mem_mode != 2)
+            PFB3_CU(cudaMalloc(&s->d_S[i], s->s_words * sizeof(uint32_t)), "cudaMalloc(S)");
     }
+    if (s->mem_mode != 0)
+        PFB3_CU(cudaMalloc(&s->d_scratch, (size_t)s->slots * s->cell_words * sizeof(float)),
+                "cudaMalloc(scratch bricks)");
     PFB3_CU(cudaMalloc(&s->d_cells, (size_t)s->N * sizeof(pfb_cell3d)), "cudaMalloc(cells)");
     PFB3_CU(cudaMalloc(&s->d_accepted, (size_t)s->N * sizeof(pfb_cell3d)), "cudaMalloc(cells)");
     PFB3_CU(cudaMalloc(&s->d_flags, PFB3D_FLAG_COUNT * sizeof(uint32_t)), "cudaMalloc(flags)");
@@ -942,13 +1004,15 @@ int restore_impl(pfb_sim3d* s, const pfb_params3d* pp, const pfb_cell3d* cells_i
     PFB3_RC(upload_tables(s));
     PFB3_CU(cudaMemcpyAsync(s->d_cells, cells.data(), (size_t)s->N * sizeof(pfb_cell3d), cudaMemcpyHostToDevice,
                             s->stream), "upload cells");
-    PFB3_CU(cudaMemsetAsync(s->d_phi[1], 0, (size_t)s->N * s->cell_words * sizeof(float), s->stream),
-            "clear phi");
+    if (s->d_phi[1])
+        PFB3_CU(cudaMemsetAsync(s->d_phi[1], 0, (size_t)s->N * s->cell_words * sizeof(float), s->stream),
+                "clear phi");
     const uint64_t st = (uint64_t)step;
     PFB3_CU(cudaMemcpyAsync(s->d_step, &st, sizeof(st), cudaMemcpyHostToDevice, s->stream), "step");
     set_accepted(s, step);
     s->cur_phi = 0;
     s->cur_S = 0;
+    s->cur_cube = 0;
     PFB3_RC(remeasure_impl(s));
     PFB3_CU(cudaStreamSynchronize(s->stream), "restore");
     return refresh_order(s);
@@ -968,7 +1032,8 @@ size_t packed_words(const pfb_sim3d* s, const std::vector<pfb_cell3d>& cells) {
 
 extern "C" {
 
-pfb_sim3d* pfb_sim3d_create(const pfb_params3d* p, const pfb_vec3* centres, int device) {
+pfb_sim3d* pfb_sim3d_create_ex(const pfb_params3d* p, const pfb_vec3* centres, int device, int memory_mode,
+                               int scratch_slots) {
     clear_error();
     if (!p || !centres) {
         set_error(PFB_E_ARG, "null params or centres");
@@ -979,6 +1044,8 @@ pfb_sim3d* pfb_sim3d_create(const pfb_params3d* p, const pfb_vec3* centres, int 
         set_error(PFB_E_NOMEM, "host allocation failed");
         return nullptr;
     }
+    s->mode_request = memory_mode;
+    s->slots = scratch_slots;
     if (create_impl(s, p, centres, device) != PFB_OK) {
         delete s;
         return nullptr;
@@ -986,8 +1053,12 @@ pfb_sim3d* pfb_sim3d_create(const pfb_params3d* p, const pfb_vec3* centres, int 
     return s;
 }
 
-pfb_sim3d* pfb_sim3d_create_from_state(const pfb_params3d* p, const pfb_cell3d* cells,
-                                       const float* phi, long long step, int device) {
+pfb_sim3d* pfb_sim3d_create(const pfb_params3d* p, const pfb_vec3* centres, int device) {
+    return pfb_sim3d_create_ex(p, centres, device, PFB3D_MEMORY_AUTO, 0);
+}
+
+pfb_sim3d* pfb_sim3d_create_from_state_ex(const pfb_params3d* p, const pfb_cell3d* cells, const float* phi,
+                                          long long step, int device, int memory_mode, int scratch_slots) {
     clear_error();
     if (!p || !cells || !phi) {
         set_error(PFB_E_ARG, "null params, cells or phi");
@@ -998,12 +1069,23 @@ pfb_sim3d* pfb_sim3d_create_from_state(const pfb_params3d* p, const pfb_cell3d* 
         set_error(PFB_E_NOMEM, "host allocation failed");
         return nullptr;
     }
+    s->mode_request = memory_mode;
+    s->slots = scratch_slots;
     if (restore_impl(s, p, cells, phi, step, device) != PFB_OK) {
         delete s;
         return nullptr;
     }
     return s;
 }
+
+pfb_sim3d* pfb_sim3d_create_from_state(const pfb_params3d* p, const pfb_cell3d* cells,
+                                       const float* phi, long long step, int device) {
+    return pfb_sim3d_create_from_state_ex(p, cells, phi, step, device, PFB3D_MEMORY_AUTO, 0);
+}
+
+int pfb_sim3d_memory_mode(const pfb_sim3d* s) { return s ? s->mem_mode : -1; }
+
+int pfb_sim3d_scratch_slots(const pfb_sim3d* s) { return s ? s->slots : -1; }
 
 void pfb_sim3d_destroy(pfb_sim3d* s) { delete s; }
 
@@ -1012,7 +1094,7 @@ int pfb_sim3d_measure_wall(pfb_sim3d* s) {
     if (!hard_wall_channel(s->p.boundary_flags) || !s->d_wall_psi)
         return set_error(PFB_E_CONFIG, "wall diagnostics need the hard-wall channel");
     PFB3_CU(cudaSetDevice(s->device), "cudaSetDevice");
-    k_wall_diag3d<<<s->N, kWallThreads, 0, s->stream>>>(s->d_phi[s->cur_phi], s->d_cube[s->cur_phi],
+    k_wall_diag3d<<<s->N, kWallThreads, 0, s->stream>>>(s->d_phi[s->cur_phi], s->d_cube[s->cur_cube],
                                                        s->d_cells, s->B,
                                                        s->p.Nz, s->p.channel_padding,
                                                        s->p.channel_height, s->d_wall_psi);
@@ -1036,7 +1118,7 @@ int pfb_sim3d_verify(pfb_sim3d* s, double* max_rel_V, uint32_t* max_S,
         cudaMemsetAsync(d_m, 0, 4, s->stream) != cudaSuccess) {
         rc = set_error(PFB_E_CUDA, "verify: allocation failed");
     } else {
-        k_verify3d<<<s->N, kWallThreads, 0, s->stream>>>(s->d_phi[s->cur_phi], s->d_cube[s->cur_phi],
+        k_verify3d<<<s->N, kWallThreads, 0, s->stream>>>(s->d_phi[s->cur_phi], s->d_cube[s->cur_cube],
                                                          s->d_cells, s->B, s->p.Nz,
                                                          periodic ? 1 : 0,
                                                          substrate_slab(s->p.boundary_flags) ? 1 : 0, d_r);
@@ -1076,7 +1158,7 @@ int pfb_sim3d_boundary_open(pfb_sim3d* s, const char* path, int projection, long
 int pfb_sim3d_boundary_capture(pfb_sim3d* s) {
     if (!s || !s->bnd) return set_error(PFB_E_STATE, "no boundary recorder is open");
     PFB3_CU(cudaSetDevice(s->device), "cudaSetDevice");
-    return pfb::boundary3d_capture(s->bnd, s->d_phi[s->cur_phi], s->d_cube[s->cur_phi], s->d_cells, s->B,
+    return pfb::boundary3d_capture(s->bnd, s->d_phi[s->cur_phi], s->d_cube[s->cur_cube], s->d_cells, s->B,
                                    s->stream,
                               s->steps_done, (double)s->steps_done * s->p.dt);
 }
@@ -1182,7 +1264,7 @@ int pfb_sim3d_get_packed(pfb_sim3d* s, float* out) {
     for (int n = 0; n < s->N; ++n) {
         const int E = edge_of(s, c[(size_t)n]);
         const size_t words = (size_t)E * E * E;
-        const float* src = E > s->B ? s->h_cube[s->cur_phi][(size_t)n]
+        const float* src = E > s->B ? s->h_cube[s->cur_cube][(size_t)n]
                                     : s->d_phi[s->cur_phi] + (size_t)n * s->cell_words;
         if (!src) return set_error(PFB_E_STATE, "cell %d has no cube of edge %d", n, E);
         PFB3_CU(cudaMemcpy(out + off, src, words * sizeof(float), cudaMemcpyDeviceToHost), "copy field");

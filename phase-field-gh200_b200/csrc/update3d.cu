@@ -17,6 +17,8 @@
 // non-zero voxel.
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "device_util.cuh"
 #include "pfb3d_common.cuh"
 #include "pfb_internal.h"
@@ -40,9 +42,12 @@ struct UpdateHeader {
 };
 constexpr int kUHeader = (int)((sizeof(UpdateHeader) + 127) / 128 * 128);
 
-// GEO: 0 periodic, 1 substrate slab, 2 hard-wall channel
+// GEO: 0 periodic, 1 substrate slab, 2 hard-wall channel. out_by_slot: the
+// output brick of selection slot k is phi_out + k B^3 (the scratch bricks of
+// the in-place modes) instead of the cell's own slot.
 template <int GEO>
-__global__ void __launch_bounds__(kUThreads, 2) k_update3d(const __grid_constant__ pfb_update_args3d A) {
+__global__ void __launch_bounds__(kUThreads, 2)
+    k_update3d(const __grid_constant__ pfb_update_args3d A, int out_by_slot) {
     extern __shared__ __align__(128) char smem[];
     UpdateHeader& H = *reinterpret_cast<UpdateHeader*>(smem);
     const int B = A.B;
@@ -55,7 +60,7 @@ __global__ void __launch_bounds__(kUThreads, 2) k_update3d(const __grid_constant
     const pfb_layout3d L = A.layout;
     const size_t words = (size_t)B * B * B;
     const float* src = A.phi_in + (size_t)n * words;
-    float* dst = A.phi_out + (size_t)n * words;
+    float* dst = A.phi_out + (size_t)(out_by_slot ? slot_cell : n) * words;
     const int PB = B / kUCtasPerCell;
     const int d0 = part * PB, d1 = d0 + PB;
     const int64_t oz = cell->origin_z;
@@ -186,10 +191,7 @@ int check_update(const pfb_update_args3d* a, bool pools) {
     return PFB_OK;
 }
 
-int update3d_launch(const pfb_update_args3d* a, cudaStream_t stream) {
-    const int rc = check_update(a);
-    if (rc) return rc;
-    const pfb_update_args3d& A = *a;
+static int update_launch(const pfb_update_args3d& A, int out_by_slot, cudaStream_t stream) {
     const uint32_t bf = A.layout.boundary_flags;
     const int count = A.selection.ids ? A.selection.count : A.N;
     if (count == 0) return PFB_OK;
@@ -199,17 +201,98 @@ int update3d_launch(const pfb_update_args3d* a, cudaStream_t stream) {
     cudaError_t e;
     if (periodic_xyz(bf)) {
         e = cudaFuncSetAttribute(k_update3d<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e == cudaSuccess) k_update3d<0><<<grid, kUThreads, smem, stream>>>(A);
+        if (e == cudaSuccess) k_update3d<0><<<grid, kUThreads, smem, stream>>>(A, out_by_slot);
     } else if (substrate_slab(bf)) {
         e = cudaFuncSetAttribute(k_update3d<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e == cudaSuccess) k_update3d<1><<<grid, kUThreads, smem, stream>>>(A);
+        if (e == cudaSuccess) k_update3d<1><<<grid, kUThreads, smem, stream>>>(A, out_by_slot);
     } else {
         e = cudaFuncSetAttribute(k_update3d<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e == cudaSuccess) k_update3d<2><<<grid, kUThreads, smem, stream>>>(A);
+        if (e == cudaSuccess) k_update3d<2><<<grid, kUThreads, smem, stream>>>(A, out_by_slot);
     }
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) return set_error(PFB_E_CUDA, "update launch: %s", cudaGetErrorString(e));
     return PFB_OK;
+}
+
+int update3d_launch(const pfb_update_args3d* a, cudaStream_t stream) {
+    const int rc = check_update(a);
+    if (rc) return rc;
+    return update_launch(*a, 0, stream);
+}
+
+// In-place commit: the scratch brick of selection slot k becomes cell
+// ids[k]'s field unless the cell or the step holds a fatal flag, in which
+// case the field stays and the planned shift is dropped (reference
+// k_update_inplace_impl, src/pf3d/kernels.cu:1996-2045).
+__global__ void k_commit3d(float* pool, const float* scratch, pfb_cell3d* cells, const uint32_t* g,
+                           const int* ids, int B) {
+    __shared__ int keep;
+    const int k = (int)blockIdx.x;
+    const int n = ids[k];
+    pfb_cell3d* cell = &cells[n];
+    if (cell->storage_edge > (uint32_t)B) return;
+    if (threadIdx.x == 0) {
+        keep = fatal3(cell, g) ? 1 : 0;
+        if (keep) {
+            cell->pending_shift_x = 0;
+            cell->pending_shift_y = 0;
+            cell->pending_shift_z = 0;
+        }
+    }
+    __syncthreads();
+    if (keep) return;
+    const size_t v4 = (size_t)B * B * B / 4;
+    const float4* s4 = reinterpret_cast<const float4*>(scratch + (size_t)k * B * B * B);
+    float4* d4 = reinterpret_cast<float4*>(pool + (size_t)n * B * B * B);
+    for (size_t i = threadIdx.x; i < v4; i += blockDim.x) d4[i] = s4[i];
+}
+
+// The in-place update of the reference's balanced and compact modes
+// (launch_update_inplace[_fast]): the selected cells, `slots` at a time,
+// update from the single pool A.phi_in into the scratch bricks, then commit.
+// A.phi_out is ignored; A.S_out may be null (compact: the caller rebuilds S).
+int update3d_inplace_launch(const pfb_update_args3d* a, float* scratch, int slots,
+                            cudaStream_t stream) {
+    if (!a) return set_error(PFB_E_ARG, "null update arguments");
+    if (!scratch || slots <= 0 || ((uintptr_t)scratch & 15u))
+        return set_error(PFB_E_ARG, "in-place update needs aligned scratch bricks");
+    pfb_update_args3d A = *a;
+    A.phi_out = scratch;
+    int rc = check_update(&A, false);
+    if (rc) return rc;
+    if (!A.phi_in || ((uintptr_t)A.phi_in & 15u)) return set_error(PFB_E_ARG, "invalid phi pool");
+    const int count = A.selection.ids ? A.selection.count : A.N;
+    std::vector<int> identity;
+    const int* ids = A.selection.ids;
+    int* d_ids = nullptr;
+    if (!ids) {
+        // no selection: every cell in id order
+        identity.resize((size_t)count);
+        for (int i = 0; i < count; ++i) identity[(size_t)i] = i;
+        if (cudaMalloc(&d_ids, identity.size() * sizeof(int)) != cudaSuccess ||
+            cudaMemcpyAsync(d_ids, identity.data(), identity.size() * sizeof(int), cudaMemcpyHostToDevice,
+                            stream) != cudaSuccess) {
+            cudaFree(d_ids);
+            return set_error(PFB_E_CUDA, "in-place id list");
+        }
+        ids = d_ids;
+    }
+    for (int b0 = 0; b0 < count && !rc; b0 += slots) {
+        const int nb = count - b0 < slots ? count - b0 : slots;
+        A.selection.ids = ids + b0;
+        A.selection.count = nb;
+        rc = update_launch(A, 1, stream);
+        if (!rc) {
+            k_commit3d<<<nb, 256, 0, stream>>>(a->phi_in, scratch, A.cells, A.global_flags, ids + b0, A.B);
+            const cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) rc = set_error(PFB_E_CUDA, "in-place commit: %s", cudaGetErrorString(e));
+        }
+    }
+    if (d_ids) {
+        cudaStreamSynchronize(stream);
+        cudaFree(d_ids);
+    }
+    return rc;
 }
 
 int update3d_read_status(unsigned* out, int clear) {
@@ -229,4 +312,10 @@ int update3d_read_status(unsigned* out, int clear) {
 
 extern "C" int pfb3d_update(const pfb_update_args3d* args, void* stream) {
     return pfb::p3::update3d_launch(args, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int pfb3d_update_inplace(const pfb_update_args3d* args, float* scratch, int scratch_slots,
+                                    void* stream) {
+    return pfb::p3::update3d_inplace_launch(args, scratch, scratch_slots,
+                                            static_cast<cudaStream_t>(stream));
 }

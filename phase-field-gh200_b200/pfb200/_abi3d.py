@@ -174,6 +174,11 @@ _abi._SIGS.update({
                          C.POINTER(C.c_double)]),
     "pfb_sim3d_create": (P, [C.POINTER(Params3D), P, I]),
     "pfb_sim3d_create_from_state": (P, [C.POINTER(Params3D), P, P, C.c_longlong, I]),
+    "pfb_sim3d_create_ex": (P, [C.POINTER(Params3D), P, I, I, I]),
+    "pfb_sim3d_create_from_state_ex": (P, [C.POINTER(Params3D), P, P, C.c_longlong, I, I, I]),
+    "pfb_sim3d_memory_mode": (I, [P]),
+    "pfb_sim3d_scratch_slots": (I, [P]),
+    "pfb3d_update_inplace": (I, [C.POINTER(UpdateArgs3D), P, I, P]),
     "pfb_sim3d_measure_current": (I, [P]),
     "pfb_sim3d_measure_wall": (I, [P]),
     "pfb_sim3d_verify": (I, [P, C.POINTER(C.c_double), C.POINTER(C.c_uint32),

@@ -80,6 +80,7 @@ _abi._SIGS.update({
     "pfb_ckpt3d_payload_words": (I, [C.c_char_p, C.POINTER(C.c_ulonglong)]),
     "pfb_ckpt3d_write": (I, [C.c_char_p, C.POINTER(CkptParams3D), C.c_longlong, I, P, P, I]),
     "pfb_sim3d_write_checkpoint": (I, [P, C.c_char_p, C.POINTER(CkptParams3D)]),
+    "pfb_sim3d_create_from_checkpoint_ex": (P, [C.c_char_p, I, I, I]),
     "pfb_sim3d_create_from_checkpoint": (P, [C.c_char_p, I]),
     "pfb_ckpt2d_params_from": (I, [C.POINTER(Params2D), C.POINTER(CkptParams2D)]),
     "pfb_ckpt2d_params_to": (I, [C.POINTER(CkptParams2D), I, C.POINTER(Params2D)]),
@@ -215,8 +216,9 @@ def write_sim3d(sim, path, rec: CkptParams3D | None = None) -> None:
     check(lib().pfb_sim3d_write_checkpoint(sim._h, _path(path), C.byref(rec)), "write_checkpoint")
 
 
-def restart3d(path, device: int = 0):
-    """A Sim3D continuing from the PF3D checkpoint at `path`."""
+def restart3d(path, device: int = 0, memory_mode: str = "auto", scratch_slots: int = 0):
+    """A Sim3D continuing from the PF3D checkpoint at `path` (storage mode
+    as Sim3D's)."""
     from .sim3d import GEOMETRIES, Sim3D, SimParams3D
     ck3 = read3d(path)
     pc = Params3D()
@@ -225,4 +227,5 @@ def restart3d(path, device: int = 0):
     from dataclasses import fields
     kw = {f.name: getattr(pc, f.name) for f in fields(SimParams3D) if f.name != "geometry"}
     p = SimParams3D(geometry=geometry, **kw)
-    return Sim3D(p, cells=ck3.cells, phi=ck3.packed, step=ck3.step, device=device)
+    return Sim3D(p, cells=ck3.cells, phi=ck3.packed, step=ck3.step, device=device,
+                 memory_mode=memory_mode, scratch_slots=scratch_slots)

@@ -133,8 +133,11 @@ def flags_report3(flags: np.ndarray) -> dict[str, int]:
 class Sim3D:
     """Device-resident 3D simulation driven through the C ABI."""
 
+    MEMORY_MODES = {"auto": -1, "throughput": 0, "balanced": 1, "compact": 2}
+
     def __init__(self, params: SimParams3D, centres: np.ndarray | None = None, *, device: int = 0,
-                 cells: np.ndarray | None = None, phi: np.ndarray | None = None, step: int = 0):
+                 cells: np.ndarray | None = None, phi: np.ndarray | None = None, step: int = 0,
+                 memory_mode: str = "auto", scratch_slots: int = 0):
         """Fresh start from centres, or a restart from cell records and fields
         (cells, phi) of step `step`: phi is (N, B, B, B) or each cell's field
         packed in cell order (E^3 values for a cell on a promoted cube)."""
@@ -144,13 +147,15 @@ class Sim3D:
             self._cells0 = np.ascontiguousarray(cells, dtype=CELL3D_DTYPE)
             self._phi0 = np.ascontiguousarray(phi, dtype=np.float32)
             assert self._cells0.shape == (params.num_cells,)
-            h = lib().pfb_sim3d_create_from_state(C.byref(self._pc), ptr(self._cells0),
-                                                  ptr(self._phi0), step, device)
+            h = lib().pfb_sim3d_create_from_state_ex(C.byref(self._pc), ptr(self._cells0),
+                                                     ptr(self._phi0), step, device,
+                                                     self.MEMORY_MODES[memory_mode], scratch_slots)
             del self._cells0, self._phi0
         else:
             c = np.ascontiguousarray(centres, dtype=np.float64)
             assert c.shape == (params.num_cells, 3)
-            h = lib().pfb_sim3d_create(C.byref(self._pc), ptr(c), device)
+            h = lib().pfb_sim3d_create_ex(C.byref(self._pc), ptr(c), device,
+                                          self.MEMORY_MODES[memory_mode], scratch_slots)
         if not h:
             raise RuntimeError("pfb_sim3d_create failed: " + lib().pfb_last_error().decode())
         self._h = h
@@ -205,6 +210,15 @@ class Sim3D:
             out.append(flat[off:off + e ** 3].reshape(e, e, e))
             off += e ** 3
         return out
+
+    @property
+    def memory_mode(self) -> str:
+        m = int(lib().pfb_sim3d_memory_mode(self._h))
+        return {v: k for k, v in self.MEMORY_MODES.items()}[m]
+
+    @property
+    def scratch_slots(self) -> int:
+        return int(lib().pfb_sim3d_scratch_slots(self._h))
 
     @property
     def promoted_count(self) -> int:

@@ -82,11 +82,11 @@ def test_help():
     (("--geometry", "channel", "--lambda", 3, "--wall-padding", 5), "smaller than the minimum"),
     (("--geometry", "slab", "--radius", 8, "--lambda", 3, "--slab-height", 3), "must exceed"),
     (("--cancer-fraction", 1.5), "--cancer-fraction expects"),
-    (("--memory-mode", "compact"), "in-place storage modes are not provided"),
     (("--memory-mode", "fast"), "--memory-mode expects"),
     (("--measure-shards", 8), "measures with --measure-shards 4 only"),
     (("--promoted-measure-shards", 4), "--promoted-measure-shards 0 only"),
-    (("--scratch-slots", 2), "unknown option"),
+    (("--scratch-slots", -2), "--scratch-slots expects"),
+    (("--peer-device", 1), "unknown option"),
     (("--trajectory-interval", 0), "--trajectory-interval expects"),
     (("--seed", -4), "unsigned"),
     (("--out",), "requires a value"),
