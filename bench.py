@@ -319,6 +319,7 @@ def run_3d(a):
     p, c = workload3d(1234 + rank, a.workload)
     if a.brick_edge:
         p.B = a.brick_edge
+    p.phi_storage = a.phi_storage
     sim = pfb200.Sim3D(p, c, device=local)
     if a.fused3d == "off":
         sim.set_fused(False)
@@ -329,7 +330,8 @@ def run_3d(a):
     fused = sim.fused
     B, N = sim.B, p.num_cells
     sites = N * B ** 3
-    alg = sites * 8 + p.Nx * p.Ny * p.Nz * 8
+    phi_b = 2 if a.phi_storage else 4
+    alg = sites * 2 * phi_b + p.Nx * p.Ny * p.Nz * 8
     slab = a.workload == "c3s"
     ext = torch.cuda.ExternalStream(sim.stream, device=local)
 
@@ -386,19 +388,23 @@ def run_3d(a):
             "metric": "site-cell updates/s", "value": world * sites * a.steps / (ms / 1000.0),
             "unit": "site-cell updates/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": ("f32", "f32 arithmetic, f16 phi storage",
+                      "f32 arithmetic, bf16 phi storage")[a.phi_storage], "data": "synthetic",
             "config": {"workload": WORKLOAD3D_SLAB if slab else WORKLOAD3D,
                        "domain": [p.Nx, p.Ny, p.Nz], "geometry": p.geometry, "cells": N,
                        "radius": 10.0, "B": B, "sites_per_step": sites,
                        "step": "fused measure + motion + update launch" if fused else
                                "separate measure, motion and update launches",
                        "visit_order": a.order3d,
+                       "phi_storage": ("binary32", "binary16", "bfloat16")[a.phi_storage],
                        "l2": "inputs larger than L2: two %d MB phi pools and two %d MB "
                              "aggregate slots; no flush between steps" % (
-                                 N * B ** 3 * 4 // 2 ** 20, p.Nx * p.Ny * p.Nz * 4 // 2 ** 20),
+                                 N * B ** 3 * phi_b // 2 ** 20, p.Nx * p.Ny * p.Nz * 4 // 2 ** 20),
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": read_ncu_traffic3d(a.workload),
+                         "frac": achieved / peak,
+                         "traffic": read_ncu_traffic3d(a.workload) if not a.phi_storage else None,
                          "kernel": ("pfb::p3::k_step3d<%d, %d> (one step)" % (
                              pfb200.lib().pfb3d_step_cluster(B), 1 if slab else 0)) if fused else
                                    ("pfb::p3::k_measure3d<%d> + k_update3d<%d> (one step)" % (

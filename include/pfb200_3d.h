@@ -381,6 +381,11 @@ typedef struct pfb_params3d {
      * soft_fraction N) identities drawn without replacement take gamma_soft */
     double gamma_soft;
     double soft_fraction;
+    /* storage of the base phi pools: 0 binary32 (the reference's layout),
+     * 1 binary16, 2 bfloat16, both with binary32 arithmetic and stochastic
+     * rounding of every stored value (seeded by `seed`); promoted cubes stay
+     * binary32, and fields are read and written as binary32 */
+    int phi_storage;
 } pfb_params3d;
 
 typedef struct pfb_sim3d pfb_sim3d;

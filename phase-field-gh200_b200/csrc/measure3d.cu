@@ -20,6 +20,7 @@
 #include "pfb_internal.h"
 #include "measure3d_common.cuh"
 #include "ring3d.cuh"
+#include "storage2d.cuh"
 
 namespace pfb {
 namespace p3 {
@@ -36,7 +37,9 @@ struct MeasureHeader {
     MeasureFold<K> fold;
 };
 
-template <int K>
+// T: storage type of the phi pool (binary32, or binary16 / bfloat16 widened
+// on load).
+template <int K, typename T>
 __global__ void __launch_bounds__(kThreads3, 2) k_measure3d(const __grid_constant__ pfb_measure_args3d A) {
     extern __shared__ __align__(128) char smem[];
     MeasureHeader<K>& H = *reinterpret_cast<MeasureHeader<K>*>(smem);
@@ -50,7 +53,7 @@ __global__ void __launch_bounds__(kThreads3, 2) k_measure3d(const __grid_constan
     // Promoted cells are uniform over the cluster: every CTA returns.
     if (cell->storage_edge > (uint32_t)B) return;
 
-    PlaneRing<kMeasureRing> ring{reinterpret_cast<float*>(smem + kHeader), H.bars, B * B};
+    PlaneRing<kMeasureRing, T> ring{reinterpret_cast<T*>(smem + kHeader), H.bars, B * B};
     ring.init();
     if (tid == 0) {
         fold_init<K>(H.fold, rank);
@@ -70,7 +73,7 @@ __global__ void __launch_bounds__(kThreads3, 2) k_measure3d(const __grid_constan
     M.oy = wrap_origin(cell->origin_y, L.ny);
     M.wall = hard_wall_channel(bf) && A.wall.values;
     M.surface = A.compute_surface != 0;
-    const float* field = A.phi + (size_t)n * (size_t)B * B * B;
+    const T* field = reinterpret_cast<const T*>(A.phi) + (size_t)n * (size_t)B * B * B;
     const int PB = B / K;
     const int z0 = rank * PB;
 
@@ -160,9 +163,9 @@ __global__ void k_motion3d(const __grid_constant__ pfb_measure_args3d A) {
 // Host side
 // ---------------------------------------------------------------------------
 template <int K>
-static size_t measure_smem(int B) {
+static size_t measure_smem(int B, int bytes) {
     const size_t header = (sizeof(MeasureHeader<K>) + 127) / 128 * 128;
-    return header + (size_t)kMeasureRing * (size_t)B * B * 4;
+    return header + (size_t)kMeasureRing * (size_t)B * B * bytes;
 }
 
 int geometry_ok3(int B, const pfb_layout3d& L) {
@@ -192,14 +195,14 @@ int check_measure(const pfb_measure_args3d* a) {
     return PFB_OK;
 }
 
-template <int K>
+template <int K, typename T>
 static int measure_launch_k(const pfb_measure_args3d& A, int count, cudaStream_t stream) {
-    const size_t smem = measure_smem<K>(A.B);
+    const size_t smem = measure_smem<K>(A.B, (int)sizeof(T));
     if (smem > 227 * 1024) return set_error(PFB_E_CONFIG, "brick edge too large for the plane ring");
-    cudaError_t e = cudaFuncSetAttribute(k_measure3d<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(k_measure3d<K, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e == cudaSuccess && K > 8)
-        e = cudaFuncSetAttribute(k_measure3d<K>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        e = cudaFuncSetAttribute(k_measure3d<K, T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (e != cudaSuccess) return set_error(PFB_E_CUDA, "measure attribute: %s", cudaGetErrorString(e));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(count * K), 1, 1);
@@ -213,7 +216,7 @@ static int measure_launch_k(const pfb_measure_args3d& A, int count, cudaStream_t
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    e = cudaLaunchKernelEx(&cfg, k_measure3d<K>, A);
+    e = cudaLaunchKernelEx(&cfg, k_measure3d<K, T>, A);
     if (e != cudaSuccess) return set_error(PFB_E_CUDA, "measure launch: %s", cudaGetErrorString(e));
     return PFB_OK;
 }
@@ -223,19 +226,21 @@ static int measure_launch_k(const pfb_measure_args3d& A, int count, cudaStream_t
 int measure3d_cluster(int) { return 4; }
 
 int measure3d_launch(const pfb_measure_args3d* a, cudaStream_t stream) {
+    return measure3d_launch_pool(a, kStoreF32, stream);
+}
+
+int measure3d_launch_pool(const pfb_measure_args3d* a, int storage, cudaStream_t stream) {
     int rc = check_measure(a);
     if (rc) return rc;
     const pfb_measure_args3d& A = *a;
     const int count = A.selection.ids ? A.selection.count : A.N;
     if (count == 0) return PFB_OK;
     const int K = measure3d_cluster(A.B);
-    if (A.B % K != 0) return set_error(PFB_E_CONFIG, "brick edge is not a multiple of the cluster size");
-    switch (K) {
-        case 4: return measure_launch_k<4>(A, count, stream);
-        case 8: return measure_launch_k<8>(A, count, stream);
-        case 16: return measure_launch_k<16>(A, count, stream);
-        default: return set_error(PFB_E_CONFIG, "unsupported measurement cluster size %d", K);
-    }
+    if (K != 4 || A.B % K != 0) return set_error(PFB_E_CONFIG, "brick edge is not a multiple of 4");
+    if (storage == kStoreF16) return measure_launch_k<4, __half>(A, count, stream);
+    if (storage == kStoreBF16) return measure_launch_k<4, __nv_bfloat16>(A, count, stream);
+    if (storage != kStoreF32) return set_error(PFB_E_ARG, "unknown phi storage");
+    return measure_launch_k<4, float>(A, count, stream);
 }
 
 int motion3d_launch(const pfb_measure_args3d* a, cudaStream_t stream) {

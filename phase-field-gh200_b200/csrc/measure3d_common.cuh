@@ -13,6 +13,7 @@
 
 #include "device_util.cuh"
 #include "pfb3d_common.cuh"
+#include "phi3d.cuh"
 
 namespace pfb {
 namespace p3 {
@@ -42,26 +43,24 @@ struct MeasureCell {
 };
 
 // Six values of row y of a plane: columns x0 - 1 .. x0 + 4 (zero outside).
-__device__ __forceinline__ void load_row6(const float* plane, int B, int y, int x0, float* v) {
+template <typename T>
+__device__ __forceinline__ void load_row6(const T* plane, int B, int y, int x0, float* v) {
     if ((unsigned)y >= (unsigned)B) {
 #pragma unroll
         for (int c = 0; c < 6; ++c) v[c] = 0.0f;
         return;
     }
-    const float* row = plane + y * B;
-    const float4 m = *reinterpret_cast<const float4*>(row + x0);
-    v[0] = x0 > 0 ? row[x0 - 1] : 0.0f;
-    v[1] = m.x;
-    v[2] = m.y;
-    v[3] = m.z;
-    v[4] = m.w;
-    v[5] = x0 + 4 < B ? row[x0 + 4] : 0.0f;
+    const T* row = plane + y * B;
+    phi_ld4(row + x0, v + 1);
+    v[0] = x0 > 0 ? phi_ld1(row + x0 - 1) : 0.0f;
+    v[5] = x0 + 4 < B ? phi_ld1(row + x0 + 4) : 0.0f;
 }
 
 // Sums of one item: columns x0 .. x0 + 3 of rows y0 .. y0 + 3 of brick plane
 // z (world plane wz); pm, pc, pp are planes z - 1, z, z + 1.
-__device__ __forceinline__ void measure_item(const MeasureCell& M, const float* pm,
-                                             const float* pc, const float* pp, int x0, int y0,
+template <typename T = float>
+__device__ __forceinline__ void measure_item(const MeasureCell& M, const T* pm,
+                                             const T* pc, const T* pp, int x0, int y0,
                                              int z, int wz, float wallv, bool top_plane,
                                              Acc3& acc, MeasureCounts& cnt) {
     const int B = M.B;
@@ -84,10 +83,9 @@ __device__ __forceinline__ void measure_item(const MeasureCell& M, const float* 
     for (int r = 0; r < 4; ++r) {
         const int y = y0 + r;
         load_row6(pc, B, y + 1, x0, rn);
-        const float4 zm = *reinterpret_cast<const float4*>(pm + y * B + x0);
-        const float4 zp = *reinterpret_cast<const float4*>(pp + y * B + x0);
-        const float zmv[4] = {zm.x, zm.y, zm.z, zm.w};
-        const float zpv[4] = {zp.x, zp.y, zp.z, zp.w};
+        float zmv[4], zpv[4];
+        phi_ld4(pm + y * B + x0, zmv);
+        phi_ld4(pp + y * B + x0, zpv);
         uint32_t agg[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) agg[j] = agg_next[j];

@@ -7,6 +7,7 @@
 
 #include "pfb3d_common.cuh"
 #include "pfb_internal.h"
+#include "phi3d.cuh"
 
 namespace pfb {
 namespace p3 {
@@ -46,16 +47,17 @@ __global__ void k_clear3d(uint4* S, size_t vec4, uint32_t* tail, size_t tail_wor
         for (size_t i = threadIdx.x; i < tail_words; i += blockDim.x) tail[i] = 0u;
 }
 
-// Scatter every selected cell's field (world mapping from `pending` shifts
-// when use_pending): one CTA per cell, one warp per brick row.
-__global__ void k_scatter3d(const float* phi, pfb_cell3d* cells, uint32_t* S, uint32_t* g,
+// Scatter every selected cell's field: one CTA per cell, one warp per brick
+// row. T: storage type of the pool.
+template <typename T>
+__global__ void k_scatter3d(const T* phi, pfb_cell3d* cells, uint32_t* S, uint32_t* g,
                             pfb_layout3d L, int N, int B, pfb_selection3d sel, int guard_fatal) {
     if (guard_fatal && !fatal_global(g)) return;
     const int slot = (int)blockIdx.x;
     const int n = sel.ids ? sel.ids[slot] : slot;
     pfb_cell3d* cell = &cells[n];
     if (cell->storage_edge != 0u) return;
-    const float* tile = phi + (size_t)n * B * B * B;
+    const T* tile = phi + (size_t)n * B * B * B;
     const int ox = wrap_origin(cell->origin_x, L.nx), oy = wrap_origin(cell->origin_y, L.ny);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, warps = blockDim.x >> 5;
     for (int row = warp; row < B * B; row += warps) {
@@ -63,9 +65,9 @@ __global__ void k_scatter3d(const float* phi, pfb_cell3d* cells, uint32_t* S, ui
         int wz;
         if (!aggregate_z(L, cell->origin_z, z, &wz)) continue;
         const size_t base = s_index(L, 0, wrap_offset(oy, y, L.ny), wz);
-        const float* gr = tile + (size_t)row * B;
+        const T* gr = tile + (size_t)row * B;
         for (int x = lane; x < B; x += 32) {
-            const float v = gr[x];
+            const float v = phi_ld1(gr + x);
             if (!isfinite(v)) {
                 raise1(cell, g, PFB3D_FLAG_NONFINITE);
                 continue;
@@ -75,18 +77,19 @@ __global__ void k_scatter3d(const float* phi, pfb_cell3d* cells, uint32_t* S, ui
     }
 }
 
-// Fatal-step repair of one cell: phi_out = phi_in, pending shift cleared.
-__global__ void k_repair_copy3d(const float* in, float* out, pfb_cell3d* cells, const uint32_t* g,
-                                int B, pfb_selection3d sel) {
+// Fatal-step repair of one cell: phi_out = phi_in (values of `bytes` each),
+// pending shift cleared.
+__global__ void k_repair_copy3d(const void* in, void* out, pfb_cell3d* cells, const uint32_t* g,
+                                int B, int bytes, pfb_selection3d sel) {
     if (!fatal_global(g)) return;
     const int slot = (int)blockIdx.x;
     const int n = sel.ids ? sel.ids[slot] : slot;
     pfb_cell3d* cell = &cells[n];
     if (cell->storage_edge != 0u) return;
-    const size_t words = (size_t)B * B * B;
-    const float4* s4 = reinterpret_cast<const float4*>(in + (size_t)n * words);
-    float4* d4 = reinterpret_cast<float4*>(out + (size_t)n * words);
-    for (size_t i = threadIdx.x; i < words / 4; i += blockDim.x) d4[i] = s4[i];
+    const size_t brick = (size_t)B * B * B * bytes;
+    const float4* s4 = reinterpret_cast<const float4*>(static_cast<const char*>(in) + (size_t)n * brick);
+    float4* d4 = reinterpret_cast<float4*>(static_cast<char*>(out) + (size_t)n * brick);
+    for (size_t i = threadIdx.x; i < brick / 16; i += blockDim.x) d4[i] = s4[i];
     if (threadIdx.x == 0) {
         cell->pending_shift_x = 0;
         cell->pending_shift_y = 0;
@@ -193,7 +196,28 @@ int clear3d_launch(uint32_t* S, const pfb_layout3d* L, const uint32_t* guard,
     return e == cudaSuccess ? PFB_OK : set_error(PFB_E_CUDA, "clear launch: %s", cudaGetErrorString(e));
 }
 
+template <typename T>
+static void scatter_t(const void* phi, const pfb_scatter_args3d& A, uint32_t* S, int count, int guard,
+                      cudaStream_t stream) {
+    k_scatter3d<T><<<count, 256, 0, stream>>>(static_cast<const T*>(phi), A.cells, S, A.global_flags,
+                                              A.layout, A.N, A.B, A.selection, guard);
+}
+
+static void scatter_pool(int storage, const void* phi, const pfb_scatter_args3d& A, uint32_t* S, int count,
+                         int guard, cudaStream_t stream) {
+    if (storage == kStoreF16)
+        scatter_t<__half>(phi, A, S, count, guard, stream);
+    else if (storage == kStoreBF16)
+        scatter_t<__nv_bfloat16>(phi, A, S, count, guard, stream);
+    else
+        scatter_t<float>(phi, A, S, count, guard, stream);
+}
+
 int scatter3d_launch(const pfb_scatter_args3d* a, cudaStream_t stream) {
+    return scatter3d_launch_pool(a, kStoreF32, stream);
+}
+
+int scatter3d_launch_pool(const pfb_scatter_args3d* a, int storage, cudaStream_t stream) {
     if (!a) return set_error(PFB_E_ARG, "null scatter arguments");
     const pfb_scatter_args3d& A = *a;
     if (A.storage.z_cap != 0) return set_error(PFB_E_CONFIG, "compact cell storage is not supported");
@@ -202,13 +226,16 @@ int scatter3d_launch(const pfb_scatter_args3d* a, cudaStream_t stream) {
         return set_error(PFB_E_ARG, "invalid scatter arguments");
     const int count = sel_count(A.selection, A.N);
     if (count == 0) return PFB_OK;
-    k_scatter3d<<<count, 256, 0, stream>>>(A.phi, A.cells, A.S, A.global_flags, A.layout, A.N, A.B,
-                                           A.selection, 0);
+    scatter_pool(storage, A.phi, A, A.S, count, 0, stream);
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? PFB_OK : set_error(PFB_E_CUDA, "scatter launch: %s", cudaGetErrorString(e));
 }
 
 int repair3d_launch(const pfb_update_args3d* a, cudaStream_t stream) {
+    return repair3d_launch_pool(a, kStoreF32, stream);
+}
+
+int repair3d_launch_pool(const pfb_update_args3d* a, int storage, cudaStream_t stream) {
     if (!a) return set_error(PFB_E_ARG, "null update arguments");
     const pfb_update_args3d& A = *a;
     if (A.storage.z_cap != 0) return set_error(PFB_E_CONFIG, "compact cell storage is not supported");
@@ -222,10 +249,17 @@ int repair3d_launch(const pfb_update_args3d* a, cudaStream_t stream) {
     }
     if (count > 0 && A.phi_out)
         k_repair_copy3d<<<count, 256, 0, stream>>>(A.phi_in, A.phi_out, A.cells, A.global_flags,
-                                                   A.B, A.selection);
-    if (count > 0 && A.S_out)
-        k_scatter3d<<<count, 256, 0, stream>>>(A.phi_in, A.cells, A.S_out, A.global_flags,
-                                               A.layout, A.N, A.B, A.selection, 1);
+                                                   A.B, storage ? 2 : 4, A.selection);
+    if (count > 0 && A.S_out) {
+        pfb_scatter_args3d sa{};
+        sa.cells = A.cells;
+        sa.global_flags = A.global_flags;
+        sa.layout = A.layout;
+        sa.N = A.N;
+        sa.B = A.B;
+        sa.selection = A.selection;
+        scatter_pool(storage, A.phi_in, sa, A.S_out, count, 1, stream);
+    }
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? PFB_OK : set_error(PFB_E_CUDA, "repair launch: %s", cudaGetErrorString(e));
 }

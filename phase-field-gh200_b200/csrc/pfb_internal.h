@@ -154,17 +154,26 @@ int conv_read_status(unsigned* out, int clear);
 namespace p3 {
 // measure3d.cu / update3d.cu / misc3d.cu (pfb200_3d.h records)
 int measure3d_launch(const pfb_measure_args3d* a, cudaStream_t stream);
+int measure3d_launch_pool(const pfb_measure_args3d* a, int storage, cudaStream_t stream);
 int motion3d_launch(const pfb_measure_args3d* a, cudaStream_t stream);
 int update3d_launch(const pfb_update_args3d* a, cudaStream_t stream);
 // in-place modes: update into `slots` scratch bricks, then commit (reference
 // launch_update_inplace); a->phi_out is ignored
 int update3d_inplace_launch(const pfb_update_args3d* a, float* scratch, int slots, cudaStream_t stream);
+// the same two updates on pools of storage type `storage` (PhiStorage; the
+// pointers of `a` then address 16-bit pools), rounding stream of (*step, seed)
+int update3d_launch_pool(const pfb_update_args3d* a, int storage, const uint64_t* step, uint64_t seed,
+                         cudaStream_t stream);
+int update3d_inplace_launch_pool(const pfb_update_args3d* a, void* scratch, int slots, int storage,
+                                 const uint64_t* step, uint64_t seed, cudaStream_t stream);
 // clears S; with a non-null guard only when a fatal global flag is set
 int clear3d_launch(uint32_t* S, const pfb_layout3d* L, const uint32_t* guard,
                    cudaStream_t stream);
 int repair3d_launch(const pfb_update_args3d* a, cudaStream_t stream);
+int repair3d_launch_pool(const pfb_update_args3d* a, int storage, cudaStream_t stream);
 int init3d_launch(const pfb_init_args3d* a, cudaStream_t stream);
 int scatter3d_launch(const pfb_scatter_args3d* a, cudaStream_t stream);
+int scatter3d_launch_pool(const pfb_scatter_args3d* a, int storage, cudaStream_t stream);
 int measure3d_read_status(unsigned* out, int clear);
 int update3d_read_status(unsigned* out, int clear);
 int check_measure(const pfb_measure_args3d* a);

@@ -1,8 +1,9 @@
 // Shared-memory ring of whole brick planes for the 3D kernels.
 //
-// A brick plane (B x B floats, x fastest) is contiguous in HBM, so one bulk
-// asynchronous copy (cp.async.bulk, no multicast) stages it; a plane that
-// stands for the zero halo is written with zeros by the CTA instead. Slot
+// A brick plane (B x B values of the pool's storage type T, x fastest) is
+// contiguous in HBM, so one bulk asynchronous copy (cp.async.bulk, no
+// multicast) stages it; a plane that stands for the zero halo is written with
+// zeros by the CTA instead. Slot
 // j of the ring serves requests k = j, j + R, j + 2R, ...; request k waits
 // on the slot's mbarrier with parity (k / R) & 1.
 //
@@ -23,13 +24,13 @@ namespace p3 {
 // hardware-defined interval).
 constexpr uint32_t kPlaneWaitPolls = 1u << 24;
 
-template <int R>
+template <int R, typename T = float>
 struct PlaneRing {
-    float* base;      // R * plane_words floats, 16-byte aligned
+    T* base;          // R * plane_words values, 16-byte aligned
     uint64_t* bars;   // R mbarriers
     int plane_words;  // B * B
 
-    __device__ __forceinline__ float* slot(int k) const {
+    __device__ __forceinline__ T* slot(int k) const {
         return base + (size_t)(k % R) * (size_t)plane_words;
     }
 
@@ -40,12 +41,12 @@ struct PlaneRing {
     }
 
     // Request k: local plane `src` of `field` (src < 0: a zero plane).
-    __device__ __forceinline__ void issue(int k, const float* field, int src) const {
-        float* dst = slot(k);
+    __device__ __forceinline__ void issue(int k, const T* field, int src) const {
+        T* dst = slot(k);
         uint64_t* bar = &bars[k % R];
         if (src >= 0) {
             if (threadIdx.x == 0) {
-                const uint32_t bytes = (uint32_t)plane_words * 4u;
+                const uint32_t bytes = (uint32_t)plane_words * (uint32_t)sizeof(T);
                 // earlier generic-proxy writes to this slot precede the copy
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 dev::mbar_arrive_expect_tx(bar, bytes);
@@ -54,7 +55,8 @@ struct PlaneRing {
         } else {
             float4* d4 = reinterpret_cast<float4*>(dst);
             const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-            for (int i = threadIdx.x; i < plane_words / 4; i += blockDim.x) d4[i] = z;
+            const int n4 = plane_words * (int)sizeof(T) / 16;
+            for (int i = threadIdx.x; i < n4; i += blockDim.x) d4[i] = z;
             if (threadIdx.x == 0) dev::mbar_arrive_expect_tx(bar, 0u);
         }
     }

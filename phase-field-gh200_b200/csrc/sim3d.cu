@@ -91,6 +91,12 @@ struct pfb_sim3d {
     int mode_request = -1;              // as created: -1 auto
     int slots = 0;                      // scratch bricks of the in-place modes
     float* d_scratch = nullptr;
+    // base pools of binary16 / bfloat16 values (PhiStorage): the float
+    // pointers above then address 16-bit data; d_wide holds a binary32 copy
+    // of the current pool for the diagnostics and read-outs
+    int store = 0;
+    float* d_wide = nullptr;
+    size_t vbytes() const { return store ? 2 : 4; }
 
     void drop_graph() {
         if (graph_exec) cudaGraphExecDestroy(graph_exec);
@@ -122,6 +128,7 @@ struct pfb_sim3d {
         cudaFree(d_prom_ids);
         cudaFree(d_requests);
         cudaFree(d_scratch);
+        cudaFree(d_wide);
     }
     int prom_count() const { return (int)prom_ids.size(); }
 };
@@ -332,6 +339,7 @@ int validate3(const pfb_params3d& p) {
             return set_error(PFB_E_ARG, "channel Nz must equal H + 2*padding");
     }
     if (p.num_cells <= 0) return set_error(PFB_E_ARG, "num_cells must be positive");
+    if (p.phi_storage < 0 || p.phi_storage > 2) return set_error(PFB_E_ARG, "phi_storage must be 0, 1 or 2");
     if (!(p.dt > 0.0) || !(p.lambda > 0.0) || !(p.target_radius > 0.0) || !(p.xi > 0.0) ||
         !(p.tau > 0.0) || p.kappa < 0.0 || p.mu < 0.0 || p.v_A < 0.0 || !(p.gamma > 0.0))
         return set_error(PFB_E_ARG, "invalid model parameters");
@@ -423,6 +431,24 @@ bool full_step(const pfb_sim3d* s, long long step) {
     return s->p.full_moment_every > 0 && step % s->p.full_moment_every == 0;
 }
 
+// The current base pool as binary32 (a widened copy for 16-bit pools).
+int wide_pool(pfb_sim3d* s, const float** out) {
+    if (!s->store) {
+        *out = s->d_phi[s->cur_phi];
+        return PFB_OK;
+    }
+    const size_t n = (size_t)s->N * s->cell_words;
+    if (!s->d_wide) PFB3_CU(cudaMalloc(&s->d_wide, n * sizeof(float)), "cudaMalloc(widened pool)");
+    PFB3_RC(widen_pool(s->d_phi[s->cur_phi], s->d_wide, n, s->store, s->stream));
+    *out = s->d_wide;
+    return PFB_OK;
+}
+
+// Base slot n of pool b, in bytes of the storage type.
+void* pool_slot(pfb_sim3d* s, int b, int n) {
+    return static_cast<char*>(static_cast<void*>(s->d_phi[b])) + (size_t)n * s->cell_words * s->vbytes();
+}
+
 // The launches of one step on the current buffers (no host state changes).
 int launch_step(pfb_sim3d* s, bool full) {
     PFB3_CU(cudaMemcpyAsync(s->d_accepted, s->d_cells, (size_t)s->N * sizeof(pfb_cell3d),
@@ -433,23 +459,24 @@ int launch_step(pfb_sim3d* s, bool full) {
     const int np = s->prom_count();
     float* const* cur = s->d_cube[s->cur_cube];
     float* const* nxt = s->d_cube[1 - s->cur_cube];
-    if (s->fused && np == 0 && s->mem_mode == 0) {
+    if (s->fused && np == 0 && s->mem_mode == 0 && s->store == 0) {
         PFB3_RC(clear3d_launch(s->d_S[1 - s->cur_S], &s->L, nullptr, s->stream));
         PFB3_RC(step3d_launch(&m, &u, s->stream));
     } else {
         // base bricks, then the promoted cubes; motion after every measurement
-        PFB3_RC(measure3d_launch(&m, s->stream));
+        PFB3_RC(measure3d_launch_pool(&m, s->store, s->stream));
         if (np) PFB3_RC(measure3d_promoted_launch(&m, cur, s->d_prom_ids, np, s->max_edge, s->stream));
         PFB3_RC(motion3d_launch(&m, s->stream));
         if (u.S_out) PFB3_RC(clear3d_launch(u.S_out, &s->L, nullptr, s->stream));
         if (s->mem_mode == 0)
-            PFB3_RC(update3d_launch(&u, s->stream));
+            PFB3_RC(update3d_launch_pool(&u, s->store, s->d_step, s->p.seed, s->stream));
         else
-            PFB3_RC(update3d_inplace_launch(&u, s->d_scratch, s->slots, s->stream));
+            PFB3_RC(update3d_inplace_launch_pool(&u, s->d_scratch, s->slots, s->store, s->d_step, s->p.seed,
+                                                 s->stream));
         if (np)
             PFB3_RC(update3d_promoted_launch(&u, cur, nxt, s->d_prom_ids, np, s->max_edge, s->stream));
     }
-    PFB3_RC(repair3d_launch(&u, s->stream));
+    PFB3_RC(repair3d_launch_pool(&u, s->store, s->stream));
     if (np) PFB3_RC(repair3d_promoted_launch(&u, cur, nxt, s->d_prom_ids, np, s->max_edge, s->stream));
     PFB3_RC(pfb3d_finalize_origins(s->d_cells, s->N, s->d_flags, s->stream));
     PFB3_RC(pfb3d_restore_cells_after_fatal(s->d_cells, s->d_accepted, s->N, s->d_flags,
@@ -466,7 +493,7 @@ int launch_step(pfb_sim3d* s, bool full) {
         sa.layout = s->L;
         sa.N = s->N;
         sa.B = s->B;
-        PFB3_RC(scatter3d_launch(&sa, s->stream));
+        PFB3_RC(scatter3d_launch_pool(&sa, s->store, s->stream));
         if (np) PFB3_RC(scatter3d_promoted_launch(&sa, nxt, s->d_prom_ids, np, s->max_edge, 0, s->stream));
     }
     PFB3_RC(pfb3d_advance_step(s->d_step, s->d_flags, s->stream));
@@ -498,7 +525,7 @@ int reconstruct_S(pfb_sim3d* s) {
     sa.layout = s->L;
     sa.N = s->N;
     sa.B = s->B;
-    PFB3_RC(scatter3d_launch(&sa, s->stream));
+    PFB3_RC(scatter3d_launch_pool(&sa, s->store, s->stream));
     if (s->prom_count())
         PFB3_RC(scatter3d_promoted_launch(&sa, s->d_cube[s->cur_cube], s->d_prom_ids, s->prom_count(),
                                           s->max_edge, 0, s->stream));
@@ -509,7 +536,7 @@ int reconstruct_S(pfb_sim3d* s) {
 // only when asked (reference Sim3D::refresh_measurements).
 int refresh(pfb_sim3d* s, bool surface, bool motion) {
     const pfb_measure_args3d m = measure_args(s, false, surface);
-    PFB3_RC(measure3d_launch(&m, s->stream));
+    PFB3_RC(measure3d_launch_pool(&m, s->store, s->stream));
     if (s->prom_count())
         PFB3_RC(measure3d_promoted_launch(&m, s->d_cube[s->cur_cube], s->d_prom_ids, s->prom_count(),
                                           s->max_edge, s->stream));
@@ -591,23 +618,37 @@ int resize_cells(pfb_sim3d* s, const std::vector<std::pair<int, int>>& req,
         moves.push_back(m);
     }
     const size_t bw = (size_t)s->B * s->B * s->B;
+    const float* wide = nullptr;
+    float* brick = nullptr;  // a binary32 base brick on its way into a 16-bit pool
+    int rc0 = wide_pool(s, &wide);
+    if (!rc0 && s->store && cudaMalloc(&brick, bw * sizeof(float)) != cudaSuccess)
+        rc0 = set_error(PFB_E_NOMEM, "no device memory for a staging brick");
     for (Move& m : moves) {
-        const float* src = m.Eo > s->B ? s->h_cube[s->cur_cube][(size_t)m.id]
-                                       : s->d_phi[s->cur_phi] + (size_t)m.id * bw;
-        for (int b = 0; b < 2; ++b) {
+        const float* src = m.Eo > s->B ? s->h_cube[s->cur_cube][(size_t)m.id] : wide + (size_t)m.id * bw;
+        for (int b = 0; b < 2 && !rc0; ++b) {
             if (m.En == s->B && !s->d_phi[b]) continue;  // one pool in place
-            float* dst = m.En > s->B ? m.cube[b] : s->d_phi[b] + (size_t)m.id * bw;
-            const int rc = copy_centred3d_launch(src, m.Eo, dst, m.En, s->stream);
-            if (rc) {
-                release();
-                return rc;
+            if (m.En > s->B) {
+                rc0 = copy_centred3d_launch(src, m.Eo, m.cube[b], m.En, s->stream);
+            } else if (!s->store) {
+                rc0 = copy_centred3d_launch(src, m.Eo, s->d_phi[b] + (size_t)m.id * bw, m.En, s->stream);
+            } else {
+                rc0 = copy_centred3d_launch(src, m.Eo, brick, m.En, s->stream);
+                if (!rc0) rc0 = narrow_pool(brick, pool_slot(s, b, m.id), bw, s->store, s->stream);
             }
         }
     }
+    if (rc0) {
+        cudaStreamSynchronize(s->stream);
+        cudaFree(brick);
+        release();
+        return rc0;
+    }
     if (cudaStreamSynchronize(s->stream) != cudaSuccess) {
+        cudaFree(brick);
         release();
         return set_error(PFB_E_CUDA, "cube copies failed");
     }
+    cudaFree(brick);
     // install: tables, id list, records; then free the replaced cubes
     for (Move& m : moves)
         for (int b = 0; b < 2; ++b) {
@@ -820,8 +861,9 @@ int choose_storage(pfb_sim3d* s) {
         size_t free_b = 0, total_b = 0;
         if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = (size_t)-1;
         const double budget = 0.9 * (double)free_b;
-        const double pool = (double)s->N * (double)s->cell_words * 4.0, agg = (double)s->s_words * 4.0;
-        const double brick = (double)s->cell_words * 4.0;
+        const double vb = (double)s->vbytes();
+        const double pool = (double)s->N * (double)s->cell_words * vb, agg = (double)s->s_words * 4.0;
+        const double brick = (double)s->cell_words * vb;
         mode = 2 * pool + 2 * agg <= budget ? 0 : pool + 2 * agg + want * brick <= budget ? 1 : 2;
     }
     s->mem_mode = mode;
@@ -847,6 +889,7 @@ int alloc_impl(pfb_sim3d* s, const pfb_params3d* pp, int device) {
     s->L.boundary_flags = p.boundary_flags;
     if (!geometry_ok3(s->B, s->L)) return set_error(PFB_E_ARG, "the brick must fit inside the domain");
     s->V0 = volume0(p);
+    s->store = p.phi_storage;
     s->fused = 0;  // the separate launches measure faster (both are issue-bound)
     s->s_words = (size_t)s->L.pitch_x * s->L.ny * s->L.nz;
     s->cell_words = (size_t)s->B * s->B * s->B;
@@ -854,12 +897,12 @@ int alloc_impl(pfb_sim3d* s, const pfb_params3d* pp, int device) {
     PFB3_RC(choose_storage(s));
     for (int i = 0; i < 2; ++i) {
         if (i == 0 || s->mem_mode == 0)
-            PFB3_CU(cudaMalloc(&s->d_phi[i], (size_t)s->N * s->cell_words * sizeof(float)), "cudaMalloc(phi)");
+            PFB3_CU(cudaMalloc(&s->d_phi[i], (size_t)s->N * s->cell_words * s->vbytes()), "cudaMalloc(phi)");
         if (i == 0 || s->mem_mode != 2)
             PFB3_CU(cudaMalloc(&s->d_S[i], s->s_words * sizeof(uint32_t)), "cudaMalloc(S)");
     }
     if (s->mem_mode != 0)
-        PFB3_CU(cudaMalloc(&s->d_scratch, (size_t)s->slots * s->cell_words * sizeof(float)),
+        PFB3_CU(cudaMalloc(&s->d_scratch, (size_t)s->slots * s->cell_words * s->vbytes()),
                 "cudaMalloc(scratch bricks)");
     PFB3_CU(cudaMalloc(&s->d_cells, (size_t)s->N * sizeof(pfb_cell3d)), "cudaMalloc(cells)");
     PFB3_CU(cudaMalloc(&s->d_accepted, (size_t)s->N * sizeof(pfb_cell3d)), "cudaMalloc(cells)");
@@ -945,8 +988,15 @@ int create_impl(pfb_sim3d* s, const pfb_params3d* pp, const pfb_vec3* centres, i
     double seed = 0.0;
     PFB3_RC(pfb3d_calibrate_seed_radius(p.target_radius, p.lambda, s->B, &seed, nullptr));
     pfb_init_args3d ia{};
-    ia.phi_even = s->d_phi[0];
-    ia.phi_odd = s->d_phi[1];
+    float* seeded = nullptr;  // 16-bit pools: seeded in binary32, then rounded to nearest
+    if (s->store) {
+        PFB3_CU(cudaMalloc(&seeded, (size_t)s->N * s->cell_words * sizeof(float)), "cudaMalloc(seeding)");
+        if (s->d_phi[1])
+            PFB3_CU(cudaMemsetAsync(s->d_phi[1], 0, (size_t)s->N * s->cell_words * s->vbytes(), s->stream),
+                    "clear pool");
+    }
+    ia.phi_even = s->store ? seeded : s->d_phi[0];
+    ia.phi_odd = s->store ? nullptr : s->d_phi[1];
     ia.cells = s->d_cells;
     ia.centres = s->d_centres;
     ia.N = s->N;
@@ -954,7 +1004,13 @@ int create_impl(pfb_sim3d* s, const pfb_params3d* pp, const pfb_vec3* centres, i
     ia.layout = s->L;
     ia.lambda = (float)p.lambda;
     ia.seed_radius = (float)seed;
-    PFB3_RC(init3d_launch(&ia, s->stream));
+    int rc = init3d_launch(&ia, s->stream);
+    if (!rc && s->store) rc = narrow_pool(seeded, s->d_phi[0], (size_t)s->N * s->cell_words, s->store, s->stream);
+    if (seeded) {
+        cudaStreamSynchronize(s->stream);
+        cudaFree(seeded);
+    }
+    PFB3_RC(rc);
     PFB3_RC(remeasure_impl(s));
     PFB3_CU(cudaStreamSynchronize(s->stream), "fresh initialisation");
     set_accepted(s, 0);
@@ -982,11 +1038,14 @@ int restore_impl(pfb_sim3d* s, const pfb_params3d* pp, const pfb_cell3d* cells_i
     }
     const size_t bw = s->cell_words;
     size_t off = 0;
+    // 16-bit pools: the base bricks go through a binary32 copy, rounded to nearest
+    float* staged = s->d_phi[0];
+    if (s->store) PFB3_CU(cudaMalloc(&staged, (size_t)s->N * bw * sizeof(float)), "cudaMalloc(staging)");
     for (int i = 0; i < s->N; ++i) {
         const int E = edge_of(s, cells[(size_t)i]);
         const size_t words = (size_t)E * E * E;
         if (E == s->B) {
-            PFB3_CU(cudaMemcpy(s->d_phi[0] + (size_t)i * bw, phi + off, words * sizeof(float),
+            PFB3_CU(cudaMemcpy(staged + (size_t)i * bw, phi + off, words * sizeof(float),
                                cudaMemcpyHostToDevice),
                     "upload brick");
         } else {
@@ -1001,11 +1060,17 @@ int restore_impl(pfb_sim3d* s, const pfb_params3d* pp, const pfb_cell3d* cells_i
         }
         off += words;
     }
+    if (s->store) {
+        const int rc = narrow_pool(staged, s->d_phi[0], (size_t)s->N * bw, s->store, s->stream);
+        cudaStreamSynchronize(s->stream);
+        cudaFree(staged);
+        PFB3_RC(rc);
+    }
     PFB3_RC(upload_tables(s));
     PFB3_CU(cudaMemcpyAsync(s->d_cells, cells.data(), (size_t)s->N * sizeof(pfb_cell3d), cudaMemcpyHostToDevice,
                             s->stream), "upload cells");
     if (s->d_phi[1])
-        PFB3_CU(cudaMemsetAsync(s->d_phi[1], 0, (size_t)s->N * s->cell_words * sizeof(float), s->stream),
+        PFB3_CU(cudaMemsetAsync(s->d_phi[1], 0, (size_t)s->N * s->cell_words * s->vbytes(), s->stream),
                 "clear phi");
     const uint64_t st = (uint64_t)step;
     PFB3_CU(cudaMemcpyAsync(s->d_step, &st, sizeof(st), cudaMemcpyHostToDevice, s->stream), "step");
@@ -1094,7 +1159,9 @@ int pfb_sim3d_measure_wall(pfb_sim3d* s) {
     if (!hard_wall_channel(s->p.boundary_flags) || !s->d_wall_psi)
         return set_error(PFB_E_CONFIG, "wall diagnostics need the hard-wall channel");
     PFB3_CU(cudaSetDevice(s->device), "cudaSetDevice");
-    k_wall_diag3d<<<s->N, kWallThreads, 0, s->stream>>>(s->d_phi[s->cur_phi], s->d_cube[s->cur_cube],
+    const float* wide = nullptr;
+    PFB3_RC(wide_pool(s, &wide));
+    k_wall_diag3d<<<s->N, kWallThreads, 0, s->stream>>>(wide, s->d_cube[s->cur_cube],
                                                        s->d_cells, s->B,
                                                        s->p.Nz, s->p.channel_padding,
                                                        s->p.channel_height, s->d_wall_psi);
@@ -1118,7 +1185,9 @@ int pfb_sim3d_verify(pfb_sim3d* s, double* max_rel_V, uint32_t* max_S,
         cudaMemsetAsync(d_m, 0, 4, s->stream) != cudaSuccess) {
         rc = set_error(PFB_E_CUDA, "verify: allocation failed");
     } else {
-        k_verify3d<<<s->N, kWallThreads, 0, s->stream>>>(s->d_phi[s->cur_phi], s->d_cube[s->cur_cube],
+        const float* wide = nullptr;
+        if (wide_pool(s, &wide)) return PFB_E_CUDA;
+        k_verify3d<<<s->N, kWallThreads, 0, s->stream>>>(wide, s->d_cube[s->cur_cube],
                                                          s->d_cells, s->B, s->p.Nz,
                                                          periodic ? 1 : 0,
                                                          substrate_slab(s->p.boundary_flags) ? 1 : 0, d_r);
@@ -1158,7 +1227,9 @@ int pfb_sim3d_boundary_open(pfb_sim3d* s, const char* path, int projection, long
 int pfb_sim3d_boundary_capture(pfb_sim3d* s) {
     if (!s || !s->bnd) return set_error(PFB_E_STATE, "no boundary recorder is open");
     PFB3_CU(cudaSetDevice(s->device), "cudaSetDevice");
-    return pfb::boundary3d_capture(s->bnd, s->d_phi[s->cur_phi], s->d_cube[s->cur_cube], s->d_cells, s->B,
+    const float* wide = nullptr;
+    PFB3_RC(wide_pool(s, &wide));
+    return pfb::boundary3d_capture(s->bnd, wide, s->d_cube[s->cur_cube], s->d_cells, s->B,
                                    s->stream,
                               s->steps_done, (double)s->steps_done * s->p.dt);
 }
@@ -1188,6 +1259,8 @@ int pfb_sim3d_set_fused(pfb_sim3d* s, int fused) {
     if (!s) return set_error(PFB_E_ARG, "null sim");
     if (fused && step3d_cluster(s->B) == 0)
         return set_error(PFB_E_CONFIG, "brick edge %d does not fit the fused step", s->B);
+    if (fused && (s->store || s->mem_mode))
+        return set_error(PFB_E_CONFIG, "the fused step needs binary32 pools in the throughput mode");
     const int f = fused ? 1 : 0;
     if (f != s->fused) {
         PFB3_CU(cudaStreamSynchronize(s->stream), "sync");
@@ -1241,9 +1314,10 @@ int pfb_sim3d_get_cells(pfb_sim3d* s, pfb_cell3d* out) {
 
 int pfb_sim3d_get_phi(pfb_sim3d* s, float* out) {
     if (!s || !out) return set_error(PFB_E_ARG, "null argument");
+    const float* wide = nullptr;
+    PFB3_RC(wide_pool(s, &wide));
     PFB3_CU(cudaStreamSynchronize(s->stream), "sync");
-    PFB3_CU(cudaMemcpy(out, s->d_phi[s->cur_phi], (size_t)s->N * s->cell_words * sizeof(float),
-                       cudaMemcpyDeviceToHost),
+    PFB3_CU(cudaMemcpy(out, wide, (size_t)s->N * s->cell_words * sizeof(float), cudaMemcpyDeviceToHost),
             "copy phi");
     return PFB_OK;
 }
@@ -1260,12 +1334,14 @@ int pfb_sim3d_get_packed(pfb_sim3d* s, float* out) {
     if (!s || !out) return set_error(PFB_E_ARG, "null argument");
     std::vector<pfb_cell3d> c((size_t)s->N);
     PFB3_RC(pfb_sim3d_get_cells(s, c.data()));
+    const float* wide = nullptr;
+    PFB3_RC(wide_pool(s, &wide));
+    PFB3_CU(cudaStreamSynchronize(s->stream), "sync");
     size_t off = 0;
     for (int n = 0; n < s->N; ++n) {
         const int E = edge_of(s, c[(size_t)n]);
         const size_t words = (size_t)E * E * E;
-        const float* src = E > s->B ? s->h_cube[s->cur_cube][(size_t)n]
-                                    : s->d_phi[s->cur_phi] + (size_t)n * s->cell_words;
+        const float* src = E > s->B ? s->h_cube[s->cur_cube][(size_t)n] : wide + (size_t)n * s->cell_words;
         if (!src) return set_error(PFB_E_STATE, "cell %d has no cube of edge %d", n, E);
         PFB3_CU(cudaMemcpy(out + off, src, words * sizeof(float), cudaMemcpyDeviceToHost), "copy field");
         off += words;

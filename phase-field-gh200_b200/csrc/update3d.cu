@@ -23,6 +23,7 @@
 #include "pfb3d_common.cuh"
 #include "pfb_internal.h"
 #include "ring3d.cuh"
+#include "storage2d.cuh"
 #include "update3d_common.cuh"
 
 namespace pfb {
@@ -42,12 +43,18 @@ struct UpdateHeader {
 };
 constexpr int kUHeader = (int)((sizeof(UpdateHeader) + 127) / 128 * 128);
 
-// GEO: 0 periodic, 1 substrate slab, 2 hard-wall channel. out_by_slot: the
-// output brick of selection slot k is phi_out + k B^3 (the scratch bricks of
-// the in-place modes) instead of the cell's own slot.
-template <int GEO>
+// GEO: 0 periodic, 1 substrate slab, 2 hard-wall channel; T: storage type
+// of the phi pools. out_by_slot: the output brick of selection slot k is
+// phi_out + k B^3 (the scratch bricks of the in-place modes) instead of the
+// cell's own slot. Rounding of 16-bit pools: stream of (step, cell, sr_seed).
+struct PoolRounding {
+    const uint64_t* step;
+    uint64_t seed;
+};
+
+template <int GEO, typename T>
 __global__ void __launch_bounds__(kUThreads, 2)
-    k_update3d(const __grid_constant__ pfb_update_args3d A, int out_by_slot) {
+    k_update3d(const __grid_constant__ pfb_update_args3d A, int out_by_slot, PoolRounding R) {
     extern __shared__ __align__(128) char smem[];
     UpdateHeader& H = *reinterpret_cast<UpdateHeader*>(smem);
     const int B = A.B;
@@ -59,11 +66,12 @@ __global__ void __launch_bounds__(kUThreads, 2)
     if (cell->storage_edge > (uint32_t)B) return;
     const pfb_layout3d L = A.layout;
     const size_t words = (size_t)B * B * B;
-    const float* src = A.phi_in + (size_t)n * words;
-    float* dst = A.phi_out + (size_t)(out_by_slot ? slot_cell : n) * words;
+    const T* src = reinterpret_cast<const T*>(A.phi_in) + (size_t)n * words;
+    T* dst = reinterpret_cast<T*>(A.phi_out) + (size_t)(out_by_slot ? slot_cell : n) * words;
     const int PB = B / kUCtasPerCell;
     const int d0 = part * PB, d1 = d0 + PB;
     const int64_t oz = cell->origin_z;
+    const uint32_t sr = Store<T>::kHalf ? sr_stream(R.step ? *R.step : 0ull, cell->global_id, R.seed) : 0u;
 
     UpdateCell U;
     U.S_in = A.S_in;
@@ -97,7 +105,7 @@ __global__ void __launch_bounds__(kUThreads, 2)
     U.k.inter = A.interaction_coeff;
     U.k.dt = A.dt;
 
-    PlaneRing<kURing> ring{reinterpret_cast<float*>(smem + kUHeader), H.bars, B * B};
+    PlaneRing<kURing, T> ring{reinterpret_cast<T*>(smem + kUHeader), H.bars, B * B};
     ring.init();
     __syncthreads();
     // request k <-> requested source plane d0 + sz - 1 + k, k = 0 .. PB + 1
@@ -137,8 +145,9 @@ __global__ void __launch_bounds__(kUThreads, 2)
         for (int it = tid; it < items; it += kUThreads) {
             const int x0 = 4 * (it % strips);
             const int y0 = 4 * (it / strips);
-            update_item<GEO>(U, ring.slot(i), ring.slot(i + 1), ring.slot(i + 2), x0, y0, sx, sy,
-                             live, wz, wallv, top_plane, dst + ((size_t)dz * B + y0) * B + x0, cnt);
+            const uint32_t pix0 = (uint32_t)(((size_t)dz * B + y0) * B + x0);
+            update_item<GEO, T>(U, ring.slot(i), ring.slot(i + 1), ring.slot(i + 2), x0, y0, sx, sy,
+                                live, wz, wallv, top_plane, dst + pix0, cnt, sr, pix0);
         }
         __syncthreads();
         // after a timed-out wait nothing more is issued into the ring
@@ -154,7 +163,7 @@ __global__ void __launch_bounds__(kUThreads, 2)
 
     unsigned clip = 0u;
     if ((sx | sy | sz) != 0 && !H.abort)
-        clip = clip_check<GEO>(U, src, wall, d0, d1, sx, sy, sz, oz, cnt, kUThreads);
+        clip = clip_check<GEO, T>(U, src, wall, d0, d1, sx, sy, sz, oz, cnt, kUThreads);
     raise_update_counts<kUThreads>(H.cnt, cnt, clip, cell, A.global_flags);
 }
 
@@ -163,7 +172,9 @@ __global__ void __launch_bounds__(kUThreads, 2)
 // ---------------------------------------------------------------------------
 int geometry_ok3(int B, const pfb_layout3d& L);
 
-size_t update3d_smem(int B) { return (size_t)kUHeader + (size_t)kURing * (size_t)B * B * 4; }
+size_t update3d_smem(int B, int bytes = 4) {
+    return (size_t)kUHeader + (size_t)kURing * (size_t)B * B * bytes;
+}
 
 int check_update(const pfb_update_args3d* a, bool pools) {
     if (!a) return set_error(PFB_E_ARG, "null update arguments");
@@ -191,41 +202,61 @@ int check_update(const pfb_update_args3d* a, bool pools) {
     return PFB_OK;
 }
 
-static int update_launch(const pfb_update_args3d& A, int out_by_slot, cudaStream_t stream) {
+template <int GEO, typename T>
+static cudaError_t update_launch_gt(const pfb_update_args3d& A, int out_by_slot, PoolRounding R,
+                                    dim3 grid, size_t smem, cudaStream_t stream) {
+    cudaError_t e = cudaFuncSetAttribute(k_update3d<GEO, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e == cudaSuccess) k_update3d<GEO, T><<<grid, kUThreads, smem, stream>>>(A, out_by_slot, R);
+    return e;
+}
+
+template <typename T>
+static cudaError_t update_launch_t(const pfb_update_args3d& A, int out_by_slot, PoolRounding R, dim3 grid,
+                                   size_t smem, cudaStream_t stream) {
     const uint32_t bf = A.layout.boundary_flags;
+    if (periodic_xyz(bf)) return update_launch_gt<0, T>(A, out_by_slot, R, grid, smem, stream);
+    if (substrate_slab(bf)) return update_launch_gt<1, T>(A, out_by_slot, R, grid, smem, stream);
+    return update_launch_gt<2, T>(A, out_by_slot, R, grid, smem, stream);
+}
+
+static int update_launch(const pfb_update_args3d& A, int out_by_slot, int storage, PoolRounding R,
+                         cudaStream_t stream) {
     const int count = A.selection.ids ? A.selection.count : A.N;
     if (count == 0) return PFB_OK;
-    const size_t smem = update3d_smem(A.B);
+    const size_t smem = update3d_smem(A.B, storage ? 2 : 4);
     if (smem > 227 * 1024) return set_error(PFB_E_CONFIG, "brick edge too large for the plane ring");
     const dim3 grid((unsigned)(count * kUCtasPerCell));
     cudaError_t e;
-    if (periodic_xyz(bf)) {
-        e = cudaFuncSetAttribute(k_update3d<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e == cudaSuccess) k_update3d<0><<<grid, kUThreads, smem, stream>>>(A, out_by_slot);
-    } else if (substrate_slab(bf)) {
-        e = cudaFuncSetAttribute(k_update3d<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e == cudaSuccess) k_update3d<1><<<grid, kUThreads, smem, stream>>>(A, out_by_slot);
-    } else {
-        e = cudaFuncSetAttribute(k_update3d<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e == cudaSuccess) k_update3d<2><<<grid, kUThreads, smem, stream>>>(A, out_by_slot);
-    }
+    if (storage == kStoreF16)
+        e = update_launch_t<__half>(A, out_by_slot, R, grid, smem, stream);
+    else if (storage == kStoreBF16)
+        e = update_launch_t<__nv_bfloat16>(A, out_by_slot, R, grid, smem, stream);
+    else
+        e = update_launch_t<float>(A, out_by_slot, R, grid, smem, stream);
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) return set_error(PFB_E_CUDA, "update launch: %s", cudaGetErrorString(e));
     return PFB_OK;
 }
 
 int update3d_launch(const pfb_update_args3d* a, cudaStream_t stream) {
+    return update3d_launch_pool(a, kStoreF32, nullptr, 0, stream);
+}
+
+int update3d_launch_pool(const pfb_update_args3d* a, int storage, const uint64_t* step, uint64_t seed,
+                         cudaStream_t stream) {
     const int rc = check_update(a);
     if (rc) return rc;
-    return update_launch(*a, 0, stream);
+    if (storage < kStoreF32 || storage > kStoreBF16) return set_error(PFB_E_ARG, "unknown phi storage");
+    return update_launch(*a, 0, storage, PoolRounding{step, seed}, stream);
 }
 
 // In-place commit: the scratch brick of selection slot k becomes cell
 // ids[k]'s field unless the cell or the step holds a fatal flag, in which
 // case the field stays and the planned shift is dropped (reference
 // k_update_inplace_impl, src/pf3d/kernels.cu:1996-2045).
-__global__ void k_commit3d(float* pool, const float* scratch, pfb_cell3d* cells, const uint32_t* g,
-                           const int* ids, int B) {
+__global__ void k_commit3d(void* pool, const void* scratch, pfb_cell3d* cells, const uint32_t* g,
+                           const int* ids, int B, int bytes) {
     __shared__ int keep;
     const int k = (int)blockIdx.x;
     const int n = ids[k];
@@ -241,10 +272,10 @@ __global__ void k_commit3d(float* pool, const float* scratch, pfb_cell3d* cells,
     }
     __syncthreads();
     if (keep) return;
-    const size_t v4 = (size_t)B * B * B / 4;
-    const float4* s4 = reinterpret_cast<const float4*>(scratch + (size_t)k * B * B * B);
-    float4* d4 = reinterpret_cast<float4*>(pool + (size_t)n * B * B * B);
-    for (size_t i = threadIdx.x; i < v4; i += blockDim.x) d4[i] = s4[i];
+    const size_t brick = (size_t)B * B * B * bytes;
+    const float4* s4 = reinterpret_cast<const float4*>(static_cast<const char*>(scratch) + (size_t)k * brick);
+    float4* d4 = reinterpret_cast<float4*>(static_cast<char*>(pool) + (size_t)n * brick);
+    for (size_t i = threadIdx.x; i < brick / 16; i += blockDim.x) d4[i] = s4[i];
 }
 
 // The in-place update of the reference's balanced and compact modes
@@ -253,11 +284,16 @@ __global__ void k_commit3d(float* pool, const float* scratch, pfb_cell3d* cells,
 // A.phi_out is ignored; A.S_out may be null (compact: the caller rebuilds S).
 int update3d_inplace_launch(const pfb_update_args3d* a, float* scratch, int slots,
                             cudaStream_t stream) {
+    return update3d_inplace_launch_pool(a, scratch, slots, kStoreF32, nullptr, 0, stream);
+}
+
+int update3d_inplace_launch_pool(const pfb_update_args3d* a, void* scratch, int slots, int storage,
+                                 const uint64_t* step, uint64_t seed, cudaStream_t stream) {
     if (!a) return set_error(PFB_E_ARG, "null update arguments");
     if (!scratch || slots <= 0 || ((uintptr_t)scratch & 15u))
         return set_error(PFB_E_ARG, "in-place update needs aligned scratch bricks");
     pfb_update_args3d A = *a;
-    A.phi_out = scratch;
+    A.phi_out = static_cast<float*>(scratch);
     int rc = check_update(&A, false);
     if (rc) return rc;
     if (!A.phi_in || ((uintptr_t)A.phi_in & 15u)) return set_error(PFB_E_ARG, "invalid phi pool");
@@ -281,9 +317,10 @@ int update3d_inplace_launch(const pfb_update_args3d* a, float* scratch, int slot
         const int nb = count - b0 < slots ? count - b0 : slots;
         A.selection.ids = ids + b0;
         A.selection.count = nb;
-        rc = update_launch(A, 1, stream);
+        rc = update_launch(A, 1, storage, PoolRounding{step, seed}, stream);
         if (!rc) {
-            k_commit3d<<<nb, 256, 0, stream>>>(a->phi_in, scratch, A.cells, A.global_flags, ids + b0, A.B);
+            k_commit3d<<<nb, 256, 0, stream>>>(a->phi_in, scratch, A.cells, A.global_flags, ids + b0, A.B,
+                                               storage ? 2 : 4);
             const cudaError_t e = cudaGetLastError();
             if (e != cudaSuccess) rc = set_error(PFB_E_CUDA, "in-place commit: %s", cudaGetErrorString(e));
         }

@@ -13,6 +13,7 @@
 
 #include "device_util.cuh"
 #include "pfb3d_common.cuh"
+#include "phi3d.cuh"
 
 namespace pfb {
 namespace p3 {
@@ -58,27 +59,23 @@ __device__ __forceinline__ void stencil27w(const float (&w)[3][3][6], int j, flo
 // Six source values of one row, columns xs0 - 1 .. xs0 + 4 (zero outside the
 // brick or when the row is outside it); the alignment decision is taken once
 // per strip.
-__device__ __forceinline__ void row6v(const float* plane, int B, int ys, int xs0, bool vec_ok,
-                                      float* v) {
+template <typename T>
+__device__ __forceinline__ void row6v(const T* plane, int B, int ys, int xs0, bool vec_ok, float* v) {
     if ((unsigned)ys >= (unsigned)B) {
 #pragma unroll
         for (int c = 0; c < 6; ++c) v[c] = 0.0f;
         return;
     }
-    const float* row = plane + ys * B;
+    const T* row = plane + ys * B;
     if (vec_ok) {
-        const float4 m = *reinterpret_cast<const float4*>(row + xs0);
-        v[0] = xs0 > 0 ? row[xs0 - 1] : 0.0f;
-        v[1] = m.x;
-        v[2] = m.y;
-        v[3] = m.z;
-        v[4] = m.w;
-        v[5] = xs0 + 4 < B ? row[xs0 + 4] : 0.0f;
+        phi_ld4(row + xs0, v + 1);
+        v[0] = xs0 > 0 ? phi_ld1(row + xs0 - 1) : 0.0f;
+        v[5] = xs0 + 4 < B ? phi_ld1(row + xs0 + 4) : 0.0f;
     } else {
 #pragma unroll
         for (int c = 0; c < 6; ++c) {
             const int x = xs0 - 1 + c;
-            v[c] = (unsigned)x < (unsigned)B ? row[x] : 0.0f;
+            v[c] = (unsigned)x < (unsigned)B ? phi_ld1(row + x) : 0.0f;
         }
     }
 }
@@ -132,22 +129,25 @@ struct UpdateCounts {
 // One item of destination plane dz: columns x0 .. x0 + 3 of rows
 // y0 .. y0 + 3, read from source plane dz + sz (p1) and its neighbours p0,
 // p2 at in-plane offset (sx, sy); `live` false (source plane outside the
-// brick or the domain) writes zeros. orow points at (dz, y0, x0) of phi_out.
+// brick or the domain) writes zeros. orow points at (dz, y0, x0) of phi_out,
+// voxel pix0 of the brick (16-bit pools: rounding stream sr).
 // GEO: 0 periodic, 1 substrate slab, 2 hard-wall channel.
-template <int GEO>
-__device__ __forceinline__ void update_item(const UpdateCell& U, const float* p0, const float* p1,
-                                            const float* p2, int x0, int y0, int sx, int sy,
+template <int GEO, typename T = float>
+__device__ __forceinline__ void update_item(const UpdateCell& U, const T* p0, const T* p1,
+                                            const T* p2, int x0, int y0, int sx, int sy,
                                             bool live, int wz, float wallv, bool top_plane,
-                                            float* orow, UpdateCounts& c) {
+                                            T* orow, UpdateCounts& c, uint32_t sr = 0u,
+                                            uint32_t pix0 = 0u) {
     const int B = U.B;
     const pfb_layout3d& L = U.L;
     if (!live) {
-        const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float z[4] = {0.f, 0.f, 0.f, 0.f};
+        const uint16_t zb[4] = {0, 0, 0, 0};
 #pragma unroll
-        for (int r = 0; r < 4; ++r) __stcs(reinterpret_cast<float4*>(orow + r * B), z4);
+        for (int r = 0; r < 4; ++r) phi_st4(orow + r * B, z, zb);
         return;
     }
-    const float* pl[3] = {p0, p1, p2};
+    const T* pl[3] = {p0, p1, p2};
     const int xs0 = x0 + sx;
     const bool vec_ok = (xs0 & 3) == 0 && xs0 >= 0 && xs0 + 4 <= B;
     float w[3][3][6];
@@ -194,6 +194,7 @@ __device__ __forceinline__ void update_item(const UpdateCell& U, const float* p0
 #pragma unroll
         for (int j = 0; j < 4; ++j) stencil27r(w, s0, s1, s2, j, lap[j], gx[j], gy[j], gz[j]);
         float out[4];
+        uint16_t ob[4] = {0, 0, 0, 0};
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const bool present = yin && wxj[j] >= 0;
@@ -203,14 +204,17 @@ __device__ __forceinline__ void update_item(const UpdateCell& U, const float* p0
             const bool neg = agg[j] < own;
             float other = neg ? 0.0f : (float)(agg[j] - own) * kQInv;
             if (GEO == 2) other += wallv;
-            const float next = cv + U.k.dt * rhs3(U.k, cv, lap[j], gx[j], gy[j], gz[j], other);
-            const bool nfin = isfinite(next);
+            const float exact = cv + U.k.dt * rhs3(U.k, cv, lap[j], gx[j], gy[j], gz[j], other);
+            const bool nfin = isfinite(exact);
+            // the stored value (binary32: exact)
+            const float next = phi_round<T>(exact, sr, pix0 + (uint32_t)(r * B + j), &ob[j]);
             const bool top = GEO == 1 && top_plane && fabsf(next) > kSupportEps3;
             c.nf += (present && (!cfin || !nfin)) ? 1u : 0u;
             c.neg += (present && cfin && neg) ? 1u : 0u;
             c.top += (present && cfin && nfin && top) ? 1u : 0u;
             const bool keep = present && cfin && nfin && !top;
             out[j] = keep ? next : 0.0f;
+            if (!keep) ob[j] = 0;
             q_prev[j] = 0u;
             old_prev[j] = 0u;
             if (has_out) {
@@ -220,7 +224,7 @@ __device__ __forceinline__ void update_item(const UpdateCell& U, const float* p0
                 old_prev[j] = dev::atom_add_nonzero(U.S_out + srow + (keep ? wxj[j] : 0), qv);
             }
         }
-        __stcs(reinterpret_cast<float4*>(orow + r * B), make_float4(out[0], out[1], out[2], out[3]));
+        phi_st4(orow + r * B, out, ob);
     }
 #pragma unroll
     for (int j = 0; j < 4; ++j) c.ovf += old_prev[j] > 0xFFFFFFFFu - q_prev[j] ? 1u : 0u;
@@ -228,14 +232,15 @@ __device__ __forceinline__ void update_item(const UpdateCell& U, const float* p0
 
 // Fatal step: destination planes [d0, d1) keep the accepted field, which is
 // scattered again (reference kernels.cu:505-559). Every thread of the CTA.
-__device__ __forceinline__ void keep_planes(const UpdateCell& U, const float* src, float* dst,
-                                            int d0, int d1, int64_t oz, pfb_cell3d* cell,
-                                            uint32_t* gflags, int nthreads) {
+template <typename T = float>
+__device__ __forceinline__ void keep_planes(const UpdateCell& U, const T* src, T* dst, int d0, int d1,
+                                            int64_t oz, pfb_cell3d* cell, uint32_t* gflags,
+                                            int nthreads) {
     const int B = U.B;
     const pfb_layout3d& L = U.L;
     for (size_t q = (size_t)d0 * B * B + threadIdx.x; q < (size_t)d1 * B * B; q += nthreads) {
-        const float v = src[q];
-        dst[q] = v;
+        dst[q] = src[q];
+        const float v = phi_ld1(src + q);
         if (U.S_out && isfinite(v)) {
             const int x = (int)(q % B), y = (int)((q / B) % B), z = (int)(q / ((size_t)B * B));
             int wz;
@@ -255,8 +260,8 @@ __device__ __forceinline__ void keep_planes(const UpdateCell& U, const float* sr
 // after the shift: nothing is written, but a supported new value is a
 // DESTINATION_CLIP (read from global memory; shifts are rare). Adds to the
 // non-finite, negative and top counts as the update would.
-template <int GEO>
-__device__ __forceinline__ unsigned clip_check(const UpdateCell& U, const float* src, const float* wall,
+template <int GEO, typename T = float>
+__device__ __forceinline__ unsigned clip_check(const UpdateCell& U, const T* src, const float* wall,
                                                int d0, int d1, int sx, int sy, int sz, int64_t oz,
                                                UpdateCounts& c, int nthreads) {
     const int B = U.B;
@@ -266,7 +271,7 @@ __device__ __forceinline__ unsigned clip_check(const UpdateCell& U, const float*
         if ((unsigned)x >= (unsigned)B || (unsigned)y >= (unsigned)B) return 0.0f;
         int s;
         if (!fetch_plane(L, oz, z, B, &s)) return 0.0f;
-        return src[((size_t)s * B + y) * B + x];
+        return phi_ld1(src + ((size_t)s * B + y) * B + x);
     };
     const size_t plane = (size_t)B * B;
     for (size_t q = (size_t)d0 * plane + threadIdx.x; q < (size_t)d1 * plane; q += nthreads) {
@@ -276,7 +281,7 @@ __device__ __forceinline__ unsigned clip_check(const UpdateCell& U, const float*
             continue;
         int wz;
         if (!aggregate_z(L, oz, z, &wz)) continue;
-        const float cv = src[q];
+        const float cv = phi_ld1(src + q);
         if (!isfinite(cv)) {
             ++c.nf;
             continue;

@@ -131,7 +131,7 @@ class Params3D(C.Structure):
         ("aging_time", C.c_double), ("wall_kappa", C.c_double), ("wall_width", C.c_double),
         ("channel_height", C.c_int), ("channel_padding", C.c_int),
         ("seed", C.c_uint64), ("polarity_seed", C.c_uint64), ("full_moment_every", C.c_int),
-        ("gamma_soft", C.c_double), ("soft_fraction", C.c_double),
+        ("gamma_soft", C.c_double), ("soft_fraction", C.c_double), ("phi_storage", C.c_int),
     ]
 
 

@@ -49,6 +49,7 @@ class SimParams3D:
     full_moment_every: int = 100
     gamma_soft: float = 0.35     # soft cells' stiffness (reference gamma_cancer)
     soft_fraction: float = 0.0   # share of soft identities (reference cancer_fraction)
+    phi_storage: int = 0         # base pools: 0 binary32, 1 binary16, 2 bfloat16
 
     def to_c(self) -> Params3D:
         p = Params3D()
