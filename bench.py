@@ -608,6 +608,7 @@ def run_surrogate(a):
     if rank != 0:
         return 0
     torch.cuda.set_device(local)
+    pfb200.lib().pfb_conv_set_pipeline(a.conv_pipeline)
     if a.profile_forward:
         net = sg.Surrogate2D(max_batch=512, seed=1, device=local)
         ms = net.bench_forward(512, 3)
@@ -617,7 +618,9 @@ def run_surrogate(a):
         for _ in range(2):
             net.train_step(x, t, idx, 1e-4)
         net.sync()
-        print(json.dumps({"profile_forward_ms": ms, "batch": 512}), flush=True)
+        print(json.dumps({"profile_forward_ms": ms, "batch": 512,
+                          "tflops": sg.forward_flops(512) / (ms / 1000.0) / 1e12,
+                          "conv_pipeline": a.conv_pipeline}), flush=True)
         net.close()
         return 0
     interval, history, heal = 8000, 100, 100
@@ -744,6 +747,8 @@ def main():
     ap.add_argument("--repeats", type=int, default=3, help="cs: relaxations per method (median)")
     ap.add_argument("--max-steps", type=int, default=150000,
                     help="cs: plain solver steps after which a relaxation gives up")
+    ap.add_argument("--conv-pipeline", type=int, default=1, choices=[0, 1],
+                    help="cs: 1 the persistent warp-specialised forward convolution, 0 one tile per CTA")
     ap.add_argument("--profile-forward", action="store_true",
                     help="cs: only 3 forward passes and 2 training steps of the U-Net on 512 "
                          "zero crops (a short command for ncu)")

@@ -87,6 +87,15 @@ int pfb_conv3x3_wgrad_noalloc(const void* x, const void* dy, float* dw_oihw, flo
  * tensor-core MMAs gave up (the kernel skipped its output). clear != 0
  * resets it. */
 int pfb_conv_status(unsigned* out, int clear);
+/* (pfb_conv_status bit 1: the persistent forward found its shared memory
+ * misaligned for TMA and computed nothing.) */
+/* 1 (default): the forward / data-gradient convolution runs as a persistent
+ * warp-specialised kernel (TMA loads of the activation tiles into a two-stage
+ * ring, tcgen05 MMAs into two TMEM accumulators, epilogue warps draining the
+ * previous tile) where the image width allows one TMA box per half tile
+ * (W <= 124); 0: one CTA per tile that stages, multiplies and writes in turn.
+ * Both give the same values. */
+int pfb_conv_set_pipeline(int on);
 
 /* ---- relaxation measurements and crops of a pfb_sim2d system ---------------
  * (binary32 pools only; PFB_E_CONFIG otherwise) */

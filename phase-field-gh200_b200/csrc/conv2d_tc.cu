@@ -28,8 +28,10 @@
 // same MMAs. Each CTA reduces a range of positions of one image into TMEM
 // and writes its partial sums; a second kernel adds the partials in a fixed
 // order, so the result is deterministic.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <cstdint>
 #include <mutex>
@@ -205,6 +207,236 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3x3_fwd(const __grid_const
                         make_float4(acc[4 * h], acc[4 * h + 1], acc[4 * h + 2], acc[4 * h + 3]);
             }
             }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, NCOLS);
+}
+
+// ---- forward, persistent and warp-specialised ----------------------------------
+// The same contraction as k_conv3x3_fwd with the three stages of a tile in
+// separate warps so that they overlap across tiles: warp 0 loads a tile's
+// chunk planes with TMA (cp.async.bulk.tensor, a 4D view of the activations:
+// 8 channels x channel chunk x position x image, so positions outside the
+// image arrive as zeros) into a two-stage ring; warp 1 issues the tile's
+// tcgen05 MMAs into one of two TMEM accumulators and commits; warps 2-5
+// (one TMEM lane quadrant each) run the epilogue of the previous tile. The
+// packed weights are staged once per CTA with one bulk copy. Each CTA walks
+// tiles c, c + G, c + 2G, ... of the B x tiles work list.
+constexpr int kWsThreads = 192;
+constexpr int kWsStages = 2;
+
+// rows per TMA box: half the staged rows, rounded up to 8 (two boxes per plane)
+__host__ __device__ constexpr int ws_box(int W) { return round_up((fwd_rows(W) + 1) / 2, 8); }
+__host__ __device__ constexpr int ws_plane(int W) { return round_up(2 * ws_box(W) * 16, 128); }
+
+template <int CIN, int COUT>
+__host__ __device__ constexpr int ws_smem(int W) {
+    return 1024 + kWsStages * (CIN / 8) * ws_plane(W) + 9 * (CIN / 8) * COUT * 16;
+}
+
+struct WsHeader {
+    uint64_t full[kWsStages], empty[kWsStages], acc_full[2], acc_empty[2], wbar;
+    uint32_t tmem_slot;
+    int fail;
+};
+
+__device__ __forceinline__ void tma_load4(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2,
+                                          int c3, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
+        : "memory");
+}
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(kWsThreads)
+    k_conv3x3_fwd_ws(const __grid_constant__ ConvFwdArgs A, const __grid_constant__ CUtensorMap X) {
+    static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= 64, "channel counts");
+    constexpr int NCA = CIN / 8;
+    constexpr uint32_t NCOLS = 2 * fwd_tmem_cols<COUT>();  // two accumulators
+    constexpr uint32_t ACC = fwd_tmem_cols<COUT>();
+    extern __shared__ __align__(1024) unsigned char smem[];
+    WsHeader& H = *reinterpret_cast<WsHeader*>(smem);
+    const int W2 = A.W + 2;
+    const int P2 = (A.H + 2) * W2;
+    const int CH = ws_plane(A.W);
+    const int BOX = ws_box(A.W);
+    unsigned char* sA = smem + 1024;                                // stages x planes
+    unsigned char* sW = sA + (size_t)kWsStages * NCA * CH;          // packed weights
+    const uint32_t sa = dev::smem_addr(sA), sw = dev::smem_addr(sW);
+    const uint32_t stage_bytes = (uint32_t)(NCA * 2 * BOX * 16);
+    const uint32_t wbytes = (uint32_t)(9 * NCA * COUT * 16);
+
+    const int tid = (int)threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int items = A.B * A.tiles;
+    const int q_end = (A.H + 1) * W2;
+
+    // every TMA destination below is 128-byte aligned when the dynamic
+    // shared memory is; refuse to run otherwise
+    if (dev::smem_addr(smem) & 127u) {
+        if (tid == 0) atomicOr(&g_conv_status, 2u);
+        return;
+    }
+    if (tid == 0) {
+        for (int s = 0; s < kWsStages; ++s) {
+            dev::mbar_init(&H.full[s], 1);
+            dev::mbar_init(&H.empty[s], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            dev::mbar_init(&H.acc_full[a], 1);
+            dev::mbar_init(&H.acc_empty[a], 4);  // one arrival per epilogue warp
+        }
+        dev::mbar_init(&H.wbar, 1);
+        H.fail = 0;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        dev::mbar_arrive_expect_tx(&H.wbar, wbytes);
+        dev::bulk_g2s(sW, A.w, wbytes, &H.wbar);
+    }
+    if (warp == 0) {
+        tc::tmem_alloc(&H.tmem_slot, NCOLS);
+        tc::tmem_relinquish();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = H.tmem_slot;
+    auto give_up = [&]() {
+        H.fail = 1;
+        atomicOr(&g_conv_status, 1u);
+    };
+
+    if (warp == 0 && lane == 0) {
+        // ---- producer: chunk planes of each tile, two boxes per plane
+        int k = 0;
+        for (int it = (int)blockIdx.x; it < items && !H.fail; it += (int)gridDim.x, ++k) {
+            const int s = k % kWsStages;
+            if (!dev::mbar_wait_bounded(&H.empty[s], (uint32_t)(((k / kWsStages) & 1) ^ 1), tc::kMmaWaitPolls)) {
+                give_up();
+                break;
+            }
+            const int b = it / A.tiles, t = it - b * A.tiles;
+            const int qa = t * (kConvMT * 128) - 1;  // first staged position (W2 + t 256 - (W2 + 1))
+            const uint32_t bar = dev::smem_addr(&H.full[s]);
+            dev::mbar_arrive_expect_tx(&H.full[s], stage_bytes);
+            for (int c = 0; c < NCA; ++c)
+                for (int h = 0; h < 2; ++h)
+                    tma_load4(sa + (uint32_t)((s * NCA + c) * CH + h * BOX * 16), &X, 0, c, qa + h * BOX, b,
+                              bar);
+        }
+        // no copy may still target shared memory at exit
+        for (int j = (k > kWsStages ? k - kWsStages : 0); j < k; ++j)
+            (void)dev::mbar_wait_bounded(&H.full[j % kWsStages], (uint32_t)((j / kWsStages) & 1),
+                                         tc::kMmaWaitPolls);
+    } else if (warp == 1 && lane == 0) {
+        // ---- MMA issue
+        if (!dev::mbar_wait_bounded(&H.wbar, 0, tc::kMmaWaitPolls)) give_up();
+        constexpr uint32_t idesc = tc::idesc_bf16_f32(128, COUT, false, false);
+        int k = 0;
+        for (int it = (int)blockIdx.x; it < items && !H.fail; it += (int)gridDim.x, ++k) {
+            const int s = k % kWsStages, a = k & 1;
+            if (!dev::mbar_wait_bounded(&H.full[s], (uint32_t)((k / kWsStages) & 1), tc::kMmaWaitPolls) ||
+                !dev::mbar_wait_bounded(&H.acc_empty[a], (uint32_t)(((k >> 1) & 1) ^ 1), tc::kMmaWaitPolls)) {
+                give_up();
+                break;
+            }
+            tc::fence_after_sync();
+            const uint32_t st = sa + (uint32_t)(s * NCA * CH);
+            for (int m = 0; m < kConvMT; ++m)
+                for (int tap = 0; tap < 9; ++tap) {
+                    const int dy = tap / 3, dx = tap - 3 * (tap / 3);
+                    const int row = m * 128 + dy * W2 + dx;
+                    for (int ks = 0; ks < CIN / 16; ++ks) {
+                        const uint64_t ad =
+                            tc::smem_desc(st + (uint32_t)(2 * ks * CH + row * 16), (uint32_t)CH, 128u);
+                        const uint64_t bd = tc::smem_desc(sw + (uint32_t)((tap * NCA + 2 * ks) * COUT * 16),
+                                                          (uint32_t)(COUT * 16), 128u);
+                        tc::mma_bf16(tmem + (uint32_t)(a * ACC + m * COUT), ad, bd, idesc,
+                                     (tap | ks) ? 1u : 0u);
+                    }
+                }
+            tc::mma_commit(&H.empty[s]);     // the stage may be refilled
+            tc::mma_commit(&H.acc_full[a]);  // the accumulator may be read
+        }
+        // no MMA may still be writing TMEM when it is released
+        if (k > 0)
+            (void)dev::mbar_wait_bounded(&H.acc_full[(k - 1) & 1], (uint32_t)(((k - 1) >> 1) & 1),
+                                         tc::kMmaWaitPolls);
+    } else if (warp >= 2) {
+        // ---- epilogue: TMEM lane quadrant warp % 4
+        const int quad = warp & 3;
+        const int r = quad * 32 + lane;
+        int k = 0;
+        for (int it = (int)blockIdx.x; it < items; it += (int)gridDim.x, ++k) {
+            const int a = k & 1;
+            const bool ok = dev::mbar_wait_bounded(&H.acc_full[a], (uint32_t)((k >> 1) & 1), tc::kMmaWaitPolls);
+            if (!__all_sync(0xFFFFFFFFu, ok) || H.fail) {
+                if (lane == 0 && !ok) give_up();
+                break;
+            }
+            tc::fence_after_sync();
+            const int b = it / A.tiles, t = it - b * A.tiles;
+            const int q0 = W2 + t * (kConvMT * 128);
+            for (int m = 0; m < kConvMT; ++m) {
+                float acc[COUT];
+                __syncwarp();  // the TMEM loads are warp-collective
+#pragma unroll
+                for (int h = 0; h < COUT / 16; ++h) {
+                    uint32_t v[16];
+                    tc::tmem_ld16(tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * ACC + m * COUT + 16 * h), v);
+                    tc::tmem_wait_ld();
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) acc[16 * h + j] = __uint_as_float(v[j]);
+                }
+                const int q = q0 + m * 128 + r;
+                if (q >= q_end) continue;
+                const int xp = q % W2;
+                const bool interior = xp >= 1 && xp <= A.W;
+                const size_t o = ((size_t)b * P2 + q) * COUT;
+                float g[COUT];
+#pragma unroll
+                for (int j = 0; j < COUT; ++j) g[j] = 1.0f;
+                if (A.gate && interior) {
+#pragma unroll
+                    for (int h = 0; h < COUT / 8; ++h) {
+                        const uint4 gv = *reinterpret_cast<const uint4*>(A.gate + o + 8 * h);
+                        const bf16* ge = reinterpret_cast<const bf16*>(&gv);
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) g[8 * h + j] = __bfloat162float(ge[j]) > 0.0f ? 1.0f : 0.0f;
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < COUT; ++j) {
+                    float v = acc[j];
+                    if (A.bias) v += A.bias[j];
+                    if (A.relu) v = fmaxf(v, 0.0f);
+                    v *= g[j];
+                    acc[j] = interior ? v : 0.0f;
+                }
+                if (A.y) {
+#pragma unroll
+                    for (int h = 0; h < COUT / 8; ++h) {
+                        uint4 pk;
+                        __nv_bfloat162* p2 = reinterpret_cast<__nv_bfloat162*>(&pk);
+#pragma unroll
+                        for (int j = 0; j < 4; ++j)
+                            p2[j] = __floats2bfloat162_rn(acc[8 * h + 2 * j], acc[8 * h + 2 * j + 1]);
+                        *reinterpret_cast<uint4*>(A.y + o + 8 * h) = pk;
+                    }
+                }
+                if (A.yf) {
+#pragma unroll
+                    for (int h = 0; h < COUT / 4; ++h)
+                        *reinterpret_cast<float4*>(A.yf + o + 4 * h) =
+                            make_float4(acc[4 * h], acc[4 * h + 1], acc[4 * h + 2], acc[4 * h + 3]);
+                }
+            }
+            // the accumulator is free again
+            tc::fence_before_sync();
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(dev::smem_addr(&H.acc_empty[a])) : "memory");
         }
     }
     tc::fence_before_sync();
@@ -404,12 +636,73 @@ __global__ void k_pack_weights(const float* __restrict__ w, bf16* __restrict__ p
 }
 
 template <int CIN, int COUT>
+cudaError_t launch_fwd_ws(const ConvFwdArgs& a, cudaStream_t s, bool* used);
+
+template <int CIN, int COUT>
 cudaError_t launch_fwd(const ConvFwdArgs& a, cudaStream_t s) {
+    bool used = false;
+    cudaError_t e0 = launch_fwd_ws<CIN, COUT>(a, s, &used);
+    if (e0 != cudaSuccess || used) return e0;
     const int smem = fwd_smem<CIN, COUT>(a.W);
     cudaError_t e = cudaFuncSetAttribute(k_conv3x3_fwd<CIN, COUT>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     k_conv3x3_fwd<CIN, COUT><<<a.B * a.tiles, kConvThreads, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+// 1: the persistent warp-specialised forward where the width allows it
+int g_conv_pipeline = 1;
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// The persistent forward; *used = false (nothing launched) when the shape or
+// the driver does not allow it.
+template <int CIN, int COUT>
+cudaError_t launch_fwd_ws(const ConvFwdArgs& a, cudaStream_t s, bool* used) {
+    *used = false;
+    const int smem = ws_smem<CIN, COUT>(a.W);
+    PFN_cuTensorMapEncodeTiled_v12000 encode = encode_tiled();
+    if (!g_conv_pipeline || !encode || ws_box(a.W) > 256 || smem > 227 * 1024) return cudaSuccess;
+    const int P2 = (a.H + 2) * (a.W + 2);
+    // activations [B][P2][CIN] as 8 channels x CIN/8 chunks x P2 positions x B images
+    const cuuint64_t dims[4] = {8, (cuuint64_t)(CIN / 8), (cuuint64_t)P2, (cuuint64_t)a.B};
+    const cuuint64_t strides[3] = {16, (cuuint64_t)CIN * 2, (cuuint64_t)P2 * CIN * 2};
+    const cuuint32_t box[4] = {8, 1, (cuuint32_t)ws_box(a.W), 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUtensorMap map;
+    if (encode(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(a.x), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(k_conv3x3_fwd_ws<CIN, COUT>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    int per = 0, dev = 0, sms = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_conv3x3_fwd_ws<CIN, COUT>, kWsThreads,
+                                                           smem)) != cudaSuccess ||
+        (e = cudaGetDevice(&dev)) != cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+        return e;
+    // every resident CTA must get its TMEM columns (512 per SM)
+    const int cols = 2 * (int)fwd_tmem_cols<COUT>();
+    per = per < 512 / cols ? per : 512 / cols;
+    if (per < 1) return cudaSuccess;
+    const int items = a.B * a.tiles;
+    const int grid = items < sms * per ? items : sms * per;
+    k_conv3x3_fwd_ws<CIN, COUT><<<grid, kWsThreads, smem, s>>>(a, map);
+    *used = true;
     return cudaGetLastError();
 }
 
@@ -568,6 +861,11 @@ int pfb_conv3x3_wgrad(const void* x, const void* dy, float* workspace, size_t wo
 }
 
 int pfb_conv_status(unsigned* out, int clear) { return pfb::conv_read_status(out, clear); }
+
+int pfb_conv_set_pipeline(int on) {
+    pfb::g_conv_pipeline = on ? 1 : 0;
+    return PFB_OK;
+}
 
 }  // extern "C"
 

@@ -15,6 +15,7 @@ _abi._SIGS.update({
     "pfb_conv3x3_wgrad": (I, [P, P, P, C.c_size_t, P, P, I, I, I, I, I, P]),
     "pfb_conv3x3_wgrad_noalloc": (I, [P, P, P, P, I, I, I, I, I, P]),
     "pfb_conv_status": (I, [C.POINTER(C.c_uint), I]),
+    "pfb_conv_set_pipeline": (C.c_int, [C.c_int]),
     "pfb_sim2d_residual_step": (I, [P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "pfb_sur2d_extract": (I, [P, P, P, P]),
     "pfb_sur2d_extract_at": (I, [P, P, P, C.c_float, P, P]),

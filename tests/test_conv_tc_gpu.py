@@ -179,3 +179,33 @@ def test_rejects_unbuilt_channels_and_small_workspace():
         check(lib().pfb_conv3x3_forward(8, 16, None, 32, None, None, 1, 8, 8, 8, 32, 0, None), "f")
     with pytest.raises(pfb200.PfbError):
         check(lib().pfb_conv3x3_wgrad(16, 16, 16, 4, 16, None, 1, 8, 8, 32, 32, None), "w")
+
+
+@pytest.mark.parametrize("cin,cout,B,H,W", [(32, 32, 600, 32, 32), (16, 32, 40, 64, 64),
+                                            (32, 16, 7, 30, 124), (32, 32, 3, 20, 126)])
+def test_pipelined_forward_equals_one_tile_per_cta(cin, cout, B, H, W):
+    """The persistent warp-specialised forward (TMA ring, two TMEM
+    accumulators; W <= 124) and the one-tile-per-CTA kernel give the same
+    bits, including when each CTA walks many tiles (600 images) and at the
+    widths on either side of the TMA box limit."""
+    t = torch()
+    x, w, b = inputs(B, H, W, cin, cout, 5 + cin + W)
+    xd = dev_bf16(co.to_padded(x))
+    p, _ = pack(w, False)
+    bd = dev_f32(b)
+    P2 = (H + 2) * (W + 2)
+    outs = []
+    try:
+        for pipe in (1, 0):
+            check(lib().pfb_conv_set_pipeline(pipe), "pipeline")
+            yf = t.full((B, P2, cout), 7.0, dtype=t.float32, device="cuda")
+            y = t.zeros((B, P2, cout), dtype=t.bfloat16, device="cuda")
+            check(lib().pfb_conv3x3_forward(xd.data_ptr(), y.data_ptr(), yf.data_ptr(), p.data_ptr(),
+                                            bd.data_ptr(), None, B, H, W, cin, cout, 1, None), "forward")
+            t.cuda.synchronize()
+            assert status_ok()
+            outs.append((yf.cpu().numpy(), y.float().cpu().numpy()))
+    finally:
+        check(lib().pfb_conv_set_pipeline(1), "pipeline")
+    assert outs[0][0].tobytes() == outs[1][0].tobytes()
+    assert outs[0][1].tobytes() == outs[1][1].tobytes()
