@@ -594,6 +594,60 @@ WORKLOAD_CS = ("passive relaxation (v_A = 0) of a 1024^2 periodic lattice with 4
                "of the learned surrogate judged by the plain solver")
 
 
+def profile_conv_layers(local, batch=512, repeats=20):
+    """One JSON line per U-Net layer shape (channels in -> out, crop edge):
+    the median CUDA-event time of one pfb_conv3x3_forward (bias, ReLU,
+    bfloat16 output) over `repeats` launches after 3 warm-up ones, L2
+    flushed by a 256 MB write before each, with the persistent
+    warp-specialised kernel (pipeline mode 2) and with one tile per CTA
+    (mode 0); the useful FLOPs and the activation bytes in and out give the
+    rates."""
+    import torch
+    import pfb200
+    from pfb200 import check
+    L = pfb200.lib()
+    dev = f"cuda:{local}"
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream().cuda_stream
+    try:
+        for cin, cout, h in ((32, 32, 64), (32, 32, 32), (16, 32, 64), (32, 16, 64), (32, 16, 32),
+                             (16, 32, 32), (16, 16, 64)):
+            p2 = (h + 2) * (h + 2)
+            g = torch.Generator(device=dev).manual_seed(cin * 100 + cout + h)
+            x = torch.randn(batch, p2, cin, device=dev, generator=g).to(torch.bfloat16)
+            w = torch.randn(cout, cin, 3, 3, device=dev, generator=g) * 0.1
+            wp = torch.zeros(9 * cin * cout, dtype=torch.bfloat16, device=dev)
+            check(L.pfb_conv3x3_pack(w.data_ptr(), wp.data_ptr(), cin, cout, 0, None), "pack")
+            bias = torch.randn(cout, device=dev, generator=g)
+            y = torch.empty(batch, p2, cout, dtype=torch.bfloat16, device=dev)
+            row = {"layer": f"{cin}->{cout}", "crop": h, "batch": batch}
+            for mode in (0, 2):
+                check(L.pfb_conv_set_pipeline(mode), "pipeline")
+                times = []
+                for it in range(3 + repeats):
+                    flush.zero_()
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record()
+                    check(L.pfb_conv3x3_forward(x.data_ptr(), y.data_ptr(), None, wp.data_ptr(),
+                                                bias.data_ptr(), None, batch, h, h, cin, cout, 1,
+                                                stream), "forward")
+                    e1.record()
+                    torch.cuda.synchronize()
+                    if it >= 3:
+                        times.append(e0.elapsed_time(e1) * 1e3)
+                times.sort()
+                us = times[len(times) // 2]
+                key = "persistent" if mode else "tile_per_cta"
+                row[key + "_us"] = us
+                row[key + "_tflops"] = 2.0 * batch * h * h * 9 * cin * cout / us / 1e6
+                row[key + "_gbs"] = batch * p2 * (cin + cout) * 2 / us / 1e3
+            print(json.dumps(row), flush=True)
+    finally:
+        L.pfb_conv_set_pipeline(1)
+    return 0
+
+
 def run_surrogate(a):
     """The surrogate workload: training data from plain-solver pairs (10 runs x
     5 pairs x 400 cells = 20,000 crops, increments over 8,000 steps, inputs
@@ -609,6 +663,8 @@ def run_surrogate(a):
         return 0
     torch.cuda.set_device(local)
     pfb200.lib().pfb_conv_set_pipeline(a.conv_pipeline)
+    if a.profile_layers:
+        return profile_conv_layers(local)
     if a.profile_forward:
         net = sg.Surrogate2D(max_batch=512, seed=1, device=local)
         ms = net.bench_forward(512, 3)
@@ -747,8 +803,12 @@ def main():
     ap.add_argument("--repeats", type=int, default=3, help="cs: relaxations per method (median)")
     ap.add_argument("--max-steps", type=int, default=150000,
                     help="cs: plain solver steps after which a relaxation gives up")
-    ap.add_argument("--conv-pipeline", type=int, default=1, choices=[0, 1],
-                    help="cs: 1 the persistent warp-specialised forward convolution, 0 one tile per CTA")
+    ap.add_argument("--conv-pipeline", type=int, default=1, choices=[0, 1, 2],
+                    help="cs: forward convolution kernel: 2 persistent warp-specialised for every "
+                         "channel pair, 1 for the 32 -> 32 pair only, 0 one tile per CTA")
+    ap.add_argument("--profile-layers", action="store_true",
+                    help="cs: time each U-Net layer shape's forward convolution with both kernels "
+                         "and exit")
     ap.add_argument("--profile-forward", action="store_true",
                     help="cs: only 3 forward passes and 2 training steps of the U-Net on 512 "
                          "zero crops (a short command for ncu)")

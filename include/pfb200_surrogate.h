@@ -89,13 +89,16 @@ int pfb_conv3x3_wgrad_noalloc(const void* x, const void* dy, float* dw_oihw, flo
 int pfb_conv_status(unsigned* out, int clear);
 /* (pfb_conv_status bit 1: the persistent forward found its shared memory
  * misaligned for TMA and computed nothing.) */
-/* 1 (default): the forward / data-gradient convolution runs as a persistent
- * warp-specialised kernel (TMA loads of the activation tiles into a two-stage
- * ring, tcgen05 MMAs into two TMEM accumulators, epilogue warps draining the
- * previous tile) where the image width allows one TMA box per half tile
- * (W <= 124); 0: one CTA per tile that stages, multiplies and writes in turn.
- * Both give the same values. */
-int pfb_conv_set_pipeline(int on);
+/* Forward / data-gradient kernel choice. 2: every built channel pair runs as
+ * a persistent warp-specialised kernel (TMA loads of the activation tiles
+ * into a two-stage ring, tcgen05 MMAs into two TMEM accumulators, epilogue
+ * warps draining the previous tile) where the image width allows one TMA box
+ * per half tile (W <= 124); 1 (default): the persistent kernel for the
+ * 32 -> 32 pair only, the one where it is faster (124 vs 134 us at 512 x 64^2
+ * on a B200; 7-27 % slower at 16 -> 32, 32 -> 16 and 16 -> 16); 0: one CTA per
+ * tile that stages, multiplies and writes in turn. All give the same values.
+ * PFB_E_ARG for any other mode. */
+int pfb_conv_set_pipeline(int mode);
 
 /* ---- relaxation measurements and crops of a pfb_sim2d system ---------------
  * (binary32 pools only; PFB_E_CONFIG otherwise) */

@@ -122,3 +122,17 @@ def test_3d_launchers_reject_bad_arguments_without_touching_a_device():
     m.layout = u.layout
     m.storage.z_cap = 8
     assert L.pfb3d_measure_cells_only(C.byref(m), None) == -3  # compact storage
+
+
+def test_conv_pipeline_modes():
+    """pfb_conv_set_pipeline takes 0, 1 (default) and 2 and rejects the rest
+    without touching a device."""
+    L = pfb200.lib()
+    try:
+        for mode in (0, 2, 1):
+            assert L.pfb_conv_set_pipeline(mode) == 0
+        assert L.pfb_conv_set_pipeline(3) == -1
+        assert L.pfb_conv_set_pipeline(-1) == -1
+        assert b"pipeline" in L.pfb_last_error()
+    finally:
+        L.pfb_conv_set_pipeline(1)
