@@ -384,6 +384,18 @@ int pfb_sim2d_set_state(pfb_sim2d* s, const pfb_cell2d* cells,
                         const float* phi, long long step);
 /* Pack the per-cell trajectory record into host memory `out` (N records). */
 int pfb_sim2d_pack_traj(pfb_sim2d* s, pfb_traj_cell2d* out);
+/* Advance `steps` steps and, after every `every`-th step of this call, pack
+ * the trajectory records (as pfb_sim2d_pack_traj) and copy them to frame
+ * k % frames of `ring` (frames x N records), k = 0, 1, ... counting this
+ * call's records: the driver loop of the reference's trajectory output
+ * (src/sim.cu:864-930, --trajectory-interval) without a host wait per record.
+ * Returns once the work is queued on the simulator's stream; the ring holds
+ * the frames after pfb_sim2d_sync. `ring` should be page-locked host memory
+ * for the copies to run asynchronously. Six-step graphs replace single
+ * launches where no record falls inside the six steps. PFB_E_ARG for a null
+ * ring, every < 1, frames < 1 or steps < 0. */
+int pfb_sim2d_advance_record(pfb_sim2d* s, long long steps, int every, pfb_traj_cell2d* ring,
+                             int frames);
 /* In-memory device checkpoint (no reference counterpart): save copies the
  * current pool, cells, aggregate and flags into buffers of the system
  * (allocated on the first save); restore returns to that step exactly as a

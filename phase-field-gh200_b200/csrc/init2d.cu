@@ -366,6 +366,44 @@ __global__ void k_pack_traj2d(const pfb_cell2d* __restrict__ cell, const uint8_t
         out[n] = traj_record(cell[n], (int)clsv[n], L);
 }
 
+// Trajectory frames written by the device straight into page-locked host
+// memory (the records of one frame leave each CTA as consecutive 16-byte
+// chunks, so the host link sees full-width writes). Every CTA reads the
+// ring's frame counter first; the last CTA to finish advances it, so frames
+// follow each other in stream order, graph replays included.
+constexpr int kRingThreads = 128;
+static_assert(sizeof(pfb_traj_cell2d) == 48, "trajectory record is three 16-byte chunks");
+
+__global__ void k_ring_begin(TrajRing2D* r, pfb_traj_cell2d* base, int frames) {
+    r->base = base;
+    r->frames = frames;
+    r->k = 0ull;
+    r->arrived = 0u;
+}
+
+__global__ void __launch_bounds__(kRingThreads)
+    k_pack_traj2d_ring(const pfb_cell2d* __restrict__ cell, const uint8_t* __restrict__ clsv,
+                       TrajRing2D* ring, int N, int L) {
+    __shared__ uint4 stage[kRingThreads * 3];
+    const TrajRing2D rg = *ring;
+    uint4* dst = reinterpret_cast<uint4*>(rg.base + (size_t)(rg.k % (unsigned long long)rg.frames) * N);
+    for (int n0 = (int)blockIdx.x * kRingThreads; n0 < N; n0 += (int)gridDim.x * kRingThreads) {
+        const int n = n0 + (int)threadIdx.x;
+        if (n < N) reinterpret_cast<pfb_traj_cell2d*>(stage)[threadIdx.x] = traj_record(cell[n], (int)clsv[n], L);
+        __syncthreads();
+        const int chunks = 3 * min(kRingThreads, N - n0);
+        for (int i = (int)threadIdx.x; i < chunks; i += kRingThreads) dst[(size_t)3 * n0 + i] = stage[i];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&ring->arrived, 1u) == gridDim.x - 1) {
+            ring->arrived = 0u;
+            ring->k = rg.k + 1ull;
+        }
+    }
+}
+
 int launch_status(const char* what) {
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return set_error(PFB_E_CUDA, "%s: %s", what, cudaGetErrorString(e));
@@ -457,6 +495,21 @@ int pack_traj2d(const pfb_cell2d* cell, const uint8_t* cls, pfb_traj_cell2d* out
     if (N == 0) return PFB_OK;
     k_pack_traj2d<<<std::min((N + 127) / 128, 148 * 4), 128, 0, s>>>(cell, cls, out, N, L);
     return launch_status("pack_traj2d");
+}
+
+int ring_begin2d(TrajRing2D* ring, pfb_traj_cell2d* base, int frames, cudaStream_t s) {
+    if (!ring || !base || frames < 1 || ((uintptr_t)base & 15u))
+        return set_error(PFB_E_ARG, "ring_begin2d: bad argument");
+    k_ring_begin<<<1, 1, 0, s>>>(ring, base, frames);
+    return launch_status("ring_begin2d");
+}
+
+int pack_traj2d_ring(const pfb_cell2d* cell, const uint8_t* cls, TrajRing2D* ring, int N, int L,
+                     cudaStream_t s) {
+    if (!cell || !cls || !ring || N < 1 || L <= 0) return set_error(PFB_E_ARG, "pack_traj2d_ring: bad argument");
+    k_pack_traj2d_ring<<<std::min((N + kRingThreads - 1) / kRingThreads, 148), kRingThreads, 0, s>>>(
+        cell, cls, ring, N, L);
+    return launch_status("pack_traj2d_ring");
 }
 
 int init2d_read_status(unsigned* out, int clear) {

@@ -116,6 +116,17 @@ int verify_cells2d(const float* phi, const pfb_cell2d* cell, const uint8_t* cls,
 int verify_S(const uint32_t* S, size_t n, uint32_t* out_max, cudaStream_t s);
 int pack_traj2d(const pfb_cell2d* cell, const uint8_t* cls, pfb_traj_cell2d* out, int N, int L,
                 cudaStream_t s);
+// A ring of trajectory frames in page-locked host memory (device-visible
+// address), filled by pack_traj2d_ring: frame k goes to base + (k % frames) * N.
+struct TrajRing2D {
+    pfb_traj_cell2d* base;
+    unsigned long long k;     // frames packed so far in this call
+    int frames;
+    unsigned int arrived;     // CTAs of the running pack that are done
+};
+int ring_begin2d(TrajRing2D* ring, pfb_traj_cell2d* base, int frames, cudaStream_t s);
+int pack_traj2d_ring(const pfb_cell2d* cell, const uint8_t* cls, TrajRing2D* ring, int N, int L,
+                     cudaStream_t s);
 
 // sim2d.cu: device-side view of a pfb_sim2d for the relaxation tools
 struct Sim2DView {

@@ -55,6 +55,11 @@ struct pfb_sim2d {
     bool graph_ready = false;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
+    // six-step graphs that also pack a trajectory frame into the host ring
+    // after every `every`-th step, [every - 1][phase] for every = 1, 2, 3, 6
+    // and the call's step count modulo `every` at the graph's start
+    cudaGraphExec_t rec_exec[6][6] = {};
+    TrajRing2D* d_ring = nullptr;
     Velocity2D* vel = nullptr;  // open PFVMOM4 recorder
     Boundary2D* bnd = nullptr;  // open PFB recorder
     uint32_t* d_perm = nullptr;  // Morton visit order (null: launch order)
@@ -93,6 +98,9 @@ struct pfb_sim2d {
         if (bnd) (void)boundary2d_close(bnd);
         if (graph_exec) cudaGraphExecDestroy(graph_exec);
         if (graph) cudaGraphDestroy(graph);
+        for (auto& row : rec_exec)
+            for (cudaGraphExec_t& e : row)
+                if (e) cudaGraphExecDestroy(e);
         if (stream) cudaStreamDestroy(stream);
         cudaFree(d_phi[0]);
         cudaFree(d_phi[1]);
@@ -103,6 +111,7 @@ struct pfb_sim2d {
         cudaFree(d_step);
         cudaFree(d_flags);
         cudaFree(d_traj);
+        cudaFree(d_ring);
         cudaFree(d_perm);
         cudaFree(d_cell_prev);
         cudaFree(d_bins);
@@ -228,6 +237,37 @@ struct pfb_sim2d {
         graph_exec = nullptr;
         graph = nullptr;
         graph_ready = false;
+        for (auto& row : rec_exec)
+            for (cudaGraphExec_t& e : row) {
+                if (e) cudaGraphExecDestroy(e);
+                e = nullptr;
+            }
+    }
+
+    // The six steps of the plain graph with a ring frame packed after local
+    // step s whenever (phase + s + 1) is a multiple of `every` (every
+    // divides 6, 0 <= phase < every).
+    int build_record_graph(int every, int phase) {
+        if (const int rc = settle_bins()) return rc;
+        PFB_CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        int rc = PFB_OK;
+        for (int s = 0; s < 6 && rc == PFB_OK; ++s) {
+            rc = launch_one(s);
+            if (rc == PFB_OK && (phase + s + 1) % every == 0)
+                rc = pack_traj2d_ring(d_cell, d_cls, d_ring, N, L, stream);
+        }
+        bins_pending = false;
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(stream, &g);
+        if (rc != PFB_OK) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        PFB_CU(e, "end capture");
+        const cudaError_t ie = cudaGraphInstantiateWithFlags(&rec_exec[every - 1][phase], g, 0);
+        cudaGraphDestroy(g);
+        PFB_CU(ie, "graph instantiate");
+        return PFB_OK;
     }
 
     int build_graph() {
@@ -289,6 +329,71 @@ struct pfb_sim2d {
         }
         // nothing stays pending across calls: the caller may read flags or
         // change the field next
+        return settle_bins();
+    }
+
+    // `steps` steps with the trajectory records of every `every`-th step
+    // written to ring frame k % frames (k = 0, 1, ... in this call), all
+    // queued without a host wait. A ring in page-locked memory is written by
+    // the device directly, and six-step graphs carry the records where the
+    // interval divides six; any other ring gets a copy after each pack.
+    // Plain six-step graphs run where no record falls inside the six steps.
+    int advance_record(long long steps, int every, pfb_traj_cell2d* ring, int frames) {
+        const size_t frame_bytes = (size_t)N * sizeof(pfb_traj_cell2d);
+        pfb_traj_cell2d* dring = nullptr;
+        cudaPointerAttributes at{};
+        if (cudaPointerGetAttributes(&at, ring) == cudaSuccess && at.type == cudaMemoryTypeHost &&
+            at.devicePointer && !((uintptr_t)at.devicePointer & 15u))
+            dring = static_cast<pfb_traj_cell2d*>(at.devicePointer);
+        (void)cudaGetLastError();  // an unregistered pointer is not an error here
+        if (dring) {
+            if (!d_ring) PFB_CU(cudaMalloc(&d_ring, sizeof(TrajRing2D)), "alloc ring");
+            if (const int rc = ring_begin2d(d_ring, dring, frames, stream)) return rc;
+        }
+        const bool rec_graph = dring && !vel && use_graph && 6 % every == 0;
+        long long done = 0, k = 0;
+        while (done < steps) {
+            const bool aligned = !vel && use_graph && steps_done % 6 == 0 && steps - done >= 6;
+            if (rec_graph && aligned) {
+                const int phase = (int)(done % every);
+                if (!rec_exec[every - 1][phase]) {
+                    if (const int rc = build_record_graph(every, phase)) return rc;
+                }
+                PFB_CU(cudaGraphLaunch(rec_exec[every - 1][phase], stream), "graph launch");
+                bins_pending = variant == 0 || variant == 1;
+                steps_done += 6;
+                done += 6;
+                continue;
+            }
+            if (!vel && use_graph && !graph_ready) {
+                const int rc = build_graph();
+                if (rc) return rc;
+            }
+            // next record after step index `due` of this call (1-based)
+            const long long due = (done / every + 1) * every;
+            if (aligned && graph_ready && due >= done + 6) {
+                PFB_CU(cudaGraphLaunch(graph_exec, stream), "graph launch");
+                bins_pending = variant == 0 || variant == 1;
+                steps_done += 6;
+                done += 6;
+            } else {
+                const int rc = vel ? launch_observed() : launch_one((int)(steps_done % 6));
+                if (rc) return rc;
+                steps_done += 1;
+                done += 1;
+            }
+            if (done % every == 0) {
+                if (dring) {
+                    if (const int rc = pack_traj2d_ring(d_cell, d_cls, d_ring, N, L, stream)) return rc;
+                } else {
+                    if (const int rc = pack_traj2d(d_cell, d_cls, d_traj, N, L, stream)) return rc;
+                    PFB_CU(cudaMemcpyAsync(reinterpret_cast<unsigned char*>(ring) + (size_t)(k % frames) * frame_bytes,
+                                           d_traj, frame_bytes, cudaMemcpyDeviceToHost, stream),
+                           "download traj");
+                }
+                ++k;
+            }
+        }
         return settle_bins();
     }
 
@@ -842,6 +947,14 @@ int pfb_sim2d_pack_traj(pfb_sim2d* s, pfb_traj_cell2d* out) {
                            cudaMemcpyDeviceToHost, s->stream), "download traj");
     PFB_CU(cudaStreamSynchronize(s->stream), "sync");
     return PFB_OK;
+}
+
+int pfb_sim2d_advance_record(pfb_sim2d* s, long long steps, int every, pfb_traj_cell2d* ring,
+                             int frames) {
+    if (!s || steps < 0 || every < 1 || !ring || frames < 1)
+        return set_error(PFB_E_ARG, "advance_record: bad argument");
+    PFB_CU(cudaSetDevice(s->device), "cudaSetDevice");
+    return s->advance_record(steps, every, ring, frames);
 }
 
 int pfb_sim2d_bench(pfb_sim2d* s, int warmup, int steps, double* ms_per_step) {

@@ -240,6 +240,17 @@ class Sim2D:
         check(lib().pfb_sim2d_pack_traj(self._h, ptr(out)), "pack_traj")
         return out
 
+    def advance_record(self, steps: int, every: int, ring: np.ndarray) -> None:
+        """Advance `steps` steps, copying the trajectory records of every
+        `every`-th step into frame k % len(ring) of `ring` (a TRAJ_DTYPE array
+        of shape (frames, num_cells), ideally in page-locked memory) without a
+        host wait; the frames are valid after sync()."""
+        if ring.dtype != TRAJ_DTYPE or ring.ndim != 2 or ring.shape[1] != self.num_cells or \
+                not ring.flags.c_contiguous:
+            raise ValueError("ring must be a C-contiguous (frames, num_cells) TRAJ_DTYPE array")
+        check(lib().pfb_sim2d_advance_record(self._h, steps, every, ptr(ring), ring.shape[0]),
+              "advance_record")
+
     def set_state(self, cells: np.ndarray, phi: np.ndarray, step: int) -> None:
         cells = np.ascontiguousarray(cells, dtype=CELL_DTYPE)
         phi = np.ascontiguousarray(phi, dtype=np.float32)
