@@ -503,36 +503,52 @@ def run_ensemble(a):
     # trajectory records of all replicas read back, the final fields read back
     e2e = None
     if not a.no_e2e:
-        from pfb200._abi import check, lib
+        from pfb200._abi import TRAJ_DTYPE, check, lib
         views = [ens.system(r) for r in range(len(ps))]
         up = [(torch.from_numpy(v.cells().view(np.uint8).copy()).pin_memory(),
                torch.from_numpy(np.ascontiguousarray(v.phi())).pin_memory()) for v in views]
-        trajs = [torch.empty((p.num_cells, 48), dtype=torch.uint8).pin_memory() for p in ps]
         outs = [torch.empty_like(u[1]).pin_memory() for u in up]
+        chunk = 30
+        total = ens.total_cells
+        # two halves of a page-locked ring of all systems' records: the host
+        # reads one while the device fills the other
+        ring = torch.empty((2, chunk, total * TRAJ_DTYPE.itemsize), dtype=torch.uint8).pin_memory()
+        halves = [ring[h].numpy().view(TRAJ_DTYPE).reshape(chunk, total) for h in range(2)]
+        ext_e = torch.cuda.ExternalStream(ens.stream, device=local)
+        done_ev = [torch.cuda.Event(), torch.cuda.Event()]
+        track = []
         step0 = ens.step
-        e2e_steps = max(6, min(a.steps, 60))
+        e2e_steps = chunk * max(2, min(a.steps, 600) // chunk)
         ens.sync()
         barrier()
         t0 = time.perf_counter()
         for v, (c_h, p_h) in zip(views, up):
             check(lib().pfb_sim2d_set_state(v._h, c_h.data_ptr(), p_h.data_ptr(), step0),
                   "set_state")
-        for _ in range(e2e_steps):
-            ens.advance(1)
-            for v, t in zip(views, trajs):
-                check(lib().pfb_sim2d_pack_traj(v._h, t.data_ptr()), "pack_traj")
+        for c in range(e2e_steps // chunk):
+            ens.advance_record(chunk, 1, halves[c % 2])
+            done_ev[c % 2].record(ext_e)
+            if c:
+                done_ev[(c - 1) % 2].synchronize()
+                f = halves[(c - 1) % 2]
+                track.append((f["cx"].mean(axis=1), f["cy"].mean(axis=1)))
         for v, o in zip(views, outs):
             check(lib().pfb_sim2d_get_phi(v._h, o.data_ptr()), "get_phi")
         ens.sync()
         el = max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{local}")
+        f = halves[(e2e_steps // chunk - 1) % 2]
+        track.append((f["cx"].mean(axis=1), f["cy"].mean(axis=1)))
+        assert len(track) * chunk == e2e_steps
         h2d = sum(c.numel() + p_.numel() * p_.element_size() for c, p_ in up)
-        d2h = sum(t.numel() for t in trajs) * e2e_steps + sum(o.numel() * o.element_size() for o in outs)
+        d2h = total * TRAJ_DTYPE.itemsize * e2e_steps + sum(o.numel() * o.element_size() for o in outs)
         e2e = {"value": world * sites * e2e_steps / el, "unit": "site-cell updates/s",
                "h2d_bytes_per_step": h2d / e2e_steps, "d2h_bytes_per_step": d2h / e2e_steps,
                "steps": e2e_steps,
                "note": "host wall clock; states of all replicas uploaded from pinned memory, "
-                       "one batched launch per step, every replica's trajectory records read "
-                       "back every step, final fields read back"}
+                       "one batched launch per step, every replica's trajectory records of every "
+                       "step written to a page-locked ring (pfb_ens2d_advance_record, 30-step "
+                       "chunks, two halves read on the host while the next chunk runs), final "
+                       "fields read back"}
     cpu = None
     if world == 1 and a.cpu_steps > 0 and a.phi_storage == 0:
         # one time step of every replica on the OpenMP restatement (oracle/)

@@ -469,10 +469,18 @@ int pfb_ens2d_set_cluster(pfb_ens2d* e, int cluster);
  * steps advance the systems). */
 int pfb_ens2d_autotune(pfb_ens2d* e, int steps, int* chosen);
 int pfb_ens2d_advance(pfb_ens2d* e, int steps);
+/* pfb_sim2d_advance_record for every system at once: frame k of `ring`
+ * (frames x total records) holds system 0's records, then system 1's, and so
+ * on, packed by one launch for all systems after every `every`-th step. */
+int pfb_ens2d_advance_record(pfb_ens2d* e, long long steps, int every, pfb_traj_cell2d* ring,
+                             int frames);
 /* The same steps launched one system at a time (the baseline the batched
  * launch is measured against). */
 int pfb_ens2d_advance_serial(pfb_ens2d* e, int steps);
 int pfb_ens2d_sync(pfb_ens2d* e);
+/* The ensemble's CUDA stream (cudaStream_t), on which its steps and
+ * recordings are queued. */
+void* pfb_ens2d_stream(pfb_ens2d* e);
 long long pfb_ens2d_step(const pfb_ens2d* e);
 /* System r as a pfb_sim2d handle owned by the ensemble (after finishing the
  * ensemble's queued work): use pfb_sim2d_get_* on it; do not destroy it. */

@@ -404,6 +404,42 @@ __global__ void __launch_bounds__(kRingThreads)
     }
 }
 
+// The same for many systems in one launch: global record g belongs to the
+// last system r with src[r].off <= g; the frame holds `total` records.
+__global__ void __launch_bounds__(kRingThreads)
+    k_pack_traj2d_ring_batch(const TrajSource2D* __restrict__ src, int R, int total, TrajRing2D* ring) {
+    __shared__ uint4 stage[kRingThreads * 3];
+    const TrajRing2D rg = *ring;
+    uint4* dst = reinterpret_cast<uint4*>(rg.base + (size_t)(rg.k % (unsigned long long)rg.frames) * total);
+    for (int g0 = (int)blockIdx.x * kRingThreads; g0 < total; g0 += (int)gridDim.x * kRingThreads) {
+        const int g = g0 + (int)threadIdx.x;
+        if (g < total) {
+            int lo = 0, hi = R - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (src[mid].off <= g)
+                    lo = mid;
+                else
+                    hi = mid - 1;
+            }
+            const TrajSource2D& t = src[lo];
+            const int n = g - t.off;
+            reinterpret_cast<pfb_traj_cell2d*>(stage)[threadIdx.x] = traj_record(t.cell[n], (int)t.cls[n], t.L);
+        }
+        __syncthreads();
+        const int chunks = 3 * min(kRingThreads, total - g0);
+        for (int i = (int)threadIdx.x; i < chunks; i += kRingThreads) dst[(size_t)3 * g0 + i] = stage[i];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&ring->arrived, 1u) == gridDim.x - 1) {
+            ring->arrived = 0u;
+            ring->k = rg.k + 1ull;
+        }
+    }
+}
+
 int launch_status(const char* what) {
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return set_error(PFB_E_CUDA, "%s: %s", what, cudaGetErrorString(e));
@@ -510,6 +546,13 @@ int pack_traj2d_ring(const pfb_cell2d* cell, const uint8_t* cls, TrajRing2D* rin
     k_pack_traj2d_ring<<<std::min((N + kRingThreads - 1) / kRingThreads, 148), kRingThreads, 0, s>>>(
         cell, cls, ring, N, L);
     return launch_status("pack_traj2d_ring");
+}
+
+int pack_traj2d_ring_batch(const TrajSource2D* src, int R, int total, TrajRing2D* ring, cudaStream_t s) {
+    if (!src || R < 1 || total < 1 || !ring) return set_error(PFB_E_ARG, "pack_traj2d_ring_batch: bad argument");
+    k_pack_traj2d_ring_batch<<<std::min((total + kRingThreads - 1) / kRingThreads, 148), kRingThreads, 0, s>>>(
+        src, R, total, ring);
+    return launch_status("pack_traj2d_ring_batch");
 }
 
 int init2d_read_status(unsigned* out, int clear) {

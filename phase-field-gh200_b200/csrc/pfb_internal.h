@@ -125,6 +125,15 @@ struct TrajRing2D {
     unsigned int arrived;     // CTAs of the running pack that are done
 };
 int ring_begin2d(TrajRing2D* ring, pfb_traj_cell2d* base, int frames, cudaStream_t s);
+// One system of a batched pack: its records go to positions off .. off+N-1
+// of each frame.
+struct TrajSource2D {
+    const pfb_cell2d* cell;
+    const uint8_t* cls;
+    int L;
+    int off;
+};
+int pack_traj2d_ring_batch(const TrajSource2D* src, int R, int total, TrajRing2D* ring, cudaStream_t s);
 int pack_traj2d_ring(const pfb_cell2d* cell, const uint8_t* cls, TrajRing2D* ring, int N, int L,
                      cudaStream_t s);
 

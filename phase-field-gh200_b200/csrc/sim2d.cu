@@ -1015,12 +1015,23 @@ struct pfb_ens2d {
     bool tables_ready = false;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
+    // trajectory recording: sources of the batched pack (system order), the
+    // ring header, a device frame for pageable rings, record graphs
+    // [every - 1][phase] as pfb_sim2d's
+    TrajSource2D* d_src = nullptr;
+    TrajRing2D* d_ring = nullptr;
+    pfb_traj_cell2d* d_frame = nullptr;
+    int total_cells = 0;
+    cudaGraphExec_t rec_exec[6][6] = {};
 
     ~pfb_ens2d() {
         drop_graph();
         if (stream) cudaStreamDestroy(stream);
         cudaFree(d_args);
         cudaFree(d_start);
+        cudaFree(d_src);
+        cudaFree(d_ring);
+        cudaFree(d_frame);
         for (pfb_sim2d* s : sims) delete s;
     }
 
@@ -1031,6 +1042,111 @@ struct pfb_ens2d {
         if (graph) cudaGraphDestroy(graph);
         graph_exec = nullptr;
         graph = nullptr;
+        for (auto& row : rec_exec)
+            for (cudaGraphExec_t& e : row) {
+                if (e) cudaGraphExecDestroy(e);
+                e = nullptr;
+            }
+    }
+
+    // The pack sources in system order (buffers are fixed for the life of
+    // the ensemble).
+    int build_sources() {
+        std::vector<TrajSource2D> h((size_t)R());
+        int off = 0;
+        for (int r = 0; r < R(); ++r) {
+            h[(size_t)r] = TrajSource2D{sims[(size_t)r]->d_cell, sims[(size_t)r]->d_cls, sims[(size_t)r]->L, off};
+            off += sims[(size_t)r]->N;
+        }
+        total_cells = off;
+        PFB_CU(cudaMalloc(&d_src, h.size() * sizeof(TrajSource2D)), "alloc sources");
+        PFB_CU(cudaMalloc(&d_ring, sizeof(TrajRing2D)), "alloc ring");
+        PFB_CU(cudaMalloc(&d_frame, (size_t)total_cells * sizeof(pfb_traj_cell2d)), "alloc frame");
+        PFB_CU(cudaMemcpyAsync(d_src, h.data(), h.size() * sizeof(TrajSource2D), cudaMemcpyHostToDevice,
+                               stream),
+               "upload sources");
+        PFB_CU(cudaStreamSynchronize(stream), "sources");
+        return PFB_OK;
+    }
+
+    int pack() { return pack_traj2d_ring_batch(d_src, R(), total_cells, d_ring, stream); }
+
+    int build_record_graph(int every, int phase) {
+        PFB_CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        int rc = PFB_OK;
+        for (int s = 0; s < 6 && rc == PFB_OK; ++s) {
+            rc = launch_slot(s);
+            if (rc == PFB_OK && (phase + s + 1) % every == 0) rc = pack();
+        }
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(stream, &g);
+        if (rc != PFB_OK) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        PFB_CU(e, "end capture");
+        const cudaError_t ie = cudaGraphInstantiateWithFlags(&rec_exec[every - 1][phase], g, 0);
+        cudaGraphDestroy(g);
+        PFB_CU(ie, "graph instantiate");
+        return PFB_OK;
+    }
+
+    // `steps` steps with every system's trajectory records of every
+    // `every`-th step in ring frame k % frames (frames x total_cells records,
+    // system r after the earlier systems' cells).
+    int advance_record(long long steps, int every, pfb_traj_cell2d* ring, int frames) {
+        if (!tables_ready) {
+            if (const int rc = build_tables()) return rc;
+        }
+        if (!d_src) {
+            if (const int rc = build_sources()) return rc;
+        }
+        const size_t frame_bytes = (size_t)total_cells * sizeof(pfb_traj_cell2d);
+        pfb_traj_cell2d* dring = nullptr;
+        cudaPointerAttributes at{};
+        if (cudaPointerGetAttributes(&at, ring) == cudaSuccess && at.type == cudaMemoryTypeHost &&
+            at.devicePointer && !((uintptr_t)at.devicePointer & 15u))
+            dring = static_cast<pfb_traj_cell2d*>(at.devicePointer);
+        (void)cudaGetLastError();  // an unregistered pointer is not an error here
+        if (const int rc = ring_begin2d(d_ring, dring ? dring : d_frame, dring ? frames : 1, stream)) return rc;
+        const bool rec_graph = dring && 6 % every == 0;
+        long long done = 0, k = 0;
+        while (done < steps) {
+            const bool aligned = steps_done % 6 == 0 && steps - done >= 6;
+            if (rec_graph && aligned) {
+                const int phase = (int)(done % every);
+                if (!rec_exec[every - 1][phase]) {
+                    if (const int rc = build_record_graph(every, phase)) return rc;
+                }
+                PFB_CU(cudaGraphLaunch(rec_exec[every - 1][phase], stream), "graph launch");
+                steps_done += 6;
+                done += 6;
+                continue;
+            }
+            const long long due = (done / every + 1) * every;
+            if (aligned && due >= done + 6) {
+                if (!graph_exec) {
+                    if (const int rc = build_graph()) return rc;
+                }
+                PFB_CU(cudaGraphLaunch(graph_exec, stream), "graph launch");
+                steps_done += 6;
+                done += 6;
+            } else {
+                if (const int rc = launch_slot((int)(steps_done % 6))) return rc;
+                steps_done += 1;
+                done += 1;
+            }
+            if (done % every == 0) {
+                if (const int rc = pack()) return rc;
+                if (!dring)
+                    PFB_CU(cudaMemcpyAsync(reinterpret_cast<unsigned char*>(ring) + (size_t)(k % frames) * frame_bytes,
+                                           d_frame, frame_bytes, cudaMemcpyDeviceToHost, stream),
+                           "download traj");
+                ++k;
+            }
+        }
+        for (pfb_sim2d* s : sims) s->steps_done = steps_done;
+        return PFB_OK;
     }
 
     // Argument tables for the six slots and the CTA offsets for `cluster`.
@@ -1186,6 +1302,15 @@ int pfb_ens2d_advance(pfb_ens2d* e, int steps) {
     if (!e || steps < 0) return set_error(PFB_E_ARG, "advance: bad argument");
     PFB_CU(cudaSetDevice(e->device), "cudaSetDevice");
     return e->advance(steps);
+}
+
+void* pfb_ens2d_stream(pfb_ens2d* e) { return e ? (void*)e->stream : nullptr; }
+
+int pfb_ens2d_advance_record(pfb_ens2d* e, long long steps, int every, pfb_traj_cell2d* ring, int frames) {
+    if (!e || steps < 0 || every < 1 || !ring || frames < 1)
+        return set_error(PFB_E_ARG, "advance_record: bad argument");
+    PFB_CU(cudaSetDevice(e->device), "cudaSetDevice");
+    return e->advance_record(steps, every, ring, frames);
 }
 
 int pfb_ens2d_advance_serial(pfb_ens2d* e, int steps) {

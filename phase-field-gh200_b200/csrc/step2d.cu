@@ -38,13 +38,26 @@
 namespace pfb {
 
 // Block shape: threads per CTA and the CTAs per SM the register budget is
-// sized for (overridable at build time to sweep launch shapes).
+// sized for (overridable at build time to sweep launch shapes). By default
+// the budget follows the shared-memory limit of the staged band: 2 CTAs per
+// SM at clusters of 2 (96 registers), 3 at clusters of 4 and 8 (72).
 #ifndef PFB_STEP2D_THREADS
 #define PFB_STEP2D_THREADS 288
 #endif
-#ifndef PFB_STEP2D_MINB
-#define PFB_STEP2D_MINB 3
+#ifdef PFB_STEP2D_MINB
+__host__ __device__ constexpr int min_blocks(int) { return PFB_STEP2D_MINB; }
+#else
+__host__ __device__ constexpr int min_blocks(int k) { return k == 2 ? 2 : 3; }
 #endif
+// Rows per iteration of the pass-1 and pass-2 strip loops (0: by cluster
+// size, 3 rows of pass 2 at clusters of 2 where the registers allow, else 1).
+#ifndef PFB_STEP2D_P1_UNROLL
+#define PFB_STEP2D_P1_UNROLL 1  // pass 1 stays rolled
+#endif
+#ifndef PFB_STEP2D_P2_UNROLL
+#define PFB_STEP2D_P2_UNROLL 0
+#endif
+__host__ __device__ constexpr int row_unroll(int v, int k) { return v > 0 ? v : (k == 2 ? 3 : 1); }
 // L2 eviction priorities (bit 0: the staged phi_in and S_rd rows are read
 // evict-first).
 #ifndef PFB_STEP2D_L2HINTS
@@ -109,23 +122,84 @@ template <int CLS, int K> struct QuadMap {
 // Euler update of four consecutive pixels of one row from the rolling
 // three-row window (s = row above, c = this row, n = row below; w/e are the
 // pixels left and right of the four).
+//
+// Pixels (0, 1) and (2, 3) are updated as pairs with the sm_100 packed
+// binary32 instructions (__ffma2_rn, __fadd2_rn, __fmul2_rn; each half
+// rounds exactly as the scalar instruction). The operation sequence is the
+// one the compiler gives rhs_pixel_m and lap9 as scalars, contractions
+// included, measured on a B200 to agree bit for bit on 2^22 random inputs:
+//   lap = fma(-20, c, fma(4, s1, s2)) * (1/6)  (s1, s2 summed left to right)
+//   a   = fma(-(rep*phi), S_other, fma(vol, phi, fma(gam, lap, -(dw*X))))
+//   rhs = fma(mrel, a, -fma(vx, gx, vy*gy)),  phi' = fma(dt, rhs, phi)
+// with X = (phi*(1-phi))*fma(-2, phi, 1). Negated coefficients are exact
+// sign flips of the scalar products. The shifted neighbours of the
+// Laplacian sums and of gx are not register pairs, so those stay scalar.
+struct PairCoeffs {
+    float gam, dwC, volC, repC, vx, vy, mrel, dt;
+};
+
+__device__ __forceinline__ float2 dup(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 neg2(float2 v) { return make_float2(-v.x, -v.y); }
+
+template <int J>
+__device__ __forceinline__ float2 update_pair(const float (&S)[6], const float (&C)[6],
+                                              const float (&N)[6], float2 so, const PairCoeffs& k) {
+    const float2 ns = __fadd2_rn(make_float2(N[J + 1], N[J + 2]), make_float2(S[J + 1], S[J + 2]));
+    const float s1a = __fadd_rn(__fadd_rn(ns.x, C[J + 2]), C[J]);
+    const float s1b = __fadd_rn(__fadd_rn(ns.y, C[J + 3]), C[J + 1]);
+    const float s2a = __fadd_rn(__fadd_rn(__fadd_rn(N[J + 2], N[J]), S[J + 2]), S[J]);
+    const float s2b = __fadd_rn(__fadd_rn(__fadd_rn(N[J + 3], N[J + 1]), S[J + 3]), S[J + 1]);
+    const float2 phi = make_float2(C[J + 1], C[J + 2]);
+    float2 t = __ffma2_rn(dup(4.0f), make_float2(s1a, s1b), make_float2(s2a, s2b));
+    t = __ffma2_rn(dup(-20.0f), phi, t);
+    const float2 lap = __fmul2_rn(t, dup((float)(1.0 / 6.0)));
+    const float2 gx = __fmul2_rn(dup(0.5f), make_float2(__fsub_rn(C[J + 2], C[J]), __fsub_rn(C[J + 3], C[J + 1])));
+    const float2 gy = __fmul2_rn(dup(0.5f),
+                                 __fadd2_rn(make_float2(N[J + 1], N[J + 2]), neg2(make_float2(S[J + 1], S[J + 2]))));
+    const float2 om = __fadd2_rn(dup(1.0f), neg2(phi));
+    const float2 tp = __ffma2_rn(dup(-2.0f), phi, dup(1.0f));
+    const float2 X = __fmul2_rn(__fmul2_rn(phi, om), tp);
+    float2 a = __ffma2_rn(dup(k.gam), lap, __fmul2_rn(dup(-k.dwC), X));
+    a = __ffma2_rn(dup(k.volC), phi, a);
+    a = __ffma2_rn(__fmul2_rn(dup(-k.repC), phi), so, a);
+    const float2 adv = __ffma2_rn(dup(k.vx), gx, __fmul2_rn(dup(k.vy), gy));
+    const float2 rhs = __ffma2_rn(dup(k.mrel), a, neg2(adv));
+    return __ffma2_rn(dup(k.dt), rhs, phi);
+}
+
+// Packed pairs at clusters of 2 (96 registers); the scalar form at 4 and 8,
+// where the packed one spills under the 72-register budget (both give the
+// same bits). 0 selects the scalar form everywhere.
+#ifndef PFB_STEP2D_PACKED
+#define PFB_STEP2D_PACKED 1
+#endif
+
+template <bool PACKED>
 __device__ __forceinline__ void stencil4(float ws, float4 vs, float es, float wc, float4 vc,
                                          float ec, float wn, float4 vn, float en,
-                                         const float (&so)[4], float gam, float dwC, float volC,
-                                         float repC, float vx, float vy, float mrel, float dtf,
+                                         const float (&so)[4], const PairCoeffs& k,
                                          float (&pn)[4]) {
     const float S[6] = {ws, vs.x, vs.y, vs.z, vs.w, es};
     const float C[6] = {wc, vc.x, vc.y, vc.z, vc.w, ec};
     const float N[6] = {wn, vn.x, vn.y, vn.z, vn.w, en};
+    if constexpr (PACKED) {
+        const float2 lo = update_pair<0>(S, C, N, make_float2(so[0], so[1]), k);
+        const float2 hi = update_pair<2>(S, C, N, make_float2(so[2], so[3]), k);
+        pn[0] = lo.x;
+        pn[1] = lo.y;
+        pn[2] = hi.x;
+        pn[3] = hi.y;
+    } else {
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const float lap =
-            lap9(N[j], N[j + 1], N[j + 2], C[j], C[j + 1], C[j + 2], S[j], S[j + 1], S[j + 2]);
-        const float gx = 0.5f * (C[j + 2] - C[j]);
-        const float gy = 0.5f * (N[j + 1] - S[j + 1]);
-        const float rhs =
-            rhs_pixel_m(lap, C[j + 1], so[j], gx, gy, gam, dwC, volC, repC, vx, vy, mrel);
-        pn[j] = C[j + 1] + dtf * rhs;
+        for (int j = 0; j < 4; ++j) {
+            const float lap =
+                lap9(N[j], N[j + 1], N[j + 2], C[j], C[j + 1], C[j + 2], S[j], S[j + 1], S[j + 2]);
+            const float gx = 0.5f * (C[j + 2] - C[j]);
+            const float gy = 0.5f * (N[j + 1] - S[j + 1]);
+            const float rhs = rhs_pixel_m(lap, C[j + 1], so[j], gx, gy, k.gam, k.dwC, k.volC,
+                                          k.repC, k.vx, k.vy, k.mrel);
+            pn[j] = C[j + 1] + k.dt * rhs;
+        }
     }
 }
 
@@ -354,6 +428,9 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
     // H rows tall; rows run in a rolled loop with a three-row register window.
     using QM = QuadMap<CLS, K>;
     constexpr int H = QM::H;
+    constexpr int kRowsP1 = row_unroll(PFB_STEP2D_P1_UNROLL, K);
+    constexpr int kRowsP2 = row_unroll(PFB_STEP2D_P2_UNROLL, K);
+    constexpr bool kPacked = PFB_STEP2D_PACKED && K == 2;
     const bool active = !abort && tid < QM::NQ * QM::G;
     const int x0 = 4 * (tid % QM::NQ);
     const int r0 = (tid / QM::NQ) * H;
@@ -373,7 +450,7 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
         load_row(r0, wc, vc, ec);
         uint32_t* qrow = ps_s + (r0 + 1) * PX + soff + x0;
         uint32_t neg = 0u;
-#pragma unroll 1
+#pragma unroll kRowsP1
         for (int r = 0; r < nr; ++r) {
             float wn, en;
             float4 vn;
@@ -413,6 +490,7 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
     const float gam = P.gam, dwC = P.dwC, volC = P.volC;
     const float vx = sh.red.vx, vy = sh.red.vy, mrel = P.mrel;
     const float repC = A.rep_coeff, dtf = A.dt;
+    const PairCoeffs kc{gam, dwC, volC, repC, vx, vy, mrel, dtf};
     const int sx = P.sx, sy = P.sy;
     const int dwx = P.dwx, dwy = P.dwy, dtx0 = P.dtx0, dty0 = P.dty0;
     const int gx0n = P.gx0n, gy0n = P.gy0n;
@@ -469,7 +547,7 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
                 // overflow checks of a row's atomics run one row later, so the
                 // atomic round trip overlaps the next row's arithmetic
                 uint32_t old_prev[4] = {0u, 0u, 0u, 0u}, q_prev[4] = {0u, 0u, 0u, 0u};
-#pragma unroll 1
+#pragma unroll kRowsP2
                 for (int r = 0; r < nr; ++r) {
                     float wn, en;
                     float4 vn;
@@ -477,8 +555,7 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
                     const float so[4] = {__uint_as_float(qrow[0]), __uint_as_float(qrow[1]),
                                          __uint_as_float(qrow[2]), __uint_as_float(qrow[3])};
                     float pn[4];
-                    stencil4(ws, vs, es, wc, vc, ec, wn, vn, en, so, gam, dwC, volC, repC, vx,
-                             vy, mrel, dtf, pn);
+                    stencil4<kPacked>(ws, vs, es, wc, vc, ec, wn, vn, en, so, kc, pn);
                     // pn becomes the stored value (16-bit pools round here)
                     store4<T>(o, pn, sr_seed, (uint32_t)(o - tile_out));
                     uint32_t* srow = A.S_sc + (size_t)gy * Pp;
@@ -565,8 +642,7 @@ __device__ __forceinline__ void staged_cell(const pfb_step_args2d& A, int n, int
                     const float so[4] = {__uint_as_float(qrow[0]), __uint_as_float(qrow[1]),
                                          __uint_as_float(qrow[2]), __uint_as_float(qrow[3])};
                     float pn[4];
-                    stencil4(ws, vs, es, wc, vc, ec, wn, vn, en, so, gam, dwC, volC, repC, vx,
-                             vy, mrel, dtf, pn);
+                    stencil4<kPacked>(ws, vs, es, wc, vc, ec, wn, vn, en, so, kc, pn);
                     const int b = y0 + r0 + r - sy;
                     if ((unsigned)b < (unsigned)dwy) {
                         int gyn = gy0n + b;
@@ -797,7 +873,7 @@ __device__ __forceinline__ void step_body(const pfb_step_args2d& A, int lb, int 
 }
 
 template <int K, typename T = float, int OBS = PFB_VELOCITY_DISABLED, bool BINS = false>
-__global__ void __launch_bounds__(kThreads, PFB_STEP2D_MINB)
+__global__ void __launch_bounds__(kThreads, min_blocks(K))
     k_step2d(const __grid_constant__ pfb_step_args2d A, const __grid_constant__ BinArgs B) {
     extern __shared__ __align__(128) char smem[];
     step_body<K, T, OBS, BINS>(A, (int)blockIdx.x, (int)gridDim.x, smem, B);
@@ -808,7 +884,7 @@ __global__ void __launch_bounds__(kThreads, PFB_STEP2D_MINB)
 // straddle systems); its arguments are copied into shared memory. All
 // systems of one launch share the pool storage type T.
 template <int K, typename T = float>
-__global__ void __launch_bounds__(kThreads, PFB_STEP2D_MINB)
+__global__ void __launch_bounds__(kThreads, min_blocks(K))
     k_step2d_batch(const pfb_step_args2d* __restrict__ args, const int* __restrict__ block_start,
                    int R) {
     extern __shared__ __align__(128) char smem[];

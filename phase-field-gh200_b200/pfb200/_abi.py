@@ -174,6 +174,8 @@ _SIGS = {
     "pfb_sim2d_set_state": (I, [P, P, P, C.c_longlong]),
     "pfb_sim2d_pack_traj": (I, [P, P]),
     "pfb_sim2d_advance_record": (I, [P, C.c_longlong, I, P, I]),
+    "pfb_ens2d_advance_record": (I, [P, C.c_longlong, I, P, I]),
+    "pfb_ens2d_stream": (P, [P]),
     "pfb_sim2d_save": (I, [P]),
     "pfb_sim2d_restore": (I, [P]),
     "pfb_sim2d_velocity_open": (I, [P, C.c_char_p, I, C.c_longlong, I]),

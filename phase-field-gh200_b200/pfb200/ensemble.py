@@ -6,7 +6,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._abi import Params2D, check, lib
+from ._abi import TRAJ_DTYPE, Params2D, check, lib
 from .sim2d import Sim2D, SimParams2D
 
 
@@ -54,6 +54,25 @@ class Ensemble2D:
 
     def advance(self, steps: int) -> None:
         check(lib().pfb_ens2d_advance(self._h, steps), "advance")
+
+    @property
+    def total_cells(self) -> int:
+        return int(sum(p.num_cells for p in self.params))
+
+    @property
+    def stream(self) -> int:
+        return int(lib().pfb_ens2d_stream(self._h) or 0)
+
+    def advance_record(self, steps: int, every: int, ring: np.ndarray) -> None:
+        """Advance every system `steps` steps; frame k % len(ring) of `ring`
+        (a C-contiguous (frames, total_cells) TRAJ_DTYPE array, ideally in
+        page-locked memory) receives the trajectory records of all systems,
+        system 0 first, after every `every`-th step. Valid after sync()."""
+        if ring.dtype != TRAJ_DTYPE or ring.ndim != 2 or ring.shape[1] != self.total_cells or \
+                not ring.flags.c_contiguous:
+            raise ValueError("ring must be a C-contiguous (frames, total_cells) TRAJ_DTYPE array")
+        check(lib().pfb_ens2d_advance_record(self._h, steps, every, ring.ctypes.data, ring.shape[0]),
+              "advance_record")
 
     def advance_serial(self, steps: int) -> None:
         check(lib().pfb_ens2d_advance_serial(self._h, steps), "advance_serial")

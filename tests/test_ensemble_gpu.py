@@ -65,3 +65,37 @@ def test_autotune_picks_a_cluster_size(storage):
     assert k in ((2, 4, 8) if storage == 0 else (2, 4))
     assert all(int(e.system(r).flags().sum()) == 0 for r in range(len(ps)))
     e.close()
+
+
+@pytest.mark.parametrize("pinned", [True, False], ids=["page-locked", "pageable"])
+@pytest.mark.parametrize("every", [1, 3, 4])
+def test_advance_record_frames(every, pinned):
+    """pfb_ens2d_advance_record: frame k holds every system's trajectory
+    records (system 0 first) after step (k + 1) * every, as each system's
+    pfb_sim2d_pack_traj after one-step advances gives them."""
+    import torch
+    from pfb200._abi import TRAJ_DTYPE
+    ps, cs = make(seed_shift=3)
+    a = pfb200.Ensemble2D(ps, cs)
+    b = pfb200.Ensemble2D(ps, cs)
+    n = 24
+    want = []
+    for _ in range(n):
+        a.advance(1)
+        a.sync()
+        want.append(np.concatenate([a.system(r).traj() for r in range(len(ps))]))
+    frames = n // every
+    if pinned:
+        buf = torch.zeros((frames, b.total_cells * TRAJ_DTYPE.itemsize), dtype=torch.uint8).pin_memory()
+        ring = buf.numpy().view(TRAJ_DTYPE).reshape(frames, b.total_cells)
+    else:
+        ring = np.zeros((frames, b.total_cells), TRAJ_DTYPE)
+    b.advance_record(n, every, ring)
+    b.sync()
+    assert b.step == n
+    for k in range(frames):
+        assert ring[k].tobytes() == want[(k + 1) * every - 1].tobytes(), k
+    for r in range(len(ps)):
+        assert state(a.system(r)) == state(b.system(r))
+    a.close()
+    b.close()
