@@ -595,22 +595,53 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3x3_wgrad(const __grid_con
     if (warp == 0) tc::tmem_dealloc(tmem, NCOLS);
 }
 
-// dW[co][ci][tap] = sum over CTAs of partial[cta][tap][co][ci]; db[co] likewise
-// (fixed CTA order).
-__global__ void k_wgrad_reduce(const float* __restrict__ partial, int grid, int cx, int cy,
-                               float* __restrict__ dw, float* __restrict__ db) {
+// dW[co][ci][tap] = sum over CTAs of partial[cta][tap][co][ci]; db[co] likewise.
+// Two levels in a fixed order: thread row j of a CTA sums the blocks
+// g = j, j + 16, j + 32, ... of 32 consecutive outputs (each warp reads 128
+// contiguous bytes per block), then the 16 row sums are added in row order.
+// The result does not depend on scheduling.
+constexpr int kRedCols = 32, kRedRows = 16;
+
+__global__ void __launch_bounds__(kRedCols * kRedRows)
+    k_wgrad_reduce(const float* __restrict__ partial, int grid, int cx, int cy,
+                   float* __restrict__ dw, float* __restrict__ db) {
+    __shared__ float part[kRedRows][kRedCols + 1];
     const int per = 9 * cy * cx + cy;
-    const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x);
-    if (i >= per) return;
+    const int i = (int)blockIdx.x * kRedCols + (int)threadIdx.x;
+    const int j = (int)threadIdx.y;
     float s = 0.0f;
-    for (int g = 0; g < grid; ++g) s += partial[(size_t)g * per + i];
+    if (i < per) {
+        int g = j;
+        // four independent loads in flight, summed in order
+        for (; g + 3 * kRedRows < grid; g += 4 * kRedRows) {
+            const float a = partial[(size_t)g * per + i];
+            const float b = partial[(size_t)(g + kRedRows) * per + i];
+            const float c = partial[(size_t)(g + 2 * kRedRows) * per + i];
+            const float d = partial[(size_t)(g + 3 * kRedRows) * per + i];
+            s = (((s + a) + b) + c) + d;
+        }
+        for (; g < grid; g += kRedRows) s += partial[(size_t)g * per + i];
+    }
+    part[j][threadIdx.x] = s;
+    __syncthreads();
+    if (j != 0 || i >= per) return;
+    float t = part[0][threadIdx.x];
+#pragma unroll
+    for (int r = 1; r < kRedRows; ++r) t += part[r][threadIdx.x];
     if (i < 9 * cy * cx) {
         const int tap = i / (cy * cx), rem = i - tap * cy * cx;
         const int co = rem / cx, ci = rem - co * cx;
-        dw[((size_t)co * cx + ci) * 9 + tap] = s;
+        dw[((size_t)co * cx + ci) * 9 + tap] = t;
     } else if (db) {
-        db[i - 9 * cy * cx] = s;
+        db[i - 9 * cy * cx] = t;
     }
+}
+
+void launch_wgrad_reduce(const float* partial, int grid, int cx, int cy, float* dw, float* db,
+                         cudaStream_t s) {
+    const int per = 9 * cy * cx + cy;
+    k_wgrad_reduce<<<(per + kRedCols - 1) / kRedCols, dim3(kRedCols, kRedRows), 0, s>>>(partial, grid, cx,
+                                                                                        cy, dw, db);
 }
 
 // Packed weights from OIHW binary32 W[co][ci][3][3] (cout x cin):
@@ -799,8 +830,7 @@ int conv3x3_wgrad(const void* x, const void* dy, float* workspace, size_t worksp
     else
         return set_error(PFB_E_CONFIG, "conv3x3_wgrad: channels %d, %d not built", cx, cy);
     if (e != cudaSuccess) return set_error(PFB_E_CUDA, "conv3x3_wgrad: %s", cudaGetErrorString(e));
-    const int per = 9 * cy * cx + cy;
-    k_wgrad_reduce<<<(per + 255) / 256, 256, 0, s>>>(workspace, B * a.ctas, cx, cy, dw, db);
+    launch_wgrad_reduce(workspace, B * a.ctas, cx, cy, dw, db, s);
     e = cudaGetLastError();
     if (e != cudaSuccess) return set_error(PFB_E_CUDA, "wgrad reduce: %s", cudaGetErrorString(e));
     return PFB_OK;
